@@ -1,0 +1,341 @@
+"""Benchmark of the cuda backend's database scan (GCUPS), one JSON line on rank 0.
+
+Workload (one "step"): the protein SW ScoreEnd scan of 16 queries (lengths 100, 250, 500, 1000,
+5000 cycled) against a resident database of 500,000 sequences (log-normal lengths, median 300,
+sigma 0.8, clipped to 20..35,000; residues i.i.d. from a fixed seeded background; a seeded
+symmetric 20x20 matrix with diagonal U[4,11] and off-diagonal U[-4,3]; gap_open 11, gap_ext 1).
+All inputs are seeded synthetic data of that shape. GCUPS counts real cells only:
+sum over queries and targets of |q| * |t| per second.
+
+`value` is timed on the device (CUDA events on the scan's stream, inputs resident in HBM);
+`e2e` goes through the public host API (hy_scan: query host->device, hit device->host per call).
+Under torchrun each rank holds its own 500,000-sequence shard of an N-times larger database
+(weak scaling) and the per-shard best hits are all-gathered over NCCL and reduced with the
+reference's tie-break (highest score, then smallest global index).
+
+--impl reference times the CPU baseline instead: a C++ restatement of hyalite's AVX2 backend
+(oracle/avx2_port.cpp) over all host threads, on a bounded sample of the same database.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+QUERY_LENGTHS = [100, 250, 500, 1000, 5000]
+N_QUERIES = 16
+N_SEQS = 500_000
+GO, GE = 11, 1
+AL = 20
+
+
+def make_workload(seed: int, n_seqs: int = N_SEQS):
+    """The config-2 generator: seeded matrix, background, lengths, residues and queries."""
+    rng = np.random.default_rng(seed)
+    base = np.random.default_rng(12345)  # the matrix and background are fixed across shards
+    mat = base.integers(-4, 4, size=(AL, AL))
+    mat = np.triu(mat) + np.triu(mat, 1).T
+    mat[np.diag_indices(AL)] = base.integers(4, 12, size=AL)
+    background = base.dirichlet(np.full(AL, 4.0))
+    lengths = np.clip(np.round(np.exp(math.log(300.0) + 0.8 * rng.standard_normal(n_seqs))), 20, 35_000).astype(np.int64)
+    offsets = np.zeros(n_seqs + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum(lengths)
+    residues = rng.choice(AL, size=int(offsets[-1]), p=background).astype(np.uint8)
+    qrng = np.random.default_rng(777)
+    queries = [qrng.choice(AL, size=QUERY_LENGTHS[i % len(QUERY_LENGTHS)], p=background).astype(np.uint8)
+               for i in range(N_QUERIES)]
+    return mat.reshape(-1).astype(np.int32), residues, offsets, queries
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_run(mat, residues, offsets, queries, sample_seqs, threads, steps=1, warmup=0):
+    """The AVX2 restatement over `threads` host threads on the first `sample_seqs` sequences;
+    returns (GCUPS, seconds per step, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    off = offsets[: sample_seqs + 1]
+    res = residues[: int(off[-1])]
+    db = pyoracle.Avx2Db(res, off, mat, AL, GO, GE, 0, 1, max(len(q) for q in queries))
+    qlist = [list(map(int, q)) for q in queries]
+    cells = float(sum(len(q) for q in queries)) * float(off[-1])
+    for _ in range(warmup):
+        db.scan_many(qlist, threads)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        db.scan_many(qlist, threads)
+    dt = (time.perf_counter() - t0) / steps
+    return cells / dt / 1e9, dt, (f"{N_QUERIES} queries ({'/'.join(map(str, QUERY_LENGTHS))} aa, cycled) against the "
+                                  f"first {sample_seqs} of the {N_SEQS} sequences ({int(off[-1])} residues)")
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    mat, residues, offsets, queries = make_workload(args.seed, n_seqs=args.ref_seqs)
+    threads = os.cpu_count() or 1
+    gcups, dt, sample = cpu_baseline_run(mat, residues, offsets, queries, args.ref_seqs, threads,
+                                         steps=args.steps, warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": "GCUPS", "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "i8/i16/i32 lanes (AVX2)", "data": "synthetic",
+        "config": {"workload": "config 2: protein SW ScoreEnd scan (bounded sample)", "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_cuda(args):
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import hyalite_b200 as hy
+    from hyalite_b200 import _abi
+
+    lib = _abi.lib
+    mat, residues, offsets, queries = make_workload(args.seed + rank)
+    n_seqs = len(offsets) - 1
+    t_build = time.perf_counter()
+    db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
+          .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(max(QUERY_LENGTHS)).build())
+    build_s = time.perf_counter() - t_build
+    sc = hy.Scratch(db)
+    n16, n32 = db.partition()
+    total_res = float(offsets[-1])
+    cells_step = float(sum(len(q) for q in queries)) * total_res  # this rank's shard
+    # i16/i32 residue split for the roofline's per-launch cells
+    lens = np.diff(offsets.astype(np.int64))
+
+    stream = torch.cuda.ExternalStream(sc.stream_ptr())
+    d_queries = [torch.from_numpy(q).to(f"cuda:{local}") for q in queries]
+    d_hits = torch.zeros((N_QUERIES, 32), dtype=torch.uint8, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    def device_step():
+        for i, q in enumerate(d_queries):
+            st = lib.hy_scan_device(db._h, sc._h, C.c_void_p(q.data_ptr()), len(queries[i]),
+                                    C.c_void_p(d_hits[i].data_ptr()))
+            if st != 0:
+                raise hy.Error.from_status(st)
+
+    def gather_best(hits_dev):
+        if world == 1:
+            return hits_dev
+        import torch.distributed as dist
+
+        out = [torch.empty_like(hits_dev) for _ in range(world)]
+        with torch.cuda.stream(stream):
+            dist.all_gather(out, hits_dev)
+        return out
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        device_step()
+        gather_best(d_hits)
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    lib.hy_scratch_profile(sc._h, 1)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        device_step()
+        gather_best(d_hits)
+    end.record(stream)
+    torch.cuda.synchronize()
+    kms = (C.c_double * 2)()
+    kl = (C.c_uint64 * 2)()
+    all_l = C.c_uint64()
+    lib.hy_scratch_profile_read(sc._h, kms, kl, C.byref(all_l))
+    lib.hy_scratch_profile(sc._h, 0)
+    clk = clocks.stop()
+    elapsed_ms = start.elapsed_time(end)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([elapsed_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    barrier()
+
+    # ---- e2e: the public host API, host buffers, copies inside the timed region ----
+    host_queries = [bytes(q) for q in queries]
+    for _ in range(1):
+        for q in host_queries:
+            db.scan(sc, q)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        hits = [db.scan(sc, q) for q in host_queries]
+        if world > 1:
+            import torch.distributed as dist
+
+            hb = torch.tensor([[h.score, h.db_index + rank * n_seqs] for h in hits], dtype=torch.int64,
+                              device=f"cuda:{local}")
+            allh = [torch.empty_like(hb) for _ in range(world)]
+            dist.all_gather(allh, hb)
+            _ = [max(((int(a[i, 0]), -int(a[i, 1])) for a in allh)) for i in range(N_QUERIES)]
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    # ---- roofline of the dominant kernel (int16x2 pair kernel) ----
+    peak = C.c_double()
+    lib.hy_measure_dpx_peak(C.byref(peak))
+    peak_gcups = peak.value / 1e9
+    # int16-partition cells per launch: all residues except the int32 partition's
+    sorted_lens = np.sort(lens)  # the int32 partition is the longest sequences
+    res32 = float(sorted_lens[len(sorted_lens) - n32:].sum()) if n32 else 0.0
+    res16 = total_res - res32
+    launches16 = max(int(kl[0]), 1)
+    cells16_per_launch = res16 * sum(len(q) for q in queries) / N_QUERIES
+    avg16_ms = kms[0] / launches16
+    achieved = cells16_per_launch / (avg16_ms * 1e-3) / 1e9 if avg16_ms > 0 else 0.0
+    meas = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = meas.get("hbm_gbs", 6650.0)
+
+    total_cells = cells_step * args.steps * world
+    value = total_cells / (elapsed_ms * 1e-3) / 1e9
+    e2e_value = total_cells / e2e_s / 1e9
+
+    if rank == 0:
+        threads = os.cpu_count() or 1
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            g, dt, sample = cpu_baseline_run(mat, residues, offsets, queries, args.cpu_sample_seqs, threads)
+            cpu = {"value": g, "unit": "GCUPS", "cores": threads, "kind": "port", "sample": sample}
+        line = {
+            "metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "i16x2 (int32 for long sequences)",
+            "data": "synthetic (seeded, config-2 generator)",
+            "config": {
+                "workload": "config 2: protein SW ScoreEnd scan, plain per-query form",
+                "n_seqs_per_gpu": n_seqs, "residues_per_gpu": int(total_res), "queries_per_step": N_QUERIES,
+                "query_lengths": QUERY_LENGTHS, "cells_per_step_per_gpu": cells_step,
+                "partition_i16x2_i32": [n16, n32], "db_build_s": round(build_s, 2),
+                "db_device_bytes": db.device_bytes(), "scratch_bytes": db.scratch_bytes(),
+                "l2": "inputs larger than L2 (packed database + boundary rows >> 126 MB)",
+                "parallelism": f"db shards x{world}" if world > 1 else "single GPU",
+            },
+            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": sum(len(q) for q in queries),
+                    "d2h_bytes_per_step": 32 * N_QUERIES},
+            "gpu_launches": int(all_l.value),
+            "roofline": {"bound": "dpx_int16x2", "achieved": achieved, "peak": peak_gcups, "unit": "GCUPS",
+                         "frac": achieved / peak_gcups if peak_gcups else None, "traffic": None,
+                         "kernel": "scan_kernel<Pair16,8,16,SW>", "avg_launch_ms": avg16_ms,
+                         "launches": int(kl[0]), "peak_source": "measured: hy_measure_dpx_peak (register-resident per-cell DPX mix)"},
+            "roofline_hbm": {"bound": "hbm", "peak": hbm_peak, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs" if meas else "fallback"},
+            "clocks": clk,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-sample-seqs", type=int, default=12_000)
+    ap.add_argument("--ref-seqs", type=int, default=12_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

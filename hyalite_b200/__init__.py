@@ -1,0 +1,504 @@
+"""hyalite_b200 -- the B200 `cuda` backend of hyalite's inter-sequence database scan.
+
+A Python mirror of hyalite's public API for this path (src/lib.rs:54-67): ``Scoring``, ``Mode``,
+``SearchType``, ``BestHit``, ``Backend`` / ``BackendChoice`` / ``BACKEND_ENV_VAR``, ``Layout`` /
+``LayoutChoice``, ``ScoreWidth``, ``Database`` / ``DatabaseBuilder`` / ``Scratch`` and
+``align_pairs``, with the same names, argument meanings and error behaviour, over the C ABI of
+include/hyalite_cuda.h. All compute runs in the in-tree CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass
+from typing import Iterable, List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import lib
+
+BACKEND_ENV_VAR = "HYALITE_BACKEND"
+
+
+# ---- errors (src/error.rs:16-96) -----------------------------------------------------------------
+
+class Error(Exception):
+    """A hyalite error. ``kind`` is the variant name of src/error.rs (or a C-ABI-only condition such
+    as ``QueryTooLong`` / ``Cuda``); ``fields`` holds the variant's fields."""
+
+    _FIELDS = {
+        "MatrixShape": ("alphabet_len", "expected", "got"),
+        "NegativeGapPenalty": ("gap_open", "gap_ext"),
+        "GapOpenLessThanExtend": ("gap_open", "gap_ext"),
+        "ScoreRangeTooWide": ("bound",),
+        "SymbolOutOfRange": ("symbol", "alphabet_len"),
+        "BackendUnavailable": ("backend",),
+        "QueryTooLong": ("len", "max"),
+        "Cuda": ("code",),
+    }
+
+    def __init__(self, kind: str, **fields):
+        self.kind = kind
+        self.fields = fields
+        super().__init__(f"{kind}{fields if fields else ''}")
+
+    def __eq__(self, other):
+        return isinstance(other, Error) and (self.kind, self.fields) == (other.kind, other.fields)
+
+    def __hash__(self):
+        return hash((self.kind, tuple(sorted(self.fields.items()))))
+
+    @classmethod
+    def from_status(cls, status: int) -> "Error":
+        kind = _abi.STATUS_NAMES.get(status, f"Status{status}")
+        d = _abi.last_detail()
+        names = cls._FIELDS.get(kind, ())
+        fields = {n: int(d[i]) for i, n in enumerate(names)}
+        if kind == "BackendUnavailable":
+            fields["backend"] = Backend(fields["backend"])
+        return cls(kind, **fields)
+
+
+def _check(status: int) -> None:
+    if status != _abi.OK:
+        raise Error.from_status(status)
+
+
+# ---- enums ----------------------------------------------------------------------------------------
+
+class Mode(enum.IntEnum):
+    """Alignment mode (src/mode.rs:11-27)."""
+    Sw = 0
+    Nw = 1
+    Hw = 2
+    Ov = 3
+    Shw = 4
+
+    def is_local(self) -> bool:
+        return self is Mode.Sw
+
+    def code(self) -> str:
+        return {0: "SW", 1: "NW", 2: "HW", 3: "OV", 4: "SHW"}[int(self)]
+
+    def __str__(self) -> str:
+        return self.code()
+
+
+ALL_MODES = (Mode.Sw, Mode.Nw, Mode.Hw, Mode.Ov, Mode.Shw)
+
+
+class SearchType(enum.IntEnum):
+    """What a search returns (src/search.rs:13-27). ``Alignment`` (traceback) is not built by this
+    backend."""
+    Score = 0
+    ScoreEnd = 1
+
+    def tracks_end(self) -> bool:
+        return self is SearchType.ScoreEnd
+
+
+class ScoreWidth(enum.IntEnum):
+    """src/width.rs:26-34."""
+    I8 = 0
+    I16 = 1
+    I32 = 2
+
+    def max_abs(self) -> int:
+        return {0: 127, 1: 32767, 2: 536870911}[int(self)]
+
+    def bytes(self) -> int:
+        return {0: 1, 1: 2, 2: 4}[int(self)]
+
+
+class Backend(enum.IntEnum):
+    """src/backend.rs:25-36, plus ``Cuda`` (the enum is non-exhaustive upstream)."""
+    Scalar = 0
+    Sse41 = 1
+    Avx2 = 2
+    Neon = 3
+    Cuda = 4
+
+    def name_str(self) -> str:
+        return lib.hy_backend_name(int(self)).decode()
+
+    def is_available(self) -> bool:
+        return bool(lib.hy_backend_is_available(int(self)))
+
+    def __str__(self) -> str:
+        return self.name_str()
+
+
+@dataclass(frozen=True)
+class BackendChoice:
+    """``Auto`` or ``Force(backend)`` (src/backend.rs:123-133)."""
+    forced: Optional[Backend] = None
+
+    @staticmethod
+    def Auto() -> "BackendChoice":
+        return BackendChoice(None)
+
+    @staticmethod
+    def Force(b: Backend) -> "BackendChoice":
+        return BackendChoice(Backend(b))
+
+    @staticmethod
+    def parse(s: str) -> "BackendChoice":
+        """BackendChoice::parse (src/backend.rs:143-155), plus ``"cuda"``."""
+        out = C.c_int()
+        st = lib.hy_backend_parse(s.encode(), C.byref(out))
+        if st != _abi.OK:
+            raise Error("InvalidBackendName", name=s)
+        return BackendChoice.Auto() if out.value == _abi.CHOICE_AUTO else BackendChoice.Force(Backend(out.value))
+
+    def _code(self) -> int:
+        return _abi.CHOICE_AUTO if self.forced is None else int(self.forced)
+
+
+class Layout(enum.IntEnum):
+    """src/inter.rs:317-330. On the device: Gathered interleaves two per-letter query profiles per
+    cell pair."""
+    Gathered = 0
+    Precomputed = 1
+
+
+@dataclass(frozen=True)
+class LayoutChoice:
+    forced: Optional[Layout] = None
+
+    @staticmethod
+    def Auto() -> "LayoutChoice":
+        return LayoutChoice(None)
+
+    @staticmethod
+    def Force(layout: Layout) -> "LayoutChoice":
+        return LayoutChoice(Layout(layout))
+
+    def _code(self) -> int:
+        return _abi.LAYOUT_AUTO if self.forced is None else int(self.forced)
+
+
+@dataclass(frozen=True)
+class BestHit:
+    """src/hit.rs:16-25: 0-based ends, ``None`` when nothing aligned or for ``Score`` searches."""
+    score: int
+    db_index: int
+    query_end: Optional[int]
+    target_end: Optional[int]
+
+    @staticmethod
+    def _from(h: _abi.HyHit) -> "BestHit":
+        return BestHit(int(h.score), int(h.db_index), None if h.query_end < 0 else int(h.query_end),
+                       None if h.target_end < 0 else int(h.target_end))
+
+
+# ---- scoring (src/scoring.rs) ----------------------------------------------------------------------
+
+def _i32_array(values) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.int64)).astype(np.int32)
+
+
+class Scoring:
+    """A validated substitution matrix plus affine gaps (src/scoring.rs:41-100): a gap of length n
+    costs ``gap_open + (n - 1) * gap_ext``."""
+
+    def __init__(self, alphabet_len: int, matrix: Sequence[int], gap_open: int, gap_ext: int):
+        mat = _i32_array(matrix) if len(matrix) else np.zeros(0, dtype=np.int32)
+        _check(lib.hy_scoring_validate(alphabet_len, mat.ctypes.data_as(_abi._i32p), len(mat),
+                                       gap_open, gap_ext))
+        self._al = int(alphabet_len)
+        self._matrix = mat
+        self._go = int(gap_open)
+        self._ge = int(gap_ext)
+
+    @staticmethod
+    def new(alphabet_len, matrix, gap_open, gap_ext) -> "Scoring":
+        return Scoring(alphabet_len, matrix, gap_open, gap_ext)
+
+    def alphabet_len(self) -> int:
+        return self._al
+
+    def gap_open(self) -> int:
+        return self._go
+
+    def gap_ext(self) -> int:
+        return self._ge
+
+    def matrix(self) -> np.ndarray:
+        return self._matrix
+
+    def entry_bounds(self):
+        return int(self._matrix.min()), int(self._matrix.max())
+
+    def score(self, q: int, t: int) -> int:
+        if not (0 <= q < self._al and 0 <= t < self._al):
+            raise IndexError(f"symbol index out of range: q={q}, t={t}, alphabet_len={self._al}")
+        return int(self._matrix[q * self._al + t])
+
+    def required_width(self, mode: Mode, max_query_len: int, max_target_len: int) -> ScoreWidth:
+        lo, hi = self.entry_bounds()
+        return required_width(mode, lo, hi, self._go, self._ge, max_query_len, max_target_len)
+
+    def __eq__(self, other):
+        return (isinstance(other, Scoring) and self._al == other._al and self._go == other._go
+                and self._ge == other._ge and np.array_equal(self._matrix, other._matrix))
+
+
+def required_width(mode, min_entry, max_entry, gap_open, gap_ext, max_query_len, max_target_len):
+    """width::required_width (src/width.rs:145-169)."""
+    w = C.c_int()
+    b = C.c_int64()
+    _check(lib.hy_required_width(int(mode), min_entry, max_entry, gap_open, gap_ext,
+                                 min(int(max_query_len), 2**64 - 1), min(int(max_target_len), 2**64 - 1),
+                                 C.byref(w), C.byref(b)))
+    return ScoreWidth(w.value)
+
+
+# ---- sequences ---------------------------------------------------------------------------------------
+
+def _as_u8(seq) -> np.ndarray:
+    if isinstance(seq, np.ndarray):
+        return np.ascontiguousarray(seq, dtype=np.uint8)
+    if isinstance(seq, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bytes(seq), dtype=np.uint8)
+    return np.asarray(list(seq), dtype=np.int64).astype(np.uint8) if len(seq) else np.zeros(0, np.uint8)
+
+
+def concat(seqs: Iterable) -> tuple:
+    """Concatenate sequences into (residues uint8, offsets uint64 of len n+1)."""
+    parts = [_as_u8(s) for s in seqs]
+    offsets = np.zeros(len(parts) + 1, dtype=np.uint64)
+    if parts:
+        offsets[1:] = np.cumsum([len(p) for p in parts], dtype=np.uint64)
+    residues = np.concatenate(parts) if parts and offsets[-1] > 0 else np.zeros(1, np.uint8)
+    return np.ascontiguousarray(residues, dtype=np.uint8), offsets
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+# ---- database (src/database.rs) ------------------------------------------------------------------------
+
+class Database:
+    """An immutable, device-resident database (src/database.rs:47-63). Shareable across threads;
+    each thread scans with its own ``Scratch``."""
+
+    def __init__(self, handle, n_seqs):
+        self._h = C.c_void_p(handle)
+        self._n = n_seqs
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.hy_db_destroy(h)
+            self._h = C.c_void_p(None)
+
+    @staticmethod
+    def builder() -> "DatabaseBuilder":
+        return DatabaseBuilder()
+
+    # -- scans --
+    def scan(self, scratch: "Scratch", query) -> BestHit:
+        q = _as_u8(query)
+        out = _abi.HyHit()
+        _check(lib.hy_scan(self._h, scratch._h, _ptr(q, _abi._u8p), len(q), C.byref(out)))
+        return BestHit._from(out)
+
+    def scan_all(self, scratch: "Scratch", query, out: list) -> None:
+        arr = self.scan_all_array(scratch, query)
+        out.clear()
+        for h in arr:
+            out.append(BestHit._from(h))
+
+    def scan_all_array(self, scratch: "Scratch", query):
+        q = _as_u8(query)
+        arr = (_abi.HyHit * self._n)()
+        _check(lib.hy_scan_all(self._h, scratch._h, _ptr(q, _abi._u8p), len(q), arr))
+        return arr
+
+    def scan_scores(self, scratch: "Scratch", query, out: list) -> None:
+        res = self.scan_scores_array(scratch, query)
+        out.clear()
+        out.extend(int(x) for x in res)
+
+    def scan_scores_array(self, scratch: "Scratch", query) -> np.ndarray:
+        q = _as_u8(query)
+        res = np.empty(self._n, dtype=np.int32)
+        _check(lib.hy_scan_scores(self._h, scratch._h, _ptr(q, _abi._u8p), len(q), _ptr(res, _abi._i32p)))
+        return res
+
+    # -- accessors (src/database.rs:570-638) --
+    def sequence_count(self) -> int:
+        return self._n
+
+    def mode(self) -> Mode:
+        return Mode(lib.hy_db_mode(self._h))
+
+    def search_type(self) -> SearchType:
+        return SearchType(lib.hy_db_search_type(self._h))
+
+    def score_width(self) -> ScoreWidth:
+        return ScoreWidth(lib.hy_db_score_width(self._h))
+
+    def backend(self) -> Backend:
+        return Backend(lib.hy_db_backend(self._h))
+
+    def layout(self) -> Optional[Layout]:
+        return Layout(lib.hy_db_layout(self._h))
+
+    def max_query_len(self) -> int:
+        return int(lib.hy_db_max_query_len(self._h))
+
+    def max_target_len(self) -> int:
+        return int(lib.hy_db_max_target_len(self._h))
+
+    def device_bytes(self) -> int:
+        return int(lib.hy_db_device_bytes(self._h))
+
+    def scratch_bytes(self) -> int:
+        return int(lib.hy_db_scratch_bytes(self._h))
+
+    def partition(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        lib.hy_db_partition(self._h, C.byref(a), C.byref(b))
+        return int(a.value), int(b.value)
+
+
+class DatabaseBuilder:
+    """DatabaseBuilder (src/database.rs:657-877). Required: sequences, scoring, mode,
+    max_query_len; search_type defaults to Score."""
+
+    def __init__(self):
+        self._seqs = None
+        self._scoring = None
+        self._mode = None
+        self._st = None
+        self._mql = None
+        self._backend = None
+        self._layout = None
+
+    def sequences(self, seqs) -> "DatabaseBuilder":
+        self._seqs = concat(seqs)
+        return self
+
+    def sequences_concat(self, residues: np.ndarray, offsets: np.ndarray) -> "DatabaseBuilder":
+        """The same database given already concatenated: sequence k is
+        residues[offsets[k]:offsets[k+1]]."""
+        res = np.ascontiguousarray(residues, dtype=np.uint8)
+        if res.size == 0:
+            res = np.zeros(1, np.uint8)
+        self._seqs = (res, np.ascontiguousarray(offsets, dtype=np.uint64))
+        return self
+
+    def scoring(self, scoring: Scoring) -> "DatabaseBuilder":
+        self._scoring = scoring
+        return self
+
+    def mode(self, mode: Mode) -> "DatabaseBuilder":
+        self._mode = Mode(mode)
+        return self
+
+    def search_type(self, st: SearchType) -> "DatabaseBuilder":
+        self._st = SearchType(st)
+        return self
+
+    def max_query_len(self, n: int) -> "DatabaseBuilder":
+        self._mql = int(n)
+        return self
+
+    def backend(self, choice: BackendChoice) -> "DatabaseBuilder":
+        self._backend = choice
+        return self
+
+    def layout(self, choice: LayoutChoice) -> "DatabaseBuilder":
+        self._layout = choice
+        return self
+
+    def build(self) -> Database:
+        for name, val in (("sequences", self._seqs), ("scoring", self._scoring),
+                          ("mode", self._mode), ("max_query_len", self._mql)):
+            if val is None:
+                raise Error("IncompleteBuilder", field=name)
+        res, off = self._seqs
+        n = len(off) - 1
+        sc = self._scoring
+        st = self._st if self._st is not None else SearchType.Score
+        choice = _abi.CHOICE_UNSET if self._backend is None else self._backend._code()
+        layout = _abi.LAYOUT_AUTO if self._layout is None else self._layout._code()
+        h = C.c_void_p()
+        status = lib.hy_db_create(_ptr(res, _abi._u8p), _ptr(off, _abi._u64p), n,
+                                  _ptr(sc._matrix, _abi._i32p), sc._al, sc._go, sc._ge, int(self._mode),
+                                  int(st), self._mql, choice, layout, C.byref(h))
+        if status == 10:  # InvalidBackendName from HYALITE_BACKEND
+            raise Error("InvalidBackendName", name=os.environ.get(BACKEND_ENV_VAR, ""))
+        _check(status)
+        return Database(h.value, n)
+
+
+class Scratch:
+    """Per-thread working memory (src/database.rs:954-998): one CUDA stream plus device buffers."""
+
+    def __init__(self, db: Database):
+        h = C.c_void_p()
+        _check(lib.hy_scratch_create(db._h, C.byref(h)))
+        self._h = h
+        self._db = db  # keep the database alive while the scratch exists
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.hy_scratch_destroy(h)
+            self._h = C.c_void_p(None)
+
+    @staticmethod
+    def new(db: Database) -> "Scratch":
+        return Scratch(db)
+
+    def stream_ptr(self) -> int:
+        return int(lib.hy_scratch_stream(self._h) or 0)
+
+
+# ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------------------
+
+def align_pairs_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, mode: Mode, search_type: SearchType):
+    """align_pairs over concatenated queries and targets; returns (hits ctypes array, error or None).
+    On an error, hits[:failed] are valid."""
+    q_res = np.ascontiguousarray(q_res, dtype=np.uint8)
+    t_res = np.ascontiguousarray(t_res, dtype=np.uint8)
+    q_res = q_res if q_res.size else np.zeros(1, np.uint8)
+    t_res = t_res if t_res.size else np.zeros(1, np.uint8)
+    q_off = np.ascontiguousarray(q_off, dtype=np.uint64)
+    t_off = np.ascontiguousarray(t_off, dtype=np.uint64)
+    n = len(q_off) - 1
+    out = (_abi.HyHit * max(n, 1))()
+    failed = C.c_uint64()
+    st = lib.hy_align_pairs(_ptr(q_res, _abi._u8p), _ptr(q_off, _abi._u64p), _ptr(t_res, _abi._u8p),
+                            _ptr(t_off, _abi._u64p), n, _ptr(scoring._matrix, _abi._i32p), scoring._al,
+                            scoring._go, scoring._ge, int(mode), int(search_type), out, C.byref(failed))
+    err = None if st == _abi.OK else Error.from_status(st)
+    return out, (err, int(failed.value))
+
+
+def align_pairs(pairs, scoring: Scoring, mode: Mode, search_type: SearchType, out: list) -> None:
+    """Align independent (query, target) pairs; one BestHit per pair in input order with
+    db_index = pair index. Raises the first failing pair's error; ``out`` then holds the hits of
+    the pairs before it (src/kernel.rs:429-452)."""
+    qs, ts = zip(*pairs) if pairs else ((), ())
+    q_res, q_off = concat(qs)
+    t_res, t_off = concat(ts)
+    hits, (err, failed) = align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, mode, search_type)
+    out.clear()
+    upto = len(pairs) if err is None else failed
+    for k in range(upto):
+        out.append(BestHit._from(hits[k]))
+    if err is not None:
+        raise err
+
+
+__all__ = [
+    "BACKEND_ENV_VAR", "Backend", "BackendChoice", "BestHit", "Database", "DatabaseBuilder", "Error",
+    "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
+    "align_pairs", "align_pairs_arrays", "required_width", "concat",
+]

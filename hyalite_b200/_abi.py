@@ -1,0 +1,104 @@
+"""ctypes declarations of the C ABI in include/hyalite_cuda.h.
+
+The shared library is built in-tree (hyalite_b200/libhyalite_cuda.so). There is no fallback:
+importing the package without the library raises, so a missing build is never silently replaced by
+CPU code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhyalite_cuda.so")
+
+# Status codes (hy_status).
+OK = 0
+STATUS_NAMES = {
+    0: "Ok", 1: "EmptyAlphabet", 2: "MatrixShape", 3: "NegativeGapPenalty",
+    4: "GapOpenLessThanExtend", 5: "ScoreRangeTooWide", 6: "SymbolOutOfRange",
+    7: "IncompleteBuilder", 8: "EmptyDatabase", 9: "BackendUnavailable",
+    10: "InvalidBackendName", 11: "TracebackBudgetExceeded", 20: "InvalidArgument",
+    21: "QueryTooLong", 22: "Cuda", 23: "OutOfMemory", 24: "Timeout", 25: "Unsupported",
+    26: "Rejected",
+}
+CHOICE_UNSET = -2
+CHOICE_AUTO = -1
+LAYOUT_AUTO = -1
+
+
+class HyHit(C.Structure):
+    _fields_ = [("score", C.c_int32), ("reserved", C.c_uint32), ("db_index", C.c_uint64),
+                ("query_end", C.c_int64), ("target_end", C.c_int64)]
+
+
+_u8p = C.POINTER(C.c_uint8)
+_u64p = C.POINTER(C.c_uint64)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_vp = C.c_void_p
+_st = C.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "hy_last_error_detail": (None, [_i64p]),
+    "hy_status_name": (C.c_char_p, [_st]),
+    "hy_backend_parse": (_st, [C.c_char_p, C.POINTER(C.c_int)]),
+    "hy_backend_is_available": (C.c_int, [C.c_int]),
+    "hy_backend_resolve": (_st, [C.c_int, C.POINTER(C.c_int)]),
+    "hy_backend_name": (C.c_char_p, [C.c_int]),
+    "hy_scoring_validate": (_st, [C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32]),
+    "hy_required_width": (_st, [C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+                                C.c_uint64, C.POINTER(C.c_int), _i64p]),
+    "hy_db_create": (_st, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32,
+                           C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "hy_db_destroy": (None, [_vp]),
+    "hy_db_sequence_count": (C.c_uint64, [_vp]),
+    "hy_db_mode": (C.c_int, [_vp]),
+    "hy_db_search_type": (C.c_int, [_vp]),
+    "hy_db_score_width": (C.c_int, [_vp]),
+    "hy_db_backend": (C.c_int, [_vp]),
+    "hy_db_layout": (C.c_int, [_vp]),
+    "hy_db_max_query_len": (C.c_uint64, [_vp]),
+    "hy_db_max_target_len": (C.c_uint64, [_vp]),
+    "hy_db_device_bytes": (C.c_uint64, [_vp]),
+    "hy_db_scratch_bytes": (C.c_uint64, [_vp]),
+    "hy_db_partition": (None, [_vp, _u64p, _u64p]),
+    "hy_scratch_create": (_st, [_vp, C.POINTER(_vp)]),
+    "hy_scratch_destroy": (None, [_vp]),
+    "hy_scratch_stream": (_vp, [_vp]),
+    "hy_scan": (_st, [_vp, _vp, _u8p, C.c_uint64, C.POINTER(HyHit)]),
+    "hy_scan_all": (_st, [_vp, _vp, _u8p, C.c_uint64, C.POINTER(HyHit)]),
+    "hy_scan_scores": (_st, [_vp, _vp, _u8p, C.c_uint64, _i32p]),
+    "hy_scan_device": (_st, [_vp, _vp, _vp, C.c_uint64, _vp]),
+    "hy_scan_scores_device": (_st, [_vp, _vp, _vp, C.c_uint64, _vp]),
+    "hy_query_validate": (_st, [_vp, _u8p, C.c_uint64]),
+    "hy_scratch_sync": (_st, [_vp]),
+    "hy_scratch_profile": (_st, [_vp, C.c_int]),
+    "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, _u64p]),
+    "hy_measure_dpx_peak": (_st, [C.POINTER(C.c_double)]),
+    "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
+                             C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
+}
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: the cuda backend has no CPU fallback. Build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (or `make -C hyalite_b200/csrc`).")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = load()
+
+
+def last_detail():
+    d = (C.c_int64 * 3)()
+    lib.hy_last_error_detail(d)
+    return tuple(d)

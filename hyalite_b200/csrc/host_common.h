@@ -1,0 +1,32 @@
+// host_common.h -- host-side pieces shared by the runtime translation units: status reporting,
+// the width proof and scoring validation (pure host code, callable without a GPU).
+#pragma once
+
+#include <stdint.h>
+
+#include "../../include/hyalite_cuda.h"
+
+namespace hy {
+
+// Records the detail fields of the status being returned on this thread (hy_last_error_detail).
+hy_status fail(hy_status st, int64_t d0 = 0, int64_t d1 = 0, int64_t d2 = 0);
+
+// width::magnitude_bound clamped to i64 (src/width.rs:107-137, 157).
+int64_t magnitude_bound(int mode, int32_t min_entry, int32_t max_entry, int32_t gap_open,
+                        int32_t gap_ext, uint64_t max_query_len, uint64_t max_target_len);
+
+// ScoreWidth::narrowest_for (src/width.rs:69-71): 0/1/2, or -1 when nothing fits.
+int narrowest_width(int64_t bound);
+
+// Scoring::new validation (src/scoring.rs:65-100), with error details recorded.
+hy_status validate_scoring(uint64_t al, const int32_t *matrix, uint64_t matrix_len, int32_t go,
+                           int32_t ge);
+
+// The device's own per-sequence width rule: a sequence runs in packed int16 lanes when its
+// magnitude bound plus gap_open fits int16 (every kernel intermediate is then exact), else in
+// int32 lanes with the oracle's sentinel.
+inline bool device_fits_i16(int64_t bound, int32_t gap_open) {
+    return bound + (int64_t)gap_open <= 32767;
+}
+
+}  // namespace hy

@@ -1,0 +1,721 @@
+// runtime.cu -- host runtime of the cuda backend: the device-resident database (build, width
+// partition, length sort, packing), per-thread scratch, and the scan entry points of the C ABI.
+//
+// Mirrors DatabaseBuilder::build (src/database.rs:737-877), Scratch::new (965-998) and
+// Database::scan / scan_all / scan_scores (83-144, 347-464, 481-515); the device kernels live in
+// scan_kernel.cuh.
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "host_common.h"
+#include "scan_kernel.cuh"
+
+using namespace hy;
+
+namespace hy {
+
+// Launch shapes. Main scan: groups of MAIN_G lanes, MAIN_R query rows per lane. Winner end
+// recovery: one full warp per item.
+constexpr int MAIN_G = 8;
+constexpr int MAIN_R16 = 16;
+constexpr int MAIN_R32 = 16;
+constexpr int WIN_G = 32;
+constexpr int WIN_R = 16;
+constexpr int BLOCK = 256;
+
+struct Partition {
+    uint32_t n_items = 0;
+    uint64_t n_seqs = 0;
+    uint64_t total_cols = 0;
+    ItemMeta *d_meta = nullptr;
+    void *d_res = nullptr;
+};
+
+template <class A>
+struct ElemSize {
+    static constexpr size_t pe = sizeof(typename A::PE);
+};
+
+struct QueryPlan {
+    int32_t n_passes = 0;
+    int32_t vrow0 = 1;
+    uint32_t pass_bytes = 0;
+};
+
+static QueryPlan plan(uint64_t qlen, int rpp, uint64_t al, size_t pe) {
+    QueryPlan q;
+    q.n_passes = (int32_t)((qlen + rpp - 1) / rpp);
+    q.vrow0 = (int32_t)qlen - q.n_passes * rpp + 1;
+    q.pass_bytes = (uint32_t)((al + 1) * (uint64_t)rpp * pe);
+    return q;
+}
+
+}  // namespace hy
+
+struct hy_db {
+    int device = 0;
+    uint64_t n_seqs = 0, mql = 0, max_t = 0, al = 0;
+    int32_t go = 0, ge = 0, min_e = 0, max_e = 0;
+    int mode = 0, search_type = 0, layout = HY_LAYOUT_GATHERED;
+    hy_score_width width = HY_WIDTH_I8;
+    hy_backend backend = HY_BACKEND_CUDA;
+    int32_t *d_matrix = nullptr;
+    Partition p16, p32;
+    uint32_t *d_loc = nullptr;
+    uint64_t device_bytes = 0;
+};
+
+struct hy_scratch {
+    const hy_db *db = nullptr;
+    cudaStream_t stream = nullptr;
+    uint8_t *d_query = nullptr;
+    uint8_t *d_prof16 = nullptr, *d_prof32 = nullptr, *d_profw16 = nullptr, *d_profw32 = nullptr;
+    void *d_bnd16 = nullptr, *d_bnd32 = nullptr;
+    int32_t *d_scores = nullptr, *d_qend = nullptr, *d_tend = nullptr;
+    unsigned long long *d_key = nullptr;
+    uint32_t *d_win = nullptr;
+    hy_hit *d_hit = nullptr;
+    int *d_err = nullptr;
+    uint8_t *h_query = nullptr;
+    hy_hit *h_hit = nullptr;
+    int *h_err = nullptr;
+    int32_t *h_out = nullptr;  // 3 * n_seqs int32 (scores, qend, tend), allocated on first use
+    uint64_t bytes = 0;
+    // Optional event timing of the main scan kernels (hy_scratch_profile).
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<int> event_part;  // 0: int16x2 pair kernel, 1: int32 kernel
+    size_t n_events = 0;
+    uint64_t launches = 0;        // every kernel this scratch launched since the last read
+};
+
+namespace hy {
+
+#define HY_CK(call)                                                                  \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            cudaGetLastError();                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e_); \
+        }                                                                            \
+    } while (0)
+
+template <class A, int G, int R, int MODE, bool ENDS>
+static cudaError_t launch_mode(const ScanParams &p, int blocks, int threads, size_t smem,
+                               cudaStream_t st) {
+    auto kern = scan_kernel<A, G, R, MODE, ENDS>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<blocks, threads, smem, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <class A, int G, int R>
+static cudaError_t launch_scan(int mode, bool ends, const ScanParams &p, int blocks, int threads,
+                               size_t smem, cudaStream_t st) {
+#define HY_MODE_CASE(M)                                                              \
+    case M:                                                                          \
+        return ends ? launch_mode<A, G, R, M, true>(p, blocks, threads, smem, st)    \
+                    : launch_mode<A, G, R, M, false>(p, blocks, threads, smem, st);
+    switch (mode) {
+        HY_MODE_CASE(MODE_SW)
+        HY_MODE_CASE(MODE_NW)
+        HY_MODE_CASE(MODE_HW)
+        HY_MODE_CASE(MODE_OV)
+        HY_MODE_CASE(MODE_SHW)
+    }
+#undef HY_MODE_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <class A, int G, int R>
+static cudaError_t launch_profile(const hy_db *db, const uint8_t *d_query, uint64_t qlen,
+                                  const QueryPlan &qp, int32_t lim, uint8_t *out, cudaStream_t st) {
+    const int64_t total = (int64_t)(db->al + 1) * G * R * qp.n_passes;
+    if (total == 0) return cudaSuccess;
+    int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+    const bool top_free = db->mode == MODE_SW || db->mode == MODE_HW || db->mode == MODE_OV;
+    build_profile_kernel<A, G, R><<<blocks, 256, 0, st>>>(
+        d_query, (int32_t)qlen, db->d_matrix, (int32_t)db->al, db->go, lim, top_free ? 1 : 0,
+        qp.vrow0, qp.n_passes, reinterpret_cast<typename A::PE *>(out));
+    return cudaGetLastError();
+}
+
+static constexpr int32_t LIM32 = 536870911;
+static int32_t lim16(const hy_db *db) { return 32767 - db->go; }
+
+// Fill per-target scores (and ends) for every sequence; optionally fold the best hit key.
+template <class A, int G, int R>
+static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partition &part,
+                                   const uint8_t *d_query, uint64_t qlen, bool ends,
+                                   unsigned long long *key, int32_t *scores, uint8_t *prof,
+                                   void *bnd, const uint32_t *item_ptr, int blocks, int threads) {
+    const bool i16 = sizeof(typename A::V) == 4 && A::NH == 2;
+    QueryPlan qp = plan(qlen, G * R, db->al, sizeof(typename A::PE));
+    HY_CK((launch_profile<A, G, R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof, sc->stream)));
+    sc->launches += qp.n_passes > 0 ? 2 : 1;
+    ScanParams p;
+    p.meta = part.d_meta;
+    p.n_items = part.n_items;
+    p.item_ptr = item_ptr;
+    p.res = part.d_res;
+    p.profile = prof;
+    p.pass_bytes = qp.pass_bytes;
+    p.n_passes = qp.n_passes;
+    p.vrow0 = qp.vrow0;
+    p.qlen = (int32_t)qlen;
+    p.go = db->go;
+    p.ge = db->ge;
+    p.sentinel = i16 ? (-32768 + db->ge) : (INT32_MIN / 4);
+    p.boundary = bnd;
+    p.scores = scores;
+    p.qend = sc->d_qend;
+    p.tend = sc->d_tend;
+    p.best_key = key;
+    p.err = sc->d_err;
+    size_t smem = 2 * (size_t)qp.pass_bytes + 16;
+    const bool timed = sc->profile && item_ptr == nullptr;
+    if (timed) {
+        if (sc->n_events == sc->events.size()) {
+            cudaEvent_t a, b;
+            HY_CK(cudaEventCreate(&a));
+            HY_CK(cudaEventCreate(&b));
+            sc->events.push_back({a, b});
+            sc->event_part.push_back(0);
+        }
+        sc->event_part[sc->n_events] = i16 ? 0 : 1;
+        HY_CK(cudaEventRecord(sc->events[sc->n_events].first, sc->stream));
+    }
+    HY_CK((launch_scan<A, G, R>(db->mode, ends, p, blocks, threads, smem, sc->stream)));
+    if (timed) {
+        HY_CK(cudaEventRecord(sc->events[sc->n_events].second, sc->stream));
+        ++sc->n_events;
+    }
+    return fail(HY_OK);
+}
+
+static hy_status enqueue_scores(const hy_db *db, hy_scratch *sc, const uint8_t *d_query,
+                                uint64_t qlen, bool ends, unsigned long long *key, int32_t *scores) {
+    hy_status st;
+    if (db->p16.n_items) {
+        int gpb = BLOCK / MAIN_G;
+        int blocks = (int)((db->p16.n_items + gpb - 1) / gpb);
+        st = enqueue_partition<Pair16, MAIN_G, MAIN_R16>(db, sc, db->p16, d_query, qlen, ends, key,
+                                                        scores, sc->d_prof16, sc->d_bnd16, nullptr,
+                                                        blocks, BLOCK);
+        if (st != HY_OK) return st;
+    }
+    if (db->p32.n_items) {
+        int gpb = BLOCK / MAIN_G;
+        int blocks = (int)((db->p32.n_items + gpb - 1) / gpb);
+        st = enqueue_partition<Single32, MAIN_G, MAIN_R32>(db, sc, db->p32, d_query, qlen, ends,
+                                                          key, scores, sc->d_prof32, sc->d_bnd32,
+                                                          nullptr, blocks, BLOCK);
+        if (st != HY_OK) return st;
+    }
+    return fail(HY_OK);
+}
+
+// Locate the winning sequence's item in its partition (or NO_INDEX in the other partition).
+__global__ void winner_loc_kernel(const unsigned long long *key, const uint32_t *loc, uint32_t *win) {
+    const uint32_t idx = ~(uint32_t)(*key & 0xffffffffu);
+    const uint32_t l = loc[idx];
+    const uint32_t part = l >> 31, item = l & 0x7fffffffu;
+    win[0] = part == 0 ? item : NO_INDEX;
+    win[1] = part == 1 ? item : NO_INDEX;
+}
+
+// Compose the BestHit of a single-best scan from the reduced key (and the winner's ends).
+__global__ void finalize_kernel(const unsigned long long *key, const int32_t *qend,
+                                const int32_t *tend, int with_ends, hy_hit *out) {
+    const unsigned long long k = *key;
+    const uint32_t idx = ~(uint32_t)(k & 0xffffffffu);
+    hy_hit h;
+    h.score = (int32_t)((uint32_t)(k >> 32) ^ 0x80000000u);
+    h.reserved = 0;
+    h.db_index = idx;
+    h.query_end = with_ends ? (int64_t)qend[idx] : -1;
+    h.target_end = with_ends ? (int64_t)tend[idx] : -1;
+    *out = h;
+}
+
+static hy_status enqueue_scan(const hy_db *db, hy_scratch *sc, const uint8_t *d_query,
+                              uint64_t qlen, hy_hit *d_out) {
+    HY_CK(cudaMemsetAsync(sc->d_key, 0, sizeof(unsigned long long), sc->stream));
+    hy_status st = enqueue_scores(db, sc, d_query, qlen, false, sc->d_key, sc->d_scores);
+    if (st != HY_OK) return st;
+    const bool ends = db->search_type == HY_SEARCH_SCORE_END;
+    if (ends) {
+        // End positions of the winner only (src/database.rs:186-197): rerun its item with
+        // position tracking, one warp wide.
+        winner_loc_kernel<<<1, 1, 0, sc->stream>>>(sc->d_key, db->d_loc, sc->d_win);
+        HY_CK(cudaGetLastError());
+        ++sc->launches;
+        if (db->p16.n_items) {
+            st = enqueue_partition<Pair16, WIN_G, WIN_R>(db, sc, db->p16, d_query, qlen, true,
+                                                        nullptr, sc->d_scores, sc->d_profw16,
+                                                        sc->d_bnd16, sc->d_win, 1, WIN_G);
+            if (st != HY_OK) return st;
+        }
+        if (db->p32.n_items) {
+            st = enqueue_partition<Single32, WIN_G, WIN_R>(db, sc, db->p32, d_query, qlen, true,
+                                                          nullptr, sc->d_scores, sc->d_profw32,
+                                                          sc->d_bnd32, sc->d_win + 1, 1, WIN_G);
+            if (st != HY_OK) return st;
+        }
+    }
+    finalize_kernel<<<1, 1, 0, sc->stream>>>(sc->d_key, sc->d_qend, sc->d_tend, ends ? 1 : 0, d_out);
+    HY_CK(cudaGetLastError());
+    ++sc->launches;
+    return fail(HY_OK);
+}
+
+static hy_status check_query(const hy_db *db, const uint8_t *query, uint64_t qlen) {
+    if (qlen > db->mql) return fail(HY_ERR_QUERY_TOO_LONG, (int64_t)qlen, (int64_t)db->mql);
+    if (qlen && !query) return fail(HY_ERR_INVALID_ARGUMENT);
+    for (uint64_t i = 0; i < qlen; ++i)
+        if (query[i] >= db->al) return fail(HY_ERR_SYMBOL_OUT_OF_RANGE, query[i], (int64_t)db->al);
+    return fail(HY_OK);
+}
+
+static hy_status upload_query(hy_scratch *sc, const uint8_t *query, uint64_t qlen) {
+    if (qlen) {
+        memcpy(sc->h_query, query, qlen);
+        HY_CK(cudaMemcpyAsync(sc->d_query, sc->h_query, qlen, cudaMemcpyHostToDevice, sc->stream));
+    }
+    return fail(HY_OK);
+}
+
+static hy_status sync_and_check(hy_scratch *sc) {
+    HY_CK(cudaMemcpyAsync(sc->h_err, sc->d_err, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+    HY_CK(cudaStreamSynchronize(sc->stream));
+    if (*sc->h_err) {
+        *sc->h_err = 0;
+        HY_CK(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
+        HY_CK(cudaStreamSynchronize(sc->stream));
+        return fail(HY_ERR_TIMEOUT);
+    }
+    return fail(HY_OK);
+}
+
+static hy_status ensure_host_out(hy_scratch *sc) {
+    if (!sc->h_out) {
+        size_t bytes = 3 * sizeof(int32_t) * std::max<uint64_t>(sc->db->n_seqs, 1);
+        HY_CK(cudaMallocHost(&sc->h_out, bytes));
+    }
+    return fail(HY_OK);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Build one partition: `order` lists its global indices sorted by length, longest first.
+static hy_status build_partition(hy_db *db, Partition &part, const std::vector<uint32_t> &order,
+                                 const uint8_t *residues, const uint64_t *offsets, bool pairs) {
+    part.n_seqs = order.size();
+    if (order.empty()) return fail(HY_OK);
+    const uint64_t per = pairs ? 2 : 1;
+    const uint64_t align = pairs ? 8 : 16;
+    part.n_items = (uint32_t)((order.size() + per - 1) / per);
+    std::vector<ItemMeta> meta(part.n_items);
+    uint64_t cols = 0;
+    for (uint32_t it = 0; it < part.n_items; ++it) {
+        ItemMeta &m = meta[it];
+        m.col_off = cols;
+        m.pad_ = 0;
+        for (int h = 0; h < 2; ++h) {
+            uint64_t k = (uint64_t)it * per + h;
+            if (h < (int)per && k < order.size()) {
+                m.idx[h] = order[k];
+                m.n[h] = (uint32_t)(offsets[order[k] + 1] - offsets[order[k]]);
+            } else {
+                m.idx[h] = NO_INDEX;
+                m.n[h] = 0;
+            }
+        }
+        m.w = std::max(m.n[0], m.n[1]);
+        cols += (m.w + align - 1) / align * align;
+    }
+    part.total_cols = cols;
+    HY_CK(cudaMalloc(&part.d_meta, sizeof(ItemMeta) * part.n_items));
+    HY_CK(cudaMemcpy(part.d_meta, meta.data(), sizeof(ItemMeta) * part.n_items, cudaMemcpyHostToDevice));
+    db->device_bytes += sizeof(ItemMeta) * part.n_items;
+    if (pairs) {
+        std::vector<uint16_t> res(std::max<uint64_t>(cols, 1), (uint16_t)(db->al | (db->al << 8)));
+        for (uint32_t it = 0; it < part.n_items; ++it) {
+            const ItemMeta &m = meta[it];
+            const uint8_t *t0 = residues + offsets[m.idx[0]];
+            const uint8_t *t1 = m.idx[1] == NO_INDEX ? nullptr : residues + offsets[m.idx[1]];
+            for (uint32_t j = 0; j < m.w; ++j) {
+                uint16_t lo = j < m.n[0] ? t0[j] : (uint16_t)db->al;
+                uint16_t hi = (t1 && j < m.n[1]) ? t1[j] : (uint16_t)db->al;
+                res[m.col_off + j] = (uint16_t)(lo | (hi << 8));
+            }
+        }
+        HY_CK(cudaMalloc(&part.d_res, res.size() * sizeof(uint16_t)));
+        HY_CK(cudaMemcpy(part.d_res, res.data(), res.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        db->device_bytes += res.size() * sizeof(uint16_t);
+    } else {
+        std::vector<uint8_t> res(std::max<uint64_t>(cols, 1), 0);
+        for (uint32_t it = 0; it < part.n_items; ++it) {
+            const ItemMeta &m = meta[it];
+            memcpy(&res[m.col_off], residues + offsets[m.idx[0]], m.n[0]);
+        }
+        HY_CK(cudaMalloc(&part.d_res, res.size()));
+        HY_CK(cudaMemcpy(part.d_res, res.data(), res.size(), cudaMemcpyHostToDevice));
+        db->device_bytes += res.size();
+    }
+    return fail(HY_OK);
+}
+
+static void free_db(hy_db *db) {
+    if (!db) return;
+    cudaFree(db->d_matrix);
+    cudaFree(db->p16.d_meta);
+    cudaFree(db->p16.d_res);
+    cudaFree(db->p32.d_meta);
+    cudaFree(db->p32.d_res);
+    cudaFree(db->d_loc);
+    delete db;
+}
+
+static uint64_t npass(uint64_t mql, int rpp) { return (mql + rpp - 1) / rpp; }
+
+}  // namespace hy
+
+extern "C" {
+
+hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                       const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
+                       int32_t gap_ext, hy_mode mode, hy_search_type search_type,
+                       uint64_t max_query_len, int backend_choice, int layout, hy_db **out) {
+    if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
+    *out = nullptr;
+    if ((int)mode < 0 || (int)mode > 4) return fail(HY_ERR_INVALID_ARGUMENT);
+    if ((int)search_type != HY_SEARCH_SCORE && (int)search_type != HY_SEARCH_SCORE_END)
+        return fail(HY_ERR_UNSUPPORTED);
+    hy_status st = validate_scoring(alphabet_len, matrix, alphabet_len * alphabet_len, gap_open, gap_ext);
+    if (st != HY_OK) return st;
+    if (n_seqs == 0) return fail(HY_ERR_EMPTY_DATABASE);
+    if (!offsets || (!residues && offsets[n_seqs] > 0)) return fail(HY_ERR_INVALID_ARGUMENT);
+    for (uint64_t k = 0; k < n_seqs; ++k) {
+        if (offsets[k + 1] < offsets[k]) return fail(HY_ERR_INVALID_ARGUMENT);
+        for (uint64_t i = offsets[k]; i < offsets[k + 1]; ++i)
+            if (residues[i] >= alphabet_len)
+                return fail(HY_ERR_SYMBOL_OUT_OF_RANGE, residues[i], (int64_t)alphabet_len);
+    }
+    uint64_t max_t = 0;
+    for (uint64_t k = 0; k < n_seqs; ++k) max_t = std::max(max_t, offsets[k + 1] - offsets[k]);
+    const int32_t min_e = *std::min_element(matrix, matrix + alphabet_len * alphabet_len);
+    const int32_t max_e = *std::max_element(matrix, matrix + alphabet_len * alphabet_len);
+    const int64_t bound = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, max_query_len, max_t);
+    const int width = narrowest_width(bound);
+    if (width < 0) return fail(HY_ERR_SCORE_RANGE_TOO_WIDE, bound);
+    hy_backend backend;
+    st = hy_backend_resolve(backend_choice, &backend);
+    if (st != HY_OK) return st;
+    if (layout == HY_LAYOUT_PRECOMPUTED) return fail(HY_ERR_UNSUPPORTED);
+    if (layout != HY_LAYOUT_AUTO && layout != HY_LAYOUT_GATHERED) return fail(HY_ERR_INVALID_ARGUMENT);
+    // Device limits: 32-bit db indices (one value reserved), byte residues plus a padding symbol.
+    if (n_seqs >= (uint64_t)NO_INDEX || alphabet_len > 255 || max_t >= (1ull << 31) ||
+        max_query_len >= (1ull << 30))
+        return fail(HY_ERR_UNSUPPORTED);
+
+    hy_db *db = new hy_db;
+    cudaGetDevice(&db->device);
+    db->n_seqs = n_seqs;
+    db->mql = max_query_len;
+    db->max_t = max_t;
+    db->al = alphabet_len;
+    db->go = gap_open;
+    db->ge = gap_ext;
+    db->min_e = min_e;
+    db->max_e = max_e;
+    db->mode = mode;
+    db->search_type = search_type;
+    db->layout = HY_LAYOUT_GATHERED;
+    db->width = (hy_score_width)width;
+    db->backend = backend;
+
+    // Per-sequence device width, then a length sort (longest first) inside each partition.
+    std::vector<uint32_t> o16, o32;
+    for (uint64_t k = 0; k < n_seqs; ++k) {
+        uint64_t len = offsets[k + 1] - offsets[k];
+        int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, max_query_len, len);
+        (device_fits_i16(b, gap_open) ? o16 : o32).push_back((uint32_t)k);
+    }
+    auto by_len = [&](uint32_t a, uint32_t b) {
+        uint64_t la = offsets[a + 1] - offsets[a], lb = offsets[b + 1] - offsets[b];
+        return la != lb ? la > lb : a < b;
+    };
+    std::sort(o16.begin(), o16.end(), by_len);
+    std::sort(o32.begin(), o32.end(), by_len);
+
+    hy_status bst = HY_OK;
+    auto ck = [&](cudaError_t e) {
+        if (e != cudaSuccess && bst == HY_OK) {
+            cudaGetLastError();
+            bst = fail(e == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e);
+        }
+    };
+    ck(cudaMalloc(&db->d_matrix, sizeof(int32_t) * alphabet_len * alphabet_len));
+    if (bst == HY_OK)
+        ck(cudaMemcpy(db->d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
+                      cudaMemcpyHostToDevice));
+    if (bst == HY_OK) bst = build_partition(db, db->p16, o16, residues, offsets, true);
+    if (bst == HY_OK) bst = build_partition(db, db->p32, o32, residues, offsets, false);
+    if (bst == HY_OK) {
+        std::vector<uint32_t> loc(n_seqs);
+        for (size_t i = 0; i < o16.size(); ++i) loc[o16[i]] = (uint32_t)(i / 2);
+        for (size_t i = 0; i < o32.size(); ++i) loc[o32[i]] = (uint32_t)i | 0x80000000u;
+        ck(cudaMalloc(&db->d_loc, sizeof(uint32_t) * n_seqs));
+        if (bst == HY_OK)
+            ck(cudaMemcpy(db->d_loc, loc.data(), sizeof(uint32_t) * n_seqs, cudaMemcpyHostToDevice));
+        db->device_bytes += sizeof(uint32_t) * n_seqs + sizeof(int32_t) * alphabet_len * alphabet_len;
+    }
+    if (bst != HY_OK) {
+        int64_t d[3];
+        hy_last_error_detail(d);
+        free_db(db);
+        return fail(bst, d[0], d[1], d[2]);
+    }
+    *out = db;
+    return fail(HY_OK);
+}
+
+void hy_db_destroy(hy_db *db) {
+    if (!db) return;
+    DeviceGuard g(db->device);
+    free_db(db);
+}
+
+uint64_t hy_db_sequence_count(const hy_db *db) { return db ? db->n_seqs : 0; }
+hy_mode hy_db_mode(const hy_db *db) { return (hy_mode)db->mode; }
+hy_search_type hy_db_search_type(const hy_db *db) { return (hy_search_type)db->search_type; }
+hy_score_width hy_db_score_width(const hy_db *db) { return db->width; }
+hy_backend hy_db_backend(const hy_db *db) { return db->backend; }
+int hy_db_layout(const hy_db *db) { return db->layout; }
+uint64_t hy_db_max_query_len(const hy_db *db) { return db->mql; }
+uint64_t hy_db_max_target_len(const hy_db *db) { return db->max_t; }
+uint64_t hy_db_device_bytes(const hy_db *db) { return db->device_bytes; }
+void hy_db_partition(const hy_db *db, uint64_t *n_i16, uint64_t *n_i32) {
+    if (n_i16) *n_i16 = db->p16.n_seqs;
+    if (n_i32) *n_i32 = db->p32.n_seqs;
+}
+
+uint64_t hy_db_scratch_bytes(const hy_db *db) {
+    const uint64_t mq = std::max<uint64_t>(db->mql, 1);
+    uint64_t b = mq + 3 * 4 * db->n_seqs + 64 + sizeof(hy_hit);
+    b += npass(mq, MAIN_G * MAIN_R16) * (db->al + 1) * MAIN_G * MAIN_R16 * 2;
+    b += npass(mq, MAIN_G * MAIN_R32) * (db->al + 1) * MAIN_G * MAIN_R32 * 4;
+    b += npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 6;
+    if (mq > (uint64_t)std::min(MAIN_G * MAIN_R16, MAIN_G * MAIN_R32))
+        b += 8 * (db->p16.total_cols + db->p32.total_cols);
+    return b;
+}
+
+hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
+    if (!db || !out) return fail(HY_ERR_INVALID_ARGUMENT);
+    DeviceGuard g(db->device);
+    hy_scratch *sc = new hy_scratch;
+    sc->db = db;
+    hy_status st = HY_OK;
+    auto ck = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == HY_OK) {
+            cudaGetLastError();
+            st = fail(e == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e);
+        }
+    };
+    const uint64_t mq = std::max<uint64_t>(db->mql, 1);
+    const uint64_t n = std::max<uint64_t>(db->n_seqs, 1);
+    ck(cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking));
+    ck(cudaMalloc(&sc->d_query, mq));
+    ck(cudaMalloc(&sc->d_prof16, std::max<uint64_t>(1, npass(mq, MAIN_G * MAIN_R16) * (db->al + 1) * MAIN_G * MAIN_R16 * 2)));
+    ck(cudaMalloc(&sc->d_prof32, std::max<uint64_t>(1, npass(mq, MAIN_G * MAIN_R32) * (db->al + 1) * MAIN_G * MAIN_R32 * 4)));
+    ck(cudaMalloc(&sc->d_profw16, std::max<uint64_t>(1, npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 2)));
+    ck(cudaMalloc(&sc->d_profw32, std::max<uint64_t>(1, npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 4)));
+    const bool multipass = mq > (uint64_t)std::min(MAIN_G * MAIN_R16, MAIN_G * MAIN_R32);
+    ck(cudaMalloc(&sc->d_bnd16, multipass ? std::max<uint64_t>(8, 8 * db->p16.total_cols) : 8));
+    ck(cudaMalloc(&sc->d_bnd32, multipass ? std::max<uint64_t>(8, 8 * db->p32.total_cols) : 8));
+    ck(cudaMalloc(&sc->d_scores, 4 * n));
+    ck(cudaMalloc(&sc->d_qend, 4 * n));
+    ck(cudaMalloc(&sc->d_tend, 4 * n));
+    ck(cudaMalloc(&sc->d_key, 64));
+    ck(cudaMalloc(&sc->d_win, 64));
+    ck(cudaMalloc(&sc->d_hit, sizeof(hy_hit)));
+    ck(cudaMalloc(&sc->d_err, 64));
+    ck(cudaMallocHost(&sc->h_query, mq));
+    ck(cudaMallocHost(&sc->h_hit, sizeof(hy_hit)));
+    ck(cudaMallocHost(&sc->h_err, sizeof(int)));
+    if (st == HY_OK) {
+        ck(cudaMemset(sc->d_err, 0, 64));
+        *sc->h_err = 0;
+        sc->bytes = hy_db_scratch_bytes(db);
+    }
+    if (st != HY_OK) {
+        int64_t d[3];
+        hy_last_error_detail(d);
+        hy_scratch_destroy(sc);
+        return fail(st, d[0], d[1], d[2]);
+    }
+    *out = sc;
+    return fail(HY_OK);
+}
+
+void hy_scratch_destroy(hy_scratch *sc) {
+    if (!sc) return;
+    DeviceGuard g(sc->db->device);
+    if (sc->stream) cudaStreamSynchronize(sc->stream);
+    cudaFree(sc->d_query);
+    cudaFree(sc->d_prof16);
+    cudaFree(sc->d_prof32);
+    cudaFree(sc->d_profw16);
+    cudaFree(sc->d_profw32);
+    cudaFree(sc->d_bnd16);
+    cudaFree(sc->d_bnd32);
+    cudaFree(sc->d_scores);
+    cudaFree(sc->d_qend);
+    cudaFree(sc->d_tend);
+    cudaFree(sc->d_key);
+    cudaFree(sc->d_win);
+    cudaFree(sc->d_hit);
+    cudaFree(sc->d_err);
+    cudaFreeHost(sc->h_query);
+    cudaFreeHost(sc->h_hit);
+    cudaFreeHost(sc->h_err);
+    cudaFreeHost(sc->h_out);
+    for (auto &e : sc->events) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    if (sc->stream) cudaStreamDestroy(sc->stream);
+    delete sc;
+}
+
+void *hy_scratch_stream(hy_scratch *sc) { return sc ? (void *)sc->stream : nullptr; }
+
+hy_status hy_scratch_profile(hy_scratch *sc, int enable) {
+    if (!sc) return fail(HY_ERR_INVALID_ARGUMENT);
+    sc->profile = enable != 0;
+    sc->n_events = 0;
+    sc->launches = 0;
+    return fail(HY_OK);
+}
+
+hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[2], uint64_t launches[2],
+                                  uint64_t *all_launches) {
+    if (!sc || !kernel_ms || !launches) return fail(HY_ERR_INVALID_ARGUMENT);
+    DeviceGuard g(sc->db->device);
+    HY_CK(cudaStreamSynchronize(sc->stream));
+    kernel_ms[0] = kernel_ms[1] = 0.0;
+    launches[0] = launches[1] = 0;
+    for (size_t i = 0; i < sc->n_events; ++i) {
+        float ms = 0.f;
+        HY_CK(cudaEventElapsedTime(&ms, sc->events[i].first, sc->events[i].second));
+        kernel_ms[sc->event_part[i]] += ms;
+        launches[sc->event_part[i]] += 1;
+    }
+    if (all_launches) *all_launches = sc->launches;
+    sc->n_events = 0;
+    sc->launches = 0;
+    return fail(HY_OK);
+}
+
+hy_status hy_query_validate(const hy_db *db, const uint8_t *query, uint64_t qlen) {
+    if (!db) return fail(HY_ERR_INVALID_ARGUMENT);
+    return check_query(db, query, qlen);
+}
+
+hy_status hy_scratch_sync(hy_scratch *sc) {
+    if (!sc) return fail(HY_ERR_INVALID_ARGUMENT);
+    DeviceGuard g(sc->db->device);
+    return sync_and_check(sc);
+}
+
+hy_status hy_scan(const hy_db *db, hy_scratch *sc, const uint8_t *query, uint64_t qlen, hy_hit *out) {
+    if (!db || !sc || !out || sc->db != db) return fail(HY_ERR_INVALID_ARGUMENT);
+    hy_status st = check_query(db, query, qlen);
+    if (st != HY_OK) return st;
+    DeviceGuard g(db->device);
+    if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
+    if ((st = enqueue_scan(db, sc, sc->d_query, qlen, sc->d_hit)) != HY_OK) return st;
+    HY_CK(cudaMemcpyAsync(sc->h_hit, sc->d_hit, sizeof(hy_hit), cudaMemcpyDeviceToHost, sc->stream));
+    if ((st = sync_and_check(sc)) != HY_OK) return st;
+    *out = *sc->h_hit;
+    return fail(HY_OK);
+}
+
+hy_status hy_scan_device(const hy_db *db, hy_scratch *sc, const uint8_t *d_query, uint64_t qlen,
+                         hy_hit *d_out) {
+    if (!db || !sc || !d_out || sc->db != db) return fail(HY_ERR_INVALID_ARGUMENT);
+    if (qlen > db->mql) return fail(HY_ERR_QUERY_TOO_LONG, (int64_t)qlen, (int64_t)db->mql);
+    DeviceGuard g(db->device);
+    return enqueue_scan(db, sc, d_query, qlen, d_out);
+}
+
+hy_status hy_scan_scores_device(const hy_db *db, hy_scratch *sc, const uint8_t *d_query,
+                                uint64_t qlen, int32_t *d_out) {
+    if (!db || !sc || !d_out || sc->db != db) return fail(HY_ERR_INVALID_ARGUMENT);
+    if (qlen > db->mql) return fail(HY_ERR_QUERY_TOO_LONG, (int64_t)qlen, (int64_t)db->mql);
+    DeviceGuard g(db->device);
+    return enqueue_scores(db, sc, d_query, qlen, false, nullptr, d_out);
+}
+
+hy_status hy_scan_scores(const hy_db *db, hy_scratch *sc, const uint8_t *query, uint64_t qlen,
+                         int32_t *out) {
+    if (!db || !sc || !out || sc->db != db) return fail(HY_ERR_INVALID_ARGUMENT);
+    hy_status st = check_query(db, query, qlen);
+    if (st != HY_OK) return st;
+    DeviceGuard g(db->device);
+    if ((st = ensure_host_out(sc)) != HY_OK) return st;
+    if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
+    if ((st = enqueue_scores(db, sc, sc->d_query, qlen, false, nullptr, sc->d_scores)) != HY_OK) return st;
+    HY_CK(cudaMemcpyAsync(sc->h_out, sc->d_scores, 4 * db->n_seqs, cudaMemcpyDeviceToHost, sc->stream));
+    if ((st = sync_and_check(sc)) != HY_OK) return st;
+    memcpy(out, sc->h_out, 4 * db->n_seqs);
+    return fail(HY_OK);
+}
+
+hy_status hy_scan_all(const hy_db *db, hy_scratch *sc, const uint8_t *query, uint64_t qlen,
+                      hy_hit *out) {
+    if (!db || !sc || !out || sc->db != db) return fail(HY_ERR_INVALID_ARGUMENT);
+    hy_status st = check_query(db, query, qlen);
+    if (st != HY_OK) return st;
+    DeviceGuard g(db->device);
+    const bool ends = db->search_type == HY_SEARCH_SCORE_END;
+    const uint64_t n = db->n_seqs;
+    if ((st = ensure_host_out(sc)) != HY_OK) return st;
+    if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
+    if ((st = enqueue_scores(db, sc, sc->d_query, qlen, ends, nullptr, sc->d_scores)) != HY_OK) return st;
+    HY_CK(cudaMemcpyAsync(sc->h_out, sc->d_scores, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
+    if (ends) {
+        HY_CK(cudaMemcpyAsync(sc->h_out + n, sc->d_qend, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
+        HY_CK(cudaMemcpyAsync(sc->h_out + 2 * n, sc->d_tend, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
+    }
+    if ((st = sync_and_check(sc)) != HY_OK) return st;
+    for (uint64_t k = 0; k < n; ++k) {
+        out[k].score = sc->h_out[k];
+        out[k].reserved = 0;
+        out[k].db_index = k;
+        out[k].query_end = ends ? (int64_t)sc->h_out[n + k] : -1;
+        out[k].target_end = ends ? (int64_t)sc->h_out[2 * n + k] : -1;
+    }
+    return fail(HY_OK);
+}
+
+}  // extern "C"

@@ -1,0 +1,679 @@
+// scan_kernel.cuh -- the device side of the inter-sequence database scan.
+//
+// One "item" is either a PAIR of database sequences packed into the two int16 halves of every
+// 32-bit register (Pair16), or ONE sequence in int32 lanes (Single32). A group of G consecutive
+// lanes of a warp runs one item: lane L owns R consecutive query rows of the current pass and
+// sweeps the item's columns one step behind lane L-1 (an anti-diagonal wavefront); the H and F
+// values of a lane's last row move to the next lane with one shuffle each per step. A pass covers
+// G*R query rows; the last row of a pass is handed to the next pass through a boundary row in
+// global memory. The query profile of the current pass is staged into shared memory by a TMA bulk
+// copy (cp.async.bulk) with an mbarrier, double-buffered across passes.
+//
+// The recurrence is the Gotoh recurrence of the scalar oracle (src/kernel.rs:168-217):
+//   E[i][j] = max(E[i][j-1] - ge, H[i][j-1] - go)
+//   F[i][j] = max(F[i-1][j] - ge, H[i-1][j] - go)
+//   H[i][j] = max(H[i-1][j-1] + sub(q_i, t_j), E[i][j], F[i][j])   (SW: also max with 0)
+// carried as G = H - go so every cell costs five DPX operations:
+//   E = max(E + (-ge), G_left)           __viaddmax
+//   F = max(F + (-ge), G_up)             __viaddmax
+//   T = max(E, F)                        __vimax (SW: __vimax_relu)
+//   H = max(G_diag + P, T)               __viaddmax, P = sub + go from the profile
+//   G = H + (-go)                        __viaddmax against the type minimum
+// Width safety: the host routes a sequence to Pair16 only when its magnitude bound plus gap_open
+// fits int16 (bound + go <= 32767), which keeps every intermediate above exactly representable,
+// so the packed arithmetic never wraps on a real cell and the results equal the i32 oracle.
+//
+// Rows: the query is padded at the FRONT so the last query row always sits in the last slot of
+// the last lane of the last pass. Virtual rows (index <= 0) reproduce the border row 0 exactly:
+// left border 0 and a profile value of `go` (free top border) or 0 (penalised top border).
+// Columns: in a Pair16 item the shorter sequence is padded with a symbol whose profile value is
+// the most negative representable; padded columns never feed a real cell and are excluded from
+// every answer region (or, for SW, can only tie a real cell at a larger column).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hy {
+
+enum { MODE_SW = 0, MODE_NW = 1, MODE_HW = 2, MODE_OV = 3, MODE_SHW = 4 };
+
+// Flags::for_mode (src/kernel.rs:43-98).
+template <int MODE>
+struct ModeFlags {
+    static constexpr bool top_free = MODE == MODE_SW || MODE == MODE_HW || MODE == MODE_OV;
+    static constexpr bool left_free = MODE == MODE_SW || MODE == MODE_OV || MODE == MODE_SHW;
+    static constexpr bool last_row = MODE == MODE_HW || MODE == MODE_OV;
+    static constexpr bool last_col = MODE == MODE_OV || MODE == MODE_SHW;
+    static constexpr bool local = MODE == MODE_SW;
+    static constexpr bool corner = MODE == MODE_NW;
+};
+
+struct ItemMeta {
+    uint64_t col_off;  // first column of the item in the residue / boundary arrays
+    uint32_t w;        // columns swept (the longer length of the pair)
+    uint32_t n[2];     // sequence lengths; a lone sequence has n[1] = 0 and idx[1] = NO_INDEX
+    uint32_t idx[2];   // global db indices
+    uint32_t pad_;
+};
+static constexpr uint32_t NO_INDEX = 0xffffffffu;
+
+struct ScanParams {
+    const ItemMeta *meta;
+    uint32_t n_items;
+    const uint32_t *item_ptr;  // when set: run the single item *item_ptr (NO_INDEX: nothing)
+    const void *res;           // Pair16: uint16 (lo | hi << 8); Single32: uint8
+    const uint8_t *profile;    // pass-major profile slices, pass_bytes each
+    uint32_t pass_bytes;
+    int32_t n_passes;
+    int32_t vrow0;  // grid row of pass 0, lane 0, slot 0 (<= 1)
+    int32_t qlen;
+    int32_t go, ge;
+    int32_t sentinel;
+    void *boundary;  // 2 values (G, F) per column
+    int32_t *scores;
+    int32_t *qend;
+    int32_t *tend;
+    unsigned long long *best_key;
+    int *err;
+};
+
+// ---- lane arithmetic -----------------------------------------------------------------------
+
+struct Pair16 {
+    typedef uint32_t V;
+    typedef int16_t PE;
+    typedef uint16_t RES;
+    static constexpr int NH = 2;
+    static constexpr int EPV = 8;  // profile elements per 16-byte vector
+    static constexpr int32_t VMIN = -32768, VMAX = 32767;
+    __device__ __forceinline__ static V splat(int64_t x) {
+        x = x < VMIN ? VMIN : (x > VMAX ? VMAX : x);
+        uint32_t h = (uint16_t)(int16_t)x;
+        return h | (h << 16);
+    }
+    __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s16x2(a, b, c); }
+    __device__ __forceinline__ static V vmax(V a, V b) { return __vmaxs2(a, b); }
+    __device__ __forceinline__ static V vmax_relu(V a, V b) { return __vimax_s16x2_relu(a, b); }
+    __device__ __forceinline__ static V vmax3(V a, V b, V c) { return __vimax3_s16x2(a, b, c); }
+    __device__ __forceinline__ static V vadd(V a, V b) { return __viaddmax_s16x2(a, b, 0x80008000u); }
+    __device__ __forceinline__ static int32_t get(V v, int h) {
+        return h ? (int32_t)(int16_t)(v >> 16) : (int32_t)(int16_t)(v & 0xffffu);
+    }
+    // Running maximum; up[h] is set where x is strictly greater than best in half h.
+    __device__ __forceinline__ static V bmax(V best, V x, bool &up0, bool &up1) {
+        bool ph, pl;
+        V r = __vibmax_s16x2(best, x, &ph, &pl);
+        up0 = !pl;
+        up1 = !ph;
+        return r;
+    }
+    __device__ __forceinline__ static void residues(RES r, int &a, int &b) {
+        a = r & 0xff;
+        b = r >> 8;
+    }
+    // Profile values of R rows for the two letters (a, b): interleave two int16 rows.
+    // prof_a serves the low half's letter a, prof_b the high half's letter b.
+    template <int R, int G>
+    __device__ __forceinline__ static void load_profile(const uint8_t *prof_a, const uint8_t *prof_b,
+                                                        int a, int b, int lane, V (&P)[R]) {
+        constexpr int KCH = R / EPV;
+        const uint4 *pa = reinterpret_cast<const uint4 *>(prof_a) + (size_t)a * KCH * G + lane;
+        const uint4 *pb = reinterpret_cast<const uint4 *>(prof_b) + (size_t)b * KCH * G + lane;
+#pragma unroll
+        for (int k = 0; k < KCH; ++k) {
+            uint4 A = pa[k * G], B = pb[k * G];
+            P[8 * k + 0] = __byte_perm(A.x, B.x, 0x5410);
+            P[8 * k + 1] = __byte_perm(A.x, B.x, 0x7632);
+            P[8 * k + 2] = __byte_perm(A.y, B.y, 0x5410);
+            P[8 * k + 3] = __byte_perm(A.y, B.y, 0x7632);
+            P[8 * k + 4] = __byte_perm(A.z, B.z, 0x5410);
+            P[8 * k + 5] = __byte_perm(A.z, B.z, 0x7632);
+            P[8 * k + 6] = __byte_perm(A.w, B.w, 0x5410);
+            P[8 * k + 7] = __byte_perm(A.w, B.w, 0x7632);
+        }
+    }
+};
+
+struct Single32 {
+    typedef int32_t V;
+    typedef int32_t PE;
+    typedef uint8_t RES;
+    static constexpr int NH = 1;
+    static constexpr int EPV = 4;
+    static constexpr int64_t VMIN = INT32_MIN, VMAX = INT32_MAX;
+    __device__ __forceinline__ static V splat(int64_t x) {
+        return (V)(x < VMIN ? VMIN : (x > VMAX ? VMAX : x));
+    }
+    __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s32(a, b, c); }
+    __device__ __forceinline__ static V vmax(V a, V b) { return max(a, b); }
+    __device__ __forceinline__ static V vmax_relu(V a, V b) { return __vimax_s32_relu(a, b); }
+    __device__ __forceinline__ static V vmax3(V a, V b, V c) { return __vimax3_s32(a, b, c); }
+    __device__ __forceinline__ static V vadd(V a, V b) { return a + b; }
+    __device__ __forceinline__ static int32_t get(V v, int) { return v; }
+    __device__ __forceinline__ static V bmax(V best, V x, bool &up0, bool &up1) {
+        bool p;
+        V r = __vibmax_s32(best, x, &p);
+        up0 = !p;
+        up1 = false;
+        return r;
+    }
+    __device__ __forceinline__ static void residues(RES r, int &a, int &b) {
+        a = r;
+        b = r;
+    }
+    template <int R, int G>
+    __device__ __forceinline__ static void load_profile(const uint8_t *prof_a, const uint8_t *,
+                                                        int a, int, int lane, V (&P)[R]) {
+        constexpr int KCH = R / EPV;
+        const int4 *pa = reinterpret_cast<const int4 *>(prof_a) + (size_t)a * KCH * G + lane;
+#pragma unroll
+        for (int k = 0; k < KCH; ++k) {
+            int4 A = pa[k * G];
+            P[4 * k + 0] = A.x;
+            P[4 * k + 1] = A.y;
+            P[4 * k + 2] = A.z;
+            P[4 * k + 3] = A.w;
+        }
+    }
+};
+
+// ---- small helpers -------------------------------------------------------------------------
+
+// gap_penalty (src/kernel.rs:103-109).
+__device__ __forceinline__ int64_t gap_pen(int32_t go, int32_t ge, int64_t len) {
+    return len <= 0 ? 0 : (int64_t)go + (len - 1) * (int64_t)ge;
+}
+
+// Answer candidate under the tie-break of Best::consider (src/kernel.rs:113-129): higher score,
+// then smaller grid column, then smaller grid row.
+struct Cand {
+    int32_t s;
+    int32_t col;
+    int32_t row;
+};
+__device__ __forceinline__ bool better(const Cand &a, const Cand &b) {
+    return a.s > b.s || (a.s == b.s && (a.col < b.col || (a.col == b.col && a.row < b.row)));
+}
+__device__ __forceinline__ void consider(Cand &b, int32_t s, int32_t col, int32_t row) {
+    Cand c = {s, col, row};
+    if (better(c, b)) b = c;
+}
+
+// Best border-cell candidate of the mode's answer region (reduce_answer, src/kernel.rs:223-260,
+// restricted to row 0 and column 0), for query length m and target length n.
+template <int MODE>
+__device__ __forceinline__ Cand border_seed(int32_t m, int32_t n, int32_t go, int32_t ge) {
+    const Cand none = {INT32_MIN, INT32_MAX, INT32_MAX};
+    switch (MODE) {
+    case MODE_SW: return {0, 0, 0};
+    case MODE_NW:
+        if (m == 0) return {(int32_t)-gap_pen(go, ge, n), n, 0};
+        if (n == 0) return {(int32_t)-gap_pen(go, ge, m), 0, m};
+        return none;
+    case MODE_HW:
+        if (m == 0) return {0, 0, 0};
+        return {(int32_t)-gap_pen(go, ge, m), 0, m};
+    case MODE_SHW:
+        if (n == 0) return {0, 0, 0};
+        return {(int32_t)-gap_pen(go, ge, n), n, 0};
+    default: /* OV */
+        if (m == 0 || n == 0) return {0, 0, 0};
+        return {0, 0, m};
+    }
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Issue one TMA bulk copy global -> shared whose completion is tracked by `bar`.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, "
+        "0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after a fixed number of polls (each poll may itself suspend briefly).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 24); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ unsigned long long hit_key(int32_t score, uint32_t idx) {
+    return ((unsigned long long)((uint32_t)score ^ 0x80000000u) << 32) | (uint32_t)(~idx);
+}
+
+// ---- one pass of the wavefront -------------------------------------------------------------
+//
+// Sweeps the item's columns for the G*R query rows of one pass. `steps` is warp-uniform (every
+// lane of the warp shuffles every step). Lane L works on column j = s - L + 1 at step s; the G and
+// F values of its last row at column j reach lane L+1 at step s+1. Lane 0 reads the row above the
+// pass from the boundary row (or the top border in the first pass); lane G-1 writes the pass's
+// last row to the boundary row unless this is the last pass.
+template <class A, int G, int R, int MODE, bool ENDS>
+__device__ __forceinline__ void sweep_pass(const int lane, const int steps, const int32_t w,
+                                           const uint32_t (&n)[2],
+                                           const typename A::RES *__restrict__ res,
+                                           const uint8_t *prof_a, const uint8_t *prof_b,
+                                           const int32_t row0, const bool first_pass,
+                                           const bool last_pass, typename A::V *bnd,
+                                           const int32_t qlen, const int32_t go, const int32_t ge,
+                                           const typename A::V Sv, typename A::V &best,
+                                           Cand (&cand)[2]) {
+    typedef typename A::V V;
+    typedef ModeFlags<MODE> Fl;
+    const V negge = A::splat(-(int64_t)ge), neggo = A::splat(-(int64_t)go);
+
+    V Gp[R], E[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int32_t row = row0 + r;
+        const int64_t lb = (row <= 0 || Fl::left_free) ? 0 : -gap_pen(go, ge, row);
+        Gp[r] = A::splat(lb - go);
+        E[r] = Sv;
+    }
+    V diag;
+    {
+        const int32_t row = row0 - 1;
+        const int64_t lb = (row <= 0 || Fl::left_free) ? 0 : -gap_pen(go, ge, row);
+        diag = A::splat(lb - go);
+    }
+    V botG = A::splat(0), botF = A::splat(0);
+    // SW end tracking within this pass: the running per-half maximum and the cell id
+    // (column * R + slot) where it was first reached; column-major order inside the lane means
+    // the first strict improvement is the smallest (column, row).
+    V pbest = A::splat(INT32_MIN);
+    int32_t pid0 = -1, pid1 = -1;
+
+    for (int s = 0; s < steps; ++s) {
+        const int32_t j = s - lane + 1;
+        V upG = __shfl_up_sync(0xffffffffu, botG, 1, G);
+        V upF = __shfl_up_sync(0xffffffffu, botF, 1, G);
+        const bool live = j >= 1 && j <= w;
+        if (lane == 0) {
+            if (first_pass) {
+                const int64_t tb = Fl::top_free ? 0 : -gap_pen(go, ge, j);
+                upG = A::splat(tb - go);
+                upF = Sv;
+            } else if (live) {
+                upG = bnd[2 * (j - 1)];
+                upF = bnd[2 * (j - 1) + 1];
+            }
+        }
+        if (live) {
+            int a, b;
+            A::residues(res[j - 1], a, b);
+            V P[R];
+            A::template load_profile<R, G>(prof_a, prof_b, a, b, lane, P);
+            V g_up = upG, f = upF, gd = diag, hprev = A::splat(0), hlast = A::splat(0);
+            const int32_t jR = j * R;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                E[r] = A::addmax(E[r], negge, Gp[r]);
+                f = A::addmax(f, negge, g_up);
+                const V t = Fl::local ? A::vmax_relu(E[r], f) : A::vmax(E[r], f);
+                const V h = A::addmax(gd, P[r], t);
+                gd = Gp[r];
+                const V g = A::vadd(h, neggo);
+                Gp[r] = g;
+                g_up = g;
+                if (Fl::local) {
+                    if (ENDS) {
+                        bool u0, u1;
+                        pbest = A::bmax(pbest, h, u0, u1);
+                        if (u0) pid0 = jR + r;
+                        if (u1) pid1 = jR + r;
+                    } else {
+                        if (r & 1)
+                            best = A::vmax3(best, hprev, h);
+                        else
+                            hprev = h;
+                    }
+                }
+                if (r == R - 1) hlast = h;
+            }
+            if (Fl::local && !ENDS && (R & 1)) best = A::vmax(best, hprev);
+            botG = g_up;
+            botF = f;
+            diag = upG;
+            if (lane == G - 1 && !last_pass) {
+                bnd[2 * (j - 1)] = botG;
+                bnd[2 * (j - 1) + 1] = botF;
+            }
+            // Last query row (grid row qlen): slot R-1 of lane G-1 in the last pass.
+            if ((Fl::last_row || Fl::corner) && last_pass && lane == G - 1) {
+#pragma unroll
+                for (int h = 0; h < A::NH; ++h) {
+                    const int32_t nh = (int32_t)n[h];
+                    if (Fl::last_row ? (j <= nh) : (j == nh)) consider(cand[h], A::get(hlast, h), j, qlen);
+                }
+            }
+            // Last column of each sequence (grid column n): every real row of this lane.
+            if (Fl::last_col) {
+#pragma unroll
+                for (int h = 0; h < A::NH; ++h) {
+                    if (j == (int32_t)n[h]) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r)
+                            if (row0 + r >= 1) consider(cand[h], A::get(Gp[r], h) + go, j, row0 + r);
+                    }
+                }
+            }
+        }
+    }
+    if (Fl::local && ENDS) {
+        if (pid0 >= 0) consider(cand[0], A::get(pbest, 0), pid0 / R, row0 + pid0 % R);
+        if (A::NH > 1 && pid1 >= 0) consider(cand[1], A::get(pbest, 1), pid1 / R, row0 + pid1 % R);
+    }
+}
+
+// Group reduction of the per-lane candidates, border seeds, output and best-key fold. Every lane
+// of the warp must call it (it shuffles).
+template <class A, int G, int MODE, bool ENDS>
+__device__ __forceinline__ void finish_item(const int lane, const bool active, const ItemMeta &meta,
+                                            const int32_t qlen, const int32_t go, const int32_t ge,
+                                            const typename A::V best, Cand (&cand)[2],
+                                            int32_t *scores, int32_t *qend, int32_t *tend,
+                                            unsigned long long *best_key) {
+    typedef ModeFlags<MODE> Fl;
+    if (Fl::local && !ENDS) {
+#pragma unroll
+        for (int h = 0; h < A::NH; ++h) cand[h].s = A::get(best, h);
+    }
+#pragma unroll
+    for (int h = 0; h < A::NH; ++h) {
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) {
+            Cand o;
+            o.s = __shfl_xor_sync(0xffffffffu, cand[h].s, off, G);
+            o.col = __shfl_xor_sync(0xffffffffu, cand[h].col, off, G);
+            o.row = __shfl_xor_sync(0xffffffffu, cand[h].row, off, G);
+            if (Fl::local && !ENDS) {
+                if (o.s > cand[h].s) cand[h] = o;
+            } else if (better(o, cand[h])) {
+                cand[h] = o;
+            }
+        }
+    }
+    unsigned long long key = 0;
+    if (active && lane == 0) {
+#pragma unroll
+        for (int h = 0; h < A::NH; ++h) {
+            const uint32_t idx = meta.idx[h];
+            if (idx == NO_INDEX) continue;
+            Cand c = border_seed<MODE>(qlen, (int32_t)meta.n[h], go, ge);
+            if (Fl::local && !ENDS) {
+                if (cand[h].s > c.s) c.s = cand[h].s;
+            } else if (better(cand[h], c)) {
+                c = cand[h];
+            }
+            scores[idx] = c.s;
+            if (ENDS) {
+                qend[idx] = c.row - 1;
+                tend[idx] = c.col - 1;
+            }
+            const unsigned long long k = hit_key(c.s, idx);
+            key = k > key ? k : key;
+        }
+    }
+    if (best_key) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+            key = o > key ? o : key;
+        }
+        if ((threadIdx.x & 31) == 0 && key != 0) atomicMax(best_key, key);
+    }
+}
+
+// ---- the database scan kernel ---------------------------------------------------------------
+//
+// All groups of a block step through the passes together: the pass's query profile is one
+// contiguous slice, brought into shared memory by a TMA bulk copy while the previous pass runs.
+template <class A, int G, int R, int MODE, bool ENDS>
+__global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
+    typedef typename A::V V;
+    constexpr int RPP = G * R;
+    static_assert(R % A::EPV == 0, "rows per lane must fill whole profile vectors");
+    static_assert(32 % G == 0, "groups must tile a warp");
+
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t *prof_buf[2] = {smem, smem + p.pass_bytes};
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)p.pass_bytes);
+
+    const int lane = threadIdx.x % G;
+    const int gpb = blockDim.x / G;
+    uint32_t item;
+    if (p.item_ptr) {
+        const uint32_t want = *p.item_ptr;
+        item = (blockIdx.x == 0 && threadIdx.x / G == 0) ? want : NO_INDEX;
+    } else {
+        item = blockIdx.x * gpb + threadIdx.x / G;
+    }
+    const bool active = item != NO_INDEX && item < p.n_items;
+    ItemMeta meta;
+    if (active) {
+        meta = p.meta[item];
+    } else {
+        meta.col_off = 0;
+        meta.w = 0;
+        meta.n[0] = meta.n[1] = 0;
+        meta.idx[0] = meta.idx[1] = NO_INDEX;
+    }
+    const V Sv = A::splat(p.sentinel);
+    const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
+    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
+    const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
+
+    V best = A::splat(0);
+    Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
+
+    if (p.n_passes > 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            bulk_load(prof_buf[0], p.profile, p.pass_bytes, &bars[0]);
+            if (p.n_passes > 1) bulk_load(prof_buf[1], p.profile + p.pass_bytes, p.pass_bytes, &bars[1]);
+        }
+    }
+    for (int pass = 0; pass < p.n_passes; ++pass) {
+        const int buf = pass & 1;
+        const bool ok = mbar_wait_bounded(&bars[buf], (uint32_t)((pass >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicExch(p.err, 1);
+            return;
+        }
+        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, (int32_t)meta.w, meta.n, res, prof_buf[buf],
+                                        prof_buf[buf], p.vrow0 + pass * RPP + lane * R, pass == 0,
+                                        pass == p.n_passes - 1, bnd, p.qlen, p.go, p.ge, Sv, best,
+                                        cand);
+        __syncthreads();  // the profile buffer and boundary row are free again
+        if (threadIdx.x == 0 && pass + 2 < p.n_passes)
+            bulk_load(prof_buf[buf], p.profile + (size_t)(pass + 2) * p.pass_bytes, p.pass_bytes,
+                      &bars[buf]);
+    }
+    finish_item<A, G, MODE, ENDS>(lane, active, meta, p.qlen, p.go, p.ge, best, cand, p.scores,
+                                  p.qend, p.tend, p.best_key);
+}
+
+// ---- the batched pairwise kernel (align_pairs) -----------------------------------------------
+//
+// Every item carries its own queries (one per half, of equal length), so each group builds the
+// profile slice of its own pass in its own region of shared memory, then sweeps it. Groups of a
+// warp run their items' passes in step; there is no block-wide synchronisation.
+struct PairParams {
+    const ItemMeta *meta;  // n[h]: target lengths; idx[h]: pair indices
+    const uint32_t *qlen;  // per item
+    const uint64_t *qoff;  // per item and half: offset of the query residues in q_res
+    uint32_t n_items;
+    const uint8_t *q_res;
+    const void *res;       // packed target residues, as in the scan
+    const int32_t *matrix;
+    int32_t al;
+    int32_t lim;
+    int32_t go, ge;
+    int32_t sentinel;
+    int top_free;
+    uint32_t group_bytes;  // shared memory per group (both halves of one pass slice)
+    void *boundary;
+    int32_t *scores;
+    int32_t *qend;
+    int32_t *tend;
+};
+
+template <class A, int G, int R>
+__device__ __forceinline__ void build_group_profile(uint8_t *dst, const uint8_t *q, int32_t qlen,
+                                                    int32_t row_base, const int32_t *matrix,
+                                                    int32_t al, int32_t lim, int32_t go,
+                                                    int top_free, int lane) {
+    constexpr int KCH = R / A::EPV;
+    typename A::PE *out = reinterpret_cast<typename A::PE *>(dst);
+    const int64_t pad = -(int64_t)lim - 1 + go;
+    for (int letter = 0; letter <= al; ++letter) {
+#pragma unroll
+        for (int k = 0; k < KCH; ++k) {
+#pragma unroll
+            for (int e = 0; e < A::EPV; ++e) {
+                const int32_t row = row_base + lane * R + k * A::EPV + e;
+                int64_t v;
+                if (row <= 0) {
+                    v = top_free ? go : 0;
+                } else if (letter == al) {
+                    v = pad;
+                } else {
+                    int64_t sub = matrix[(int32_t)q[row - 1] * al + letter];
+                    if (sub < -(int64_t)lim - 1) sub = -(int64_t)lim - 1;
+                    if (sub > lim) sub = lim;
+                    v = sub + go;
+                }
+                out[(((size_t)letter * KCH + k) * G + lane) * A::EPV + e] = (typename A::PE)v;
+            }
+        }
+    }
+}
+
+template <class A, int G, int R, int MODE, bool ENDS>
+__global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
+    typedef typename A::V V;
+    constexpr int RPP = G * R;
+    extern __shared__ __align__(128) uint8_t smem[];
+    const int lane = threadIdx.x % G;
+    const int gib = threadIdx.x / G;
+    const uint32_t item = blockIdx.x * (blockDim.x / G) + gib;
+    const bool active = item < p.n_items;
+    ItemMeta meta;
+    int32_t qlen = 0;
+    if (active) {
+        meta = p.meta[item];
+        qlen = (int32_t)p.qlen[item];
+    } else {
+        meta.col_off = 0;
+        meta.w = 0;
+        meta.n[0] = meta.n[1] = 0;
+        meta.idx[0] = meta.idx[1] = NO_INDEX;
+    }
+    const int32_t n_passes = (qlen + RPP - 1) / RPP;
+    const int32_t vrow0 = qlen - n_passes * RPP + 1;
+    const uint8_t *qa = active ? p.q_res + p.qoff[2 * (size_t)item] : p.q_res;
+    const uint8_t *qb = (active && A::NH > 1 && meta.idx[1] != NO_INDEX) ? p.q_res + p.qoff[2 * (size_t)item + 1] : qa;
+    uint8_t *gprof_a = smem + (size_t)gib * p.group_bytes;
+    uint8_t *gprof_b = gprof_a + p.group_bytes / 2;
+    const V Sv = A::splat(p.sentinel);
+    const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
+    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
+    const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
+    const int32_t pmax = (int32_t)__reduce_max_sync(0xffffffffu, (uint32_t)n_passes);
+
+    V best = A::splat(0);
+    Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
+    for (int pass = 0; pass < pmax; ++pass) {
+        const bool mine = pass < n_passes;
+        const int32_t row_base = vrow0 + pass * RPP;
+        if (mine) {
+            build_group_profile<A, G, R>(gprof_a, qa, qlen, row_base, p.matrix, p.al, p.lim, p.go,
+                                         p.top_free, lane);
+            if (A::NH > 1)
+                build_group_profile<A, G, R>(gprof_b, qb, qlen, row_base, p.matrix, p.al, p.lim,
+                                             p.go, p.top_free, lane);
+        }
+        __syncwarp();
+        // `steps` stays warp-uniform; a group past its last pass sweeps zero columns.
+        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, mine ? (int32_t)meta.w : 0, meta.n,
+                                        res, gprof_a, gprof_b, row_base + lane * R, pass == 0,
+                                        pass == n_passes - 1, bnd, qlen, p.go, p.ge, Sv, best, cand);
+        __syncwarp();
+    }
+    finish_item<A, G, MODE, ENDS>(lane, active, meta, qlen, p.go, p.ge, best, cand, p.scores,
+                                  p.qend, p.tend, nullptr);
+}
+
+// ---- query profile ----------------------------------------------------------------------------
+//
+// Layout of one pass slice: [letter 0..al][chunk k < R/EPV][lane < G][EPV elements], element e of
+// chunk k of lane L being grid row vrow0 + pass*G*R + L*R + k*EPV + e. Letter `al` is the padding
+// symbol. Values are P = clamp(sub, -(lim+1), lim) + go; virtual rows (<= 0) get go (free top
+// border) or 0 (penalised top border); the padding symbol gets -(lim+1) + go.
+template <class A, int G, int R>
+__global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32_t *matrix,
+                                     int32_t al, int32_t go, int32_t lim, int top_free,
+                                     int32_t vrow0, int32_t n_passes, typename A::PE *out) {
+    constexpr int KCH = R / A::EPV;
+    const int64_t per_pass = (int64_t)(al + 1) * G * R;
+    const int64_t total = per_pass * n_passes;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pass = i / per_pass;
+        int64_t rem = i % per_pass;
+        const int e = (int)(rem % A::EPV);
+        rem /= A::EPV;
+        const int lane = (int)(rem % G);
+        rem /= G;
+        const int k = (int)(rem % KCH);
+        const int letter = (int)(rem / KCH);
+        const int64_t row = vrow0 + pass * (G * R) + (int64_t)lane * R + k * A::EPV + e;
+        const int64_t pad = -(int64_t)lim - 1 + go;
+        int64_t v;
+        if (row <= 0) {
+            v = top_free ? go : 0;
+        } else if (letter == al) {
+            v = pad;
+        } else {
+            int64_t sub = matrix[(int64_t)q[row - 1] * al + letter];
+            if (sub < -(int64_t)lim - 1) sub = -(int64_t)lim - 1;
+            if (sub > lim) sub = lim;
+            v = sub + go;
+        }
+        out[i] = (typename A::PE)v;
+    }
+}
+
+}  // namespace hy

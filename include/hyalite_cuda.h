@@ -1,0 +1,199 @@
+/*
+ * hyalite_cuda.h -- C ABI of the B200 `cuda` backend for hyalite's inter-sequence database scan.
+ *
+ * Plain pointers and sizes only; no CUDA or torch types cross this boundary (the one stream
+ * accessor hands out an opaque pointer). Each declaration names the reference interface it
+ * replaces (paths inside Psy-Fer/hyalite). The matching Rust-side `extern "C"` block a maintainer
+ * would add is in INTEGRATION.md.
+ *
+ * Threading (src/database.rs:1-7, tests/database.rs:136-176): an hy_db is immutable after
+ * creation and may be shared by any number of host threads; an hy_scratch belongs to one thread
+ * at a time. Every call returns a status; error details are per thread (hy_last_error_detail).
+ * Residues are pre-encoded alphabet indices (0..alphabet_len), never ASCII (DETERMINISM.md).
+ */
+#ifndef HYALITE_CUDA_H
+#define HYALITE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. 1..11 mirror hyalite's Error variants one to one (src/error.rs:16-96); the rest
+ * are conditions the reference expresses as panics or that only a device backend has. */
+typedef enum {
+    HY_OK = 0,
+    HY_ERR_EMPTY_ALPHABET = 1,           /* Error::EmptyAlphabet */
+    HY_ERR_MATRIX_SHAPE = 2,             /* Error::MatrixShape {alphabet_len, expected, got} */
+    HY_ERR_NEGATIVE_GAP_PENALTY = 3,     /* Error::NegativeGapPenalty {gap_open, gap_ext} */
+    HY_ERR_GAP_OPEN_LESS_THAN_EXTEND = 4,/* Error::GapOpenLessThanExtend {gap_open, gap_ext} */
+    HY_ERR_SCORE_RANGE_TOO_WIDE = 5,     /* Error::ScoreRangeTooWide {bound} */
+    HY_ERR_SYMBOL_OUT_OF_RANGE = 6,      /* Error::SymbolOutOfRange {symbol, alphabet_len} */
+    HY_ERR_INCOMPLETE_BUILDER = 7,       /* Error::IncompleteBuilder (raised by host bindings) */
+    HY_ERR_EMPTY_DATABASE = 8,           /* Error::EmptyDatabase */
+    HY_ERR_BACKEND_UNAVAILABLE = 9,      /* Error::BackendUnavailable {backend} */
+    HY_ERR_INVALID_BACKEND_NAME = 10,    /* Error::InvalidBackendName {name} */
+    HY_ERR_TRACEBACK_BUDGET_EXCEEDED = 11,/* Error::TracebackBudgetExceeded (traceback not built) */
+    HY_ERR_INVALID_ARGUMENT = 20,        /* null pointer, bad enum value */
+    HY_ERR_QUERY_TOO_LONG = 21,          /* query longer than max_query_len (reference: debug_assert) */
+    HY_ERR_CUDA = 22,                    /* a CUDA runtime call failed; detail[0] = cudaError_t */
+    HY_ERR_OUT_OF_MEMORY = 23,           /* device or pinned allocation failed */
+    HY_ERR_TIMEOUT = 24,                 /* a bounded device wait ran out; the context stays usable */
+    HY_ERR_UNSUPPORTED = 25,             /* a search type or option this backend does not build */
+    HY_ERR_REJECTED = 26                 /* serving: admission refused (queue or memory full) */
+} hy_status;
+
+typedef enum { HY_MODE_SW = 0, HY_MODE_NW = 1, HY_MODE_HW = 2, HY_MODE_OV = 3, HY_MODE_SHW = 4 } hy_mode;
+typedef enum { HY_SEARCH_SCORE = 0, HY_SEARCH_SCORE_END = 1 } hy_search_type;
+typedef enum { HY_WIDTH_I8 = 0, HY_WIDTH_I16 = 1, HY_WIDTH_I32 = 2 } hy_score_width;
+/* Backend names of src/backend.rs:25-36 plus the new `Cuda` (the enum is #[non_exhaustive]). */
+typedef enum {
+    HY_BACKEND_SCALAR = 0, HY_BACKEND_SSE41 = 1, HY_BACKEND_AVX2 = 2, HY_BACKEND_NEON = 3,
+    HY_BACKEND_CUDA = 4
+} hy_backend;
+/* BackendChoice (src/backend.rs:123-133) as an int: HY_CHOICE_UNSET consults HYALITE_BACKEND,
+ * HY_CHOICE_AUTO detects, a hy_backend value forces that backend. */
+#define HY_CHOICE_UNSET (-2)
+#define HY_CHOICE_AUTO (-1)
+/* Layout / LayoutChoice (src/inter.rs:317-351): on the device, Gathered interleaves two per-letter
+ * query profiles per cell pair; Precomputed loads a pre-packed pair profile. Results identical. */
+#define HY_LAYOUT_AUTO (-1)
+#define HY_LAYOUT_GATHERED 0
+#define HY_LAYOUT_PRECOMPUTED 1
+
+/* BestHit (src/hit.rs:16-25). query_end / target_end are 0-based; -1 encodes None. */
+typedef struct {
+    int32_t score;
+    uint32_t reserved;
+    uint64_t db_index;
+    int64_t query_end;
+    int64_t target_end;
+} hy_hit;
+
+typedef struct hy_db hy_db;
+typedef struct hy_scratch hy_scratch;
+
+/* ---- errors -------------------------------------------------------------------------------- */
+
+/* The fields of the last error raised on this thread: MatrixShape {alphabet_len, expected, got};
+ * NegativeGapPenalty / GapOpenLessThanExtend {gap_open, gap_ext}; ScoreRangeTooWide {bound};
+ * SymbolOutOfRange {symbol, alphabet_len}; BackendUnavailable {backend}; QueryTooLong {len, max};
+ * Cuda {cudaError_t}. Unused fields are 0. */
+void hy_last_error_detail(int64_t detail[3]);
+/* A static, human-readable name for a status ("ScoreRangeTooWide", ...). */
+const char *hy_status_name(hy_status status);
+
+/* ---- backend selection (src/backend.rs) ------------------------------------------------------ */
+
+/* BackendChoice::parse (src/backend.rs:143-155), plus "cuda": case-insensitive, trimmed. Writes
+ * HY_CHOICE_AUTO or a hy_backend to *choice. */
+hy_status hy_backend_parse(const char *name, int *choice);
+/* Backend::is_available (src/backend.rs:77-84): only HY_BACKEND_CUDA is built here, and it is
+ * available iff a CUDA device can be used. */
+int hy_backend_is_available(hy_backend backend);
+/* resolve (src/backend.rs:176-187) + choice_from_env (195-204): HY_CHOICE_UNSET reads
+ * HYALITE_BACKEND, then falls back to auto. */
+hy_status hy_backend_resolve(int choice, hy_backend *out);
+/* Backend::name (src/backend.rs:40-48). */
+const char *hy_backend_name(hy_backend backend);
+
+/* ---- scoring and width proof ----------------------------------------------------------------- */
+
+/* Scoring::new validation (src/scoring.rs:65-100). */
+hy_status hy_scoring_validate(uint64_t alphabet_len, const int32_t *matrix, uint64_t matrix_len,
+                              int32_t gap_open, int32_t gap_ext);
+/* width::required_width (src/width.rs:145-169). *bound receives the clamped magnitude bound. */
+hy_status hy_required_width(hy_mode mode, int32_t min_entry, int32_t max_entry, int32_t gap_open,
+                            int32_t gap_ext, uint64_t max_query_len, uint64_t max_target_len,
+                            hy_score_width *width, int64_t *bound);
+
+/* ---- database (src/database.rs) -------------------------------------------------------------- */
+
+/* DatabaseBuilder::build (src/database.rs:737-877): sequence k is residues[offsets[k] ..
+ * offsets[k+1]] (offsets has n_seqs + 1 entries). Validates in the reference's order (scoring,
+ * empty database, symbols in db order, whole-database width proof, backend), then packs the
+ * database into device memory on the current CUDA device, where it stays until hy_db_destroy.
+ * backend_choice: HY_CHOICE_UNSET / HY_CHOICE_AUTO / a hy_backend. layout: HY_LAYOUT_*. */
+hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                       const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
+                       int32_t gap_ext, hy_mode mode, hy_search_type search_type,
+                       uint64_t max_query_len, int backend_choice, int layout, hy_db **out);
+void hy_db_destroy(hy_db *db);
+
+/* Accessors (src/database.rs:570-638). score_width is the reference's whole-database proof (the
+ * widest width); the device partitions by its own per-sequence proof. */
+uint64_t hy_db_sequence_count(const hy_db *db);
+hy_mode hy_db_mode(const hy_db *db);
+hy_search_type hy_db_search_type(const hy_db *db);
+hy_score_width hy_db_score_width(const hy_db *db);
+hy_backend hy_db_backend(const hy_db *db);
+int hy_db_layout(const hy_db *db);
+uint64_t hy_db_max_query_len(const hy_db *db);
+uint64_t hy_db_max_target_len(const hy_db *db);
+/* Device bytes held by the database, and device bytes one hy_scratch needs. */
+uint64_t hy_db_device_bytes(const hy_db *db);
+uint64_t hy_db_scratch_bytes(const hy_db *db);
+/* Number of sequences the device runs in packed int16x2 pairs and in int32 lanes. */
+void hy_db_partition(const hy_db *db, uint64_t *n_i16, uint64_t *n_i32);
+
+/* Scratch::new (src/database.rs:965-998): one CUDA stream plus device work and output buffers,
+ * sized for the database. Exclusive to one host thread at a time. */
+hy_status hy_scratch_create(const hy_db *db, hy_scratch **out);
+void hy_scratch_destroy(hy_scratch *scratch);
+/* The scratch's cudaStream_t, as an opaque pointer (for event timing and graph capture). */
+void *hy_scratch_stream(hy_scratch *scratch);
+
+/* Database::scan (src/database.rs:83-144): the single best hit; ties go to the smallest db_index.
+ * Host query in, host hit out; blocks until the result is in *out. */
+hy_status hy_scan(const hy_db *db, hy_scratch *scratch, const uint8_t *query, uint64_t qlen,
+                  hy_hit *out);
+/* Database::scan_all (src/database.rs:347-464): one hit per sequence in db order (out has
+ * hy_db_sequence_count entries). */
+hy_status hy_scan_all(const hy_db *db, hy_scratch *scratch, const uint8_t *query, uint64_t qlen,
+                      hy_hit *out);
+/* Database::scan_scores (src/database.rs:481-515): every sequence's best score in db order. */
+hy_status hy_scan_scores(const hy_db *db, hy_scratch *scratch, const uint8_t *query,
+                         uint64_t qlen, int32_t *out);
+
+/* Device-resident forms of scan / scan_scores: the query is already in device memory and the
+ * result is written to device memory, asynchronously on the scratch's stream (no host sync).
+ * The query's symbols must already be validated (hy_query_validate). */
+hy_status hy_scan_device(const hy_db *db, hy_scratch *scratch, const uint8_t *d_query,
+                         uint64_t qlen, hy_hit *d_out);
+hy_status hy_scan_scores_device(const hy_db *db, hy_scratch *scratch, const uint8_t *d_query,
+                                uint64_t qlen, int32_t *d_out);
+/* The checks hy_scan performs on a host query (length, then symbols). */
+hy_status hy_query_validate(const hy_db *db, const uint8_t *query, uint64_t qlen);
+/* Waits for the scratch's stream; returns HY_ERR_TIMEOUT if a kernel's bounded wait ran out. */
+hy_status hy_scratch_sync(hy_scratch *scratch);
+
+/* ---- measurement (no reference counterpart: the reference benches with criterion) ------------ */
+
+/* While enabled, every main scan-kernel launch on this scratch is bracketed by CUDA events on the
+ * scratch's stream. _read synchronises and returns, since the last read (or enable), the summed
+ * kernel time and launch count of the int16x2 pair kernel ([0]) and the int32 kernel ([1]), plus
+ * the number of kernels of every kind this scratch launched; then it resets them. */
+hy_status hy_scratch_profile(hy_scratch *scratch, int enable);
+hy_status hy_scratch_profile_read(hy_scratch *scratch, double kernel_ms[2], uint64_t launches[2],
+                                  uint64_t *all_launches);
+/* The packed-int16 DPX roofline of the current device: the scan's per-cell instruction mix run
+ * register resident on every SM, in DP cells per second. */
+hy_status hy_measure_dpx_peak(double *cells_per_second);
+
+/* ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------- */
+
+/* align_pairs: pair p is (q_res[q_off[p]..q_off[p+1]], t_res[t_off[p]..t_off[p+1]]). Each pair is
+ * validated in order (symbols query-then-target, then the width proof on its exact lengths); on
+ * the first failing pair the call returns its error, *failed_pair receives its index and out[0 ..
+ * index) holds the hits of the pairs before it. db_index of each hit is its pair index. */
+hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                         const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
+                         uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
+                         hy_search_type search_type, hy_hit *out, uint64_t *failed_pair);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,425 @@
+/*
+ * hyoracle.c -- TEST INFRASTRUCTURE ONLY (see hyoracle.h).
+ *
+ * Plain-C restatement of hyalite's scalar reference kernel and of its database/pairwise result
+ * semantics. Arithmetic is carried in int64 so no intermediate can overflow; for every input the
+ * reference's width proof accepts, the reference's i32 arithmetic never wraps either, so the two
+ * compute identical values.
+ */
+#include "hyoracle.h"
+
+#include <limits.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Status codes: must equal the HY_* values of include/hyalite_cuda.h. */
+enum {
+    ST_OK = 0,
+    ST_EMPTY_ALPHABET = 1,
+    ST_MATRIX_SHAPE = 2,
+    ST_NEGATIVE_GAP_PENALTY = 3,
+    ST_GAP_OPEN_LESS_THAN_EXTEND = 4,
+    ST_SCORE_RANGE_TOO_WIDE = 5,
+    ST_SYMBOL_OUT_OF_RANGE = 6,
+};
+
+/* kernel::NEG = i32::MIN / 4 (src/kernel.rs:39). */
+#define ORC_NEG ((int64_t)(INT32_MIN / 4))
+
+/* Flags::for_mode (src/kernel.rs:43-98). */
+typedef struct {
+    int top_row_free, left_col_free, answer_last_row, answer_last_col, local;
+} flags_t;
+
+static flags_t flags_for_mode(int mode) {
+    flags_t f = {0, 0, 0, 0, 0};
+    switch (mode) {
+    case 0: /* SW */ f.top_row_free = 1; f.left_col_free = 1; f.local = 1; break;
+    case 1: /* NW */ break;
+    case 2: /* HW */ f.top_row_free = 1; f.answer_last_row = 1; break;
+    case 3: /* OV */
+        f.top_row_free = 1; f.left_col_free = 1; f.answer_last_row = 1; f.answer_last_col = 1;
+        break;
+    default: /* SHW */ f.left_col_free = 1; f.answer_last_col = 1; break;
+    }
+    return f;
+}
+
+/* gap_penalty (src/kernel.rs:103-109): computed in i64, cast to i32 like the reference. */
+static int64_t gap_penalty(int32_t go, int32_t ge, uint64_t len) {
+    if (len == 0) return 0;
+    int64_t v = (int64_t)go + ((int64_t)len - 1) * (int64_t)ge;
+    return (int64_t)(int32_t)v;
+}
+
+/* Best::consider (src/kernel.rs:113-129): maximise score, then minimise (grid_col, grid_row). */
+typedef struct {
+    int64_t score;
+    uint64_t row, col;
+} best_t;
+
+static inline void consider(best_t *b, int64_t s, uint64_t row, uint64_t col) {
+    if (s > b->score || (s == b->score && (col < b->col || (col == b->col && row < b->row)))) {
+        b->score = s;
+        b->row = row;
+        b->col = col;
+    }
+}
+
+int hyo_scoring_validate(uint64_t alphabet_len, const int32_t *matrix, uint64_t matrix_len,
+                         int32_t gap_open, int32_t gap_ext, int64_t *d1, int64_t *d2, int64_t *d3) {
+    (void)matrix;
+    if (alphabet_len == 0) return ST_EMPTY_ALPHABET;
+    unsigned __int128 sq = (unsigned __int128)alphabet_len * alphabet_len;
+    if (sq != matrix_len) {
+        if (d1) *d1 = (int64_t)alphabet_len;
+        if (d2) *d2 = sq > (unsigned __int128)INT64_MAX ? INT64_MAX : (int64_t)sq;
+        if (d3) *d3 = (int64_t)matrix_len;
+        return ST_MATRIX_SHAPE;
+    }
+    if (gap_open < 0 || gap_ext < 0) {
+        if (d1) *d1 = gap_open;
+        if (d2) *d2 = gap_ext;
+        return ST_NEGATIVE_GAP_PENALTY;
+    }
+    if (gap_open < gap_ext) {
+        if (d1) *d1 = gap_open;
+        if (d2) *d2 = gap_ext;
+        return ST_GAP_OPEN_LESS_THAN_EXTEND;
+    }
+    return ST_OK;
+}
+
+/* magnitude_bound (src/width.rs:107-137), in 128-bit so products cannot wrap, then the i64 clamp
+ * of required_width (src/width.rs:157). */
+int64_t hyo_magnitude_bound(int mode, int32_t min_entry, int32_t max_entry, int32_t gap_open,
+                            int32_t gap_ext, uint64_t max_query_len, uint64_t max_target_len) {
+    __int128 m = (__int128)max_query_len;
+    __int128 n = (__int128)max_target_len;
+    __int128 min_ij = m < n ? m : n;
+    __int128 max_pos = max_entry > 0 ? (__int128)max_entry : 0;
+    __int128 max_neg = -(__int128)min_entry > 0 ? -(__int128)min_entry : 0;
+    __int128 go = gap_open, ge = gap_ext;
+    __int128 positive = min_ij * max_pos;
+    __int128 negative;
+    if (mode == 0) {
+        negative = go;
+    } else if (mode == 3) {
+        negative = min_ij * max_neg + go;
+    } else {
+        __int128 run = m + n - 1;
+        if (run < 0) run = 0;
+        negative = (m + n) * max_neg + go + run * ge;
+    }
+    __int128 bound = positive > negative ? positive : negative;
+    if (bound > (__int128)INT64_MAX) bound = INT64_MAX;
+    return (int64_t)bound;
+}
+
+/* required_width + ScoreWidth::narrowest_for/max_abs (src/width.rs:49-71, 145-169). */
+int hyo_required_width(int mode, int32_t min_entry, int32_t max_entry, int32_t gap_open,
+                       int32_t gap_ext, uint64_t max_query_len, uint64_t max_target_len,
+                       int64_t *bound_out) {
+    int64_t b = hyo_magnitude_bound(mode, min_entry, max_entry, gap_open, gap_ext, max_query_len,
+                                    max_target_len);
+    if (bound_out) *bound_out = b;
+    if (b <= 127) return 0;
+    if (b <= 32767) return 1;
+    if (b <= 536870911) return 2;
+    return -1;
+}
+
+/* fill_dp + reduce_answer (src/kernel.rs:168-260), restated with rolling rows: the same cells are
+ * computed in the same order with the same arithmetic, and the answer region and tie-break of
+ * reduce_answer are applied to them (the tie-break is an explicit comparison, so visiting order
+ * does not matter). */
+void hyo_align_core(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
+                    const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
+                    int mode, int32_t *score, int64_t *query_end, int64_t *target_end) {
+    flags_t fl = flags_for_mode(mode);
+    const int64_t go = gap_open, ge = gap_ext;
+    uint64_t cols = n + 1;
+    int64_t *prev = (int64_t *)malloc(sizeof(int64_t) * cols);
+    int64_t *cur = (int64_t *)malloc(sizeof(int64_t) * cols);
+    int64_t *f = (int64_t *)malloc(sizeof(int64_t) * cols);
+    int64_t *lastcol = (int64_t *)malloc(sizeof(int64_t) * (m + 1));
+    best_t best = {ORC_NEG, 0, 0};
+
+    for (uint64_t j = 0; j <= n; ++j) {
+        prev[j] = (j == 0 || fl.top_row_free) ? 0 : -gap_penalty(gap_open, gap_ext, j);
+        f[j] = ORC_NEG;
+    }
+    if (fl.local)
+        for (uint64_t j = 0; j <= n; ++j) consider(&best, prev[j], 0, j);
+    lastcol[0] = prev[n];
+
+    for (uint64_t i = 1; i <= m; ++i) {
+        cur[0] = fl.left_col_free ? 0 : -gap_penalty(gap_open, gap_ext, i);
+        int64_t e = ORC_NEG;
+        const int32_t *qrow = matrix + (uint64_t)q[i - 1] * al;
+        for (uint64_t j = 1; j <= n; ++j) {
+            int64_t a = cur[j - 1] - go, b = e - ge;
+            e = a > b ? a : b;
+            int64_t c = prev[j] - go, d = f[j] - ge;
+            f[j] = c > d ? c : d;
+            int64_t diag = prev[j - 1] + (int64_t)qrow[t[j - 1]];
+            int64_t cell = diag > e ? diag : e;
+            if (f[j] > cell) cell = f[j];
+            if (fl.local && cell < 0) cell = 0;
+            cur[j] = cell;
+        }
+        if (fl.local)
+            for (uint64_t j = 0; j <= n; ++j) consider(&best, cur[j], i, j);
+        lastcol[i] = cur[n];
+        int64_t *tmp = prev;
+        prev = cur;
+        cur = tmp;
+    }
+    /* prev holds row m. */
+    if (!fl.local) {
+        consider(&best, prev[n], m, n);
+        if (fl.answer_last_row)
+            for (uint64_t j = 0; j <= n; ++j) consider(&best, prev[j], m, j);
+        if (fl.answer_last_col)
+            for (uint64_t i = 0; i <= m; ++i) consider(&best, lastcol[i], i, n);
+    }
+    *score = (int32_t)best.score;
+    *query_end = best.row == 0 ? -1 : (int64_t)best.row - 1;
+    *target_end = best.col == 0 ? -1 : (int64_t)best.col - 1;
+    free(prev);
+    free(cur);
+    free(f);
+    free(lastcol);
+}
+
+/* Database::scan: highest score, smallest db_index on a tie (src/database.rs:117-130, 173-180);
+ * ScoreEnd ends come from one scalar re-alignment of the winner (186-197), Score drops them. */
+void hyo_scan(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+              const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext, int mode,
+              int search_type, const uint8_t *query, uint64_t qlen, hyo_hit *out) {
+    int64_t best_score = INT32_MIN;
+    uint64_t best_index = 0;
+    int64_t bq = -1, bt = -1;
+    for (uint64_t k = 0; k < n_seqs; ++k) {
+        int32_t s;
+        int64_t qe, te;
+        hyo_align_core(query, qlen, residues + offsets[k], offsets[k + 1] - offsets[k], matrix,
+                       al, gap_open, gap_ext, mode, &s, &qe, &te);
+        if (s > best_score) {
+            best_score = s;
+            best_index = k;
+            bq = qe;
+            bt = te;
+        }
+    }
+    out->score = (int32_t)best_score;
+    out->db_index = best_index;
+    out->query_end = search_type == 1 ? bq : -1;
+    out->target_end = search_type == 1 ? bt : -1;
+}
+
+static void scan_all_range(const uint8_t *residues, const uint64_t *offsets, uint64_t lo,
+                           uint64_t hi, const int32_t *matrix, uint64_t al, int32_t go,
+                           int32_t ge, int mode, int search_type, const uint8_t *query,
+                           uint64_t qlen, hyo_hit *out) {
+    for (uint64_t k = lo; k < hi; ++k) {
+        int32_t s;
+        int64_t qe, te;
+        hyo_align_core(query, qlen, residues + offsets[k], offsets[k + 1] - offsets[k], matrix,
+                       al, go, ge, mode, &s, &qe, &te);
+        out[k].score = s;
+        out[k].db_index = k;
+        out[k].query_end = search_type == 1 ? qe : -1;
+        out[k].target_end = search_type == 1 ? te : -1;
+    }
+}
+
+/* Database::scan_all (src/database.rs:347-464): one hit per sequence in db order; ScoreEnd ends
+ * equal the scalar oracle's (end = grid - 1, None at grid 0: 395-402). */
+void hyo_scan_all(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                  const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext, int mode,
+                  int search_type, const uint8_t *query, uint64_t qlen, hyo_hit *out) {
+    scan_all_range(residues, offsets, 0, n_seqs, matrix, al, gap_open, gap_ext, mode, search_type,
+                   query, qlen, out);
+}
+
+/* Database::scan_scores (src/database.rs:481-515): every sequence's best score in db order. */
+void hyo_scan_scores(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                     const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
+                     int mode, const uint8_t *query, uint64_t qlen, int32_t *out) {
+    for (uint64_t k = 0; k < n_seqs; ++k) {
+        int64_t qe, te;
+        hyo_align_core(query, qlen, residues + offsets[k], offsets[k + 1] - offsets[k], matrix,
+                       al, gap_open, gap_ext, mode, &out[k], &qe, &te);
+    }
+}
+
+void hyo_scan_scores_mt(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                        const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
+                        int mode, const uint8_t *query, uint64_t qlen, int32_t *out, int threads) {
+    if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+    for (int64_t k = 0; k < (int64_t)n_seqs; ++k) {
+        int64_t qe, te;
+        hyo_align_core(query, qlen, residues + offsets[k], offsets[k + 1] - offsets[k], matrix,
+                       al, gap_open, gap_ext, mode, &out[k], &qe, &te);
+    }
+}
+
+void hyo_scan_all_mt(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                     const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
+                     int mode, int search_type, const uint8_t *query, uint64_t qlen, hyo_hit *out,
+                     int threads) {
+    if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+    for (int64_t k = 0; k < (int64_t)n_seqs; ++k)
+        scan_all_range(residues, offsets, (uint64_t)k, (uint64_t)k + 1, matrix, al, gap_open,
+                       gap_ext, mode, search_type, query, qlen, out);
+}
+
+/* align_pairs (src/kernel.rs:429-452) -> align_pair_with (354-415): per pair, symbols are checked
+ * query-then-target (362-370), then the width proof on the pair's exact lengths (373); the first
+ * failing pair's error is returned and the hits of the pairs before it stay written. The striped
+ * Score fast path (378-397) is bit-identical to align_core, so align_core stands for both. */
+int hyo_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                    const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix, uint64_t al,
+                    int32_t gap_open, int32_t gap_ext, int mode, int search_type, hyo_hit *out,
+                    int threads, int64_t *d1, int64_t *d2) {
+    int32_t min_e = INT32_MAX, max_e = INT32_MIN;
+    for (uint64_t i = 0; i < al * al; ++i) {
+        if (matrix[i] < min_e) min_e = matrix[i];
+        if (matrix[i] > max_e) max_e = matrix[i];
+    }
+    uint64_t n_ok = n_pairs;
+    int status = ST_OK;
+    for (uint64_t p = 0; p < n_pairs && status == ST_OK; ++p) {
+        const uint8_t *seqs[2] = {q_res + q_off[p], t_res + t_off[p]};
+        uint64_t lens[2] = {q_off[p + 1] - q_off[p], t_off[p + 1] - t_off[p]};
+        for (int s = 0; s < 2 && status == ST_OK; ++s)
+            for (uint64_t i = 0; i < lens[s]; ++i)
+                if (seqs[s][i] >= al) {
+                    status = ST_SYMBOL_OUT_OF_RANGE;
+                    if (d1) *d1 = seqs[s][i];
+                    if (d2) *d2 = (int64_t)al;
+                    break;
+                }
+        if (status == ST_OK) {
+            int64_t bound;
+            if (hyo_required_width(mode, min_e, max_e, gap_open, gap_ext, lens[0], lens[1],
+                                   &bound) < 0) {
+                status = ST_SCORE_RANGE_TOO_WIDE;
+                if (d1) *d1 = bound;
+            }
+        }
+        if (status != ST_OK) n_ok = p;
+    }
+    if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t p = 0; p < (int64_t)n_ok; ++p) {
+        int32_t s;
+        int64_t qe, te;
+        hyo_align_core(q_res + q_off[p], q_off[p + 1] - q_off[p], t_res + t_off[p],
+                       t_off[p + 1] - t_off[p], matrix, al, gap_open, gap_ext, mode, &s, &qe, &te);
+        out[p].score = s;
+        out[p].db_index = (uint64_t)p;
+        out[p].query_end = search_type == 1 ? qe : -1;
+        out[p].target_end = search_type == 1 ? te : -1;
+    }
+    return status;
+}
+
+/* ---- brute force (tests/common/mod.rs:65-171) ------------------------------------------- */
+
+typedef struct {
+    const uint8_t *q, *t;
+    uint64_t m, n;
+    const int32_t *mat;
+    uint64_t al;
+    int32_t go, ge;
+} prob_t;
+
+static int32_t sat_add(int32_t a, int32_t b) {
+    int64_t s = (int64_t)a + b;
+    if (s > INT32_MAX) return INT32_MAX;
+    if (s < INT32_MIN) return INT32_MIN;
+    return (int32_t)s;
+}
+
+/* brute_nw's recursion: every path, affine gaps charged from maximal same-direction runs.
+ * last: 0 start/diagonal, 1 right (gap in query), 2 down (gap in target). */
+static int32_t brute_rec(const prob_t *p, uint64_t i, uint64_t j, int last) {
+    if (i == p->m && j == p->n) return 0;
+    int32_t best = INT32_MIN;
+    if (i < p->m && j < p->n) {
+        int32_t s = p->mat[(uint64_t)p->q[i] * p->al + p->t[j]];
+        int32_t v = sat_add(s, brute_rec(p, i + 1, j + 1, 0));
+        if (v > best) best = v;
+    }
+    if (j < p->n) {
+        int32_t cost = last == 1 ? p->ge : p->go;
+        int32_t v = sat_add(-cost, brute_rec(p, i, j + 1, 1));
+        if (v > best) best = v;
+    }
+    if (i < p->m) {
+        int32_t cost = last == 2 ? p->ge : p->go;
+        int32_t v = sat_add(-cost, brute_rec(p, i + 1, j, 2));
+        if (v > best) best = v;
+    }
+    return best;
+}
+
+static int32_t brute_nw(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
+                        const int32_t *mat, uint64_t al, int32_t go, int32_t ge) {
+    prob_t p = {q, t, m, n, mat, al, go, ge};
+    return brute_rec(&p, 0, 0, 0);
+}
+
+int32_t hyo_brute(int mode, const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
+                  const int32_t *mat, uint64_t al, int32_t go, int32_t ge) {
+    int32_t best;
+    switch (mode) {
+    case 1: /* NW */
+        return brute_nw(q, m, t, n, mat, al, go, ge);
+    case 0: /* SW: best over every substring pair, floored at 0 */
+        best = 0;
+        for (uint64_t a = 0; a <= m; ++a)
+            for (uint64_t b = a; b <= m; ++b)
+                for (uint64_t c = 0; c <= n; ++c)
+                    for (uint64_t d = c; d <= n; ++d) {
+                        int32_t v = brute_nw(q + a, b - a, t + c, d - c, mat, al, go, ge);
+                        if (v > best) best = v;
+                    }
+        return best;
+    case 2: /* HW: whole query against the best target window */
+        best = INT32_MIN;
+        for (uint64_t c = 0; c <= n; ++c)
+            for (uint64_t d = c; d <= n; ++d) {
+                int32_t v = brute_nw(q, m, t + c, d - c, mat, al, go, ge);
+                if (v > best) best = v;
+            }
+        return best;
+    case 3: /* OV: substring pairs touching a border at both ends, floored at 0 */
+        best = 0;
+        for (uint64_t a = 0; a <= m; ++a)
+            for (uint64_t b = a; b <= m; ++b)
+                for (uint64_t c = 0; c <= n; ++c)
+                    for (uint64_t d = c; d <= n; ++d)
+                        if ((a == 0 || c == 0) && (b == m || d == n)) {
+                            int32_t v = brute_nw(q + a, b - a, t + c, d - c, mat, al, go, ge);
+                            if (v > best) best = v;
+                        }
+        return best;
+    default: /* SHW: whole target against the best query window */
+        best = INT32_MIN;
+        for (uint64_t a = 0; a <= m; ++a)
+            for (uint64_t b = a; b <= m; ++b) {
+                int32_t v = brute_nw(q + a, b - a, t, n, mat, al, go, ge);
+                if (v > best) best = v;
+            }
+        return best;
+    }
+}

@@ -1,0 +1,206 @@
+"""TEST/BENCH INFRASTRUCTURE ONLY: ctypes access to oracle/liboracle.so.
+
+The scalar oracle (hyoracle.c) checks the CUDA backend in tests/ and __graft_entry__.smoke(); the
+AVX2 restatement (avx2_port.cpp) is the CPU baseline bench.py times. The shipped package never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+class Hit(C.Structure):
+    _fields_ = [("score", C.c_int32), ("db_index", C.c_uint64), ("query_end", C.c_int64),
+                ("target_end", C.c_int64)]
+
+
+_u8p = C.POINTER(C.c_uint8)
+_u64p = C.POINTER(C.c_uint64)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+def _load():
+    if not os.path.exists(LIB):
+        build()
+    lib = C.CDLL(LIB)
+    sig = {
+        "hyo_scoring_validate": (C.c_int, [C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, _i64p, _i64p, _i64p]),
+        "hyo_magnitude_bound": (C.c_int64, [C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64]),
+        "hyo_required_width": (C.c_int, [C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, _i64p]),
+        "hyo_align_core": (None, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _i32p, _i64p, _i64p]),
+        "hyo_scan": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, _u8p, C.c_uint64, C.POINTER(Hit)]),
+        "hyo_scan_all_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, _u8p, C.c_uint64, C.POINTER(Hit), C.c_int]),
+        "hyo_scan_scores_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _u8p, C.c_uint64, _i32p, C.c_int]),
+        "hyo_align_pairs": (C.c_int, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, C.POINTER(Hit), C.c_int, _i64p, _i64p]),
+        "hyo_brute": (C.c_int32, [C.c_int, _u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32]),
+        "hyb_db_create": (C.c_void_p, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, C.c_uint64, C.c_int]),
+        "hyb_db_destroy": (None, [C.c_void_p]),
+        "hyb_scratch_create": (C.c_void_p, []),
+        "hyb_scratch_destroy": (None, [C.c_void_p]),
+        "hyb_scan": (None, [C.c_void_p, C.c_void_p, _u8p, C.c_uint64, C.POINTER(Hit)]),
+        "hyb_scan_scores": (None, [C.c_void_p, C.c_void_p, _u8p, C.c_uint64, _i32p]),
+        "hyb_scan_many": (None, [C.c_void_p, _u8p, _u64p, C.c_uint64, C.POINTER(Hit), C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _u8(a):
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    return a if a.size else np.zeros(1, np.uint8)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def as_hit(h):
+    """(score, db_index, query_end or None, target_end or None)."""
+    return (int(h.score), int(h.db_index), None if h.query_end < 0 else int(h.query_end),
+            None if h.target_end < 0 else int(h.target_end))
+
+
+def _mat(matrix):
+    return np.ascontiguousarray(np.asarray(matrix, dtype=np.int64).astype(np.int32))
+
+
+def concat(seqs):
+    parts = [np.asarray(list(s) if not isinstance(s, np.ndarray) else s, dtype=np.int64).astype(np.uint8)
+             for s in seqs]
+    off = np.zeros(len(parts) + 1, np.uint64)
+    if parts:
+        off[1:] = np.cumsum([len(p) for p in parts])
+    res = np.concatenate(parts) if parts and off[-1] else np.zeros(1, np.uint8)
+    return _u8(res), off
+
+
+def required_width(mode, min_e, max_e, go, ge, m, n):
+    b = C.c_int64()
+    w = lib.hyo_required_width(int(mode), min_e, max_e, go, ge, m, n, C.byref(b))
+    return w, int(b.value)
+
+
+def magnitude_bound(mode, min_e, max_e, go, ge, m, n):
+    return int(lib.hyo_magnitude_bound(int(mode), min_e, max_e, go, ge, m, n))
+
+
+def align_pair(q, t, matrix, al, go, ge, mode, search_type=1):
+    """(score, query_end, target_end) of one pair (align_core); ends None for Score."""
+    qa = np.asarray(list(q), dtype=np.int64).astype(np.uint8)
+    ta = np.asarray(list(t), dtype=np.int64).astype(np.uint8)
+    qb, tb, mat = _u8(qa), _u8(ta), _mat(matrix)
+    s, qe, te = C.c_int32(), C.c_int64(), C.c_int64()
+    lib.hyo_align_core(_p(qb, _u8p), len(qa), _p(tb, _u8p), len(ta), _p(mat, _i32p), al, go, ge,
+                       int(mode), C.byref(s), C.byref(qe), C.byref(te))
+    if search_type == 0:
+        return int(s.value), None, None
+    return (int(s.value), None if qe.value < 0 else int(qe.value),
+            None if te.value < 0 else int(te.value))
+
+
+class OracleDb:
+    """The scalar oracle's view of a database: scan / scan_all / scan_scores semantics."""
+
+    def __init__(self, seqs_or_concat, matrix, al, go, ge, mode, search_type):
+        if isinstance(seqs_or_concat, tuple):
+            self.res, self.off = _u8(seqs_or_concat[0]), np.ascontiguousarray(seqs_or_concat[1], dtype=np.uint64)
+        else:
+            self.res, self.off = concat(seqs_or_concat)
+        self.n = len(self.off) - 1
+        self.mat = _mat(matrix)
+        self.al, self.go, self.ge, self.mode, self.st = al, go, ge, int(mode), int(search_type)
+
+    def _args(self):
+        return (_p(self.res, _u8p), _p(self.off, _u64p), self.n, _p(self.mat, _i32p), self.al,
+                self.go, self.ge, self.mode)
+
+    def scan(self, query):
+        q = _u8(np.asarray(list(query), dtype=np.int64).astype(np.uint8) if not isinstance(query, np.ndarray) else query)
+        ql = len(query)
+        h = Hit()
+        lib.hyo_scan(*self._args(), self.st, _p(q, _u8p), ql, C.byref(h))
+        return as_hit(h)
+
+    def scan_all(self, query, threads=8):
+        q = _u8(np.asarray(list(query), dtype=np.int64).astype(np.uint8) if not isinstance(query, np.ndarray) else query)
+        out = (Hit * max(self.n, 1))()
+        lib.hyo_scan_all_mt(*self._args(), self.st, _p(q, _u8p), len(query), out, threads)
+        return [as_hit(out[k]) for k in range(self.n)]
+
+    def scan_scores(self, query, threads=8):
+        q = _u8(np.asarray(list(query), dtype=np.int64).astype(np.uint8) if not isinstance(query, np.ndarray) else query)
+        out = np.empty(max(self.n, 1), np.int32)
+        lib.hyo_scan_scores_mt(*self._args(), _p(q, _u8p), len(query), _p(out, _i32p), threads)
+        return out[: self.n]
+
+
+def align_pairs(pairs_q, pairs_t, matrix, al, go, ge, mode, search_type, threads=8):
+    """Returns (status, failed_index, hits list)."""
+    qr, qo = concat(pairs_q)
+    tr, to = concat(pairs_t)
+    mat = _mat(matrix)
+    n = len(qo) - 1
+    out = (Hit * max(n, 1))()
+    d1, d2 = C.c_int64(), C.c_int64()
+    st = lib.hyo_align_pairs(_p(qr, _u8p), _p(qo, _u64p), _p(tr, _u8p), _p(to, _u64p), n, _p(mat, _i32p),
+                             al, go, ge, int(mode), int(search_type), out, threads, C.byref(d1), C.byref(d2))
+    return st, [as_hit(out[k]) for k in range(n)], (int(d1.value), int(d2.value))
+
+
+def brute(mode, q, t, matrix, al, go, ge):
+    qa = _u8(np.asarray(list(q), dtype=np.int64).astype(np.uint8))
+    ta = _u8(np.asarray(list(t), dtype=np.int64).astype(np.uint8))
+    mat = _mat(matrix)
+    return int(lib.hyo_brute(int(mode), _p(qa, _u8p), len(q), _p(ta, _u8p), len(t), _p(mat, _i32p), al, go, ge))
+
+
+class Avx2Db:
+    """The AVX2 baseline restatement (db-order batches, Precomputed, width groups)."""
+
+    def __init__(self, res, off, matrix, al, go, ge, mode, search_type, max_query_len, gathered_i8=False):
+        self.res, self.off = _u8(res), np.ascontiguousarray(off, dtype=np.uint64)
+        self.mat = _mat(matrix)
+        self.h = lib.hyb_db_create(_p(self.res, _u8p), _p(self.off, _u64p), len(self.off) - 1,
+                                   _p(self.mat, _i32p), al, go, ge, int(mode), int(search_type),
+                                   max_query_len, 1 if gathered_i8 else 0)
+        if not self.h:
+            raise ValueError("width proof failed")
+        self.n = len(self.off) - 1
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.hyb_db_destroy(self.h)
+            self.h = None
+
+    def scan_many(self, queries, threads):
+        qr, qo = concat(queries)
+        out = (Hit * max(len(queries), 1))()
+        lib.hyb_scan_many(self.h, _p(qr, _u8p), _p(qo, _u64p), len(queries), out, threads)
+        return [as_hit(out[k]) for k in range(len(queries))]
+
+    def scan_scores(self, query):
+        q = _u8(np.asarray(list(query), dtype=np.int64).astype(np.uint8))
+        sc = lib.hyb_scratch_create()
+        out = np.empty(max(self.n, 1), np.int32)
+        lib.hyb_scan_scores(self.h, sc, _p(q, _u8p), len(query), _p(out, _i32p))
+        lib.hyb_scratch_destroy(sc)
+        return out[: self.n]

@@ -1,0 +1,148 @@
+"""CPU-side checks of the product library: it loads, exports every symbol include/hyalite_cuda.h
+declares, and its host logic (validation order, backend selection, width proof) mirrors the
+reference. No kernel runs here."""
+import ctypes as C
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+from conftest import DNA, ROOT, identity_matrix
+
+import hyalite_b200 as hy
+from hyalite_b200 import _abi
+
+
+def _declared_functions():
+    text = open(os.path.join(ROOT, "include", "hyalite_cuda.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hy_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = _declared_functions()
+    assert len(names) >= 30
+    lib = C.CDLL(_abi.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(_abi.SIGNATURES), set(names) ^ set(_abi.SIGNATURES)
+
+
+def test_library_links_no_oracle_code():
+    out = subprocess.run(["nm", "-D", "--defined-only", _abi.LIB_PATH], capture_output=True, text=True).stdout
+    assert "hyo_" not in out and "hyb_" not in out
+
+
+def test_status_names_cover_error_variants():
+    for code, name in _abi.STATUS_NAMES.items():
+        assert _abi.lib.hy_status_name(code).decode() == name
+
+
+def test_scoring_validation_order():
+    # src/scoring.rs:65-100 and its tests
+    with pytest.raises(hy.Error) as e:
+        hy.Scoring(0, [], 1, 1)
+    assert e.value.kind == "EmptyAlphabet"
+    with pytest.raises(hy.Error) as e:
+        hy.Scoring(3, [1, 2], 1, 1)
+    assert e.value == hy.Error("MatrixShape", alphabet_len=3, expected=9, got=2)
+    with pytest.raises(hy.Error) as e:
+        hy.Scoring(2, [1, -1, -1, 1], -1, 0)
+    assert e.value == hy.Error("NegativeGapPenalty", gap_open=-1, gap_ext=0)
+    with pytest.raises(hy.Error) as e:
+        hy.Scoring(2, identity_matrix(2, 1, -1), 1, 2)  # Opal #28 (tests/opal_regressions.rs:70-82)
+    assert e.value == hy.Error("GapOpenLessThanExtend", gap_open=1, gap_ext=2)
+    s = hy.Scoring(4, DNA, 2, 1)
+    assert s.entry_bounds() == (-1, 2) and s.score(2, 2) == 2
+
+
+def test_required_width_matches_reference_cases():
+    assert hy.required_width(hy.Mode.Ov, -2, 1, 2, 2, 91, 33) == hy.ScoreWidth.I8
+    assert hy.required_width(hy.Mode.Nw, -2, 1, 2, 2, 91, 33) == hy.ScoreWidth.I16
+    assert hy.required_width(hy.Mode.Nw, -1, 1, 2, 1, 30_000, 30_000) == hy.ScoreWidth.I32
+    with pytest.raises(hy.Error) as e:
+        hy.required_width(hy.Mode.Nw, 0, 0, 2_000_000_000, 1, 1, 1)
+    assert e.value == hy.Error("ScoreRangeTooWide", bound=2_000_000_001)
+
+
+def test_backend_parse_mirrors_reference():
+    # src/backend.rs:226-265
+    assert hy.BackendChoice.parse("auto") == hy.BackendChoice.Auto()
+    assert hy.BackendChoice.parse("AUTO") == hy.BackendChoice.Auto()
+    assert hy.BackendChoice.parse("  SSE41 ") == hy.BackendChoice.Force(hy.Backend.Sse41)
+    assert hy.BackendChoice.parse("sse4.1") == hy.BackendChoice.Force(hy.Backend.Sse41)
+    assert hy.BackendChoice.parse("Avx2") == hy.BackendChoice.Force(hy.Backend.Avx2)
+    assert hy.BackendChoice.parse("cuda") == hy.BackendChoice.Force(hy.Backend.Cuda)
+    for b in hy.Backend:
+        assert hy.BackendChoice.parse(b.name_str()) == hy.BackendChoice.Force(b)
+    for bad in ["", "sse2", "ssse3", "avx512", "gpu", "x"]:
+        with pytest.raises(hy.Error) as e:
+            hy.BackendChoice.parse(bad)
+        assert e.value == hy.Error("InvalidBackendName", name=bad)
+
+
+def test_only_cuda_is_built():
+    for b in (hy.Backend.Scalar, hy.Backend.Sse41, hy.Backend.Avx2, hy.Backend.Neon):
+        assert not b.is_available()
+
+
+def test_builder_reports_every_missing_required_field():
+    # src/database.rs:1036-1066
+    base = hy.Database.builder
+    for builder, field in [
+        (base(), "sequences"),
+        (base().sequences([[0]]), "scoring"),
+        (base().sequences([[0]]).scoring(hy.Scoring(4, DNA, 2, 1)), "mode"),
+        (base().sequences([[0]]).scoring(hy.Scoring(4, DNA, 2, 1)).mode(hy.Mode.Sw), "max_query_len"),
+    ]:
+        with pytest.raises(hy.Error) as e:
+            builder.build()
+        assert e.value == hy.Error("IncompleteBuilder", field=field)
+
+
+def _build(seqs, **kw):
+    b = hy.Database.builder().sequences(seqs).scoring(kw.get("scoring", hy.Scoring(4, DNA, 2, 1)))
+    return b.mode(kw.get("mode", hy.Mode.Sw)).max_query_len(kw.get("mql", 8)).backend(
+        kw.get("backend", hy.BackendChoice.Auto())).build()
+
+
+def test_build_validation_order_before_any_device_work():
+    # src/database.rs:737-794: empty -> symbols -> width proof -> backend
+    with pytest.raises(hy.Error) as e:
+        _build([])
+    assert e.value.kind == "EmptyDatabase"
+    with pytest.raises(hy.Error) as e:
+        _build([[0, 1], [2, 9]])
+    assert e.value == hy.Error("SymbolOutOfRange", symbol=9, alphabet_len=4)
+    with pytest.raises(hy.Error) as e:
+        _build([[0]], scoring=hy.Scoring(2, [0, 0, 0, 0], 2_000_000_000, 1), mode=hy.Mode.Nw, mql=1)
+    assert e.value.kind == "ScoreRangeTooWide"
+
+
+@pytest.mark.skipif(hy.Backend.Cuda.is_available(), reason="only meaningful without a GPU")
+def test_build_without_a_gpu_is_backend_unavailable():
+    with pytest.raises(hy.Error) as e:
+        _build([[0, 1, 2]])
+    assert e.value == hy.Error("BackendUnavailable", backend=hy.Backend.Cuda)
+    with pytest.raises(hy.Error) as e:
+        _build([[0, 1, 2]], backend=hy.BackendChoice.Force(hy.Backend.Avx2))
+    assert e.value == hy.Error("BackendUnavailable", backend=hy.Backend.Avx2)
+
+
+def test_env_var_precedence_in_a_fresh_process():
+    # tests/backend_env.rs:39-97: an invalid HYALITE_BACKEND is an error at build unless the builder
+    # forces a backend explicitly.
+    code = (
+        "import hyalite_b200 as hy\n"
+        "b = hy.Database.builder().sequences([[0]]).scoring(hy.Scoring(4, [2,-1,-1,-1,-1,2,-1,-1,-1,-1,2,-1,-1,-1,-1,2], 2, 1))"
+        ".mode(hy.Mode.Sw).max_query_len(4)\n"
+        "try:\n    b.build(); print('built')\nexcept hy.Error as e: print(e.kind)\n"
+        "try:\n    b.backend(hy.BackendChoice.Force(hy.Backend.Avx2)).build(); print('built')\nexcept hy.Error as e: print(e.kind)\n"
+    )
+    env = dict(os.environ, HYALITE_BACKEND="definitely-not-a-backend", PYTHONPATH=ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, cwd=ROOT)
+    lines = out.stdout.split()
+    assert lines[0] == "InvalidBackendName", out.stderr
+    assert lines[1] == "BackendUnavailable"
