@@ -11,66 +11,13 @@
 #include <numeric>
 #include <vector>
 
-#include "host_common.h"
-#include "scan_kernel.cuh"
+#include "db_internal.h"
 
 using namespace hy;
 
-namespace hy {
-
-// Launch shapes. Main scan: groups of MAIN_G lanes, MAIN_R query rows per lane. Winner end
-// recovery: one full warp per item.
-constexpr int MAIN_G = 8;
-constexpr int MAIN_R16 = 16;
-constexpr int MAIN_R32 = 16;
-constexpr int WIN_G = 32;
-constexpr int WIN_R = 16;
-constexpr int BLOCK = 256;
-
-struct Partition {
-    uint32_t n_items = 0;
-    uint64_t n_seqs = 0;
-    uint64_t total_cols = 0;
-    ItemMeta *d_meta = nullptr;
-    void *d_res = nullptr;
-};
-
-template <class A>
-struct ElemSize {
-    static constexpr size_t pe = sizeof(typename A::PE);
-};
-
-struct QueryPlan {
-    int32_t n_passes = 0;
-    int32_t vrow0 = 1;
-    uint32_t pass_bytes = 0;
-};
-
-static QueryPlan plan(uint64_t qlen, int rpp, uint64_t al, size_t pe) {
-    QueryPlan q;
-    q.n_passes = (int32_t)((qlen + rpp - 1) / rpp);
-    q.vrow0 = (int32_t)qlen - q.n_passes * rpp + 1;
-    q.pass_bytes = (uint32_t)((al + 1) * (uint64_t)rpp * pe);
-    return q;
-}
-
-}  // namespace hy
-
-struct hy_db {
-    int device = 0;
-    uint64_t n_seqs = 0, mql = 0, max_t = 0, al = 0;
-    int32_t go = 0, ge = 0, min_e = 0, max_e = 0;
-    int mode = 0, search_type = 0, layout = HY_LAYOUT_GATHERED;
-    hy_score_width width = HY_WIDTH_I8;
-    hy_backend backend = HY_BACKEND_CUDA;
-    int32_t *d_matrix = nullptr;
-    Partition p16, p32;
-    uint32_t *d_loc = nullptr;
-    uint64_t device_bytes = 0;
-};
-
 struct hy_scratch {
     const hy_db *db = nullptr;
+    int device = 0;  // copied from the database: destroying a scratch never reads its database
     cudaStream_t stream = nullptr;
     uint8_t *d_query = nullptr;
     uint8_t *d_prof16 = nullptr, *d_prof32 = nullptr, *d_profw16 = nullptr, *d_profw32 = nullptr;
@@ -312,15 +259,19 @@ static hy_status ensure_host_out(hy_scratch *sc) {
     return fail(HY_OK);
 }
 
+// Makes `dev` current for the scope of a call and restores the caller's device afterwards. Any
+// error of these bookkeeping calls is cleared so it cannot surface in a later launch check.
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {
         if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
         if (prev != dev) cudaSetDevice(dev);
+        cudaGetLastError();
     }
     ~DeviceGuard() {
         int cur;
         if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+        cudaGetLastError();
     }
 };
 
@@ -534,6 +485,7 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
     DeviceGuard g(db->device);
     hy_scratch *sc = new hy_scratch;
     sc->db = db;
+    sc->device = db->device;
     hy_status st = HY_OK;
     auto ck = [&](cudaError_t e) {
         if (e != cudaSuccess && st == HY_OK) {
@@ -579,7 +531,7 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
 
 void hy_scratch_destroy(hy_scratch *sc) {
     if (!sc) return;
-    DeviceGuard g(sc->db->device);
+    DeviceGuard g(sc->device);
     if (sc->stream) cudaStreamSynchronize(sc->stream);
     cudaFree(sc->d_query);
     cudaFree(sc->d_prof16);
@@ -620,7 +572,7 @@ hy_status hy_scratch_profile(hy_scratch *sc, int enable) {
 hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[2], uint64_t launches[2],
                                   uint64_t *all_launches) {
     if (!sc || !kernel_ms || !launches) return fail(HY_ERR_INVALID_ARGUMENT);
-    DeviceGuard g(sc->db->device);
+    DeviceGuard g(sc->device);
     HY_CK(cudaStreamSynchronize(sc->stream));
     kernel_ms[0] = kernel_ms[1] = 0.0;
     launches[0] = launches[1] = 0;
@@ -643,7 +595,7 @@ hy_status hy_query_validate(const hy_db *db, const uint8_t *query, uint64_t qlen
 
 hy_status hy_scratch_sync(hy_scratch *sc) {
     if (!sc) return fail(HY_ERR_INVALID_ARGUMENT);
-    DeviceGuard g(sc->db->device);
+    DeviceGuard g(sc->device);
     return sync_and_check(sc);
 }
 

@@ -123,7 +123,8 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
 void hy_db_destroy(hy_db *db);
 
 /* Accessors (src/database.rs:570-638). score_width is the reference's whole-database proof (the
- * widest width); the device partitions by its own per-sequence proof. */
+ * widest width); the device partitions sequences by its own per-sequence rule (bound + gap_open
+ * must fit int16 for the packed int16x2 kernel, else int32), which never changes results. */
 uint64_t hy_db_sequence_count(const hy_db *db);
 hy_mode hy_db_mode(const hy_db *db);
 hy_search_type hy_db_search_type(const hy_db *db);
