@@ -73,6 +73,7 @@ SIGNATURES = {
     "hy_scan_device": (_st, [_vp, _vp, _vp, C.c_uint64, _vp]),
     "hy_scan_scores_device": (_st, [_vp, _vp, _vp, C.c_uint64, _vp]),
     "hy_query_validate": (_st, [_vp, _u8p, C.c_uint64]),
+    "hy_scan_scores_noalloc": (_st, [_vp, _vp, C.c_uint64, _vp, _vp]),
     "hy_scratch_sync": (_st, [_vp]),
     "hy_scratch_profile": (_st, [_vp, C.c_int]),
     "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, _u64p]),

@@ -165,6 +165,18 @@ hy_status hy_scan_device(const hy_db *db, hy_scratch *scratch, const uint8_t *d_
                          uint64_t qlen, hy_hit *d_out);
 hy_status hy_scan_scores_device(const hy_db *db, hy_scratch *scratch, const uint8_t *d_query,
                                 uint64_t qlen, int32_t *d_out);
+/* No counterpart in the reference: an allocation-free form of hy_scan_scores for callers that cannot
+ * call cudaMalloc once running (device memory already owned by another allocator, or a loop that
+ * cannot take cudaMalloc's implicit synchronisation). Query and scores are the caller's device
+ * buffers; the kernels' scratch is a fixed 16 MiB __device__ array inside this library, which
+ * every GPU that loads the library holds until exit. A call needing more scratch than that (the
+ * boundary rows of a multi-pass query grow with the database) returns HY_ERR_UNSUPPORTED with
+ * detail {needed_bytes, limit}. Runs on `stream` (a cudaStream_t, or NULL for the legacy default
+ * stream) and returns once the scores are written. Calls share the array: calls whose kernels
+ * overlap on the GPU race and must be serialised by the caller. The query's symbols must already
+ * be validated (hy_query_validate); the current device must be the database's. */
+hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_query, uint64_t qlen,
+                                 int32_t *d_scores, void *stream);
 /* The checks hy_scan performs on a host query (length, then symbols). */
 hy_status hy_query_validate(const hy_db *db, const uint8_t *query, uint64_t qlen);
 /* Waits for the scratch's stream; returns HY_ERR_TIMEOUT if a kernel's bounded wait ran out. */
