@@ -165,7 +165,7 @@ def run_cuda(args):
     from hyalite_b200 import _abi
 
     lib = _abi.lib
-    mat, residues, offsets, queries = make_workload(args.seed + rank)
+    mat, residues, offsets, queries = make_workload(args.seed + rank, n_seqs=N_SEQS)
     n_seqs = len(offsets) - 1
     t_build = time.perf_counter()
     db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
@@ -223,8 +223,9 @@ def run_cuda(args):
     torch.cuda.synchronize()
     kms = (C.c_double * 2)()
     kl = (C.c_uint64 * 2)()
+    kcells = (C.c_double * 2)()
     all_l = C.c_uint64()
-    lib.hy_scratch_profile_read(sc._h, kms, kl, C.byref(all_l))
+    lib.hy_scratch_profile_read(sc._h, kms, kl, kcells, C.byref(all_l))
     lib.hy_scratch_profile(sc._h, 0)
     clk = clocks.stop()
     elapsed_ms = start.elapsed_time(end)
@@ -265,14 +266,14 @@ def run_cuda(args):
     peak = C.c_double()
     lib.hy_measure_dpx_peak(C.byref(peak))
     peak_gcups = peak.value / 1e9
-    # int16-partition cells per launch: all residues except the int32 partition's
-    sorted_lens = np.sort(lens)  # the int32 partition is the longest sequences
-    res32 = float(sorted_lens[len(sorted_lens) - n32:].sum()) if n32 else 0.0
-    res16 = total_res - res32
+    # The dominant kernel is the int16x2 pair kernel: its real cells per launch over its average
+    # launch time (CUDA events on its own stream).
     launches16 = max(int(kl[0]), 1)
-    cells16_per_launch = res16 * sum(len(q) for q in queries) / N_QUERIES
+    cells16_per_launch = kcells[0] / launches16
     avg16_ms = kms[0] / launches16
     achieved = cells16_per_launch / (avg16_ms * 1e-3) / 1e9 if avg16_ms > 0 else 0.0
+    i32_info = {"launches": int(kl[1]), "total_ms": kms[1], "cells": kcells[1],
+                "gcups": kcells[1] / (kms[1] * 1e-3) / 1e9 if kms[1] > 0 else None}
     meas = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm_peak = meas.get("hbm_gbs", 6650.0)
@@ -307,7 +308,11 @@ def run_cuda(args):
             "roofline": {"bound": "dpx_int16x2", "achieved": achieved, "peak": peak_gcups, "unit": "GCUPS",
                          "frac": achieved / peak_gcups if peak_gcups else None, "traffic": None,
                          "kernel": "scan_kernel<Pair16,8,16,SW>", "avg_launch_ms": avg16_ms,
-                         "launches": int(kl[0]), "peak_source": "measured: hy_measure_dpx_peak (register-resident per-cell DPX mix)"},
+                         "launches": int(kl[0]), "cells_per_launch": cells16_per_launch,
+                         "peak_source": "measured: hy_measure_dpx_peak (register-resident per-cell DPX mix)"},
+            "int32_kernel": i32_info,
+            "step_breakdown_ms": {"int16x2_kernels": kms[0] / args.steps, "int32_kernels_concurrent": kms[1] / args.steps,
+                                  "step": elapsed_ms / args.steps},
             "roofline_hbm": {"bound": "hbm", "peak": hbm_peak, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs" if meas else "fallback"},
             "clocks": clk,
         }
@@ -321,6 +326,7 @@ def run_cuda(args):
 
 
 def main():
+    global N_SEQS, QUERY_LENGTHS, N_QUERIES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -330,7 +336,14 @@ def main():
     ap.add_argument("--cpu-sample-seqs", type=int, default=12_000)
     ap.add_argument("--ref-seqs", type=int, default=12_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # Smaller shapes of the same generator (profiling cases; the default is the benchmark).
+    ap.add_argument("--n-seqs", type=int, default=N_SEQS)
+    ap.add_argument("--query-lengths", default=",".join(map(str, QUERY_LENGTHS)))
+    ap.add_argument("--n-queries", type=int, default=N_QUERIES)
     args = ap.parse_args()
+    N_SEQS = args.n_seqs
+    QUERY_LENGTHS = [int(x) for x in args.query_lengths.split(",")]
+    N_QUERIES = args.n_queries
     if args.impl == "reference":
         run_reference(args)
     else:

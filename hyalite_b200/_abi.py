@@ -76,7 +76,7 @@ SIGNATURES = {
     "hy_scan_scores_noalloc": (_st, [_vp, _vp, C.c_uint64, _vp, _vp]),
     "hy_scratch_sync": (_st, [_vp]),
     "hy_scratch_profile": (_st, [_vp, C.c_int]),
-    "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, _u64p]),
+    "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, C.POINTER(C.c_double), _u64p]),
     "hy_measure_dpx_peak": (_st, [C.POINTER(C.c_double)]),
     "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),

@@ -3,24 +3,31 @@
 
 #include <stdint.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "host_common.h"
 #include "scan_kernel.cuh"
 
 namespace hy {
 
-// Launch shapes. Main scan: groups of MAIN_G lanes, MAIN_R query rows per lane. Winner end
-// recovery: one full warp per item.
+// Launch shapes. Main scan: int16x2 pairs in groups of MAIN_G lanes with MAIN_R16 query rows per
+// lane; int32 items (the long sequences) one full warp each. Winner end recovery: the band kernel,
+// one warp per band of WIN_G * WIN_R query rows.
 constexpr int MAIN_G = 8;
 constexpr int MAIN_R16 = 16;
+constexpr int MAIN_G32 = 32;
 constexpr int MAIN_R32 = 16;
 constexpr int WIN_G = 32;
-constexpr int WIN_R = 16;
+constexpr int WIN_R = 8;
 constexpr int BLOCK = 256;
+constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;
 
 struct Partition {
     uint32_t n_items = 0;
     uint64_t n_seqs = 0;
     uint64_t total_cols = 0;
+    std::vector<uint64_t> res_prefix;  // host: residues of items [0, i) (both halves of a pair)
     ItemMeta *d_meta = nullptr;
     void *d_res = nullptr;
 };
@@ -54,8 +61,55 @@ struct hy_db {
     hy_score_width width = HY_WIDTH_I8;
     hy_backend backend = HY_BACKEND_CUDA;
     int32_t *d_matrix = nullptr;
+    // Every sequence in int16x2 pairs over the global length order (longest first); the longest
+    // ones (those the whole-database proof cannot place in int16) also as int32 singles.
     hy::Partition p16, p32;
-    uint32_t *d_loc = nullptr;
+    std::vector<uint32_t> pair_w;  // host: longer length of each pair, non-increasing
+    uint32_t *d_rank = nullptr;    // device: rank of each global index in the length order
     uint64_t device_bytes = 0;
 };
+
+namespace hy {
+
+// Which items one query runs in which lanes. The width proof is redone with the actual query
+// length: pairs [k0, n) fit int16 for this query and run packed; the 2*k0 longest sequences run
+// in int32 (always inside the int32 layout, which holds the static int32 set plus one).
+struct QuerySplit {
+    uint32_t k0 = 0;      // first int16x2 pair item
+    uint32_t n_i32 = 0;   // int32 items [0, n_i32)
+};
+
+inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen) {
+    QuerySplit q;
+    // Longest target length t whose bound for this query keeps the int16 kernel exact.
+    auto fits = [&](uint64_t n) {
+        return device_fits_i16(magnitude_bound(db->mode, db->min_e, db->max_e, db->go, db->ge, qlen, n), db->go);
+    };
+    uint64_t t;
+    if (fits(db->max_t)) {
+        t = db->max_t;
+    } else {
+        uint64_t lo = 0, hi = db->max_t;  // fits(lo) may be false only if even length 0 fails
+        if (!fits(0)) {
+            t = 0;
+            lo = hi = 0;
+        }
+        while (lo < hi) {
+            uint64_t mid = lo + (hi - lo + 1) / 2;
+            if (fits(mid)) lo = mid; else hi = mid - 1;
+        }
+        t = lo;
+    }
+    // First pair whose longer sequence is <= t (pair_w is non-increasing).
+    uint32_t a = 0, b = (uint32_t)db->pair_w.size();
+    while (a < b) {
+        uint32_t mid = a + (b - a) / 2;
+        if (db->pair_w[mid] <= t) b = mid; else a = mid + 1;
+    }
+    q.k0 = a;
+    q.n_i32 = (uint32_t)std::min<uint64_t>(2ull * a, db->n_seqs);
+    return q;
+}
+
+}  // namespace hy
 

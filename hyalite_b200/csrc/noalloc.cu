@@ -93,10 +93,10 @@ Region plan_region(const hy_db *db, const Partition &part, uint64_t qlen, size_t
 }
 
 template <class A, int G, int R>
-hy_status run_partition(const hy_db *db, const Partition &part, const Region &rg, uint8_t *base,
-                        const uint8_t *d_query, uint64_t qlen, int32_t *d_scores, int *d_err,
-                        cudaStream_t st) {
-    if (!part.n_items) return fail(HY_OK);
+hy_status run_partition(const hy_db *db, const Partition &part, uint32_t item_base,
+                        uint32_t item_end, const Region &rg, uint8_t *base, const uint8_t *d_query,
+                        uint64_t qlen, int32_t *d_scores, int *d_err, cudaStream_t st) {
+    if (item_base >= item_end) return fail(HY_OK);
     const bool i16 = A::NH == 2;
     const int32_t lim = i16 ? 32767 - db->go : 536870911;
     const int64_t total = (int64_t)(db->al + 1) * G * R * rg.qp.n_passes;
@@ -111,7 +111,8 @@ hy_status run_partition(const hy_db *db, const Partition &part, const Region &rg
     }
     ScanParams p;
     p.meta = part.d_meta;
-    p.n_items = part.n_items;
+    p.item_base = item_base;
+    p.n_items = item_end;
     p.item_ptr = nullptr;
     p.res = part.d_res;
     p.profile = base + rg.prof_off;
@@ -129,7 +130,7 @@ hy_status run_partition(const hy_db *db, const Partition &part, const Region &rg
     p.best_key = nullptr;
     p.err = d_err;
     const int gpb = BLOCK / G;
-    const int blocks = (int)((part.n_items + gpb - 1) / gpb);
+    const int blocks = (int)((item_end - item_base + gpb - 1) / gpb);
     cudaError_t e = launch_scores_mode<A, G, R>(db->mode, p, blocks, 2 * (size_t)rg.qp.pass_bytes + 16, st);
     if (e != cudaSuccess) return fail(HY_ERR_CUDA, e);
     return fail(HY_OK);
@@ -148,7 +149,7 @@ extern "C" hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_qu
     // Lay out this call's scratch: the timeout flag, then profile and boundary rows per partition.
     size_t cursor = 256;
     const Region r16 = plan_region<Pair16, MAIN_G, MAIN_R16>(db, db->p16, qlen, cursor);
-    const Region r32 = plan_region<Single32, MAIN_G, MAIN_R32>(db, db->p32, qlen, cursor);
+    const Region r32 = plan_region<Single32, MAIN_G32, MAIN_R32>(db, db->p32, qlen, cursor);
     if (cursor > NOALLOC_SCRATCH_BYTES)
         return fail(HY_ERR_UNSUPPORTED, (int64_t)cursor, (int64_t)NOALLOC_SCRATCH_BYTES);
     uint8_t *base = nullptr;
@@ -158,9 +159,13 @@ extern "C" hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_qu
     int *d_err = reinterpret_cast<int *>(base);
     e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
     if (e != cudaSuccess) return fail(HY_ERR_CUDA, e);
-    st = run_partition<Pair16, MAIN_G, MAIN_R16>(db, db->p16, r16, base, d_query, qlen, d_scores, d_err, s);
+    // The same per-query split as hy_scan_scores: pairs [k0, n) packed, the 2*k0 longest in int32.
+    const QuerySplit split = split_for_query(db, qlen);
+    st = run_partition<Pair16, MAIN_G, MAIN_R16>(db, db->p16, split.k0, db->p16.n_items, r16, base,
+                                                d_query, qlen, d_scores, d_err, s);
     if (st != HY_OK) return st;
-    st = run_partition<Single32, MAIN_G, MAIN_R32>(db, db->p32, r32, base, d_query, qlen, d_scores, d_err, s);
+    st = run_partition<Single32, MAIN_G32, MAIN_R32>(db, db->p32, 0, split.n_i32, r32, base, d_query,
+                                                  qlen, d_scores, d_err, s);
     if (st != HY_OK) return st;
     int err = 0;
     e = cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);

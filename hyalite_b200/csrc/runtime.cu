@@ -19,6 +19,9 @@ struct hy_scratch {
     const hy_db *db = nullptr;
     int device = 0;  // copied from the database: destroying a scratch never reads its database
     cudaStream_t stream = nullptr;
+    // The int32 part of a scan runs on a second stream, forked from and joined back into `stream`.
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     uint8_t *d_query = nullptr;
     uint8_t *d_prof16 = nullptr, *d_prof32 = nullptr, *d_profw16 = nullptr, *d_profw32 = nullptr;
     void *d_bnd16 = nullptr, *d_bnd32 = nullptr;
@@ -36,6 +39,7 @@ struct hy_scratch {
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     std::vector<int> event_part;  // 0: int16x2 pair kernel, 1: int32 kernel
+    double event_cells[2] = {0.0, 0.0};  // real DP cells the timed launches computed
     size_t n_events = 0;
     uint64_t launches = 0;        // every kernel this scratch launched since the last read
 };
@@ -98,18 +102,22 @@ static constexpr int32_t LIM32 = 536870911;
 static int32_t lim16(const hy_db *db) { return 32767 - db->go; }
 
 // Fill per-target scores (and ends) for every sequence; optionally fold the best hit key.
+// Items [item_base, item_end) of `part` (or the single item *item_ptr) on stream `st`.
 template <class A, int G, int R>
 static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partition &part,
-                                   const uint8_t *d_query, uint64_t qlen, bool ends,
-                                   unsigned long long *key, int32_t *scores, uint8_t *prof,
-                                   void *bnd, const uint32_t *item_ptr, int blocks, int threads) {
+                                   uint32_t item_base, uint32_t item_end, const uint8_t *d_query,
+                                   uint64_t qlen, bool ends, unsigned long long *key,
+                                   int32_t *scores, uint8_t *prof, void *bnd,
+                                   const uint32_t *item_ptr, int blocks, int threads,
+                                   cudaStream_t st_) {
     const bool i16 = sizeof(typename A::V) == 4 && A::NH == 2;
     QueryPlan qp = plan(qlen, G * R, db->al, sizeof(typename A::PE));
-    HY_CK((launch_profile<A, G, R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof, sc->stream)));
+    HY_CK((launch_profile<A, G, R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof, st_)));
     sc->launches += qp.n_passes > 0 ? 2 : 1;
     ScanParams p;
     p.meta = part.d_meta;
-    p.n_items = part.n_items;
+    p.item_base = item_base;
+    p.n_items = item_end;
     p.item_ptr = item_ptr;
     p.res = part.d_res;
     p.profile = prof;
@@ -137,45 +145,116 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
             sc->event_part.push_back(0);
         }
         sc->event_part[sc->n_events] = i16 ? 0 : 1;
-        HY_CK(cudaEventRecord(sc->events[sc->n_events].first, sc->stream));
+        sc->event_cells[i16 ? 0 : 1] +=
+            (double)qlen * (double)(part.res_prefix[item_end] - part.res_prefix[item_base]);
+        HY_CK(cudaEventRecord(sc->events[sc->n_events].first, st_));
     }
-    HY_CK((launch_scan<A, G, R>(db->mode, ends, p, blocks, threads, smem, sc->stream)));
+    HY_CK((launch_scan<A, G, R>(db->mode, ends, p, blocks, threads, smem, st_)));
     if (timed) {
-        HY_CK(cudaEventRecord(sc->events[sc->n_events].second, sc->stream));
+        HY_CK(cudaEventRecord(sc->events[sc->n_events].second, st_));
         ++sc->n_events;
     }
     return fail(HY_OK);
 }
 
+// Per-target scores (and ends) for every sequence, optionally folding the best-hit key. The
+// int32 items of this query run on the scratch's second stream, concurrently with the int16x2
+// pairs, and are joined back before the call's later work.
 static hy_status enqueue_scores(const hy_db *db, hy_scratch *sc, const uint8_t *d_query,
                                 uint64_t qlen, bool ends, unsigned long long *key, int32_t *scores) {
     hy_status st;
-    if (db->p16.n_items) {
-        int gpb = BLOCK / MAIN_G;
-        int blocks = (int)((db->p16.n_items + gpb - 1) / gpb);
-        st = enqueue_partition<Pair16, MAIN_G, MAIN_R16>(db, sc, db->p16, d_query, qlen, ends, key,
-                                                        scores, sc->d_prof16, sc->d_bnd16, nullptr,
-                                                        blocks, BLOCK);
+    const QuerySplit split = split_for_query(db, qlen);
+    const int gpb = BLOCK / MAIN_G;
+    const bool forked = split.n_i32 > 0;
+    if (forked) {
+        HY_CK(cudaEventRecord(sc->ev_fork, sc->stream));
+        HY_CK(cudaStreamWaitEvent(sc->stream2, sc->ev_fork, 0));
+        const int gpb32 = BLOCK / MAIN_G32;
+        const int blocks = (int)((split.n_i32 + gpb32 - 1) / gpb32);
+        st = enqueue_partition<Single32, MAIN_G32, MAIN_R32>(db, sc, db->p32, 0, split.n_i32, d_query,
+                                                          qlen, ends, key, scores, sc->d_prof32,
+                                                          sc->d_bnd32, nullptr, blocks, BLOCK,
+                                                          sc->stream2);
+        if (st != HY_OK) return st;
+        HY_CK(cudaEventRecord(sc->ev_join, sc->stream2));
+    }
+    if (split.k0 < db->p16.n_items) {
+        const int blocks = (int)((db->p16.n_items - split.k0 + gpb - 1) / gpb);
+        st = enqueue_partition<Pair16, MAIN_G, MAIN_R16>(db, sc, db->p16, split.k0, db->p16.n_items,
+                                                        d_query, qlen, ends, key, scores,
+                                                        sc->d_prof16, sc->d_bnd16, nullptr, blocks,
+                                                        BLOCK, sc->stream);
         if (st != HY_OK) return st;
     }
-    if (db->p32.n_items) {
-        int gpb = BLOCK / MAIN_G;
-        int blocks = (int)((db->p32.n_items + gpb - 1) / gpb);
-        st = enqueue_partition<Single32, MAIN_G, MAIN_R32>(db, sc, db->p32, d_query, qlen, ends,
-                                                          key, scores, sc->d_prof32, sc->d_bnd32,
-                                                          nullptr, blocks, BLOCK);
-        if (st != HY_OK) return st;
-    }
+    if (forked) HY_CK(cudaStreamWaitEvent(sc->stream, sc->ev_join, 0));
     return fail(HY_OK);
 }
 
-// Locate the winning sequence's item in its partition (or NO_INDEX in the other partition).
-__global__ void winner_loc_kernel(const unsigned long long *key, const uint32_t *loc, uint32_t *win) {
+// The winner's item: its int16x2 pair when that pair ran packed for this query (pair >= k0),
+// else its int32 single (the 2*k0 longest sequences). The other slot gets NO_INDEX.
+__global__ void winner_loc_kernel(const unsigned long long *key, const uint32_t *rank, uint32_t k0,
+                                  uint32_t *win) {
     const uint32_t idx = ~(uint32_t)(*key & 0xffffffffu);
-    const uint32_t l = loc[idx];
-    const uint32_t part = l >> 31, item = l & 0x7fffffffu;
-    win[0] = part == 0 ? item : NO_INDEX;
-    win[1] = part == 1 ? item : NO_INDEX;
+    const uint32_t r = rank[idx];
+    const bool packed = r / 2 >= k0;
+    win[0] = packed ? r / 2 : NO_INDEX;
+    win[1] = packed ? NO_INDEX : r;
+}
+
+template <class A, int MODE>
+static cudaError_t launch_band_mode(const ScanParams &p, int warps, size_t smem, cudaStream_t st) {
+    auto kern = band_kernel<A, WIN_R, MODE>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<1, 32 * warps, smem, st>>>(p);
+    return cudaGetLastError();
+}
+
+// End positions of the single item *item_ptr with the block-cooperative band kernel.
+template <class A>
+static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &part,
+                              uint32_t item_end, const uint8_t *d_query, uint64_t qlen,
+                              uint8_t *prof, void *bnd, const uint32_t *item_ptr) {
+    const bool i16 = A::NH == 2;
+    QueryPlan qp = plan(qlen, WIN_G * WIN_R, db->al, sizeof(typename A::PE));
+    HY_CK((launch_profile<A, WIN_G, WIN_R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof,
+                                            sc->stream)));
+    ScanParams p;
+    p.meta = part.d_meta;
+    p.item_base = 0;
+    p.n_items = item_end;
+    p.item_ptr = item_ptr;
+    p.res = part.d_res;
+    p.profile = prof;
+    p.pass_bytes = qp.pass_bytes;
+    p.n_passes = qp.n_passes;
+    p.vrow0 = qp.vrow0;
+    p.qlen = (int32_t)qlen;
+    p.go = db->go;
+    p.ge = db->ge;
+    p.sentinel = i16 ? (-32768 + db->ge) : (INT32_MIN / 4);
+    p.boundary = bnd;
+    p.scores = sc->d_scores;
+    p.qend = sc->d_qend;
+    p.tend = sc->d_tend;
+    p.best_key = nullptr;
+    p.err = sc->d_err;
+    int warps = (int)std::min<size_t>(32, BAND_SMEM_BUDGET / std::max<uint32_t>(qp.pass_bytes, 1));
+    warps = std::max(1, std::min(warps, std::max(qp.n_passes, 1)));
+    const size_t smem = (size_t)warps * qp.pass_bytes + 16;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (db->mode) {
+    case MODE_SW: e = launch_band_mode<A, MODE_SW>(p, warps, smem, sc->stream); break;
+    case MODE_NW: e = launch_band_mode<A, MODE_NW>(p, warps, smem, sc->stream); break;
+    case MODE_HW: e = launch_band_mode<A, MODE_HW>(p, warps, smem, sc->stream); break;
+    case MODE_OV: e = launch_band_mode<A, MODE_OV>(p, warps, smem, sc->stream); break;
+    case MODE_SHW: e = launch_band_mode<A, MODE_SHW>(p, warps, smem, sc->stream); break;
+    }
+    HY_CK(e);
+    sc->launches += qp.n_passes > 0 ? 2 : 1;
+    return fail(HY_OK);
 }
 
 // Compose the BestHit of a single-best scan from the reduced key (and the winner's ends).
@@ -200,20 +279,19 @@ static hy_status enqueue_scan(const hy_db *db, hy_scratch *sc, const uint8_t *d_
     const bool ends = db->search_type == HY_SEARCH_SCORE_END;
     if (ends) {
         // End positions of the winner only (src/database.rs:186-197): rerun its item with
-        // position tracking, one warp wide.
-        winner_loc_kernel<<<1, 1, 0, sc->stream>>>(sc->d_key, db->d_loc, sc->d_win);
+        // position tracking on a whole block (the band kernel).
+        const QuerySplit split = split_for_query(db, qlen);
+        winner_loc_kernel<<<1, 1, 0, sc->stream>>>(sc->d_key, db->d_rank, split.k0, sc->d_win);
         HY_CK(cudaGetLastError());
         ++sc->launches;
-        if (db->p16.n_items) {
-            st = enqueue_partition<Pair16, WIN_G, WIN_R>(db, sc, db->p16, d_query, qlen, true,
-                                                        nullptr, sc->d_scores, sc->d_profw16,
-                                                        sc->d_bnd16, sc->d_win, 1, WIN_G);
+        if (split.k0 < db->p16.n_items) {
+            st = enqueue_band<Pair16>(db, sc, db->p16, db->p16.n_items, d_query, qlen, sc->d_profw16,
+                                      sc->d_bnd16, sc->d_win);
             if (st != HY_OK) return st;
         }
-        if (db->p32.n_items) {
-            st = enqueue_partition<Single32, WIN_G, WIN_R>(db, sc, db->p32, d_query, qlen, true,
-                                                          nullptr, sc->d_scores, sc->d_profw32,
-                                                          sc->d_bnd32, sc->d_win + 1, 1, WIN_G);
+        if (split.n_i32 > 0) {
+            st = enqueue_band<Single32>(db, sc, db->p32, split.n_i32, d_query, qlen, sc->d_profw32,
+                                        sc->d_bnd32, sc->d_win + 1);
             if (st != HY_OK) return st;
         }
     }
@@ -303,6 +381,9 @@ static hy_status build_partition(hy_db *db, Partition &part, const std::vector<u
         cols += (m.w + align - 1) / align * align;
     }
     part.total_cols = cols;
+    part.res_prefix.assign(part.n_items + 1, 0);
+    for (uint32_t it = 0; it < part.n_items; ++it)
+        part.res_prefix[it + 1] = part.res_prefix[it] + meta[it].n[0] + meta[it].n[1];
     HY_CK(cudaMalloc(&part.d_meta, sizeof(ItemMeta) * part.n_items));
     HY_CK(cudaMemcpy(part.d_meta, meta.data(), sizeof(ItemMeta) * part.n_items, cudaMemcpyHostToDevice));
     db->device_bytes += sizeof(ItemMeta) * part.n_items;
@@ -341,7 +422,7 @@ static void free_db(hy_db *db) {
     cudaFree(db->p16.d_res);
     cudaFree(db->p32.d_meta);
     cudaFree(db->p32.d_res);
-    cudaFree(db->d_loc);
+    cudaFree(db->d_rank);
     delete db;
 }
 
@@ -403,19 +484,28 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
     db->width = (hy_score_width)width;
     db->backend = backend;
 
-    // Per-sequence device width, then a length sort (longest first) inside each partition.
-    std::vector<uint32_t> o16, o32;
-    for (uint64_t k = 0; k < n_seqs; ++k) {
-        uint64_t len = offsets[k + 1] - offsets[k];
-        int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, max_query_len, len);
-        (device_fits_i16(b, gap_open) ? o16 : o32).push_back((uint32_t)k);
-    }
+    // One global length order (longest first, ties by index). Every sequence is packed in int16x2
+    // pairs over it; the prefix the whole-database proof cannot place in int16 (plus one, so a
+    // pair straddling any query's split is covered) is also packed as int32 singles.
+    std::vector<uint32_t> order(n_seqs);
+    for (uint64_t k = 0; k < n_seqs; ++k) order[k] = (uint32_t)k;
     auto by_len = [&](uint32_t a, uint32_t b) {
         uint64_t la = offsets[a + 1] - offsets[a], lb = offsets[b + 1] - offsets[b];
         return la != lb ? la > lb : a < b;
     };
-    std::sort(o16.begin(), o16.end(), by_len);
-    std::sort(o32.begin(), o32.end(), by_len);
+    std::sort(order.begin(), order.end(), by_len);
+    uint64_t k32 = 0;
+    while (k32 < n_seqs) {
+        const uint64_t len = offsets[order[k32] + 1] - offsets[order[k32]];
+        if (device_fits_i16(magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, max_query_len, len), gap_open))
+            break;
+        ++k32;
+    }
+    if (k32 > 0) k32 = std::min<uint64_t>(n_seqs, k32 + 1);
+    std::vector<uint32_t> o32(order.begin(), order.begin() + k32);
+    db->pair_w.resize((n_seqs + 1) / 2);
+    for (uint64_t p = 0; p < db->pair_w.size(); ++p)
+        db->pair_w[p] = (uint32_t)(offsets[order[2 * p] + 1] - offsets[order[2 * p]]);
 
     hy_status bst = HY_OK;
     auto ck = [&](cudaError_t e) {
@@ -428,15 +518,14 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
     if (bst == HY_OK)
         ck(cudaMemcpy(db->d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                       cudaMemcpyHostToDevice));
-    if (bst == HY_OK) bst = build_partition(db, db->p16, o16, residues, offsets, true);
+    if (bst == HY_OK) bst = build_partition(db, db->p16, order, residues, offsets, true);
     if (bst == HY_OK) bst = build_partition(db, db->p32, o32, residues, offsets, false);
     if (bst == HY_OK) {
-        std::vector<uint32_t> loc(n_seqs);
-        for (size_t i = 0; i < o16.size(); ++i) loc[o16[i]] = (uint32_t)(i / 2);
-        for (size_t i = 0; i < o32.size(); ++i) loc[o32[i]] = (uint32_t)i | 0x80000000u;
-        ck(cudaMalloc(&db->d_loc, sizeof(uint32_t) * n_seqs));
+        std::vector<uint32_t> rank(n_seqs);
+        for (uint64_t r = 0; r < n_seqs; ++r) rank[order[r]] = (uint32_t)r;
+        ck(cudaMalloc(&db->d_rank, sizeof(uint32_t) * n_seqs));
         if (bst == HY_OK)
-            ck(cudaMemcpy(db->d_loc, loc.data(), sizeof(uint32_t) * n_seqs, cudaMemcpyHostToDevice));
+            ck(cudaMemcpy(db->d_rank, rank.data(), sizeof(uint32_t) * n_seqs, cudaMemcpyHostToDevice));
         db->device_bytes += sizeof(uint32_t) * n_seqs + sizeof(int32_t) * alphabet_len * alphabet_len;
     }
     if (bst != HY_OK) {
@@ -473,9 +562,9 @@ uint64_t hy_db_scratch_bytes(const hy_db *db) {
     const uint64_t mq = std::max<uint64_t>(db->mql, 1);
     uint64_t b = mq + 3 * 4 * db->n_seqs + 64 + sizeof(hy_hit);
     b += npass(mq, MAIN_G * MAIN_R16) * (db->al + 1) * MAIN_G * MAIN_R16 * 2;
-    b += npass(mq, MAIN_G * MAIN_R32) * (db->al + 1) * MAIN_G * MAIN_R32 * 4;
+    b += npass(mq, MAIN_G32 * MAIN_R32) * (db->al + 1) * MAIN_G32 * MAIN_R32 * 4;
     b += npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 6;
-    if (mq > (uint64_t)std::min(MAIN_G * MAIN_R16, MAIN_G * MAIN_R32))
+    if (mq > (uint64_t)std::min({MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R}))
         b += 8 * (db->p16.total_cols + db->p32.total_cols);
     return b;
 }
@@ -496,12 +585,15 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
     const uint64_t mq = std::max<uint64_t>(db->mql, 1);
     const uint64_t n = std::max<uint64_t>(db->n_seqs, 1);
     ck(cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking));
+    ck(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));
+    ck(cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming));
+    ck(cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming));
     ck(cudaMalloc(&sc->d_query, mq));
     ck(cudaMalloc(&sc->d_prof16, std::max<uint64_t>(1, npass(mq, MAIN_G * MAIN_R16) * (db->al + 1) * MAIN_G * MAIN_R16 * 2)));
-    ck(cudaMalloc(&sc->d_prof32, std::max<uint64_t>(1, npass(mq, MAIN_G * MAIN_R32) * (db->al + 1) * MAIN_G * MAIN_R32 * 4)));
+    ck(cudaMalloc(&sc->d_prof32, std::max<uint64_t>(1, npass(mq, MAIN_G32 * MAIN_R32) * (db->al + 1) * MAIN_G32 * MAIN_R32 * 4)));
     ck(cudaMalloc(&sc->d_profw16, std::max<uint64_t>(1, npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 2)));
     ck(cudaMalloc(&sc->d_profw32, std::max<uint64_t>(1, npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 4)));
-    const bool multipass = mq > (uint64_t)std::min(MAIN_G * MAIN_R16, MAIN_G * MAIN_R32);
+    const bool multipass = mq > (uint64_t)std::min({MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R});
     ck(cudaMalloc(&sc->d_bnd16, multipass ? std::max<uint64_t>(8, 8 * db->p16.total_cols) : 8));
     ck(cudaMalloc(&sc->d_bnd32, multipass ? std::max<uint64_t>(8, 8 * db->p32.total_cols) : 8));
     ck(cudaMalloc(&sc->d_scores, 4 * n));
@@ -555,6 +647,10 @@ void hy_scratch_destroy(hy_scratch *sc) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
+    if (sc->stream2) cudaStreamSynchronize(sc->stream2);
+    if (sc->ev_fork) cudaEventDestroy(sc->ev_fork);
+    if (sc->ev_join) cudaEventDestroy(sc->ev_join);
+    if (sc->stream2) cudaStreamDestroy(sc->stream2);
     if (sc->stream) cudaStreamDestroy(sc->stream);
     delete sc;
 }
@@ -566,11 +662,12 @@ hy_status hy_scratch_profile(hy_scratch *sc, int enable) {
     sc->profile = enable != 0;
     sc->n_events = 0;
     sc->launches = 0;
+    sc->event_cells[0] = sc->event_cells[1] = 0.0;
     return fail(HY_OK);
 }
 
 hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[2], uint64_t launches[2],
-                                  uint64_t *all_launches) {
+                                  double cells[2], uint64_t *all_launches) {
     if (!sc || !kernel_ms || !launches) return fail(HY_ERR_INVALID_ARGUMENT);
     DeviceGuard g(sc->device);
     HY_CK(cudaStreamSynchronize(sc->stream));
@@ -582,9 +679,14 @@ hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[2], uint64_t 
         kernel_ms[sc->event_part[i]] += ms;
         launches[sc->event_part[i]] += 1;
     }
+    if (cells) {
+        cells[0] = sc->event_cells[0];
+        cells[1] = sc->event_cells[1];
+    }
     if (all_launches) *all_launches = sc->launches;
     sc->n_events = 0;
     sc->launches = 0;
+    sc->event_cells[0] = sc->event_cells[1] = 0.0;
     return fail(HY_OK);
 }
 

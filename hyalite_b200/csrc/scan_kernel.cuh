@@ -60,6 +60,7 @@ static constexpr uint32_t NO_INDEX = 0xffffffffu;
 
 struct ScanParams {
     const ItemMeta *meta;
+    uint32_t item_base;        // first item of the launch: items [item_base, n_items) run
     uint32_t n_items;
     const uint32_t *item_ptr;  // when set: run the single item *item_ptr (NO_INDEX: nothing)
     const void *res;           // Pair16: uint16 (lo | hi << 8); Single32: uint8
@@ -268,50 +269,62 @@ __device__ __forceinline__ unsigned long long hit_key(int32_t score, uint32_t id
 
 // ---- one pass of the wavefront -------------------------------------------------------------
 //
-// Sweeps the item's columns for the G*R query rows of one pass. `steps` is warp-uniform (every
+// Sweeps the item's columns for the G*R query rows of one pass. Steps are warp-uniform (every
 // lane of the warp shuffles every step). Lane L works on column j = s - L + 1 at step s; the G and
 // F values of its last row at column j reach lane L+1 at step s+1. Lane 0 reads the row above the
 // pass from the boundary row (or the top border in the first pass); lane G-1 writes the pass's
-// last row to the boundary row unless this is the last pass.
-template <class A, int G, int R, int MODE, bool ENDS>
-__device__ __forceinline__ void sweep_pass(const int lane, const int steps, const int32_t w,
-                                           const uint32_t (&n)[2],
-                                           const typename A::RES *__restrict__ res,
-                                           const uint8_t *prof_a, const uint8_t *prof_b,
-                                           const int32_t row0, const bool first_pass,
-                                           const bool last_pass, typename A::V *bnd,
-                                           const int32_t qlen, const int32_t go, const int32_t ge,
-                                           const typename A::V Sv, typename A::V &best,
-                                           Cand (&cand)[2]) {
-    typedef typename A::V V;
-    typedef ModeFlags<MODE> Fl;
-    const V negge = A::splat(-(int64_t)ge), neggo = A::splat(-(int64_t)go);
+// last row to the boundary row unless this is the last pass. The state lives in a Sweep so a
+// pass can be run in windows of steps (the block-cooperative band kernel interleaves warps).
+template <class A, int R>
+struct Sweep {
+    typename A::V Gp[R], E[R];  // G (= H - go) of the previous column and E, per row slot
+    typename A::V diag;         // G of the row above at the previous column (row slot 0)
+    typename A::V botG, botF;   // this lane's last row at its current column, for lane L+1
+    // SW end tracking within a pass: the running per-half maximum and the cell id
+    // (column * R + slot) where it was first reached; column-major order inside the lane means
+    // the first strict improvement is the smallest (column, row).
+    typename A::V pbest;
+    int32_t pid0, pid1;
+};
 
-    V Gp[R], E[R];
+template <class A, int R, int MODE>
+__device__ __forceinline__ void sweep_begin(Sweep<A, R> &sw, const int32_t row0, const int32_t go,
+                                            const int32_t ge, const typename A::V Sv) {
+    typedef ModeFlags<MODE> Fl;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int32_t row = row0 + r;
         const int64_t lb = (row <= 0 || Fl::left_free) ? 0 : -gap_pen(go, ge, row);
-        Gp[r] = A::splat(lb - go);
-        E[r] = Sv;
+        sw.Gp[r] = A::splat(lb - go);
+        sw.E[r] = Sv;
     }
-    V diag;
-    {
-        const int32_t row = row0 - 1;
-        const int64_t lb = (row <= 0 || Fl::left_free) ? 0 : -gap_pen(go, ge, row);
-        diag = A::splat(lb - go);
-    }
-    V botG = A::splat(0), botF = A::splat(0);
-    // SW end tracking within this pass: the running per-half maximum and the cell id
-    // (column * R + slot) where it was first reached; column-major order inside the lane means
-    // the first strict improvement is the smallest (column, row).
-    V pbest = A::splat(INT32_MIN);
-    int32_t pid0 = -1, pid1 = -1;
+    const int32_t row = row0 - 1;
+    const int64_t lb = (row <= 0 || Fl::left_free) ? 0 : -gap_pen(go, ge, row);
+    sw.diag = A::splat(lb - go);
+    sw.botG = A::splat(0);
+    sw.botF = A::splat(0);
+    sw.pbest = A::splat(INT32_MIN);
+    sw.pid0 = -1;
+    sw.pid1 = -1;
+}
 
-    for (int s = 0; s < steps; ++s) {
+template <class A, int G, int R, int MODE, bool ENDS>
+__device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, const int s_end,
+                                          const int lane, const int32_t w, const uint32_t (&n)[2],
+                                          const typename A::RES *__restrict__ res,
+                                          const uint8_t *prof_a, const uint8_t *prof_b,
+                                          const int32_t row0, const bool first_pass,
+                                          const bool last_pass, typename A::V *bnd,
+                                          const int32_t qlen, const int32_t go, const int32_t ge,
+                                          const typename A::V Sv, typename A::V &best,
+                                          Cand (&cand)[2]) {
+    typedef typename A::V V;
+    typedef ModeFlags<MODE> Fl;
+    const V negge = A::splat(-(int64_t)ge), neggo = A::splat(-(int64_t)go);
+    for (int s = s_begin; s < s_end; ++s) {
         const int32_t j = s - lane + 1;
-        V upG = __shfl_up_sync(0xffffffffu, botG, 1, G);
-        V upF = __shfl_up_sync(0xffffffffu, botF, 1, G);
+        V upG = __shfl_up_sync(0xffffffffu, sw.botG, 1, G);
+        V upF = __shfl_up_sync(0xffffffffu, sw.botF, 1, G);
         const bool live = j >= 1 && j <= w;
         if (lane == 0) {
             if (first_pass) {
@@ -328,24 +341,24 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
             A::residues(res[j - 1], a, b);
             V P[R];
             A::template load_profile<R, G>(prof_a, prof_b, a, b, lane, P);
-            V g_up = upG, f = upF, gd = diag, hprev = A::splat(0), hlast = A::splat(0);
+            V g_up = upG, f = upF, gd = sw.diag, hprev = A::splat(0), hlast = A::splat(0);
             const int32_t jR = j * R;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                E[r] = A::addmax(E[r], negge, Gp[r]);
+                sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
                 f = A::addmax(f, negge, g_up);
-                const V t = Fl::local ? A::vmax_relu(E[r], f) : A::vmax(E[r], f);
+                const V t = Fl::local ? A::vmax_relu(sw.E[r], f) : A::vmax(sw.E[r], f);
                 const V h = A::addmax(gd, P[r], t);
-                gd = Gp[r];
+                gd = sw.Gp[r];
                 const V g = A::vadd(h, neggo);
-                Gp[r] = g;
+                sw.Gp[r] = g;
                 g_up = g;
                 if (Fl::local) {
                     if (ENDS) {
                         bool u0, u1;
-                        pbest = A::bmax(pbest, h, u0, u1);
-                        if (u0) pid0 = jR + r;
-                        if (u1) pid1 = jR + r;
+                        sw.pbest = A::bmax(sw.pbest, h, u0, u1);
+                        if (u0) sw.pid0 = jR + r;
+                        if (u1) sw.pid1 = jR + r;
                     } else {
                         if (r & 1)
                             best = A::vmax3(best, hprev, h);
@@ -356,12 +369,12 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
                 if (r == R - 1) hlast = h;
             }
             if (Fl::local && !ENDS && (R & 1)) best = A::vmax(best, hprev);
-            botG = g_up;
-            botF = f;
-            diag = upG;
+            sw.botG = g_up;
+            sw.botF = f;
+            sw.diag = upG;
             if (lane == G - 1 && !last_pass) {
-                bnd[2 * (j - 1)] = botG;
-                bnd[2 * (j - 1) + 1] = botF;
+                bnd[2 * (j - 1)] = sw.botG;
+                bnd[2 * (j - 1) + 1] = sw.botF;
             }
             // Last query row (grid row qlen): slot R-1 of lane G-1 in the last pass.
             if ((Fl::last_row || Fl::corner) && last_pass && lane == G - 1) {
@@ -378,16 +391,38 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
                     if (j == (int32_t)n[h]) {
 #pragma unroll
                         for (int r = 0; r < R; ++r)
-                            if (row0 + r >= 1) consider(cand[h], A::get(Gp[r], h) + go, j, row0 + r);
+                            if (row0 + r >= 1) consider(cand[h], A::get(sw.Gp[r], h) + go, j, row0 + r);
                     }
                 }
             }
         }
     }
-    if (Fl::local && ENDS) {
-        if (pid0 >= 0) consider(cand[0], A::get(pbest, 0), pid0 / R, row0 + pid0 % R);
-        if (A::NH > 1 && pid1 >= 0) consider(cand[1], A::get(pbest, 1), pid1 / R, row0 + pid1 % R);
+}
+
+template <class A, int R, int MODE, bool ENDS>
+__device__ __forceinline__ void sweep_end(const Sweep<A, R> &sw, const int32_t row0, Cand (&cand)[2]) {
+    if (ModeFlags<MODE>::local && ENDS) {
+        if (sw.pid0 >= 0) consider(cand[0], A::get(sw.pbest, 0), sw.pid0 / R, row0 + sw.pid0 % R);
+        if (A::NH > 1 && sw.pid1 >= 0) consider(cand[1], A::get(sw.pbest, 1), sw.pid1 / R, row0 + sw.pid1 % R);
     }
+}
+
+// One whole pass: begin, every step, end.
+template <class A, int G, int R, int MODE, bool ENDS>
+__device__ __forceinline__ void sweep_pass(const int lane, const int steps, const int32_t w,
+                                           const uint32_t (&n)[2],
+                                           const typename A::RES *__restrict__ res,
+                                           const uint8_t *prof_a, const uint8_t *prof_b,
+                                           const int32_t row0, const bool first_pass,
+                                           const bool last_pass, typename A::V *bnd,
+                                           const int32_t qlen, const int32_t go, const int32_t ge,
+                                           const typename A::V Sv, typename A::V &best,
+                                           Cand (&cand)[2]) {
+    Sweep<A, R> sw;
+    sweep_begin<A, R, MODE>(sw, row0, go, ge, Sv);
+    sweep_run<A, G, R, MODE, ENDS>(sw, 0, steps, lane, w, n, res, prof_a, prof_b, row0, first_pass,
+                                   last_pass, bnd, qlen, go, ge, Sv, best, cand);
+    sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
 }
 
 // Group reduction of the per-lane candidates, border seeds, output and best-key fold. Every lane
@@ -471,7 +506,7 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
         const uint32_t want = *p.item_ptr;
         item = (blockIdx.x == 0 && threadIdx.x / G == 0) ? want : NO_INDEX;
     } else {
-        item = blockIdx.x * gpb + threadIdx.x / G;
+        item = p.item_base + blockIdx.x * gpb + threadIdx.x / G;
     }
     const bool active = item != NO_INDEX && item < p.n_items;
     ItemMeta meta;
@@ -524,6 +559,101 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
                                   p.qend, p.tend, p.best_key);
 }
 
+// ---- the block-cooperative band kernel (one long item, with end positions) -------------------
+//
+// Recovers the end positions of a single item (the winner of a scan) with a whole block. Every
+// warp is one 32-lane group running one pass (a band of 32*R query rows); the block takes the
+// passes in rounds of W = blockDim/32. Inside a round warp w runs BAND_K*2*w steps behind warp w-1
+// with a block barrier every BAND_K steps, so each boundary-row column a band reads was written
+// by the band above in an earlier window (the write of column j happens 2*BAND_K - (G - 1) >
+// BAND_K steps before the read). The round's profile slices are staged by one TMA bulk copy.
+constexpr int BAND_K = 32;
+
+template <class A, int R, int MODE>
+__global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
+    typedef typename A::V V;
+    constexpr int G = 32;
+    constexpr int RPP = G * R;
+    static_assert(BAND_K >= G, "the lag must cover the lane skew of a warp");
+    static_assert(R % A::EPV == 0, "rows per lane must fill whole profile vectors");
+    extern __shared__ __align__(128) uint8_t smem[];
+    const int W = blockDim.x / G;
+    const int warp = threadIdx.x / G, lane = threadIdx.x % G;
+    const uint32_t item = *p.item_ptr;
+    if (item == NO_INDEX || item >= p.n_items) return;  // the same for every thread of the block
+    const ItemMeta meta = p.meta[item];
+    const int32_t w = (int32_t)meta.w;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)W * p.pass_bytes);
+    const V Sv = A::splat(p.sentinel);
+    const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
+    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
+    V best = A::splat(0);
+    Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int pass_steps = w + G - 1;
+    const int rounds = (p.n_passes + W - 1) / W;
+    for (int round = 0; round < rounds; ++round) {
+        const int first = round * W;
+        const int cnt = min(W, p.n_passes - first);
+        if (threadIdx.x == 0)
+            bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
+        const bool ok = mbar_wait_bounded(bar, (uint32_t)(round & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicExch(p.err, 1);
+            return;
+        }
+        const int pass = first + warp;
+        const bool mine = warp < cnt && w > 0;
+        const int32_t row0 = p.vrow0 + pass * RPP + lane * R;
+        const uint8_t *prof = smem + (size_t)warp * p.pass_bytes;
+        Sweep<A, R> sw;
+        sweep_begin<A, R, MODE>(sw, row0, p.go, p.ge, Sv);
+        const int lag = 2 * BAND_K * warp;
+        const int total = pass_steps + 2 * BAND_K * (cnt - 1);
+        for (int t0 = 0; t0 < total; t0 += BAND_K) {
+            const int s0 = max(t0 - lag, 0), s1 = min(t0 + BAND_K - lag, pass_steps);
+            if (mine && s0 < s1)
+                sweep_run<A, G, R, MODE, true>(sw, s0, s1, lane, w, meta.n, res, prof, prof, row0,
+                                               pass == 0, pass == p.n_passes - 1, bnd, p.qlen, p.go,
+                                               p.ge, Sv, best, cand);
+            __syncthreads();
+        }
+        if (mine) sweep_end<A, R, MODE, true>(sw, row0, cand);
+        __syncthreads();  // the slices may be restaged for the next round
+    }
+    // Reduce every lane's candidates: inside each warp, then across warps in shared memory.
+    __shared__ Cand s_cand[32][2];
+#pragma unroll
+    for (int h = 0; h < A::NH; ++h) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            Cand o;
+            o.s = __shfl_xor_sync(0xffffffffu, cand[h].s, off);
+            o.col = __shfl_xor_sync(0xffffffffu, cand[h].col, off);
+            o.row = __shfl_xor_sync(0xffffffffu, cand[h].row, off);
+            if (better(o, cand[h])) cand[h] = o;
+        }
+        if (lane == 0) s_cand[warp][h] = cand[h];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int h = 0; h < A::NH; ++h) {
+            const uint32_t idx = meta.idx[h];
+            if (idx == NO_INDEX) continue;
+            Cand c = border_seed<MODE>(p.qlen, (int32_t)meta.n[h], p.go, p.ge);
+            for (int k = 0; k < W; ++k)
+                if (better(s_cand[k][h], c)) c = s_cand[k][h];
+            p.scores[idx] = c.s;
+            p.qend[idx] = c.row - 1;
+            p.tend[idx] = c.col - 1;
+        }
+    }
+}
+
 // ---- the batched pairwise kernel (align_pairs) -----------------------------------------------
 //
 // Every item carries its own queries (one per half, of equal length), so each group builds the
@@ -554,6 +684,7 @@ __device__ __forceinline__ void build_group_profile(uint8_t *dst, const uint8_t 
                                                     int32_t row_base, const int32_t *matrix,
                                                     int32_t al, int32_t lim, int32_t go,
                                                     int top_free, int lane) {
+    static_assert(R % A::EPV == 0 && R >= A::EPV, "rows per lane must fill whole profile vectors");
     constexpr int KCH = R / A::EPV;
     typename A::PE *out = reinterpret_cast<typename A::PE *>(dst);
     const int64_t pad = -(int64_t)lim - 1 + go;
@@ -646,6 +777,7 @@ template <class A, int G, int R>
 __global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32_t *matrix,
                                      int32_t al, int32_t go, int32_t lim, int top_free,
                                      int32_t vrow0, int32_t n_passes, typename A::PE *out) {
+    static_assert(R % A::EPV == 0 && R >= A::EPV, "rows per lane must fill whole profile vectors");
     constexpr int KCH = R / A::EPV;
     const int64_t per_pass = (int64_t)(al + 1) * G * R;
     const int64_t total = per_pass * n_passes;
