@@ -221,9 +221,9 @@ def run_cuda(args):
         gather_best(d_hits)
     end.record(stream)
     torch.cuda.synchronize()
-    kms = (C.c_double * 2)()
-    kl = (C.c_uint64 * 2)()
-    kcells = (C.c_double * 2)()
+    kms = (C.c_double * 3)()
+    kl = (C.c_uint64 * 3)()
+    kcells = (C.c_double * 3)()
     all_l = C.c_uint64()
     lib.hy_scratch_profile_read(sc._h, kms, kl, kcells, C.byref(all_l))
     lib.hy_scratch_profile(sc._h, 0)
@@ -272,8 +272,10 @@ def run_cuda(args):
     cells16_per_launch = kcells[0] / launches16
     avg16_ms = kms[0] / launches16
     achieved = cells16_per_launch / (avg16_ms * 1e-3) / 1e9 if avg16_ms > 0 else 0.0
-    i32_info = {"launches": int(kl[1]), "total_ms": kms[1], "cells": kcells[1],
-                "gcups": kcells[1] / (kms[1] * 1e-3) / 1e9 if kms[1] > 0 else None}
+    def _kinfo(i):
+        return {"launches": int(kl[i]), "ms_per_step": kms[i] / args.steps, "cells_per_step": kcells[i] / args.steps,
+                "gcups": kcells[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None}
+    kernels = {"bulk_int16x2_pairs": _kinfo(0), "long_int16x2_pairs": _kinfo(2), "int32_items": _kinfo(1)}
     meas = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm_peak = meas.get("hbm_gbs", 6650.0)
@@ -310,9 +312,7 @@ def run_cuda(args):
                          "kernel": "scan_kernel<Pair16,8,16,SW>", "avg_launch_ms": avg16_ms,
                          "launches": int(kl[0]), "cells_per_launch": cells16_per_launch,
                          "peak_source": "measured: hy_measure_dpx_peak (register-resident per-cell DPX mix)"},
-            "int32_kernel": i32_info,
-            "step_breakdown_ms": {"int16x2_kernels": kms[0] / args.steps, "int32_kernels_concurrent": kms[1] / args.steps,
-                                  "step": elapsed_ms / args.steps},
+            "kernels": kernels,
             "roofline_hbm": {"bound": "hbm", "peak": hbm_peak, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs" if meas else "fallback"},
             "clocks": clk,
         }

@@ -20,7 +20,15 @@ constexpr int MAIN_G32 = 32;
 constexpr int MAIN_R32 = 16;
 constexpr int WIN_G = 32;
 constexpr int WIN_R = 8;
+// Pairs longer than LONG_W columns: one full warp each (LONG_G lanes of LONG_R rows), launched
+// on a high-priority stream so the longest items start first and do not form the kernel's tail.
+constexpr int LONG_G = 32;
+constexpr int LONG_R = 8;
+constexpr uint32_t LONG_W = 2048;
 constexpr int BLOCK = 256;
+// Rows per lane of the bulk int16x2 kernel for a query of length qlen (passes of MAIN_G * rows).
+inline int bulk_rows(uint64_t qlen) { return qlen <= 64 ? 8 : qlen <= 192 ? 16 : 32; }
+constexpr int BULK_MAX_RPP = 8 * 32;
 constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;
 
 struct Partition {
@@ -76,6 +84,7 @@ namespace hy {
 // in int32 (always inside the int32 layout, which holds the static int32 set plus one).
 struct QuerySplit {
     uint32_t k0 = 0;      // first int16x2 pair item
+    uint32_t kl = 0;      // pairs [k0, kl) are long (one warp each), [kl, n) the bulk
     uint32_t n_i32 = 0;   // int32 items [0, n_i32)
 };
 
@@ -108,6 +117,12 @@ inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen) {
     }
     q.k0 = a;
     q.n_i32 = (uint32_t)std::min<uint64_t>(2ull * a, db->n_seqs);
+    b = (uint32_t)db->pair_w.size();
+    while (a < b) {
+        uint32_t mid = a + (b - a) / 2;
+        if (db->pair_w[mid] <= LONG_W) b = mid; else a = mid + 1;
+    }
+    q.kl = a;
     return q;
 }
 

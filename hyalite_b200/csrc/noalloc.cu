@@ -82,7 +82,7 @@ template <class A, int G, int R>
 Region plan_region(const hy_db *db, const Partition &part, uint64_t qlen, size_t &cursor) {
     Region r;
     if (!part.n_items) return r;
-    r.qp = plan(qlen, G * R, db->al, sizeof(typename A::PE));
+    r.qp = plan(qlen, G * R, db->al, profile_row_bytes<A>());
     r.prof_off = cursor;
     r.prof_bytes = (size_t)r.qp.n_passes * r.qp.pass_bytes;
     cursor = align256(cursor + r.prof_bytes);

@@ -142,7 +142,7 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
                           int32_t *d_qend, int32_t *d_tend) {
     if (pp.meta.empty()) return fail(HY_OK);
     const bool two = A::NH == 2;
-    const size_t group_bytes = 2 * (size_t)(al + 1) * G * R * sizeof(typename A::PE);
+    const size_t group_bytes = (size_t)(al + 1) * G * R * profile_row_bytes<A>();
     int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
     gpb = gpb / (32 / G) * (32 / G);  // whole warps
     if (gpb == 0) return fail(HY_ERR_UNSUPPORTED);

@@ -22,6 +22,10 @@ struct hy_scratch {
     // The int32 part of a scan runs on a second stream, forked from and joined back into `stream`.
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // The long int16x2 pairs run on a third stream; both side streams have the highest priority.
+    cudaStream_t stream3 = nullptr;
+    cudaEvent_t ev_join3 = nullptr;
+    uint8_t *d_prof16l = nullptr;
     uint8_t *d_query = nullptr;
     uint8_t *d_prof16 = nullptr, *d_prof32 = nullptr, *d_profw16 = nullptr, *d_profw32 = nullptr;
     void *d_bnd16 = nullptr, *d_bnd32 = nullptr;
@@ -38,8 +42,9 @@ struct hy_scratch {
     // Optional event timing of the main scan kernels (hy_scratch_profile).
     bool profile = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
-    std::vector<int> event_part;  // 0: int16x2 pair kernel, 1: int32 kernel
-    double event_cells[2] = {0.0, 0.0};  // real DP cells the timed launches computed
+    // Kernel class of each timed launch: 0 bulk int16x2 pairs, 1 int32 items, 2 long int16x2 pairs.
+    std::vector<int> event_part;
+    double event_cells[3] = {0.0, 0.0, 0.0};  // real DP cells the timed launches computed
     size_t n_events = 0;
     uint64_t launches = 0;        // every kernel this scratch launched since the last read
 };
@@ -111,7 +116,7 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
                                    const uint32_t *item_ptr, int blocks, int threads,
                                    cudaStream_t st_) {
     const bool i16 = sizeof(typename A::V) == 4 && A::NH == 2;
-    QueryPlan qp = plan(qlen, G * R, db->al, sizeof(typename A::PE));
+    QueryPlan qp = plan(qlen, G * R, db->al, profile_row_bytes<A>());
     HY_CK((launch_profile<A, G, R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof, st_)));
     sc->launches += qp.n_passes > 0 ? 2 : 1;
     ScanParams p;
@@ -144,8 +149,9 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
             sc->events.push_back({a, b});
             sc->event_part.push_back(0);
         }
-        sc->event_part[sc->n_events] = i16 ? 0 : 1;
-        sc->event_cells[i16 ? 0 : 1] +=
+        const int cls = i16 ? (G == LONG_G ? 2 : 0) : 1;
+        sc->event_part[sc->n_events] = cls;
+        sc->event_cells[cls] +=
             (double)qlen * (double)(part.res_prefix[item_end] - part.res_prefix[item_base]);
         HY_CK(cudaEventRecord(sc->events[sc->n_events].first, st_));
     }
@@ -178,15 +184,34 @@ static hy_status enqueue_scores(const hy_db *db, hy_scratch *sc, const uint8_t *
         if (st != HY_OK) return st;
         HY_CK(cudaEventRecord(sc->ev_join, sc->stream2));
     }
-    if (split.k0 < db->p16.n_items) {
-        const int blocks = (int)((db->p16.n_items - split.k0 + gpb - 1) / gpb);
-        st = enqueue_partition<Pair16, MAIN_G, MAIN_R16>(db, sc, db->p16, split.k0, db->p16.n_items,
-                                                        d_query, qlen, ends, key, scores,
-                                                        sc->d_prof16, sc->d_bnd16, nullptr, blocks,
-                                                        BLOCK, sc->stream);
+    const bool long_pairs = split.kl > split.k0;
+    if (long_pairs) {
+        HY_CK(cudaEventRecord(sc->ev_fork, sc->stream));
+        HY_CK(cudaStreamWaitEvent(sc->stream3, sc->ev_fork, 0));
+        const int gpbl = BLOCK / LONG_G;
+        const int blocks = (int)((split.kl - split.k0 + gpbl - 1) / gpbl);
+        st = enqueue_partition<Pair16, LONG_G, LONG_R>(db, sc, db->p16, split.k0, split.kl, d_query,
+                                                      qlen, ends, key, scores, sc->d_prof16l,
+                                                      sc->d_bnd16, nullptr, blocks, BLOCK,
+                                                      sc->stream3);
+        if (st != HY_OK) return st;
+        HY_CK(cudaEventRecord(sc->ev_join3, sc->stream3));
+    }
+    if (split.kl < db->p16.n_items) {
+        const int blocks = (int)((db->p16.n_items - split.kl + gpb - 1) / gpb);
+        // Rows per lane by query length: more rows amortise the per-step work, fewer keep the
+        // padding of a short query's single pass small.
+        const int rows = bulk_rows(qlen);
+#define HY_BULK(RR)                                                                              \
+    enqueue_partition<Pair16, MAIN_G, RR>(db, sc, db->p16, split.kl, db->p16.n_items, d_query,   \
+                                          qlen, ends, key, scores, sc->d_prof16, sc->d_bnd16,    \
+                                          nullptr, blocks, BLOCK, sc->stream)
+        st = rows == 8 ? HY_BULK(8) : rows == 16 ? HY_BULK(16) : HY_BULK(32);
+#undef HY_BULK
         if (st != HY_OK) return st;
     }
     if (forked) HY_CK(cudaStreamWaitEvent(sc->stream, sc->ev_join, 0));
+    if (long_pairs) HY_CK(cudaStreamWaitEvent(sc->stream, sc->ev_join3, 0));
     return fail(HY_OK);
 }
 
@@ -218,7 +243,7 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
                               uint32_t item_end, const uint8_t *d_query, uint64_t qlen,
                               uint8_t *prof, void *bnd, const uint32_t *item_ptr) {
     const bool i16 = A::NH == 2;
-    QueryPlan qp = plan(qlen, WIN_G * WIN_R, db->al, sizeof(typename A::PE));
+    QueryPlan qp = plan(qlen, WIN_G * WIN_R, db->al, profile_row_bytes<A>());
     HY_CK((launch_profile<A, WIN_G, WIN_R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof,
                                             sc->stream)));
     ScanParams p;
@@ -561,10 +586,12 @@ void hy_db_partition(const hy_db *db, uint64_t *n_i16, uint64_t *n_i32) {
 uint64_t hy_db_scratch_bytes(const hy_db *db) {
     const uint64_t mq = std::max<uint64_t>(db->mql, 1);
     uint64_t b = mq + 3 * 4 * db->n_seqs + 64 + sizeof(hy_hit);
-    b += npass(mq, MAIN_G * MAIN_R16) * (db->al + 1) * MAIN_G * MAIN_R16 * 2;
-    b += npass(mq, MAIN_G32 * MAIN_R32) * (db->al + 1) * MAIN_G32 * MAIN_R32 * 4;
-    b += npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 6;
-    if (mq > (uint64_t)std::min({MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R}))
+    b += npass(mq, BULK_MAX_RPP) * (db->al + 1) * BULK_MAX_RPP * profile_row_bytes<Pair16>();
+    b += npass(mq, LONG_G * LONG_R) * (db->al + 1) * LONG_G * LONG_R * profile_row_bytes<Pair16>();
+    b += npass(mq, MAIN_G32 * MAIN_R32) * (db->al + 1) * MAIN_G32 * MAIN_R32 * profile_row_bytes<Single32>();
+    b += npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R *
+         (profile_row_bytes<Pair16>() + profile_row_bytes<Single32>());
+    if (mq > (uint64_t)std::min({MAIN_G * 8, MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R}))
         b += 8 * (db->p16.total_cols + db->p32.total_cols);
     return b;
 }
@@ -585,15 +612,23 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
     const uint64_t mq = std::max<uint64_t>(db->mql, 1);
     const uint64_t n = std::max<uint64_t>(db->n_seqs, 1);
     ck(cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking));
-    ck(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));
+    int prio_low = 0, prio_high = 0;
+    ck(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    ck(cudaStreamCreateWithPriority(&sc->stream2, cudaStreamNonBlocking, prio_high));
+    ck(cudaStreamCreateWithPriority(&sc->stream3, cudaStreamNonBlocking, prio_high));
+    ck(cudaEventCreateWithFlags(&sc->ev_join3, cudaEventDisableTiming));
     ck(cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming));
     ck(cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming));
     ck(cudaMalloc(&sc->d_query, mq));
-    ck(cudaMalloc(&sc->d_prof16, std::max<uint64_t>(1, npass(mq, MAIN_G * MAIN_R16) * (db->al + 1) * MAIN_G * MAIN_R16 * 2)));
-    ck(cudaMalloc(&sc->d_prof32, std::max<uint64_t>(1, npass(mq, MAIN_G32 * MAIN_R32) * (db->al + 1) * MAIN_G32 * MAIN_R32 * 4)));
-    ck(cudaMalloc(&sc->d_profw16, std::max<uint64_t>(1, npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 2)));
-    ck(cudaMalloc(&sc->d_profw32, std::max<uint64_t>(1, npass(mq, WIN_G * WIN_R) * (db->al + 1) * WIN_G * WIN_R * 4)));
-    const bool multipass = mq > (uint64_t)std::min({MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R});
+    auto prof_bytes = [&](int rpp, size_t row_bytes) {
+        return std::max<uint64_t>(1, npass(mq, rpp) * (db->al + 1) * rpp * row_bytes);
+    };
+    ck(cudaMalloc(&sc->d_prof16, prof_bytes(BULK_MAX_RPP, profile_row_bytes<Pair16>())));
+    ck(cudaMalloc(&sc->d_prof16l, prof_bytes(LONG_G * LONG_R, profile_row_bytes<Pair16>())));
+    ck(cudaMalloc(&sc->d_prof32, prof_bytes(MAIN_G32 * MAIN_R32, profile_row_bytes<Single32>())));
+    ck(cudaMalloc(&sc->d_profw16, prof_bytes(WIN_G * WIN_R, profile_row_bytes<Pair16>())));
+    ck(cudaMalloc(&sc->d_profw32, prof_bytes(WIN_G * WIN_R, profile_row_bytes<Single32>())));
+    const bool multipass = mq > (uint64_t)std::min({MAIN_G * 8, MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R});
     ck(cudaMalloc(&sc->d_bnd16, multipass ? std::max<uint64_t>(8, 8 * db->p16.total_cols) : 8));
     ck(cudaMalloc(&sc->d_bnd32, multipass ? std::max<uint64_t>(8, 8 * db->p32.total_cols) : 8));
     ck(cudaMalloc(&sc->d_scores, 4 * n));
@@ -627,6 +662,7 @@ void hy_scratch_destroy(hy_scratch *sc) {
     if (sc->stream) cudaStreamSynchronize(sc->stream);
     cudaFree(sc->d_query);
     cudaFree(sc->d_prof16);
+    cudaFree(sc->d_prof16l);
     cudaFree(sc->d_prof32);
     cudaFree(sc->d_profw16);
     cudaFree(sc->d_profw32);
@@ -648,6 +684,9 @@ void hy_scratch_destroy(hy_scratch *sc) {
         cudaEventDestroy(e.second);
     }
     if (sc->stream2) cudaStreamSynchronize(sc->stream2);
+    if (sc->stream3) cudaStreamSynchronize(sc->stream3);
+    if (sc->ev_join3) cudaEventDestroy(sc->ev_join3);
+    if (sc->stream3) cudaStreamDestroy(sc->stream3);
     if (sc->ev_fork) cudaEventDestroy(sc->ev_fork);
     if (sc->ev_join) cudaEventDestroy(sc->ev_join);
     if (sc->stream2) cudaStreamDestroy(sc->stream2);
@@ -662,17 +701,17 @@ hy_status hy_scratch_profile(hy_scratch *sc, int enable) {
     sc->profile = enable != 0;
     sc->n_events = 0;
     sc->launches = 0;
-    sc->event_cells[0] = sc->event_cells[1] = 0.0;
+    sc->event_cells[0] = sc->event_cells[1] = sc->event_cells[2] = 0.0;
     return fail(HY_OK);
 }
 
-hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[2], uint64_t launches[2],
-                                  double cells[2], uint64_t *all_launches) {
+hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[3], uint64_t launches[3],
+                                  double cells[3], uint64_t *all_launches) {
     if (!sc || !kernel_ms || !launches) return fail(HY_ERR_INVALID_ARGUMENT);
     DeviceGuard g(sc->device);
     HY_CK(cudaStreamSynchronize(sc->stream));
-    kernel_ms[0] = kernel_ms[1] = 0.0;
-    launches[0] = launches[1] = 0;
+    kernel_ms[0] = kernel_ms[1] = kernel_ms[2] = 0.0;
+    launches[0] = launches[1] = launches[2] = 0;
     for (size_t i = 0; i < sc->n_events; ++i) {
         float ms = 0.f;
         HY_CK(cudaEventElapsedTime(&ms, sc->events[i].first, sc->events[i].second));
@@ -682,11 +721,12 @@ hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[2], uint64_t 
     if (cells) {
         cells[0] = sc->event_cells[0];
         cells[1] = sc->event_cells[1];
+        cells[2] = sc->event_cells[2];
     }
     if (all_launches) *all_launches = sc->launches;
     sc->n_events = 0;
     sc->launches = 0;
-    sc->event_cells[0] = sc->event_cells[1] = 0.0;
+    sc->event_cells[0] = sc->event_cells[1] = sc->event_cells[2] = 0.0;
     return fail(HY_OK);
 }
 

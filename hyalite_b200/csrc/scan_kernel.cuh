@@ -80,13 +80,20 @@ struct ScanParams {
 };
 
 // ---- lane arithmetic -----------------------------------------------------------------------
+//
+// Per cell the recurrence issues three ops on the ALU pipe (two __viaddmax for E and F, one
+// __vimax3 for H) and, for int16x2, three on the FMA pipe (__vadd2 for the diagonal's two profile
+// words and for G = H - go); the two half-rate pipes run in parallel.
 
 struct Pair16 {
     typedef uint32_t V;
-    typedef int16_t PE;
+    // Profile words: a low-half table holding (P, 0) and a high-half table holding (0, P), so the
+    // two sequences' substitution values are merged by per-halfword adds on the FMA pipe.
+    typedef uint32_t PE;
     typedef uint16_t RES;
     static constexpr int NH = 2;
-    static constexpr int EPV = 8;  // profile elements per 16-byte vector
+    static constexpr int EPV = 4;     // profile words per 16-byte vector
+    static constexpr int TABLES = 2;  // per pass slice: the low-half table, then the high-half one
     static constexpr int32_t VMIN = -32768, VMAX = 32767;
     __device__ __forceinline__ static V splat(int64_t x) {
         x = x < VMIN ? VMIN : (x > VMAX ? VMAX : x);
@@ -95,9 +102,10 @@ struct Pair16 {
     }
     __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s16x2(a, b, c); }
     __device__ __forceinline__ static V vmax(V a, V b) { return __vmaxs2(a, b); }
-    __device__ __forceinline__ static V vmax_relu(V a, V b) { return __vimax_s16x2_relu(a, b); }
     __device__ __forceinline__ static V vmax3(V a, V b, V c) { return __vimax3_s16x2(a, b, c); }
-    __device__ __forceinline__ static V vadd(V a, V b) { return __viaddmax_s16x2(a, b, 0x80008000u); }
+    __device__ __forceinline__ static V vmax3_relu(V a, V b, V c) { return __vimax3_s16x2_relu(a, b, c); }
+    __device__ __forceinline__ static V vadd(V a, V b) { return __vadd2(a, b); }
+    __device__ __forceinline__ static V diag(V g, V pa, V pb) { return __vadd2(__vadd2(g, pa), pb); }
     __device__ __forceinline__ static int32_t get(V v, int h) {
         return h ? (int32_t)(int16_t)(v >> 16) : (int32_t)(int16_t)(v & 0xffffu);
     }
@@ -113,26 +121,22 @@ struct Pair16 {
         a = r & 0xff;
         b = r >> 8;
     }
-    // Profile values of R rows for the two letters (a, b): interleave two int16 rows.
-    // prof_a serves the low half's letter a, prof_b the high half's letter b.
+    // Chunk k (EPV rows) of the profile for letters (a, b): prof_lo is the low-half table used by
+    // the low sequence, prof_hi the high-half table used by the high sequence.
     template <int R, int G>
-    __device__ __forceinline__ static void load_profile(const uint8_t *prof_a, const uint8_t *prof_b,
-                                                        int a, int b, int lane, V (&P)[R]) {
+    __device__ __forceinline__ static void load_chunk(const uint8_t *prof_lo, const uint8_t *prof_hi,
+                                                      int a, int b, int lane, int k, V (&pa)[EPV],
+                                                      V (&pb)[EPV]) {
         constexpr int KCH = R / EPV;
-        const uint4 *pa = reinterpret_cast<const uint4 *>(prof_a) + (size_t)a * KCH * G + lane;
-        const uint4 *pb = reinterpret_cast<const uint4 *>(prof_b) + (size_t)b * KCH * G + lane;
-#pragma unroll
-        for (int k = 0; k < KCH; ++k) {
-            uint4 A = pa[k * G], B = pb[k * G];
-            P[8 * k + 0] = __byte_perm(A.x, B.x, 0x5410);
-            P[8 * k + 1] = __byte_perm(A.x, B.x, 0x7632);
-            P[8 * k + 2] = __byte_perm(A.y, B.y, 0x5410);
-            P[8 * k + 3] = __byte_perm(A.y, B.y, 0x7632);
-            P[8 * k + 4] = __byte_perm(A.z, B.z, 0x5410);
-            P[8 * k + 5] = __byte_perm(A.z, B.z, 0x7632);
-            P[8 * k + 6] = __byte_perm(A.w, B.w, 0x5410);
-            P[8 * k + 7] = __byte_perm(A.w, B.w, 0x7632);
-        }
+        const uint4 A = reinterpret_cast<const uint4 *>(prof_lo)[((size_t)a * KCH + k) * G + lane];
+        const uint4 B = reinterpret_cast<const uint4 *>(prof_hi)[((size_t)b * KCH + k) * G + lane];
+        pa[0] = A.x; pa[1] = A.y; pa[2] = A.z; pa[3] = A.w;
+        pb[0] = B.x; pb[1] = B.y; pb[2] = B.z; pb[3] = B.w;
+    }
+    // The profile word of value v in table t (0: low half, 1: high half).
+    __host__ __device__ __forceinline__ static PE word(int64_t v, int t) {
+        const uint32_t h = (uint16_t)(int16_t)v;
+        return t ? (h << 16) : h;
     }
 };
 
@@ -142,15 +146,17 @@ struct Single32 {
     typedef uint8_t RES;
     static constexpr int NH = 1;
     static constexpr int EPV = 4;
+    static constexpr int TABLES = 1;
     static constexpr int64_t VMIN = INT32_MIN, VMAX = INT32_MAX;
     __device__ __forceinline__ static V splat(int64_t x) {
         return (V)(x < VMIN ? VMIN : (x > VMAX ? VMAX : x));
     }
     __device__ __forceinline__ static V addmax(V a, V b, V c) { return __viaddmax_s32(a, b, c); }
     __device__ __forceinline__ static V vmax(V a, V b) { return max(a, b); }
-    __device__ __forceinline__ static V vmax_relu(V a, V b) { return __vimax_s32_relu(a, b); }
     __device__ __forceinline__ static V vmax3(V a, V b, V c) { return __vimax3_s32(a, b, c); }
+    __device__ __forceinline__ static V vmax3_relu(V a, V b, V c) { return __vimax3_s32_relu(a, b, c); }
     __device__ __forceinline__ static V vadd(V a, V b) { return a + b; }
+    __device__ __forceinline__ static V diag(V g, V pa, V) { return g + pa; }
     __device__ __forceinline__ static int32_t get(V v, int) { return v; }
     __device__ __forceinline__ static V bmax(V best, V x, bool &up0, bool &up1) {
         bool p;
@@ -164,20 +170,22 @@ struct Single32 {
         b = r;
     }
     template <int R, int G>
-    __device__ __forceinline__ static void load_profile(const uint8_t *prof_a, const uint8_t *,
-                                                        int a, int, int lane, V (&P)[R]) {
+    __device__ __forceinline__ static void load_chunk(const uint8_t *prof, const uint8_t *, int a,
+                                                      int, int lane, int k, V (&pa)[EPV],
+                                                      V (&pb)[EPV]) {
         constexpr int KCH = R / EPV;
-        const int4 *pa = reinterpret_cast<const int4 *>(prof_a) + (size_t)a * KCH * G + lane;
-#pragma unroll
-        for (int k = 0; k < KCH; ++k) {
-            int4 A = pa[k * G];
-            P[4 * k + 0] = A.x;
-            P[4 * k + 1] = A.y;
-            P[4 * k + 2] = A.z;
-            P[4 * k + 3] = A.w;
-        }
+        const int4 A = reinterpret_cast<const int4 *>(prof)[((size_t)a * KCH + k) * G + lane];
+        pa[0] = A.x; pa[1] = A.y; pa[2] = A.z; pa[3] = A.w;
+        pb[0] = pb[1] = pb[2] = pb[3] = 0;
     }
+    __host__ __device__ __forceinline__ static PE word(int64_t v, int) { return (PE)v; }
 };
+
+// Profile bytes per (letter, query row) of one lane arithmetic: every table's word.
+template <class A>
+constexpr size_t profile_row_bytes() {
+    return A::TABLES * sizeof(typename A::PE);
+}
 
 // ---- small helpers -------------------------------------------------------------------------
 
@@ -308,29 +316,37 @@ __device__ __forceinline__ void sweep_begin(Sweep<A, R> &sw, const int32_t row0,
     sw.pid1 = -1;
 }
 
-template <class A, int G, int R, int MODE, bool ENDS>
-__device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, const int s_end,
-                                          const int lane, const int32_t w, const uint32_t (&n)[2],
-                                          const typename A::RES *__restrict__ res,
-                                          const uint8_t *prof_a, const uint8_t *prof_b,
-                                          const int32_t row0, const bool first_pass,
-                                          const bool last_pass, typename A::V *bnd,
-                                          const int32_t qlen, const int32_t go, const int32_t ge,
-                                          const typename A::V Sv, typename A::V &best,
-                                          Cand (&cand)[2]) {
+// Constants of a sweep that do not change from step to step.
+template <class A>
+struct SweepConst {
+    typename A::V negge, neggo, Sv;
+    typename A::V top_free_g;  // G of the free top border row (H = 0)
+};
+
+// One step s of one lane. CHECKED steps test whether the lane's column is inside [1, w]; the
+// caller runs unchecked steps only where every lane of the warp is live.
+template <class A, int G, int R, int MODE, bool ENDS, bool CHECKED>
+__device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const int lane,
+                                           const int32_t w, const uint32_t (&n)[2],
+                                           const typename A::RES *__restrict__ res,
+                                           const uint8_t *prof_a, const uint8_t *prof_b,
+                                           const int32_t row0, const bool first_pass,
+                                           const bool last_pass, typename A::V *bnd,
+                                           const int32_t qlen, const int32_t go, const int32_t ge,
+                                           const SweepConst<A> &k, typename A::V &best,
+                                           Cand (&cand)[2]) {
     typedef typename A::V V;
     typedef ModeFlags<MODE> Fl;
-    const V negge = A::splat(-(int64_t)ge), neggo = A::splat(-(int64_t)go);
-    for (int s = s_begin; s < s_end; ++s) {
+    const V negge = k.negge, neggo = k.neggo;
+    {
         const int32_t j = s - lane + 1;
         V upG = __shfl_up_sync(0xffffffffu, sw.botG, 1, G);
         V upF = __shfl_up_sync(0xffffffffu, sw.botF, 1, G);
-        const bool live = j >= 1 && j <= w;
+        const bool live = !CHECKED || (j >= 1 && j <= w);
         if (lane == 0) {
             if (first_pass) {
-                const int64_t tb = Fl::top_free ? 0 : -gap_pen(go, ge, j);
-                upG = A::splat(tb - go);
-                upF = Sv;
+                upG = Fl::top_free ? k.top_free_g : A::splat(-gap_pen(go, ge, j) - go);
+                upF = k.Sv;
             } else if (live) {
                 upG = bnd[2 * (j - 1)];
                 upF = bnd[2 * (j - 1) + 1];
@@ -339,16 +355,17 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
         if (live) {
             int a, b;
             A::residues(res[j - 1], a, b);
-            V P[R];
-            A::template load_profile<R, G>(prof_a, prof_b, a, b, lane, P);
+            V pa[A::EPV], pb[A::EPV];
             V g_up = upG, f = upF, gd = sw.diag, hprev = A::splat(0), hlast = A::splat(0);
             const int32_t jR = j * R;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+                if (r % A::EPV == 0)
+                    A::template load_chunk<R, G>(prof_a, prof_b, a, b, lane, r / A::EPV, pa, pb);
                 sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
                 f = A::addmax(f, negge, g_up);
-                const V t = Fl::local ? A::vmax_relu(sw.E[r], f) : A::vmax(sw.E[r], f);
-                const V h = A::addmax(gd, P[r], t);
+                const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
+                const V h = Fl::local ? A::vmax3_relu(d, sw.E[r], f) : A::vmax3(d, sw.E[r], f);
                 gd = sw.Gp[r];
                 const V g = A::vadd(h, neggo);
                 sw.Gp[r] = g;
@@ -399,6 +416,39 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
     }
 }
 
+// Steps [s_begin, s_end) of one lane. `w_min` is the smallest item width in the warp: steps in
+// [G-1, w_min) have every lane of the warp on a real column and skip the per-lane checks. All
+// bounds are warp-uniform.
+template <class A, int G, int R, int MODE, bool ENDS>
+__device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, const int s_end,
+                                          const int w_min, const int lane, const int32_t w,
+                                          const uint32_t (&n)[2],
+                                          const typename A::RES *__restrict__ res,
+                                          const uint8_t *prof_a, const uint8_t *prof_b,
+                                          const int32_t row0, const bool first_pass,
+                                          const bool last_pass, typename A::V *bnd,
+                                          const int32_t qlen, const int32_t go, const int32_t ge,
+                                          const typename A::V Sv, typename A::V &best,
+                                          Cand (&cand)[2]) {
+    SweepConst<A> k;
+    k.negge = A::splat(-(int64_t)ge);
+    k.neggo = A::splat(-(int64_t)go);
+    k.Sv = Sv;
+    k.top_free_g = A::splat(-(int64_t)go);
+    const int fast_lo = max(s_begin, G - 1);
+    const int fast_hi = max(fast_lo, min(s_end, w_min));
+    const int head_end = min(s_end, fast_lo);
+    for (int s = s_begin; s < head_end; ++s)
+        sweep_step<A, G, R, MODE, ENDS, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                              first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+    for (int s = fast_lo; s < fast_hi; ++s)
+        sweep_step<A, G, R, MODE, ENDS, false>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                               first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+    for (int s = max(fast_hi, head_end); s < s_end; ++s)
+        sweep_step<A, G, R, MODE, ENDS, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                              first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+}
+
 template <class A, int R, int MODE, bool ENDS>
 __device__ __forceinline__ void sweep_end(const Sweep<A, R> &sw, const int32_t row0, Cand (&cand)[2]) {
     if (ModeFlags<MODE>::local && ENDS) {
@@ -409,8 +459,8 @@ __device__ __forceinline__ void sweep_end(const Sweep<A, R> &sw, const int32_t r
 
 // One whole pass: begin, every step, end.
 template <class A, int G, int R, int MODE, bool ENDS>
-__device__ __forceinline__ void sweep_pass(const int lane, const int steps, const int32_t w,
-                                           const uint32_t (&n)[2],
+__device__ __forceinline__ void sweep_pass(const int lane, const int steps, const int w_min,
+                                           const int32_t w, const uint32_t (&n)[2],
                                            const typename A::RES *__restrict__ res,
                                            const uint8_t *prof_a, const uint8_t *prof_b,
                                            const int32_t row0, const bool first_pass,
@@ -420,8 +470,8 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
                                            Cand (&cand)[2]) {
     Sweep<A, R> sw;
     sweep_begin<A, R, MODE>(sw, row0, go, ge, Sv);
-    sweep_run<A, G, R, MODE, ENDS>(sw, 0, steps, lane, w, n, res, prof_a, prof_b, row0, first_pass,
-                                   last_pass, bnd, qlen, go, ge, Sv, best, cand);
+    sweep_run<A, G, R, MODE, ENDS>(sw, 0, steps, w_min, lane, w, n, res, prof_a, prof_b, row0,
+                                   first_pass, last_pass, bnd, qlen, go, ge, Sv, best, cand);
     sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
 }
 
@@ -522,6 +572,7 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
     const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
     V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
+    const int w_min = (int)__reduce_min_sync(0xffffffffu, meta.w);
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
 
     V best = A::splat(0);
@@ -546,8 +597,9 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
             if (threadIdx.x == 0) atomicExch(p.err, 1);
             return;
         }
-        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, (int32_t)meta.w, meta.n, res, prof_buf[buf],
-                                        prof_buf[buf], p.vrow0 + pass * RPP + lane * R, pass == 0,
+        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof_buf[buf],
+                                        prof_buf[buf] + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
+                                        p.vrow0 + pass * RPP + lane * R, pass == 0,
                                         pass == p.n_passes - 1, bnd, p.qlen, p.go, p.ge, Sv, best,
                                         cand);
         __syncthreads();  // the profile buffer and boundary row are free again
@@ -610,6 +662,7 @@ __global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
         const bool mine = warp < cnt && w > 0;
         const int32_t row0 = p.vrow0 + pass * RPP + lane * R;
         const uint8_t *prof = smem + (size_t)warp * p.pass_bytes;
+        const uint8_t *prof_hi = prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES);
         Sweep<A, R> sw;
         sweep_begin<A, R, MODE>(sw, row0, p.go, p.ge, Sv);
         const int lag = 2 * BAND_K * warp;
@@ -617,7 +670,7 @@ __global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
         for (int t0 = 0; t0 < total; t0 += BAND_K) {
             const int s0 = max(t0 - lag, 0), s1 = min(t0 + BAND_K - lag, pass_steps);
             if (mine && s0 < s1)
-                sweep_run<A, G, R, MODE, true>(sw, s0, s1, lane, w, meta.n, res, prof, prof, row0,
+                sweep_run<A, G, R, MODE, true>(sw, s0, s1, w, lane, w, meta.n, res, prof, prof_hi, row0,
                                                pass == 0, pass == p.n_passes - 1, bnd, p.qlen, p.go,
                                                p.ge, Sv, best, cand);
             __syncthreads();
@@ -683,7 +736,7 @@ template <class A, int G, int R>
 __device__ __forceinline__ void build_group_profile(uint8_t *dst, const uint8_t *q, int32_t qlen,
                                                     int32_t row_base, const int32_t *matrix,
                                                     int32_t al, int32_t lim, int32_t go,
-                                                    int top_free, int lane) {
+                                                    int top_free, int lane, int table) {
     static_assert(R % A::EPV == 0 && R >= A::EPV, "rows per lane must fill whole profile vectors");
     constexpr int KCH = R / A::EPV;
     typename A::PE *out = reinterpret_cast<typename A::PE *>(dst);
@@ -705,7 +758,7 @@ __device__ __forceinline__ void build_group_profile(uint8_t *dst, const uint8_t 
                     if (sub > lim) sub = lim;
                     v = sub + go;
                 }
-                out[(((size_t)letter * KCH + k) * G + lane) * A::EPV + e] = (typename A::PE)v;
+                out[(((size_t)letter * KCH + k) * G + lane) * A::EPV + e] = A::word(v, table);
             }
         }
     }
@@ -735,8 +788,9 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     const int32_t vrow0 = qlen - n_passes * RPP + 1;
     const uint8_t *qa = active ? p.q_res + p.qoff[2 * (size_t)item] : p.q_res;
     const uint8_t *qb = (active && A::NH > 1 && meta.idx[1] != NO_INDEX) ? p.q_res + p.qoff[2 * (size_t)item + 1] : qa;
+    // The group's region: the low-half table of query a, then (int16x2) the high-half table of b.
     uint8_t *gprof_a = smem + (size_t)gib * p.group_bytes;
-    uint8_t *gprof_b = gprof_a + p.group_bytes / 2;
+    uint8_t *gprof_b = gprof_a + (A::TABLES - 1) * (p.group_bytes / A::TABLES);
     const V Sv = A::splat(p.sentinel);
     const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
     V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
@@ -751,14 +805,16 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
         const int32_t row_base = vrow0 + pass * RPP;
         if (mine) {
             build_group_profile<A, G, R>(gprof_a, qa, qlen, row_base, p.matrix, p.al, p.lim, p.go,
-                                         p.top_free, lane);
-            if (A::NH > 1)
+                                         p.top_free, lane, 0);
+            if (A::TABLES > 1)
                 build_group_profile<A, G, R>(gprof_b, qb, qlen, row_base, p.matrix, p.al, p.lim,
-                                             p.go, p.top_free, lane);
+                                             p.go, p.top_free, lane, 1);
         }
         __syncwarp();
         // `steps` stays warp-uniform; a group past its last pass sweeps zero columns.
-        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, mine ? (int32_t)meta.w : 0, meta.n,
+        const int w_here = mine ? (int)meta.w : 0;
+        const int w_min = (int)__reduce_min_sync(0xffffffffu, (uint32_t)w_here);
+        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, w_here, meta.n,
                                         res, gprof_a, gprof_b, row_base + lane * R, pass == 0,
                                         pass == n_passes - 1, bnd, qlen, p.go, p.ge, Sv, best, cand);
         __syncwarp();
@@ -769,22 +825,25 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
 
 // ---- query profile ----------------------------------------------------------------------------
 //
-// Layout of one pass slice: [letter 0..al][chunk k < R/EPV][lane < G][EPV elements], element e of
-// chunk k of lane L being grid row vrow0 + pass*G*R + L*R + k*EPV + e. Letter `al` is the padding
-// symbol. Values are P = clamp(sub, -(lim+1), lim) + go; virtual rows (<= 0) get go (free top
-// border) or 0 (penalised top border); the padding symbol gets -(lim+1) + go.
+// Layout of one pass slice: [table < TABLES][letter 0..al][chunk k < R/EPV][lane < G][EPV words],
+// word e of chunk k of lane L being grid row vrow0 + pass*G*R + L*R + k*EPV + e. Letter `al` is the
+// padding symbol. Values are P = clamp(sub, -(lim+1), lim) + go; virtual rows (<= 0) get go (free
+// top border) or 0 (penalised top border); the padding symbol gets -(lim+1) + go. For int16x2 the
+// first table holds each value in the low half of its word, the second in the high half.
 template <class A, int G, int R>
 __global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32_t *matrix,
                                      int32_t al, int32_t go, int32_t lim, int top_free,
                                      int32_t vrow0, int32_t n_passes, typename A::PE *out) {
     static_assert(R % A::EPV == 0 && R >= A::EPV, "rows per lane must fill whole profile vectors");
     constexpr int KCH = R / A::EPV;
-    const int64_t per_pass = (int64_t)(al + 1) * G * R;
+    const int64_t per_table = (int64_t)(al + 1) * G * R;
+    const int64_t per_pass = per_table * A::TABLES;
     const int64_t total = per_pass * n_passes;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pass = i / per_pass;
-        int64_t rem = i % per_pass;
+        const int table = (int)((i % per_pass) / per_table);
+        int64_t rem = i % per_table;
         const int e = (int)(rem % A::EPV);
         rem /= A::EPV;
         const int lane = (int)(rem % G);
@@ -804,7 +863,7 @@ __global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32
             if (sub > lim) sub = lim;
             v = sub + go;
         }
-        out[i] = (typename A::PE)v;
+        out[i] = A::word(v, table);
     }
 }
 

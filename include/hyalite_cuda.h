@@ -186,11 +186,12 @@ hy_status hy_scratch_sync(hy_scratch *scratch);
 
 /* While enabled, every main scan-kernel launch on this scratch is bracketed by CUDA events on the
  * stream it runs on. _read synchronises and returns, since the last read (or enable), the summed
- * kernel time, launch count and real DP cells of the int16x2 pair kernel ([0]) and the int32
- * kernel ([1]), plus the number of kernels of every kind this scratch launched; then resets them. */
+ * kernel time, launch count and real DP cells of the bulk int16x2 pair kernel ([0]), the int32
+ * kernel ([1]) and the long-pair int16x2 kernel ([2]), plus the number of kernels of every kind
+ * this scratch launched; then resets them. */
 hy_status hy_scratch_profile(hy_scratch *scratch, int enable);
-hy_status hy_scratch_profile_read(hy_scratch *scratch, double kernel_ms[2], uint64_t launches[2],
-                                  double cells[2], uint64_t *all_launches);
+hy_status hy_scratch_profile_read(hy_scratch *scratch, double kernel_ms[3], uint64_t launches[3],
+                                  double cells[3], uint64_t *all_launches);
 /* The packed-int16 DPX roofline of the current device: the scan's per-cell instruction mix run
  * register resident on every SM, in DP cells per second. */
 hy_status hy_measure_dpx_peak(double *cells_per_second);
