@@ -37,10 +37,15 @@ N_QUERIES = 16
 N_SEQS = 500_000
 GO, GE = 11, 1
 AL = 20
+# DRAM bytes (read + write) per DP cell of the int16x2 pair kernel, from one ncu capture of
+# scan_kernel<Pair16, 8, 32> on 400,000 sequences x one 1000-residue query: 1.349e9 bytes for
+# 1.563e11 cells. The traffic is the boundary rows between query passes plus the residues, so it
+# grows with cells at a fixed rows-per-pass; profiles/ holds the capture's summary and command.
+DRAM_BYTES_PER_CELL = 1.349e9 / 1.563e11
 
 
 def make_workload(seed: int, n_seqs: int = N_SEQS):
-    """The config-2 generator: seeded matrix, background, lengths, residues and queries."""
+    """The protein workload generator: seeded matrix, background, lengths, residues and queries."""
     rng = np.random.default_rng(seed)
     base = np.random.default_rng(12345)  # the matrix and background are fixed across shards
     mat = base.integers(-4, 4, size=(AL, AL))
@@ -143,7 +148,7 @@ def run_reference(args):
         "impl": "reference", "metric": "GCUPS", "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "i8/i16/i32 lanes (AVX2)", "data": "synthetic",
-        "config": {"workload": "config 2: protein SW ScoreEnd scan (bounded sample)", "parallelism": f"{threads} host threads"},
+        "config": {"workload": "protein SW ScoreEnd scan, 500k log-normal sequences x 16 queries (100..5000), AVX2 port on a bounded sample", "parallelism": f"{threads} host threads"},
         "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -294,9 +299,9 @@ def run_cuda(args):
             "metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "i16x2 (int32 for long sequences)",
-            "data": "synthetic (seeded, config-2 generator)",
+            "data": "synthetic (seeded protein generator: log-normal lengths, fixed background)",
             "config": {
-                "workload": "config 2: protein SW ScoreEnd scan, plain per-query form",
+                "workload": "protein SW ScoreEnd scan, 500k log-normal sequences x 16 queries (100..5000), plain per-query form",
                 "n_seqs_per_gpu": n_seqs, "residues_per_gpu": int(total_res), "queries_per_step": N_QUERIES,
                 "query_lengths": QUERY_LENGTHS, "cells_per_step_per_gpu": cells_step,
                 "partition_i16x2_i32": [n16, n32], "db_build_s": round(build_s, 2),
@@ -308,8 +313,12 @@ def run_cuda(args):
                     "d2h_bytes_per_step": 32 * N_QUERIES},
             "gpu_launches": int(all_l.value),
             "roofline": {"bound": "dpx_int16x2", "achieved": achieved, "peak": peak_gcups, "unit": "GCUPS",
-                         "frac": achieved / peak_gcups if peak_gcups else None, "traffic": None,
-                         "kernel": "scan_kernel<Pair16,8,16,SW>", "avg_launch_ms": avg16_ms,
+                         "frac": achieved / peak_gcups if peak_gcups else None,
+                         "traffic": cells16_per_launch * DRAM_BYTES_PER_CELL,
+                         "traffic_note": "bytes per launch: dram read+write per cell from one ncu capture "
+                                         "(400k sequences x 1000-residue query) times this launch's cells",
+                         "kernel": "scan_kernel<Pair16,8,R,SW>, R = 8/16/32 rows per lane by query length",
+                         "avg_launch_ms": avg16_ms,
                          "launches": int(kl[0]), "cells_per_launch": cells16_per_launch,
                          "peak_source": "measured: hy_measure_dpx_peak (register-resident per-cell DPX mix)"},
             "kernels": kernels,
