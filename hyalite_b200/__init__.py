@@ -460,6 +460,87 @@ class Scratch:
         return int(lib.hy_scratch_stream(self._h) or 0)
 
 
+# ---- batched scan (no reference counterpart) ---------------------------------------------------------------
+
+class Batch:
+    """Many queries per call, each against one of a fixed list of databases (any modes): the same
+    BestHit per query as ``Database.scan``, computed by persistent kernels under a CUDA graph
+    (hy_scan_batch). With ``autotune`` the first call of each batch shape tunes the launch shapes."""
+
+    def __init__(self, dbs: Sequence[Database], max_queries: int, autotune: bool = True):
+        dbs = list(dbs)
+        arr = (C.c_void_p * len(dbs))(*[d._h.value for d in dbs])
+        h = C.c_void_p()
+        _check(lib.hy_batch_create(arr, len(dbs), int(max_queries), 1 if autotune else 0, C.byref(h)))
+        self._h = h
+        self._dbs = dbs  # keep the databases alive while the batch exists
+        self.max_queries = int(max_queries)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.hy_batch_destroy(h)
+            self._h = C.c_void_p(None)
+
+    @staticmethod
+    def _pack(queries, db_of_query):
+        qs = [_as_u8(q) for q in queries]
+        off = np.zeros(len(qs) + 1, dtype=np.uint64)
+        off[1:] = np.cumsum([len(q) for q in qs]) if qs else []
+        res = np.concatenate(qs) if qs and off[-1] > 0 else np.zeros(1, np.uint8)
+        dbq = np.zeros(len(qs), np.uint32) if db_of_query is None else np.ascontiguousarray(db_of_query, np.uint32)
+        if len(dbq) != len(qs):
+            raise ValueError("db_of_query must name one database per query")
+        return res, off, dbq
+
+    def scan_arrays(self, q_res, q_off, db_of_query):
+        """Hits (a ctypes array of hy_hit) for concatenated queries; raises the first query's error
+        with ``failed_query`` set on the exception."""
+        q_res = np.ascontiguousarray(q_res, dtype=np.uint8)
+        q_res = q_res if q_res.size else np.zeros(1, np.uint8)
+        q_off = np.ascontiguousarray(q_off, dtype=np.uint64)
+        dbq = np.ascontiguousarray(db_of_query, dtype=np.uint32)
+        n = len(q_off) - 1
+        out = (_abi.HyHit * max(n, 1))()
+        failed = C.c_uint32(0)
+        st = lib.hy_scan_batch(self._h, n, _ptr(dbq, _abi._u32p), _ptr(q_res, _abi._u8p),
+                               _ptr(q_off, _abi._u64p), out, C.byref(failed))
+        if st != _abi.OK:
+            err = Error.from_status(st)
+            err.failed_query = int(failed.value)
+            raise err
+        return out
+
+    def scan(self, queries, db_of_query=None) -> List[BestHit]:
+        res, off, dbq = self._pack(queries, db_of_query)
+        arr = self.scan_arrays(res, off, dbq)
+        return [BestHit._from(arr[i]) for i in range(len(off) - 1)]
+
+    def tune(self, queries, db_of_query=None, stride: int = 0) -> float:
+        """Runs the autotuner on this batch now; returns the chosen configuration's sampled ms."""
+        res, off, dbq = self._pack(queries, db_of_query)
+        ms = C.c_double()
+        _check(lib.hy_batch_tune(self._h, len(off) - 1, _ptr(dbq, _abi._u32p), _ptr(res, _abi._u8p),
+                                 _ptr(off, _abi._u64p), int(stride), C.byref(ms)))
+        return float(ms.value)
+
+    def config(self):
+        """(max query length with 8 rows per lane, with 16 rows, long-pair width split)."""
+        c = (C.c_int32 * 3)()
+        _check(lib.hy_batch_get_config(self._h, c))
+        return tuple(int(x) for x in c)
+
+    def set_config(self, rows8_max: int, rows16_max: int, long_w: int) -> None:
+        c = (C.c_int32 * 3)(rows8_max, rows16_max, long_w)
+        _check(lib.hy_batch_set_config(self._h, c))
+
+    def device_bytes(self) -> int:
+        return int(lib.hy_batch_device_bytes(self._h))
+
+    def stream_ptr(self) -> int:
+        return int(lib.hy_batch_stream(self._h) or 0)
+
+
 # ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------------------
 
 def align_pairs_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, mode: Mode, search_type: SearchType):
@@ -499,6 +580,6 @@ def align_pairs(pairs, scoring: Scoring, mode: Mode, search_type: SearchType, ou
 
 __all__ = [
     "BACKEND_ENV_VAR", "Backend", "BackendChoice", "BestHit", "Database", "DatabaseBuilder", "Error",
-    "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
+    "Batch", "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
     "align_pairs", "align_pairs_arrays", "required_width", "concat",
 ]

@@ -35,6 +35,7 @@ class HyHit(C.Structure):
 _u8p = C.POINTER(C.c_uint8)
 _u64p = C.POINTER(C.c_uint64)
 _i32p = C.POINTER(C.c_int32)
+_u32p = C.POINTER(C.c_uint32)
 _i64p = C.POINTER(C.c_int64)
 _vp = C.c_void_p
 _st = C.c_int
@@ -80,6 +81,14 @@ SIGNATURES = {
     "hy_measure_dpx_peak": (_st, [C.POINTER(C.c_double)]),
     "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
+    "hy_batch_create": (_st, [C.POINTER(_vp), C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_vp)]),
+    "hy_batch_destroy": (None, [_vp]),
+    "hy_scan_batch": (_st, [_vp, C.c_uint32, _u32p, _u8p, _u64p, C.POINTER(HyHit), _u32p]),
+    "hy_batch_tune": (_st, [_vp, C.c_uint32, _u32p, _u8p, _u64p, C.c_uint32, C.POINTER(C.c_double)]),
+    "hy_batch_get_config": (_st, [_vp, _i32p]),
+    "hy_batch_set_config": (_st, [_vp, _i32p]),
+    "hy_batch_device_bytes": (C.c_uint64, [_vp]),
+    "hy_batch_stream": (_vp, [_vp]),
 }
 
 

@@ -1,0 +1,788 @@
+// batch.cu -- the batched form of the database scan.
+//
+// Many queries, each against its own Database (any mode and search type; all databases on one
+// device), run in persistent kernels that pull (query, item chunk) units from a device work queue.
+// The queue is walked chunk-major: chunk 0 (the longest targets, the databases being length
+// sorted) for every query, longest query first, then chunk 1, and so on, so the largest units go
+// first and the queue drains with a short tail; all queries reading the same chunk at about the
+// same time also share its residues in L2. Each class of launch shape (int16x2 pairs with 8, 16 or
+// 32 rows per lane; pairs wider than the long-pair split, one warp each; int32 items) has its own
+// persistent kernel and queue. The winners' end positions are recovered by one block per query.
+//
+// All device work of a batch is captured once into a CUDA graph: the kernels read the batch from
+// device descriptors (BatchQuery, BatchCtl) that each call rewrites with a few copies before
+// replaying the graph. An autotuner times candidate launch configurations (rows per lane by query
+// length, the long-pair width split) on a sampled part of a batch and keeps the fastest per batch
+// shape. Results are bit-identical to hy_scan per query: the same per-cell kernels, reduction keys
+// and winner-ends recovery.
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
+
+#include "db_internal.h"
+
+using namespace hy;
+
+namespace hy {
+
+// Launch classes (one persistent kernel each) and profile kinds (one query profile each).
+enum { BC_BULK8 = 0, BC_BULK16 = 1, BC_BULK32 = 2, BC_LONG = 3, BC_I32 = 4, BC_N = 5 };
+enum { PK_BULK = 0, PK_W16 = 1, PK_I32 = 2, PK_W32 = 3, PK_N = 4 };
+static constexpr int LCG = LONG_G, LCR = LONG_R;      // long pairs and the int16x2 band
+static constexpr int ICG = MAIN_G32, ICR = MAIN_R32;  // int32 items
+static constexpr uint32_t LONG_W_MAX = 4096;          // largest long-pair split the tuner tries
+
+struct BatchQuery {
+    // Per profile kind: everything its launches need except the block's boundary region.
+    ScanParams sp[PK_N];
+    const int32_t *matrix;
+    const uint8_t *q;
+    const uint32_t *rank;
+    int32_t qlen, mode, ends, bulk_rows, top_free, al, lim16;
+    uint32_t k0, kl, n_i32, n16;
+};
+
+struct BatchCtl {
+    uint32_t count[BC_N];     // query slots in each class's order list
+    uint32_t n_chunks[BC_N];  // item chunks each class's queue walks
+    uint32_t head[BC_N];      // work counters (zeroed by the graph)
+    uint32_t n_queries;
+    uint32_t chunk_stride;    // 1, or k to run only every k-th chunk (autotuner samples)
+};
+
+struct ClassLaunch {
+    const BatchQuery *queries;
+    const uint32_t *order;  // this class's query slots, longest query first
+    BatchCtl *ctl;
+    int cls;
+    uint8_t *bnd;           // block-private boundary regions
+    size_t bnd_stride;
+};
+
+struct BandLaunch {
+    const BatchQuery *queries;
+    const BatchCtl *ctl;
+    uint8_t *bnd;           // one boundary region per query slot
+    size_t bnd_stride;
+    int32_t *ends;          // {score, query end, target end} per query slot
+};
+
+__device__ __forceinline__ void class_range(const BatchQuery &bq, int cls, uint32_t &lo, uint32_t &hi) {
+    if (cls == BC_LONG) {
+        lo = bq.k0;
+        hi = bq.kl;
+    } else if (cls == BC_I32) {
+        lo = 0;
+        hi = bq.n_i32;
+    } else {
+        lo = bq.kl;
+        hi = bq.n16;
+    }
+}
+
+// Resident 256-thread blocks per SM each launch shape is compiled for (its register budget): the
+// plain scan kernels of the same shapes reach these occupancies.
+template <class A, int G, int R>
+constexpr int batch_min_blocks() {
+    return A::NH == 1 ? 2 : (G == 8 && R == 8) ? 4 : (G == 8 && R == 32) ? 2 : 3;
+}
+
+// One persistent kernel per launch class: blocks take units off the class queue until it is empty.
+// Shared memory: the two profile mbarriers, then two pass slices of the largest pass of the batch.
+template <class A, int G, int R, int PK>
+__global__ void __launch_bounds__(256, batch_min_blocks<A, G, R>()) batch_scan_kernel(const ClassLaunch L) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint32_t s_unit;
+    constexpr uint32_t IPU = 256 / G;  // items per unit: one per group of the block
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    uint8_t *bufs = smem + 128;
+    const uint32_t nq = L.ctl->count[L.cls];
+    const uint32_t stride = L.ctl->chunk_stride;
+    const uint32_t n_chunks = (L.ctl->n_chunks[L.cls] + stride - 1) / stride;
+    const uint32_t n_units = n_chunks * nq;
+    if (n_units == 0) return;
+    init_profile_bars(bars);
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(&L.ctl->head[L.cls], 1u);
+        __syncthreads();
+        const uint32_t u = s_unit;
+        __syncthreads();  // every thread has read s_unit before thread 0 takes the next unit
+        if (u >= n_units) break;
+        const uint32_t chunk = (u / nq) * stride;
+        const uint32_t slot = L.order[u % nq];
+        const BatchQuery &bq = L.queries[slot];
+        uint32_t lo, hi;
+        class_range(bq, L.cls, lo, hi);
+        const uint32_t first = max(lo, chunk * IPU), end = min(hi, (chunk + 1) * IPU);
+        if (first >= end) continue;
+        ScanParams p = bq.sp[PK];
+        p.boundary = L.bnd + (size_t)blockIdx.x * L.bnd_stride;
+        p.bnd_col0 = p.meta[first].col_off;
+        bool ok = true;
+        switch (bq.mode) {
+        case MODE_SW: ok = scan_unit<A, G, R, MODE_SW, false>(p, first, end, bufs, bars, phase); break;
+        case MODE_NW: ok = scan_unit<A, G, R, MODE_NW, false>(p, first, end, bufs, bars, phase); break;
+        case MODE_HW: ok = scan_unit<A, G, R, MODE_HW, false>(p, first, end, bufs, bars, phase); break;
+        case MODE_OV: ok = scan_unit<A, G, R, MODE_OV, false>(p, first, end, bufs, bars, phase); break;
+        default: ok = scan_unit<A, G, R, MODE_SHW, false>(p, first, end, bufs, bars, phase); break;
+        }
+        if (!ok) return;
+    }
+}
+
+// Query profiles of every (query slot, profile kind) the batch needs: blockIdx.y names the job.
+__global__ void batch_profile_kernel(const BatchQuery *queries, const BatchCtl *ctl) {
+    const uint32_t slot = blockIdx.y / PK_N;
+    const int kind = (int)(blockIdx.y % PK_N);
+    if (slot >= ctl->n_queries) return;
+    const BatchQuery &bq = queries[slot];
+    const ScanParams &sp = bq.sp[kind];
+    if (sp.profile == nullptr || sp.n_passes == 0) return;
+    const int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    uint8_t *out = const_cast<uint8_t *>(sp.profile);
+    const int32_t lim32 = 536870911;
+    switch (kind) {
+    case PK_BULK:
+        if (bq.bulk_rows == 8)
+            build_profile_words<Pair16, MAIN_G, 8>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                   sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        else if (bq.bulk_rows == 16)
+            build_profile_words<Pair16, MAIN_G, 16>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                    sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        else
+            build_profile_words<Pair16, MAIN_G, 32>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                    sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        break;
+    case PK_W16:
+        build_profile_words<Pair16, LCG, LCR>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                              sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        break;
+    case PK_I32:
+        build_profile_words<Single32, ICG, ICR>(bq.q, bq.matrix, bq.al, sp.go, lim32, bq.top_free,
+                                                sp.vrow0, sp.n_passes, (int32_t *)out, first, stride);
+        break;
+    default:
+        build_profile_words<Single32, WIN_G, WIN_R>(bq.q, bq.matrix, bq.al, sp.go, lim32, bq.top_free,
+                                                    sp.vrow0, sp.n_passes, (int32_t *)out, first, stride);
+        break;
+    }
+}
+
+// End positions of each ScoreEnd query's winner: block `slot` reruns the winner's item with
+// position tracking when the winner lives in this kernel's partition (int16x2 pair or int32 item).
+template <class A, int PK>
+__global__ void __launch_bounds__(1024) batch_band_kernel(const BandLaunch L) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    const uint32_t slot = blockIdx.x;
+    if (slot >= L.ctl->n_queries) return;
+    const BatchQuery &bq = L.queries[slot];
+    if (!bq.ends) return;
+    const ScanParams &sp0 = bq.sp[PK];
+    const unsigned long long key = *sp0.best_key;
+    if (key == 0) return;
+    const uint32_t idx = ~(uint32_t)(key & 0xffffffffu);
+    const uint32_t r = bq.rank[idx];
+    const bool packed = r / 2 >= bq.k0;
+    uint32_t item;
+    if (A::NH == 2) {
+        if (!packed) return;
+        item = r / 2;
+    } else {
+        if (packed) return;
+        item = r;
+    }
+    ScanParams p = sp0;
+    p.boundary = L.bnd + (size_t)slot * L.bnd_stride;
+    p.bnd_col0 = p.meta[item].col_off;
+    p.ends_out = L.ends + 3 * (size_t)slot;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    switch (bq.mode) {
+    case MODE_SW: band_item<A, WIN_R, MODE_SW>(p, item, smem + 128, bar, phase); break;
+    case MODE_NW: band_item<A, WIN_R, MODE_NW>(p, item, smem + 128, bar, phase); break;
+    case MODE_HW: band_item<A, WIN_R, MODE_HW>(p, item, smem + 128, bar, phase); break;
+    case MODE_OV: band_item<A, WIN_R, MODE_OV>(p, item, smem + 128, bar, phase); break;
+    default: band_item<A, WIN_R, MODE_SHW>(p, item, smem + 128, bar, phase); break;
+    }
+}
+
+__global__ void batch_finalize_kernel(const BatchQuery *queries, const BatchCtl *ctl,
+                                      const int32_t *ends, hy_hit *out) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= ctl->n_queries) return;
+    const BatchQuery &bq = queries[slot];
+    const unsigned long long k = *bq.sp[PK_BULK].best_key;
+    hy_hit h;
+    h.score = (int32_t)((uint32_t)(k >> 32) ^ 0x80000000u);
+    h.reserved = 0;
+    h.db_index = ~(uint32_t)(k & 0xffffffffu);
+    h.query_end = bq.ends ? (int64_t)ends[3 * (size_t)slot + 1] : -1;
+    h.target_end = bq.ends ? (int64_t)ends[3 * (size_t)slot + 2] : -1;
+    out[slot] = h;
+}
+
+}  // namespace hy
+
+// ---- host side ------------------------------------------------------------------------------
+
+struct BatchConfig {
+    int32_t rows8_max = 64;    // queries up to this length: 8 rows per lane
+    int32_t rows16_max = 192;  // up to this length: 16 rows per lane; longer: 32
+    uint32_t long_w = LONG_W;  // pairs wider than this run one warp each
+};
+
+struct hy_batch {
+    int device = 0;
+    std::vector<const hy_db *> dbs;
+    uint32_t max_queries = 0;
+    uint64_t max_q_res = 0;
+    int32_t al_max = 0;
+    uint64_t mql_max = 0, max_t = 0;
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    BatchQuery *d_queries = nullptr, *h_queries = nullptr;
+    BatchCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    uint32_t *d_order = nullptr, *h_order = nullptr;  // BC_N lists of max_queries slots
+    uint8_t *d_qres = nullptr, *h_qres = nullptr;
+    uint8_t *d_prof = nullptr;
+    size_t prof_per_query = 0;
+    uint8_t *d_bnd_bulk = nullptr, *d_bnd_side = nullptr, *d_bnd_band = nullptr;
+    size_t stride_bulk = 0, stride_side = 0, stride_band = 0;
+    unsigned long long *d_keys = nullptr;
+    int32_t *d_ends = nullptr;
+    hy_hit *d_hits = nullptr, *h_hits = nullptr;
+    int *d_err = nullptr, *h_err = nullptr;
+    int grid[BC_N] = {0, 0, 0, 0, 0};
+    size_t smem[BC_N] = {0, 0, 0, 0, 0};
+    int band_threads = 32;
+    size_t band_smem = 0;
+    cudaGraphExec_t exec = nullptr;
+    BatchConfig cfg;
+    bool autotune = true;
+    std::map<uint64_t, BatchConfig> tuned;  // batch shape signature -> configuration
+    uint64_t device_bytes = 0;
+    uint64_t runs = 0;
+    double last_tune_ms = 0.0;
+};
+
+namespace hy {
+
+#define HB_CK(call)                                                                  \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            cudaGetLastError();                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e_); \
+        }                                                                            \
+    } while (0)
+
+
+static size_t align128(size_t x) { return (x + 127) / 128 * 128; }
+
+static size_t pass_bytes_of(int32_t al, int rpp, size_t row_bytes) {
+    return (size_t)(al + 1) * rpp * row_bytes;
+}
+
+template <class A, int G, int R, int PK>
+static cudaError_t prepare_class(hy_batch *b, int cls, size_t smem, int n_sm) {
+    auto kern = batch_scan_kernel<A, G, R, PK>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
+    if (e != cudaSuccess) return e;
+    b->grid[cls] = std::max(1, per_sm) * n_sm;
+    b->smem[cls] = smem;
+    return cudaSuccess;
+}
+
+template <class A, int G, int R, int PK>
+static void launch_class(hy_batch *b, int cls, uint8_t *bnd, size_t stride, cudaStream_t st) {
+    ClassLaunch L;
+    L.queries = b->d_queries;
+    L.order = b->d_order + (size_t)cls * b->max_queries;
+    L.ctl = b->d_ctl;
+    L.cls = cls;
+    L.bnd = bnd;
+    L.bnd_stride = stride;
+    batch_scan_kernel<A, G, R, PK><<<b->grid[cls], 256, b->smem[cls], st>>>(L);
+}
+
+// Records the batch's device work on b->stream (under stream capture).
+static hy_status record_graph_body(hy_batch *b) {
+    HB_CK(cudaMemsetAsync(&b->d_ctl->head[0], 0, sizeof(uint32_t) * BC_N, b->stream));
+    HB_CK(cudaMemsetAsync(b->d_keys, 0, sizeof(unsigned long long) * b->max_queries, b->stream));
+    batch_profile_kernel<<<dim3(32, b->max_queries * PK_N), 256, 0, b->stream>>>(b->d_queries, b->d_ctl);
+    HB_CK(cudaGetLastError());
+    HB_CK(cudaEventRecord(b->ev_fork, b->stream));
+    HB_CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+    launch_class<Pair16, LCG, LCR, PK_W16>(b, BC_LONG, b->d_bnd_side, b->stride_side, b->side);
+    launch_class<Single32, ICG, ICR, PK_I32>(b, BC_I32, b->d_bnd_side, b->stride_side, b->side);
+    HB_CK(cudaGetLastError());
+    HB_CK(cudaEventRecord(b->ev_join, b->side));
+    launch_class<Pair16, MAIN_G, 32, PK_BULK>(b, BC_BULK32, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<Pair16, MAIN_G, 16, PK_BULK>(b, BC_BULK16, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<Pair16, MAIN_G, 8, PK_BULK>(b, BC_BULK8, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    HB_CK(cudaGetLastError());
+    HB_CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+    BandLaunch bl;
+    bl.queries = b->d_queries;
+    bl.ctl = b->d_ctl;
+    bl.bnd = b->d_bnd_band;
+    bl.bnd_stride = b->stride_band;
+    bl.ends = b->d_ends;
+    batch_band_kernel<Pair16, PK_W16><<<b->max_queries, b->band_threads, b->band_smem, b->stream>>>(bl);
+    batch_band_kernel<Single32, PK_W32><<<b->max_queries, b->band_threads, b->band_smem, b->stream>>>(bl);
+    batch_finalize_kernel<<<(b->max_queries + 127) / 128, 128, 0, b->stream>>>(b->d_queries, b->d_ctl,
+                                                                               b->d_ends, b->d_hits);
+    HB_CK(cudaGetLastError());
+    return fail(HY_OK);
+}
+
+static void free_batch(hy_batch *b) {
+    if (!b) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    void *dev[] = {b->d_queries, b->d_ctl, b->d_order, b->d_qres, b->d_prof, b->d_bnd_bulk,
+                   b->d_bnd_side, b->d_bnd_band, b->d_keys, b->d_ends, b->d_hits, b->d_err};
+    for (void *p : dev)
+        if (p) cudaFree(p);
+    void *host[] = {b->h_queries, b->h_ctl, b->h_order, b->h_qres, b->h_hits, b->h_err};
+    for (void *p : host)
+        if (p) cudaFreeHost(p);
+    cudaEvent_t evs[] = {b->ev_fork, b->ev_join, b->ev_t0, b->ev_t1};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->side) cudaStreamDestroy(b->side);
+    cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    delete b;
+}
+
+struct BatchDeviceGuard {
+    int prev = -1;
+    explicit BatchDeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+        cudaGetLastError();
+    }
+    ~BatchDeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+        cudaGetLastError();
+    }
+};
+
+// Validates the queries and writes the batch's descriptors into the pinned staging buffers.
+static hy_status stage_batch(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_t *q_res,
+                             const uint64_t *q_off, int32_t *const *d_scores, const BatchConfig &cfg,
+                             uint32_t chunk_stride, uint32_t *failed) {
+    if (n > b->max_queries) return fail(HY_ERR_INVALID_ARGUMENT, n, b->max_queries);
+    if (n > 0 && (!dbq || !q_off)) return fail(HY_ERR_INVALID_ARGUMENT);
+    const uint64_t total_res = n ? q_off[n] - q_off[0] : 0;
+    if (total_res > b->max_q_res) return fail(HY_ERR_INVALID_ARGUMENT, (int64_t)total_res, (int64_t)b->max_q_res);
+    if (total_res && !q_res) return fail(HY_ERR_INVALID_ARGUMENT);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (failed) *failed = i;
+        if (dbq[i] >= b->dbs.size()) return fail(HY_ERR_INVALID_ARGUMENT, dbq[i], (int64_t)b->dbs.size());
+        if (q_off[i + 1] < q_off[i]) return fail(HY_ERR_INVALID_ARGUMENT);
+        const hy_db *db = b->dbs[dbq[i]];
+        const uint64_t qlen = q_off[i + 1] - q_off[i];
+        if (qlen > db->mql) return fail(HY_ERR_QUERY_TOO_LONG, (int64_t)qlen, (int64_t)db->mql);
+        const uint8_t *q = q_res + (q_off[i] - q_off[0]);
+        for (uint64_t k = 0; k < qlen; ++k)
+            if (q[k] >= db->al) return fail(HY_ERR_SYMBOL_OUT_OF_RANGE, q[k], (int64_t)db->al);
+    }
+    if (failed) *failed = n;
+    if (total_res) memcpy(b->h_qres, q_res, total_res);
+    BatchCtl &ctl = *b->h_ctl;
+    memset(&ctl, 0, sizeof(ctl));
+    ctl.n_queries = n;
+    ctl.chunk_stride = std::max<uint32_t>(1, chunk_stride);
+    std::vector<std::vector<uint32_t>> lists(BC_N);
+    size_t prof_off = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const hy_db *db = b->dbs[dbq[i]];
+        const uint64_t qlen = q_off[i + 1] - q_off[i];
+        BatchQuery &bq = b->h_queries[i];
+        memset(&bq, 0, sizeof(bq));
+        const QuerySplit sp = split_for_query(db, qlen, cfg.long_w);
+        bq.matrix = db->d_matrix;
+        bq.q = b->d_qres + (q_off[i] - q_off[0]);
+        bq.rank = db->d_rank;
+        bq.qlen = (int32_t)qlen;
+        bq.mode = db->mode;
+        bq.ends = db->search_type == HY_SEARCH_SCORE_END ? 1 : 0;
+        bq.bulk_rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
+        bq.top_free = (db->mode == MODE_SW || db->mode == MODE_HW || db->mode == MODE_OV) ? 1 : 0;
+        bq.al = (int32_t)db->al;
+        bq.lim16 = 32767 - db->go;
+        bq.k0 = sp.k0;
+        bq.kl = sp.kl;
+        bq.n_i32 = sp.n_i32;
+        bq.n16 = db->p16.n_items;
+        const bool need[PK_N] = {sp.kl < db->p16.n_items, sp.kl > sp.k0 || bq.ends, sp.n_i32 > 0,
+                                 bq.ends && sp.n_i32 > 0};
+        const int rpp[PK_N] = {MAIN_G * bq.bulk_rows, LCG * LCR, ICG * ICR, WIN_G * WIN_R};
+        for (int k = 0; k < PK_N; ++k) {
+            ScanParams &p = bq.sp[k];
+            const bool i16 = k == PK_BULK || k == PK_W16;
+            const Partition &part = i16 ? db->p16 : db->p32;
+            p.meta = part.d_meta;
+            p.n_items = part.n_items;
+            p.res = part.d_res;
+            p.qlen = (int32_t)qlen;
+            p.go = db->go;
+            p.ge = db->ge;
+            p.sentinel = i16 ? (-32768 + db->ge) : (INT32_MIN / 4);
+            p.scores = d_scores ? d_scores[i] : nullptr;
+            p.best_key = b->d_keys + i;
+            p.err = b->d_err;
+            if (!need[k]) continue;
+            const QueryPlan qp = plan(qlen, rpp[k], db->al, i16 ? profile_row_bytes<Pair16>() : profile_row_bytes<Single32>());
+            p.pass_bytes = qp.pass_bytes;
+            p.n_passes = qp.n_passes;
+            p.vrow0 = qp.vrow0;
+            p.profile = b->d_prof + (size_t)i * b->prof_per_query + prof_off;
+            prof_off += align128((size_t)qp.pass_bytes * qp.n_passes);
+        }
+        prof_off = 0;
+        const int bulk_cls = bq.bulk_rows == 8 ? BC_BULK8 : bq.bulk_rows == 16 ? BC_BULK16 : BC_BULK32;
+        if (sp.kl < db->p16.n_items) {
+            lists[bulk_cls].push_back(i);
+            ctl.n_chunks[bulk_cls] = std::max<uint32_t>(ctl.n_chunks[bulk_cls], (db->p16.n_items + 31) / 32);
+        }
+        if (sp.kl > sp.k0) {
+            lists[BC_LONG].push_back(i);
+            ctl.n_chunks[BC_LONG] = std::max<uint32_t>(ctl.n_chunks[BC_LONG], (sp.kl + 7) / 8);
+        }
+        if (sp.n_i32 > 0) {
+            lists[BC_I32].push_back(i);
+            ctl.n_chunks[BC_I32] = std::max<uint32_t>(ctl.n_chunks[BC_I32], (sp.n_i32 + 7) / 8);
+        }
+    }
+    for (int c = 0; c < BC_N; ++c) {
+        std::vector<uint32_t> &l = lists[c];
+        std::stable_sort(l.begin(), l.end(), [&](uint32_t x, uint32_t y) {
+            return b->h_queries[x].qlen > b->h_queries[y].qlen;
+        });
+        ctl.count[c] = (uint32_t)l.size();
+        std::copy(l.begin(), l.end(), b->h_order + (size_t)c * b->max_queries);
+    }
+    return fail(HY_OK);
+}
+
+// Copies the staged batch to the device and replays the graph (asynchronous on b->stream).
+static hy_status launch_staged(hy_batch *b, uint32_t n, uint64_t total_res) {
+    if (total_res) HB_CK(cudaMemcpyAsync(b->d_qres, b->h_qres, total_res, cudaMemcpyHostToDevice, b->stream));
+    if (n) HB_CK(cudaMemcpyAsync(b->d_queries, b->h_queries, sizeof(BatchQuery) * n, cudaMemcpyHostToDevice, b->stream));
+    HB_CK(cudaMemcpyAsync(b->d_order, b->h_order, sizeof(uint32_t) * BC_N * b->max_queries,
+                          cudaMemcpyHostToDevice, b->stream));
+    HB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
+    HB_CK(cudaGraphLaunch(b->exec, b->stream));
+    ++b->runs;
+    return fail(HY_OK);
+}
+
+static hy_status finish_run(hy_batch *b, uint32_t n, hy_hit *out) {
+    if (n && out) HB_CK(cudaMemcpyAsync(b->h_hits, b->d_hits, sizeof(hy_hit) * n, cudaMemcpyDeviceToHost, b->stream));
+    HB_CK(cudaMemcpyAsync(b->h_err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    HB_CK(cudaStreamSynchronize(b->stream));
+    if (*b->h_err) {
+        *b->h_err = 0;
+        HB_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
+        HB_CK(cudaStreamSynchronize(b->stream));
+        return fail(HY_ERR_TIMEOUT);
+    }
+    if (n && out) memcpy(out, b->h_hits, sizeof(hy_hit) * n);
+    return fail(HY_OK);
+}
+
+// Shape signature of a batch: the share of queries in each (mode, log2 length) bucket, in
+// eighths, plus the databases used.
+static uint64_t batch_signature(const hy_batch *b, uint32_t n, const uint32_t *dbq, const uint64_t *q_off) {
+    std::vector<uint32_t> hist(5 * 24, 0);
+    std::vector<char> used(b->dbs.size(), 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint64_t qlen = q_off[i + 1] - q_off[i];
+        int lg = 0;
+        while (lg < 23 && (1ull << (lg + 1)) <= qlen + 1) ++lg;
+        ++hist[b->dbs[dbq[i]]->mode * 24 + lg];
+        used[dbq[i]] = 1;
+    }
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+    for (uint32_t c : hist) mix(n ? (uint64_t)std::lround(8.0 * c / n) : 0);
+    for (char u : used) mix((uint64_t)u);
+    return h;
+}
+
+// Times one configuration on a sampled part of the batch (every `stride`-th item chunk).
+static hy_status time_config(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_t *q_res,
+                             const uint64_t *q_off, const BatchConfig &cfg, uint32_t stride, float *ms) {
+    hy_status st = stage_batch(b, n, dbq, q_res, q_off, nullptr, cfg, stride, nullptr);
+    if (st != HY_OK) return st;
+    HB_CK(cudaEventRecord(b->ev_t0, b->stream));
+    st = launch_staged(b, n, n ? q_off[n] - q_off[0] : 0);
+    if (st != HY_OK) return st;
+    HB_CK(cudaEventRecord(b->ev_t1, b->stream));
+    st = finish_run(b, 0, nullptr);
+    if (st != HY_OK) return st;
+    HB_CK(cudaEventElapsedTime(ms, b->ev_t0, b->ev_t1));
+    return fail(HY_OK);
+}
+
+static hy_status tune(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_t *q_res,
+                      const uint64_t *q_off, uint32_t stride, BatchConfig *best_cfg, double *best_ms) {
+    static const int32_t rows_c[][2] = {{64, 192}, {0, 256}, {128, 512}, {0, 0}, {64, 64}, {32, 128}};
+    static const uint32_t long_c[] = {1024, 2048, 4096};
+    BatchConfig best = b->cfg;
+    float best_t = 1e30f;
+    for (const auto &rc : rows_c) {
+        BatchConfig c;
+        c.rows8_max = rc[0];
+        c.rows16_max = rc[1];
+        c.long_w = LONG_W;
+        float t = 0;
+        hy_status st = time_config(b, n, dbq, q_res, q_off, c, stride, &t);
+        if (st != HY_OK) return st;
+        if (t < best_t) {
+            best_t = t;
+            best = c;
+        }
+    }
+    for (uint32_t lw : long_c) {
+        if (lw == LONG_W) continue;
+        BatchConfig c = best;
+        c.long_w = lw;
+        float t = 0;
+        hy_status st = time_config(b, n, dbq, q_res, q_off, c, stride, &t);
+        if (st != HY_OK) return st;
+        if (t < best_t) {
+            best_t = t;
+            best = c;
+        }
+    }
+    *best_cfg = best;
+    if (best_ms) *best_ms = best_t;
+    return fail(HY_OK);
+}
+
+// The sampling stride that leaves about 256 bulk chunks per query in a tuning run.
+static uint32_t sample_stride(const hy_batch *b) {
+    uint32_t n16 = 0;
+    for (const hy_db *db : b->dbs) n16 = std::max(n16, db->p16.n_items);
+    return std::max<uint32_t>(1, (n16 + 31) / 32 / 256);
+}
+
+}  // namespace hy
+
+extern "C" {
+
+hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_queries,
+                          int autotune, hy_batch **out) {
+    if (!dbs || n_dbs == 0 || max_queries == 0 || !out) return fail(HY_ERR_INVALID_ARGUMENT);
+    *out = nullptr;
+    for (uint32_t i = 0; i < n_dbs; ++i) {
+        if (!dbs[i]) return fail(HY_ERR_INVALID_ARGUMENT);
+        if (dbs[i]->device != dbs[0]->device) return fail(HY_ERR_INVALID_ARGUMENT, i);
+    }
+    if (max_queries > 16000) return fail(HY_ERR_INVALID_ARGUMENT, max_queries, 16000);
+    hy_batch *b = new hy_batch();
+    b->device = dbs[0]->device;
+    b->dbs.assign(dbs, dbs + n_dbs);
+    b->max_queries = max_queries;
+    b->autotune = autotune != 0;
+    for (const hy_db *db : b->dbs) {
+        b->al_max = std::max<int32_t>(b->al_max, (int32_t)db->al);
+        b->mql_max = std::max(b->mql_max, db->mql);
+        b->max_t = std::max(b->max_t, db->max_t);
+    }
+    b->max_q_res = std::max<uint64_t>(1, (uint64_t)max_queries * b->mql_max);
+    BatchDeviceGuard guard(b->device);
+    hy_status st = HY_OK;
+    auto ck = [&](cudaError_t e) {
+        if (st == HY_OK && e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(e == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e);
+        }
+    };
+    int n_sm = 0, smem_optin = 0;
+    ck(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, b->device));
+    ck(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
+    const int32_t al = b->al_max;
+    const size_t pb16 = profile_row_bytes<Pair16>(), pb32 = profile_row_bytes<Single32>();
+    const size_t sm_bulk32 = 128 + 2 * pass_bytes_of(al, MAIN_G * 32, pb16);
+    const size_t sm_bulk16 = 128 + 2 * pass_bytes_of(al, MAIN_G * 16, pb16);
+    const size_t sm_bulk8 = 128 + 2 * pass_bytes_of(al, MAIN_G * 8, pb16);
+    const size_t sm_long = 128 + 2 * pass_bytes_of(al, LCG * LCR, pb16);
+    const size_t sm_i32 = 128 + 2 * pass_bytes_of(al, ICG * ICR, pb32);
+    const size_t band_pass = std::max(pass_bytes_of(al, WIN_G * WIN_R, pb16), pass_bytes_of(al, WIN_G * WIN_R, pb32));
+    if (st == HY_OK && (std::max({sm_bulk32, sm_long, sm_i32}) > (size_t)smem_optin ||
+                        128 + band_pass > (size_t)smem_optin)) {
+        st = fail(HY_ERR_UNSUPPORTED, al, smem_optin);
+    }
+    if (st == HY_OK) {
+        ck(prepare_class<Pair16, MAIN_G, 8, PK_BULK>(b, BC_BULK8, sm_bulk8, n_sm));
+        ck(prepare_class<Pair16, MAIN_G, 16, PK_BULK>(b, BC_BULK16, sm_bulk16, n_sm));
+        ck(prepare_class<Pair16, MAIN_G, 32, PK_BULK>(b, BC_BULK32, sm_bulk32, n_sm));
+        ck(prepare_class<Pair16, LCG, LCR, PK_W16>(b, BC_LONG, sm_long, n_sm));
+        ck(prepare_class<Single32, ICG, ICR, PK_I32>(b, BC_I32, sm_i32, n_sm));
+        int warps = (int)std::min<size_t>(32, BAND_SMEM_BUDGET / std::max<size_t>(band_pass, 1));
+        warps = std::max(1, warps);
+        b->band_threads = 32 * warps;
+        b->band_smem = 128 + (size_t)warps * band_pass;
+        ck(cudaFuncSetAttribute(batch_band_kernel<Pair16, PK_W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->band_smem));
+        ck(cudaFuncSetAttribute(batch_band_kernel<Single32, PK_W32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->band_smem));
+    }
+    // Boundary regions: a block's unit spans at most IPU items of the class's widest width.
+    const bool multipass = b->mql_max > (uint64_t)MAIN_G * 8;
+    const uint64_t w_bulk = std::min<uint64_t>(b->max_t, LONG_W_MAX) + 16;
+    b->stride_bulk = multipass ? align128(32 * w_bulk * 2 * sizeof(uint32_t)) : 128;
+    b->stride_side = multipass ? align128(8 * (b->max_t + 16) * 2 * sizeof(uint32_t)) : 128;
+    b->stride_band = align128((b->max_t + 16) * 2 * sizeof(uint32_t));
+    const int side_grid = std::max(b->grid[BC_LONG], b->grid[BC_I32]);
+    const int bulk_grid = std::max({b->grid[BC_BULK8], b->grid[BC_BULK16], b->grid[BC_BULK32]});
+    const uint64_t mq = b->mql_max;
+    b->prof_per_query = align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +   // bulk, any rows
+                        align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +   // long / band int16x2
+                        align128(pass_bytes_of(al, 1, pb32) * (mq + 511)) +   // int32
+                        align128(pass_bytes_of(al, 1, pb32) * (mq + 255)) + 512;  // band int32
+    if (st == HY_OK) {
+        ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        ck(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+        ck(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        ck(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+        ck(cudaEventCreate(&b->ev_t0));
+        ck(cudaEventCreate(&b->ev_t1));
+        auto dalloc = [&](void **p, size_t bytes) {
+            ck(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+            if (st == HY_OK) b->device_bytes += bytes;
+        };
+        dalloc((void **)&b->d_queries, sizeof(BatchQuery) * max_queries);
+        dalloc((void **)&b->d_ctl, sizeof(BatchCtl));
+        dalloc((void **)&b->d_order, sizeof(uint32_t) * BC_N * max_queries);
+        dalloc((void **)&b->d_qres, b->max_q_res);
+        dalloc((void **)&b->d_prof, b->prof_per_query * max_queries);
+        dalloc((void **)&b->d_bnd_bulk, b->stride_bulk * bulk_grid);
+        dalloc((void **)&b->d_bnd_side, b->stride_side * side_grid);
+        dalloc((void **)&b->d_bnd_band, b->stride_band * max_queries);
+        dalloc((void **)&b->d_keys, sizeof(unsigned long long) * max_queries);
+        dalloc((void **)&b->d_ends, 3 * sizeof(int32_t) * max_queries);
+        dalloc((void **)&b->d_hits, sizeof(hy_hit) * max_queries);
+        dalloc((void **)&b->d_err, 64);
+        ck(cudaMallocHost((void **)&b->h_queries, sizeof(BatchQuery) * max_queries));
+        ck(cudaMallocHost((void **)&b->h_ctl, sizeof(BatchCtl)));
+        ck(cudaMallocHost((void **)&b->h_order, sizeof(uint32_t) * BC_N * max_queries));
+        ck(cudaMallocHost((void **)&b->h_qres, b->max_q_res));
+        ck(cudaMallocHost((void **)&b->h_hits, sizeof(hy_hit) * max_queries));
+        ck(cudaMallocHost((void **)&b->h_err, sizeof(int)));
+    }
+    if (st == HY_OK) {
+        ck(cudaMemset(b->d_err, 0, 64));
+        ck(cudaMemset(b->d_ctl, 0, sizeof(BatchCtl)));
+        *b->h_err = 0;
+    }
+    if (st == HY_OK) {
+        cudaGraph_t graph = nullptr;
+        ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        if (st == HY_OK) {
+            hy_status rs = record_graph_body(b);
+            cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+            if (rs != HY_OK && st == HY_OK) st = rs;
+            ck(e);
+        }
+        if (st == HY_OK) ck(cudaGraphInstantiate(&b->exec, graph, 0));
+        if (graph) cudaGraphDestroy(graph);
+    }
+    if (st != HY_OK) {
+        int64_t d[3];
+        hy_last_error_detail(d);
+        free_batch(b);
+        return fail(st, d[0], d[1], d[2]);
+    }
+    *out = b;
+    return fail(HY_OK);
+}
+
+void hy_batch_destroy(hy_batch *b) { free_batch(b); }
+
+uint64_t hy_batch_device_bytes(const hy_batch *b) { return b ? b->device_bytes : 0; }
+
+void *hy_batch_stream(hy_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+hy_status hy_batch_get_config(const hy_batch *b, int32_t cfg[3]) {
+    if (!b || !cfg) return fail(HY_ERR_INVALID_ARGUMENT);
+    cfg[0] = b->cfg.rows8_max;
+    cfg[1] = b->cfg.rows16_max;
+    cfg[2] = (int32_t)b->cfg.long_w;
+    return fail(HY_OK);
+}
+
+hy_status hy_batch_set_config(hy_batch *b, const int32_t cfg[3]) {
+    if (!b || !cfg || cfg[2] < 1 || (uint32_t)cfg[2] > LONG_W_MAX) return fail(HY_ERR_INVALID_ARGUMENT);
+    b->cfg.rows8_max = cfg[0];
+    b->cfg.rows16_max = cfg[1];
+    b->cfg.long_w = (uint32_t)cfg[2];
+    b->autotune = false;
+    return fail(HY_OK);
+}
+
+hy_status hy_batch_tune(hy_batch *b, uint32_t n_queries, const uint32_t *db_of_query,
+                        const uint8_t *q_res, const uint64_t *q_off, uint32_t stride, double *best_ms) {
+    if (!b) return fail(HY_ERR_INVALID_ARGUMENT);
+    BatchDeviceGuard guard(b->device);
+    if (stride == 0) stride = sample_stride(b);
+    BatchConfig best;
+    hy_status st = tune(b, n_queries, db_of_query, q_res, q_off, stride, &best, best_ms);
+    if (st != HY_OK) return st;
+    b->cfg = best;
+    if (n_queries) b->tuned[batch_signature(b, n_queries, db_of_query, q_off)] = best;
+    return fail(HY_OK);
+}
+
+hy_status hy_scan_batch(hy_batch *b, uint32_t n_queries, const uint32_t *db_of_query,
+                        const uint8_t *q_res, const uint64_t *q_off, hy_hit *out,
+                        uint32_t *failed_query) {
+    if (!b || (n_queries && !out)) return fail(HY_ERR_INVALID_ARGUMENT);
+    BatchDeviceGuard guard(b->device);
+    // Validate before any tuning so that errors are reported for the caller's batch as given.
+    hy_status st = stage_batch(b, n_queries, db_of_query, q_res, q_off, nullptr, b->cfg, 1, failed_query);
+    if (st != HY_OK) return st;
+    if (b->autotune && n_queries) {
+        const uint64_t sig = batch_signature(b, n_queries, db_of_query, q_off);
+        auto it = b->tuned.find(sig);
+        if (it == b->tuned.end()) {
+            double ms = 0;
+            BatchConfig best;
+            st = tune(b, n_queries, db_of_query, q_res, q_off, sample_stride(b), &best, &ms);
+            if (st != HY_OK) return st;
+            b->tuned[sig] = best;
+            b->last_tune_ms = ms;
+            b->cfg = best;
+        } else {
+            b->cfg = it->second;
+        }
+        st = stage_batch(b, n_queries, db_of_query, q_res, q_off, nullptr, b->cfg, 1, failed_query);
+        if (st != HY_OK) return st;
+    }
+    st = launch_staged(b, n_queries, n_queries ? q_off[n_queries] - q_off[0] : 0);
+    if (st != HY_OK) return st;
+    return finish_run(b, n_queries, out);
+}
+
+}  // extern "C"

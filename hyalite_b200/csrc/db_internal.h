@@ -88,7 +88,7 @@ struct QuerySplit {
     uint32_t n_i32 = 0;   // int32 items [0, n_i32)
 };
 
-inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen) {
+inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen, uint32_t long_w = LONG_W) {
     QuerySplit q;
     // Longest target length t whose bound for this query keeps the int16 kernel exact.
     auto fits = [&](uint64_t n) {
@@ -120,7 +120,7 @@ inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen) {
     b = (uint32_t)db->pair_w.size();
     while (a < b) {
         uint32_t mid = a + (b - a) / 2;
-        if (db->pair_w[mid] <= LONG_W) b = mid; else a = mid + 1;
+        if (db->pair_w[mid] <= long_w) b = mid; else a = mid + 1;
     }
     q.kl = a;
     return q;

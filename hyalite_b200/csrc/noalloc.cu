@@ -109,7 +109,7 @@ hy_status run_partition(const hy_db *db, const Partition &part, uint32_t item_ba
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return fail(HY_ERR_CUDA, e);
     }
-    ScanParams p;
+    ScanParams p{};
     p.meta = part.d_meta;
     p.item_base = item_base;
     p.n_items = item_end;

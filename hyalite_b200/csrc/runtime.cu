@@ -119,7 +119,7 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
     QueryPlan qp = plan(qlen, G * R, db->al, profile_row_bytes<A>());
     HY_CK((launch_profile<A, G, R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof, st_)));
     sc->launches += qp.n_passes > 0 ? 2 : 1;
-    ScanParams p;
+    ScanParams p{};
     p.meta = part.d_meta;
     p.item_base = item_base;
     p.n_items = item_end;
@@ -246,7 +246,7 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     QueryPlan qp = plan(qlen, WIN_G * WIN_R, db->al, profile_row_bytes<A>());
     HY_CK((launch_profile<A, WIN_G, WIN_R>(db, d_query, qlen, qp, i16 ? lim16(db) : LIM32, prof,
                                             sc->stream)));
-    ScanParams p;
+    ScanParams p{};
     p.meta = part.d_meta;
     p.item_base = 0;
     p.n_items = item_end;

@@ -71,12 +71,16 @@ struct ScanParams {
     int32_t qlen;
     int32_t go, ge;
     int32_t sentinel;
-    void *boundary;  // 2 values (G, F) per column
-    int32_t *scores;
+    void *boundary;     // 2 values (G, F) per column, starting at column bnd_col0
+    uint64_t bnd_col0;  // first column the boundary region covers
+    int32_t *scores;    // per-target outputs by global index (may be null: best key only)
     int32_t *qend;
     int32_t *tend;
     unsigned long long *best_key;
     int *err;
+    // Band recovery only: when set, the winner named by *best_key is written here as {score,
+    // query end, target end} instead of to scores / qend / tend.
+    int32_t *ends_out;
 };
 
 // ---- lane arithmetic -----------------------------------------------------------------------
@@ -515,7 +519,7 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
             } else if (better(cand[h], c)) {
                 c = cand[h];
             }
-            scores[idx] = c.s;
+            if (scores) scores[idx] = c.s;
             if (ENDS) {
                 qend[idx] = c.row - 1;
                 tend[idx] = c.col - 1;
@@ -538,39 +542,47 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
 //
 // All groups of a block step through the passes together: the pass's query profile is one
 // contiguous slice, brought into shared memory by a TMA bulk copy while the previous pass runs.
+
+// Initialise the block's two profile mbarriers (thread 0; the caller synchronises the block).
+__device__ __forceinline__ void init_profile_bars(uint64_t *bars) {
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+}
+
+// One unit of work for one block: group g of the block runs item `item_first + g` if that is
+// below `item_end`, through every pass of the query in `p`. The block's two profile buffers and
+// mbarriers live in `smem` / `bars`; `phase` holds the parity each barrier waits for next (bit b
+// for barrier b) and is carried from unit to unit by a persistent caller. Every thread of the
+// block must call it with the same arguments. Returns false if a profile copy did not arrive in
+// time (the error flag is then set and the block must stop).
 template <class A, int G, int R, int MODE, bool ENDS>
-__global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
+__device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t item_first,
+                                          const uint32_t item_end, uint8_t *smem, uint64_t *bars,
+                                          uint32_t &phase) {
     typedef typename A::V V;
     constexpr int RPP = G * R;
     static_assert(R % A::EPV == 0, "rows per lane must fill whole profile vectors");
     static_assert(32 % G == 0, "groups must tile a warp");
-
-    extern __shared__ __align__(128) uint8_t smem[];
     uint8_t *prof_buf[2] = {smem, smem + p.pass_bytes};
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)p.pass_bytes);
 
     const int lane = threadIdx.x % G;
-    const int gpb = blockDim.x / G;
-    uint32_t item;
-    if (p.item_ptr) {
-        const uint32_t want = *p.item_ptr;
-        item = (blockIdx.x == 0 && threadIdx.x / G == 0) ? want : NO_INDEX;
-    } else {
-        item = p.item_base + blockIdx.x * gpb + threadIdx.x / G;
-    }
-    const bool active = item != NO_INDEX && item < p.n_items;
+    const uint32_t item = item_first == NO_INDEX ? NO_INDEX : item_first + threadIdx.x / G;
+    const bool active = item != NO_INDEX && item < item_end;
     ItemMeta meta;
     if (active) {
         meta = p.meta[item];
     } else {
-        meta.col_off = 0;
+        meta.col_off = p.bnd_col0;
         meta.w = 0;
         meta.n[0] = meta.n[1] = 0;
         meta.idx[0] = meta.idx[1] = NO_INDEX;
     }
     const V Sv = A::splat(p.sentinel);
     const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
-    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
+    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * (meta.col_off - p.bnd_col0);
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
     const int w_min = (int)__reduce_min_sync(0xffffffffu, meta.w);
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
@@ -578,24 +590,17 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
     V best = A::splat(0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
 
-    if (p.n_passes > 0) {
-        if (threadIdx.x == 0) {
-            mbar_init(&bars[0], 1);
-            mbar_init(&bars[1], 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            bulk_load(prof_buf[0], p.profile, p.pass_bytes, &bars[0]);
-            if (p.n_passes > 1) bulk_load(prof_buf[1], p.profile + p.pass_bytes, p.pass_bytes, &bars[1]);
-        }
+    if (threadIdx.x == 0 && p.n_passes > 0) {
+        bulk_load(prof_buf[0], p.profile, p.pass_bytes, &bars[0]);
+        if (p.n_passes > 1) bulk_load(prof_buf[1], p.profile + p.pass_bytes, p.pass_bytes, &bars[1]);
     }
     for (int pass = 0; pass < p.n_passes; ++pass) {
         const int buf = pass & 1;
-        const bool ok = mbar_wait_bounded(&bars[buf], (uint32_t)((pass >> 1) & 1));
+        const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u);
+        phase ^= 1u << buf;
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicExch(p.err, 1);
-            return;
+            return false;
         }
         sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof_buf[buf],
                                         prof_buf[buf] + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
@@ -609,6 +614,28 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
     }
     finish_item<A, G, MODE, ENDS>(lane, active, meta, p.qlen, p.go, p.ge, best, cand, p.scores,
                                   p.qend, p.tend, p.best_key);
+    return true;
+}
+
+template <class A, int G, int R, int MODE, bool ENDS>
+__global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)p.pass_bytes);
+    const int gpb = blockDim.x / G;
+    uint32_t first, end;
+    if (p.item_ptr) {
+        // One item, run by group 0 of block 0.
+        const uint32_t want = *p.item_ptr;
+        first = blockIdx.x == 0 ? want : NO_INDEX;
+        end = (first == NO_INDEX || first >= p.n_items) ? first : first + 1;
+    } else {
+        first = p.item_base + blockIdx.x * gpb;
+        end = p.n_items;
+    }
+    init_profile_bars(bars);
+    __syncthreads();
+    uint32_t phase = 0;
+    scan_unit<A, G, R, MODE, ENDS>(p, first, end, smem, bars, phase);
 }
 
 // ---- the block-cooperative band kernel (one long item, with end positions) -------------------
@@ -621,31 +648,26 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
 // BAND_K steps before the read). The round's profile slices are staged by one TMA bulk copy.
 constexpr int BAND_K = 32;
 
+// The band recovery of item `item` (a valid item of p.meta) by the whole block. `bar` is an
+// initialised mbarrier whose next wait parity is `phase`; the block's dynamic shared memory
+// (`smem`) holds W = blockDim/32 pass slices. Every thread of the block must call it.
 template <class A, int R, int MODE>
-__global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
+__device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t item, uint8_t *smem,
+                                          uint64_t *bar, uint32_t &phase) {
     typedef typename A::V V;
     constexpr int G = 32;
     constexpr int RPP = G * R;
     static_assert(BAND_K >= G, "the lag must cover the lane skew of a warp");
     static_assert(R % A::EPV == 0, "rows per lane must fill whole profile vectors");
-    extern __shared__ __align__(128) uint8_t smem[];
     const int W = blockDim.x / G;
     const int warp = threadIdx.x / G, lane = threadIdx.x % G;
-    const uint32_t item = *p.item_ptr;
-    if (item == NO_INDEX || item >= p.n_items) return;  // the same for every thread of the block
     const ItemMeta meta = p.meta[item];
     const int32_t w = (int32_t)meta.w;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)W * p.pass_bytes);
     const V Sv = A::splat(p.sentinel);
     const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
-    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * meta.col_off;
+    V *bnd = reinterpret_cast<V *>(p.boundary) + 2 * (meta.col_off - p.bnd_col0);
     V best = A::splat(0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
     const int pass_steps = w + G - 1;
     const int rounds = (p.n_passes + W - 1) / W;
     for (int round = 0; round < rounds; ++round) {
@@ -653,7 +675,8 @@ __global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
         const int cnt = min(W, p.n_passes - first);
         if (threadIdx.x == 0)
             bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
-        const bool ok = mbar_wait_bounded(bar, (uint32_t)(round & 1));
+        const bool ok = mbar_wait_bounded(bar, phase & 1u);
+        phase ^= 1u;
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicExch(p.err, 1);
             return;
@@ -680,6 +703,7 @@ __global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
     }
     // Reduce every lane's candidates: inside each warp, then across warps in shared memory.
     __shared__ Cand s_cand[32][2];
+    __syncthreads();  // a previous item's reduction may still be reading s_cand
 #pragma unroll
     for (int h = 0; h < A::NH; ++h) {
 #pragma unroll
@@ -700,11 +724,35 @@ __global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
             Cand c = border_seed<MODE>(p.qlen, (int32_t)meta.n[h], p.go, p.ge);
             for (int k = 0; k < W; ++k)
                 if (better(s_cand[k][h], c)) c = s_cand[k][h];
-            p.scores[idx] = c.s;
-            p.qend[idx] = c.row - 1;
-            p.tend[idx] = c.col - 1;
+            if (p.ends_out) {
+                if (idx == ~(uint32_t)(*p.best_key & 0xffffffffu)) {
+                    p.ends_out[0] = c.s;
+                    p.ends_out[1] = c.row - 1;
+                    p.ends_out[2] = c.col - 1;
+                }
+            } else {
+                p.scores[idx] = c.s;
+                p.qend[idx] = c.row - 1;
+                p.tend[idx] = c.col - 1;
+            }
         }
     }
+}
+
+template <class A, int R, int MODE>
+__global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    const uint32_t item = *p.item_ptr;
+    if (item == NO_INDEX || item >= p.n_items) return;  // the same for every thread of the block
+    const int W = blockDim.x / 32;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)W * p.pass_bytes);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    band_item<A, R, MODE>(p, item, smem, bar, phase);
 }
 
 // ---- the batched pairwise kernel (align_pairs) -----------------------------------------------
@@ -830,17 +878,19 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
 // padding symbol. Values are P = clamp(sub, -(lim+1), lim) + go; virtual rows (<= 0) get go (free
 // top border) or 0 (penalised top border); the padding symbol gets -(lim+1) + go. For int16x2 the
 // first table holds each value in the low half of its word, the second in the high half.
+// Words [first, total) in steps of `stride` of the profile described above.
 template <class A, int G, int R>
-__global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32_t *matrix,
-                                     int32_t al, int32_t go, int32_t lim, int top_free,
-                                     int32_t vrow0, int32_t n_passes, typename A::PE *out) {
+__device__ __forceinline__ void build_profile_words(const uint8_t *q, const int32_t *matrix,
+                                                    int32_t al, int32_t go, int32_t lim,
+                                                    int top_free, int32_t vrow0, int32_t n_passes,
+                                                    typename A::PE *out, int64_t first,
+                                                    int64_t stride) {
     static_assert(R % A::EPV == 0 && R >= A::EPV, "rows per lane must fill whole profile vectors");
     constexpr int KCH = R / A::EPV;
     const int64_t per_table = (int64_t)(al + 1) * G * R;
     const int64_t per_pass = per_table * A::TABLES;
     const int64_t total = per_pass * n_passes;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = first; i < total; i += stride) {
         const int64_t pass = i / per_pass;
         const int table = (int)((i % per_pass) / per_table);
         int64_t rem = i % per_table;
@@ -865,6 +915,16 @@ __global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32
         }
         out[i] = A::word(v, table);
     }
+}
+
+template <class A, int G, int R>
+__global__ void build_profile_kernel(const uint8_t *q, int32_t qlen, const int32_t *matrix,
+                                     int32_t al, int32_t go, int32_t lim, int top_free,
+                                     int32_t vrow0, int32_t n_passes, typename A::PE *out) {
+    (void)qlen;
+    build_profile_words<A, G, R>(q, matrix, al, go, lim, top_free, vrow0, n_passes, out,
+                                 blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
+                                 (int64_t)gridDim.x * blockDim.x);
 }
 
 }  // namespace hy

@@ -196,6 +196,44 @@ hy_status hy_scratch_profile_read(hy_scratch *scratch, double kernel_ms[3], uint
  * register resident on every SM, in DP cells per second. */
 hy_status hy_measure_dpx_peak(double *cells_per_second);
 
+/* ---- batched scan (no reference counterpart: the reference scans one query per call) ---------- */
+
+/* A batch runner over a fixed set of databases on one device. hy_scan_batch computes, for many
+ * queries at once, exactly what hy_scan returns for each (same score, db_index and ends), with
+ * every query against its own database (any mode and search type). The device work is persistent
+ * kernels over a work queue (chunks of length-sorted targets x queries, largest first), one
+ * recovery of the winner's ends per ScoreEnd query, all captured once into a CUDA graph that
+ * every call replays. max_queries bounds the queries of one call (at most 16000); query
+ * residues of one call are bounded by max_queries x the largest max_query_len. With autotune
+ * set, the first call of each batch shape (the mix of modes and query lengths) first times
+ * candidate launch configurations on a sampled part of the batch and keeps the fastest.
+ * Returns HY_ERR_UNSUPPORTED when the largest alphabet's query profiles do not fit in shared
+ * memory. The databases must outlive the batch. One host thread at a time per batch. */
+typedef struct hy_batch hy_batch;
+hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_queries,
+                          int autotune, hy_batch **out);
+void hy_batch_destroy(hy_batch *batch);
+/* Query i is q_res[q_off[i] - q_off[0] .. q_off[i+1] - q_off[0]) against dbs[db_of_query[i]];
+ * out[i] receives its BestHit. Queries are validated in order like hy_scan's (length, then
+ * symbols); on the first failing query the call returns its error, writes its index to
+ * *failed_query (if not NULL) and runs nothing. Blocks until the hits are in `out`. */
+hy_status hy_scan_batch(hy_batch *batch, uint32_t n_queries, const uint32_t *db_of_query,
+                        const uint8_t *q_res, const uint64_t *q_off, hy_hit *out,
+                        uint32_t *failed_query);
+/* Runs the autotuner on this batch now (every `stride`-th item chunk; 0 picks a stride leaving
+ * about 256 chunks) and keeps the fastest configuration; *best_ms is its sampled time. */
+hy_status hy_batch_tune(hy_batch *batch, uint32_t n_queries, const uint32_t *db_of_query,
+                        const uint8_t *q_res, const uint64_t *q_off, uint32_t stride,
+                        double *best_ms);
+/* The launch configuration in use: {largest query length run with 8 rows per lane, largest with
+ * 16 rows (longer: 32), the pair width above which a pair runs one warp each}. Setting one turns
+ * autotuning off; the width must be 1..4096. */
+hy_status hy_batch_get_config(const hy_batch *batch, int32_t cfg[3]);
+hy_status hy_batch_set_config(hy_batch *batch, const int32_t cfg[3]);
+uint64_t hy_batch_device_bytes(const hy_batch *batch);
+/* The batch's cudaStream_t, as an opaque pointer. */
+void *hy_batch_stream(hy_batch *batch);
+
 /* ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------- */
 
 /* align_pairs: pair p is (q_res[q_off[p]..q_off[p+1]], t_res[t_off[p]..t_off[p+1]]). Each pair is
