@@ -541,6 +541,87 @@ class Batch:
         return int(lib.hy_batch_stream(self._h) or 0)
 
 
+# ---- served scan (no reference counterpart) -----------------------------------------------------------------
+
+class ServerRequest:
+    """A submitted request: its id and, for a scores request, the array the scores land in."""
+
+    def __init__(self, rid: int, db: int, scores: Optional[np.ndarray]):
+        self.id = rid
+        self.db = db
+        self.scores = scores
+
+
+class Server:
+    """A request loop over a fixed list of databases (hy_server): requests are admitted by memory
+    into device batches, several batches run at once, and each result equals the plain call's."""
+
+    def __init__(self, dbs: Sequence[Database], max_batch: int = 64, in_flight: int = 2,
+                 max_pending: int = 4096, profile_budget: int = 0, scores_budget: int = 0,
+                 launch_config=None):
+        dbs = list(dbs)
+        arr = (C.c_void_p * len(dbs))(*[d._h.value for d in dbs])
+        cfg = _abi.HyServerConfig()
+        cfg.max_batch, cfg.in_flight, cfg.max_pending = max_batch, in_flight, max_pending
+        cfg.profile_budget, cfg.scores_budget = profile_budget, scores_budget
+        if launch_config is not None:
+            for i, v in enumerate(launch_config):
+                cfg.launch_config[i] = int(v)
+        h = C.c_void_p()
+        _check(lib.hy_server_create(arr, len(dbs), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._dbs = dbs
+        # Requests not yet waited for: the server writes their score arrays at completion, so the
+        # arrays stay referenced here until wait() or close().
+        self._live = {}
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.hy_server_destroy(h)
+            self._h = C.c_void_p(None)
+        self._live = {}
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, query, db: int = 0, want_scores: bool = False) -> ServerRequest:
+        q = _as_u8(query)
+        qb = q if q.size else np.zeros(1, np.uint8)
+        scores = np.empty(self._dbs[db].sequence_count(), dtype=np.int32) if want_scores else None
+        sp = _ptr(scores, _abi._i32p) if want_scores else None
+        rid = C.c_uint64()
+        _check(lib.hy_server_submit(self._h, int(db), _ptr(qb, _abi._u8p), len(q), 1 if want_scores else 0,
+                                    sp, C.byref(rid)))
+        req = ServerRequest(int(rid.value), int(db), scores)
+        self._live[req.id] = req
+        return req
+
+    def request_bytes(self, qlen: int, db: int = 0, want_scores: bool = False):
+        """(query-profile bytes, score-output bytes) a request takes from its batch's budgets."""
+        sb = C.c_uint64()
+        pb = lib.hy_server_request_bytes(self._h, int(db), int(qlen), 1 if want_scores else 0, C.byref(sb))
+        return int(pb), int(sb.value)
+
+    def poll(self, req: ServerRequest) -> bool:
+        done = C.c_int()
+        _check(lib.hy_server_poll(self._h, req.id, C.byref(done)))
+        return bool(done.value)
+
+    def wait(self, req: ServerRequest, timeout: float = 600.0) -> BestHit:
+        out = _abi.HyHit()
+        st = lib.hy_server_wait(self._h, req.id, float(timeout), C.byref(out))
+        if st != _abi.TIMEOUT:
+            self._live.pop(req.id, None)
+        _check(st)
+        return BestHit._from(out)
+
+    def stats(self, reset: bool = False) -> dict:
+        s = _abi.HyServerStats()
+        _check(lib.hy_server_stats_read(self._h, 1 if reset else 0, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+
 # ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------------------
 
 def align_pairs_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, mode: Mode, search_type: SearchType):
@@ -581,5 +662,6 @@ def align_pairs(pairs, scoring: Scoring, mode: Mode, search_type: SearchType, ou
 __all__ = [
     "BACKEND_ENV_VAR", "Backend", "BackendChoice", "BestHit", "Database", "DatabaseBuilder", "Error",
     "Batch", "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
+    "Server", "ServerRequest",
     "align_pairs", "align_pairs_arrays", "required_width", "concat",
 ]

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libhyalite_cuda.so")
 
 # Status codes (hy_status).
 OK = 0
+TIMEOUT = 24
 STATUS_NAMES = {
     0: "Ok", 1: "EmptyAlphabet", 2: "MatrixShape", 3: "NegativeGapPenalty",
     4: "GapOpenLessThanExtend", 5: "ScoreRangeTooWide", 6: "SymbolOutOfRange",
@@ -30,6 +31,20 @@ LAYOUT_AUTO = -1
 class HyHit(C.Structure):
     _fields_ = [("score", C.c_int32), ("reserved", C.c_uint32), ("db_index", C.c_uint64),
                 ("query_end", C.c_int64), ("target_end", C.c_int64)]
+
+
+class HyServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("in_flight", C.c_uint32), ("max_pending", C.c_uint32),
+                ("reserved", C.c_uint32), ("profile_budget", C.c_uint64), ("scores_budget", C.c_uint64),
+                ("launch_config", C.c_int32 * 3)]
+
+
+class HyServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64),
+                ("batches", C.c_uint64), ("pending", C.c_uint64), ("mean_batch", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("cells", C.c_double), ("seconds", C.c_double),
+                ("gcups", C.c_double)]
 
 
 _u8p = C.POINTER(C.c_uint8)
@@ -89,6 +104,13 @@ SIGNATURES = {
     "hy_batch_set_config": (_st, [_vp, _i32p]),
     "hy_batch_device_bytes": (C.c_uint64, [_vp]),
     "hy_batch_stream": (_vp, [_vp]),
+    "hy_server_create": (_st, [C.POINTER(_vp), C.c_uint32, C.POINTER(HyServerConfig), C.POINTER(_vp)]),
+    "hy_server_destroy": (None, [_vp]),
+    "hy_server_submit": (_st, [_vp, C.c_uint32, _u8p, C.c_uint64, C.c_int, _i32p, _u64p]),
+    "hy_server_request_bytes": (C.c_uint64, [_vp, C.c_uint32, C.c_uint64, C.c_int, _u64p]),
+    "hy_server_poll": (_st, [_vp, C.c_uint64, C.POINTER(C.c_int)]),
+    "hy_server_wait": (_st, [_vp, C.c_uint64, C.c_double, C.POINTER(HyHit)]),
+    "hy_server_stats_read": (_st, [_vp, C.c_int, C.POINTER(HyServerStats)]),
 }
 
 

@@ -22,36 +22,15 @@
 #include <map>
 #include <vector>
 
-#include "db_internal.h"
+#include "batch_internal.h"
 
 using namespace hy;
 
 namespace hy {
 
-// Launch classes (one persistent kernel each) and profile kinds (one query profile each).
-enum { BC_BULK8 = 0, BC_BULK16 = 1, BC_BULK32 = 2, BC_LONG = 3, BC_I32 = 4, BC_N = 5 };
-enum { PK_BULK = 0, PK_W16 = 1, PK_I32 = 2, PK_W32 = 3, PK_N = 4 };
 static constexpr int LCG = LONG_G, LCR = LONG_R;      // long pairs and the int16x2 band
 static constexpr int ICG = MAIN_G32, ICR = MAIN_R32;  // int32 items
-static constexpr uint32_t LONG_W_MAX = 4096;          // largest long-pair split the tuner tries
-
-struct BatchQuery {
-    // Per profile kind: everything its launches need except the block's boundary region.
-    ScanParams sp[PK_N];
-    const int32_t *matrix;
-    const uint8_t *q;
-    const uint32_t *rank;
-    int32_t qlen, mode, ends, bulk_rows, top_free, al, lim16;
-    uint32_t k0, kl, n_i32, n16;
-};
-
-struct BatchCtl {
-    uint32_t count[BC_N];     // query slots in each class's order list
-    uint32_t n_chunks[BC_N];  // item chunks each class's queue walks
-    uint32_t head[BC_N];      // work counters (zeroed by the graph)
-    uint32_t n_queries;
-    uint32_t chunk_stride;    // 1, or k to run only every k-th chunk (autotuner samples)
-};
+static constexpr uint32_t LONG_W_MAX = 4096;          // largest long-pair split allowed
 
 struct ClassLaunch {
     const BatchQuery *queries;
@@ -232,51 +211,7 @@ __global__ void batch_finalize_kernel(const BatchQuery *queries, const BatchCtl 
     out[slot] = h;
 }
 
-}  // namespace hy
-
 // ---- host side ------------------------------------------------------------------------------
-
-struct BatchConfig {
-    int32_t rows8_max = 64;    // queries up to this length: 8 rows per lane
-    int32_t rows16_max = 192;  // up to this length: 16 rows per lane; longer: 32
-    uint32_t long_w = LONG_W;  // pairs wider than this run one warp each
-};
-
-struct hy_batch {
-    int device = 0;
-    std::vector<const hy_db *> dbs;
-    uint32_t max_queries = 0;
-    uint64_t max_q_res = 0;
-    int32_t al_max = 0;
-    uint64_t mql_max = 0, max_t = 0;
-    cudaStream_t stream = nullptr, side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
-    BatchQuery *d_queries = nullptr, *h_queries = nullptr;
-    BatchCtl *d_ctl = nullptr, *h_ctl = nullptr;
-    uint32_t *d_order = nullptr, *h_order = nullptr;  // BC_N lists of max_queries slots
-    uint8_t *d_qres = nullptr, *h_qres = nullptr;
-    uint8_t *d_prof = nullptr;
-    size_t prof_per_query = 0;
-    uint8_t *d_bnd_bulk = nullptr, *d_bnd_side = nullptr, *d_bnd_band = nullptr;
-    size_t stride_bulk = 0, stride_side = 0, stride_band = 0;
-    unsigned long long *d_keys = nullptr;
-    int32_t *d_ends = nullptr;
-    hy_hit *d_hits = nullptr, *h_hits = nullptr;
-    int *d_err = nullptr, *h_err = nullptr;
-    int grid[BC_N] = {0, 0, 0, 0, 0};
-    size_t smem[BC_N] = {0, 0, 0, 0, 0};
-    int band_threads = 32;
-    size_t band_smem = 0;
-    cudaGraphExec_t exec = nullptr;
-    BatchConfig cfg;
-    bool autotune = true;
-    std::map<uint64_t, BatchConfig> tuned;  // batch shape signature -> configuration
-    uint64_t device_bytes = 0;
-    uint64_t runs = 0;
-    double last_tune_ms = 0.0;
-};
-
-namespace hy {
 
 #define HB_CK(call)                                                                  \
     do {                                                                             \
@@ -287,11 +222,36 @@ namespace hy {
         }                                                                            \
     } while (0)
 
-
 static size_t align128(size_t x) { return (x + 127) / 128 * 128; }
 
 static size_t pass_bytes_of(int32_t al, int rpp, size_t row_bytes) {
     return (size_t)(al + 1) * rpp * row_bytes;
+}
+
+// Which profiles one query needs and their shapes.
+struct QueryKinds {
+    QuerySplit split;
+    int rows = 8;
+    bool need[PK_N] = {false, false, false, false};
+    QueryPlan qp[PK_N];
+    uint64_t bytes = 0;  // device bytes of all needed profiles (128-byte aligned each)
+};
+
+static void plan_kinds(const hy_db *db, uint64_t qlen, bool ends, const BatchConfig &cfg, QueryKinds &k) {
+    k.split = split_for_query(db, qlen, cfg.long_w);
+    k.rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
+    const QuerySplit &sp = k.split;
+    k.need[PK_BULK] = sp.kl < db->p16.n_items;
+    k.need[PK_W16] = sp.kl > sp.k0 || ends;
+    k.need[PK_I32] = sp.n_i32 > 0;
+    k.need[PK_W32] = ends && sp.n_i32 > 0;
+    const int rpp[PK_N] = {MAIN_G * k.rows, LCG * LCR, ICG * ICR, WIN_G * WIN_R};
+    k.bytes = 0;
+    for (int i = 0; i < PK_N; ++i) {
+        const bool i16 = i == PK_BULK || i == PK_W16;
+        k.qp[i] = plan(qlen, rpp[i], db->al, i16 ? profile_row_bytes<Pair16>() : profile_row_bytes<Single32>());
+        if (k.need[i]) k.bytes += align128((size_t)k.qp[i].pass_bytes * k.qp[i].n_passes);
+    }
 }
 
 template <class A, int G, int R, int PK>
@@ -347,14 +307,16 @@ static hy_status record_graph_body(hy_batch *b) {
     batch_finalize_kernel<<<(b->max_queries + 127) / 128, 128, 0, b->stream>>>(b->d_queries, b->d_ctl,
                                                                                b->d_ends, b->d_hits);
     HB_CK(cudaGetLastError());
+    b->kernels_per_run = 10;
     return fail(HY_OK);
 }
 
-static void free_batch(hy_batch *b) {
+void batch_free(hy_batch *b) {
     if (!b) return;
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     void *dev[] = {b->d_queries, b->d_ctl, b->d_order, b->d_qres, b->d_prof, b->d_bnd_bulk,
                    b->d_bnd_side, b->d_bnd_band, b->d_keys, b->d_ends, b->d_hits, b->d_err};
@@ -387,47 +349,58 @@ struct BatchDeviceGuard {
     }
 };
 
-// Validates the queries and writes the batch's descriptors into the pinned staging buffers.
-static hy_status stage_batch(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_t *q_res,
-                             const uint64_t *q_off, int32_t *const *d_scores, const BatchConfig &cfg,
-                             uint32_t chunk_stride, uint32_t *failed) {
+uint64_t batch_profile_bytes(const hy_batch *b, const hy_db *db, uint64_t qlen, bool ends) {
+    QueryKinds k;
+    plan_kinds(db, qlen, ends && db->search_type == HY_SEARCH_SCORE_END, b->cfg, k);
+    return k.bytes;
+}
+
+hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const BatchConfig &cfg,
+                      uint32_t chunk_stride, uint32_t *failed) {
     if (n > b->max_queries) return fail(HY_ERR_INVALID_ARGUMENT, n, b->max_queries);
-    if (n > 0 && (!dbq || !q_off)) return fail(HY_ERR_INVALID_ARGUMENT);
-    const uint64_t total_res = n ? q_off[n] - q_off[0] : 0;
-    if (total_res > b->max_q_res) return fail(HY_ERR_INVALID_ARGUMENT, (int64_t)total_res, (int64_t)b->max_q_res);
-    if (total_res && !q_res) return fail(HY_ERR_INVALID_ARGUMENT);
+    if (n > 0 && !items) return fail(HY_ERR_INVALID_ARGUMENT);
+    uint64_t total_res = 0;
     for (uint32_t i = 0; i < n; ++i) {
         if (failed) *failed = i;
-        if (dbq[i] >= b->dbs.size()) return fail(HY_ERR_INVALID_ARGUMENT, dbq[i], (int64_t)b->dbs.size());
-        if (q_off[i + 1] < q_off[i]) return fail(HY_ERR_INVALID_ARGUMENT);
-        const hy_db *db = b->dbs[dbq[i]];
-        const uint64_t qlen = q_off[i + 1] - q_off[i];
-        if (qlen > db->mql) return fail(HY_ERR_QUERY_TOO_LONG, (int64_t)qlen, (int64_t)db->mql);
-        const uint8_t *q = q_res + (q_off[i] - q_off[0]);
-        for (uint64_t k = 0; k < qlen; ++k)
-            if (q[k] >= db->al) return fail(HY_ERR_SYMBOL_OUT_OF_RANGE, q[k], (int64_t)db->al);
+        const BatchItem &it = items[i];
+        if (it.db >= b->dbs.size()) return fail(HY_ERR_INVALID_ARGUMENT, it.db, (int64_t)b->dbs.size());
+        const hy_db *db = b->dbs[it.db];
+        if (it.qlen > db->mql) return fail(HY_ERR_QUERY_TOO_LONG, (int64_t)it.qlen, (int64_t)db->mql);
+        if (it.qlen && !it.q) return fail(HY_ERR_INVALID_ARGUMENT);
+        for (uint64_t k = 0; k < it.qlen; ++k)
+            if (it.q[k] >= db->al) return fail(HY_ERR_SYMBOL_OUT_OF_RANGE, it.q[k], (int64_t)db->al);
+        total_res += it.qlen;
     }
     if (failed) *failed = n;
-    if (total_res) memcpy(b->h_qres, q_res, total_res);
+    if (total_res > b->max_q_res) return fail(HY_ERR_INVALID_ARGUMENT, (int64_t)total_res, (int64_t)b->max_q_res);
     BatchCtl &ctl = *b->h_ctl;
     memset(&ctl, 0, sizeof(ctl));
     ctl.n_queries = n;
     ctl.chunk_stride = std::max<uint32_t>(1, chunk_stride);
     std::vector<std::vector<uint32_t>> lists(BC_N);
-    size_t prof_off = 0;
+    uint64_t prof_off = 0, q_off = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        const hy_db *db = b->dbs[dbq[i]];
-        const uint64_t qlen = q_off[i + 1] - q_off[i];
+        const BatchItem &it = items[i];
+        const hy_db *db = b->dbs[it.db];
+        const uint64_t qlen = it.qlen;
+        if (qlen) memcpy(b->h_qres + q_off, it.q, qlen);
         BatchQuery &bq = b->h_queries[i];
         memset(&bq, 0, sizeof(bq));
-        const QuerySplit sp = split_for_query(db, qlen, cfg.long_w);
+        const bool ends = it.ends && db->search_type == HY_SEARCH_SCORE_END;
+        QueryKinds k;
+        plan_kinds(db, qlen, ends, cfg, k);
+        if (prof_off + k.bytes > b->prof_cap) {
+            if (failed) *failed = i;
+            return fail(HY_ERR_REJECTED, (int64_t)(prof_off + k.bytes), (int64_t)b->prof_cap);
+        }
+        const QuerySplit &sp = k.split;
         bq.matrix = db->d_matrix;
-        bq.q = b->d_qres + (q_off[i] - q_off[0]);
+        bq.q = b->d_qres + q_off;
         bq.rank = db->d_rank;
         bq.qlen = (int32_t)qlen;
         bq.mode = db->mode;
-        bq.ends = db->search_type == HY_SEARCH_SCORE_END ? 1 : 0;
-        bq.bulk_rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
+        bq.ends = ends ? 1 : 0;
+        bq.bulk_rows = k.rows;
         bq.top_free = (db->mode == MODE_SW || db->mode == MODE_HW || db->mode == MODE_OV) ? 1 : 0;
         bq.al = (int32_t)db->al;
         bq.lim16 = 32767 - db->go;
@@ -435,12 +408,9 @@ static hy_status stage_batch(hy_batch *b, uint32_t n, const uint32_t *dbq, const
         bq.kl = sp.kl;
         bq.n_i32 = sp.n_i32;
         bq.n16 = db->p16.n_items;
-        const bool need[PK_N] = {sp.kl < db->p16.n_items, sp.kl > sp.k0 || bq.ends, sp.n_i32 > 0,
-                                 bq.ends && sp.n_i32 > 0};
-        const int rpp[PK_N] = {MAIN_G * bq.bulk_rows, LCG * LCR, ICG * ICR, WIN_G * WIN_R};
-        for (int k = 0; k < PK_N; ++k) {
-            ScanParams &p = bq.sp[k];
-            const bool i16 = k == PK_BULK || k == PK_W16;
+        for (int kk = 0; kk < PK_N; ++kk) {
+            ScanParams &p = bq.sp[kk];
+            const bool i16 = kk == PK_BULK || kk == PK_W16;
             const Partition &part = i16 ? db->p16 : db->p32;
             p.meta = part.d_meta;
             p.n_items = part.n_items;
@@ -449,19 +419,18 @@ static hy_status stage_batch(hy_batch *b, uint32_t n, const uint32_t *dbq, const
             p.go = db->go;
             p.ge = db->ge;
             p.sentinel = i16 ? (-32768 + db->ge) : (INT32_MIN / 4);
-            p.scores = d_scores ? d_scores[i] : nullptr;
+            p.scores = it.d_scores;
             p.best_key = b->d_keys + i;
             p.err = b->d_err;
-            if (!need[k]) continue;
-            const QueryPlan qp = plan(qlen, rpp[k], db->al, i16 ? profile_row_bytes<Pair16>() : profile_row_bytes<Single32>());
-            p.pass_bytes = qp.pass_bytes;
-            p.n_passes = qp.n_passes;
-            p.vrow0 = qp.vrow0;
-            p.profile = b->d_prof + (size_t)i * b->prof_per_query + prof_off;
-            prof_off += align128((size_t)qp.pass_bytes * qp.n_passes);
+            if (!k.need[kk]) continue;
+            p.pass_bytes = k.qp[kk].pass_bytes;
+            p.n_passes = k.qp[kk].n_passes;
+            p.vrow0 = k.qp[kk].vrow0;
+            p.profile = b->d_prof + prof_off;
+            prof_off += align128((size_t)p.pass_bytes * p.n_passes);
         }
-        prof_off = 0;
-        const int bulk_cls = bq.bulk_rows == 8 ? BC_BULK8 : bq.bulk_rows == 16 ? BC_BULK16 : BC_BULK32;
+        q_off += qlen;
+        const int bulk_cls = k.rows == 8 ? BC_BULK8 : k.rows == 16 ? BC_BULK16 : BC_BULK32;
         if (sp.kl < db->p16.n_items) {
             lists[bulk_cls].push_back(i);
             ctl.n_chunks[bulk_cls] = std::max<uint32_t>(ctl.n_chunks[bulk_cls], (db->p16.n_items + 31) / 32);
@@ -486,22 +455,22 @@ static hy_status stage_batch(hy_batch *b, uint32_t n, const uint32_t *dbq, const
     return fail(HY_OK);
 }
 
-// Copies the staged batch to the device and replays the graph (asynchronous on b->stream).
-static hy_status launch_staged(hy_batch *b, uint32_t n, uint64_t total_res) {
+hy_status batch_launch(hy_batch *b, uint32_t n) {
+    uint64_t total_res = 0;
+    for (uint32_t i = 0; i < n; ++i) total_res += (uint64_t)b->h_queries[i].qlen;
     if (total_res) HB_CK(cudaMemcpyAsync(b->d_qres, b->h_qres, total_res, cudaMemcpyHostToDevice, b->stream));
     if (n) HB_CK(cudaMemcpyAsync(b->d_queries, b->h_queries, sizeof(BatchQuery) * n, cudaMemcpyHostToDevice, b->stream));
     HB_CK(cudaMemcpyAsync(b->d_order, b->h_order, sizeof(uint32_t) * BC_N * b->max_queries,
                           cudaMemcpyHostToDevice, b->stream));
     HB_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, b->stream));
     HB_CK(cudaGraphLaunch(b->exec, b->stream));
+    if (n) HB_CK(cudaMemcpyAsync(b->h_hits, b->d_hits, sizeof(hy_hit) * n, cudaMemcpyDeviceToHost, b->stream));
+    HB_CK(cudaMemcpyAsync(b->h_err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     ++b->runs;
     return fail(HY_OK);
 }
 
-static hy_status finish_run(hy_batch *b, uint32_t n, hy_hit *out) {
-    if (n && out) HB_CK(cudaMemcpyAsync(b->h_hits, b->d_hits, sizeof(hy_hit) * n, cudaMemcpyDeviceToHost, b->stream));
-    HB_CK(cudaMemcpyAsync(b->h_err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
-    HB_CK(cudaStreamSynchronize(b->stream));
+hy_status batch_collect(hy_batch *b, uint32_t n, hy_hit *out) {
     if (*b->h_err) {
         *b->h_err = 0;
         HB_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
@@ -512,17 +481,23 @@ static hy_status finish_run(hy_batch *b, uint32_t n, hy_hit *out) {
     return fail(HY_OK);
 }
 
+static hy_status run_sync(hy_batch *b, uint32_t n, hy_hit *out) {
+    hy_status st = batch_launch(b, n);
+    if (st != HY_OK) return st;
+    HB_CK(cudaStreamSynchronize(b->stream));
+    return batch_collect(b, n, out);
+}
+
 // Shape signature of a batch: the share of queries in each (mode, log2 length) bucket, in
 // eighths, plus the databases used.
-static uint64_t batch_signature(const hy_batch *b, uint32_t n, const uint32_t *dbq, const uint64_t *q_off) {
+static uint64_t batch_signature(const hy_batch *b, const BatchItem *items, uint32_t n) {
     std::vector<uint32_t> hist(5 * 24, 0);
     std::vector<char> used(b->dbs.size(), 0);
     for (uint32_t i = 0; i < n; ++i) {
-        const uint64_t qlen = q_off[i + 1] - q_off[i];
         int lg = 0;
-        while (lg < 23 && (1ull << (lg + 1)) <= qlen + 1) ++lg;
-        ++hist[b->dbs[dbq[i]]->mode * 24 + lg];
-        used[dbq[i]] = 1;
+        while (lg < 23 && (1ull << (lg + 1)) <= items[i].qlen + 1) ++lg;
+        ++hist[b->dbs[items[i].db]->mode * 24 + lg];
+        used[items[i].db] = 1;
     }
     uint64_t h = 1469598103934665603ull;
     auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
@@ -532,22 +507,24 @@ static uint64_t batch_signature(const hy_batch *b, uint32_t n, const uint32_t *d
 }
 
 // Times one configuration on a sampled part of the batch (every `stride`-th item chunk).
-static hy_status time_config(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_t *q_res,
-                             const uint64_t *q_off, const BatchConfig &cfg, uint32_t stride, float *ms) {
-    hy_status st = stage_batch(b, n, dbq, q_res, q_off, nullptr, cfg, stride, nullptr);
+static hy_status time_config(hy_batch *b, const BatchItem *items, uint32_t n, const BatchConfig &cfg,
+                             uint32_t stride, float *ms) {
+    hy_status st = batch_stage(b, items, n, cfg, stride, nullptr);
     if (st != HY_OK) return st;
     HB_CK(cudaEventRecord(b->ev_t0, b->stream));
-    st = launch_staged(b, n, n ? q_off[n] - q_off[0] : 0);
+    st = batch_launch(b, n);
     if (st != HY_OK) return st;
     HB_CK(cudaEventRecord(b->ev_t1, b->stream));
-    st = finish_run(b, 0, nullptr);
+    HB_CK(cudaStreamSynchronize(b->stream));
+    st = batch_collect(b, 0, nullptr);
     if (st != HY_OK) return st;
     HB_CK(cudaEventElapsedTime(ms, b->ev_t0, b->ev_t1));
     return fail(HY_OK);
 }
 
-static hy_status tune(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_t *q_res,
-                      const uint64_t *q_off, uint32_t stride, BatchConfig *best_cfg, double *best_ms) {
+// Coordinate search: the rows-per-lane thresholds first (at the default split), then the split.
+static hy_status tune(hy_batch *b, const BatchItem *items, uint32_t n, uint32_t stride,
+                      BatchConfig *best_cfg, double *best_ms) {
     static const int32_t rows_c[][2] = {{64, 192}, {0, 256}, {128, 512}, {0, 0}, {64, 64}, {32, 128}};
     static const uint32_t long_c[] = {1024, 2048, 4096};
     BatchConfig best = b->cfg;
@@ -558,7 +535,7 @@ static hy_status tune(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_
         c.rows16_max = rc[1];
         c.long_w = LONG_W;
         float t = 0;
-        hy_status st = time_config(b, n, dbq, q_res, q_off, c, stride, &t);
+        hy_status st = time_config(b, items, n, c, stride, &t);
         if (st != HY_OK) return st;
         if (t < best_t) {
             best_t = t;
@@ -570,7 +547,7 @@ static hy_status tune(hy_batch *b, uint32_t n, const uint32_t *dbq, const uint8_
         BatchConfig c = best;
         c.long_w = lw;
         float t = 0;
-        hy_status st = time_config(b, n, dbq, q_res, q_off, c, stride, &t);
+        hy_status st = time_config(b, items, n, c, stride, &t);
         if (st != HY_OK) return st;
         if (t < best_t) {
             best_t = t;
@@ -589,12 +566,26 @@ static uint32_t sample_stride(const hy_batch *b) {
     return std::max<uint32_t>(1, (n16 + 31) / 32 / 256);
 }
 
-}  // namespace hy
+static hy_status items_from_arrays(const hy_batch *b, uint32_t n, const uint32_t *dbq,
+                                   const uint8_t *q_res, const uint64_t *q_off,
+                                   std::vector<BatchItem> &items) {
+    if (n > 0 && (!dbq || !q_off)) return fail(HY_ERR_INVALID_ARGUMENT);
+    items.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (q_off[i + 1] < q_off[i]) return fail(HY_ERR_INVALID_ARGUMENT);
+        items[i].db = dbq[i];
+        items[i].qlen = q_off[i + 1] - q_off[i];
+        items[i].q = items[i].qlen ? q_res + (q_off[i] - q_off[0]) : nullptr;
+        items[i].d_scores = nullptr;
+        items[i].ends = true;
+        if (items[i].qlen && !q_res) return fail(HY_ERR_INVALID_ARGUMENT);
+    }
+    (void)b;
+    return fail(HY_OK);
+}
 
-extern "C" {
-
-hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_queries,
-                          int autotune, hy_batch **out) {
+hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_queries,
+                       uint64_t prof_cap, bool autotune, hy_batch **out) {
     if (!dbs || n_dbs == 0 || max_queries == 0 || !out) return fail(HY_ERR_INVALID_ARGUMENT);
     *out = nullptr;
     for (uint32_t i = 0; i < n_dbs; ++i) {
@@ -606,7 +597,7 @@ hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_
     b->device = dbs[0]->device;
     b->dbs.assign(dbs, dbs + n_dbs);
     b->max_queries = max_queries;
-    b->autotune = autotune != 0;
+    b->autotune = autotune;
     for (const hy_db *db : b->dbs) {
         b->al_max = std::max<int32_t>(b->al_max, (int32_t)db->al);
         b->mql_max = std::max(b->mql_max, db->mql);
@@ -658,10 +649,11 @@ hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_
     const int side_grid = std::max(b->grid[BC_LONG], b->grid[BC_I32]);
     const int bulk_grid = std::max({b->grid[BC_BULK8], b->grid[BC_BULK16], b->grid[BC_BULK32]});
     const uint64_t mq = b->mql_max;
-    b->prof_per_query = align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +   // bulk, any rows
-                        align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +   // long / band int16x2
-                        align128(pass_bytes_of(al, 1, pb32) * (mq + 511)) +   // int32
-                        align128(pass_bytes_of(al, 1, pb32) * (mq + 255)) + 512;  // band int32
+    const uint64_t per_query = align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +  // bulk, any rows
+                               align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +  // long / band int16x2
+                               align128(pass_bytes_of(al, 1, pb32) * (mq + 511)) +  // int32
+                               align128(pass_bytes_of(al, 1, pb32) * (mq + 255));   // band int32
+    b->prof_cap = prof_cap ? prof_cap : per_query * max_queries;
     if (st == HY_OK) {
         ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         ck(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
@@ -677,7 +669,7 @@ hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_
         dalloc((void **)&b->d_ctl, sizeof(BatchCtl));
         dalloc((void **)&b->d_order, sizeof(uint32_t) * BC_N * max_queries);
         dalloc((void **)&b->d_qres, b->max_q_res);
-        dalloc((void **)&b->d_prof, b->prof_per_query * max_queries);
+        dalloc((void **)&b->d_prof, b->prof_cap);
         dalloc((void **)&b->d_bnd_bulk, b->stride_bulk * bulk_grid);
         dalloc((void **)&b->d_bnd_side, b->stride_side * side_grid);
         dalloc((void **)&b->d_bnd_band, b->stride_band * max_queries);
@@ -712,14 +704,23 @@ hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_
     if (st != HY_OK) {
         int64_t d[3];
         hy_last_error_detail(d);
-        free_batch(b);
+        batch_free(b);
         return fail(st, d[0], d[1], d[2]);
     }
     *out = b;
     return fail(HY_OK);
 }
 
-void hy_batch_destroy(hy_batch *b) { free_batch(b); }
+}  // namespace hy
+
+extern "C" {
+
+hy_status hy_batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_queries,
+                          int autotune, hy_batch **out) {
+    return batch_create(dbs, n_dbs, max_queries, 0, autotune != 0, out);
+}
+
+void hy_batch_destroy(hy_batch *b) { batch_free(b); }
 
 uint64_t hy_batch_device_bytes(const hy_batch *b) { return b ? b->device_bytes : 0; }
 
@@ -746,12 +747,15 @@ hy_status hy_batch_tune(hy_batch *b, uint32_t n_queries, const uint32_t *db_of_q
                         const uint8_t *q_res, const uint64_t *q_off, uint32_t stride, double *best_ms) {
     if (!b) return fail(HY_ERR_INVALID_ARGUMENT);
     BatchDeviceGuard guard(b->device);
+    std::vector<BatchItem> items;
+    hy_status st = items_from_arrays(b, n_queries, db_of_query, q_res, q_off, items);
+    if (st != HY_OK) return st;
     if (stride == 0) stride = sample_stride(b);
     BatchConfig best;
-    hy_status st = tune(b, n_queries, db_of_query, q_res, q_off, stride, &best, best_ms);
+    st = tune(b, items.data(), n_queries, stride, &best, best_ms);
     if (st != HY_OK) return st;
     b->cfg = best;
-    if (n_queries) b->tuned[batch_signature(b, n_queries, db_of_query, q_off)] = best;
+    if (n_queries) b->tuned[batch_signature(b, items.data(), n_queries)] = best;
     return fail(HY_OK);
 }
 
@@ -760,29 +764,28 @@ hy_status hy_scan_batch(hy_batch *b, uint32_t n_queries, const uint32_t *db_of_q
                         uint32_t *failed_query) {
     if (!b || (n_queries && !out)) return fail(HY_ERR_INVALID_ARGUMENT);
     BatchDeviceGuard guard(b->device);
+    std::vector<BatchItem> items;
+    hy_status st = items_from_arrays(b, n_queries, db_of_query, q_res, q_off, items);
+    if (st != HY_OK) return st;
     // Validate before any tuning so that errors are reported for the caller's batch as given.
-    hy_status st = stage_batch(b, n_queries, db_of_query, q_res, q_off, nullptr, b->cfg, 1, failed_query);
+    st = batch_stage(b, items.data(), n_queries, b->cfg, 1, failed_query);
     if (st != HY_OK) return st;
     if (b->autotune && n_queries) {
-        const uint64_t sig = batch_signature(b, n_queries, db_of_query, q_off);
+        const uint64_t sig = batch_signature(b, items.data(), n_queries);
         auto it = b->tuned.find(sig);
         if (it == b->tuned.end()) {
-            double ms = 0;
             BatchConfig best;
-            st = tune(b, n_queries, db_of_query, q_res, q_off, sample_stride(b), &best, &ms);
+            st = tune(b, items.data(), n_queries, sample_stride(b), &best, nullptr);
             if (st != HY_OK) return st;
             b->tuned[sig] = best;
-            b->last_tune_ms = ms;
             b->cfg = best;
         } else {
             b->cfg = it->second;
         }
-        st = stage_batch(b, n_queries, db_of_query, q_res, q_off, nullptr, b->cfg, 1, failed_query);
+        st = batch_stage(b, items.data(), n_queries, b->cfg, 1, failed_query);
         if (st != HY_OK) return st;
     }
-    st = launch_staged(b, n_queries, n_queries ? q_off[n_queries] - q_off[0] : 0);
-    if (st != HY_OK) return st;
-    return finish_run(b, n_queries, out);
+    return run_sync(b, n_queries, out);
 }
 
 }  // extern "C"

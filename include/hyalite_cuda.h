@@ -234,6 +234,62 @@ uint64_t hy_batch_device_bytes(const hy_batch *batch);
 /* The batch's cudaStream_t, as an opaque pointer. */
 void *hy_batch_stream(hy_batch *batch);
 
+/* ---- served scan (no reference counterpart) ------------------------------------------------- */
+
+/* A request loop on its own host thread over a fixed set of databases. Requests ask for the best
+ * hit of a query (like hy_scan, with ends for ScoreEnd databases) or for every target's score
+ * (like hy_scan_scores; the hit then carries the best score and index without ends). Queued
+ * requests are admitted in arrival order into device batches while a batch's query-profile and
+ * score-output budgets hold; up to `in_flight` batches run on the GPU at once, so requests that
+ * arrive while others run are batched and overlap them on the device. Results equal the plain
+ * calls' for the same query. Zero fields take the defaults named below. */
+typedef struct {
+    uint32_t max_batch;        /* queries per device batch (64) */
+    uint32_t in_flight;        /* device batches that may run at once (2) */
+    uint32_t max_pending;      /* queued requests beyond which hy_server_submit rejects (4096) */
+    uint32_t reserved;
+    uint64_t profile_budget;   /* device bytes of query profiles per batch (max_batch queries of
+                                  the largest max_query_len) */
+    uint64_t scores_budget;    /* device (and pinned host) bytes of score outputs per batch
+                                  (max_batch x 4 x the largest database's sequence count) */
+    int32_t launch_config[3];  /* as hy_batch_set_config; {0, 0, 0}: the defaults */
+} hy_server_config;
+
+typedef struct {
+    uint64_t submitted, completed, rejected, batches, pending;
+    double mean_batch;                      /* requests per device batch */
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> result ready, completed requests */
+    double cells;                           /* DP cells of the completed requests */
+    double seconds;                         /* first submit -> last completion */
+    double gcups;                           /* cells / seconds / 1e9 */
+} hy_server_stats;
+
+typedef struct hy_server hy_server;
+hy_status hy_server_create(const hy_db *const *dbs, uint32_t n_dbs, const hy_server_config *config,
+                           hy_server **out);
+/* Stops accepting requests, completes every queued and running one, and frees the server.
+ * Results not yet waited for are discarded. */
+void hy_server_destroy(hy_server *server);
+/* Queues a query against dbs[db]. With want_scores, `scores_out` (the database's sequence count
+ * of int32, owned by the caller) receives every target's score when the request completes, so it
+ * must stay valid until the request is waited for or the server is destroyed. Validates like
+ * hy_scan; HY_ERR_REJECTED when the queue is full or the request alone exceeds a batch budget.
+ * Thread-safe. */
+hy_status hy_server_submit(hy_server *server, uint32_t db, const uint8_t *query, uint64_t qlen,
+                           int want_scores, int32_t *scores_out, uint64_t *request_id);
+/* The query-profile bytes a request of length qlen against dbs[db] takes from its batch's
+ * profile budget (the admission rule); *score_bytes (if not NULL) receives its score-output
+ * bytes. 0 for a bad server or database index. */
+uint64_t hy_server_request_bytes(const hy_server *server, uint32_t db, uint64_t qlen,
+                                 int want_scores, uint64_t *score_bytes);
+/* *done = 1 once the request's result is ready. */
+hy_status hy_server_poll(hy_server *server, uint64_t request_id, int *done);
+/* Waits up to timeout_s for the request; on completion writes its hit, releases the request and
+ * returns its status. HY_ERR_TIMEOUT leaves the request queued. */
+hy_status hy_server_wait(hy_server *server, uint64_t request_id, double timeout_s, hy_hit *out);
+/* Counters and latency percentiles since the last reset (reset != 0 clears them). */
+hy_status hy_server_stats_read(hy_server *server, int reset, hy_server_stats *out);
+
 /* ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------- */
 
 /* align_pairs: pair p is (q_res[q_off[p]..q_off[p+1]], t_res[t_off[p]..t_off[p+1]]). Each pair is
