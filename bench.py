@@ -450,6 +450,216 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_served(args):
+    """The served workload: a resident protein database (the generator above at --served-seqs
+    sequences), Poisson arrivals at each offered rate, query lengths log-normal (median 350,
+    sigma 0.8, clipped 50..3000), half the requests a ScoreEnd scan and half scan_scores (every
+    target's i32 score). Reports per rate the p50/p99 latency (submit -> result ready) and the
+    GCUPS the server sustained, beside the plain per-request calls (Database.scan /
+    scan_scores one at a time)."""
+    import torch
+
+    import hyalite_b200 as hy
+
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    mat, residues, offsets, _ = make_workload(args.seed, n_seqs=args.served_seqs)
+    gen_s = time.perf_counter() - t0
+    db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
+          .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(3000).build())
+    total_res = float(offsets[-1])
+    base = np.random.default_rng(12345)
+    base.integers(-4, 4, size=(AL, AL))
+    base.integers(4, 12, size=AL)
+    background = base.dirichlet(np.full(AL, 4.0))
+    rng = np.random.default_rng(args.seed + 7)
+
+    def request():
+        L = int(np.clip(round(math.exp(math.log(350.0) + 0.8 * rng.standard_normal())), 50, 3000))
+        return rng.choice(AL, size=L, p=background).astype(np.uint8), bool(rng.random() < 0.5)
+
+    srv = hy.Server([db], max_batch=args.served_batch, in_flight=2)
+    # Warm-up: one request of each kind.
+    for kind in (False, True):
+        q, _ = request()
+        srv.wait(srv.submit(q, want_scores=kind))
+    srv.stats(reset=True)
+    rates = [float(x) for x in args.served_rates.split(",")]
+    points = []
+    clocks = Clocks(0)
+    clocks.start()
+    for rate in rates:
+        n = int(min(args.served_max_requests, max(20, rate * args.served_seconds)))
+        reqs = [request() for _ in range(n)]
+        gaps = rng.exponential(1.0 / rate, n)
+        handles = []
+        t_start = time.perf_counter()
+        t_next = t_start
+        rejected = 0
+        for (q, kind), g in zip(reqs, gaps):
+            t_next += g
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            try:
+                handles.append((srv.submit(q, want_scores=kind), len(q)))
+            except hy.Error as e:
+                if e.kind != "Rejected":
+                    raise
+                rejected += 1
+        for h, _ in handles:
+            srv.wait(h)
+        wall = time.perf_counter() - t_start
+        st = srv.stats(reset=True)
+        points.append({"offered_qps": rate, "requests": n, "completed": int(st["completed"]),
+                       "rejected": int(st["rejected"]) + rejected, "achieved_qps": st["completed"] / wall,
+                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                       "max_ms": st["max_ms"], "mean_batch": st["mean_batch"], "gcups": st["gcups"],
+                       "wall_s": wall})
+    clk = clocks.stop()
+    srv.close()
+    # The plain form: the same kind of requests one at a time through the host API.
+    sc = hy.Scratch(db)
+    plain = [request() for _ in range(args.served_plain_requests)]
+    db.scan(sc, plain[0][0])
+    t0 = time.perf_counter()
+    cells = 0.0
+    for q, kind in plain:
+        if kind:
+            db.scan_scores_array(sc, q)
+        else:
+            db.scan(sc, q)
+        cells += len(q) * total_res
+    plain_s = time.perf_counter() - t0
+    plain_gcups = cells / plain_s / 1e9
+    best = max(points, key=lambda p: p["gcups"])
+    line = {
+        "metric": "GCUPS", "value": best["gcups"], "unit": "GCUPS", "n_gpus": 1, "steps": len(rates),
+        "warmup": 2, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "i16x2 (int32 for long sequences)", "data": "synthetic (seeded protein generator)",
+        "config": {"workload": f"served protein scan: {args.served_seqs} sequences, Poisson arrivals, "
+                               "log-normal query lengths (median 350, 50..3000), half ScoreEnd scan and "
+                               "half scan_scores (i32 per target)",
+                   "residues": int(total_res), "gen_s": round(gen_s, 1), "max_batch": args.served_batch,
+                   "in_flight": 2},
+        "served": points,
+        "plain": {"value": plain_gcups, "unit": "GCUPS", "requests": len(plain),
+                  "form": "Database.scan / scan_scores one request at a time"},
+        "served_over_plain": best["gcups"] / plain_gcups,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def make_pairs_workload(seed: int, n_pairs: int, genome_len: int = 10_000_000, read_len: int = 150):
+    """(read, window) pairs: reads of `read_len` from a seeded uniform genome with 2% substitutions
+    and, with probability 0.75 per read (0.5% per base), one 1..3-bp insertion or deletion; each
+    window 200..500 bp long and placed so that it contains the read's origin."""
+    rng = np.random.default_rng(seed)
+    genome = rng.integers(0, 4, genome_len, dtype=np.uint8)
+    reads = np.empty((n_pairs, read_len), np.uint8)
+    wlen = rng.integers(200, 501, n_pairs).astype(np.int64)
+    wstart = np.empty(n_pairs, np.int64)
+    j = np.arange(read_len)[None, :]
+    span = read_len + 3
+    for lo in range(0, n_pairs, 250_000):
+        n = min(250_000, n_pairs - lo)
+        W = wlen[lo:lo + n]
+        origin = rng.integers(600, genome_len - 600, n)
+        win = genome[origin[:, None] + np.arange(span)[None, :]]
+        p = rng.integers(0, read_len, n)[:, None]
+        dl = rng.integers(1, 4, n)[:, None]
+        kind = rng.random(n)
+        deletion = (kind < 0.375)[:, None]
+        insertion = ((kind >= 0.375) & (kind < 0.75))[:, None]
+        idx = np.where(deletion, j + dl * (j >= p), np.where(insertion, np.maximum(j - dl * (j >= p + dl), 0), j))
+        r = np.take_along_axis(win, idx, axis=1)
+        r = np.where(insertion & (j >= p) & (j < p + dl), rng.integers(0, 4, (n, read_len), dtype=np.uint8), r)
+        sub = rng.random((n, read_len)) < 0.02
+        r = np.where(sub, (r + rng.integers(1, 4, (n, read_len), dtype=np.uint8)) % 4, r).astype(np.uint8)
+        reads[lo:lo + n] = r
+        wstart[lo:lo + n] = origin - rng.integers(0, W - read_len + 1)
+    t_off = np.zeros(n_pairs + 1, np.uint64)
+    t_off[1:] = np.cumsum(wlen)
+    t_res = np.empty(int(t_off[-1]), np.uint8)
+    for lo in range(0, n_pairs, 250_000):
+        hi = min(n_pairs, lo + 250_000)
+        W = wlen[lo:hi]
+        base = int(t_off[lo])
+        seg = (np.repeat(wstart[lo:hi] - (t_off[lo:hi].astype(np.int64) - base), W)
+               + np.arange(int(t_off[hi]) - base, dtype=np.int64))
+        t_res[base:int(t_off[hi])] = genome[seg]
+    q_off = np.arange(n_pairs + 1, dtype=np.uint64) * read_len
+    return reads.reshape(-1), q_off, t_res, t_off
+
+
+def run_pairs(args):
+    """align_pairs over (read, window) pairs: Mode::Hw, ScoreEnd, +2/-1, gap_open 6, gap_ext 1.
+    `value` is real cells / the pair kernels' device time; `e2e` is the whole hy_align_pairs call
+    (host validation, sort and packing, copies, kernels, results) with host buffers."""
+    import torch
+
+    import hyalite_b200 as hy
+
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    q_res, q_off, t_res, t_off = make_pairs_workload(args.seed, args.n_pairs)
+    gen_s = time.perf_counter() - t0
+    dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
+    scoring = hy.Scoring(4, dna, 6, 1)
+    cells = float(np.dot(np.diff(q_off).astype(np.float64), np.diff(t_off).astype(np.float64)))
+    for _ in range(args.warmup):
+        hy.align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
+    clocks = Clocks(0)
+    clocks.start()
+    kms, cms = 0.0, 0.0
+    for _ in range(args.steps):
+        hits, (err, _) = hy.align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
+        assert err is None
+        k, c = hy.align_pairs_timing()
+        kms += k
+        cms += c
+    clk = clocks.stop()
+    # Parity on a sample against the oracle, and the CPU baseline (the reference's align_pairs is
+    # the scalar align_core loop) on a bounded sample over all host threads.
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    rng = np.random.default_rng(1)
+    sample = np.sort(rng.choice(args.n_pairs, min(args.n_pairs, 2000), replace=False))
+    qs = [q_res[int(q_off[i]):int(q_off[i + 1])] for i in sample]
+    ts = [t_res[int(t_off[i]):int(t_off[i + 1])] for i in sample]
+    st, want, _ = pyoracle.align_pairs(qs, ts, dna, 4, 6, 1, 2, 1)
+    got = [(hits[i].score, None if hits[i].query_end < 0 else hits[i].query_end,
+            None if hits[i].target_end < 0 else hits[i].target_end) for i in sample]
+    identical = st == 0 and got == [(w[0], w[2], w[3]) for w in want]
+    threads = os.cpu_count() or 1
+    n_cpu = min(args.n_pairs, args.cpu_pairs)
+    cq = [q_res[int(q_off[i]):int(q_off[i + 1])] for i in range(n_cpu)]
+    ct = [t_res[int(t_off[i]):int(t_off[i + 1])] for i in range(n_cpu)]
+    ccells = float(sum(len(a) * len(b) for a, b in zip(cq, ct)))
+    t0 = time.perf_counter()
+    pyoracle.align_pairs(cq, ct, dna, 4, 6, 1, 2, 1, threads=threads)
+    cpu_s = time.perf_counter() - t0
+    value = cells * args.steps / (kms * 1e-3)
+    line = {
+        "metric": "GCUPS", "value": value / 1e9, "unit": "GCUPS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": kms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "i16x2", "data": "synthetic (seeded genome reads and windows)",
+        "config": {"workload": f"align_pairs: {args.n_pairs} (150-bp read, 200..500-bp window) pairs, HW, "
+                               "ScoreEnd, +2/-1, gap_open 6, gap_ext 1",
+                   "cells_per_step": cells, "gen_s": round(gen_s, 1),
+                   "l2": "inputs larger than L2 (reads and windows: gigabytes)"},
+        "e2e": {"value": cells * args.steps / (cms * 1e-3) / 1e9, "unit": "GCUPS",
+                "h2d_bytes_per_step": int(len(q_res) + len(t_res) + 16 * args.n_pairs),
+                "d2h_bytes_per_step": 12 * args.n_pairs, "call_ms": cms / args.steps},
+        "identical_to_oracle_on_sample": identical,
+        "cpu_baseline": {"value": ccells / cpu_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+                         "sample": f"the first {n_cpu} pairs, scalar align_core restatement over {threads} threads"},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SEQS, QUERY_LENGTHS, N_QUERIES
     ap = argparse.ArgumentParser()
@@ -466,9 +676,17 @@ def main():
     ap.add_argument("--query-lengths", default=",".join(map(str, QUERY_LENGTHS)))
     ap.add_argument("--n-queries", type=int, default=N_QUERIES)
     # Other workloads of the same backend (not the default benchmark line).
-    ap.add_argument("--workload", default="scan", choices=["scan", "batched"])
+    ap.add_argument("--workload", default="scan", choices=["scan", "batched", "served", "pairs"])
+    ap.add_argument("--n-pairs", type=int, default=10_000_000)
+    ap.add_argument("--cpu-pairs", type=int, default=100_000)
     ap.add_argument("--n-reads", type=int, default=1_000_000)
     ap.add_argument("--n-batch-queries", type=int, default=256)
+    ap.add_argument("--served-seqs", type=int, default=1_000_000)
+    ap.add_argument("--served-rates", default="5,10,20,30,50,100,1000,20000")
+    ap.add_argument("--served-seconds", type=float, default=8.0)
+    ap.add_argument("--served-max-requests", type=int, default=300)
+    ap.add_argument("--served-batch", type=int, default=64)
+    ap.add_argument("--served-plain-requests", type=int, default=40)
     args = ap.parse_args()
     N_SEQS = args.n_seqs
     QUERY_LENGTHS = [int(x) for x in args.query_lengths.split(",")]
@@ -477,6 +695,10 @@ def main():
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "served":
+        run_served(args)
+    elif args.workload == "pairs":
+        run_pairs(args)
     else:
         run_cuda(args)
 

@@ -643,6 +643,13 @@ def align_pairs_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, mode: Mode,
     return out, (err, int(failed.value))
 
 
+def align_pairs_timing():
+    """(pair kernels' device ms, whole call ms) of this thread's last align_pairs call."""
+    k, c = C.c_double(), C.c_double()
+    _check(lib.hy_align_pairs_timing(C.byref(k), C.byref(c)))
+    return float(k.value), float(c.value)
+
+
 def align_pairs(pairs, scoring: Scoring, mode: Mode, search_type: SearchType, out: list) -> None:
     """Align independent (query, target) pairs; one BestHit per pair in input order with
     db_index = pair index. Raises the first failing pair's error; ``out`` then holds the hits of

@@ -4,11 +4,15 @@
 // align_pair_with (src/kernel.rs:354-415): symbols of the query then the target, then the width
 // proof on the pair's own lengths; the first failure ends the batch. The accepted prefix is
 // partitioned by the device width rule, sorted by (query length, target length), and packed two
-// pairs of EQUAL query length per int16x2 item so both halves share one row structure.
+// pairs of EQUAL query length per int16x2 item so both halves share one row structure. Rows per
+// lane are chosen per query length so that a pass (8 lanes x rows) wastes the fewest padded
+// rows; items of one choice run in one launch. Validation and packing run on all host threads.
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "host_common.h"
@@ -19,22 +23,27 @@ using namespace hy;
 namespace hy {
 
 constexpr int PAIR_G = 8;
-constexpr int PAIR_R16 = 16;
 constexpr int PAIR_R32 = 16;
 constexpr size_t PAIR_SMEM_LIMIT = 200 * 1024;
+// Rows per lane the int16x2 pair kernel is compiled for.
+constexpr int PAIR_ROWS[] = {8, 12, 16, 20, 24, 32};
 
 // Grow-only device and pinned buffers of the calling thread (align_pairs keeps one PairScratch
 // per call in the reference; here the device buffers survive across calls of the same thread).
 struct PairsContext {
     int device = -1;
     cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     struct Buf {
         void *p = nullptr;
         size_t n = 0;
     };
     Buf b[13];
+    double kernel_ms = 0.0, call_ms = 0.0;  // the last call: pair kernels' device time, whole call
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
     }
     cudaError_t get(int slot, size_t bytes, void **out) {
@@ -51,6 +60,7 @@ struct PairsContext {
         return cudaSuccess;
     }
 };
+
 static thread_local PairsContext g_ctx;
 
 #define HY_CK(call)                                                                                \
@@ -61,6 +71,30 @@ static thread_local PairsContext g_ctx;
             return fail(e_ == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e_); \
         }                                                                                          \
     } while (0)
+
+// Runs f(begin, end) over [0, n) split across the host's threads.
+template <class F>
+static void parallel_for(uint64_t n, uint64_t min_chunk, F f) {
+    unsigned t = std::max(1u, std::thread::hardware_concurrency());
+    t = (unsigned)std::min<uint64_t>(t, std::max<uint64_t>(1, n / std::max<uint64_t>(min_chunk, 1)));
+    if (t <= 1) {
+        f(0, n, 0);
+        return;
+    }
+    std::vector<std::thread> th;
+    const uint64_t per = (n + t - 1) / t;
+    for (unsigned i = 0; i < t; ++i) {
+        const uint64_t a = i * per, e = std::min(n, a + per);
+        if (a >= e) break;
+        th.emplace_back(f, a, e, i);
+    }
+    for (auto &x : th) x.join();
+}
+
+static unsigned host_threads(uint64_t n, uint64_t min_chunk) {
+    unsigned t = std::max(1u, std::thread::hardware_concurrency());
+    return (unsigned)std::min<uint64_t>(t, std::max<uint64_t>(1, n / std::max<uint64_t>(min_chunk, 1)));
+}
 
 template <class A, int G, int R, int MODE, bool ENDS>
 static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int threads, size_t smem,
@@ -92,6 +126,44 @@ static cudaError_t launch_pairs(int mode, bool ends, const PairParams &p, int bl
     return cudaErrorInvalidValue;
 }
 
+template <class A, int G>
+static cudaError_t launch_pairs_rows(int rows, int mode, bool ends, const PairParams &p, int blocks,
+                                     int threads, size_t smem, cudaStream_t st) {
+    if constexpr (A::NH == 2) {
+        switch (rows) {
+        case 8: return launch_pairs<A, G, 8>(mode, ends, p, blocks, threads, smem, st);
+        case 12: return launch_pairs<A, G, 12>(mode, ends, p, blocks, threads, smem, st);
+        case 16: return launch_pairs<A, G, 16>(mode, ends, p, blocks, threads, smem, st);
+        case 20: return launch_pairs<A, G, 20>(mode, ends, p, blocks, threads, smem, st);
+        case 24: return launch_pairs<A, G, 24>(mode, ends, p, blocks, threads, smem, st);
+        case 32: return launch_pairs<A, G, 32>(mode, ends, p, blocks, threads, smem, st);
+        }
+        return cudaErrorInvalidValue;
+    } else {
+        (void)rows;
+        return launch_pairs<A, G, PAIR_R32>(mode, ends, p, blocks, threads, smem, st);
+    }
+}
+
+// Rows per lane for an int16x2 item of query length q: the fewest padded rows over the pass
+// shapes whose per-group profile keeps at least two warps of groups per block; ties go to more
+// rows (fewer passes).
+static int pair_rows(uint64_t q, int32_t al) {
+    int best = 8;
+    uint64_t best_pad = ~0ull;
+    for (int r : PAIR_ROWS) {
+        const size_t group_bytes = (size_t)(al + 1) * PAIR_G * r * profile_row_bytes<Pair16>();
+        if (r > 8 && group_bytes * 8 > PAIR_SMEM_LIMIT) continue;
+        const uint64_t rpp = (uint64_t)PAIR_G * r;
+        const uint64_t pad = (q + rpp - 1) / rpp * rpp;
+        if (pad <= best_pad) {
+            best_pad = pad;
+            best = r;
+        }
+    }
+    return best;
+}
+
 struct PairPart {
     std::vector<ItemMeta> meta;
     std::vector<uint32_t> qlen;
@@ -105,6 +177,7 @@ static void pack_pairs(const std::vector<uint32_t> &order, const uint64_t *q_off
                        const uint64_t *t_off, bool two, PairPart &pp) {
     const uint64_t align = two ? 8 : 16;
     size_t i = 0;
+    pp.meta.reserve(two ? order.size() / 2 + 1 : order.size());
     while (i < order.size()) {
         ItemMeta m;
         m.pad_ = 0;
@@ -135,17 +208,13 @@ static void pack_pairs(const std::vector<uint32_t> &order, const uint64_t *q_off
     }
 }
 
-template <class A, int G, int R>
+template <class A, int G>
 static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, const uint8_t *t_res,
                           const uint64_t *t_off, const uint8_t *d_q, const int32_t *d_matrix,
                           int32_t al, int32_t go, int32_t ge, int mode, bool ends, int32_t *d_scores,
                           int32_t *d_qend, int32_t *d_tend) {
     if (pp.meta.empty()) return fail(HY_OK);
     const bool two = A::NH == 2;
-    const size_t group_bytes = (size_t)(al + 1) * G * R * profile_row_bytes<A>();
-    int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
-    gpb = gpb / (32 / G) * (32 / G);  // whole warps
-    if (gpb == 0) return fail(HY_ERR_UNSUPPORTED);
     const size_t n_items = pp.meta.size();
     void *d_meta, *d_qlen, *d_qoff, *d_res, *d_bnd;
     HY_CK(ctx.get(slot0 + 0, sizeof(ItemMeta) * n_items, &d_meta));
@@ -153,25 +222,33 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     HY_CK(ctx.get(slot0 + 2, sizeof(uint64_t) * 2 * n_items, &d_qoff));
     const size_t res_bytes = pp.cols * sizeof(typename A::RES);
     HY_CK(ctx.get(slot0 + 3, res_bytes, &d_res));
-    size_t max_q = 0;
-    for (uint32_t q : pp.qlen) max_q = std::max<size_t>(max_q, q);
-    const bool multipass = max_q > (size_t)(G * R);
+    // Rows per lane of each item (a function of its query length; items are sorted by it).
+    std::vector<int> rows(n_items);
+    bool multipass = false;
+    for (size_t i = 0; i < n_items; ++i) {
+        rows[i] = two ? pair_rows(pp.qlen[i], al) : PAIR_R32;
+        multipass = multipass || pp.qlen[i] > (uint32_t)(G * rows[i]);
+    }
     HY_CK(ctx.get(slot0 + 4, multipass ? 2 * sizeof(typename A::V) * pp.cols : 16, &d_bnd));
     // Pack target residues (the shorter half of a pair item padded with symbol `al`).
-    std::vector<typename A::RES> res(std::max<size_t>(pp.cols, 1), (typename A::RES)(two ? (al | (al << 8)) : 0));
-    for (const ItemMeta &m : pp.meta) {
-        const uint8_t *t0 = t_res + t_off[m.idx[0]];
-        const uint8_t *t1 = m.idx[1] == NO_INDEX ? nullptr : t_res + t_off[m.idx[1]];
-        for (uint32_t j = 0; j < m.w; ++j) {
-            if (two) {
-                uint32_t lo = j < m.n[0] ? t0[j] : (uint32_t)al;
-                uint32_t hi = (t1 && j < m.n[1]) ? t1[j] : (uint32_t)al;
-                res[m.col_off + j] = (typename A::RES)(lo | (hi << 8));
-            } else {
-                res[m.col_off + j] = (typename A::RES)t0[j];
+    std::vector<typename A::RES> res(std::max<size_t>(pp.cols, 1));
+    parallel_for(n_items, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
+        for (uint64_t it = a; it < e; ++it) {
+            const ItemMeta &m = pp.meta[it];
+            const uint64_t end = it + 1 < n_items ? pp.meta[it + 1].col_off : pp.cols;
+            const uint8_t *t0 = t_res + t_off[m.idx[0]];
+            const uint8_t *t1 = m.idx[1] == NO_INDEX ? nullptr : t_res + t_off[m.idx[1]];
+            for (uint64_t j = 0; j < end - m.col_off; ++j) {
+                if (two) {
+                    uint32_t lo = j < m.n[0] ? t0[j] : (uint32_t)al;
+                    uint32_t hi = (t1 && j < m.n[1]) ? t1[j] : (uint32_t)al;
+                    res[m.col_off + j] = (typename A::RES)(lo | (hi << 8));
+                } else {
+                    res[m.col_off + j] = (typename A::RES)(j < m.n[0] ? t0[j] : 0);
+                }
             }
         }
-    }
+    });
     HY_CK(cudaMemcpyAsync(d_meta, pp.meta.data(), sizeof(ItemMeta) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qlen, pp.qlen.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qoff, pp.qoff.data(), sizeof(uint64_t) * 2 * n_items, cudaMemcpyHostToDevice, ctx.stream));
@@ -180,7 +257,6 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     p.meta = (const ItemMeta *)d_meta;
     p.qlen = (const uint32_t *)d_qlen;
     p.qoff = (const uint64_t *)d_qoff;
-    p.n_items = (uint32_t)n_items;
     p.q_res = d_q;
     p.res = d_res;
     p.matrix = d_matrix;
@@ -190,15 +266,32 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     p.ge = ge;
     p.sentinel = two ? -32768 + ge : INT32_MIN / 4;
     p.top_free = (mode == MODE_SW || mode == MODE_HW || mode == MODE_OV) ? 1 : 0;
-    p.group_bytes = (uint32_t)group_bytes;
     p.boundary = d_bnd;
     p.scores = d_scores;
     p.qend = d_qend;
     p.tend = d_tend;
-    const int blocks = (int)((n_items + gpb - 1) / gpb);
-    HY_CK((launch_pairs<A, G, R>(mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
+    HY_CK(cudaEventRecord(ctx.ev0, ctx.stream));
+    for (size_t i0 = 0; i0 < n_items;) {
+        size_t i1 = i0;
+        while (i1 < n_items && rows[i1] == rows[i0]) ++i1;
+        const int r = rows[i0];
+        const size_t group_bytes = (size_t)(al + 1) * G * r * profile_row_bytes<A>();
+        int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
+        gpb = gpb / (32 / G) * (32 / G);  // whole warps
+        if (gpb == 0) return fail(HY_ERR_UNSUPPORTED);
+        p.group_bytes = (uint32_t)group_bytes;
+        p.item_base = (uint32_t)i0;
+        p.n_items = (uint32_t)i1;
+        const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
+        HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
+        i0 = i1;
+    }
+    HY_CK(cudaEventRecord(ctx.ev1, ctx.stream));
     // The host staging vector must outlive the async copy.
     HY_CK(cudaStreamSynchronize(ctx.stream));
+    float ms = 0.0f;
+    HY_CK(cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1));
+    ctx.kernel_ms += ms;
     return fail(HY_OK);
 }
 
@@ -209,6 +302,10 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                                     const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
                                     int32_t gap_ext, hy_mode mode, hy_search_type search_type,
                                     hy_hit *out, uint64_t *failed_pair) {
+    const auto t_call = std::chrono::steady_clock::now();
+    PairsContext &ctx = g_ctx;
+    ctx.kernel_ms = 0.0;
+    ctx.call_ms = 0.0;
     if (failed_pair) *failed_pair = n_pairs;
     if ((int)mode < 0 || (int)mode > 4) return fail(HY_ERR_INVALID_ARGUMENT);
     if ((int)search_type != HY_SEARCH_SCORE && (int)search_type != HY_SEARCH_SCORE_END)
@@ -221,40 +318,66 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
     const int32_t min_e = *std::min_element(matrix, matrix + alphabet_len * alphabet_len);
     const int32_t max_e = *std::max_element(matrix, matrix + alphabet_len * alphabet_len);
 
-    // Validate in input order; remember the first failure.
+    // Validate in input order, chunked over the host threads: each chunk stops at its own first
+    // failure, and the batch's first failure is that of the first chunk that has one. The pairs
+    // before it are partitioned by the device width rule in input order.
+    const unsigned nt = host_threads(n_pairs, 1 << 15);
+    struct Chunk {
+        uint64_t first_bad = ~0ull;
+        hy_status st = HY_OK;
+        int64_t d[3] = {0, 0, 0};
+        std::vector<uint32_t> o16, o32;
+    };
+    std::vector<Chunk> chunks(nt);
+    const uint64_t per = (n_pairs + nt - 1) / nt;
+    parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
+        for (uint64_t c = ca; c < ce; ++c) {
+            Chunk &ch = chunks[c];
+            const uint64_t a = c * per, e = std::min(n_pairs, a + per);
+            for (uint64_t k = a; k < e && ch.st == HY_OK; ++k) {
+                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
+                for (int s = 0; s < 2 && ch.st == HY_OK; ++s) {
+                    const uint8_t *seq = s == 0 ? q_res + q_off[k] : t_res + t_off[k];
+                    const uint64_t len = s == 0 ? ql : tl;
+                    for (uint64_t i = 0; i < len; ++i)
+                        if (seq[i] >= alphabet_len) {
+                            ch.st = HY_ERR_SYMBOL_OUT_OF_RANGE;
+                            ch.d[0] = seq[i];
+                            ch.d[1] = (int64_t)alphabet_len;
+                            break;
+                        }
+                }
+                if (ch.st == HY_OK) {
+                    const int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, ql, tl);
+                    if (narrowest_width(b) < 0) {
+                        ch.st = HY_ERR_SCORE_RANGE_TOO_WIDE;
+                        ch.d[0] = b;
+                    } else if (ql >= (1u << 30) || tl >= (1u << 31)) {
+                        ch.st = HY_ERR_UNSUPPORTED;
+                    } else {
+                        (device_fits_i16(b, gap_open) ? ch.o16 : ch.o32).push_back((uint32_t)k);
+                    }
+                }
+                if (ch.st != HY_OK) ch.first_bad = k;
+            }
+        }
+    });
     uint64_t n_ok = n_pairs;
     hy_status first = HY_OK;
     int64_t d[3] = {0, 0, 0};
     std::vector<uint32_t> o16, o32;
-    for (uint64_t k = 0; k < n_pairs && first == HY_OK; ++k) {
-        const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-        for (int s = 0; s < 2 && first == HY_OK; ++s) {
-            const uint8_t *seq = s == 0 ? q_res + q_off[k] : t_res + t_off[k];
-            const uint64_t len = s == 0 ? ql : tl;
-            for (uint64_t i = 0; i < len; ++i)
-                if (seq[i] >= alphabet_len) {
-                    first = HY_ERR_SYMBOL_OUT_OF_RANGE;
-                    d[0] = seq[i];
-                    d[1] = (int64_t)alphabet_len;
-                    break;
-                }
+    for (Chunk &ch : chunks) {
+        o16.insert(o16.end(), ch.o16.begin(), ch.o16.end());
+        o32.insert(o32.end(), ch.o32.begin(), ch.o32.end());
+        if (ch.st != HY_OK) {
+            first = ch.st;
+            n_ok = ch.first_bad;
+            memcpy(d, ch.d, sizeof(d));
+            break;
         }
-        if (first == HY_OK) {
-            const int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, ql, tl);
-            if (narrowest_width(b) < 0) {
-                first = HY_ERR_SCORE_RANGE_TOO_WIDE;
-                d[0] = b;
-            } else if (ql >= (1u << 30) || tl >= (1u << 31)) {
-                first = HY_ERR_UNSUPPORTED;
-            } else {
-                (device_fits_i16(b, gap_open) ? o16 : o32).push_back((uint32_t)k);
-            }
-        }
-        if (first != HY_OK) n_ok = k;
     }
     if (failed_pair && first != HY_OK) *failed_pair = n_ok;
     if (n_ok > 0) {
-        PairsContext &ctx = g_ctx;
         int dev = 0;
         HY_CK(cudaGetDevice(&dev));
         if (ctx.device != dev) {
@@ -262,15 +385,22 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             new (&ctx) PairsContext();
             ctx.device = dev;
             HY_CK(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
+            HY_CK(cudaEventCreate(&ctx.ev0));
+            HY_CK(cudaEventCreate(&ctx.ev1));
         }
-        auto shape = [&](uint32_t a, uint32_t b) {
-            const uint64_t qa = q_off[a + 1] - q_off[a], qb = q_off[b + 1] - q_off[b];
-            if (qa != qb) return qa > qb;
-            const uint64_t ta = t_off[a + 1] - t_off[a], tb = t_off[b + 1] - t_off[b];
-            return ta != tb ? ta > tb : a < b;
+        // Sort by (query length desc, target length desc, index asc) through 64-bit keys.
+        auto sort_part = [&](std::vector<uint32_t> &o) {
+            std::vector<std::pair<uint64_t, uint32_t>> key(o.size());
+            for (size_t i = 0; i < o.size(); ++i) {
+                const uint32_t k = o[i];
+                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
+                key[i] = {~((ql << 32) | tl), k};
+            }
+            std::sort(key.begin(), key.end());
+            for (size_t i = 0; i < o.size(); ++i) o[i] = key[i].second;
         };
-        std::sort(o16.begin(), o16.end(), shape);
-        std::sort(o32.begin(), o32.end(), shape);
+        sort_part(o16);
+        sort_part(o32);
         PairPart p16, p32;
         pack_pairs(o16, q_off, t_off, true, p16);
         pack_pairs(o32, q_off, t_off, false, p32);
@@ -287,24 +417,33 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                               cudaMemcpyHostToDevice, ctx.stream));
         int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + n_ok, *d_tend = d_qend + n_ok;
         const bool ends = search_type == HY_SEARCH_SCORE_END;
-        st = run_part<Pair16, PAIR_G, PAIR_R16>(ctx, 0, p16, t_res, t_off, (const uint8_t *)d_q,
-                                                (const int32_t *)d_matrix, (int32_t)alphabet_len,
-                                                gap_open, gap_ext, mode, ends, d_scores, d_qend, d_tend);
+        st = run_part<Pair16, PAIR_G>(ctx, 0, p16, t_res, t_off, (const uint8_t *)d_q,
+                                      (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
+                                      gap_ext, mode, ends, d_scores, d_qend, d_tend);
         if (st != HY_OK) return st;
-        st = run_part<Single32, PAIR_G, PAIR_R32>(ctx, 5, p32, t_res, t_off, (const uint8_t *)d_q,
-                                                  (const int32_t *)d_matrix, (int32_t)alphabet_len,
-                                                  gap_open, gap_ext, mode, ends, d_scores, d_qend, d_tend);
+        st = run_part<Single32, PAIR_G>(ctx, 5, p32, t_res, t_off, (const uint8_t *)d_q,
+                                        (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
+                                        gap_ext, mode, ends, d_scores, d_qend, d_tend);
         if (st != HY_OK) return st;
         std::vector<int32_t> h(3 * n_ok);
         HY_CK(cudaMemcpyAsync(h.data(), d_out, 3 * sizeof(int32_t) * n_ok, cudaMemcpyDeviceToHost, ctx.stream));
         HY_CK(cudaStreamSynchronize(ctx.stream));
-        for (uint64_t k = 0; k < n_ok; ++k) {
-            out[k].score = h[k];
-            out[k].reserved = 0;
-            out[k].db_index = k;
-            out[k].query_end = ends ? (int64_t)h[n_ok + k] : -1;
-            out[k].target_end = ends ? (int64_t)h[2 * n_ok + k] : -1;
-        }
+        parallel_for(n_ok, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
+            for (uint64_t k = a; k < e; ++k) {
+                out[k].score = h[k];
+                out[k].reserved = 0;
+                out[k].db_index = k;
+                out[k].query_end = ends ? (int64_t)h[n_ok + k] : -1;
+                out[k].target_end = ends ? (int64_t)h[2 * n_ok + k] : -1;
+            }
+        });
     }
+    ctx.call_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
     return fail(first, d[0], d[1], d[2]);
+}
+
+extern "C" hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms) {
+    if (kernel_ms) *kernel_ms = g_ctx.kernel_ms;
+    if (call_ms) *call_ms = g_ctx.call_ms;
+    return fail(HY_OK);
 }

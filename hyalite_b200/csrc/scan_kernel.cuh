@@ -764,6 +764,7 @@ struct PairParams {
     const ItemMeta *meta;  // n[h]: target lengths; idx[h]: pair indices
     const uint32_t *qlen;  // per item
     const uint64_t *qoff;  // per item and half: offset of the query residues in q_res
+    uint32_t item_base;    // items [item_base, n_items) run
     uint32_t n_items;
     const uint8_t *q_res;
     const void *res;       // packed target residues, as in the scan
@@ -819,7 +820,7 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     extern __shared__ __align__(128) uint8_t smem[];
     const int lane = threadIdx.x % G;
     const int gib = threadIdx.x / G;
-    const uint32_t item = blockIdx.x * (blockDim.x / G) + gib;
+    const uint32_t item = p.item_base + blockIdx.x * (blockDim.x / G) + gib;
     const bool active = item < p.n_items;
     ItemMeta meta;
     int32_t qlen = 0;

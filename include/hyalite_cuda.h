@@ -300,6 +300,9 @@ hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint
                          const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
                          uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
                          hy_search_type search_type, hy_hit *out, uint64_t *failed_pair);
+/* Timing of this thread's last hy_align_pairs call (no reference counterpart): the device time of
+ * its pair kernels (CUDA events around the launches) and the wall time of the whole call. */
+hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
 
 #ifdef __cplusplus
 }

@@ -79,3 +79,39 @@ def test_pairs_validation_returns_first_error_and_prefix():
                        hy.Mode.Nw, hy.SearchType.Score, out)
     assert e.value.kind == "ScoreRangeTooWide"
     assert len(out) == 0 or out[0].db_index == 0
+
+
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_every_rows_per_lane_choice_in_one_call(mode):
+    # Query lengths around every pass height of the 8/12/16/20/24/32-row shapes, DNA and protein:
+    # one call runs several launches (one per rows choice) over consecutive items.
+    rng = np.random.default_rng(60 + mode)
+    lengths = [1, 63, 64, 65, 96, 97, 128, 129, 150, 160, 161, 192, 193, 250, 256, 257, 400]
+    for al, mat, go in ((4, DNA, 6), (20, BLOSUM62, 11)):
+        qs, ts = [], []
+        for L in lengths:
+            for _ in range(3):  # three pairs per length: two share an int16x2 item
+                qs.append(list(rng.integers(0, al, L)))
+                ts.append(list(rng.integers(0, al, int(rng.integers(1, 520)))))
+        got, want = run_both(qs, ts, mat, al, go, 1, mode, 1)
+        assert got == want
+
+
+def test_first_failure_found_in_a_later_host_chunk():
+    # Enough pairs that validation runs in several host-thread chunks; the bad pair sits late.
+    rng = np.random.default_rng(77)
+    n = 200_000
+    qs = [[int(x) for x in rng.integers(0, 4, 8)] for _ in range(n)]
+    ts = [[int(x) for x in rng.integers(0, 4, 12)] for _ in range(n)]
+    bad = 150_001
+    ts[bad] = ts[bad][:5] + [7] + ts[bad][6:]
+    out = []
+    with pytest.raises(hy.Error) as e:
+        hy.align_pairs(list(zip(qs, ts)), hy.Scoring(4, DNA, 2, 1), hy.Mode.Hw, hy.SearchType.ScoreEnd, out)
+    assert e.value == hy.Error("SymbolOutOfRange", symbol=7, alphabet_len=4)
+    assert len(out) == bad
+    sample = list(range(0, bad, 9973)) + [bad - 1]
+    status, want, _ = o.align_pairs([qs[i] for i in sample], [ts[i] for i in sample], DNA, 4, 2, 1, 2, 1)
+    assert status == 0
+    assert [(h.score, h.query_end, h.target_end) for h in (out[i] for i in sample)] == \
+        [(w[0], w[2], w[3]) for w in want]
