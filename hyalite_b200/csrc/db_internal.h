@@ -63,6 +63,9 @@ inline QueryPlan plan(uint64_t qlen, int rpp, uint64_t al, size_t pe) {
 
 struct hy_db {
     int device = 0;
+    // Largest dynamic shared memory one block may use on the device (opt-in): launch shapes whose
+    // query-profile slices exceed it read the profile from global memory instead.
+    size_t smem_limit = 48 * 1024;
     uint64_t n_seqs = 0, mql = 0, max_t = 0, al = 0;
     int32_t go = 0, ge = 0, min_e = 0, max_e = 0;
     int mode = 0, search_type = 0, layout = HY_LAYOUT_GATHERED;

@@ -152,6 +152,10 @@ extern "C" hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_qu
     const Region r32 = plan_region<Single32, MAIN_G32, MAIN_R32>(db, db->p32, qlen, cursor);
     if (cursor > NOALLOC_SCRATCH_BYTES)
         return fail(HY_ERR_UNSUPPORTED, (int64_t)cursor, (int64_t)NOALLOC_SCRATCH_BYTES);
+    // This form stages its profile slices in shared memory only (large alphabets: hy_scan_scores).
+    const size_t smem_need = 2 * (size_t)std::max(r16.qp.pass_bytes, r32.qp.pass_bytes) + 16;
+    if (smem_need > db->smem_limit)
+        return fail(HY_ERR_UNSUPPORTED, (int64_t)smem_need, (int64_t)db->smem_limit);
     uint8_t *base = nullptr;
     hy_status st = scratch_address(device, &base);
     if (st != HY_OK) return st;

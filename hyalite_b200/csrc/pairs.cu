@@ -25,6 +25,8 @@ namespace hy {
 constexpr int PAIR_G = 8;
 constexpr int PAIR_R32 = 16;
 constexpr size_t PAIR_SMEM_LIMIT = 200 * 1024;
+// Largest global scratch for group profiles that do not fit in shared memory, per launch.
+constexpr size_t PAIR_GPROF_BYTES = 256ull << 20;
 // Rows per lane the int16x2 pair kernel is compiled for.
 constexpr int PAIR_ROWS[] = {8, 12, 16, 20, 24, 32};
 
@@ -38,7 +40,7 @@ struct PairsContext {
         void *p = nullptr;
         size_t n = 0;
     };
-    Buf b[13];
+    Buf b[14];
     double kernel_ms = 0.0, call_ms = 0.0;  // the last call: pair kernels' device time, whole call
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
@@ -96,10 +98,10 @@ static unsigned host_threads(uint64_t n, uint64_t min_chunk) {
     return (unsigned)std::min<uint64_t>(t, std::max<uint64_t>(1, n / std::max<uint64_t>(min_chunk, 1)));
 }
 
-template <class A, int G, int R, int MODE, bool ENDS>
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF>
 static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int threads, size_t smem,
                                      cudaStream_t st) {
-    auto kern = pairs_kernel<A, G, R, MODE, ENDS>;
+    auto kern = pairs_kernel<A, G, R, MODE, ENDS, GPROF>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -108,13 +110,36 @@ static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int thread
     return cudaGetLastError();
 }
 
+// The form with group profiles in global memory (p.gprof set): only the smallest row shape of
+// each lane arithmetic, which is what a large alphabet runs.
+template <class A, int G, int R>
+static cudaError_t launch_pairs_gprof(int mode, bool ends, const PairParams &p, int blocks,
+                                      int threads, cudaStream_t st) {
+    if constexpr ((A::NH == 2 && R == 8) || (A::NH == 1 && R == PAIR_R32)) {
+#define HY_MODE_CASE(M)                                                                     \
+    case M:                                                                                 \
+        return ends ? launch_pairs_mode<A, G, R, M, true, true>(p, blocks, threads, 0, st)  \
+                    : launch_pairs_mode<A, G, R, M, false, true>(p, blocks, threads, 0, st);
+        switch (mode) {
+            HY_MODE_CASE(MODE_SW)
+            HY_MODE_CASE(MODE_NW)
+            HY_MODE_CASE(MODE_HW)
+            HY_MODE_CASE(MODE_OV)
+            HY_MODE_CASE(MODE_SHW)
+        }
+#undef HY_MODE_CASE
+    }
+    return cudaErrorInvalidValue;
+}
+
 template <class A, int G, int R>
 static cudaError_t launch_pairs(int mode, bool ends, const PairParams &p, int blocks, int threads,
                                 size_t smem, cudaStream_t st) {
-#define HY_MODE_CASE(M)                                                                 \
-    case M:                                                                             \
-        return ends ? launch_pairs_mode<A, G, R, M, true>(p, blocks, threads, smem, st) \
-                    : launch_pairs_mode<A, G, R, M, false>(p, blocks, threads, smem, st);
+    if (p.gprof) return launch_pairs_gprof<A, G, R>(mode, ends, p, blocks, threads, st);
+#define HY_MODE_CASE(M)                                                                        \
+    case M:                                                                                    \
+        return ends ? launch_pairs_mode<A, G, R, M, true, false>(p, blocks, threads, smem, st) \
+                    : launch_pairs_mode<A, G, R, M, false, false>(p, blocks, threads, smem, st);
     switch (mode) {
         HY_MODE_CASE(MODE_SW)
         HY_MODE_CASE(MODE_NW)
@@ -253,7 +278,7 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     HY_CK(cudaMemcpyAsync(d_qlen, pp.qlen.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qoff, pp.qoff.data(), sizeof(uint64_t) * 2 * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_res, res.data(), res_bytes, cudaMemcpyHostToDevice, ctx.stream));
-    PairParams p;
+    PairParams p{};
     p.meta = (const ItemMeta *)d_meta;
     p.qlen = (const uint32_t *)d_qlen;
     p.qoff = (const uint64_t *)d_qoff;
@@ -270,6 +295,7 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     p.scores = d_scores;
     p.qend = d_qend;
     p.tend = d_tend;
+    p.gprof = nullptr;
     HY_CK(cudaEventRecord(ctx.ev0, ctx.stream));
     for (size_t i0 = 0; i0 < n_items;) {
         size_t i1 = i0;
@@ -278,12 +304,31 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
         const size_t group_bytes = (size_t)(al + 1) * G * r * profile_row_bytes<A>();
         int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
         gpb = gpb / (32 / G) * (32 / G);  // whole warps
-        if (gpb == 0) return fail(HY_ERR_UNSUPPORTED);
         p.group_bytes = (uint32_t)group_bytes;
-        p.item_base = (uint32_t)i0;
-        p.n_items = (uint32_t)i1;
-        const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
-        HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
+        if (gpb == 0) {
+            // Not one warp of group profiles fits in shared memory (a large alphabet): the groups
+            // keep their profiles in a global scratch region, in launches of bounded size.
+            gpb = 256 / G;
+            const size_t per_block = (size_t)gpb * group_bytes;
+            const size_t max_blocks = std::max<size_t>(1, PAIR_GPROF_BYTES / per_block);
+            const size_t need_blocks = (i1 - i0 + gpb - 1) / gpb;
+            void *d_gprof;
+            HY_CK(ctx.get(13, std::min(max_blocks, need_blocks) * per_block, &d_gprof));
+            p.gprof = (uint8_t *)d_gprof;
+            for (size_t j0 = i0; j0 < i1; j0 += max_blocks * gpb) {
+                const size_t j1 = std::min(i1, j0 + max_blocks * gpb);
+                p.item_base = (uint32_t)j0;
+                p.n_items = (uint32_t)j1;
+                const int blocks = (int)((j1 - j0 + gpb - 1) / gpb);
+                HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, 0, ctx.stream)));
+            }
+            p.gprof = nullptr;
+        } else {
+            p.item_base = (uint32_t)i0;
+            p.n_items = (uint32_t)i1;
+            const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
+            HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
+        }
         i0 = i1;
     }
     HY_CK(cudaEventRecord(ctx.ev1, ctx.stream));

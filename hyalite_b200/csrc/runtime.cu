@@ -60,10 +60,10 @@ namespace hy {
         }                                                                            \
     } while (0)
 
-template <class A, int G, int R, int MODE, bool ENDS>
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF>
 static cudaError_t launch_mode(const ScanParams &p, int blocks, int threads, size_t smem,
                                cudaStream_t st) {
-    auto kern = scan_kernel<A, G, R, MODE, ENDS>;
+    auto kern = scan_kernel<A, G, R, MODE, ENDS, GPROF>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -72,13 +72,38 @@ static cudaError_t launch_mode(const ScanParams &p, int blocks, int threads, siz
     return cudaGetLastError();
 }
 
+// The launch shapes that also exist in the global-memory-profile form (large alphabets): the bulk
+// pairs with 8 rows per lane, the long pairs and the int32 items.
 template <class A, int G, int R>
-static cudaError_t launch_scan(int mode, bool ends, const ScanParams &p, int blocks, int threads,
-                               size_t smem, cudaStream_t st) {
-#define HY_MODE_CASE(M)                                                              \
-    case M:                                                                          \
-        return ends ? launch_mode<A, G, R, M, true>(p, blocks, threads, smem, st)    \
-                    : launch_mode<A, G, R, M, false>(p, blocks, threads, smem, st);
+constexpr bool has_gprof_form() {
+    return (A::NH == 2 && G == MAIN_G && R == 8) || (A::NH == 2 && G == LONG_G && R == LONG_R) ||
+           (A::NH == 1 && G == MAIN_G32 && R == MAIN_R32);
+}
+
+template <class A, int G, int R>
+static cudaError_t launch_scan(int mode, bool ends, bool gprof, const ScanParams &p, int blocks,
+                               int threads, size_t smem, cudaStream_t st) {
+    if (gprof) {
+        if constexpr (has_gprof_form<A, G, R>()) {
+#define HY_MODE_CASE(M)                                                                   \
+    case M:                                                                               \
+        return ends ? launch_mode<A, G, R, M, true, true>(p, blocks, threads, smem, st)   \
+                    : launch_mode<A, G, R, M, false, true>(p, blocks, threads, smem, st);
+            switch (mode) {
+                HY_MODE_CASE(MODE_SW)
+                HY_MODE_CASE(MODE_NW)
+                HY_MODE_CASE(MODE_HW)
+                HY_MODE_CASE(MODE_OV)
+                HY_MODE_CASE(MODE_SHW)
+            }
+#undef HY_MODE_CASE
+        }
+        return cudaErrorInvalidValue;
+    }
+#define HY_MODE_CASE(M)                                                                    \
+    case M:                                                                                \
+        return ends ? launch_mode<A, G, R, M, true, false>(p, blocks, threads, smem, st)   \
+                    : launch_mode<A, G, R, M, false, false>(p, blocks, threads, smem, st);
     switch (mode) {
         HY_MODE_CASE(MODE_SW)
         HY_MODE_CASE(MODE_NW)
@@ -140,6 +165,8 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
     p.best_key = key;
     p.err = sc->d_err;
     size_t smem = 2 * (size_t)qp.pass_bytes + 16;
+    const bool gprof = smem > db->smem_limit;
+    if (gprof) smem = 16;
     const bool timed = sc->profile && item_ptr == nullptr;
     if (timed) {
         if (sc->n_events == sc->events.size()) {
@@ -155,7 +182,7 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
             (double)qlen * (double)(part.res_prefix[item_end] - part.res_prefix[item_base]);
         HY_CK(cudaEventRecord(sc->events[sc->n_events].first, st_));
     }
-    HY_CK((launch_scan<A, G, R>(db->mode, ends, p, blocks, threads, smem, st_)));
+    HY_CK((launch_scan<A, G, R>(db->mode, ends, gprof, p, blocks, threads, smem, st_)));
     if (timed) {
         HY_CK(cudaEventRecord(sc->events[sc->n_events].second, st_));
         ++sc->n_events;
@@ -200,8 +227,11 @@ static hy_status enqueue_scores(const hy_db *db, hy_scratch *sc, const uint8_t *
     if (split.kl < db->p16.n_items) {
         const int blocks = (int)((db->p16.n_items - split.kl + gpb - 1) / gpb);
         // Rows per lane by query length: more rows amortise the per-step work, fewer keep the
-        // padding of a short query's single pass small.
-        const int rows = bulk_rows(qlen);
+        // padding of a short query's single pass small. An alphabet whose two pass slices do not
+        // fit in shared memory runs with 8 rows, from the profile in global memory if need be.
+        int rows = bulk_rows(qlen);
+        const size_t slice = (size_t)(db->al + 1) * MAIN_G * profile_row_bytes<Pair16>();
+        if (2 * slice * rows + 16 > db->smem_limit) rows = 8;
 #define HY_BULK(RR)                                                                              \
     enqueue_partition<Pair16, MAIN_G, RR>(db, sc, db->p16, split.kl, db->p16.n_items, d_query,   \
                                           qlen, ends, key, scores, sc->d_prof16, sc->d_bnd16,    \
@@ -226,9 +256,9 @@ __global__ void winner_loc_kernel(const unsigned long long *key, const uint32_t 
     win[1] = packed ? NO_INDEX : r;
 }
 
-template <class A, int MODE>
+template <class A, int MODE, bool GPROF>
 static cudaError_t launch_band_mode(const ScanParams &p, int warps, size_t smem, cudaStream_t st) {
-    auto kern = band_kernel<A, WIN_R, MODE>;
+    auto kern = band_kernel<A, WIN_R, MODE, GPROF>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -266,17 +296,27 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     p.tend = sc->d_tend;
     p.best_key = nullptr;
     p.err = sc->d_err;
-    int warps = (int)std::min<size_t>(32, BAND_SMEM_BUDGET / std::max<uint32_t>(qp.pass_bytes, 1));
+    // One pass slice per warp in shared memory; a slice too large for that runs from the profile
+    // in global memory.
+    const size_t budget = std::min<size_t>(BAND_SMEM_BUDGET, db->smem_limit - 16);
+    const bool gprof = qp.pass_bytes > budget;
+    int warps = gprof ? 32 : (int)std::min<size_t>(32, budget / std::max<uint32_t>(qp.pass_bytes, 1));
     warps = std::max(1, std::min(warps, std::max(qp.n_passes, 1)));
-    const size_t smem = (size_t)warps * qp.pass_bytes + 16;
+    const size_t smem = gprof ? 16 : (size_t)warps * qp.pass_bytes + 16;
     cudaError_t e = cudaErrorInvalidValue;
+#define HY_BAND_CASE(M)                                                                        \
+    case M:                                                                                    \
+        e = gprof ? launch_band_mode<A, M, true>(p, warps, smem, sc->stream)                   \
+                  : launch_band_mode<A, M, false>(p, warps, smem, sc->stream);                 \
+        break;
     switch (db->mode) {
-    case MODE_SW: e = launch_band_mode<A, MODE_SW>(p, warps, smem, sc->stream); break;
-    case MODE_NW: e = launch_band_mode<A, MODE_NW>(p, warps, smem, sc->stream); break;
-    case MODE_HW: e = launch_band_mode<A, MODE_HW>(p, warps, smem, sc->stream); break;
-    case MODE_OV: e = launch_band_mode<A, MODE_OV>(p, warps, smem, sc->stream); break;
-    case MODE_SHW: e = launch_band_mode<A, MODE_SHW>(p, warps, smem, sc->stream); break;
+        HY_BAND_CASE(MODE_SW)
+        HY_BAND_CASE(MODE_NW)
+        HY_BAND_CASE(MODE_HW)
+        HY_BAND_CASE(MODE_OV)
+        HY_BAND_CASE(MODE_SHW)
     }
+#undef HY_BAND_CASE
     HY_CK(e);
     sc->launches += qp.n_passes > 0 ? 2 : 1;
     return fail(HY_OK);
@@ -495,6 +535,11 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
 
     hy_db *db = new hy_db;
     cudaGetDevice(&db->device);
+    int smem_optin = 0;
+    if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, db->device) == cudaSuccess &&
+        smem_optin > 0)
+        db->smem_limit = (size_t)smem_optin;
+    cudaGetLastError();
     db->n_seqs = n_seqs;
     db->mql = max_query_len;
     db->max_t = max_t;

@@ -557,8 +557,10 @@ __device__ __forceinline__ void init_profile_bars(uint64_t *bars) {
 // mbarriers live in `smem` / `bars`; `phase` holds the parity each barrier waits for next (bit b
 // for barrier b) and is carried from unit to unit by a persistent caller. Every thread of the
 // block must call it with the same arguments. Returns false if a profile copy did not arrive in
-// time (the error flag is then set and the block must stop).
-template <class A, int G, int R, int MODE, bool ENDS>
+// time (the error flag is then set and the block must stop). With GPROF the lanes read the pass
+// slices straight from the profile in global memory (through L1) instead of shared memory: the
+// form for alphabets whose slices do not fit in shared memory; `smem` and `bars` are then unused.
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false>
 __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t item_first,
                                           const uint32_t item_end, uint8_t *smem, uint64_t *bars,
                                           uint32_t &phase) {
@@ -566,7 +568,7 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
     constexpr int RPP = G * R;
     static_assert(R % A::EPV == 0, "rows per lane must fill whole profile vectors");
     static_assert(32 % G == 0, "groups must tile a warp");
-    uint8_t *prof_buf[2] = {smem, smem + p.pass_bytes};
+    const uint8_t *prof_buf[2] = {smem, smem + p.pass_bytes};
 
     const int lane = threadIdx.x % G;
     const uint32_t item = item_first == NO_INDEX ? NO_INDEX : item_first + threadIdx.x / G;
@@ -590,37 +592,43 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
     V best = A::splat(0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
 
-    if (threadIdx.x == 0 && p.n_passes > 0) {
-        bulk_load(prof_buf[0], p.profile, p.pass_bytes, &bars[0]);
-        if (p.n_passes > 1) bulk_load(prof_buf[1], p.profile + p.pass_bytes, p.pass_bytes, &bars[1]);
+    if (!GPROF && threadIdx.x == 0 && p.n_passes > 0) {
+        bulk_load(smem, p.profile, p.pass_bytes, &bars[0]);
+        if (p.n_passes > 1) bulk_load(smem + p.pass_bytes, p.profile + p.pass_bytes, p.pass_bytes, &bars[1]);
     }
     for (int pass = 0; pass < p.n_passes; ++pass) {
         const int buf = pass & 1;
-        const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u);
-        phase ^= 1u << buf;
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicExch(p.err, 1);
-            return false;
+        const uint8_t *prof;
+        if (GPROF) {
+            prof = p.profile + (size_t)pass * p.pass_bytes;
+        } else {
+            const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u);
+            phase ^= 1u << buf;
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicExch(p.err, 1);
+                return false;
+            }
+            prof = prof_buf[buf];
         }
-        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof_buf[buf],
-                                        prof_buf[buf] + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
+        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof,
+                                        prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
                                         p.vrow0 + pass * RPP + lane * R, pass == 0,
                                         pass == p.n_passes - 1, bnd, p.qlen, p.go, p.ge, Sv, best,
                                         cand);
         __syncthreads();  // the profile buffer and boundary row are free again
-        if (threadIdx.x == 0 && pass + 2 < p.n_passes)
-            bulk_load(prof_buf[buf], p.profile + (size_t)(pass + 2) * p.pass_bytes, p.pass_bytes,
-                      &bars[buf]);
+        if (!GPROF && threadIdx.x == 0 && pass + 2 < p.n_passes)
+            bulk_load(smem + (size_t)buf * p.pass_bytes, p.profile + (size_t)(pass + 2) * p.pass_bytes,
+                      p.pass_bytes, &bars[buf]);
     }
     finish_item<A, G, MODE, ENDS>(lane, active, meta, p.qlen, p.go, p.ge, best, cand, p.scores,
                                   p.qend, p.tend, p.best_key);
     return true;
 }
 
-template <class A, int G, int R, int MODE, bool ENDS>
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false>
 __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
     extern __shared__ __align__(128) uint8_t smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)p.pass_bytes);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (GPROF ? 0 : 2 * (size_t)p.pass_bytes));
     const int gpb = blockDim.x / G;
     uint32_t first, end;
     if (p.item_ptr) {
@@ -635,7 +643,7 @@ __global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
     init_profile_bars(bars);
     __syncthreads();
     uint32_t phase = 0;
-    scan_unit<A, G, R, MODE, ENDS>(p, first, end, smem, bars, phase);
+    scan_unit<A, G, R, MODE, ENDS, GPROF>(p, first, end, smem, bars, phase);
 }
 
 // ---- the block-cooperative band kernel (one long item, with end positions) -------------------
@@ -651,7 +659,9 @@ constexpr int BAND_K = 32;
 // The band recovery of item `item` (a valid item of p.meta) by the whole block. `bar` is an
 // initialised mbarrier whose next wait parity is `phase`; the block's dynamic shared memory
 // (`smem`) holds W = blockDim/32 pass slices. Every thread of the block must call it.
-template <class A, int R, int MODE>
+// With GPROF the warps read their pass slices from the profile in global memory; `smem` and `bar`
+// are then unused.
+template <class A, int R, int MODE, bool GPROF = false>
 __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t item, uint8_t *smem,
                                           uint64_t *bar, uint32_t &phase) {
     typedef typename A::V V;
@@ -673,18 +683,21 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
     for (int round = 0; round < rounds; ++round) {
         const int first = round * W;
         const int cnt = min(W, p.n_passes - first);
-        if (threadIdx.x == 0)
-            bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
-        const bool ok = mbar_wait_bounded(bar, phase & 1u);
-        phase ^= 1u;
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicExch(p.err, 1);
-            return;
+        if (!GPROF) {
+            if (threadIdx.x == 0)
+                bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
+            const bool ok = mbar_wait_bounded(bar, phase & 1u);
+            phase ^= 1u;
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicExch(p.err, 1);
+                return;
+            }
         }
         const int pass = first + warp;
         const bool mine = warp < cnt && w > 0;
         const int32_t row0 = p.vrow0 + pass * RPP + lane * R;
-        const uint8_t *prof = smem + (size_t)warp * p.pass_bytes;
+        const uint8_t *prof = GPROF ? p.profile + (size_t)min(pass, p.n_passes - 1) * p.pass_bytes
+                                    : smem + (size_t)warp * p.pass_bytes;
         const uint8_t *prof_hi = prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES);
         Sweep<A, R> sw;
         sweep_begin<A, R, MODE>(sw, row0, p.go, p.ge, Sv);
@@ -739,20 +752,20 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
     }
 }
 
-template <class A, int R, int MODE>
+template <class A, int R, int MODE, bool GPROF = false>
 __global__ void __launch_bounds__(1024) band_kernel(const ScanParams p) {
     extern __shared__ __align__(128) uint8_t smem[];
     const uint32_t item = *p.item_ptr;
     if (item == NO_INDEX || item >= p.n_items) return;  // the same for every thread of the block
     const int W = blockDim.x / 32;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (size_t)W * p.pass_bytes);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + (GPROF ? 0 : (size_t)W * p.pass_bytes));
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     uint32_t phase = 0;
-    band_item<A, R, MODE>(p, item, smem, bar, phase);
+    band_item<A, R, MODE, GPROF>(p, item, smem, bar, phase);
 }
 
 // ---- the batched pairwise kernel (align_pairs) -----------------------------------------------
@@ -779,6 +792,10 @@ struct PairParams {
     int32_t *scores;
     int32_t *qend;
     int32_t *tend;
+    // Global-memory-profile form (alphabets whose group profiles do not fit in shared memory):
+    // group g of block b builds and reads its profile at gprof + (b * groups_per_block + g) *
+    // group_bytes.
+    uint8_t *gprof;
 };
 
 template <class A, int G, int R>
@@ -813,7 +830,7 @@ __device__ __forceinline__ void build_group_profile(uint8_t *dst, const uint8_t 
     }
 }
 
-template <class A, int G, int R, int MODE, bool ENDS>
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false>
 __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     typedef typename A::V V;
     constexpr int RPP = G * R;
@@ -838,7 +855,8 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     const uint8_t *qa = active ? p.q_res + p.qoff[2 * (size_t)item] : p.q_res;
     const uint8_t *qb = (active && A::NH > 1 && meta.idx[1] != NO_INDEX) ? p.q_res + p.qoff[2 * (size_t)item + 1] : qa;
     // The group's region: the low-half table of query a, then (int16x2) the high-half table of b.
-    uint8_t *gprof_a = smem + (size_t)gib * p.group_bytes;
+    uint8_t *gprof_a = GPROF ? p.gprof + ((size_t)blockIdx.x * (blockDim.x / G) + gib) * p.group_bytes
+                             : smem + (size_t)gib * p.group_bytes;
     uint8_t *gprof_b = gprof_a + (A::TABLES - 1) * (p.group_bytes / A::TABLES);
     const V Sv = A::splat(p.sentinel);
     const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;

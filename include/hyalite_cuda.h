@@ -171,8 +171,10 @@ hy_status hy_scan_scores_device(const hy_db *db, hy_scratch *scratch, const uint
  * buffers; the kernels' scratch is a fixed 16 MiB __device__ array inside this library, which
  * every GPU that loads the library holds until exit. A call needing more scratch than that (the
  * boundary rows of a multi-pass query grow with the database) returns HY_ERR_UNSUPPORTED with
- * detail {needed_bytes, limit}. Runs on `stream` (a cudaStream_t, or NULL for the legacy default
- * stream) and returns once the scores are written. Calls share the array: calls whose kernels
+ * detail {needed_bytes, limit}; so does an alphabet whose query-profile slices do not fit in the
+ * device's shared memory (about 54 letters and up; hy_scan_scores handles those). Runs on
+ * `stream` (a cudaStream_t, or NULL for the legacy default stream) and returns once the scores
+ * are written. Calls share the array: calls whose kernels
  * overlap on the GPU race and must be serialised by the caller. The query's symbols must already
  * be validated (hy_query_validate); the current device must be the database's. */
 hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_query, uint64_t qlen,

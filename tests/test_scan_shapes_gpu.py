@@ -90,3 +90,53 @@ def test_large_database_properties_and_sampled_parity():
     # The self-query ties: sequence 5000 and its three copies score the same; 5000 wins.
     hit = db.scan(sc, src)
     assert hit.db_index == 5000
+
+
+@pytest.mark.parametrize("al", [64, 200, 255])
+def test_large_alphabets_read_the_profile_from_global_memory(al):
+    # Alphabets whose query-profile slices do not fit in shared memory at every launch shape: the
+    # bulk pairs drop to 8 rows per lane or read the profile from global memory, and so do the
+    # int32 items and the winner's-ends recovery. Entries up to 60 put the long targets in int32.
+    rng = np.random.default_rng(400 + al)
+    mat = [int(v) for v in rng.integers(-20, 61, al * al)]
+    seqs = rand_seqs(rng, 50, al, 1, 300) + rand_seqs(rng, 2, al, 2100, 3100)
+    queries = [list(rng.integers(0, al, n)) for n in (1, 50, 300, 700)]
+    for mode in (0, 1, 3):
+        for st in (0, 1):
+            db = check(seqs, mat, al, 5, 1, mode, st, queries, mql=700)
+    n16, n32 = db.partition()
+    assert n32 > 0
+
+
+def test_large_alphabet_pairs_keep_group_profiles_in_global_memory():
+    rng = np.random.default_rng(77)
+    al = 200
+    mat = [int(v) for v in rng.integers(-6, 9, al * al)]
+    qs = [list(rng.integers(0, al, int(rng.integers(0, 200)))) for _ in range(120)]
+    ts = [list(rng.integers(0, al, int(rng.integers(0, 300)))) for _ in range(120)]
+    for mode in (0, 2, 4):
+        out = []
+        hy.align_pairs(list(zip(qs, ts)), hy.Scoring(al, mat, 5, 1), hy.Mode(mode), hy.SearchType.ScoreEnd, out)
+        status, want, _ = o.align_pairs(qs, ts, mat, al, 5, 1, mode, 1)
+        assert status == 0
+        assert [(h.score, h.db_index, h.query_end, h.target_end) for h in out] == want
+
+
+def test_noalloc_rejects_an_alphabet_beyond_shared_memory():
+    import ctypes as C
+
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(5)
+    al = 120
+    mat = [int(v) for v in rng.integers(-4, 5, al * al)]
+    seqs = rand_seqs(rng, 20, al, 1, 100)
+    db = build(seqs, mat, al, 5, 1, 0, 0, 600)
+    qh = rng.integers(0, al, 600).astype(np.uint8)
+    q = torch.from_numpy(qh).cuda()
+    out = torch.zeros(20, dtype=torch.int32, device="cuda")
+    st = hy._abi.lib.hy_scan_scores_noalloc(db._h, C.c_void_p(q.data_ptr()), 600, C.c_void_p(out.data_ptr()),
+                                            C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert hy.Error.from_status(st).kind == "Unsupported"
+    # The allocating scan handles it.
+    want = o.OracleDb(seqs, mat, al, 5, 1, 0, 0).scan_scores(list(qh))
+    assert np.array_equal(db.scan_scores_array(hy.Scratch(db), qh), want)
