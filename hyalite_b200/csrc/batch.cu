@@ -50,7 +50,7 @@ struct BandLaunch {
 };
 
 __device__ __forceinline__ void class_range(const BatchQuery &bq, int cls, uint32_t &lo, uint32_t &hi) {
-    if (cls == BC_LONG) {
+    if (cls == BC_LONG || cls == BC_TLONG) {
         lo = bq.k0;
         hi = bq.kl;
     } else if (cls == BC_I32) {
@@ -128,7 +128,17 @@ __global__ void batch_profile_kernel(const BatchQuery *queries, const BatchCtl *
     const int32_t lim32 = 536870911;
     switch (kind) {
     case PK_BULK:
-        if (bq.bulk_rows == 8)
+        if (bq.tab) {
+            if (bq.bulk_rows == 8)
+                build_profile_words<PairTab16, MAIN_G, 8>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                          sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+            else if (bq.bulk_rows == 16)
+                build_profile_words<PairTab16, MAIN_G, 16>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                           sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+            else
+                build_profile_words<PairTab16, MAIN_G, 32>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                           sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        } else if (bq.bulk_rows == 8)
             build_profile_words<Pair16, MAIN_G, 8>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
                                                    sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
         else if (bq.bulk_rows == 16)
@@ -139,8 +149,12 @@ __global__ void batch_profile_kernel(const BatchQuery *queries, const BatchCtl *
                                                     sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
         break;
     case PK_W16:
-        build_profile_words<Pair16, LCG, LCR>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
-                                              sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        if (bq.tab)
+            build_profile_words<PairTab16, LCG, LCR>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                     sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
+        else
+            build_profile_words<Pair16, LCG, LCR>(bq.q, bq.matrix, bq.al, sp.go, bq.lim16, bq.top_free,
+                                                  sp.vrow0, sp.n_passes, (uint32_t *)out, first, stride);
         break;
     case PK_I32:
         build_profile_words<Single32, ICG, ICR>(bq.q, bq.matrix, bq.al, sp.go, lim32, bq.top_free,
@@ -170,7 +184,7 @@ __global__ void __launch_bounds__(1024) batch_band_kernel(const BandLaunch L) {
     const bool packed = r / 2 >= bq.k0;
     uint32_t item;
     if (A::NH == 2) {
-        if (!packed) return;
+        if (!packed || (bq.tab != 0) != A::PAIRTAB) return;
         item = r / 2;
     } else {
         if (packed) return;
@@ -238,6 +252,7 @@ struct QueryKinds {
 };
 
 static void plan_kinds(const hy_db *db, uint64_t qlen, bool ends, const BatchConfig &cfg, QueryKinds &k) {
+    const bool tab = db->layout == HY_LAYOUT_PRECOMPUTED;
     k.split = split_for_query(db, qlen, cfg.long_w);
     k.rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
     const QuerySplit &sp = k.split;
@@ -249,7 +264,9 @@ static void plan_kinds(const hy_db *db, uint64_t qlen, bool ends, const BatchCon
     k.bytes = 0;
     for (int i = 0; i < PK_N; ++i) {
         const bool i16 = i == PK_BULK || i == PK_W16;
-        k.qp[i] = plan(qlen, rpp[i], db->al, i16 ? profile_row_bytes<Pair16>() : profile_row_bytes<Single32>());
+        k.qp[i] = !i16 ? plan_for<Single32>(qlen, rpp[i], db->al)
+                  : tab ? plan_for<PairTab16>(qlen, rpp[i], db->al)
+                        : plan_for<Pair16>(qlen, rpp[i], db->al);
         if (k.need[i]) k.bytes += align128((size_t)k.qp[i].pass_bytes * k.qp[i].n_passes);
     }
 }
@@ -288,12 +305,16 @@ static hy_status record_graph_body(hy_batch *b) {
     HB_CK(cudaEventRecord(b->ev_fork, b->stream));
     HB_CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     launch_class<Pair16, LCG, LCR, PK_W16>(b, BC_LONG, b->d_bnd_side, b->stride_side, b->side);
+    launch_class<PairTab16, LCG, LCR, PK_W16>(b, BC_TLONG, b->d_bnd_side, b->stride_side, b->side);
     launch_class<Single32, ICG, ICR, PK_I32>(b, BC_I32, b->d_bnd_side, b->stride_side, b->side);
     HB_CK(cudaGetLastError());
     HB_CK(cudaEventRecord(b->ev_join, b->side));
     launch_class<Pair16, MAIN_G, 32, PK_BULK>(b, BC_BULK32, b->d_bnd_bulk, b->stride_bulk, b->stream);
     launch_class<Pair16, MAIN_G, 16, PK_BULK>(b, BC_BULK16, b->d_bnd_bulk, b->stride_bulk, b->stream);
     launch_class<Pair16, MAIN_G, 8, PK_BULK>(b, BC_BULK8, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<PairTab16, MAIN_G, 32, PK_BULK>(b, BC_TBULK32, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<PairTab16, MAIN_G, 16, PK_BULK>(b, BC_TBULK16, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<PairTab16, MAIN_G, 8, PK_BULK>(b, BC_TBULK8, b->d_bnd_bulk, b->stride_bulk, b->stream);
     HB_CK(cudaGetLastError());
     HB_CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
     BandLaunch bl;
@@ -303,11 +324,12 @@ static hy_status record_graph_body(hy_batch *b) {
     bl.bnd_stride = b->stride_band;
     bl.ends = b->d_ends;
     batch_band_kernel<Pair16, PK_W16><<<b->max_queries, b->band_threads, b->band_smem, b->stream>>>(bl);
+    batch_band_kernel<PairTab16, PK_W16><<<b->max_queries, b->band_threads, b->band_smem, b->stream>>>(bl);
     batch_band_kernel<Single32, PK_W32><<<b->max_queries, b->band_threads, b->band_smem, b->stream>>>(bl);
     batch_finalize_kernel<<<(b->max_queries + 127) / 128, 128, 0, b->stream>>>(b->d_queries, b->d_ctl,
                                                                                b->d_ends, b->d_hits);
     HB_CK(cudaGetLastError());
-    b->kernels_per_run = 10;
+    b->kernels_per_run = 15;
     return fail(HY_OK);
 }
 
@@ -404,6 +426,7 @@ hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const Bat
         bq.top_free = (db->mode == MODE_SW || db->mode == MODE_HW || db->mode == MODE_OV) ? 1 : 0;
         bq.al = (int32_t)db->al;
         bq.lim16 = 32767 - db->go;
+        bq.tab = db->layout == HY_LAYOUT_PRECOMPUTED ? 1 : 0;
         bq.k0 = sp.k0;
         bq.kl = sp.kl;
         bq.n_i32 = sp.n_i32;
@@ -430,14 +453,16 @@ hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const Bat
             prof_off += align128((size_t)p.pass_bytes * p.n_passes);
         }
         q_off += qlen;
-        const int bulk_cls = k.rows == 8 ? BC_BULK8 : k.rows == 16 ? BC_BULK16 : BC_BULK32;
+        const int bulk_cls = (k.rows == 8 ? BC_BULK8 : k.rows == 16 ? BC_BULK16 : BC_BULK32) +
+                             (bq.tab ? BC_TBULK8 - BC_BULK8 : 0);
+        const int long_cls = bq.tab ? BC_TLONG : BC_LONG;
         if (sp.kl < db->p16.n_items) {
             lists[bulk_cls].push_back(i);
             ctl.n_chunks[bulk_cls] = std::max<uint32_t>(ctl.n_chunks[bulk_cls], (db->p16.n_items + 31) / 32);
         }
         if (sp.kl > sp.k0) {
-            lists[BC_LONG].push_back(i);
-            ctl.n_chunks[BC_LONG] = std::max<uint32_t>(ctl.n_chunks[BC_LONG], (sp.kl + 7) / 8);
+            lists[long_cls].push_back(i);
+            ctl.n_chunks[long_cls] = std::max<uint32_t>(ctl.n_chunks[long_cls], (sp.kl + 7) / 8);
         }
         if (sp.n_i32 > 0) {
             lists[BC_I32].push_back(i);
@@ -622,8 +647,19 @@ hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_que
     const size_t sm_bulk8 = 128 + 2 * pass_bytes_of(al, MAIN_G * 8, pb16);
     const size_t sm_long = 128 + 2 * pass_bytes_of(al, LCG * LCR, pb16);
     const size_t sm_i32 = 128 + 2 * pass_bytes_of(al, ICG * ICR, pb32);
-    const size_t band_pass = std::max(pass_bytes_of(al, WIN_G * WIN_R, pb16), pass_bytes_of(al, WIN_G * WIN_R, pb32));
-    if (st == HY_OK && (std::max({sm_bulk32, sm_long, sm_i32}) > (size_t)smem_optin ||
+    // The Precomputed classes size their pair tables by the largest alphabet among the
+    // Precomputed databases (0 letters when there is none: those classes then never run).
+    int32_t al_tab = -1;
+    for (const hy_db *db : b->dbs)
+        if (db->layout == HY_LAYOUT_PRECOMPUTED) al_tab = std::max<int32_t>(al_tab, (int32_t)db->al);
+    const size_t tab_row = al_tab < 0 ? 0 : profile_slice_row_bytes<PairTab16>(al_tab);
+    const size_t sm_tbulk32 = 128 + 2 * tab_row * MAIN_G * 32;
+    const size_t sm_tbulk16 = 128 + 2 * tab_row * MAIN_G * 16;
+    const size_t sm_tbulk8 = 128 + 2 * tab_row * MAIN_G * 8;
+    const size_t sm_tlong = 128 + 2 * tab_row * LCG * LCR;
+    const size_t band_pass = std::max({pass_bytes_of(al, WIN_G * WIN_R, pb16), pass_bytes_of(al, WIN_G * WIN_R, pb32),
+                                       tab_row * WIN_G * WIN_R});
+    if (st == HY_OK && (std::max({sm_bulk32, sm_long, sm_i32, sm_tbulk32, sm_tlong}) > (size_t)smem_optin ||
                         128 + band_pass > (size_t)smem_optin)) {
         st = fail(HY_ERR_UNSUPPORTED, al, smem_optin);
     }
@@ -633,12 +669,17 @@ hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_que
         ck(prepare_class<Pair16, MAIN_G, 32, PK_BULK>(b, BC_BULK32, sm_bulk32, n_sm));
         ck(prepare_class<Pair16, LCG, LCR, PK_W16>(b, BC_LONG, sm_long, n_sm));
         ck(prepare_class<Single32, ICG, ICR, PK_I32>(b, BC_I32, sm_i32, n_sm));
+        ck(prepare_class<PairTab16, MAIN_G, 8, PK_BULK>(b, BC_TBULK8, sm_tbulk8, n_sm));
+        ck(prepare_class<PairTab16, MAIN_G, 16, PK_BULK>(b, BC_TBULK16, sm_tbulk16, n_sm));
+        ck(prepare_class<PairTab16, MAIN_G, 32, PK_BULK>(b, BC_TBULK32, sm_tbulk32, n_sm));
+        ck(prepare_class<PairTab16, LCG, LCR, PK_W16>(b, BC_TLONG, sm_tlong, n_sm));
         int warps = (int)std::min<size_t>(32, BAND_SMEM_BUDGET / std::max<size_t>(band_pass, 1));
         warps = std::max(1, warps);
         b->band_threads = 32 * warps;
         b->band_smem = 128 + (size_t)warps * band_pass;
         ck(cudaFuncSetAttribute(batch_band_kernel<Pair16, PK_W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->band_smem));
         ck(cudaFuncSetAttribute(batch_band_kernel<Single32, PK_W32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->band_smem));
+        ck(cudaFuncSetAttribute(batch_band_kernel<PairTab16, PK_W16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->band_smem));
     }
     // Boundary regions: a block's unit spans at most IPU items of the class's widest width.
     const bool multipass = b->mql_max > (uint64_t)MAIN_G * 8;
@@ -646,11 +687,13 @@ hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_que
     b->stride_bulk = multipass ? align128(32 * w_bulk * 2 * sizeof(uint32_t)) : 128;
     b->stride_side = multipass ? align128(8 * (b->max_t + 16) * 2 * sizeof(uint32_t)) : 128;
     b->stride_band = align128((b->max_t + 16) * 2 * sizeof(uint32_t));
-    const int side_grid = std::max(b->grid[BC_LONG], b->grid[BC_I32]);
-    const int bulk_grid = std::max({b->grid[BC_BULK8], b->grid[BC_BULK16], b->grid[BC_BULK32]});
+    const int side_grid = std::max({b->grid[BC_LONG], b->grid[BC_I32], b->grid[BC_TLONG]});
+    const int bulk_grid = std::max({b->grid[BC_BULK8], b->grid[BC_BULK16], b->grid[BC_BULK32],
+                                    b->grid[BC_TBULK8], b->grid[BC_TBULK16], b->grid[BC_TBULK32]});
     const uint64_t mq = b->mql_max;
-    const uint64_t per_query = align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +  // bulk, any rows
-                               align128(pass_bytes_of(al, 1, pb16) * (mq + 255)) +  // long / band int16x2
+    const uint64_t pair_row = std::max<uint64_t>(pass_bytes_of(al, 1, pb16), tab_row);
+    const uint64_t per_query = align128(pair_row * (mq + 255)) +                   // bulk, any rows
+                               align128(pair_row * (mq + 255)) +                   // long / band int16x2
                                align128(pass_bytes_of(al, 1, pb32) * (mq + 511)) +  // int32
                                align128(pass_bytes_of(al, 1, pb32) * (mq + 255));   // band int32
     b->prof_cap = prof_cap ? prof_cap : per_query * max_queries;

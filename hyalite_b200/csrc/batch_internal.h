@@ -10,8 +10,12 @@
 
 namespace hy {
 
-// Launch classes (one persistent kernel each) and profile kinds (one query profile each).
-enum { BC_BULK8 = 0, BC_BULK16 = 1, BC_BULK32 = 2, BC_LONG = 3, BC_I32 = 4, BC_N = 5 };
+// Launch classes (one persistent kernel each; the T classes run databases of the Precomputed
+// layout) and profile kinds (one query profile each).
+enum {
+    BC_BULK8 = 0, BC_BULK16 = 1, BC_BULK32 = 2, BC_LONG = 3, BC_I32 = 4,
+    BC_TBULK8 = 5, BC_TBULK16 = 6, BC_TBULK32 = 7, BC_TLONG = 8, BC_N = 9
+};
 enum { PK_BULK = 0, PK_W16 = 1, PK_I32 = 2, PK_W32 = 3, PK_N = 4 };
 
 // One query slot of a batch, as the device kernels read it.
@@ -22,6 +26,7 @@ struct BatchQuery {
     const uint8_t *q;
     const uint32_t *rank;
     int32_t qlen, mode, ends, bulk_rows, top_free, al, lim16;
+    int32_t tab;  // the database's pair columns are Precomputed codes (PairTab16)
     uint32_t k0, kl, n_i32, n16;
 };
 
@@ -71,8 +76,8 @@ struct hy_batch {
     int32_t *d_ends = nullptr;
     hy_hit *d_hits = nullptr, *h_hits = nullptr;
     int *d_err = nullptr, *h_err = nullptr;
-    int grid[hy::BC_N] = {0, 0, 0, 0, 0};
-    size_t smem[hy::BC_N] = {0, 0, 0, 0, 0};
+    int grid[hy::BC_N] = {};
+    size_t smem[hy::BC_N] = {};
     int band_threads = 32;
     size_t band_smem = 0;
     cudaGraphExec_t exec = nullptr;

@@ -59,6 +59,14 @@ inline QueryPlan plan(uint64_t qlen, int rpp, uint64_t al, size_t pe) {
     return q;
 }
 
+// The plan of lane arithmetic A (its profile has A::letters(al) letters per table).
+template <class A>
+inline QueryPlan plan_for(uint64_t qlen, int rpp, uint64_t al) {
+    QueryPlan q = plan(qlen, rpp, al, profile_row_bytes<A>());
+    q.pass_bytes = (uint32_t)(profile_slice_row_bytes<A>((int64_t)al) * (uint64_t)rpp);
+    return q;
+}
+
 }  // namespace hy
 
 struct hy_db {

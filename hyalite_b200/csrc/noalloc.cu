@@ -82,7 +82,7 @@ template <class A, int G, int R>
 Region plan_region(const hy_db *db, const Partition &part, uint64_t qlen, size_t &cursor) {
     Region r;
     if (!part.n_items) return r;
-    r.qp = plan(qlen, G * R, db->al, profile_row_bytes<A>());
+    r.qp = plan_for<A>(qlen, G * R, db->al);
     r.prof_off = cursor;
     r.prof_bytes = (size_t)r.qp.n_passes * r.qp.pass_bytes;
     cursor = align256(cursor + r.prof_bytes);
@@ -99,7 +99,7 @@ hy_status run_partition(const hy_db *db, const Partition &part, uint32_t item_ba
     if (item_base >= item_end) return fail(HY_OK);
     const bool i16 = A::NH == 2;
     const int32_t lim = i16 ? 32767 - db->go : 536870911;
-    const int64_t total = (int64_t)(db->al + 1) * G * R * rg.qp.n_passes;
+    const int64_t total = A::letters(db->al) * A::TABLES * G * R * rg.qp.n_passes;
     const bool top_free = db->mode == MODE_SW || db->mode == MODE_HW || db->mode == MODE_OV;
     if (total > 0) {
         int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
@@ -148,7 +148,9 @@ extern "C" hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_qu
     if (device != db->device) return fail(HY_ERR_INVALID_ARGUMENT);
     // Lay out this call's scratch: the timeout flag, then profile and boundary rows per partition.
     size_t cursor = 256;
-    const Region r16 = plan_region<Pair16, MAIN_G, MAIN_R16>(db, db->p16, qlen, cursor);
+    const bool tab = db->layout == HY_LAYOUT_PRECOMPUTED;
+    const Region r16 = tab ? plan_region<PairTab16, MAIN_G, MAIN_R16>(db, db->p16, qlen, cursor)
+                           : plan_region<Pair16, MAIN_G, MAIN_R16>(db, db->p16, qlen, cursor);
     const Region r32 = plan_region<Single32, MAIN_G32, MAIN_R32>(db, db->p32, qlen, cursor);
     if (cursor > NOALLOC_SCRATCH_BYTES)
         return fail(HY_ERR_UNSUPPORTED, (int64_t)cursor, (int64_t)NOALLOC_SCRATCH_BYTES);
@@ -165,7 +167,9 @@ extern "C" hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_qu
     if (e != cudaSuccess) return fail(HY_ERR_CUDA, e);
     // The same per-query split as hy_scan_scores: pairs [k0, n) packed, the 2*k0 longest in int32.
     const QuerySplit split = split_for_query(db, qlen);
-    st = run_partition<Pair16, MAIN_G, MAIN_R16>(db, db->p16, split.k0, db->p16.n_items, r16, base,
+    st = tab ? run_partition<PairTab16, MAIN_G, MAIN_R16>(db, db->p16, split.k0, db->p16.n_items, r16, base,
+                                                d_query, qlen, d_scores, d_err, s)
+             : run_partition<Pair16, MAIN_G, MAIN_R16>(db, db->p16, split.k0, db->p16.n_items, r16, base,
                                                 d_query, qlen, d_scores, d_err, s);
     if (st != HY_OK) return st;
     st = run_partition<Single32, MAIN_G32, MAIN_R32>(db, db->p32, 0, split.n_i32, r32, base, d_query,

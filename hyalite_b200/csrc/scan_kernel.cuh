@@ -142,6 +142,44 @@ struct Pair16 {
         const uint32_t h = (uint16_t)(int16_t)v;
         return t ? (h << 16) : h;
     }
+    // Profile letters of an alphabet of `al` symbols (the padding symbol included).
+    static constexpr bool PAIRTAB = false;
+    __host__ __device__ static constexpr int64_t letters(int64_t al) { return al + 1; }
+    // Residue code of a pair column (low sequence's symbol lo, high sequence's hi).
+    __host__ __device__ static constexpr uint32_t code(uint32_t lo, uint32_t hi, uint32_t) { return lo | (hi << 8); }
+};
+
+// The Precomputed layout (src/inter.rs:317-330: "a precomputed score table, so each cell's
+// substitution vector is a direct load with no gather"), restated for the device: the database
+// stores each pair column as one code c = lo * (al + 1) + hi, and the pass's profile is a single
+// table indexed by (c, query row) whose word already holds both halves' substitution values. A
+// cell pair then costs one profile load and one add instead of two of each; the table has
+// (al + 1)^2 letters, so it is compact for small alphabets only. Arithmetic as Pair16.
+struct PairTab16 : Pair16 {
+    static constexpr int TABLES = 1;
+    static constexpr bool PAIRTAB = true;
+    __host__ __device__ static constexpr int64_t letters(int64_t al) { return (al + 1) * (al + 1); }
+    __host__ __device__ static constexpr uint32_t code(uint32_t lo, uint32_t hi, uint32_t al) {
+        return lo * (al + 1) + hi;
+    }
+    __device__ __forceinline__ static V diag(V g, V p, V) { return __vadd2(g, p); }
+    __device__ __forceinline__ static void residues(RES r, int &a, int &b) {
+        a = r;
+        b = 0;
+    }
+    template <int R, int G>
+    __device__ __forceinline__ static void load_chunk(const uint8_t *prof, const uint8_t *, int c,
+                                                      int, int lane, int k, V (&pa)[EPV],
+                                                      V (&pb)[EPV]) {
+        constexpr int KCH = R / EPV;
+        const uint4 A = reinterpret_cast<const uint4 *>(prof)[((size_t)c * KCH + k) * G + lane];
+        pa[0] = A.x; pa[1] = A.y; pa[2] = A.z; pa[3] = A.w;
+        pb[0] = pb[1] = pb[2] = pb[3] = 0;
+    }
+    // The word of a pair code's two values (low half: the low sequence's).
+    __host__ __device__ __forceinline__ static PE pair_word(int64_t lo, int64_t hi) {
+        return (uint32_t)(uint16_t)(int16_t)lo | ((uint32_t)(uint16_t)(int16_t)hi << 16);
+    }
 };
 
 struct Single32 {
@@ -183,12 +221,20 @@ struct Single32 {
         pb[0] = pb[1] = pb[2] = pb[3] = 0;
     }
     __host__ __device__ __forceinline__ static PE word(int64_t v, int) { return (PE)v; }
+    static constexpr bool PAIRTAB = false;
+    __host__ __device__ static constexpr int64_t letters(int64_t al) { return al + 1; }
 };
 
 // Profile bytes per (letter, query row) of one lane arithmetic: every table's word.
 template <class A>
-constexpr size_t profile_row_bytes() {
+__host__ __device__ constexpr size_t profile_row_bytes() {
     return A::TABLES * sizeof(typename A::PE);
+}
+
+// Profile bytes of one query row of a pass slice: every letter of every table.
+template <class A>
+__host__ __device__ constexpr size_t profile_slice_row_bytes(int64_t al) {
+    return (size_t)A::letters(al) * profile_row_bytes<A>();
 }
 
 // ---- small helpers -------------------------------------------------------------------------
@@ -906,7 +952,7 @@ __device__ __forceinline__ void build_profile_words(const uint8_t *q, const int3
                                                     int64_t stride) {
     static_assert(R % A::EPV == 0 && R >= A::EPV, "rows per lane must fill whole profile vectors");
     constexpr int KCH = R / A::EPV;
-    const int64_t per_table = (int64_t)(al + 1) * G * R;
+    const int64_t per_table = A::letters(al) * G * R;
     const int64_t per_pass = per_table * A::TABLES;
     const int64_t total = per_pass * n_passes;
     for (int64_t i = first; i < total; i += stride) {
@@ -921,18 +967,19 @@ __device__ __forceinline__ void build_profile_words(const uint8_t *q, const int3
         const int letter = (int)(rem / KCH);
         const int64_t row = vrow0 + pass * (G * R) + (int64_t)lane * R + k * A::EPV + e;
         const int64_t pad = -(int64_t)lim - 1 + go;
-        int64_t v;
-        if (row <= 0) {
-            v = top_free ? go : 0;
-        } else if (letter == al) {
-            v = pad;
-        } else {
-            int64_t sub = matrix[(int64_t)q[row - 1] * al + letter];
+        // Profile value of target symbol l at this row.
+        auto value = [&](int l) -> int64_t {
+            if (row <= 0) return top_free ? go : 0;
+            if (l == al) return pad;
+            int64_t sub = matrix[(int64_t)q[row - 1] * al + l];
             if (sub < -(int64_t)lim - 1) sub = -(int64_t)lim - 1;
             if (sub > lim) sub = lim;
-            v = sub + go;
-        }
-        out[i] = A::word(v, table);
+            return sub + go;
+        };
+        if constexpr (A::PAIRTAB)
+            out[i] = A::pair_word(value(letter / (al + 1)), value(letter % (al + 1)));
+        else
+            out[i] = A::word(value(letter), table);
     }
 }
 
