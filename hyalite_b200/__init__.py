@@ -157,8 +157,9 @@ class BackendChoice:
 
 
 class Layout(enum.IntEnum):
-    """src/inter.rs:317-330. On the device: Gathered interleaves two per-letter query profiles per
-    cell pair."""
+    """src/inter.rs:317-330. On the device: Gathered adds two per-letter query-profile words per
+    cell pair; Precomputed stores each pair column as one code and loads one pair-table word (Auto
+    picks it for alphabets of at most 6 symbols). Results never depend on the layout."""
     Gathered = 0
     Precomputed = 1
 
