@@ -195,15 +195,17 @@ def run_cuda(args):
             if st != 0:
                 raise hy.Error.from_status(st)
 
+    # This rank's shard is global sequences [rank * n_seqs, (rank + 1) * n_seqs).
+    local_to_global = torch.arange(n_seqs, dtype=torch.int64, device=f"cuda:{local}") + rank * n_seqs
+
     def gather_best(hits_dev):
+        """The per-query best hits of all shards, merged on the device (one all_gather)."""
         if world == 1:
             return hits_dev
-        import torch.distributed as dist
+        from hyalite_b200 import sharded
 
-        out = [torch.empty_like(hits_dev) for _ in range(world)]
         with torch.cuda.stream(stream):
-            dist.all_gather(out, hits_dev)
-        return out
+            return sharded.all_gather_best(sharded.device_hit_rows(hits_dev, local_to_global))
 
     def barrier():
         if world > 1:
@@ -252,13 +254,10 @@ def run_cuda(args):
     for _ in range(args.steps):
         hits = [db.scan(sc, q) for q in host_queries]
         if world > 1:
-            import torch.distributed as dist
+            from hyalite_b200 import sharded
 
-            hb = torch.tensor([[h.score, h.db_index + rank * n_seqs] for h in hits], dtype=torch.int64,
-                              device=f"cuda:{local}")
-            allh = [torch.empty_like(hb) for _ in range(world)]
-            dist.all_gather(allh, hb)
-            _ = [max(((int(a[i, 0]), -int(a[i, 1])) for a in allh)) for i in range(N_QUERIES)]
+            rows = sharded.hit_rows(hits, np.arange(n_seqs) + rank * n_seqs).to(f"cuda:{local}")
+            hits = sharded.all_gather_best(rows).cpu()
     e2e_s = time.perf_counter() - t0
     if world > 1:
         import torch.distributed as dist

@@ -114,3 +114,63 @@ def test_batch_validation_reports_the_first_failing_query():
     assert e.value.kind == "InvalidArgument"
     # The batch still works after the errors.
     assert hit_tuple(batch.scan([[0, 1, 2, 3]], [0])[0]) == o.OracleDb(seqs, DNA, 4, 2, 1, 0, 1).scan([0, 1, 2, 3])
+
+
+def test_sharded_database_single_rank_equals_the_plain_scan():
+    # ShardedDatabase over one gloo rank (the exchange runs, with one participant).
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from hyalite_b200 import sharded
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        rng = np.random.default_rng(15)
+        seqs = rand_seqs(rng, 500, 20, 1, 300)
+        mat = [int(v) for v in rng.integers(-4, 12, 400)]
+        conf = lambda b: b.scoring(hy.Scoring(20, mat, 11, 1)).mode(hy.Mode.Sw).search_type(
+            hy.SearchType.ScoreEnd).max_query_len(400)
+        sdb = sharded.ShardedDatabase(seqs, conf)
+        plain = build(seqs, mat, 20, 11, 1, 0, 1, 400)
+        sc, sc2 = hy.Scratch(sdb.db), hy.Scratch(plain)
+        for L in (0, 40, 400):
+            q = list(rng.integers(0, 20, L))
+            assert sdb.scan(sc, q) == plain.scan(sc2, q)
+            assert np.array_equal(sdb.scan_scores(sc, q), plain.scan_scores_array(sc2, q))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_device_hit_rows_match_the_host_hits():
+    import ctypes as C
+
+    import torch
+
+    from hyalite_b200 import sharded
+
+    rng = np.random.default_rng(16)
+    seqs = rand_seqs(rng, 300, 20, 1, 300)
+    mat = [int(v) for v in rng.integers(-4, 12, 400)]
+    db = build(seqs, mat, 20, 11, 1, 0, 1, 300)
+    sc = hy.Scratch(db)
+    queries = [list(rng.integers(0, 20, L)) for L in (0, 30, 300)]
+    d_hits = torch.zeros((len(queries), 32), dtype=torch.uint8, device="cuda")
+    for i, q in enumerate(queries):
+        d_q = torch.tensor(q if q else [0], dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        st = hy._abi.lib.hy_scan_device(db._h, sc._h, C.c_void_p(d_q.data_ptr()), len(q),
+                                        C.c_void_p(d_hits[i].data_ptr()))
+        assert st == 0
+        lib_sync = hy._abi.lib.hy_scratch_sync(sc._h)
+        assert lib_sync == 0
+    g = torch.arange(len(seqs), dtype=torch.int64, device="cuda") + 1000
+    rows = sharded.device_hit_rows(d_hits, g).cpu()
+    want = sharded.hit_rows([db.scan(sc, q) for q in queries], np.arange(len(seqs)) + 1000)
+    assert torch.equal(rows, want)
