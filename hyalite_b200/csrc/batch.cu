@@ -62,17 +62,10 @@ __device__ __forceinline__ void class_range(const BatchQuery &bq, int cls, uint3
     }
 }
 
-// Resident 256-thread blocks per SM each launch shape is compiled for (its register budget): the
-// plain scan kernels of the same shapes reach these occupancies.
-template <class A, int G, int R>
-constexpr int batch_min_blocks() {
-    return A::NH == 1 ? 2 : (G == 8 && R == 8) ? 4 : (G == 8 && R == 32) ? 2 : 3;
-}
-
 // One persistent kernel per launch class: blocks take units off the class queue until it is empty.
 // Shared memory: the two profile mbarriers, then two pass slices of the largest pass of the batch.
 template <class A, int G, int R, int PK>
-__global__ void __launch_bounds__(256, batch_min_blocks<A, G, R>()) batch_scan_kernel(const ClassLaunch L) {
+__global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) batch_scan_kernel(const ClassLaunch L) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ uint32_t s_unit;
     constexpr uint32_t IPU = 256 / G;  // items per unit: one per group of the block

@@ -13,12 +13,13 @@
 //   E[i][j] = max(E[i][j-1] - ge, H[i][j-1] - go)
 //   F[i][j] = max(F[i-1][j] - ge, H[i-1][j] - go)
 //   H[i][j] = max(H[i-1][j-1] + sub(q_i, t_j), E[i][j], F[i][j])   (SW: also max with 0)
-// carried as G = H - go so every cell costs five DPX operations:
-//   E = max(E + (-ge), G_left)           __viaddmax
-//   F = max(F + (-ge), G_up)             __viaddmax
-//   T = max(E, F)                        __vimax (SW: __vimax_relu)
-//   H = max(G_diag + P, T)               __viaddmax, P = sub + go from the profile
-//   G = H + (-go)                        __viaddmax against the type minimum
+// carried as G = H - go, with the profile holding P = sub + go so that G_diag + P = H_diag + sub:
+//   E = max(E + (-ge), G_left)           __viaddmax            (ALU pipe)
+//   F = max(F + (-ge), G_up)             __viaddmax            (ALU)
+//   d = G_diag + P                       __vadd2 (x2 for the two Gathered tables)   (FMA pipe)
+//   H = max(d, E, F)                     __vimax3 (SW: __vimax3_relu)               (ALU)
+//   G = H + (-go)                        __vadd2               (FMA)
+// For SW scores the row-to-row chain is shortened to one op (see sweep_step).
 // Width safety: the host routes a sequence to Pair16 only when its magnitude bound plus gap_open
 // fits int16 (bound + go <= 32767), which keeps every intermediate above exactly representable,
 // so the packed arithmetic never wraps on a real cell and the results equal the i32 oracle.
@@ -375,7 +376,9 @@ struct SweepConst {
 
 // One step s of one lane. CHECKED steps test whether the lane's column is inside [1, w]; the
 // caller runs unchecked steps only where every lane of the warp is live.
-template <class A, int G, int R, int MODE, bool ENDS, bool CHECKED>
+// With PRE the step's residue code and (lane 0) boundary-row values come from the caller, which
+// loaded them one step ahead.
+template <class A, int G, int R, int MODE, bool ENDS, bool CHECKED, bool PRE = false>
 __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const int lane,
                                            const int32_t w, const uint32_t (&n)[2],
                                            const typename A::RES *__restrict__ res,
@@ -384,7 +387,8 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                                            const bool last_pass, typename A::V *bnd,
                                            const int32_t qlen, const int32_t go, const int32_t ge,
                                            const SweepConst<A> &k, typename A::V &best,
-                                           Cand (&cand)[2]) {
+                                           Cand (&cand)[2], const typename A::RES pre_r = 0,
+                                           const typename A::V pre_g = 0, const typename A::V pre_f = 0) {
     typedef typename A::V V;
     typedef ModeFlags<MODE> Fl;
     const V negge = k.negge, neggo = k.neggo;
@@ -398,28 +402,45 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                 upG = Fl::top_free ? k.top_free_g : A::splat(-gap_pen(go, ge, j) - go);
                 upF = k.Sv;
             } else if (live) {
-                upG = bnd[2 * (j - 1)];
-                upF = bnd[2 * (j - 1) + 1];
+                upG = PRE ? pre_g : bnd[2 * (j - 1)];
+                upF = PRE ? pre_f : bnd[2 * (j - 1) + 1];
             }
         }
         if (live) {
             int a, b;
-            A::residues(res[j - 1], a, b);
+            A::residues(PRE ? pre_r : res[j - 1], a, b);
             V pa[A::EPV], pb[A::EPV];
             V g_up = upG, f = upF, gd = sw.diag, hprev = A::splat(0), hlast = A::splat(0);
+            V xprev = A::splat(0);
             const int32_t jR = j * R;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (r % A::EPV == 0)
                     A::template load_chunk<R, G>(prof_a, prof_b, a, b, lane, r / A::EPV, pa, pb);
                 sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
-                f = A::addmax(f, negge, g_up);
-                const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
-                const V h = Fl::local ? A::vmax3_relu(d, sw.E[r], f) : A::vmax3(d, sw.E[r], f);
-                gd = sw.Gp[r];
-                const V g = A::vadd(h, neggo);
-                sw.Gp[r] = g;
-                g_up = g;
+                V h;
+                if (Fl::local && !ENDS) {
+                    // SW scores, with a one-op dependency chain from row to row: with x = max(d,
+                    // E, 0) - go, G = max(F - go, x) and, since go >= ge, F of the next row =
+                    // max(F - ge, G) = max(F - ge, x). x >= -go, so nothing leaves int16. h here is
+                    // G; the running maximum is kept in G (started at -go, go added at the end).
+                    f = A::addmax(f, negge, r == 0 ? g_up : xprev);
+                    const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
+                    const V x = A::vadd(A::vmax3_relu(d, sw.E[r], d), neggo);
+                    xprev = x;
+                    h = A::addmax(f, neggo, x);
+                    gd = sw.Gp[r];
+                    sw.Gp[r] = h;
+                    g_up = h;
+                } else {
+                    f = A::addmax(f, negge, g_up);
+                    const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
+                    h = Fl::local ? A::vmax3_relu(d, sw.E[r], f) : A::vmax3(d, sw.E[r], f);
+                    gd = sw.Gp[r];
+                    const V g = A::vadd(h, neggo);
+                    sw.Gp[r] = g;
+                    g_up = g;
+                }
                 if (Fl::local) {
                     if (ENDS) {
                         bool u0, u1;
@@ -469,7 +490,10 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
 // Steps [s_begin, s_end) of one lane. `w_min` is the smallest item width in the warp: steps in
 // [G-1, w_min) have every lane of the warp on a real column and skip the per-lane checks. All
 // bounds are warp-uniform.
-template <class A, int G, int R, int MODE, bool ENDS>
+// With PREFETCH the unchecked steps load the next step's residue code and boundary-row values one
+// step ahead; only for callers whose boundary row was written by an earlier, completed pass (the
+// band kernel's warps read rows another warp is writing and keep their exact read timing).
+template <class A, int G, int R, int MODE, bool ENDS, bool PREFETCH = false>
 __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, const int s_end,
                                           const int w_min, const int lane, const int32_t w,
                                           const uint32_t (&n)[2],
@@ -491,9 +515,36 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
     for (int s = s_begin; s < head_end; ++s)
         sweep_step<A, G, R, MODE, ENDS, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
                                               first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
-    for (int s = fast_lo; s < fast_hi; ++s)
-        sweep_step<A, G, R, MODE, ENDS, false>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
-                                               first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+    if (PREFETCH && fast_lo < fast_hi) {
+        typedef typename A::V V;
+        // Every lane of the warp is inside its item in [fast_lo, fast_hi): the indices below
+        // (step s - lane, clamped to the range) are real columns.
+        typename A::RES r_cur = res[fast_lo - lane];
+        V g_cur = 0, f_cur = 0;
+        if (lane == 0 && !first_pass) {
+            g_cur = bnd[2 * (fast_lo - lane)];
+            f_cur = bnd[2 * (fast_lo - lane) + 1];
+        }
+        for (int s = fast_lo; s < fast_hi; ++s) {
+            const int sn = min(s + 1, fast_hi - 1);
+            const typename A::RES r_next = res[sn - lane];
+            V g_next = g_cur, f_next = f_cur;
+            if (lane == 0 && !first_pass) {
+                g_next = bnd[2 * (sn - lane)];
+                f_next = bnd[2 * (sn - lane) + 1];
+            }
+            sweep_step<A, G, R, MODE, ENDS, false, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                                         first_pass, last_pass, bnd, qlen, go, ge, k,
+                                                         best, cand, r_cur, g_cur, f_cur);
+            r_cur = r_next;
+            g_cur = g_next;
+            f_cur = f_next;
+        }
+    } else {
+        for (int s = fast_lo; s < fast_hi; ++s)
+            sweep_step<A, G, R, MODE, ENDS, false>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                                   first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+    }
     for (int s = max(fast_hi, head_end); s < s_end; ++s)
         sweep_step<A, G, R, MODE, ENDS, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
                                               first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
@@ -520,7 +571,7 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
                                            Cand (&cand)[2]) {
     Sweep<A, R> sw;
     sweep_begin<A, R, MODE>(sw, row0, go, ge, Sv);
-    sweep_run<A, G, R, MODE, ENDS>(sw, 0, steps, w_min, lane, w, n, res, prof_a, prof_b, row0,
+    sweep_run<A, G, R, MODE, ENDS, true>(sw, 0, steps, w_min, lane, w, n, res, prof_a, prof_b, row0,
                                    first_pass, last_pass, bnd, qlen, go, ge, Sv, best, cand);
     sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
 }
@@ -536,7 +587,7 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
     typedef ModeFlags<MODE> Fl;
     if (Fl::local && !ENDS) {
 #pragma unroll
-        for (int h = 0; h < A::NH; ++h) cand[h].s = A::get(best, h);
+        for (int h = 0; h < A::NH; ++h) cand[h].s = A::get(best, h) + go;  // best is kept in G
     }
 #pragma unroll
     for (int h = 0; h < A::NH; ++h) {
@@ -635,7 +686,7 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
     const int w_min = (int)__reduce_min_sync(0xffffffffu, meta.w);
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
 
-    V best = A::splat(0);
+    V best = A::splat(ModeFlags<MODE>::local && !ENDS ? -(int64_t)p.go : 0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
 
     if (!GPROF && threadIdx.x == 0 && p.n_passes > 0) {
@@ -671,8 +722,14 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
     return true;
 }
 
+// Resident 256-thread blocks per SM each launch shape is compiled for (its register budget).
+template <class A, int G, int R>
+constexpr int scan_min_blocks() {
+    return A::NH == 1 ? 2 : (G == 8 && R == 8) ? 4 : (G == 8 && R == 32) ? 2 : 3;
+}
+
 template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false>
-__global__ void __launch_bounds__(256) scan_kernel(const ScanParams p) {
+__global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) scan_kernel(const ScanParams p) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (GPROF ? 0 : 2 * (size_t)p.pass_bytes));
     const int gpb = blockDim.x / G;
@@ -911,7 +968,7 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
     const int32_t pmax = (int32_t)__reduce_max_sync(0xffffffffu, (uint32_t)n_passes);
 
-    V best = A::splat(0);
+    V best = A::splat(ModeFlags<MODE>::local && !ENDS ? -(int64_t)p.go : 0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
     for (int pass = 0; pass < pmax; ++pass) {
         const bool mine = pass < n_passes;
