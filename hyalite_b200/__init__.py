@@ -290,10 +290,11 @@ class Database:
         self._h = C.c_void_p(handle)
         self._n = n_seqs
 
-    def __del__(self):
+    def __del__(self, _lib=lib):
+        # _lib keeps the library reachable when the module is torn down at interpreter exit.
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib.hy_db_destroy(h)
+            _lib.hy_db_destroy(h)
             self._h = C.c_void_p(None)
 
     @staticmethod
@@ -447,10 +448,11 @@ class Scratch:
         self._h = h
         self._db = db  # keep the database alive while the scratch exists
 
-    def __del__(self):
+    def __del__(self, _lib=lib):
+        # _lib keeps the library reachable when the module is torn down at interpreter exit.
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib.hy_scratch_destroy(h)
+            _lib.hy_scratch_destroy(h)
             self._h = C.c_void_p(None)
 
     @staticmethod
@@ -477,10 +479,11 @@ class Batch:
         self._dbs = dbs  # keep the databases alive while the batch exists
         self.max_queries = int(max_queries)
 
-    def __del__(self):
+    def __del__(self, _lib=lib):
+        # _lib keeps the library reachable when the module is torn down at interpreter exit.
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib.hy_batch_destroy(h)
+            _lib.hy_batch_destroy(h)
             self._h = C.c_void_p(None)
 
     @staticmethod
@@ -576,10 +579,10 @@ class Server:
         # arrays stay referenced here until wait() or close().
         self._live = {}
 
-    def close(self) -> None:
+    def close(self, _lib=lib) -> None:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib.hy_server_destroy(h)
+            _lib.hy_server_destroy(h)
             self._h = C.c_void_p(None)
         self._live = {}
 
