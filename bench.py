@@ -38,10 +38,10 @@ N_SEQS = 500_000
 GO, GE = 11, 1
 AL = 20
 # DRAM bytes (read + write) per DP cell of the int16x2 pair kernel, from one ncu capture of
-# scan_kernel<Pair16, 8, 32> on 400,000 sequences x one 1000-residue query: 1.349e9 bytes for
+# scan_kernel<Pair16, 8, 32> on 400,000 sequences x one 1000-residue query: 1.358e9 bytes for
 # 1.563e11 cells. The traffic is the boundary rows between query passes plus the residues, so it
 # grows with cells at a fixed rows-per-pass; profiles/ holds the capture's summary and command.
-DRAM_BYTES_PER_CELL = 1.349e9 / 1.563e11
+DRAM_BYTES_PER_CELL = 1.358e9 / 1.563e11
 
 
 def make_workload(seed: int, n_seqs: int = N_SEQS):
@@ -449,6 +449,69 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_dna_small(args):
+    """The small plain DNA scan: alphabet 4, +2/-1, gap_open 2, gap_ext 1, SW ScoreEnd, one query of
+    64 uniform bases per call against 10,000 sequences of uniform length 50..300 with 50 planted
+    copies of the query carrying 5% substitutions. Reports the per-call latency and GCUPS of
+    Database.scan (host query in, hit out) and the AVX2 port on the same database over all host
+    threads; every hit is checked against the oracle."""
+    import torch
+
+    import hyalite_b200 as hy
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(args.seed)
+    lengths = rng.integers(50, 301, 10_000)
+    seqs = [rng.integers(0, 4, int(n)).astype(np.uint8) for n in lengths]
+    queries = [rng.integers(0, 4, 64).astype(np.uint8) for _ in range(args.steps)]
+    planted = rng.choice(10_000, 50, replace=False)
+    for k in planted:
+        s = queries[0].copy()
+        sub = rng.choice(64, 3, replace=False)  # 5% of 64
+        s[sub] = (s[sub] + rng.integers(1, 4, 3)) % 4
+        seqs[k] = s
+    res, off = hy.concat(seqs)
+    dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
+    db = (hy.Database.builder().sequences_concat(res, off).scoring(hy.Scoring(4, dna, 2, 1)).mode(hy.Mode.Sw)
+          .search_type(hy.SearchType.ScoreEnd).max_query_len(64).build())
+    sc = hy.Scratch(db)
+    for q in queries[: args.warmup]:
+        db.scan(sc, q)
+    lat = []
+    hits = []
+    for q in queries:
+        t0 = time.perf_counter()
+        hits.append(db.scan(sc, q))
+        lat.append(time.perf_counter() - t0)
+    cells = 64.0 * float(off[-1])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    ref = pyoracle.OracleDb((res, off), dna, 4, 2, 1, 0, 1)
+    identical = all((h.score, h.db_index, h.query_end, h.target_end) == ref.scan(q) for h, q in zip(hits, queries))
+    threads = os.cpu_count() or 1
+    avx = pyoracle.Avx2Db(res, off, dna, 4, 2, 1, 0, 1, 64)
+    qlist = [list(map(int, q)) for q in queries]
+    t0 = time.perf_counter()
+    avx.scan_many(qlist, threads)
+    cpu_s = time.perf_counter() - t0
+    med = statistics.median(lat)
+    line = {
+        "metric": "GCUPS", "value": cells / med / 1e9, "unit": "GCUPS", "n_gpus": 1, "steps": len(queries),
+        "warmup": args.warmup, "ms_per_step": med * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "i16x2 (Precomputed layout)", "data": "synthetic (seeded DNA)",
+        "config": {"workload": "small plain DNA SW ScoreEnd scan: 64-bp query x 10,000 sequences of 50..300 bp "
+                               "(50 planted 5%-substituted copies), one Database.scan per query",
+                   "residues": int(off[-1]), "layout": db.layout().name},
+        "latency_ms": {"p50": med * 1e3, "p99": float(np.percentile(lat, 99)) * 1e3, "min": min(lat) * 1e3},
+        "e2e": {"value": cells / med / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": 64, "d2h_bytes_per_step": 32},
+        "identical_to_oracle": identical,
+        "planted_top_hit": int(hits[0].db_index) in set(int(k) for k in planted),
+        "cpu_baseline": {"value": cells * len(queries) / cpu_s / 1e9, "unit": "GCUPS", "cores": threads,
+                         "kind": "port", "sample": f"the same {len(queries)} queries, one per thread, AVX2 port"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_served(args):
     """The served workload: a resident protein database (the generator above at --served-seqs
     sequences), Poisson arrivals at each offered rate, query lengths log-normal (median 350,
@@ -675,7 +738,7 @@ def main():
     ap.add_argument("--query-lengths", default=",".join(map(str, QUERY_LENGTHS)))
     ap.add_argument("--n-queries", type=int, default=N_QUERIES)
     # Other workloads of the same backend (not the default benchmark line).
-    ap.add_argument("--workload", default="scan", choices=["scan", "batched", "served", "pairs"])
+    ap.add_argument("--workload", default="scan", choices=["scan", "batched", "served", "pairs", "dna_small"])
     ap.add_argument("--n-pairs", type=int, default=10_000_000)
     ap.add_argument("--cpu-pairs", type=int, default=100_000)
     ap.add_argument("--n-reads", type=int, default=1_000_000)
@@ -698,6 +761,8 @@ def main():
         run_served(args)
     elif args.workload == "pairs":
         run_pairs(args)
+    elif args.workload == "dna_small":
+        run_dna_small(args)
     else:
         run_cuda(args)
 

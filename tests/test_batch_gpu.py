@@ -51,7 +51,7 @@ def test_protein_long_targets_int32_and_long_pairs():
     # Targets wider than the long-pair split and sequences the device runs in int32 lanes.
     rng = np.random.default_rng(12)
     mat = [int(v) for v in rng.integers(-4, 12, 400)]
-    seqs = rand_seqs(rng, 120, 20, 1, 400) + rand_seqs(rng, 4, 20, 2100, 3000) + rand_seqs(rng, 3, 20, 3100, 4000)
+    seqs = rand_seqs(rng, 120, 20, 1, 400) + rand_seqs(rng, 4, 20, 2100, 3000) + rand_seqs(rng, 3, 20, 4100, 5000)
     dbs = _dbs(seqs, mat, 20, 11, 1, 3000)
     queries, dbq = [], []
     for i, L in enumerate([100, 1000, 3000, 250, 600, 2999, 17, 64]):

@@ -47,7 +47,7 @@ def _check(seqs, mat, al, go, ge, mode, st, queries, mql, layout=hy.Layout.Preco
 @pytest.mark.parametrize("mode", ALL_MODES)
 def test_precomputed_dna_every_mode(mode):
     rng = np.random.default_rng(500 + mode)
-    seqs = rand_seqs(rng, 90, 4, 0, 300) + rand_seqs(rng, 2, 4, 2100, 2600)
+    seqs = rand_seqs(rng, 90, 4, 0, 300) + rand_seqs(rng, 2, 4, 4100, 4600)
     queries = [list(rng.integers(0, 4, n)) for n in (0, 1, 40, 64, 65, 200, 257, 600)]
     for st in (0, 1):
         for layout in (hy.Layout.Precomputed, hy.Layout.Gathered):
@@ -58,7 +58,7 @@ def test_precomputed_protein_and_int32_partition():
     # A 441-letter pair table: the bulk kernel runs 8 rows per lane and the long pairs and band
     # read the table from global memory; large entries put the longest targets in int32.
     rng = np.random.default_rng(510)
-    seqs = rand_seqs(rng, 60, 20, 1, 400) + rand_seqs(rng, 3, 20, 2100, 3500)
+    seqs = rand_seqs(rng, 60, 20, 1, 400) + rand_seqs(rng, 3, 20, 2100, 4600)
     queries = [list(rng.integers(0, 20, n)) for n in (30, 300, 1000)]
     for mode in (0, 2):
         _check(seqs, BLOSUM62, 20, 11, 1, mode, 1, queries, 1000)
@@ -73,7 +73,7 @@ def test_batch_server_and_noalloc_on_mixed_layouts():
 
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(520)
-    seqs = rand_seqs(rng, 400, 4, 1, 250) + rand_seqs(rng, 2, 4, 2100, 2500)
+    seqs = rand_seqs(rng, 400, 4, 1, 250) + rand_seqs(rng, 2, 4, 4100, 4500)
     dbs = [_build(seqs, DNA, 4, 2, 1, m, 1, 700, lay)
            for m in (0, 1, 2) for lay in (hy.Layout.Precomputed, hy.Layout.Gathered)]
     pseqs = rand_seqs(rng, 200, 20, 1, 300)

@@ -1,5 +1,5 @@
 """Parity of the device scan at the launch-shape boundaries (rows per lane 8 / 16 / 32 chosen by
-query length, query passes, the warp-per-pair path for targets wider than 2048 columns) and, on a
+query length, query passes, the warp-per-pair path for targets wider than 4096 columns) and, on a
 large protein database, full-size properties plus oracle parity on a sample of targets."""
 import math
 
@@ -23,8 +23,8 @@ SHAPE_QLENS = (1, 8, 63, 64, 65, 127, 128, 129, 191, 192, 193, 255, 256, 257, 51
 def test_rows_per_lane_and_pass_boundaries(mode):
     rng = np.random.default_rng(300 + mode)
     mat = [int(v) for v in rng.integers(-4, 12, 400)]
-    # Mostly short targets (bulk int16x2 kernel), two wider than 2048 columns (one warp each).
-    seqs = rand_seqs(rng, 70, 20, 1, 400) + rand_seqs(rng, 2, 20, 2049, 2600)
+    # Mostly short targets (bulk int16x2 kernel), two wider than 4096 columns (one warp each).
+    seqs = rand_seqs(rng, 70, 20, 1, 400) + rand_seqs(rng, 2, 20, 4097, 4600)
     queries = [list(rng.integers(0, 20, n)) for n in SHAPE_QLENS]
     for st in (0, 1):
         check(seqs, mat, 20, 11, 1, mode, st, queries, mql=max(SHAPE_QLENS))
@@ -99,7 +99,7 @@ def test_large_alphabets_read_the_profile_from_global_memory(al):
     # int32 items and the winner's-ends recovery. Entries up to 60 put the long targets in int32.
     rng = np.random.default_rng(400 + al)
     mat = [int(v) for v in rng.integers(-20, 61, al * al)]
-    seqs = rand_seqs(rng, 50, al, 1, 300) + rand_seqs(rng, 2, al, 2100, 3100)
+    seqs = rand_seqs(rng, 50, al, 1, 300) + rand_seqs(rng, 2, al, 2100, 4200)
     queries = [list(rng.integers(0, al, n)) for n in (1, 50, 300, 700)]
     for mode in (0, 1, 3):
         for st in (0, 1):

@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 def _setup(seed=21):
     rng = np.random.default_rng(seed)
     mat = [int(v) for v in rng.integers(-4, 12, 400)]
-    seqs = rand_seqs(rng, 1500, 20, 1, 400) + rand_seqs(rng, 3, 20, 2200, 3200)
+    seqs = rand_seqs(rng, 1500, 20, 1, 400) + rand_seqs(rng, 3, 20, 2200, 4300)
     dbs = [build(seqs, mat, 20, 11, 1, mode, 1, 1200) for mode in (0, 2, 4)]
     reqs = []
     for i in range(36):
