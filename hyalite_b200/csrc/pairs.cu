@@ -189,6 +189,42 @@ static int pair_rows(uint64_t q, int32_t al) {
     return best;
 }
 
+// Sorts pair indices (given in ascending order) by (query length desc, target length desc), index
+// asc for equal lengths: a stable LSD radix sort on 16-bit digits of the complemented lengths
+// (target length first, then query length), skipping digits every pair shares. O(n) per pass.
+static void sort_by_shape(std::vector<uint32_t> &o, const uint64_t *q_off, const uint64_t *t_off) {
+    const size_t n = o.size();
+    if (n < 2) return;
+    std::vector<uint32_t> tmp(n);
+    std::vector<uint32_t> key(n), key_tmp(n);
+    std::vector<size_t> count(1 << 16);
+    for (int field = 0; field < 2; ++field) {  // 0: target length, 1: query length
+        for (size_t i = 0; i < n; ++i) {
+            const uint32_t k = o[i];
+            const uint64_t len = field == 0 ? t_off[k + 1] - t_off[k] : q_off[k + 1] - q_off[k];
+            key[i] = ~(uint32_t)len;
+        }
+        for (int shift = 0; shift < 32; shift += 16) {
+            std::fill(count.begin(), count.end(), 0);
+            for (size_t i = 0; i < n; ++i) ++count[(key[i] >> shift) & 0xffff];
+            if (count[(key[0] >> shift) & 0xffff] == n) continue;  // one digit value: nothing to do
+            size_t sum = 0;
+            for (size_t d = 0; d < count.size(); ++d) {
+                const size_t c = count[d];
+                count[d] = sum;
+                sum += c;
+            }
+            for (size_t i = 0; i < n; ++i) {
+                const size_t dst = count[(key[i] >> shift) & 0xffff]++;
+                tmp[dst] = o[i];
+                key_tmp[dst] = key[i];
+            }
+            o.swap(tmp);
+            key.swap(key_tmp);
+        }
+    }
+}
+
 struct PairPart {
     std::vector<ItemMeta> meta;
     std::vector<uint32_t> qlen;
@@ -434,18 +470,8 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             HY_CK(cudaEventCreate(&ctx.ev1));
         }
         // Sort by (query length desc, target length desc, index asc) through 64-bit keys.
-        auto sort_part = [&](std::vector<uint32_t> &o) {
-            std::vector<std::pair<uint64_t, uint32_t>> key(o.size());
-            for (size_t i = 0; i < o.size(); ++i) {
-                const uint32_t k = o[i];
-                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-                key[i] = {~((ql << 32) | tl), k};
-            }
-            std::sort(key.begin(), key.end());
-            for (size_t i = 0; i < o.size(); ++i) o[i] = key[i].second;
-        };
-        sort_part(o16);
-        sort_part(o32);
+        sort_by_shape(o16, q_off, t_off);
+        sort_by_shape(o32, q_off, t_off);
         PairPart p16, p32;
         pack_pairs(o16, q_off, t_off, true, p16);
         pack_pairs(o32, q_off, t_off, false, p32);
