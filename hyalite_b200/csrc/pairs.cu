@@ -41,12 +41,27 @@ struct PairsContext {
         size_t n = 0;
     };
     Buf b[14];
+    Buf pinned[2];  // grow-only pinned host staging of the packed target residues (per partition)
     double kernel_ms = 0.0, call_ms = 0.0;  // the last call: pair kernels' device time, whole call
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
+        for (auto &x : pinned) cudaFreeHost(x.p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
+    }
+    cudaError_t get_pinned(int slot, size_t bytes, void **out) {
+        bytes = std::max<size_t>(bytes, 16);
+        if (pinned[slot].n < bytes) {
+            cudaFreeHost(pinned[slot].p);
+            pinned[slot].p = nullptr;
+            pinned[slot].n = 0;
+            cudaError_t e = cudaMallocHost(&pinned[slot].p, bytes);
+            if (e != cudaSuccess) return e;
+            pinned[slot].n = bytes;
+        }
+        *out = pinned[slot].p;
+        return cudaSuccess;
     }
     cudaError_t get(int slot, size_t bytes, void **out) {
         bytes = std::max<size_t>(bytes, 16);
@@ -292,7 +307,10 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     }
     HY_CK(ctx.get(slot0 + 4, multipass ? 2 * sizeof(typename A::V) * pp.cols : 16, &d_bnd));
     // Pack target residues (the shorter half of a pair item padded with symbol `al`).
-    std::vector<typename A::RES> res(std::max<size_t>(pp.cols, 1));
+    // Packed straight into pinned staging (every column, padding included, is written below).
+    void *h_res = nullptr;
+    HY_CK(ctx.get_pinned(slot0 == 0 ? 0 : 1, res_bytes, &h_res));
+    typename A::RES *res = static_cast<typename A::RES *>(h_res);
     parallel_for(n_items, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
         for (uint64_t it = a; it < e; ++it) {
             const ItemMeta &m = pp.meta[it];
@@ -313,7 +331,7 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     HY_CK(cudaMemcpyAsync(d_meta, pp.meta.data(), sizeof(ItemMeta) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qlen, pp.qlen.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qoff, pp.qoff.data(), sizeof(uint64_t) * 2 * n_items, cudaMemcpyHostToDevice, ctx.stream));
-    HY_CK(cudaMemcpyAsync(d_res, res.data(), res_bytes, cudaMemcpyHostToDevice, ctx.stream));
+    HY_CK(cudaMemcpyAsync(d_res, res, res_bytes, cudaMemcpyHostToDevice, ctx.stream));
     PairParams p{};
     p.meta = (const ItemMeta *)d_meta;
     p.qlen = (const uint32_t *)d_qlen;
@@ -368,7 +386,7 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
         i0 = i1;
     }
     HY_CK(cudaEventRecord(ctx.ev1, ctx.stream));
-    // The host staging vector must outlive the async copy.
+    // The host staging (the item vectors and the pinned residues) must outlive the async copies.
     HY_CK(cudaStreamSynchronize(ctx.stream));
     float ms = 0.0f;
     HY_CK(cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1));

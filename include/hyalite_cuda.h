@@ -297,7 +297,9 @@ hy_status hy_server_stats_read(hy_server *server, int reset, hy_server_stats *ou
 /* align_pairs: pair p is (q_res[q_off[p]..q_off[p+1]], t_res[t_off[p]..t_off[p+1]]). Each pair is
  * validated in order (symbols query-then-target, then the width proof on its exact lengths); on
  * the first failing pair the call returns its error, *failed_pair receives its index and out[0 ..
- * index) holds the hits of the pairs before it. db_index of each hit is its pair index. */
+ * index) holds the hits of the pairs before it. db_index of each hit is its pair index. The calling
+ * thread keeps grow-only device buffers and a pinned host staging buffer for the packed targets
+ * between calls (freed at thread exit). */
 hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
                          const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
                          uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
