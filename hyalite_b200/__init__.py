@@ -2,8 +2,9 @@
 
 A Python mirror of hyalite's public API for this path (src/lib.rs:54-67): ``Scoring``, ``Mode``,
 ``SearchType``, ``BestHit``, ``Backend`` / ``BackendChoice`` / ``BACKEND_ENV_VAR``, ``Layout`` /
-``LayoutChoice``, ``ScoreWidth``, ``Database`` / ``DatabaseBuilder`` / ``Scratch`` and
-``align_pairs``, with the same names, argument meanings and error behaviour, over the C ABI of
+``LayoutChoice``, ``ScoreWidth``, ``Database`` / ``DatabaseBuilder`` / ``Scratch``,
+``align_pairs`` and the traceback (``align``, ``Alignment``, ``AlignOp``, ``AlignedHit``,
+``Database.scan_aligned`` / ``scan_all_aligned``), with the same names, argument meanings and error behaviour, over the C ABI of
 include/hyalite_cuda.h. All compute runs in the in-tree CUDA library; there is no CPU path.
 """
 from __future__ import annotations
@@ -36,6 +37,7 @@ class Error(Exception):
         "SymbolOutOfRange": ("symbol", "alphabet_len"),
         "BackendUnavailable": ("backend",),
         "QueryTooLong": ("len", "max"),
+        "TracebackBudgetExceeded": ("needed_bytes", "budget_bytes"),
         "Cuda": ("code",),
     }
 
@@ -56,6 +58,8 @@ class Error(Exception):
         d = _abi.last_detail()
         names = cls._FIELDS.get(kind, ())
         fields = {n: int(d[i]) for i, n in enumerate(names)}
+        if kind == "TracebackBudgetExceeded":  # u64 / usize fields carried in int64
+            fields = {n: v & (2**64 - 1) for n, v in fields.items()}
         if kind == "BackendUnavailable":
             fields["backend"] = Backend(fields["backend"])
         return cls(kind, **fields)
@@ -89,14 +93,37 @@ class Mode(enum.IntEnum):
 ALL_MODES = (Mode.Sw, Mode.Nw, Mode.Hw, Mode.Ov, Mode.Shw)
 
 
+USIZE_MAX = 2**64 - 1
+
+
 class SearchType(enum.IntEnum):
-    """What a search returns (src/search.rs:13-27). ``Alignment`` (traceback) is not built by this
-    backend."""
+    """What a search returns (src/search.rs:13-27). ``Alignment`` carries a traceback budget:
+    ``SearchType.alignment(max_bytes)``; the bare member means ``max_bytes = usize::MAX``."""
     Score = 0
     ScoreEnd = 1
+    Alignment = 2
 
     def tracks_end(self) -> bool:
-        return self is SearchType.ScoreEnd
+        return self is not SearchType.Score
+
+    @staticmethod
+    def alignment(max_bytes: int) -> "AlignmentSearch":
+        return AlignmentSearch(int(max_bytes))
+
+
+@dataclass(frozen=True)
+class AlignmentSearch:
+    """SearchType::Alignment { max_bytes } (src/search.rs:20-26)."""
+    max_bytes: int
+
+    def tracks_end(self) -> bool:
+        return True
+
+    def __int__(self) -> int:
+        return int(SearchType.Alignment)
+
+    def __str__(self) -> str:
+        return f"Alignment {{ max_bytes: {self.max_bytes} }}"
 
 
 class ScoreWidth(enum.IntEnum):
@@ -192,6 +219,86 @@ class BestHit:
     def _from(h: _abi.HyHit) -> "BestHit":
         return BestHit(int(h.score), int(h.db_index), None if h.query_end < 0 else int(h.query_end),
                        None if h.target_end < 0 else int(h.target_end))
+
+
+# ---- traceback results (src/align.rs:40-150) ------------------------------------------------------
+
+class AlignOp(enum.IntEnum):
+    """src/align.rs:47-56: Match / Mismatch by symbol equality; Ins consumes a query symbol, Del a
+    target symbol (the target is the reference)."""
+    Match = 0
+    Mismatch = 1
+    Ins = 2
+    Del = 3
+
+
+def _cigar(ops: bytes, extended: bool) -> str:
+    """Alignment::encode (src/align.rs:108-150): run-length of the op letters."""
+    letters = ("=", "X", "I", "D") if extended else ("M", "M", "I", "D")
+    out = []
+    prev, run = None, 0
+    for o in ops:
+        c = letters[o]
+        if c == prev:
+            run += 1
+        else:
+            if prev is not None:
+                out.append(f"{run}{prev}")
+            prev, run = c, 1
+    if prev is not None:
+        out.append(f"{run}{prev}")
+    return "".join(out)
+
+
+class Alignment:
+    """src/align.rs:57-83: score, half-open spans and the operations (kept as one byte each,
+    ``AlignOp`` codes; ``ops`` gives them as ``AlignOp`` values)."""
+    __slots__ = ("score", "query_start", "query_end", "target_start", "target_end", "ops_bytes")
+
+    def __init__(self, score, query_start, query_end, target_start, target_end, ops_bytes: bytes):
+        self.score = int(score)
+        self.query_start = int(query_start)
+        self.query_end = int(query_end)
+        self.target_start = int(target_start)
+        self.target_end = int(target_end)
+        self.ops_bytes = bytes(ops_bytes)
+
+    @property
+    def ops(self) -> List[AlignOp]:
+        return [AlignOp(o) for o in self.ops_bytes]
+
+    def cigar(self) -> str:
+        return _cigar(self.ops_bytes, False)
+
+    def cigar_extended(self) -> str:
+        return _cigar(self.ops_bytes, True)
+
+    def as_tuple(self):
+        return (self.score, self.query_start, self.query_end, self.target_start, self.target_end,
+                self.ops_bytes)
+
+    def __eq__(self, other):
+        return isinstance(other, Alignment) and self.as_tuple() == other.as_tuple()
+
+    def __hash__(self):
+        return hash(self.as_tuple())
+
+    def __repr__(self):
+        return (f"Alignment(score={self.score}, query={self.query_start}..{self.query_end}, "
+                f"target={self.target_start}..{self.target_end}, cigar={self.cigar_extended()!r})")
+
+    @staticmethod
+    def _from(a: _abi.HyAlignment, ops) -> "Alignment":
+        o, n = int(a.ops_offset), int(a.n_ops)
+        return Alignment(a.score, a.query_start, a.query_end, a.target_start, a.target_end,
+                         C.string_at(C.addressof(ops.contents) + o, n) if n else b"")
+
+
+@dataclass(frozen=True)
+class AlignedHit:
+    """src/align.rs:85-92: a database index with the alignment against that sequence."""
+    db_index: int
+    alignment: Alignment
 
 
 # ---- scoring (src/scoring.rs) ----------------------------------------------------------------------
@@ -331,15 +438,54 @@ class Database:
         _check(lib.hy_scan_scores(self._h, scratch._h, _ptr(q, _abi._u8p), len(q), _ptr(res, _abi._i32p)))
         return res
 
+    # -- traceback (src/database.rs:517-565) --
+    def scan_aligned(self, scratch: "Scratch", query) -> AlignedHit:
+        """The winner of ``scan`` (same tie-break) with its full alignment."""
+        q = _as_u8(query)
+        out = _abi.HyAlignment()
+        idx = C.c_uint64()
+        ops = _abi._u8p()
+        _check(lib.hy_scan_aligned(self._h, scratch._h, _ptr(q, _abi._u8p), len(q), C.byref(idx),
+                                   C.byref(out), C.byref(ops)))
+        return AlignedHit(int(idx.value), Alignment._from(out, ops))
+
+    def scan_all_aligned_arrays(self, scratch: "Scratch", query):
+        """The raw form of ``scan_all_aligned``: a numpy structured view of the per-sequence
+        records (score, spans, n_ops, ops_offset) and the concatenated operations (uint8)."""
+        q = _as_u8(query)
+        arr = (_abi.HyAlignment * self._n)()
+        ops = _abi._u8p()
+        _check(lib.hy_scan_all_aligned(self._h, scratch._h, _ptr(q, _abi._u8p), len(q), arr, C.byref(ops)))
+        total = 0
+        if self._n:
+            last = arr[self._n - 1]
+            total = int(last.ops_offset) + int(last.n_ops)
+        buf = np.frombuffer(C.string_at(ops, total), dtype=np.uint8) if total else np.zeros(0, np.uint8)
+        return arr, buf
+
+    def scan_all_aligned(self, scratch: "Scratch", query, out: list) -> None:
+        """One ``Alignment`` per database sequence, in database order."""
+        arr, buf = self.scan_all_aligned_arrays(scratch, query)
+        raw = buf.tobytes()
+        out.clear()
+        for a in arr:
+            o = int(a.ops_offset)
+            out.append(Alignment(a.score, a.query_start, a.query_end, a.target_start, a.target_end,
+                                 raw[o: o + int(a.n_ops)]))
+
     # -- accessors (src/database.rs:570-638) --
+    def traceback_max_bytes(self) -> int:
+        return int(lib.hy_db_traceback_max_bytes(self._h))
+
     def sequence_count(self) -> int:
         return self._n
 
     def mode(self) -> Mode:
         return Mode(lib.hy_db_mode(self._h))
 
-    def search_type(self) -> SearchType:
-        return SearchType(lib.hy_db_search_type(self._h))
+    def search_type(self):
+        st = SearchType(lib.hy_db_search_type(self._h))
+        return AlignmentSearch(self.traceback_max_bytes()) if st is SearchType.Alignment else st
 
     def score_width(self) -> ScoreWidth:
         return ScoreWidth(lib.hy_db_score_width(self._h))
@@ -402,8 +548,8 @@ class DatabaseBuilder:
         self._mode = Mode(mode)
         return self
 
-    def search_type(self, st: SearchType) -> "DatabaseBuilder":
-        self._st = SearchType(st)
+    def search_type(self, st) -> "DatabaseBuilder":
+        self._st = st if isinstance(st, AlignmentSearch) else SearchType(st)
         return self
 
     def max_query_len(self, n: int) -> "DatabaseBuilder":
@@ -427,12 +573,13 @@ class DatabaseBuilder:
         n = len(off) - 1
         sc = self._scoring
         st = self._st if self._st is not None else SearchType.Score
+        tb_budget = st.max_bytes if isinstance(st, AlignmentSearch) else USIZE_MAX
         choice = _abi.CHOICE_UNSET if self._backend is None else self._backend._code()
         layout = _abi.LAYOUT_AUTO if self._layout is None else self._layout._code()
         h = C.c_void_p()
         status = lib.hy_db_create(_ptr(res, _abi._u8p), _ptr(off, _abi._u64p), n,
                                   _ptr(sc._matrix, _abi._i32p), sc._al, sc._go, sc._ge, int(self._mode),
-                                  int(st), self._mql, choice, layout, C.byref(h))
+                                  int(st), tb_budget, self._mql, choice, layout, C.byref(h))
         if status == 10:  # InvalidBackendName from HYALITE_BACKEND
             raise Error("InvalidBackendName", name=os.environ.get(BACKEND_ENV_VAR, ""))
         _check(status)
@@ -647,6 +794,24 @@ def align_pairs_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, mode: Mode,
     return out, (err, int(failed.value))
 
 
+def align(query, target, scoring: Scoring, mode: Mode, max_bytes: int) -> Alignment:
+    """align (src/align.rs:169-222): the full alignment of one pair, traced back on the device.
+    ``max_bytes`` is the reference's traceback budget (``USIZE_MAX`` for usize::MAX)."""
+    q, t = _as_u8(query), _as_u8(target)
+    out = _abi.HyAlignment()
+    ops = np.zeros(max(1, len(q) + len(t)), np.uint8)
+    _check(lib.hy_align(_ptr(q, _abi._u8p), len(q), _ptr(t, _abi._u8p), len(t),
+                        _ptr(scoring._matrix, _abi._i32p), scoring._al, scoring._go, scoring._ge,
+                        int(Mode(mode)), int(max_bytes), C.byref(out), _ptr(ops, _abi._u8p)))
+    return Alignment(out.score, out.query_start, out.query_end, out.target_start, out.target_end,
+                     ops[: int(out.n_ops)].tobytes())
+
+
+def traceback_min_bytes_for_database(max_m: int, max_n: int) -> int:
+    """src/align.rs:245-250."""
+    return int(lib.hy_traceback_min_bytes_for_database(max_m, max_n))
+
+
 def align_pairs_timing():
     """(pair kernels' device ms, whole call ms) of this thread's last align_pairs call."""
     k, c = C.c_double(), C.c_double()
@@ -673,6 +838,7 @@ def align_pairs(pairs, scoring: Scoring, mode: Mode, search_type: SearchType, ou
 __all__ = [
     "BACKEND_ENV_VAR", "Backend", "BackendChoice", "BestHit", "Database", "DatabaseBuilder", "Error",
     "Batch", "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
-    "Server", "ServerRequest",
-    "align_pairs", "align_pairs_arrays", "required_width", "concat",
+    "Server", "ServerRequest", "AlignOp", "Alignment", "AlignedHit", "AlignmentSearch", "USIZE_MAX",
+    "align", "align_pairs", "align_pairs_arrays", "required_width", "concat",
+    "traceback_min_bytes_for_database",
 ]

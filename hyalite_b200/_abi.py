@@ -47,6 +47,12 @@ class HyServerStats(C.Structure):
                 ("gcups", C.c_double)]
 
 
+class HyAlignment(C.Structure):
+    _fields_ = [("score", C.c_int32), ("reserved", C.c_uint32), ("query_start", C.c_uint64),
+                ("query_end", C.c_uint64), ("target_start", C.c_uint64), ("target_end", C.c_uint64),
+                ("n_ops", C.c_uint64), ("ops_offset", C.c_uint64)]
+
+
 _u8p = C.POINTER(C.c_uint8)
 _u64p = C.POINTER(C.c_uint64)
 _i32p = C.POINTER(C.c_int32)
@@ -67,7 +73,15 @@ SIGNATURES = {
     "hy_required_width": (_st, [C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                 C.c_uint64, C.POINTER(C.c_int), _i64p]),
     "hy_db_create": (_st, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32,
-                           C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, C.POINTER(_vp)]),
+                           C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "hy_db_traceback_max_bytes": (C.c_uint64, [_vp]),
+    "hy_align": (_st, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32,
+                       C.c_int, C.c_uint64, C.POINTER(HyAlignment), _u8p]),
+    "hy_scan_aligned": (_st, [_vp, _vp, _u8p, C.c_uint64, _u64p, C.POINTER(HyAlignment),
+                              C.POINTER(_u8p)]),
+    "hy_scan_all_aligned": (_st, [_vp, _vp, _u8p, C.c_uint64, C.POINTER(HyAlignment), C.POINTER(_u8p)]),
+    "hy_traceback_min_bytes_for_database": (C.c_uint64, [C.c_uint64, C.c_uint64]),
+    "hy_traceback_needed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
     "hy_db_destroy": (None, [_vp]),
     "hy_db_sequence_count": (C.c_uint64, [_vp]),
     "hy_db_mode": (C.c_int, [_vp]),

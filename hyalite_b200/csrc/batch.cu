@@ -366,7 +366,7 @@ struct BatchDeviceGuard {
 
 uint64_t batch_profile_bytes(const hy_batch *b, const hy_db *db, uint64_t qlen, bool ends) {
     QueryKinds k;
-    plan_kinds(db, qlen, ends && db->search_type == HY_SEARCH_SCORE_END, b->cfg, k);
+    plan_kinds(db, qlen, ends && db->search_type != HY_SEARCH_SCORE, b->cfg, k);
     return k.bytes;
 }
 
@@ -401,7 +401,7 @@ hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const Bat
         if (qlen) memcpy(b->h_qres + q_off, it.q, qlen);
         BatchQuery &bq = b->h_queries[i];
         memset(&bq, 0, sizeof(bq));
-        const bool ends = it.ends && db->search_type == HY_SEARCH_SCORE_END;
+        const bool ends = it.ends && db->search_type != HY_SEARCH_SCORE;
         QueryKinds k;
         plan_kinds(db, qlen, ends, cfg, k);
         if (prof_off + k.bytes > b->prof_cap) {

@@ -86,6 +86,11 @@ struct hy_db {
     std::vector<uint32_t> pair_w;  // host: longer length of each pair, non-increasing
     uint32_t *d_rank = nullptr;    // device: rank of each global index in the length order
     uint64_t device_bytes = 0;
+    // Alignment search type: its budget, and every sequence's residues in db order (sequence k is
+    // d_tb_res[tb_off[k] .. tb_off[k+1]]), the targets of the traceback.
+    uint64_t tb_max_bytes = 0;
+    uint8_t *d_tb_res = nullptr;
+    std::vector<uint64_t> tb_off;
 };
 
 namespace hy {

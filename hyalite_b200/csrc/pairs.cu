@@ -407,7 +407,7 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
     ctx.call_ms = 0.0;
     if (failed_pair) *failed_pair = n_pairs;
     if ((int)mode < 0 || (int)mode > 4) return fail(HY_ERR_INVALID_ARGUMENT);
-    if ((int)search_type != HY_SEARCH_SCORE && (int)search_type != HY_SEARCH_SCORE_END)
+    if ((int)search_type < HY_SEARCH_SCORE || (int)search_type > HY_SEARCH_ALIGNMENT)
         return fail(HY_ERR_UNSUPPORTED);
     hy_status st = validate_scoring(alphabet_len, matrix, alphabet_len * alphabet_len, gap_open, gap_ext);
     if (st != HY_OK) return st;
@@ -505,7 +505,7 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
         HY_CK(cudaMemcpyAsync(d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, ctx.stream));
         int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + n_ok, *d_tend = d_qend + n_ok;
-        const bool ends = search_type == HY_SEARCH_SCORE_END;
+        const bool ends = search_type != HY_SEARCH_SCORE;
         st = run_part<Pair16, PAIR_G>(ctx, 0, p16, t_res, t_off, (const uint8_t *)d_q,
                                       (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
                                       gap_ext, mode, ends, d_scores, d_qend, d_tend);

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "db_internal.h"
+#include "traceback_internal.h"
 
 using namespace hy;
 
@@ -47,6 +48,10 @@ struct hy_scratch {
     double event_cells[3] = {0.0, 0.0, 0.0};  // real DP cells the timed launches computed
     size_t n_events = 0;
     uint64_t launches = 0;        // every kernel this scratch launched since the last read
+    // Traceback (Alignment search type): grow-only buffers, created on first use, and the
+    // operations of the last traceback call.
+    void *tb = nullptr;
+    std::vector<uint8_t> tb_ops;
 };
 
 namespace hy {
@@ -351,7 +356,7 @@ static hy_status enqueue_scan(const hy_db *db, hy_scratch *sc, const uint8_t *d_
     HY_CK(cudaMemsetAsync(sc->d_key, 0, sizeof(unsigned long long), sc->stream));
     hy_status st = enqueue_scores(db, sc, d_query, qlen, false, sc->d_key, sc->d_scores);
     if (st != HY_OK) return st;
-    const bool ends = db->search_type == HY_SEARCH_SCORE_END;
+    const bool ends = db->search_type != HY_SEARCH_SCORE;
     if (ends) {
         // End positions of the winner only (src/database.rs:186-197): rerun its item with
         // position tracking on a whole block (the band kernel).
@@ -518,6 +523,7 @@ static void free_db(hy_db *db) {
     cudaFree(db->p32.d_meta);
     cudaFree(db->p32.d_res);
     cudaFree(db->d_rank);
+    cudaFree(db->d_tb_res);
     delete db;
 }
 
@@ -530,12 +536,13 @@ extern "C" {
 hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
                        const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
                        int32_t gap_ext, hy_mode mode, hy_search_type search_type,
-                       uint64_t max_query_len, int backend_choice, int layout, hy_db **out) {
+                       uint64_t traceback_max_bytes, uint64_t max_query_len, int backend_choice,
+                       int layout, hy_db **out) {
     if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
     *out = nullptr;
     if ((int)mode < 0 || (int)mode > 4) return fail(HY_ERR_INVALID_ARGUMENT);
-    if ((int)search_type != HY_SEARCH_SCORE && (int)search_type != HY_SEARCH_SCORE_END)
-        return fail(HY_ERR_UNSUPPORTED);
+    if ((int)search_type < HY_SEARCH_SCORE || (int)search_type > HY_SEARCH_ALIGNMENT)
+        return fail(HY_ERR_INVALID_ARGUMENT);
     hy_status st = validate_scoring(alphabet_len, matrix, alphabet_len * alphabet_len, gap_open, gap_ext);
     if (st != HY_OK) return st;
     if (n_seqs == 0) return fail(HY_ERR_EMPTY_DATABASE);
@@ -553,6 +560,12 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
     const int64_t bound = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, max_query_len, max_t);
     const int width = narrowest_width(bound);
     if (width < 0) return fail(HY_ERR_SCORE_RANGE_TOO_WIDE, bound);
+    // The Alignment budget covers every problem the database can pose (src/database.rs:776-790).
+    if (search_type == HY_SEARCH_ALIGNMENT) {
+        const uint64_t needed = hy_traceback_min_bytes_for_database(max_query_len, max_t);
+        if (needed > traceback_max_bytes)
+            return fail(HY_ERR_TRACEBACK_BUDGET_EXCEEDED, (int64_t)needed, (int64_t)traceback_max_bytes);
+    }
     hy_backend backend;
     st = hy_backend_resolve(backend_choice, &backend);
     if (st != HY_OK) return st;
@@ -580,6 +593,7 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
     db->max_e = max_e;
     db->mode = mode;
     db->search_type = search_type;
+    db->tb_max_bytes = search_type == HY_SEARCH_ALIGNMENT ? traceback_max_bytes : 0;
     db->layout = layout == HY_LAYOUT_AUTO ? auto_layout(alphabet_len) : layout;
     db->width = (hy_score_width)width;
     db->backend = backend;
@@ -628,6 +642,16 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
             ck(cudaMemcpy(db->d_rank, rank.data(), sizeof(uint32_t) * n_seqs, cudaMemcpyHostToDevice));
         db->device_bytes += sizeof(uint32_t) * n_seqs + sizeof(int32_t) * alphabet_len * alphabet_len;
     }
+    // The Alignment search type traces targets back from a plain copy of the residues in db order.
+    if (bst == HY_OK && search_type == HY_SEARCH_ALIGNMENT) {
+        const uint64_t total = offsets[n_seqs] - offsets[0];
+        db->tb_off.resize(n_seqs + 1);
+        for (uint64_t k = 0; k <= n_seqs; ++k) db->tb_off[k] = offsets[k] - offsets[0];
+        ck(cudaMalloc(&db->d_tb_res, std::max<uint64_t>(total, 16)));
+        if (bst == HY_OK && total)
+            ck(cudaMemcpy(db->d_tb_res, residues + offsets[0], total, cudaMemcpyHostToDevice));
+        db->device_bytes += total;
+    }
     if (bst != HY_OK) {
         int64_t d[3];
         hy_last_error_detail(d);
@@ -647,6 +671,7 @@ void hy_db_destroy(hy_db *db) {
 uint64_t hy_db_sequence_count(const hy_db *db) { return db ? db->n_seqs : 0; }
 hy_mode hy_db_mode(const hy_db *db) { return (hy_mode)db->mode; }
 hy_search_type hy_db_search_type(const hy_db *db) { return (hy_search_type)db->search_type; }
+uint64_t hy_db_traceback_max_bytes(const hy_db *db) { return db->tb_max_bytes; }
 hy_score_width hy_db_score_width(const hy_db *db) { return db->width; }
 hy_backend hy_db_backend(const hy_db *db) { return db->backend; }
 int hy_db_layout(const hy_db *db) { return db->layout; }
@@ -742,6 +767,7 @@ void hy_scratch_destroy(hy_scratch *sc) {
     if (!sc) return;
     DeviceGuard g(sc->device);
     if (sc->stream) cudaStreamSynchronize(sc->stream);
+    tb_context_destroy(sc->tb);
     cudaFree(sc->d_query);
     cudaFree(sc->d_prof16);
     cudaFree(sc->d_prof16l);
@@ -805,7 +831,7 @@ hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[3], uint64_t 
         cells[1] = sc->event_cells[1];
         cells[2] = sc->event_cells[2];
     }
-    if (all_launches) *all_launches = sc->launches;
+    if (all_launches) *all_launches = sc->launches + tb_context_launches(sc->tb);
     sc->n_events = 0;
     sc->launches = 0;
     sc->event_cells[0] = sc->event_cells[1] = sc->event_cells[2] = 0.0;
@@ -873,7 +899,7 @@ hy_status hy_scan_all(const hy_db *db, hy_scratch *sc, const uint8_t *query, uin
     hy_status st = check_query(db, query, qlen);
     if (st != HY_OK) return st;
     DeviceGuard g(db->device);
-    const bool ends = db->search_type == HY_SEARCH_SCORE_END;
+    const bool ends = db->search_type != HY_SEARCH_SCORE;
     const uint64_t n = db->n_seqs;
     if ((st = ensure_host_out(sc)) != HY_OK) return st;
     if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
@@ -891,6 +917,38 @@ hy_status hy_scan_all(const hy_db *db, hy_scratch *sc, const uint8_t *query, uin
         out[k].query_end = ends ? (int64_t)sc->h_out[n + k] : -1;
         out[k].target_end = ends ? (int64_t)sc->h_out[2 * n + k] : -1;
     }
+    return fail(HY_OK);
+}
+
+hy_status hy_scan_aligned(const hy_db *db, hy_scratch *sc, const uint8_t *query, uint64_t qlen,
+                          uint64_t *db_index, hy_alignment *out, const uint8_t **ops) {
+    if (!db || !sc || !out || !ops || sc->db != db || db->search_type != HY_SEARCH_ALIGNMENT)
+        return fail(HY_ERR_INVALID_ARGUMENT);
+    hy_hit hit;
+    hy_status st = hy_scan(db, sc, query, qlen, &hit);
+    if (st != HY_OK) return st;
+    DeviceGuard g(db->device);
+    const uint32_t k = (uint32_t)hit.db_index;
+    st = tb_scan_targets(db, &sc->tb, sc->stream, query, qlen, &k, 1, out, sc->tb_ops);
+    if (st != HY_OK) return st;
+    if (db_index) *db_index = hit.db_index;
+    *ops = sc->tb_ops.data();
+    return fail(HY_OK);
+}
+
+hy_status hy_scan_all_aligned(const hy_db *db, hy_scratch *sc, const uint8_t *query, uint64_t qlen,
+                              hy_alignment *out, const uint8_t **ops) {
+    if (!db || !sc || !out || !ops || sc->db != db || db->search_type != HY_SEARCH_ALIGNMENT)
+        return fail(HY_ERR_INVALID_ARGUMENT);
+    hy_status st = check_query(db, query, qlen);
+    if (st != HY_OK) return st;
+    DeviceGuard g(db->device);
+    std::vector<uint32_t> idx(db->n_seqs);
+    std::iota(idx.begin(), idx.end(), 0u);
+    st = tb_scan_targets(db, &sc->tb, sc->stream, query, qlen, idx.data(), (uint32_t)db->n_seqs, out,
+                         sc->tb_ops);
+    if (st != HY_OK) return st;
+    *ops = sc->tb_ops.data();
     return fail(HY_OK);
 }
 

@@ -46,7 +46,12 @@ typedef enum {
 } hy_status;
 
 typedef enum { HY_MODE_SW = 0, HY_MODE_NW = 1, HY_MODE_HW = 2, HY_MODE_OV = 3, HY_MODE_SHW = 4 } hy_mode;
-typedef enum { HY_SEARCH_SCORE = 0, HY_SEARCH_SCORE_END = 1 } hy_search_type;
+/* SearchType (src/search.rs:13-27). HY_SEARCH_ALIGNMENT carries its max_bytes budget in the
+ * traceback_max_bytes argument of hy_db_create; it tracks ends like HY_SEARCH_SCORE_END. */
+typedef enum { HY_SEARCH_SCORE = 0, HY_SEARCH_SCORE_END = 1, HY_SEARCH_ALIGNMENT = 2 } hy_search_type;
+
+/* AlignOp (src/align.rs:47-56): one byte per operation. */
+typedef enum { HY_OP_MATCH = 0, HY_OP_MISMATCH = 1, HY_OP_INS = 2, HY_OP_DEL = 3 } hy_align_op;
 typedef enum { HY_WIDTH_I8 = 0, HY_WIDTH_I16 = 1, HY_WIDTH_I32 = 2 } hy_score_width;
 /* Backend names of src/backend.rs:25-36 plus the new `Cuda` (the enum is #[non_exhaustive]). */
 typedef enum {
@@ -71,6 +76,17 @@ typedef struct {
     int64_t query_end;
     int64_t target_end;
 } hy_hit;
+
+/* Alignment (src/align.rs:57-83): half-open spans [start, end); its operations are the n_ops bytes
+ * (hy_align_op) at ops_offset of the operation buffer the call returned or was given. */
+typedef struct {
+    int32_t score;
+    uint32_t reserved;
+    uint64_t query_start, query_end;
+    uint64_t target_start, target_end;
+    uint64_t n_ops;
+    uint64_t ops_offset;
+} hy_alignment;
 
 typedef struct hy_db hy_db;
 typedef struct hy_scratch hy_scratch;
@@ -113,13 +129,17 @@ hy_status hy_required_width(hy_mode mode, int32_t min_entry, int32_t max_entry, 
 
 /* DatabaseBuilder::build (src/database.rs:737-877): sequence k is residues[offsets[k] ..
  * offsets[k+1]] (offsets has n_seqs + 1 entries). Validates in the reference's order (scoring,
- * empty database, symbols in db order, whole-database width proof, backend), then packs the
- * database into device memory on the current CUDA device, where it stays until hy_db_destroy.
- * backend_choice: HY_CHOICE_UNSET / HY_CHOICE_AUTO / a hy_backend. layout: HY_LAYOUT_*. */
+ * empty database, symbols in db order, whole-database width proof, for HY_SEARCH_ALIGNMENT the
+ * traceback budget traceback_max_bytes against hy_traceback_min_bytes_for_database(max_query_len,
+ * longest sequence) (src/database.rs:776-790), backend), then packs the database into device
+ * memory on the current CUDA device, where it stays until hy_db_destroy. traceback_max_bytes is
+ * ignored for the other search types. backend_choice: HY_CHOICE_UNSET / HY_CHOICE_AUTO / a
+ * hy_backend. layout: HY_LAYOUT_*. */
 hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
                        const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
                        int32_t gap_ext, hy_mode mode, hy_search_type search_type,
-                       uint64_t max_query_len, int backend_choice, int layout, hy_db **out);
+                       uint64_t traceback_max_bytes, uint64_t max_query_len, int backend_choice,
+                       int layout, hy_db **out);
 void hy_db_destroy(hy_db *db);
 
 /* Accessors (src/database.rs:570-638). score_width is the reference's whole-database proof (the
@@ -307,6 +327,37 @@ hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint
 /* Timing of this thread's last hy_align_pairs call (no reference counterpart): the device time of
  * its pair kernels (CUDA events around the launches) and the wall time of the whole call. */
 hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
+
+/* ---- traceback: the Alignment search type (src/align.rs, src/database.rs:517-565) -------------- */
+
+/* align (src/align.rs:169-222): validates the scoring (src/scoring.rs:65-100), the symbols of the
+ * query then the target, the width proof on (qlen, tlen), then the traceback budget (the
+ * reference's full-matrix / sqrt-checkpoint footprint rule: HY_ERR_TRACEBACK_BUDGET_EXCEEDED with
+ * detail {needed_bytes, budget_bytes}); then traces the pair back on the current CUDA device.
+ * max_bytes = UINT64_MAX is usize::MAX. ops receives out->n_ops operations (room for qlen + tlen;
+ * out->ops_offset is 0). The device path keeps 4 bits a cell whatever the budget, and its result is
+ * the reference's for every budget that passes. The calling thread keeps grow-only buffers. */
+hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, uint64_t tlen,
+                   const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
+                   hy_mode mode, uint64_t max_bytes, hy_alignment *out, uint8_t *ops);
+/* Database::scan_aligned (src/database.rs:527-536): the winner of hy_scan (same tie-break) and its
+ * alignment. *ops points to the operations, owned by the scratch and valid until its next
+ * traceback call or its destruction. The database must be built with HY_SEARCH_ALIGNMENT
+ * (otherwise HY_ERR_INVALID_ARGUMENT, where the reference panics). */
+hy_status hy_scan_aligned(const hy_db *db, hy_scratch *scratch, const uint8_t *query, uint64_t qlen,
+                          uint64_t *db_index, hy_alignment *out, const uint8_t **ops);
+/* Database::scan_all_aligned (src/database.rs:538-549): out[k] (hy_db_sequence_count entries) is
+ * the alignment against sequence k; the operations of all of them are concatenated in db order at
+ * *ops (owned by the scratch as above), out[k].ops_offset indexing into it. */
+hy_status hy_scan_all_aligned(const hy_db *db, hy_scratch *scratch, const uint8_t *query,
+                              uint64_t qlen, hy_alignment *out, const uint8_t **ops);
+/* The budget a database built with HY_SEARCH_ALIGNMENT needs (traceback_min_bytes_for_database,
+ * src/align.rs:228-250), and traceback's rule for one problem (src/align.rs:192-222): 0 when an
+ * m x n problem traces within max_bytes, else the bytes it needs. */
+uint64_t hy_traceback_min_bytes_for_database(uint64_t max_m, uint64_t max_n);
+uint64_t hy_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes);
+/* The budget the database was built with (0 unless HY_SEARCH_ALIGNMENT). */
+uint64_t hy_db_traceback_max_bytes(const hy_db *db);
 
 #ifdef __cplusplus
 }

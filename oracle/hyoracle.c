@@ -25,6 +25,7 @@ enum {
     ST_GAP_OPEN_LESS_THAN_EXTEND = 4,
     ST_SCORE_RANGE_TOO_WIDE = 5,
     ST_SYMBOL_OUT_OF_RANGE = 6,
+    ST_TRACEBACK_BUDGET_EXCEEDED = 11,
 };
 
 /* kernel::NEG = i32::MIN / 4 (src/kernel.rs:39). */
@@ -422,4 +423,198 @@ int32_t hyo_brute(int mode, const uint8_t *q, uint64_t m, const uint8_t *t, uint
             }
         return best;
     }
+}
+
+/* ---- traceback (src/align.rs) --------------------------------------------------------------- */
+
+/* full_matrix_bytes (src/align.rs:252-258): three i32 matrices of (m+1)(n+1) cells, saturating. */
+static uint64_t sat_mul(uint64_t a, uint64_t b) {
+    unsigned __int128 p = (unsigned __int128)a * b;
+    return p > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)p;
+}
+static uint64_t full_matrix_bytes(uint64_t m, uint64_t n) {
+    return sat_mul(sat_mul(sat_mul(m + 1, n + 1), 3), 4);
+}
+/* checkpoint_bytes (src/align.rs:261-268). */
+static uint64_t checkpoint_bytes(uint64_t m, uint64_t n, uint64_t k) {
+    uint64_t num_ckpt = m / k + 1, strip_rows = k + 1;
+    return sat_mul(sat_mul(2 * num_ckpt + 3 * strip_rows, n + 1), 4);
+}
+/* u64::isqrt, then .max(1) (src/align.rs:210, 236). */
+static uint64_t strip_height(uint64_t m) {
+    uint64_t r = 0;
+    for (uint64_t bit = (uint64_t)1 << 62; bit; bit >>= 2) {
+        if (m >= r + bit) {
+            m -= r + bit;
+            r = (r >> 1) + bit;
+        } else {
+            r >>= 1;
+        }
+    }
+    return r ? r : 1;
+}
+
+/* traceback's budget rule (src/align.rs:192-222): 0 when the problem is traceable in max_bytes,
+ * else the bytes it needs (the checkpoint peak). */
+uint64_t hyo_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes) {
+    if (full_matrix_bytes(m, n) <= max_bytes || m == 0 || n == 0) return 0;
+    uint64_t peak = checkpoint_bytes(m, n, strip_height(m));
+    return peak > max_bytes ? peak : 0;
+}
+
+/* traceback_min_bytes (src/align.rs:228-236) and traceback_min_bytes_for_database (245-250). */
+static uint64_t traceback_min_bytes(uint64_t m, uint64_t n) {
+    uint64_t full = full_matrix_bytes(m, n);
+    if (m == 0 || n == 0) return full;
+    uint64_t cp = checkpoint_bytes(m, n, strip_height(m));
+    return full < cp ? full : cp;
+}
+uint64_t hyo_traceback_min_bytes_for_database(uint64_t max_m, uint64_t max_n) {
+    uint64_t v = traceback_min_bytes(max_m, max_n);
+    uint64_t a = full_matrix_bytes(max_m, 0), b = full_matrix_bytes(0, max_n);
+    if (a > v) v = a;
+    if (b > v) v = b;
+    return v;
+}
+
+/* traceback_full (src/align.rs:487-545) with fill_row (446-483), consider_row (309-327) and the
+ * shared walk (345-420): full H/E/F matrices (int64 here; every value the reference's i32
+ * arithmetic produces for an input its width proof accepts is the same), the end cell by
+ * Best::consider, then the backward walk with the reference's tie-break and stop rules, reading
+ * the three matrices' values (not a direction encoding). ops receives codes 0 Match, 1 Mismatch,
+ * 2 Ins, 3 Del (AlignOp, src/align.rs:47-56) in forward order; room for m + n codes. */
+void hyo_traceback(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
+                   const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext, int mode,
+                   hyo_alignment *out, uint8_t *ops) {
+    flags_t fl = flags_for_mode(mode);
+    const int64_t go = gap_open, ge = gap_ext;
+    const uint64_t cols = n + 1, cells = (m + 1) * cols;
+    int64_t *h = (int64_t *)malloc(sizeof(int64_t) * cells);
+    int64_t *e = (int64_t *)malloc(sizeof(int64_t) * cells);
+    int64_t *f = (int64_t *)malloc(sizeof(int64_t) * cells);
+    for (uint64_t c = 0; c < cells; ++c) {
+        h[c] = 0;
+        e[c] = ORC_NEG;
+        f[c] = ORC_NEG;
+    }
+    for (uint64_t j = 1; j <= n; ++j) {
+        h[j] = fl.top_row_free ? 0 : -gap_penalty(gap_open, gap_ext, j);
+        e[j] = fl.top_row_free ? ORC_NEG : h[j];
+    }
+    for (uint64_t i = 1; i <= m; ++i) {
+        const uint64_t b = i * cols, pb = (i - 1) * cols;
+        h[b] = fl.left_col_free ? 0 : -gap_penalty(gap_open, gap_ext, i);
+        e[b] = ORC_NEG;
+        f[b] = fl.left_col_free ? ORC_NEG : h[b];
+        for (uint64_t j = 1; j <= n; ++j) {
+            int64_t x = h[b + j - 1] - go, y = e[b + j - 1] - ge;
+            e[b + j] = x > y ? x : y;
+            x = h[pb + j] - go;
+            y = f[pb + j] - ge;
+            f[b + j] = x > y ? x : y;
+            int64_t cell = h[pb + j - 1] + matrix[(uint64_t)q[i - 1] * al + t[j - 1]];
+            if (e[b + j] > cell) cell = e[b + j];
+            if (f[b + j] > cell) cell = f[b + j];
+            if (fl.local && cell < 0) cell = 0;
+            h[b + j] = cell;
+        }
+    }
+    best_t best = {ORC_NEG, 0, 0};
+    for (uint64_t i = 0; i <= m; ++i) {
+        const int64_t *row = h + i * cols;
+        if (fl.local) {
+            for (uint64_t j = 0; j <= n; ++j) consider(&best, row[j], i, j);
+        } else {
+            if (fl.answer_last_col) consider(&best, row[n], i, n);
+            if (i == m) {
+                consider(&best, row[n], m, n);
+                if (fl.answer_last_row)
+                    for (uint64_t j = 0; j <= n; ++j) consider(&best, row[j], m, j);
+            }
+        }
+    }
+    /* walk: state 0 H, 1 E, 2 F. */
+    uint64_t i = best.row, j = best.col, k = 0;
+    int state = 0;
+    uint8_t *rev = (uint8_t *)malloc(m + n + 1);
+    for (;;) {
+        if (state == 0) {
+            const int64_t hij = h[i * cols + j];
+            if (fl.local && hij == 0) break;
+            if (i == 0 && j == 0) break;
+            if (i == 0) {
+                if (fl.top_row_free) break;
+                state = 1;
+                continue;
+            }
+            if (j == 0) {
+                if (fl.left_col_free) break;
+                state = 2;
+                continue;
+            }
+            const int64_t sub = matrix[(uint64_t)q[i - 1] * al + t[j - 1]];
+            if (hij == h[(i - 1) * cols + j - 1] + sub) {
+                rev[k++] = q[i - 1] == t[j - 1] ? 0 : 1;
+                --i;
+                --j;
+            } else if (hij == e[i * cols + j]) {
+                state = 1;
+            } else {
+                state = 2;
+            }
+        } else if (state == 1) {
+            rev[k++] = 3;
+            const int64_t ev = e[i * cols + j];
+            --j;
+            if (ev == h[i * cols + j] - go) state = 0;
+        } else {
+            rev[k++] = 2;
+            const int64_t fv = f[i * cols + j];
+            --i;
+            if (fv == h[i * cols + j] - go) state = 0;
+        }
+    }
+    for (uint64_t x = 0; x < k; ++x) ops[x] = rev[k - 1 - x];
+    out->score = (int32_t)best.score;
+    out->query_start = i;
+    out->query_end = best.row;
+    out->target_start = j;
+    out->target_end = best.col;
+    out->n_ops = k;
+    free(rev);
+    free(h);
+    free(e);
+    free(f);
+}
+
+/* align (src/align.rs:169-186) then traceback's budget rule (192-222). */
+int hyo_align(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const int32_t *matrix,
+              uint64_t al, int32_t gap_open, int32_t gap_ext, int mode, uint64_t max_bytes,
+              hyo_alignment *out, uint8_t *ops, int64_t *d1, int64_t *d2) {
+    for (uint64_t x = 0; x < m + n; ++x) {
+        const uint8_t s = x < m ? q[x] : t[x - m];
+        if (s >= al) {
+            if (d1) *d1 = s;
+            if (d2) *d2 = (int64_t)al;
+            return ST_SYMBOL_OUT_OF_RANGE;
+        }
+    }
+    int32_t mn = matrix[0], mx = matrix[0];
+    for (uint64_t x = 1; x < al * al; ++x) {
+        if (matrix[x] < mn) mn = matrix[x];
+        if (matrix[x] > mx) mx = matrix[x];
+    }
+    int64_t bound;
+    if (hyo_required_width(mode, mn, mx, gap_open, gap_ext, m, n, &bound) < 0) {
+        if (d1) *d1 = bound;
+        return ST_SCORE_RANGE_TOO_WIDE;
+    }
+    uint64_t need = hyo_traceback_needed(m, n, max_bytes);
+    if (need) {
+        if (d1) *d1 = (int64_t)need;
+        if (d2) *d2 = (int64_t)max_bytes;
+        return ST_TRACEBACK_BUDGET_EXCEEDED;
+    }
+    hyo_traceback(q, m, t, n, matrix, al, gap_open, gap_ext, mode, out, ops);
+    return ST_OK;
 }

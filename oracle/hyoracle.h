@@ -14,7 +14,7 @@
  *
  * Conventions shared with the C-ABI (include/hyalite_cuda.h):
  *   mode:        0 SW, 1 NW, 2 HW, 3 OV, 4 SHW          (src/mode.rs:11-27)
- *   search type: 0 Score, 1 ScoreEnd                   (src/search.rs:13-27)
+ *   search type: 0 Score, 1 ScoreEnd, 2 Alignment      (src/search.rs:13-27)
  *   width:       0 i8, 1 i16, 2 i32                    (src/width.rs:26-34)
  *   ends:        -1 means None                         (src/hit.rs:16-25)
  *   status:      the HY_* codes of include/hyalite_cuda.h
@@ -90,6 +90,29 @@ int hyo_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *
  * second oracle for tiny inputs. */
 int32_t hyo_brute(int mode, const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
                   const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext);
+
+/* Alignment (src/align.rs:57-83): half-open spans; ops[0 .. n_ops) hold AlignOp codes 0 Match,
+ * 1 Mismatch, 2 Ins, 3 Del (src/align.rs:47-56). */
+typedef struct {
+    int32_t score;
+    uint64_t query_start, query_end, target_start, target_end;
+    uint64_t n_ops;
+} hyo_alignment;
+
+/* traceback_full + walk (src/align.rs:345-545) on validated input (no budget): ops needs room
+ * for m + n codes. */
+void hyo_traceback(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
+                   const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext, int mode,
+                   hyo_alignment *out, uint8_t *ops);
+/* align (src/align.rs:169-222): symbols, width proof, then the traceback budget (status 11 with
+ * *d1 = needed bytes, *d2 = budget), then hyo_traceback. */
+int hyo_align(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const int32_t *matrix,
+              uint64_t al, int32_t gap_open, int32_t gap_ext, int mode, uint64_t max_bytes,
+              hyo_alignment *out, uint8_t *ops, int64_t *d1, int64_t *d2);
+/* traceback's budget rule (src/align.rs:192-222): 0 if traceable in max_bytes, else needed. */
+uint64_t hyo_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes);
+/* traceback_min_bytes_for_database (src/align.rs:228-250). */
+uint64_t hyo_traceback_min_bytes_for_database(uint64_t max_m, uint64_t max_n);
 
 #ifdef __cplusplus
 }

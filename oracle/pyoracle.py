@@ -26,6 +26,11 @@ class Hit(C.Structure):
                 ("target_end", C.c_int64)]
 
 
+class Alignment(C.Structure):
+    _fields_ = [("score", C.c_int32), ("query_start", C.c_uint64), ("query_end", C.c_uint64),
+                ("target_start", C.c_uint64), ("target_end", C.c_uint64), ("n_ops", C.c_uint64)]
+
+
 _u8p = C.POINTER(C.c_uint8)
 _u64p = C.POINTER(C.c_uint64)
 _i32p = C.POINTER(C.c_int32)
@@ -45,6 +50,10 @@ def _load():
         "hyo_scan_all_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, _u8p, C.c_uint64, C.POINTER(Hit), C.c_int]),
         "hyo_scan_scores_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _u8p, C.c_uint64, _i32p, C.c_int]),
         "hyo_align_pairs": (C.c_int, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, C.POINTER(Hit), C.c_int, _i64p, _i64p]),
+        "hyo_traceback": (None, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.POINTER(Alignment), _u8p]),
+        "hyo_align": (C.c_int, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_uint64, C.POINTER(Alignment), _u8p, _i64p, _i64p]),
+        "hyo_traceback_needed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
+        "hyo_traceback_min_bytes_for_database": (C.c_uint64, [C.c_uint64, C.c_uint64]),
         "hyo_brute": (C.c_int32, [C.c_int, _u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32]),
         "hyb_db_create": (C.c_void_p, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, C.c_uint64, C.c_int]),
         "hyb_db_destroy": (None, [C.c_void_p]),
@@ -146,6 +155,19 @@ class OracleDb:
         lib.hyo_scan_all_mt(*self._args(), self.st, _p(q, _u8p), len(query), out, threads)
         return [as_hit(out[k]) for k in range(self.n)]
 
+    def seq(self, k):
+        return self.res[int(self.off[k]): int(self.off[k + 1])]
+
+    def scan_all_aligned(self, query):
+        """Database::scan_all_aligned (src/database.rs:540-549): every sequence traced back."""
+        return [traceback(query, self.seq(k), self.mat, self.al, self.go, self.ge, self.mode)
+                for k in range(self.n)]
+
+    def scan_aligned(self, query):
+        """Database::scan_aligned (src/database.rs:527-536): (db_index, alignment) of the winner."""
+        k = self.scan(query)[1]
+        return k, traceback(query, self.seq(k), self.mat, self.al, self.go, self.ge, self.mode)
+
     def scan_scores(self, query, threads=8):
         q = _u8(np.asarray(list(query), dtype=np.int64).astype(np.uint8) if not isinstance(query, np.ndarray) else query)
         out = np.empty(max(self.n, 1), np.int32)
@@ -164,6 +186,66 @@ def align_pairs(pairs_q, pairs_t, matrix, al, go, ge, mode, search_type, threads
     st = lib.hyo_align_pairs(_p(qr, _u8p), _p(qo, _u64p), _p(tr, _u8p), _p(to, _u64p), n, _p(mat, _i32p),
                              al, go, ge, int(mode), int(search_type), out, threads, C.byref(d1), C.byref(d2))
     return st, [as_hit(out[k]) for k in range(n)], (int(d1.value), int(d2.value))
+
+
+U64_MAX = (1 << 64) - 1
+OPS = "MXID"  # AlignOp codes 0 Match, 1 Mismatch, 2 Ins, 3 Del (src/align.rs:47-56)
+
+
+def _seq(x):
+    return _u8(np.asarray(list(x) if not isinstance(x, np.ndarray) else x, dtype=np.int64).astype(np.uint8))
+
+
+def as_alignment(a, ops):
+    """(score, query_start, query_end, target_start, target_end, ops bytes)."""
+    return (int(a.score), int(a.query_start), int(a.query_end), int(a.target_start),
+            int(a.target_end), bytes(ops[: int(a.n_ops)]))
+
+
+def traceback(q, t, matrix, al, go, ge, mode):
+    """traceback_full + walk (src/align.rs:345-545) on validated input."""
+    qb, tb, mat = _seq(q), _seq(t), _mat(matrix)
+    a = Alignment()
+    ops = np.zeros(len(q) + len(t) + 1, np.uint8)
+    lib.hyo_traceback(_p(qb, _u8p), len(q), _p(tb, _u8p), len(t), _p(mat, _i32p), al, go, ge,
+                      int(mode), C.byref(a), _p(ops, _u8p))
+    return as_alignment(a, ops)
+
+
+def align(q, t, matrix, al, go, ge, mode, max_bytes=U64_MAX):
+    """align (src/align.rs:169-222): (status, alignment or None, (d1, d2))."""
+    qb, tb, mat = _seq(q), _seq(t), _mat(matrix)
+    a = Alignment()
+    ops = np.zeros(len(q) + len(t) + 1, np.uint8)
+    d1, d2 = C.c_int64(), C.c_int64()
+    st = lib.hyo_align(_p(qb, _u8p), len(q), _p(tb, _u8p), len(t), _p(mat, _i32p), al, go, ge,
+                       int(mode), max_bytes, C.byref(a), _p(ops, _u8p), C.byref(d1), C.byref(d2))
+    return st, (as_alignment(a, ops) if st == 0 else None), (int(d1.value), int(d2.value))
+
+
+def traceback_needed(m, n, max_bytes):
+    return int(lib.hyo_traceback_needed(m, n, max_bytes))
+
+
+def traceback_min_bytes_for_database(max_m, max_n):
+    return int(lib.hyo_traceback_min_bytes_for_database(max_m, max_n))
+
+
+def cigar(ops, extended=False):
+    """Alignment::cigar / cigar_extended (src/align.rs:96-130): run-length of the op letters."""
+    letters = ("=X" if extended else "MM") + "ID"
+    out, prev, run = [], None, 0
+    for o in ops:
+        c = letters[o]
+        if c == prev:
+            run += 1
+        else:
+            if prev is not None:
+                out.append(f"{run}{prev}")
+            prev, run = c, 1
+    if prev is not None:
+        out.append(f"{run}{prev}")
+    return "".join(out)
 
 
 def brute(mode, q, t, matrix, al, go, ge):
