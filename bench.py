@@ -722,6 +722,110 @@ def run_pairs(args):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes (read + write) per DP cell of the traceback fill, from one ncu capture of
+# tb_fill_kernel<16, SW> (protein generator, 20,000 sequences x the 1000-residue query); None
+# until captured. The codes alone are 0.5 byte a cell.
+TB_DRAM_BYTES_PER_CELL = None
+
+
+def run_aligned(args):
+    """Database::scan_all_aligned: the 1000-residue query of the protein workload against the first
+    --aligned-seqs sequences of the protein generator, SW, SearchType::Alignment with a usize::MAX
+    budget. `value` is real cells / the device span of the traceback (CUDA events from the first
+    fill to the end of compaction; walks overlap the next chunk's fill); `e2e` is the whole
+    hy_scan_all_aligned call (host query in, every alignment and its operations out in host
+    memory)."""
+    import torch
+
+    import hyalite_b200 as hy
+    from hyalite_b200 import _abi
+
+    torch.cuda.set_device(0)
+    mat, residues, offsets, queries = make_workload(args.seed, n_seqs=args.aligned_seqs)
+    q = next(x for x in queries if len(x) == 1000)
+    scoring = hy.Scoring(AL, [int(v) for v in mat], GO, GE)
+    t0 = time.perf_counter()
+    db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(scoring).mode(hy.Mode.Sw)
+          .search_type(hy.SearchType.alignment(hy.USIZE_MAX)).max_query_len(len(q)).build())
+    build_s = time.perf_counter() - t0
+    sc = hy.Scratch(db)
+    cells = float(len(q)) * float(offsets[-1])
+    for _ in range(args.warmup):
+        db.scan_all_aligned_arrays(sc, q)
+    lib = _abi.lib
+    kms = (C.c_double * 3)()
+    kl = (C.c_uint64 * 3)()
+    all_l = C.c_uint64()
+    lib.hy_scratch_profile_read(sc._h, kms, kl, None, C.byref(all_l))  # resets the launch count
+    clocks = Clocks(0)
+    clocks.start()
+    fill_ms = walk_ms = dev_ms = call_ms = 0.0
+    n_ops = 0
+    for _ in range(args.steps):
+        arr, buf = db.scan_all_aligned_arrays(sc, q)
+        t = hy.traceback_timing(sc)
+        fill_ms += t["fill_ms"]
+        walk_ms += t["walk_ms"]
+        dev_ms += t["device_ms"]
+        call_ms += t["call_ms"]
+        n_ops += len(buf)
+    clk = clocks.stop()
+    lib.hy_scratch_profile_read(sc._h, kms, kl, None, C.byref(all_l))
+    # Parity on a sample against the oracle's restatement of src/align.rs.
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    rng = np.random.default_rng(5)
+    sample = sorted(int(k) for k in rng.choice(args.aligned_seqs, min(args.aligned_seqs, 300), replace=False))
+    raw = buf.tobytes()
+    identical = True
+    for k in sample:
+        a = arr[k]
+        got = (int(a.score), int(a.query_start), int(a.query_end), int(a.target_start), int(a.target_end),
+               raw[int(a.ops_offset): int(a.ops_offset) + int(a.n_ops)])
+        t = residues[int(offsets[k]): int(offsets[k + 1])]
+        identical &= got == pyoracle.traceback(q, t, mat, AL, GO, GE, 0)
+    # CPU baseline: the scalar full-matrix traceback restated from src/align.rs, over all host
+    # threads, on the first --aligned-cpu-seqs sequences.
+    threads = os.cpu_count() or 1
+    n_cpu = min(args.aligned_seqs, args.aligned_cpu_seqs)
+    sub_off = offsets[: n_cpu + 1]
+    ref = pyoracle.OracleDb((residues[: int(sub_off[-1])], sub_off), mat, AL, GO, GE, 0, 1)
+    t0 = time.perf_counter()
+    ref.scan_all_aligned_mt(q, threads)
+    cpu_s = time.perf_counter() - t0
+    cpu_cells = float(len(q)) * float(sub_off[-1])
+    peak = C.c_double()
+    lib.hy_measure_dpx_peak_i32(C.byref(peak))
+    peak_gcups = peak.value / 1e9
+    fill_gcups = cells * args.steps / (fill_ms * 1e-3) / 1e9
+    line = {
+        "metric": "GCUPS", "value": cells * args.steps / (dev_ms * 1e-3) / 1e9, "unit": "GCUPS",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded protein generator: log-normal lengths, fixed background)",
+        "config": {"workload": f"scan_all_aligned: 1000-residue protein query x {args.aligned_seqs} sequences "
+                               "(the protein scan generator), SW, Alignment { max_bytes: usize::MAX }",
+                   "residues": int(offsets[-1]), "cells_per_step": cells, "db_build_s": round(build_s, 2),
+                   "ops_bytes_per_step": n_ops // args.steps,
+                   "l2": "inputs larger than L2 (walk codes: 0.5 byte a cell, gigabytes a step)"},
+        "e2e": {"value": cells * args.steps / (call_ms * 1e-3) / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": len(q),
+                "d2h_bytes_per_step": int(n_ops // args.steps + 56 * args.aligned_seqs), "call_ms": call_ms / args.steps},
+        "gpu_launches": int(all_l.value),
+        "kernels": {"fill_ms_per_step": fill_ms / args.steps, "walk_and_compaction_ms_per_step": walk_ms / args.steps},
+        "roofline": {"bound": "dpx_int32", "achieved": fill_gcups, "peak": peak_gcups, "unit": "GCUPS",
+                     "frac": fill_gcups / peak_gcups if peak_gcups else None,
+                     "traffic": (cells * TB_DRAM_BYTES_PER_CELL) if TB_DRAM_BYTES_PER_CELL else None,
+                     "kernel": "tb_fill_kernel<R, SW> (R = 16 rows per lane for the 1000-residue query)",
+                     "peak_source": "measured: hy_measure_dpx_peak_i32 (register-resident int32 per-cell DPX mix)"},
+        "identical_to_oracle_on_sample": bool(identical),
+        "cpu_baseline": {"value": cpu_cells / cpu_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+                         "sample": f"the first {n_cpu} sequences, scalar full-matrix traceback (src/align.rs) "
+                                   f"restated in C, over {threads} threads"},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SEQS, QUERY_LENGTHS, N_QUERIES
     ap = argparse.ArgumentParser()
@@ -738,7 +842,10 @@ def main():
     ap.add_argument("--query-lengths", default=",".join(map(str, QUERY_LENGTHS)))
     ap.add_argument("--n-queries", type=int, default=N_QUERIES)
     # Other workloads of the same backend (not the default benchmark line).
-    ap.add_argument("--workload", default="scan", choices=["scan", "batched", "served", "pairs", "dna_small"])
+    ap.add_argument("--workload", default="scan",
+                    choices=["scan", "batched", "served", "pairs", "dna_small", "aligned"])
+    ap.add_argument("--aligned-seqs", type=int, default=100_000)
+    ap.add_argument("--aligned-cpu-seqs", type=int, default=2_000)
     ap.add_argument("--n-pairs", type=int, default=10_000_000)
     ap.add_argument("--cpu-pairs", type=int, default=100_000)
     ap.add_argument("--n-reads", type=int, default=1_000_000)
@@ -763,6 +870,8 @@ def main():
         run_pairs(args)
     elif args.workload == "dna_small":
         run_dna_small(args)
+    elif args.workload == "aligned":
+        run_aligned(args)
     else:
         run_cuda(args)
 

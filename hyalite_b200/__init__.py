@@ -807,6 +807,15 @@ def align(query, target, scoring: Scoring, mode: Mode, max_bytes: int) -> Alignm
                      ops[: int(out.n_ops)].tobytes())
 
 
+def traceback_timing(scratch: Optional["Scratch"] = None) -> dict:
+    """Timing of the last traceback call of ``scratch`` (None: this thread's ``align``): device ms
+    of the fill and of the walk + compaction kernels, the device span (first fill to the end of
+    compaction; walks overlap the next chunk's fill), the whole call's ms, and the cells traced."""
+    out = (C.c_double * 5)()
+    _check(lib.hy_traceback_timing(None if scratch is None else scratch._h, out))
+    return {"fill_ms": out[0], "walk_ms": out[1], "device_ms": out[2], "call_ms": out[3], "cells": out[4]}
+
+
 def traceback_min_bytes_for_database(max_m: int, max_n: int) -> int:
     """src/align.rs:245-250."""
     return int(lib.hy_traceback_min_bytes_for_database(max_m, max_n))
@@ -817,6 +826,15 @@ def align_pairs_timing():
     k, c = C.c_double(), C.c_double()
     _check(lib.hy_align_pairs_timing(C.byref(k), C.byref(c)))
     return float(k.value), float(c.value)
+
+
+def align_pair(query, target, scoring: Scoring, mode: Mode, search_type) -> BestHit:
+    """align_pair (src/kernel.rs:331-352): one pair's BestHit (db_index 0). A long pair (a query of
+    256 residues or more and at least 1 Mi cells) runs on the stripe kernel, every 128 query rows
+    on their own warp."""
+    out: list = []
+    align_pairs([(query, target)], scoring, mode, search_type, out)
+    return out[0]
 
 
 def align_pairs(pairs, scoring: Scoring, mode: Mode, search_type: SearchType, out: list) -> None:
@@ -839,6 +857,6 @@ __all__ = [
     "BACKEND_ENV_VAR", "Backend", "BackendChoice", "BestHit", "Database", "DatabaseBuilder", "Error",
     "Batch", "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
     "Server", "ServerRequest", "AlignOp", "Alignment", "AlignedHit", "AlignmentSearch", "USIZE_MAX",
-    "align", "align_pairs", "align_pairs_arrays", "required_width", "concat",
-    "traceback_min_bytes_for_database",
+    "align", "align_pair", "align_pairs", "align_pairs_arrays", "required_width", "concat",
+    "traceback_min_bytes_for_database", "traceback_timing",
 ]

@@ -82,6 +82,7 @@ SIGNATURES = {
     "hy_scan_all_aligned": (_st, [_vp, _vp, _u8p, C.c_uint64, C.POINTER(HyAlignment), C.POINTER(_u8p)]),
     "hy_traceback_min_bytes_for_database": (C.c_uint64, [C.c_uint64, C.c_uint64]),
     "hy_traceback_needed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
+    "hy_traceback_timing": (_st, [_vp, C.POINTER(C.c_double)]),
     "hy_db_destroy": (None, [_vp]),
     "hy_db_sequence_count": (C.c_uint64, [_vp]),
     "hy_db_mode": (C.c_int, [_vp]),
@@ -108,6 +109,7 @@ SIGNATURES = {
     "hy_scratch_profile": (_st, [_vp, C.c_int]),
     "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, C.POINTER(C.c_double), _u64p]),
     "hy_measure_dpx_peak": (_st, [C.POINTER(C.c_double)]),
+    "hy_measure_dpx_peak_i32": (_st, [C.POINTER(C.c_double)]),
     "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
     "hy_align_pairs_timing": (_st, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),

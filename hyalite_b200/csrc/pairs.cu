@@ -17,6 +17,7 @@
 
 #include "host_common.h"
 #include "scan_kernel.cuh"
+#include "traceback_internal.h"
 
 using namespace hy;
 
@@ -27,6 +28,8 @@ constexpr int PAIR_R32 = 16;
 constexpr size_t PAIR_SMEM_LIMIT = 200 * 1024;
 // Largest global scratch for group profiles that do not fit in shared memory, per launch.
 constexpr size_t PAIR_GPROF_BYTES = 256ull << 20;
+// Most warps (128-row stripes) the long pairs of one call may take on the stripe kernel.
+constexpr uint64_t LONG_PAIR_MAX_STRIPES = 2048;
 // Rows per lane the int16x2 pair kernel is compiled for.
 constexpr int PAIR_ROWS[] = {8, 12, 16, 20, 24, 32};
 
@@ -476,6 +479,30 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
         }
     }
     if (failed_pair && first != HY_OK) *failed_pair = n_ok;
+    // A few long pairs (the single-pair path) take the score-only stripe kernel: every 128 query
+    // rows on their own warp. Many long pairs keep the packed pair kernels, whose throughput is
+    // higher once the whole GPU is busy.
+    std::vector<uint32_t> olong;
+    {
+        uint64_t stripes = 0;
+        for (const std::vector<uint32_t> *v : {&o16, &o32})
+            for (uint32_t k : *v) {
+                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
+                if (tb_long_pair(ql, tl)) {
+                    olong.push_back(k);
+                    stripes += tb_long_pair_stripes(ql);
+                }
+            }
+        if (stripes > LONG_PAIR_MAX_STRIPES) {
+            olong.clear();
+        } else if (!olong.empty()) {
+            std::vector<char> is_long(n_ok, 0);
+            for (uint32_t k : olong) is_long[k] = 1;
+            for (std::vector<uint32_t> *v : {&o16, &o32})
+                v->erase(std::remove_if(v->begin(), v->end(), [&](uint32_t k) { return is_long[k] != 0; }),
+                         v->end());
+        }
+    }
     if (n_ok > 0) {
         int dev = 0;
         HY_CK(cudaGetDevice(&dev));
@@ -506,6 +533,12 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                               cudaMemcpyHostToDevice, ctx.stream));
         int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + n_ok, *d_tend = d_qend + n_ok;
         const bool ends = search_type != HY_SEARCH_SCORE;
+        if (!olong.empty()) {
+            st = tb_long_pair_scores(q_res, q_off, t_res, t_off, olong, (const uint8_t *)d_q,
+                                     (const int32_t *)d_matrix, alphabet_len, gap_open, gap_ext, mode,
+                                     ctx.stream, d_scores, d_qend, d_tend, &ctx.kernel_ms);
+            if (st != HY_OK) return st;
+        }
         st = run_part<Pair16, PAIR_G>(ctx, 0, p16, t_res, t_off, (const uint8_t *)d_q,
                                       (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
                                       gap_ext, mode, ends, d_scores, d_qend, d_tend);

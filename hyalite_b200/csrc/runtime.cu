@@ -56,6 +56,8 @@ struct hy_scratch {
 
 namespace hy {
 
+void *scratch_tb(hy_scratch *sc) { return sc ? sc->tb : nullptr; }
+
 #define HY_CK(call)                                                                  \
     do {                                                                             \
         cudaError_t e_ = (call);                                                     \

@@ -9,8 +9,8 @@
 //
 //   bits 0-1  which state H(i,j) came from: 0 diagonal (H == H(i-1,j-1) + sub), 1 E (H == E),
 //             2 F, 3 stop (local mode and H == 0); the walk's H-state rule, tie-break included
-//   bit 2     E(i,j) == H(i,j-1) - gap_open  (leave the E state to H)
-//   bit 3     F(i,j) == H(i-1,j) - gap_open  (leave the F state to H)
+//   bit 2     E(i,j) != H(i,j-1) - gap_open  (the E state extends; clear: back to H)
+//   bit 3     F(i,j) != H(i-1,j) - gap_open  (the F state extends; clear: back to H)
 //
 // Half a byte a cell instead of twelve, written once and read only along the path. Cell values
 // are int32 with the reference's arithmetic (its width proof keeps every real cell exact), so each
@@ -18,14 +18,17 @@
 //
 // Fill kernel: one warp per (query, target) pair, each lane R consecutive query rows, lanes
 // skewed one column apart (anti-diagonal wavefront); passes of 32 * R rows joined by a boundary
-// row (H and F) in global memory. Codes are stored lane-major per step: step s of a pass writes 32
-// lanes x R/2 bytes contiguously, so every store of the warp is one coalesced 32 * R/2-byte row.
+// row (H and F) in global memory. Codes are stored step-major per lane: the R/2 bytes a lane
+// writes at consecutive steps are contiguous, so the walk's diagonal and leftward moves inside a
+// lane's rows stay within one cache line for many steps (the L2 merges the lanes' 8-byte stores
+// into full sectors before they reach DRAM).
 // The fill also reduces the end cell (Best::consider, src/align.rs:281-327) over the mode's answer
 // region. Walk kernel: one thread per pair follows the codes from the end cell, writing the
 // operations backwards into a slot of m + n bytes; a scan and a gather compact the slots.
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <mutex>
 #include <vector>
 
@@ -50,9 +53,10 @@ struct TbPair {
     uint64_t dir_off;   // code bytes
     uint64_t bnd_off;   // int2 elements: the boundary row, n + 1 entries
     uint64_t ops_off;   // operation slot of m + n bytes
+    uint64_t ends_off;  // end-cell candidates: n_ends of them (one per stripe, or one)
     uint32_t m, n, m_pad, slot;  // lengths, profile row stride, result index within the launch
     uint32_t rows;               // query rows per lane (R) of the fill
-    uint32_t pad_;
+    uint32_t n_ends;
 };
 
 // Interior end-cell candidate of a pair: the best answer-region cell with i, j >= 1.
@@ -111,150 +115,232 @@ __device__ inline void tb_store(uint8_t *p, uint32_t lo, uint32_t hi) {
     else *(uint2 *)p = make_uint2(lo, hi);
 }
 
-template <int R, int MODE>
-__global__ void __launch_bounds__(TB_BLOCK) tb_fill_kernel(TbParams P) {
-    using F = ModeFlags<MODE>;
-    const uint32_t warp = (blockIdx.x * TB_BLOCK + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= P.n_pairs) return;
-    const TbPair pr = P.pairs[warp];
-    const int m = (int)pr.m, n = (int)pr.n;
-    if (m == 0 || n == 0) return;  // border-only problems: the walk kernel resolves them alone
-    const int32_t go = P.go, ge = P.ge;
-    int2 *B = P.bnd + pr.bnd_off;
-    // Row 0: H(0, j) (src/align.rs:500-508) and F(0, j) = NEG.
-    for (int j = lane; j <= n; j += 32) {
-        int32_t h = 0;
-        if (!F::top_free && j > 0) h = (int32_t)-tb_gap(go, ge, j);
-        B[j] = make_int2(h, TB_NEG);
-    }
-    __syncwarp();
-    const uint8_t *tq = P.t_res + pr.t_off;
-    const int32_t *prof = P.prof + pr.prof_off;
-    const int rpp = 32 * R;
-    const int passes = (m + rpp - 1) / rpp;
-    const uint64_t pass_stride = (uint64_t)(n + 31) * 32 * (R / 2);
-    int32_t bs = F::local ? 0 : INT32_MIN;
-    uint32_t brow = 0, bcol = 0;
-    for (int p = 0; p < passes; ++p) {
-        const int i0 = p * rpp + lane * R + 1;  // first DP row of this lane
-        int32_t Hl[R], E[R];
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            Hl[k] = tb_left<MODE>(i0 + k, go, ge);
-            E[k] = TB_NEG;
+// Boundary rows of one pass. `in` is the row above the pass (H and F, n + 1 entries; null: row 0,
+// computed), `out` the pass's last row for the next pass (null: none). Between the warps of the
+// stripe kernel, `in_prog` / `out_prog` count the published columns of those rows.
+struct TbRows {
+    const int2 *in;
+    int2 *out;
+    const uint32_t *in_prog;
+    uint32_t *out_prog;
+    int *err;
+};
+
+constexpr uint32_t TB_PUBLISH = 32;        // columns between two progress updates of a stripe
+constexpr uint32_t TB_SPIN_LIMIT = 1u << 22;  // polls (about 0.25 us each) before a wait gives up
+
+// Waits until *prog >= need (acquire); on running out of polls records the timeout in *err and
+// stops waiting for good (the results are then discarded by the host).
+__device__ inline uint32_t tb_wait(const uint32_t *prog, uint32_t need, uint32_t avail, int *err) {
+    uint32_t it = 0;
+    while (avail < need) {
+        avail = *(const volatile uint32_t *)prog;
+        if (avail >= need) break;
+        if (++it > TB_SPIN_LIMIT) {
+            atomicExch(err, 1);
+            return 0xffffffffu;
         }
-        int32_t hdiag = tb_left<MODE>(i0 - 1, go, ge);  // H(i0 - 1, 0)
-        int32_t carry_h = 0, carry_f = TB_NEG;
-        int32_t ps = F::local ? 0 : INT32_MIN;  // this pass's best (local mode)
-        uint32_t prow = 0, pcol = 0;
-        const int km = m - i0;  // row m is Hl[km] when 0 <= km < R
-        const bool has_m = km >= 0 && km < R;
-        const int kv = min(R, m - i0 + 1);  // rows of this lane inside the query
-        uint8_t *D = P.dir + pr.dir_off + (uint64_t)p * pass_stride;
-        const int32_t *pq = prof + (i0 - 1);
-        int2 nb = make_int2(0, TB_NEG);
-        if (lane == 0) nb = B[1];
-        int cnext = (lane == 0) ? tq[0] : 0;
-        const int steps = n + 31;
-        for (int s = 0; s < steps; ++s) {
-            const int j = s - lane + 1;  // this lane's DP column
-            int32_t up_h = __shfl_up_sync(0xffffffffu, carry_h, 1);
-            int32_t up_f = __shfl_up_sync(0xffffffffu, carry_f, 1);
-            const int c = cnext;
+        __nanosleep(128);
+    }
+    __threadfence();
+    return avail;
+}
+
+// One pass of 32 * R query rows (pass p) of pair `pr` over all its columns: the DP with the walk
+// codes stored, the row for the next pass, and the pass's end-cell candidates merged into
+// (bs, brow, bcol) of this lane.
+template <int R, int MODE, bool CODES>
+__device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int p, int passes, int lane,
+                                        const TbRows &rows, int32_t &bs, uint32_t &brow, uint32_t &bcol) {
+    using F = ModeFlags<MODE>;
+    const int m = (int)pr.m, n = (int)pr.n;
+    const int32_t go = P.go, ge = P.ge;
+    const uint8_t *tq = P.t_res + pr.t_off;
+    const int rpp = 32 * R;
+    const uint64_t pass_stride = (uint64_t)(n + 31) * 32 * (R / 2);
+    const int i0 = p * rpp + lane * R + 1;  // first DP row of this lane
+    int32_t Hl[R], E[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        Hl[k] = tb_left<MODE>(i0 + k, go, ge);
+        E[k] = TB_NEG;
+    }
+    int32_t hdiag = tb_left<MODE>(i0 - 1, go, ge);  // H(i0 - 1, 0)
+    int32_t carry_h = 0, carry_f = TB_NEG;
+    int32_t ps = F::local ? 0 : INT32_MIN;  // this pass's best (local mode)
+    uint32_t prow = 0, pcol = 0;
+    const int km = m - i0;  // row m is Hl[km] when 0 <= km < R
+    const bool has_m = km >= 0 && km < R;
+    const int kv = min(R, m - i0 + 1);  // rows of this lane inside the query
+    uint8_t *D = P.dir + pr.dir_off + (uint64_t)p * pass_stride;
+    const int32_t *pq = P.prof + pr.prof_off + (i0 - 1);
+    // The row above: in place (one warp per pair), lane 0 reads it one column ahead; between
+    // stripes (published by another warp), all lanes load it 32 columns at a time from L2 once
+    // those columns are published, and lane 0 takes column j from lane (j - 1) % 32.
+    const bool batched = rows.in_prog != nullptr;
+    auto row_above = [&](int j) -> int2 {
+        if (!rows.in) {
+            int32_t h = 0;
+            if (!F::top_free && j > 0) h = (int32_t)-tb_gap(go, ge, j);
+            return make_int2(h, TB_NEG);
+        }
+        return rows.in[j];
+    };
+    uint32_t avail = 0;
+    int2 nb = make_int2(0, TB_NEG), cur = make_int2(0, TB_NEG);
+    if (lane == 0 && !batched) nb = row_above(1);
+    // Loads run ahead of the DP: the residue two steps ahead, its profile values one step ahead.
+    // Lane l works column s - l + 1 at step s.
+    auto residue = [&](int s) -> int {
+        const int col = s - lane + 1;
+        return (col >= 1 && col <= n) ? (int)tq[col - 1] : 0;
+    };
+    int4 subn[R / 4];
+    auto load_profile = [&](int s, int c) {
+        const int col = s - lane + 1;
+        if (col >= 1 && col <= n) {
+            const int32_t *pc = pq + (uint64_t)c * pr.m_pad;
+#pragma unroll
+            for (int k = 0; k < R / 4; ++k) subn[k] = *(const int4 *)(pc + 4 * k);
+        }
+    };
+    load_profile(0, residue(0));
+    int cnext = residue(1);
+    const int steps = n + 31;
+    for (int s = 0; s < steps; ++s) {
+        const int j = s - lane + 1;  // this lane's DP column
+        if (batched && (s & 31) == 0 && s < n) {
+            const uint32_t need = min((uint32_t)n, (uint32_t)s + 32);
+            if (lane == 0 && need > avail) avail = tb_wait(rows.in_prog, need, avail, rows.err);
+            __syncwarp();
+            const int col = s + 1 + lane;
+            cur = col <= n ? __ldcg(rows.in + col) : make_int2(0, TB_NEG);
+        }
+        int32_t up_h = __shfl_up_sync(0xffffffffu, carry_h, 1);
+        int32_t up_f = __shfl_up_sync(0xffffffffu, carry_f, 1);
+        if (batched) {
+            const int32_t bh = __shfl_sync(0xffffffffu, cur.x, s & 31);
+            const int32_t bf = __shfl_sync(0xffffffffu, cur.y, s & 31);
             if (lane == 0) {
-                up_h = nb.x;
-                up_f = nb.y;
-                if (j + 1 <= n) {
-                    nb = B[j + 1];
-                    cnext = tq[j];
-                }
-            } else if (j + 1 >= 1 && j + 1 <= n) {
-                cnext = tq[j];  // residue of the next step's column
+                up_h = bh;
+                up_f = bf;
             }
-            if (j >= 1 && j <= n) {
-                const int32_t *pc = pq + (uint64_t)c * pr.m_pad;
-                int32_t sub[R];
+        }
+        if (lane == 0 && !batched) {
+            up_h = nb.x;
+            up_f = nb.y;
+            if (j + 1 <= n) nb = row_above(j + 1);
+        }
+        int32_t sub[R];
 #pragma unroll
-                for (int k = 0; k < R; k += 4) {
-                    const int4 v = *(const int4 *)(pc + k);
-                    sub[k] = v.x;
-                    sub[k + 1] = v.y;
-                    sub[k + 2] = v.z;
-                    sub[k + 3] = v.w;
-                }
-                int32_t hd = hdiag, hu = up_h, fu = up_f;
-                uint32_t w0 = 0, w1 = 0;
-                int32_t colmax = 0;
+        for (int k = 0; k < R / 4; ++k) {
+            sub[4 * k] = subn[k].x;
+            sub[4 * k + 1] = subn[k].y;
+            sub[4 * k + 2] = subn[k].z;
+            sub[4 * k + 3] = subn[k].w;
+        }
+        load_profile(s + 1, cnext);
+        cnext = residue(s + 2);
+        if (j >= 1 && j <= n) {
+            int32_t hd = hdiag, hu = up_h, fu = up_f;
+            uint32_t w0 = 0, w1 = 0;
+            int32_t colmax = 0;
 #pragma unroll
-                for (int k = 0; k < R; ++k) {
-                    const int32_t hg = Hl[k] - go, eg = E[k] - ge;
-                    const int32_t e = max(hg, eg);
-                    const int32_t ug = hu - go, fg = fu - ge;
-                    const int32_t f = max(ug, fg);
+            for (int k = 0; k < R; ++k) {
+                if constexpr (!CODES) {
+                    // Score only (the DP of src/kernel.rs:168-232).
+                    const int32_t e = __viaddmax_s32(Hl[k], -go, E[k] - ge);
+                    const int32_t f = __viaddmax_s32(hu, -go, fu - ge);
                     const int32_t d = hd + sub[k];
-                    int32_t h = F::local ? __vimax3_s32_relu(d, e, f) : __vimax3_s32(d, e, f);
-                    uint32_t code = h == e ? 1u : 2u;
-                    code = h == d ? 0u : code;
-                    if (F::local) code = h == 0 ? 3u : code;
-                    code |= hg >= eg ? 4u : 0u;
-                    code |= ug >= fg ? 8u : 0u;
-                    if (k < 8) w0 |= code << (4 * k);
-                    else w1 |= code << (4 * (k - 8));
+                    const int32_t h = F::local ? __vimax3_s32_relu(d, e, f) : __vimax3_s32(d, e, f);
                     if (F::local) colmax = max(colmax, h);
                     hd = Hl[k];
                     Hl[k] = h;
                     E[k] = e;
                     hu = h;
                     fu = f;
+                    continue;
                 }
-                tb_store<R>(D + ((uint64_t)s * 32 + lane) * (R / 2), w0, w1);
-                if (lane == 31 && p + 1 < passes) B[j] = make_int2(hu, fu);
-                carry_h = hu;
-                carry_f = fu;
-                hdiag = up_h;
-                if (F::local) {
-                    if (colmax > ps) {
-                        int kk = 0;
+                // The walk's comparisons as 0/1 flags, each a difference of two values that is
+                // zero exactly when they are equal (the max is never below its operands), clamped
+                // to 1: no selects.
+                const int32_t e = __viaddmax_s32(Hl[k], -go, E[k] - ge);
+                const uint32_t e_ext = min((uint32_t)(e - Hl[k] + go), 1u);  // E != H(i,j-1) - go
+                const int32_t f = __viaddmax_s32(hu, -go, fu - ge);
+                const uint32_t f_ext = min((uint32_t)(f - hu + go), 1u);  // F != H(i-1,j) - go
+                const int32_t d = hd + sub[k];
+                int32_t h = F::local ? __vimax3_s32_relu(d, e, f) : __vimax3_s32(d, e, f);
+                const uint32_t d_ne = min((uint32_t)(h - d), 1u);
+                const uint32_t e_ne = min((uint32_t)(h - e), 1u);
+                // Source: d_ne * (1 + e_ne) is 0 diagonal, 1 E, 2 F; local H == 0 forces 3.
+                uint32_t code = d_ne * e_ne + d_ne;
+                if (F::local) code |= 3u - 3u * min((uint32_t)h, 1u);
+                code += e_ext * 4u + f_ext * 8u;
+                if (k < 8) w0 += code << (4 * k);
+                else w1 += code << (4 * (k - 8));
+                if (F::local) colmax = max(colmax, h);
+                hd = Hl[k];
+                Hl[k] = h;
+                E[k] = e;
+                hu = h;
+                fu = f;
+            }
+            if constexpr (CODES) tb_store<R>(D + ((uint64_t)lane * (n + 31) + s) * (R / 2), w0, w1);
+            if (lane == 31 && rows.out) {
+                rows.out[j] = make_int2(hu, fu);
+                if (rows.out_prog && ((uint32_t)j % TB_PUBLISH == 0 || j == n)) {
+                    __threadfence();
+                    atomicExch(rows.out_prog, (uint32_t)j);
+                }
+            }
+            carry_h = hu;
+            carry_f = fu;
+            hdiag = up_h;
+            if (F::local) {
+                if (colmax > ps) {
+                    int kk = 0;
 #pragma unroll
-                        for (int k = R - 1; k >= 0; --k)
-                            if (Hl[k] == colmax) kk = k;
-                        ps = colmax;
-                        prow = (uint32_t)(i0 + kk);
-                        pcol = (uint32_t)j;
-                    }
-                } else {
-                    if (F::last_col && j == n) {
+                    for (int k = R - 1; k >= 0; --k)
+                        if (Hl[k] == colmax) kk = k;
+                    ps = colmax;
+                    prow = (uint32_t)(i0 + kk);
+                    pcol = (uint32_t)j;
+                }
+            } else {
+                if (F::last_col && j == n) {
 #pragma unroll
-                        for (int k = 0; k < R; ++k)
-                            if (k < kv && tb_better(Hl[k], i0 + k, n, bs, brow, bcol)) {
-                                bs = Hl[k];
-                                brow = i0 + k;
-                                bcol = n;
-                            }
-                    }
-                    if (has_m && (F::last_row || j == n)) {
-                        int32_t v = Hl[0];
-#pragma unroll
-                        for (int k = 1; k < R; ++k)
-                            if (k == km) v = Hl[k];
-                        if (tb_better(v, m, j, bs, brow, bcol)) {
-                            bs = v;
-                            brow = m;
-                            bcol = j;
+                    for (int k = 0; k < R; ++k)
+                        if (k < kv && tb_better(Hl[k], i0 + k, n, bs, brow, bcol)) {
+                            bs = Hl[k];
+                            brow = i0 + k;
+                            bcol = n;
                         }
+                }
+                if (has_m && (F::last_row || j == n)) {
+                    int32_t v = Hl[0];
+#pragma unroll
+                    for (int k = 1; k < R; ++k)
+                        if (k == km) v = Hl[k];
+                    if (tb_better(v, m, j, bs, brow, bcol)) {
+                        bs = v;
+                        brow = m;
+                        bcol = j;
                     }
                 }
             }
         }
-        __syncwarp();
-        if (F::local && ps > 0 && tb_better(ps, prow, pcol, bs, brow, bcol)) {
-            bs = ps;
-            brow = prow;
-            bcol = pcol;
-        }
     }
-    // Warp reduction under the same order.
+    __syncwarp();
+    if (F::local && ps > 0 && tb_better(ps, prow, pcol, bs, brow, bcol)) {
+        bs = ps;
+        brow = prow;
+        bcol = pcol;
+    }
+}
+
+// Reduces the lanes' candidates under Best::consider's order; lane 0 writes the result.
+template <int MODE>
+__device__ inline void tb_write_end(TbEnd *dst, int lane, int32_t bs, uint32_t brow, uint32_t bcol) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const int32_t os = __shfl_xor_sync(0xffffffffu, bs, o);
@@ -267,42 +353,107 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_fill_kernel(TbParams P) {
         }
     }
     if (lane == 0) {
-        const bool valid = F::local ? bs > 0 : bs != INT32_MIN;
-        P.ends[pr.slot] = TbEnd{bs, brow, bcol, valid ? 1u : 0u};
+        const bool valid = ModeFlags<MODE>::local ? bs > 0 : bs != INT32_MIN;
+        *dst = TbEnd{bs, brow, bcol, valid ? 1u : 0u};
     }
 }
 
-// The code of interior cell (i, j), i, j >= 1, in the fill's lane-major layout.
-__device__ inline uint32_t tb_code(const uint8_t *D, uint32_t R, uint64_t pass_stride, uint32_t i,
-                                   uint32_t j) {
-    const uint32_t r = i - 1, c = j - 1;
-    const uint32_t rpp = 32 * R;
-    const uint32_t p = r / rpp, rr = r - p * rpp;
-    const uint32_t l = rr / R, k = rr - l * R;
-    const uint64_t at = (uint64_t)p * pass_stride + ((uint64_t)(c + l) * 32 + l) * (R / 2) + (k >> 1);
-    return (D[at] >> (4 * (k & 1))) & 15u;
+// Throughput form: one warp per pair, its passes in sequence, the boundary row in place.
+template <int R, int MODE>
+__global__ void __launch_bounds__(TB_BLOCK) tb_fill_kernel(TbParams P) {
+    using F = ModeFlags<MODE>;
+    const uint32_t warp = (blockIdx.x * TB_BLOCK + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= P.n_pairs) return;
+    const TbPair pr = P.pairs[warp];
+    const int m = (int)pr.m, n = (int)pr.n;
+    if (m == 0 || n == 0) return;  // border-only problems: the walk kernel resolves them alone
+    int2 *B = P.bnd + pr.bnd_off;
+    // Row 0: H(0, j) (src/align.rs:500-508) and F(0, j) = NEG.
+    for (int j = lane; j <= n; j += 32) {
+        int32_t h = 0;
+        if (!F::top_free && j > 0) h = (int32_t)-tb_gap(P.go, P.ge, j);
+        B[j] = make_int2(h, TB_NEG);
+    }
+    __syncwarp();
+    const int passes = (m + 32 * R - 1) / (32 * R);
+    int32_t bs = F::local ? 0 : INT32_MIN;
+    uint32_t brow = 0, bcol = 0;
+    for (int p = 0; p < passes; ++p) {
+        const TbRows rows{B, p + 1 < passes ? B : nullptr, nullptr, nullptr, nullptr};
+        tb_pass<R, MODE, true>(P, pr, p, passes, lane, rows, bs, brow, bcol);
+    }
+    tb_write_end<MODE>(P.ends + pr.ends_off, lane, bs, brow, bcol);
 }
 
-// The end cell (src/align.rs:309-327 over every row) and the walk (src/align.rs:345-420).
-template <int MODE>
-__global__ void __launch_bounds__(TB_BLOCK) tb_walk_kernel(TbParams P) {
+// Latency form for few long pairs: every pass (stripe) of every pair on its own warp, all warps
+// resident at once (cooperative launch). Stripe s reads the row stripe s - 1 publishes, column by
+// column, so the stripes of one pair run as a pipeline instead of in sequence. Pair x owns the
+// stripes [first[x], first[x + 1]); warp w takes stripes w, w + warps, ... in increasing order,
+// so each waits only on a lower stripe that is already running or done. CODES = false runs the
+// score-only DP (the long pairs of align_pairs) and records only the end-cell candidates.
+struct TbStripes {
+    const uint32_t *first;  // per pair: first stripe (n_pairs + 1 entries)
+    uint32_t n_stripes;
+    int2 *bnd;              // per pair: (stripes - 1) rows of n + 1 entries at TbPair::bnd_off
+    uint32_t *prog;         // per stripe: published columns of its last row (zeroed before launch)
+    int *err;
+};
+
+template <int R, int MODE, bool CODES>
+__global__ void __launch_bounds__(TB_BLOCK) tb_stripe_kernel(TbParams P, TbStripes S) {
     using F = ModeFlags<MODE>;
-    const uint32_t t = blockIdx.x * TB_BLOCK + threadIdx.x;
-    if (t >= P.n_pairs) return;
-    const TbPair pr = P.pairs[t];
+    const uint32_t warps = gridDim.x * (TB_BLOCK / 32);
+    const int lane = threadIdx.x & 31;
+    for (uint32_t g = (blockIdx.x * TB_BLOCK + threadIdx.x) >> 5; g < S.n_stripes; g += warps) {
+        uint32_t lo = 0, hi = P.n_pairs;  // the pair x with first[x] <= g < first[x + 1]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (S.first[mid] <= g) lo = mid; else hi = mid;
+        }
+        const uint32_t pi = lo, s = g - S.first[pi];
+        const TbPair pr = P.pairs[pi];
+        const int m = (int)pr.m, n = (int)pr.n;
+        if (m == 0 || n == 0) continue;
+        const int passes = (m + 32 * R - 1) / (32 * R);
+        if ((int)s >= passes) continue;
+        int2 *B = S.bnd + pr.bnd_off;
+        const TbRows rows{s == 0 ? nullptr : B + (uint64_t)(s - 1) * (n + 1),
+                          (int)s + 1 < passes ? B + (uint64_t)s * (n + 1) : nullptr,
+                          s == 0 ? nullptr : S.prog + g - 1, S.prog + g, S.err};
+        int32_t bs = F::local ? 0 : INT32_MIN;
+        uint32_t brow = 0, bcol = 0;
+        tb_pass<R, MODE, CODES>(P, pr, (int)s, passes, lane, rows, bs, brow, bcol);
+        tb_write_end<MODE>(P.ends + pr.ends_off + s, lane, bs, brow, bcol);
+    }
+}
+
+// The code of interior cell (i, j), i, j >= 1, in the fill's layout (R = 1 << r_log2 rows per lane).
+__device__ inline uint32_t tb_code(const uint8_t *D, uint32_t r_log2, uint64_t pass_stride, uint32_t n_cols,
+                                   uint32_t i, uint32_t j) {
+    const uint32_t r = i - 1, c = j - 1;
+    const uint32_t p = r >> (5 + r_log2), rr = r & ((32u << r_log2) - 1);
+    const uint32_t l = rr >> r_log2, k = rr & ((1u << r_log2) - 1);
+    const uint64_t at = (uint64_t)p * pass_stride + (((uint64_t)l * (n_cols + 31) + (c + l)) << (r_log2 - 1)) + (k >> 1);
+    return (__ldg(D + at) >> (4 * (k & 1))) & 15u;
+}
+
+// The end cell of a pair (src/align.rs:309-327 over every row): the fill's interior candidates
+// merged with the border candidates. H(0, j) and H(i, 0) never increase with j or i, so among
+// border cells of row 0 or column 0 the one nearest the corner (0, 0) wins.
+template <int MODE>
+__device__ inline void tb_end_cell(const TbPair &pr, const TbEnd *ends, int32_t go, int32_t ge, int32_t &bs,
+                                   uint32_t &brow, uint32_t &bcol) {
+    using F = ModeFlags<MODE>;
     const uint32_t m = pr.m, n = pr.n;
-    const int32_t go = P.go, ge = P.ge;
     auto top = [&](uint32_t j) -> int32_t {  // H(0, j)
         return (F::top_free || j == 0) ? 0 : (int32_t)-tb_gap(go, ge, j);
     };
     auto left = [&](uint32_t i) -> int32_t {  // H(i, 0)
         return (F::left_free || i == 0) ? 0 : (int32_t)-tb_gap(go, ge, i);
     };
-    // End cell: the fill's interior candidate merged with the border candidates. H(0, j) and
-    // H(i, 0) never increase with j or i, so among border cells of row 0 or column 0 the one
-    // nearest the corner (0, 0) wins.
-    int32_t bs = INT32_MIN;
-    uint32_t brow = 0, bcol = 0;
+    bs = INT32_MIN;
+    brow = bcol = 0;
     auto consider = [&](int32_t s, uint32_t r, uint32_t c) {
         if (tb_better(s, r, c, bs, brow, bcol)) {
             bs = s;
@@ -311,8 +462,10 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_walk_kernel(TbParams P) {
         }
     };
     if (m > 0 && n > 0) {
-        const TbEnd e = P.ends[pr.slot];
-        if (e.valid) consider(e.score, e.row, e.col);
+        for (uint32_t x = 0; x < pr.n_ends; ++x) {
+            const TbEnd e = ends[pr.ends_off + x];
+            if (e.valid) consider(e.score, e.row, e.col);
+        }
     }
     if (F::local) {
         consider(0, 0, 0);
@@ -328,9 +481,21 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_walk_kernel(TbParams P) {
             if (m == 0) consider(0, 0, 0);
         }
     }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(64) tb_walk_kernel(TbParams P) {
+    using F = ModeFlags<MODE>;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n_pairs) return;
+    const TbPair pr = P.pairs[t];
+    const uint32_t m = pr.m, n = pr.n;
+    int32_t bs;
+    uint32_t brow, bcol;
+    tb_end_cell<MODE>(pr, P.ends, P.go, P.ge, bs, brow, bcol);
     // Walk. State 0 H, 1 E, 2 F.
     const uint8_t *D = P.dir + pr.dir_off;
-    const uint32_t R = pr.rows;
+    const uint32_t R = pr.rows, r_log2 = 31 - __clz(R);
     const uint64_t pass_stride = (uint64_t)(n + 31) * 32 * (R / 2);
     const uint8_t *qs = P.q_res + pr.q_off;
     const uint8_t *ts = P.t_res + pr.t_off;
@@ -361,7 +526,7 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_walk_kernel(TbParams P) {
             }
             break;
         }
-        const uint32_t code = tb_code(D, R, pass_stride, i, j);
+        const uint32_t code = tb_code(D, r_log2, pass_stride, n, i, j);
         if (state == 0) {
             const uint32_t src = code & 3u;
             if (src == 3u) break;
@@ -369,17 +534,18 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_walk_kernel(TbParams P) {
                 if (cnt < cap) slot[cap - 1 - cnt++] = qs[i - 1] == ts[j - 1] ? 0 : 1;
                 --i;
                 --j;
-            } else {
-                state = (int)src;
+                continue;
             }
-        } else if (state == 1) {
+            state = (int)src;  // the gap step below reads the same cell's code
+        }
+        if (state == 1) {
             if (cnt < cap) slot[cap - 1 - cnt++] = 3;
             --j;
-            if (code & 4u) state = 0;
+            if (!(code & 4u)) state = 0;
         } else {
             if (cnt < cap) slot[cap - 1 - cnt++] = 2;
             --i;
-            if (code & 8u) state = 0;
+            if (!(code & 8u)) state = 0;
         }
     }
     hy_alignment a;
@@ -429,6 +595,21 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_gather_kernel(TbParams P) {
     for (uint64_t x = lane; x < a.n_ops; x += 32) dst[x] = src[x];
 }
 
+// align_pairs' long pairs: the end cell of each pair as a BestHit (score, 0-based ends or -1),
+// written at the pair's index (src/kernel.rs:239-277 via the same Best rule).
+template <int MODE>
+__global__ void tb_pair_hits_kernel(TbParams P, int32_t *scores, int32_t *qend, int32_t *tend) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n_pairs) return;
+    const TbPair pr = P.pairs[t];
+    int32_t bs;
+    uint32_t brow, bcol;
+    tb_end_cell<MODE>(pr, P.ends, P.go, P.ge, bs, brow, bcol);
+    scores[pr.slot] = bs;
+    qend[pr.slot] = brow == 0 ? -1 : (int32_t)(brow - 1);
+    tend[pr.slot] = bcol == 0 ? -1 : (int32_t)(bcol - 1);
+}
+
 // Query profile for the fill: prof[c * m_pad + r] = matrix[q[r] * al + c] for r < m, 0 for the
 // padding rows (sub = 0 there keeps every padding cell below a real cell of no larger column and
 // smaller row, so padding never wins the local end cell).
@@ -458,6 +639,20 @@ static uint32_t tb_rows(uint64_t m, uint64_t n) {
         }
     }
     return best;
+}
+
+// align_pairs sends a pair to the score-only stripe kernel when its query spans several stripes
+// and it is large: the int16x2 pair kernels give one pair one 8-lane group, far too little for a
+// single pair of thousands of residues each.
+constexpr uint64_t TB_LONG_PAIR_ROWS = 256;
+constexpr double TB_LONG_PAIR_CELLS = 1024.0 * 1024;
+
+// Few pairs of a multi-pass query fill with the stripe kernel at 4 rows per lane (128-row
+// stripes: the most warps per pair); many pairs fill one warp each at tb_rows.
+constexpr uint32_t TB_STRIPE_PAIRS = 16;
+static void tb_plan(uint64_t m, uint64_t max_n, uint32_t n_pairs, uint32_t *R, bool *stripes) {
+    *stripes = n_pairs <= TB_STRIPE_PAIRS && m > 128;
+    *R = *stripes ? 4u : tb_rows(m, max_n);  // 4: the stripe kernel's rows per lane
 }
 
 static uint64_t tb_passes(uint64_t m, uint32_t R) { return std::max<uint64_t>(1, (m + 32 * R - 1) / (32 * R)); }
@@ -497,30 +692,47 @@ static cudaError_t grow_pinned(T *&p, uint64_t &cap, uint64_t need) {
 // for hy_align).
 struct TbContext {
     int device = -1;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;    // fills, then the copies back (the caller's stream)
+    cudaStream_t stream_b = nullptr;  // walks and compaction, overlapping the next chunk's fill
     bool own_stream = false;
-    uint8_t *d_q = nullptr, *d_t = nullptr, *d_dir = nullptr, *d_ops = nullptr, *d_ops_out = nullptr;
+    uint8_t *d_q = nullptr, *d_t = nullptr, *d_ops = nullptr, *d_ops_out = nullptr;
+    uint8_t *d_dir[2] = {nullptr, nullptr};  // codes of two chunks in flight
     int32_t *d_prof = nullptr, *d_matrix = nullptr;
     int2 *d_bnd = nullptr;
     TbPair *d_pairs = nullptr;
     TbEnd *d_ends = nullptr;
     hy_alignment *d_out = nullptr;
     uint64_t *d_total = nullptr;
-    uint64_t c_q = 0, c_t = 0, c_dir = 0, c_ops = 0, c_ops_out = 0, c_prof = 0, c_matrix = 0, c_bnd = 0,
+    uint32_t *d_prog = nullptr;  // stripe kernel: error flag (first 16 bytes), then progress counters
+    uint32_t *d_first = nullptr, *h_first = nullptr;  // stripe kernel: first stripe of each pair
+    uint64_t c_prog = 0, c_first = 0, ch_first = 0;
+    uint64_t c_q = 0, c_t = 0, c_ops = 0, c_ops_out = 0, c_prof = 0, c_matrix = 0, c_bnd = 0,
              c_pairs = 0, c_ends = 0, c_out = 0, c_total = 0;
+    uint64_t c_dir[2] = {0, 0};
     TbPair *h_pairs = nullptr;
     hy_alignment *h_out = nullptr;
-    uint8_t *h_ops = nullptr;
+    uint8_t *h_ops = nullptr, *h_q = nullptr;
     uint64_t *h_total = nullptr;
-    uint64_t ch_pairs = 0, ch_out = 0, ch_ops = 0, ch_total = 0;
+    uint64_t ch_pairs = 0, ch_out = 0, ch_ops = 0, ch_total = 0, ch_q = 0;
     uint64_t launches = 0;
+    // Per chunk: fill start / end on `stream`, walk start / end on `stream_b`.
+    std::vector<cudaEvent_t> ev;
+    // Timing of the last call: the fill kernels, the walk + compaction kernels, the device span
+    // from the first fill to the end of compaction (CUDA events), the whole call (host clock), and
+    // the DP cells traced.
+    double fill_ms = 0.0, walk_ms = 0.0, device_ms = 0.0, call_ms = 0.0, cells = 0.0;
     ~TbContext() {
         if (stream) cudaStreamSynchronize(stream);
-        for (void *p : {(void *)d_q, (void *)d_t, (void *)d_dir, (void *)d_ops, (void *)d_ops_out,
-                        (void *)d_prof, (void *)d_matrix, (void *)d_bnd, (void *)d_pairs, (void *)d_ends,
-                        (void *)d_out, (void *)d_total})
+        if (stream_b) cudaStreamSynchronize(stream_b);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        for (void *p : {(void *)d_q, (void *)d_t, (void *)d_dir[0], (void *)d_dir[1], (void *)d_ops,
+                        (void *)d_ops_out, (void *)d_prof, (void *)d_matrix, (void *)d_bnd, (void *)d_pairs,
+                        (void *)d_ends, (void *)d_out, (void *)d_total, (void *)d_prog, (void *)d_first})
             cudaFree(p);
-        for (void *p : {(void *)h_pairs, (void *)h_out, (void *)h_ops, (void *)h_total}) cudaFreeHost(p);
+        for (void *p : {(void *)h_pairs, (void *)h_out, (void *)h_ops, (void *)h_total, (void *)h_q,
+                        (void *)h_first})
+            cudaFreeHost(p);
+        if (stream_b) cudaStreamDestroy(stream_b);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -543,10 +755,49 @@ static cudaError_t launch_fill(uint32_t R, const TbParams &p, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// The walk is one thread per pair and bound by the latency of its dependent code loads: small
+// blocks spread the walkers over every SM.
+constexpr int TB_WALK_BLOCK = 64;
+
 template <int MODE>
 static cudaError_t launch_walk(const TbParams &p, cudaStream_t st) {
-    tb_walk_kernel<MODE><<<(p.n_pairs + TB_BLOCK - 1) / TB_BLOCK, TB_BLOCK, 0, st>>>(p);
+    tb_walk_kernel<MODE><<<(p.n_pairs + TB_WALK_BLOCK - 1) / TB_WALK_BLOCK, TB_WALK_BLOCK, 0, st>>>(p);
     return cudaGetLastError();
+}
+
+// Rows per lane of the stripe kernel: 128-row stripes, the most warps per pair.
+constexpr uint32_t TB_STRIPE_R = 4;
+
+template <int MODE, bool CODES>
+static cudaError_t launch_stripes(const TbParams &p, const TbStripes &S, cudaStream_t st, int device) {
+    auto kern = tb_stripe_kernel<TB_STRIPE_R, MODE, CODES>;
+    int per_sm = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB_BLOCK, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    const uint64_t want = ((uint64_t)S.n_stripes * 32 + TB_BLOCK - 1) / TB_BLOCK;
+    const uint32_t blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per_sm * sms));
+    TbParams pc = p;
+    TbStripes sc = S;
+    void *args[] = {(void *)&pc, (void *)&sc};
+    return cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(TB_BLOCK), args, 0, st);
+}
+
+static cudaError_t dispatch_stripes(int mode, bool codes, const TbParams &p, const TbStripes &S,
+                                    cudaStream_t st, int device) {
+#define TB_STRIPE_CASE(M)                                                                          \
+    case M:                                                                                        \
+        return codes ? launch_stripes<M, true>(p, S, st, device) : launch_stripes<M, false>(p, S, st, device);
+    switch (mode) {
+        TB_STRIPE_CASE(MODE_SW)
+        TB_STRIPE_CASE(MODE_NW)
+        TB_STRIPE_CASE(MODE_HW)
+        TB_STRIPE_CASE(MODE_OV)
+        TB_STRIPE_CASE(MODE_SHW)
+    }
+#undef TB_STRIPE_CASE
+    return cudaErrorInvalidValue;
 }
 
 static cudaError_t dispatch_fill(int mode, uint32_t R, const TbParams &p, cudaStream_t st) {
@@ -580,6 +831,7 @@ struct TbRun {
     const uint8_t *d_t_res;        // device targets
     const uint64_t *h_t_off;       // host offsets of the targets (n_targets + 1), or null
     const uint64_t *h_t_single;    // a single target: {offset, length} when h_t_off is null
+    bool stripes;                  // fill with the stripe kernel (few long pairs)
 };
 
 static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, uint32_t n_idx,
@@ -588,109 +840,160 @@ static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, u
     auto t_len = [&](uint32_t k) {
         return run.h_t_off ? run.h_t_off[k + 1] - run.h_t_off[k] : run.h_t_single[1];
     };
-    uint64_t ops_base = 0;
-    uint32_t a = 0;
-    while (a < n_idx) {
-        // Chunk [a, b): code bytes within TB_CHUNK_BYTES (at least one pair).
-        uint32_t b = a;
-        uint64_t dir = 0, bnd = 0, ops = 0;
-        while (b < n_idx) {
-            const uint64_t n = t_len(idx[b]);
-            const uint64_t d = align16(tb_dir_bytes(run.m, n, run.R));
-            if (b > a && dir + d > TB_CHUNK_BYTES) break;
-            dir += d;
-            bnd += n + 1;
-            ops += run.m + n;
-            ++b;
+    const auto t_start = std::chrono::steady_clock::now();
+    ctx.fill_ms = ctx.walk_ms = ctx.device_ms = ctx.cells = 0.0;
+    if (!ctx.stream_b) TB_CK(cudaStreamCreateWithFlags(&ctx.stream_b, cudaStreamNonBlocking));
+    // Launch order: longest target first over the whole call, so every chunk holds targets of
+    // similar length (short tails) and the longest start first. Results keep the caller's order.
+    std::vector<uint32_t> order(n_idx);
+    for (uint32_t x = 0; x < n_idx; ++x) order[x] = x;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return t_len(idx[x]) > t_len(idx[y]); });
+    // Operation slots in the caller's order; chunks of at most TB_CHUNK_BYTES of codes.
+    TB_CK(grow_pinned(ctx.h_pairs, ctx.ch_pairs, sizeof(TbPair) * n_idx));
+    std::vector<uint64_t> ops_at(n_idx);
+    uint64_t oo = 0;
+    for (uint32_t x = 0; x < n_idx; ++x) {
+        ops_at[x] = oo;
+        oo += run.m + t_len(idx[x]);
+    }
+    std::vector<uint32_t> chunk_at{0};
+    uint64_t dir_max = 0, bnd_max = 0, dir = 0, bnd = 0;
+    const uint32_t per_pair = run.stripes ? (uint32_t)tb_passes(run.m, run.R) : 1u;
+    for (uint32_t x = 0; x < n_idx; ++x) {
+        const uint32_t s = order[x], k = idx[s];
+        const uint64_t n = t_len(k);
+        const uint64_t d = align16(tb_dir_bytes(run.m, n, run.R));
+        if (x > chunk_at.back() && dir + d > TB_CHUNK_BYTES) {
+            chunk_at.push_back(x);
+            dir = bnd = 0;
         }
-        const uint32_t cnt = b - a;
-        TB_CK(grow_pinned(ctx.h_pairs, ctx.ch_pairs, sizeof(TbPair) * cnt));
-        // Launch order: longest target first (load balance); slots stay in the caller's order.
-        std::vector<uint32_t> order(cnt);
-        for (uint32_t x = 0; x < cnt; ++x) order[x] = x;
-        std::stable_sort(order.begin(), order.end(),
-                         [&](uint32_t x, uint32_t y) { return t_len(idx[a + x]) > t_len(idx[a + y]); });
-        uint64_t od = 0, ob = 0, oo = 0;
-        std::vector<uint64_t> ops_at(cnt);
-        for (uint32_t x = 0; x < cnt; ++x) {
-            ops_at[x] = oo;
-            oo += run.m + t_len(idx[a + x]);
-        }
-        for (uint32_t x = 0; x < cnt; ++x) {
-            const uint32_t s = order[x], k = idx[a + s];
-            TbPair &pp = ctx.h_pairs[x];
-            pp.q_off = 0;
-            pp.prof_off = 0;
-            pp.t_off = t_off(k);
-            pp.m = (uint32_t)run.m;
-            pp.n = (uint32_t)t_len(k);
-            pp.m_pad = run.m_pad;
-            pp.slot = s;
-            pp.rows = run.R;
-            pp.pad_ = 0;
-            pp.dir_off = od;
-            od += align16(tb_dir_bytes(run.m, pp.n, run.R));
-            pp.bnd_off = ob;
-            ob += pp.n + 1;
-            pp.ops_off = ops_at[s];
-        }
-        TB_CK(grow(ctx.d_pairs, ctx.c_pairs, sizeof(TbPair) * cnt));
-        TB_CK(grow(ctx.d_dir, ctx.c_dir, od));
-        TB_CK(grow(ctx.d_bnd, ctx.c_bnd, sizeof(int2) * ob));
-        TB_CK(grow(ctx.d_ops, ctx.c_ops, oo));
-        TB_CK(grow(ctx.d_ops_out, ctx.c_ops_out, oo));
-        TB_CK(grow(ctx.d_ends, ctx.c_ends, sizeof(TbEnd) * cnt));
-        TB_CK(grow(ctx.d_out, ctx.c_out, sizeof(hy_alignment) * cnt));
-        TB_CK(grow(ctx.d_total, ctx.c_total, 16));
-        TB_CK(grow_pinned(ctx.h_out, ctx.ch_out, sizeof(hy_alignment) * cnt));
-        TB_CK(grow_pinned(ctx.h_total, ctx.ch_total, 16));
-        TB_CK(cudaMemcpyAsync(ctx.d_pairs, ctx.h_pairs, sizeof(TbPair) * cnt, cudaMemcpyHostToDevice, ctx.stream));
-        TbParams p;
-        p.pairs = ctx.d_pairs;
-        p.n_pairs = cnt;
-        p.q_res = ctx.d_q;
-        p.t_res = run.d_t_res;
-        p.prof = ctx.d_prof;
-        p.dir = ctx.d_dir;
-        p.bnd = ctx.d_bnd;
-        p.ends = ctx.d_ends;
-        p.out = ctx.d_out;
-        p.ops = ctx.d_ops;
-        p.ops_out = ctx.d_ops_out;
-        p.total = ctx.d_total;
-        p.go = run.go;
-        p.ge = run.ge;
-        if (run.m > 0) {
+        TbPair &pp = ctx.h_pairs[x];
+        pp.q_off = 0;
+        pp.prof_off = 0;
+        pp.t_off = t_off(k);
+        pp.m = (uint32_t)run.m;
+        pp.n = (uint32_t)n;
+        pp.m_pad = run.m_pad;
+        pp.slot = s;
+        pp.rows = run.R;
+        pp.n_ends = per_pair;
+        pp.ends_off = run.stripes ? (uint64_t)x * per_pair : s;
+        pp.dir_off = dir;
+        pp.bnd_off = bnd;
+        pp.ops_off = ops_at[s];
+        dir += d;
+        bnd += run.stripes ? (uint64_t)(per_pair - 1) * (n + 1) : n + 1;
+        dir_max = std::max(dir_max, dir);
+        bnd_max = std::max(bnd_max, bnd);
+        ctx.cells += (double)run.m * (double)n;
+    }
+    chunk_at.push_back(n_idx);
+    const size_t n_chunks = chunk_at.size() - 1;
+    TB_CK(grow(ctx.d_pairs, ctx.c_pairs, sizeof(TbPair) * n_idx));
+    TB_CK(grow(ctx.d_dir[0], ctx.c_dir[0], dir_max));
+    if (n_chunks > 1) TB_CK(grow(ctx.d_dir[1], ctx.c_dir[1], dir_max));
+    TB_CK(grow(ctx.d_bnd, ctx.c_bnd, sizeof(int2) * bnd_max));
+    TB_CK(grow(ctx.d_ops, ctx.c_ops, oo));
+    TB_CK(grow(ctx.d_ops_out, ctx.c_ops_out, oo));
+    TB_CK(grow(ctx.d_ends, ctx.c_ends, sizeof(TbEnd) * n_idx * per_pair));
+    if (run.stripes) {
+        TB_CK(grow(ctx.d_prog, ctx.c_prog, sizeof(uint32_t) * (uint64_t)n_idx * per_pair + 16));
+        TB_CK(cudaMemsetAsync(ctx.d_prog, 0, 16, ctx.stream));  // the error flag sits in front
+        // Every pair has per_pair stripes: chunk-local pair x owns [x, x + 1) * per_pair.
+        TB_CK(grow(ctx.d_first, ctx.c_first, sizeof(uint32_t) * (n_idx + 1)));
+        TB_CK(grow_pinned(ctx.h_first, ctx.ch_first, sizeof(uint32_t) * (n_idx + 1)));
+        for (uint32_t x = 0; x <= n_idx; ++x) ctx.h_first[x] = x * per_pair;
+        TB_CK(cudaMemcpyAsync(ctx.d_first, ctx.h_first, sizeof(uint32_t) * (n_idx + 1), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    }
+    TB_CK(grow(ctx.d_out, ctx.c_out, sizeof(hy_alignment) * n_idx));
+    TB_CK(grow(ctx.d_total, ctx.c_total, 16));
+    TB_CK(grow_pinned(ctx.h_out, ctx.ch_out, sizeof(hy_alignment) * n_idx));
+    TB_CK(grow_pinned(ctx.h_total, ctx.ch_total, 16));
+    while (ctx.ev.size() < 4 * n_chunks + 2) {
+        cudaEvent_t e;
+        TB_CK(cudaEventCreate(&e));
+        ctx.ev.push_back(e);
+    }
+    TB_CK(cudaMemcpyAsync(ctx.d_pairs, ctx.h_pairs, sizeof(TbPair) * n_idx, cudaMemcpyHostToDevice, ctx.stream));
+    TbParams p;
+    p.q_res = ctx.d_q;
+    p.t_res = run.d_t_res;
+    p.prof = ctx.d_prof;
+    p.bnd = ctx.d_bnd;
+    p.ends = ctx.d_ends;
+    p.out = ctx.d_out;
+    p.ops = ctx.d_ops;
+    p.ops_out = ctx.d_ops_out;
+    p.total = ctx.d_total;
+    p.go = run.go;
+    p.ge = run.ge;
+    // Chunk c: fill on `stream` into codes buffer c % 2 (once the walk of chunk c - 2 is done with
+    // it), walk on `stream_b` once the fill is done.
+    for (size_t c = 0; c < n_chunks; ++c) {
+        cudaEvent_t *e = &ctx.ev[4 * c];
+        p.pairs = ctx.d_pairs + chunk_at[c];
+        p.n_pairs = chunk_at[c + 1] - chunk_at[c];
+        p.dir = ctx.d_dir[c & 1];
+        if (c >= 2) TB_CK(cudaStreamWaitEvent(ctx.stream, ctx.ev[4 * (c - 2) + 3], 0));
+        TB_CK(cudaEventRecord(e[0], ctx.stream));
+        if (run.m > 0 && run.stripes) {
+            const uint32_t n_str = p.n_pairs * per_pair;
+            TbStripes S{ctx.d_first, n_str, ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+            TB_CK(cudaMemsetAsync(S.prog, 0, sizeof(uint32_t) * n_str, ctx.stream));
+            TB_CK(dispatch_stripes(run.mode, true, p, S, ctx.stream, ctx.device));
+            ctx.launches += 2;
+        } else if (run.m > 0) {
             TB_CK(dispatch_fill(run.mode, run.R, p, ctx.stream));
             ++ctx.launches;
         }
-        TB_CK(dispatch_walk(run.mode, p, ctx.stream));
-        tb_scan_kernel<<<1, 1024, 0, ctx.stream>>>(ctx.d_out, cnt, ctx.d_total);
-        TB_CK(cudaGetLastError());
-        tb_gather_kernel<<<(uint32_t)(((uint64_t)cnt * 32 + TB_BLOCK - 1) / TB_BLOCK), TB_BLOCK, 0, ctx.stream>>>(p);
-        TB_CK(cudaGetLastError());
-        ctx.launches += 3;
-        TB_CK(cudaMemcpyAsync(ctx.h_out, ctx.d_out, sizeof(hy_alignment) * cnt, cudaMemcpyDeviceToHost, ctx.stream));
-        TB_CK(cudaMemcpyAsync(ctx.h_total, ctx.d_total, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx.stream));
-        TB_CK(cudaStreamSynchronize(ctx.stream));
-        const uint64_t total = *ctx.h_total;
-        if (ops_direct) {
-            if (total) TB_CK(cudaMemcpy(ops_direct + ops_base, ctx.d_ops_out, total, cudaMemcpyDeviceToHost));
-        } else {
-            TB_CK(grow_pinned(ctx.h_ops, ctx.ch_ops, total));
-            if (total) {
-                TB_CK(cudaMemcpyAsync(ctx.h_ops, ctx.d_ops_out, total, cudaMemcpyDeviceToHost, ctx.stream));
-                TB_CK(cudaStreamSynchronize(ctx.stream));
-            }
-            ops_host->insert(ops_host->end(), ctx.h_ops, ctx.h_ops + total);
-        }
-        for (uint32_t x = 0; x < cnt; ++x) {
-            out[a + x] = ctx.h_out[x];
-            out[a + x].ops_offset += ops_base;
-        }
-        ops_base += total;
-        a = b;
+        TB_CK(cudaEventRecord(e[1], ctx.stream));
+        TB_CK(cudaStreamWaitEvent(ctx.stream_b, e[1], 0));
+        TB_CK(cudaEventRecord(e[2], ctx.stream_b));
+        TB_CK(dispatch_walk(run.mode, p, ctx.stream_b));
+        ++ctx.launches;
+        TB_CK(cudaEventRecord(e[3], ctx.stream_b));
     }
+    // Compaction over the whole call, in the caller's order.
+    p.pairs = ctx.d_pairs;
+    p.n_pairs = n_idx;
+    tb_scan_kernel<<<1, 1024, 0, ctx.stream_b>>>(ctx.d_out, n_idx, ctx.d_total);
+    TB_CK(cudaGetLastError());
+    tb_gather_kernel<<<(uint32_t)(((uint64_t)n_idx * 32 + TB_BLOCK - 1) / TB_BLOCK), TB_BLOCK, 0, ctx.stream_b>>>(p);
+    TB_CK(cudaGetLastError());
+    ctx.launches += 2;
+    cudaEvent_t e_end = ctx.ev[4 * n_chunks];
+    TB_CK(cudaEventRecord(e_end, ctx.stream_b));
+    TB_CK(cudaStreamWaitEvent(ctx.stream, e_end, 0));
+    TB_CK(cudaMemcpyAsync(ctx.h_out, ctx.d_out, sizeof(hy_alignment) * n_idx, cudaMemcpyDeviceToHost, ctx.stream));
+    TB_CK(cudaMemcpyAsync(ctx.h_total, ctx.d_total, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx.stream));
+    if (run.stripes) TB_CK(cudaMemcpyAsync(ctx.h_total + 1, ctx.d_prog, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.stream));
+    TB_CK(cudaStreamSynchronize(ctx.stream));
+    if (run.stripes && *(const uint32_t *)(ctx.h_total + 1)) return fail(HY_ERR_TIMEOUT);
+    const uint64_t total = *ctx.h_total;
+    if (ops_direct) {
+        if (total) TB_CK(cudaMemcpyAsync(ops_direct, ctx.d_ops_out, total, cudaMemcpyDeviceToHost, ctx.stream));
+    } else {
+        TB_CK(grow_pinned(ctx.h_ops, ctx.ch_ops, total));
+        if (total) TB_CK(cudaMemcpyAsync(ctx.h_ops, ctx.d_ops_out, total, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    TB_CK(cudaStreamSynchronize(ctx.stream));
+    if (!ops_direct) ops_host->assign(ctx.h_ops, ctx.h_ops + total);
+    memcpy(out, ctx.h_out, sizeof(hy_alignment) * n_idx);
+    for (size_t c = 0; c < n_chunks; ++c) {
+        float f_ms = 0.f, w_ms = 0.f;
+        TB_CK(cudaEventElapsedTime(&f_ms, ctx.ev[4 * c], ctx.ev[4 * c + 1]));
+        TB_CK(cudaEventElapsedTime(&w_ms, ctx.ev[4 * c + 2], ctx.ev[4 * c + 3]));
+        ctx.fill_ms += f_ms;
+        ctx.walk_ms += w_ms;
+    }
+    float span = 0.f, tail = 0.f;
+    TB_CK(cudaEventElapsedTime(&span, ctx.ev[0], e_end));
+    TB_CK(cudaEventElapsedTime(&tail, ctx.ev[4 * n_chunks - 1], e_end));
+    ctx.device_ms = span;
+    ctx.walk_ms += tail;
+    ctx.call_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     return fail(HY_OK);
 }
 
@@ -700,9 +1003,10 @@ static hy_status tb_prepare_query(TbContext &ctx, const uint8_t *query, uint64_t
     TB_CK(grow(ctx.d_q, ctx.c_q, std::max<uint64_t>(m, 1)));
     TB_CK(grow(ctx.d_prof, ctx.c_prof, sizeof(int32_t) * al * *m_pad));
     if (m) {
-        TB_CK(grow_pinned(ctx.h_ops, ctx.ch_ops, m));
-        memcpy(ctx.h_ops, query, m);
-        TB_CK(cudaMemcpyAsync(ctx.d_q, ctx.h_ops, m, cudaMemcpyHostToDevice, ctx.stream));
+        TB_CK(cudaStreamSynchronize(ctx.stream));  // the staging buffer of the previous call is free
+        TB_CK(grow_pinned(ctx.h_q, ctx.ch_q, m));
+        memcpy(ctx.h_q, query, m);
+        TB_CK(cudaMemcpyAsync(ctx.d_q, ctx.h_q, m, cudaMemcpyHostToDevice, ctx.stream));
     }
     const uint64_t total = al * (uint64_t)*m_pad;
     const uint32_t blocks = (uint32_t)std::min<uint64_t>(1024, (total + 255) / 256);
@@ -764,6 +1068,12 @@ uint64_t hy_traceback_min_bytes_for_database(uint64_t max_m, uint64_t max_n) {
 
 static thread_local TbContext *g_align_ctx = nullptr;
 
+hy_status hy_traceback_timing(hy_scratch *scratch, double out[5]) {
+    if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
+    tb_context_timing(scratch ? scratch_tb(scratch) : (void *)g_align_ctx, out);
+    return fail(HY_OK);
+}
+
 hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, uint64_t tlen,
                    const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
                    hy_mode mode, uint64_t max_bytes, hy_alignment *out, uint8_t *ops) {
@@ -810,7 +1120,9 @@ hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, u
     TB_CK(cudaMemcpyAsync(ctx.d_matrix, matrix, mat_bytes, cudaMemcpyHostToDevice, ctx.stream));
     TB_CK(grow(ctx.d_t, ctx.c_t, std::max<uint64_t>(tlen, 1)));
     if (tlen) TB_CK(cudaMemcpyAsync(ctx.d_t, target, tlen, cudaMemcpyHostToDevice, ctx.stream));
-    const uint32_t R = tb_rows(qlen, tlen);
+    uint32_t R = 0;
+    bool stripes = false;
+    tb_plan(qlen, tlen, 1, &R, &stripes);
     uint32_t m_pad = 0;
     st = tb_prepare_query(ctx, query, qlen, ctx.d_matrix, alphabet_len, R, &m_pad);
     if (st != HY_OK) return st;
@@ -821,6 +1133,7 @@ hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, u
     run.m = qlen;
     run.m_pad = m_pad;
     run.R = R;
+    run.stripes = stripes;
     run.d_t_res = ctx.d_t;
     run.h_t_off = nullptr;
     const uint64_t single[2] = {0, tlen};
@@ -847,7 +1160,9 @@ hy_status tb_scan_targets(const hy_db *db, void **ctx_slot, cudaStream_t stream,
     uint64_t max_n = 0;
     for (uint32_t x = 0; x < n_idx; ++x)
         max_n = std::max<uint64_t>(max_n, db->tb_off[idx[x] + 1] - db->tb_off[idx[x]]);
-    const uint32_t R = tb_rows(qlen, max_n);
+    uint32_t R = 0;
+    bool stripes = false;
+    tb_plan(qlen, max_n, n_idx, &R, &stripes);
     uint32_t m_pad = 0;
     hy_status st = tb_prepare_query(*ctx, query, qlen, db->d_matrix, db->al, R, &m_pad);
     if (st != HY_OK) return st;
@@ -858,11 +1173,145 @@ hy_status tb_scan_targets(const hy_db *db, void **ctx_slot, cudaStream_t stream,
     run.m = qlen;
     run.m_pad = m_pad;
     run.R = R;
+    run.stripes = stripes;
     run.d_t_res = db->d_tb_res;
     run.h_t_off = db->tb_off.data();
     run.h_t_single = nullptr;
     ops.clear();
     return tb_run(*ctx, run, idx, n_idx, out, &ops, nullptr);
+}
+
+bool tb_long_pair(uint64_t qlen, uint64_t tlen) {
+    return qlen >= TB_LONG_PAIR_ROWS && (double)qlen * (double)tlen >= TB_LONG_PAIR_CELLS;
+}
+
+uint64_t tb_long_pair_stripes(uint64_t qlen) { return tb_passes(qlen, TB_STRIPE_R); }
+
+static thread_local TbContext *g_pairs_ctx = nullptr;
+
+hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                              const uint64_t *t_off, const std::vector<uint32_t> &idx, const uint8_t *d_q,
+                              const int32_t *d_matrix, uint64_t al, int32_t go, int32_t ge, int mode,
+                              cudaStream_t stream, int32_t *d_scores, int32_t *d_qend, int32_t *d_tend,
+                              double *kernel_ms) {
+    (void)q_res;
+    const uint32_t n = (uint32_t)idx.size();
+    if (n == 0) return fail(HY_OK);
+    int dev = 0;
+    TB_CK(cudaGetDevice(&dev));
+    if (g_pairs_ctx && g_pairs_ctx->device != dev) {
+        delete g_pairs_ctx;
+        g_pairs_ctx = nullptr;
+    }
+    if (!g_pairs_ctx) {
+        g_pairs_ctx = new TbContext;
+        g_pairs_ctx->device = dev;
+    }
+    TbContext &ctx = *g_pairs_ctx;
+    ctx.stream = stream;  // the caller's stream: ordered after its query upload, before its copy back
+    if (ctx.ev.size() < 2) {
+        for (int x = 0; x < 2; ++x) {
+            cudaEvent_t e;
+            TB_CK(cudaEventCreate(&e));
+            ctx.ev.push_back(e);
+        }
+    }
+    // Targets, profiles, boundary rows and stripes of every long pair.
+    uint64_t t_total = 0, prof_total = 0, bnd_total = 0;
+    uint32_t n_str = 0;
+    TB_CK(grow_pinned(ctx.h_pairs, ctx.ch_pairs, sizeof(TbPair) * n));
+    TB_CK(grow_pinned(ctx.h_first, ctx.ch_first, sizeof(uint32_t) * (n + 1)));
+    for (uint32_t x = 0; x < n; ++x) {
+        const uint32_t k = idx[x];
+        const uint64_t m = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
+        const uint32_t S = (uint32_t)tb_passes(m, TB_STRIPE_R);
+        TbPair &pp = ctx.h_pairs[x];
+        pp.q_off = q_off[k];
+        pp.m = (uint32_t)m;
+        pp.n = (uint32_t)tl;
+        pp.m_pad = S * 32 * TB_STRIPE_R;
+        pp.prof_off = prof_total;
+        pp.t_off = t_total;
+        pp.dir_off = 0;
+        pp.bnd_off = bnd_total;
+        pp.ops_off = 0;
+        pp.ends_off = n_str;
+        pp.n_ends = S;
+        pp.slot = k;
+        pp.rows = TB_STRIPE_R;
+        ctx.h_first[x] = n_str;
+        prof_total += al * pp.m_pad;
+        t_total += tl;
+        bnd_total += (uint64_t)(S - 1) * (tl + 1);
+        n_str += S;
+    }
+    ctx.h_first[n] = n_str;
+    TB_CK(grow_pinned(ctx.h_ops, ctx.ch_ops, t_total));
+    for (uint32_t x = 0; x < n; ++x) {
+        const uint32_t k = idx[x];
+        memcpy(ctx.h_ops + ctx.h_pairs[x].t_off, t_res + t_off[k], t_off[k + 1] - t_off[k]);
+    }
+    TB_CK(grow(ctx.d_t, ctx.c_t, t_total));
+    TB_CK(grow(ctx.d_prof, ctx.c_prof, sizeof(int32_t) * prof_total));
+    TB_CK(grow(ctx.d_bnd, ctx.c_bnd, sizeof(int2) * std::max<uint64_t>(bnd_total, 1)));
+    TB_CK(grow(ctx.d_pairs, ctx.c_pairs, sizeof(TbPair) * n));
+    TB_CK(grow(ctx.d_first, ctx.c_first, sizeof(uint32_t) * (n + 1)));
+    TB_CK(grow(ctx.d_ends, ctx.c_ends, sizeof(TbEnd) * n_str));
+    TB_CK(grow(ctx.d_prog, ctx.c_prog, sizeof(uint32_t) * n_str + 16));
+    TB_CK(grow(ctx.d_dir[0], ctx.c_dir[0], 16));
+    TB_CK(cudaMemcpyAsync(ctx.d_t, ctx.h_ops, t_total, cudaMemcpyHostToDevice, stream));
+    TB_CK(cudaMemcpyAsync(ctx.d_pairs, ctx.h_pairs, sizeof(TbPair) * n, cudaMemcpyHostToDevice, stream));
+    TB_CK(cudaMemcpyAsync(ctx.d_first, ctx.h_first, sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, stream));
+    TB_CK(cudaMemsetAsync(ctx.d_prog, 0, sizeof(uint32_t) * n_str + 16, stream));
+    for (uint32_t x = 0; x < n; ++x) {
+        const TbPair &pp = ctx.h_pairs[x];
+        const uint64_t total = al * (uint64_t)pp.m_pad;
+        const uint32_t blocks = (uint32_t)std::min<uint64_t>(1024, (total + 255) / 256);
+        tb_profile_kernel<<<blocks, 256, 0, stream>>>(d_q + pp.q_off, pp.m, pp.m_pad, d_matrix, (uint32_t)al,
+                                                      ctx.d_prof + pp.prof_off);
+        TB_CK(cudaGetLastError());
+    }
+    TbParams p;
+    memset(&p, 0, sizeof(p));
+    p.pairs = ctx.d_pairs;
+    p.n_pairs = n;
+    p.q_res = d_q;
+    p.t_res = ctx.d_t;
+    p.prof = ctx.d_prof;
+    p.dir = ctx.d_dir[0];
+    p.bnd = ctx.d_bnd;
+    p.ends = ctx.d_ends;
+    p.go = go;
+    p.ge = ge;
+    TbStripes S{ctx.d_first, n_str, ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+    TB_CK(cudaEventRecord(ctx.ev[0], stream));
+    TB_CK(dispatch_stripes(mode, false, p, S, stream, dev));
+    TB_CK(cudaEventRecord(ctx.ev[1], stream));
+    switch (mode) {
+    case MODE_SW: tb_pair_hits_kernel<MODE_SW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+    case MODE_NW: tb_pair_hits_kernel<MODE_NW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+    case MODE_HW: tb_pair_hits_kernel<MODE_HW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+    case MODE_OV: tb_pair_hits_kernel<MODE_OV><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+    default: tb_pair_hits_kernel<MODE_SHW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+    }
+    TB_CK(cudaGetLastError());
+    TB_CK(grow_pinned(ctx.h_total, ctx.ch_total, 16));
+    TB_CK(cudaMemcpyAsync(ctx.h_total, ctx.d_prog, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    TB_CK(cudaStreamSynchronize(stream));
+    if (*(const uint32_t *)ctx.h_total) return fail(HY_ERR_TIMEOUT);
+    float ms = 0.f;
+    TB_CK(cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]));
+    if (kernel_ms) *kernel_ms += ms;
+    return fail(HY_OK);
+}
+
+void tb_context_timing(void *ctx, double out[5]) {
+    const TbContext *c = (const TbContext *)ctx;
+    out[0] = c ? c->fill_ms : 0.0;
+    out[1] = c ? c->walk_ms : 0.0;
+    out[2] = c ? c->device_ms : 0.0;
+    out[3] = c ? c->call_ms : 0.0;
+    out[4] = c ? c->cells : 0.0;
 }
 
 uint64_t tb_context_launches(void *ctx) {

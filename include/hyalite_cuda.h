@@ -217,6 +217,9 @@ hy_status hy_scratch_profile_read(hy_scratch *scratch, double kernel_ms[3], uint
 /* The packed-int16 DPX roofline of the current device: the scan's per-cell instruction mix run
  * register resident on every SM, in DP cells per second. */
 hy_status hy_measure_dpx_peak(double *cells_per_second);
+/* The same recurrence in int32 DPX lanes (one cell per op): the roofline of the int32 kernels
+ * (the traceback fill and the int32 scan items), in DP cells per second. */
+hy_status hy_measure_dpx_peak_i32(double *cells_per_second);
 
 /* ---- batched scan (no reference counterpart: the reference scans one query per call) ---------- */
 
@@ -356,6 +359,11 @@ hy_status hy_scan_all_aligned(const hy_db *db, hy_scratch *scratch, const uint8_
  * m x n problem traces within max_bytes, else the bytes it needs. */
 uint64_t hy_traceback_min_bytes_for_database(uint64_t max_m, uint64_t max_n);
 uint64_t hy_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes);
+/* Timing of the last traceback call of a scratch (scratch NULL: of this thread's hy_align), no
+ * reference counterpart: out = {fill kernels' device ms, walk and compaction kernels' device ms,
+ * device span from the first fill to the end of compaction in ms (walks overlap the next chunk's
+ * fill), whole call ms, DP cells traced}. Device times are CUDA events. */
+hy_status hy_traceback_timing(hy_scratch *scratch, double out[5]);
 /* The budget the database was built with (0 unless HY_SEARCH_ALIGNMENT). */
 uint64_t hy_db_traceback_max_bytes(const hy_db *db);
 

@@ -618,3 +618,21 @@ int hyo_align(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const 
     hyo_traceback(q, m, t, n, matrix, al, gap_open, gap_ext, mode, out, ops);
     return ST_OK;
 }
+
+/* Database::scan_all_aligned (src/database.rs:538-549): hyo_traceback of the query against every
+ * sequence, spread over `threads` OpenMP threads. Alignment k's operations go to the slot at
+ * ops + k * qlen + (offsets[k] - offsets[0]) (room for qlen + |t_k| codes). */
+void hyo_scan_all_aligned_mt(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                             const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
+                             int mode, const uint8_t *query, uint64_t qlen, hyo_alignment *out,
+                             uint8_t *ops, int threads) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads > 0 ? threads : 1)
+#endif
+    for (int64_t k = 0; k < (int64_t)n_seqs; ++k) {
+        const uint64_t a = offsets[k], b = offsets[k + 1];
+        hyo_traceback(query, qlen, residues + a, b - a, matrix, al, gap_open, gap_ext, mode, &out[k],
+                      ops + (uint64_t)k * qlen + (a - offsets[0]));
+    }
+    (void)threads;
+}

@@ -109,6 +109,12 @@ void hyo_traceback(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n,
 int hyo_align(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const int32_t *matrix,
               uint64_t al, int32_t gap_open, int32_t gap_ext, int mode, uint64_t max_bytes,
               hyo_alignment *out, uint8_t *ops, int64_t *d1, int64_t *d2);
+/* Database::scan_all_aligned over `threads` threads (src/database.rs:538-549): alignment k's
+ * codes go to ops + k * qlen + (offsets[k] - offsets[0]). */
+void hyo_scan_all_aligned_mt(const uint8_t *residues, const uint64_t *offsets, uint64_t n_seqs,
+                             const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
+                             int mode, const uint8_t *query, uint64_t qlen, hyo_alignment *out,
+                             uint8_t *ops, int threads);
 /* traceback's budget rule (src/align.rs:192-222): 0 if traceable in max_bytes, else needed. */
 uint64_t hyo_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes);
 /* traceback_min_bytes_for_database (src/align.rs:228-250). */

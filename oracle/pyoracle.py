@@ -52,6 +52,7 @@ def _load():
         "hyo_align_pairs": (C.c_int, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_int, C.POINTER(Hit), C.c_int, _i64p, _i64p]),
         "hyo_traceback": (None, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.POINTER(Alignment), _u8p]),
         "hyo_align": (C.c_int, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_uint64, C.POINTER(Alignment), _u8p, _i64p, _i64p]),
+        "hyo_scan_all_aligned_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _u8p, C.c_uint64, C.POINTER(Alignment), _u8p, C.c_int]),
         "hyo_traceback_needed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
         "hyo_traceback_min_bytes_for_database": (C.c_uint64, [C.c_uint64, C.c_uint64]),
         "hyo_brute": (C.c_int32, [C.c_int, _u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32]),
@@ -162,6 +163,19 @@ class OracleDb:
         """Database::scan_all_aligned (src/database.rs:540-549): every sequence traced back."""
         return [traceback(query, self.seq(k), self.mat, self.al, self.go, self.ge, self.mode)
                 for k in range(self.n)]
+
+    def scan_all_aligned_mt(self, query, threads=8):
+        """scan_all_aligned over `threads` threads: list of alignment tuples."""
+        q = _seq(query)
+        out = (Alignment * max(self.n, 1))()
+        cap = self.n * len(query) + int(self.off[-1] - self.off[0]) + 1
+        ops = np.zeros(cap, np.uint8)
+        lib.hyo_scan_all_aligned_mt(*self._args(), _p(q, _u8p), len(query), out, _p(ops, _u8p), threads)
+        res = []
+        for k in range(self.n):
+            base = k * len(query) + int(self.off[k] - self.off[0])
+            res.append(as_alignment(out[k], ops[base: base + int(out[k].n_ops)]))
+        return res
 
     def scan_aligned(self, query):
         """Database::scan_aligned (src/database.rs:527-536): (db_index, alignment) of the winner."""

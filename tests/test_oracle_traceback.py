@@ -223,3 +223,12 @@ def test_database_alignment_matches_free_align():
             best = max(a[0] for a in want)
             k, a = db.scan_aligned(q)
             assert k == [a_[0] for a_ in want].index(best) and a == want[k]
+
+
+def test_threaded_scan_all_aligned_equals_the_serial_one():
+    rng = Lcg(3)
+    seqs = [[(rng.next() % 4) for _ in range(rng.next() % 40)] for _ in range(60)]
+    q = [(rng.next() % 4) for _ in range(30)]
+    for mode in ALL_MODES:
+        db = o.OracleDb(seqs, SCORINGS[0][0], 4, 2, 1, mode, 1)
+        assert db.scan_all_aligned_mt(q, 4) == db.scan_all_aligned(q)

@@ -115,3 +115,46 @@ def test_first_failure_found_in_a_later_host_chunk():
     assert status == 0
     assert [(h.score, h.query_end, h.target_end) for h in (out[i] for i in sample)] == \
         [(w[0], w[2], w[3]) for w in want]
+
+
+def _related(rng, seq, al, rate=0.2):
+    out = []
+    for x in seq:
+        r = rng.random()
+        if r < rate / 3:
+            continue
+        out.append(int(rng.integers(0, al)) if r < 2 * rate / 3 else int(x))
+        if rate * 2 / 3 <= r < rate:
+            out.append(int(rng.integers(0, al)))
+    return out
+
+
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_long_pairs_take_the_stripe_kernel(mode):
+    """src/kernel.rs:378-397 (the single long pair): pairs with a query of 256+ residues and 1 Mi+
+    cells run on the score-only stripe kernel, mixed in one call with short pairs that keep the
+    packed kernels; int16-range and int32-range scorings; Score and ScoreEnd."""
+    rng = np.random.default_rng(70 + mode)
+    base = list(rng.integers(0, 20, 3000))
+    qs = [base[:2000], list(rng.integers(0, 20, 600)), base[500:1524], list(rng.integers(0, 20, 30))]
+    ts = [_related(rng, base[:2000], 20), list(rng.integers(0, 20, 7000)), _related(rng, base, 20, 0.4),
+          list(rng.integers(0, 20, 50))]
+    qs += [list(rng.integers(0, 20, int(rng.integers(1, 200)))) for _ in range(50)]
+    ts += [list(rng.integers(0, 20, int(rng.integers(1, 300)))) for _ in range(50)]
+    for st in (0, 1):
+        got, want = run_both(qs, ts, BLOSUM62, 20, 11, 1, mode, st)
+        assert got == want, [(k, got[k], want[k]) for k in range(len(got)) if got[k] != want[k]][:4]
+    big = [int(v) for v in rng.integers(-900, 900, 400)]
+    got, want = run_both(qs[:3], ts[:3], big, 20, 50, 3, mode, 1)
+    assert got == want
+
+
+def test_single_long_pair_align_pair():
+    """The 2000 x 2000 single pair of the single-pair path, every mode."""
+    rng = np.random.default_rng(77)
+    q = list(rng.integers(0, 20, 2000))
+    t = _related(rng, q, 20, 0.3)
+    for mode in ALL_MODES:
+        h = hy.align_pair(q, t, hy.Scoring(20, BLOSUM62, 11, 1), hy.Mode(mode), hy.SearchType.ScoreEnd)
+        assert (h.score, h.db_index, h.query_end, h.target_end) == \
+            (lambda s: (s[0], 0, s[1], s[2]))(o.align_pair(q, t, BLOSUM62, 20, 11, 1, mode))

@@ -136,6 +136,25 @@ def test_scan_all_aligned_and_scan_aligned_match_the_oracle():
             assert hit.db_index == db.scan(sc, q).db_index
 
 
+def test_few_long_pairs_take_the_stripe_pipeline():
+    """Up to 16 targets of a multi-stripe query fill with the stripe kernel (every 128-row stripe
+    on its own warp, rows handed down column by column): several pairs in one launch, an empty
+    target, targets shorter than one publish interval, and all five modes."""
+    rng = np.random.default_rng(31)
+    q = list(rng.integers(0, 20, 1500))
+    seqs = [_mutate(rng, q[a: a + L], 20, 0.2) for a, L in ((0, 1500), (300, 900), (10, 5), (700, 40))]
+    seqs += [[], [7], list(rng.integers(0, 20, 2600)), _mutate(rng, q, 20, 0.5)]
+    for mode in ALL_MODES:
+        db = _db(seqs, BLOSUM62, 20, 11, 1, mode, 1500)
+        sc = hy.Scratch(db)
+        out = []
+        db.scan_all_aligned(sc, q, out)
+        ref = o.OracleDb(seqs, BLOSUM62, 20, 11, 1, mode, 1)
+        assert [a.as_tuple() for a in out] == ref.scan_all_aligned(q), mode
+        hit = db.scan_aligned(sc, q)
+        assert (hit.db_index, hit.alignment.as_tuple()) == ref.scan_aligned(q)
+
+
 @pytest.mark.parametrize("case", G["database"], ids=lambda c: c["cite"])
 def test_database_known_answers(case):
     mat, al, go, ge = _scoring(case["scoring"])
@@ -179,27 +198,28 @@ def _rescore(a, q, t, mat, al, go, ge):
     return total
 
 
-def test_database_scale_properties():
-    """A 3000-sequence protein database against a 1000-residue query: every alignment's score is
-    the scan score, its end cell is scan_all's end, its operations re-score to the score, and a
-    sample matches the oracle exactly."""
+@pytest.mark.parametrize("mode,n_seqs", [(0, 12000), (2, 3000)])
+def test_database_scale_properties(mode, n_seqs):
+    """A protein database against a 1000-residue query: every alignment's score is the scan score,
+    its end cell is scan_all's end, its operations re-score to the score, and a sample matches the
+    oracle exactly. 12,000 sequences hold about 2.4 GB of walk codes: more than one chunk, so the
+    two-stream chunk pipeline and the whole-call compaction are exercised."""
     rng = np.random.default_rng(23)
     q = list(rng.integers(0, 20, 1000))
     seqs = []
-    for _ in range(3000):
+    for _ in range(n_seqs):
         L = int(rng.integers(50, 700))
         a = int(rng.integers(0, 1000 - min(L, 999)))
         seqs.append(_mutate(rng, q[a: a + L], 20, 0.4) if rng.random() < 0.5 else list(rng.integers(0, 20, L)))
-    for mode in (0, 2):
-        db = _db(seqs, BLOSUM62, 20, 11, 1, mode, 1000)
-        sc = hy.Scratch(db)
-        out = []
-        db.scan_all_aligned(sc, q, out)
-        hits = db.scan_all_array(sc, q)
-        for k, (a, h) in enumerate(zip(out, hits)):
-            assert a.score == h.score
-            assert a.query_end == (h.query_end + 1 if h.query_end >= 0 else 0)
-            assert a.target_end == (h.target_end + 1 if h.target_end >= 0 else 0)
-            assert _rescore(a, q, seqs[k], BLOSUM62, 20, 11, 1) == a.score
-        for k in rng.integers(0, len(seqs), 6):
-            assert out[k].as_tuple() == o.traceback(q, seqs[k], BLOSUM62, 20, 11, 1, mode)
+    db = _db(seqs, BLOSUM62, 20, 11, 1, mode, 1000)
+    sc = hy.Scratch(db)
+    out = []
+    db.scan_all_aligned(sc, q, out)
+    hits = db.scan_all_array(sc, q)
+    for k, (a, h) in enumerate(zip(out, hits)):
+        assert a.score == h.score
+        assert a.query_end == (h.query_end + 1 if h.query_end >= 0 else 0)
+        assert a.target_end == (h.target_end + 1 if h.target_end >= 0 else 0)
+        assert _rescore(a, q, seqs[k], BLOSUM62, 20, 11, 1) == a.score
+    for k in rng.integers(0, len(seqs), 6):
+        assert out[k].as_tuple() == o.traceback(q, seqs[k], BLOSUM62, 20, 11, 1, mode)
