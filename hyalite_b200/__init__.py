@@ -828,6 +828,55 @@ def align_pairs_timing():
     return float(k.value), float(c.value)
 
 
+def align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, min_score: Optional[int] = None):
+    """align_pair_position_max over many pairs (src/kernel.rs:474-553) on the device: returns
+    (hits ctypes array, column maxima int32 array aligned with t_res, score2 int32 array of
+    (score, position) per pair or None, (error or None, failed index)). ``min_score`` set: each pair's
+    score2 (src/kernel.rs:741-792) with its best score, its target end (0 when None) and the
+    matrix's largest entry; position -1 means None."""
+    q_res = np.ascontiguousarray(q_res, dtype=np.uint8)
+    t_res = np.ascontiguousarray(t_res, dtype=np.uint8)
+    q_res = q_res if q_res.size else np.zeros(1, np.uint8)
+    t_res = t_res if t_res.size else np.zeros(1, np.uint8)
+    q_off = np.ascontiguousarray(q_off, dtype=np.uint64)
+    t_off = np.ascontiguousarray(t_off, dtype=np.uint64)
+    n = len(q_off) - 1
+    out = (_abi.HyHit * max(n, 1))()
+    cm = np.zeros(max(1, int(t_off[-1] - t_off[0])) if n else 1, np.int32)
+    s2 = np.zeros(2 * max(n, 1), np.int32) if min_score is not None else None
+    failed = C.c_uint64()
+    st = lib.hy_align_pairs_position_max(
+        _ptr(q_res, _abi._u8p), _ptr(q_off, _abi._u64p), _ptr(t_res, _abi._u8p), _ptr(t_off, _abi._u64p), n,
+        _ptr(scoring._matrix, _abi._i32p), scoring._al, scoring._go, scoring._ge, _ptr(cm, _abi._i32p), out,
+        0 if min_score is None else int(min_score), None if s2 is None else _ptr(s2, _abi._i32p), C.byref(failed))
+    err = None if st == _abi.OK else Error.from_status(st)
+    return out, cm, s2, (err, int(failed.value))
+
+
+def align_pair_position_max(query, target, scoring: Scoring, out: list) -> BestHit:
+    """align_pair_position_max (src/kernel.rs:474-553): ``out`` is cleared and refilled with the
+    best SW score ending at each target position; returns the BestHit (query_end None)."""
+    q, t = _as_u8(query), _as_u8(target)
+    qo = np.array([0, len(q)], np.uint64)
+    to = np.array([0, len(t)], np.uint64)
+    hits, cm, _, (err, _) = align_pairs_position_max_arrays(q, qo, t, to, scoring)
+    out.clear()
+    if err is not None:
+        raise err
+    out.extend(int(v) for v in cm[: len(t)])
+    return BestHit._from(hits[0])
+
+
+def score2(colmax, best_score: int, best_target_end: int, matrix_max: int, min_score: int):
+    """score2 (src/kernel.rs:741-792): bwa's second-best peak outside the best hit's window, as
+    (score, position), or None."""
+    cm = np.ascontiguousarray(np.asarray(colmax, dtype=np.int64).astype(np.int32))
+    sc, pos = C.c_int32(), C.c_uint64()
+    ok = lib.hy_score2(_ptr(cm if cm.size else np.zeros(1, np.int32), _abi._i32p), len(cm), int(best_score),
+                       int(best_target_end), int(matrix_max), int(min_score), C.byref(sc), C.byref(pos))
+    return (int(sc.value), int(pos.value)) if ok else None
+
+
 def align_pair(query, target, scoring: Scoring, mode: Mode, search_type) -> BestHit:
     """align_pair (src/kernel.rs:331-352): one pair's BestHit (db_index 0). A long pair (a query of
     256 residues or more and at least 1 Mi cells) runs on the stripe kernel, every 128 query rows
@@ -858,5 +907,6 @@ __all__ = [
     "Batch", "Layout", "LayoutChoice", "Mode", "ALL_MODES", "ScoreWidth", "Scoring", "Scratch", "SearchType",
     "Server", "ServerRequest", "AlignOp", "Alignment", "AlignedHit", "AlignmentSearch", "USIZE_MAX",
     "align", "align_pair", "align_pairs", "align_pairs_arrays", "required_width", "concat",
-    "traceback_min_bytes_for_database", "traceback_timing",
+    "traceback_min_bytes_for_database", "traceback_timing", "align_pair_position_max",
+    "align_pairs_position_max_arrays", "score2",
 ]

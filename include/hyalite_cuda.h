@@ -364,6 +364,30 @@ uint64_t hy_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes);
  * device span from the first fill to the end of compaction in ms (walks overlap the next chunk's
  * fill), whole call ms, DP cells traced}. Device times are CUDA events. */
 hy_status hy_traceback_timing(hy_scratch *scratch, double out[5]);
+/* ---- per-position maxima and score2 (src/kernel.rs:454-553, 741-792) -------------------------- */
+
+/* align_pair_position_max over n_pairs independent (query, target) pairs (SW; the reference's
+ * entry is one pair, align_pair_position_max_with in a loop): pair k is q_res[q_off[k] ..
+ * q_off[k+1]] against t_res[t_off[k] .. t_off[k+1]]. Validation as align_pairs (symbols of the query
+ * then the target, then the SW width proof, pair by pair; the first failure is returned with its
+ * index in *failed_pair and the pairs before it are computed). out[k]: score = max of the pair's
+ * column maxima, query_end -1 (not tracked), target_end = first position of that maximum or -1 when
+ * the score is 0, db_index k. colmax (NULL: not copied) receives every pair's per-target-position
+ * maxima at t_off[k] - t_off[0] (|t_k| entries, each >= 0). score2 (NULL: not computed) receives
+ * {score, position} per pair: bwa's score2 (hy_score2) of the pair's maxima with its best score,
+ * its target end (position 0 when -1), the matrix's largest entry and min_score; {0, -1} when no
+ * peak qualifies. A few long pairs run on the stripe kernel, the rest one warp each. */
+hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                                      const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
+                                      uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
+                                      int32_t *colmax, hy_hit *out, int32_t min_score, int32_t *score2,
+                                      uint64_t *failed_pair);
+/* score2 (src/kernel.rs:741-792) over a host array of column maxima: returns 1 and the peak's
+ * {score, position} when a secondary peak qualifies, 0 (None) otherwise. Host code, as in the
+ * reference: a scan of one array. */
+int hy_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t best_target_end,
+              int32_t matrix_max, int32_t min_score, int32_t *score, uint64_t *pos);
+
 /* The budget the database was built with (0 unless HY_SEARCH_ALIGNMENT). */
 uint64_t hy_db_traceback_max_bytes(const hy_db *db);
 

@@ -636,3 +636,94 @@ void hyo_scan_all_aligned_mt(const uint8_t *residues, const uint64_t *offsets, u
     }
     (void)threads;
 }
+
+/* align_pair_position_max's scalar path (src/kernel.rs:526-553): the full SW matrix's column
+ * maxima (floor 0), then score = their maximum, target_end = its first position (-1 when 0). */
+int32_t hyo_position_max(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const int32_t *matrix,
+                         uint64_t al, int32_t gap_open, int32_t gap_ext, int32_t *out, int64_t *target_end) {
+    const int64_t go = gap_open, ge = gap_ext;
+    int64_t *prev = (int64_t *)malloc(sizeof(int64_t) * (n + 1));
+    int64_t *cur = (int64_t *)malloc(sizeof(int64_t) * (n + 1));
+    int64_t *f = (int64_t *)malloc(sizeof(int64_t) * (n + 1));
+    for (uint64_t j = 0; j <= n; ++j) {
+        prev[j] = 0;
+        f[j] = ORC_NEG;
+    }
+    for (uint64_t j = 0; j < n; ++j) out[j] = 0;
+    for (uint64_t i = 1; i <= m; ++i) {
+        cur[0] = 0;
+        int64_t e = ORC_NEG;
+        for (uint64_t j = 1; j <= n; ++j) {
+            int64_t a = cur[j - 1] - go, b = e - ge;
+            e = a > b ? a : b;
+            a = prev[j] - go;
+            b = f[j] - ge;
+            f[j] = a > b ? a : b;
+            int64_t c = prev[j - 1] + matrix[(uint64_t)q[i - 1] * al + t[j - 1]];
+            if (e > c) c = e;
+            if (f[j] > c) c = f[j];
+            if (c < 0) c = 0;
+            cur[j] = c;
+            if (c > out[j - 1]) out[j - 1] = (int32_t)c;
+        }
+        int64_t *tmp = prev;
+        prev = cur;
+        cur = tmp;
+    }
+    int32_t best = 0;
+    int64_t te = -1;
+    for (uint64_t j = 0; j < n; ++j)
+        if (out[j] > best) {
+            best = out[j];
+            te = (int64_t)j;
+        }
+    *target_end = te;
+    free(prev);
+    free(cur);
+    free(f);
+    return best;
+}
+
+/* score2 (src/kernel.rs:741-792): 1 and the peak when one qualifies, else 0. */
+int hyo_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t best_target_end,
+               int32_t matrix_max, int32_t min_score, int32_t *score, uint64_t *pos) {
+    if (matrix_max <= 0) return 0;
+    int64_t w = ((int64_t)(best_score > 0 ? best_score : 0) + matrix_max - 1) / matrix_max;
+    if (w < 0) w = 0;
+    const int64_t low = (int64_t)best_target_end - w, high = (int64_t)best_target_end + w;
+    int have = 0, open = 0;
+    int32_t bs = 0, cs = 0;
+    uint64_t bp = 0, cp = 0;
+    for (uint64_t i = 0; i <= n; ++i) {
+        const int finish = i == n;
+        if (!finish) {
+            const int32_t v = colmax[i];
+            if (v < min_score) continue;
+            if (open && cp + 1 == i) {
+                if (cs < v) {
+                    cs = v;
+                    cp = i;
+                }
+                continue;
+            }
+        }
+        if (open) {
+            const int64_t p = (int64_t)cp;
+            if ((p < low || p > high) && (!have || cs > bs)) {
+                have = 1;
+                bs = cs;
+                bp = cp;
+            }
+        }
+        if (!finish) {
+            open = 1;
+            cs = colmax[i];
+            cp = i;
+        }
+    }
+    if (have) {
+        *score = bs;
+        *pos = bp;
+    }
+    return have;
+}

@@ -115,6 +115,13 @@ void hyo_scan_all_aligned_mt(const uint8_t *residues, const uint64_t *offsets, u
                              const int32_t *matrix, uint64_t al, int32_t gap_open, int32_t gap_ext,
                              int mode, const uint8_t *query, uint64_t qlen, hyo_alignment *out,
                              uint8_t *ops, int threads);
+/* align_pair_position_max's scalar path (src/kernel.rs:526-553): out[0 .. n) column maxima;
+ * returns the best score, *target_end its first position (-1 when 0). */
+int32_t hyo_position_max(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const int32_t *matrix,
+                         uint64_t al, int32_t gap_open, int32_t gap_ext, int32_t *out, int64_t *target_end);
+/* score2 (src/kernel.rs:741-792). */
+int hyo_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t best_target_end,
+               int32_t matrix_max, int32_t min_score, int32_t *score, uint64_t *pos);
 /* traceback's budget rule (src/align.rs:192-222): 0 if traceable in max_bytes, else needed. */
 uint64_t hyo_traceback_needed(uint64_t m, uint64_t n, uint64_t max_bytes);
 /* traceback_min_bytes_for_database (src/align.rs:228-250). */

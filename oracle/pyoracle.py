@@ -53,6 +53,8 @@ def _load():
         "hyo_traceback": (None, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.POINTER(Alignment), _u8p]),
         "hyo_align": (C.c_int, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_uint64, C.POINTER(Alignment), _u8p, _i64p, _i64p]),
         "hyo_scan_all_aligned_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _u8p, C.c_uint64, C.POINTER(Alignment), _u8p, C.c_int]),
+        "hyo_position_max": (C.c_int32, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, _i32p, _i64p]),
+        "hyo_score2": (C.c_int, [_i32p, C.c_uint64, C.c_int32, C.c_uint64, C.c_int32, C.c_int32, _i32p, _u64p]),
         "hyo_traceback_needed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
         "hyo_traceback_min_bytes_for_database": (C.c_uint64, [C.c_uint64, C.c_uint64]),
         "hyo_brute": (C.c_int32, [C.c_int, _u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32]),
@@ -235,6 +237,25 @@ def align(q, t, matrix, al, go, ge, mode, max_bytes=U64_MAX):
     st = lib.hyo_align(_p(qb, _u8p), len(q), _p(tb, _u8p), len(t), _p(mat, _i32p), al, go, ge,
                        int(mode), max_bytes, C.byref(a), _p(ops, _u8p), C.byref(d1), C.byref(d2))
     return st, (as_alignment(a, ops) if st == 0 else None), (int(d1.value), int(d2.value))
+
+
+def position_max(q, t, matrix, al, go, ge):
+    """(column maxima list, score, target_end or None) of align_pair_position_max."""
+    qb, tb, mat = _seq(q), _seq(t), _mat(matrix)
+    out = np.zeros(max(1, len(t)), np.int32)
+    te = C.c_int64()
+    s = lib.hyo_position_max(_p(qb, _u8p), len(q), _p(tb, _u8p), len(t), _p(mat, _i32p), al, go, ge,
+                             _p(out, _i32p), C.byref(te))
+    return [int(v) for v in out[: len(t)]], int(s), (None if te.value < 0 else int(te.value))
+
+
+def score2(colmax, best_score, best_target_end, matrix_max, min_score):
+    cm = np.ascontiguousarray(np.asarray(colmax, dtype=np.int64).astype(np.int32))
+    cm1 = cm if cm.size else np.zeros(1, np.int32)
+    sc, pos = C.c_int32(), C.c_uint64()
+    ok = lib.hyo_score2(_p(cm1, _i32p), len(cm), best_score, best_target_end, matrix_max, min_score,
+                        C.byref(sc), C.byref(pos))
+    return (int(sc.value), int(pos.value)) if ok else None
 
 
 def traceback_needed(m, n, max_bytes):
