@@ -723,9 +723,9 @@ def run_pairs(args):
 
 
 # DRAM bytes (read + write) per DP cell of the traceback fill, from one ncu capture of
-# tb_fill_kernel<16, SW> (protein generator, 20,000 sequences x the 1000-residue query); None
-# until captured. The codes alone are 0.5 byte a cell.
-TB_DRAM_BYTES_PER_CELL = None
+# tb_fill_kernel<16, SW> (protein generator, 5,000 sequences x the 1000-residue query: 2.055e9
+# cells, 177.1 MB read, 1.162 GB written). The codes alone are 0.5 byte a cell.
+TB_DRAM_BYTES_PER_CELL = (177.1e6 + 1.1617e9) / 2.055e9
 
 
 def run_aligned(args):
@@ -826,6 +826,72 @@ def run_aligned(args):
     print(json.dumps(line), flush=True)
 
 
+def run_position_max(args):
+    """align_pair_position_max + score2 over --n-pos-pairs (150-bp read, 200..500-bp window) pairs
+    of the align_pairs generator (bwa's mate-rescue shape): SW, +2/-1, gap_open 6, gap_ext 1,
+    score2 with min_score 20. `value` is real cells / the device time of the kernels (profile
+    build, per-column maxima, BestHit + score2; CUDA events); `e2e` the whole call with host
+    buffers, the column maxima copied back."""
+    import torch
+
+    import hyalite_b200 as hy
+
+    torch.cuda.set_device(0)
+    q_res, q_off, t_res, t_off = make_pairs_workload(args.seed, args.n_pos_pairs)
+    dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
+    scoring = hy.Scoring(4, dna, 6, 1)
+    cells = float(np.dot(np.diff(q_off).astype(np.float64), np.diff(t_off).astype(np.float64)))
+    for _ in range(args.warmup):
+        hy.align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring, 20)
+    clocks = Clocks(0)
+    clocks.start()
+    kms = cms = 0.0
+    for _ in range(args.steps):
+        hits, cm, s2, (err, _) = hy.align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring, 20)
+        assert err is None
+        t = hy.position_max_timing()
+        kms += t["kernel_ms"]
+        cms += t["call_ms"]
+    clk = clocks.stop()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    rng = np.random.default_rng(2)
+    identical = True
+    for k in sorted(int(x) for x in rng.choice(args.n_pos_pairs, min(args.n_pos_pairs, 500), replace=False)):
+        q = q_res[int(q_off[k]):int(q_off[k + 1])]
+        t = t_res[int(t_off[k]):int(t_off[k + 1])]
+        want, score, te = pyoracle.position_max(q, t, dna, 4, 6, 1)
+        got = [int(v) for v in cm[int(t_off[k] - t_off[0]):int(t_off[k + 1] - t_off[0])]]
+        w2 = pyoracle.score2(want, score, 0 if te is None else te, 2, 20)
+        identical &= got == want and int(hits[k].score) == score and \
+            int(hits[k].target_end) == (-1 if te is None else te) and \
+            (int(s2[2 * k]), int(s2[2 * k + 1])) == ((0, -1) if w2 is None else w2)
+    threads = os.cpu_count() or 1
+    n_cpu = min(args.n_pos_pairs, args.cpu_pairs)
+    sq_off, st_off = q_off[: n_cpu + 1], t_off[: n_cpu + 1]
+    ccells = float(np.dot(np.diff(sq_off).astype(np.float64), np.diff(st_off).astype(np.float64)))
+    t0 = time.perf_counter()
+    pyoracle.position_max_many(q_res[: int(sq_off[-1])], sq_off, t_res[: int(st_off[-1])], st_off, dna, 4, 6, 1,
+                               threads)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "GCUPS", "value": cells * args.steps / (kms * 1e-3) / 1e9, "unit": "GCUPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": kms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded genome reads and windows)",
+        "config": {"workload": f"align_pair_position_max + score2: {args.n_pos_pairs} (150-bp read, 200..500-bp "
+                               "window) pairs, SW, +2/-1, gap_open 6, gap_ext 1, min_score 20",
+                   "cells_per_step": cells, "l2": "inputs larger than L2 (column maxima: 4 bytes a target residue)"},
+        "e2e": {"value": cells * args.steps / (cms * 1e-3) / 1e9, "unit": "GCUPS",
+                "h2d_bytes_per_step": int(len(q_res) + len(t_res)),
+                "d2h_bytes_per_step": int(4 * len(t_res) + 16 * args.n_pos_pairs), "call_ms": cms / args.steps},
+        "identical_to_oracle_on_sample": bool(identical),
+        "cpu_baseline": {"value": ccells / cpu_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+                         "sample": f"the first {n_cpu} pairs, scalar position-max restatement over {threads} threads"},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SEQS, QUERY_LENGTHS, N_QUERIES
     ap = argparse.ArgumentParser()
@@ -843,7 +909,8 @@ def main():
     ap.add_argument("--n-queries", type=int, default=N_QUERIES)
     # Other workloads of the same backend (not the default benchmark line).
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "batched", "served", "pairs", "dna_small", "aligned"])
+                    choices=["scan", "batched", "served", "pairs", "dna_small", "aligned", "position_max"])
+    ap.add_argument("--n-pos-pairs", type=int, default=1_000_000)
     ap.add_argument("--aligned-seqs", type=int, default=100_000)
     ap.add_argument("--aligned-cpu-seqs", type=int, default=2_000)
     ap.add_argument("--n-pairs", type=int, default=10_000_000)
@@ -872,6 +939,8 @@ def main():
         run_dna_small(args)
     elif args.workload == "aligned":
         run_aligned(args)
+    elif args.workload == "position_max":
+        run_position_max(args)
     else:
         run_cuda(args)
 

@@ -853,6 +853,13 @@ def align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring: Scoring
     return out, cm, s2, (err, int(failed.value))
 
 
+def position_max_timing() -> dict:
+    """This thread's last position-max call: device ms of its kernels, whole call ms, cells."""
+    out = (C.c_double * 3)()
+    _check(lib.hy_position_max_timing(out))
+    return {"kernel_ms": out[0], "call_ms": out[1], "cells": out[2]}
+
+
 def align_pair_position_max(query, target, scoring: Scoring, out: list) -> BestHit:
     """align_pair_position_max (src/kernel.rs:474-553): ``out`` is cleared and refilled with the
     best SW score ending at each target position; returns the BestHit (query_end None)."""
@@ -908,5 +915,5 @@ __all__ = [
     "Server", "ServerRequest", "AlignOp", "Alignment", "AlignedHit", "AlignmentSearch", "USIZE_MAX",
     "align", "align_pair", "align_pairs", "align_pairs_arrays", "required_width", "concat",
     "traceback_min_bytes_for_database", "traceback_timing", "align_pair_position_max",
-    "align_pairs_position_max_arrays", "score2",
+    "align_pairs_position_max_arrays", "score2", "position_max_timing",
 ]

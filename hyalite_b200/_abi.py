@@ -85,6 +85,7 @@ SIGNATURES = {
     "hy_traceback_timing": (_st, [_vp, C.POINTER(C.c_double)]),
     "hy_align_pairs_position_max": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                                           C.c_int32, _i32p, C.POINTER(HyHit), C.c_int32, _i32p, _u64p]),
+    "hy_position_max_timing": (_st, [C.POINTER(C.c_double)]),
     "hy_score2": (C.c_int, [_i32p, C.c_uint64, C.c_int32, C.c_uint64, C.c_int32, C.c_int32, _i32p, _u64p]),
     "hy_db_destroy": (None, [_vp]),
     "hy_db_sequence_count": (C.c_uint64, [_vp]),

@@ -18,6 +18,7 @@
 #include "host_common.h"
 #include "scan_kernel.cuh"
 #include "traceback_internal.h"
+#include "host_threads.h"
 
 using namespace hy;
 
@@ -91,30 +92,6 @@ static thread_local PairsContext g_ctx;
             return fail(e_ == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e_); \
         }                                                                                          \
     } while (0)
-
-// Runs f(begin, end) over [0, n) split across the host's threads.
-template <class F>
-static void parallel_for(uint64_t n, uint64_t min_chunk, F f) {
-    unsigned t = std::max(1u, std::thread::hardware_concurrency());
-    t = (unsigned)std::min<uint64_t>(t, std::max<uint64_t>(1, n / std::max<uint64_t>(min_chunk, 1)));
-    if (t <= 1) {
-        f(0, n, 0);
-        return;
-    }
-    std::vector<std::thread> th;
-    const uint64_t per = (n + t - 1) / t;
-    for (unsigned i = 0; i < t; ++i) {
-        const uint64_t a = i * per, e = std::min(n, a + per);
-        if (a >= e) break;
-        th.emplace_back(f, a, e, i);
-    }
-    for (auto &x : th) x.join();
-}
-
-static unsigned host_threads(uint64_t n, uint64_t min_chunk) {
-    unsigned t = std::max(1u, std::thread::hardware_concurrency());
-    return (unsigned)std::min<uint64_t>(t, std::max<uint64_t>(1, n / std::max<uint64_t>(min_chunk, 1)));
-}
 
 template <class A, int G, int R, int MODE, bool ENDS, bool GPROF>
 static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int threads, size_t smem,

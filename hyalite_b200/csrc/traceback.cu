@@ -36,6 +36,7 @@
 #include "host_common.h"
 #include "scan_kernel.cuh"
 #include "traceback_internal.h"
+#include "host_threads.h"
 
 namespace hy {
 
@@ -1497,11 +1498,20 @@ int hy_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t be
     return have ? 1 : 0;
 }
 
+hy_status hy_position_max_timing(double out[3]) {
+    if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
+    out[0] = g_pos_ctx ? g_pos_ctx->fill_ms : 0.0;
+    out[1] = g_pos_ctx ? g_pos_ctx->call_ms : 0.0;
+    out[2] = g_pos_ctx ? g_pos_ctx->cells : 0.0;
+    return fail(HY_OK);
+}
+
 hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
                                       const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
                                       uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
                                       int32_t *colmax, hy_hit *out, int32_t min_score, int32_t *score2,
                                       uint64_t *failed_pair) {
+    const auto t_call = std::chrono::steady_clock::now();
     if (failed_pair) *failed_pair = n_pairs;
     hy_status st = validate_scoring(alphabet_len, matrix, alphabet_len * alphabet_len, gap_open, gap_ext);
     if (st != HY_OK) return st;
@@ -1510,34 +1520,58 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
     if (alphabet_len > 255 || n_pairs >= (1ull << 32)) return fail(HY_ERR_UNSUPPORTED);
     const int32_t min_e = *std::min_element(matrix, matrix + alphabet_len * alphabet_len);
     const int32_t max_e = *std::max_element(matrix, matrix + alphabet_len * alphabet_len);
-    // Validation in input order (src/kernel.rs:496-511: symbols, then the SW width proof).
+    // Validation in input order (src/kernel.rs:496-511: symbols, then the SW width proof), chunked
+    // over the host threads: each chunk stops at its own first failure, and the call's first
+    // failure is that of the first chunk that has one.
+    const unsigned nt = host_threads(n_pairs, 1 << 15);
+    struct Chunk {
+        uint64_t first_bad = ~0ull;
+        hy_status st = HY_OK;
+        int64_t d[2] = {0, 0};
+    };
+    std::vector<Chunk> chunks(nt);
+    const uint64_t per = (n_pairs + nt - 1) / nt;
+    parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
+        for (uint64_t c = ca; c < ce; ++c) {
+            Chunk &ch = chunks[c];
+            const uint64_t a = c * per, e = std::min(n_pairs, a + per);
+            for (uint64_t k = a; k < e && ch.st == HY_OK; ++k) {
+                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
+                for (int side = 0; side < 2 && ch.st == HY_OK; ++side) {
+                    const uint8_t *seq = side == 0 ? q_res + q_off[k] : t_res + t_off[k];
+                    const uint64_t len = side == 0 ? ql : tl;
+                    for (uint64_t i = 0; i < len; ++i)
+                        if (seq[i] >= alphabet_len) {
+                            ch.st = HY_ERR_SYMBOL_OUT_OF_RANGE;
+                            ch.d[0] = seq[i];
+                            ch.d[1] = (int64_t)alphabet_len;
+                            break;
+                        }
+                }
+                if (ch.st == HY_OK) {
+                    const int64_t b = magnitude_bound(MODE_SW, min_e, max_e, gap_open, gap_ext, ql, tl);
+                    if (narrowest_width(b) < 0) {
+                        ch.st = HY_ERR_SCORE_RANGE_TOO_WIDE;
+                        ch.d[0] = b;
+                    } else if (ql >= (1u << 30) || tl >= (1u << 31)) {
+                        ch.st = HY_ERR_UNSUPPORTED;
+                    }
+                }
+                if (ch.st != HY_OK) ch.first_bad = k;
+            }
+        }
+    });
     uint64_t n_ok = n_pairs;
     hy_status first = HY_OK;
     int64_t d[2] = {0, 0};
-    for (uint64_t k = 0; k < n_pairs && first == HY_OK; ++k) {
-        const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-        for (int side = 0; side < 2 && first == HY_OK; ++side) {
-            const uint8_t *seq = side == 0 ? q_res + q_off[k] : t_res + t_off[k];
-            const uint64_t len = side == 0 ? ql : tl;
-            for (uint64_t i = 0; i < len; ++i)
-                if (seq[i] >= alphabet_len) {
-                    first = HY_ERR_SYMBOL_OUT_OF_RANGE;
-                    d[0] = seq[i];
-                    d[1] = (int64_t)alphabet_len;
-                    break;
-                }
+    for (const Chunk &ch : chunks)
+        if (ch.st != HY_OK) {
+            first = ch.st;
+            n_ok = ch.first_bad;
+            d[0] = ch.d[0];
+            d[1] = ch.d[1];
+            break;
         }
-        if (first == HY_OK) {
-            const int64_t b = magnitude_bound(MODE_SW, min_e, max_e, gap_open, gap_ext, ql, tl);
-            if (narrowest_width(b) < 0) {
-                first = HY_ERR_SCORE_RANGE_TOO_WIDE;
-                d[0] = b;
-            } else if (ql >= (1u << 30) || tl >= (1u << 31)) {
-                first = HY_ERR_UNSUPPORTED;
-            }
-        }
-        if (first != HY_OK) n_ok = k;
-    }
     if (failed_pair && first != HY_OK) *failed_pair = n_ok;
     if (n_ok > 0) {
         int dev = 0;
@@ -1554,6 +1588,15 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
         }
         TbContext &ctx = *g_pos_ctx;
         cudaStream_t stream = ctx.stream;
+        while (ctx.ev.size() < 2) {
+            cudaEvent_t e;
+            TB_CK(cudaEventCreate(&e));
+            ctx.ev.push_back(e);
+        }
+        ctx.fill_ms = 0.0;
+        ctx.cells = 0.0;
+        for (uint64_t k = 0; k < n_ok; ++k)
+            ctx.cells += (double)(q_off[k + 1] - q_off[k]) * (double)(t_off[k + 1] - t_off[k]);
         const uint64_t q0 = q_off[0], t0 = t_off[0];
         const uint64_t q_bytes = q_off[n_ok] - q0, t_bytes = t_off[n_ok] - t0;
         TB_CK(grow(ctx.d_q, ctx.c_q, q_bytes));
@@ -1636,6 +1679,7 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
                 TB_CK(grow(ctx.d_bnd, ctx.c_bnd, sizeof(int2) * std::max<uint64_t>(bnd_total, 1)));
                 TB_CK(grow(ctx.d_ends, ctx.c_ends, sizeof(TbEnd) * std::max<uint32_t>(n_str, 1)));
                 TB_CK(cudaMemcpyAsync(ctx.d_pairs, ctx.h_pairs, sizeof(TbPair) * (b - a), cudaMemcpyHostToDevice, stream));
+                TB_CK(cudaEventRecord(ctx.ev[0], stream));
                 tb_profile_pairs_kernel<<<b - a, 256, 0, stream>>>(ctx.d_pairs, ctx.d_q, ctx.d_matrix,
                                                                   (uint32_t)alphabet_len, ctx.d_prof);
                 TB_CK(cudaGetLastError());
@@ -1670,6 +1714,12 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
                 tb_position_hits_kernel<<<(b - a + 63) / 64, 64, 0, stream>>>(
                     p, d_scores, d_tend, max_e, min_score, score2 ? d_s2 : nullptr);
                 TB_CK(cudaGetLastError());
+                TB_CK(cudaEventRecord(ctx.ev[1], stream));
+                TB_CK(cudaEventSynchronize(ctx.ev[1]));
+                float ms = 0.f;
+                TB_CK(cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]));
+                ctx.fill_ms += ms;
+                ctx.launches += 3;
             }
             return fail(HY_OK);
         };
@@ -1698,6 +1748,7 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
                 score2[2 * k + 1] = h[2 * n_ok + 2 * k + 1];
             }
         }
+        ctx.call_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
     }
     return fail(first, d[0], d[1]);
 }

@@ -382,6 +382,9 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
                                       uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
                                       int32_t *colmax, hy_hit *out, int32_t min_score, int32_t *score2,
                                       uint64_t *failed_pair);
+/* Timing of this thread's last hy_align_pairs_position_max call (no reference counterpart):
+ * out = {device ms of its kernels (CUDA events), whole call ms, DP cells}. */
+hy_status hy_position_max_timing(double out[3]);
 /* score2 (src/kernel.rs:741-792) over a host array of column maxima: returns 1 and the peak's
  * {score, position} when a secondary peak qualifies, 0 (None) otherwise. Host code, as in the
  * reference: a scan of one array. */

@@ -727,3 +727,20 @@ int hyo_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t b
     }
     return have;
 }
+
+/* hyo_position_max over many pairs on `threads` OpenMP threads (the CPU baseline of the
+ * mate-rescue workload): pair k's column maxima go to out + (t_off[k] - t_off[0]). */
+void hyo_position_max_mt(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                         const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix, uint64_t al,
+                         int32_t gap_open, int32_t gap_ext, int32_t *out, int32_t *scores, int threads) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads > 0 ? threads : 1)
+#endif
+    for (int64_t k = 0; k < (int64_t)n_pairs; ++k) {
+        int64_t te;
+        scores[k] = hyo_position_max(q_res + q_off[k], q_off[k + 1] - q_off[k], t_res + t_off[k],
+                                     t_off[k + 1] - t_off[k], matrix, al, gap_open, gap_ext,
+                                     out + (t_off[k] - t_off[0]), &te);
+    }
+    (void)threads;
+}

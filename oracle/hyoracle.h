@@ -119,6 +119,10 @@ void hyo_scan_all_aligned_mt(const uint8_t *residues, const uint64_t *offsets, u
  * returns the best score, *target_end its first position (-1 when 0). */
 int32_t hyo_position_max(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t n, const int32_t *matrix,
                          uint64_t al, int32_t gap_open, int32_t gap_ext, int32_t *out, int64_t *target_end);
+/* hyo_position_max over many pairs on `threads` threads: pair k's maxima at out + t_off[k] - t_off[0]. */
+void hyo_position_max_mt(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                         const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix, uint64_t al,
+                         int32_t gap_open, int32_t gap_ext, int32_t *out, int32_t *scores, int threads);
 /* score2 (src/kernel.rs:741-792). */
 int hyo_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t best_target_end,
                int32_t matrix_max, int32_t min_score, int32_t *score, uint64_t *pos);

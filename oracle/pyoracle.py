@@ -54,6 +54,7 @@ def _load():
         "hyo_align": (C.c_int, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, C.c_uint64, C.POINTER(Alignment), _u8p, _i64p, _i64p]),
         "hyo_scan_all_aligned_mt": (None, [_u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _u8p, C.c_uint64, C.POINTER(Alignment), _u8p, C.c_int]),
         "hyo_position_max": (C.c_int32, [_u8p, C.c_uint64, _u8p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, _i32p, _i64p]),
+        "hyo_position_max_mt": (None, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32, C.c_int32, _i32p, _i32p, C.c_int]),
         "hyo_score2": (C.c_int, [_i32p, C.c_uint64, C.c_int32, C.c_uint64, C.c_int32, C.c_int32, _i32p, _u64p]),
         "hyo_traceback_needed": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
         "hyo_traceback_min_bytes_for_database": (C.c_uint64, [C.c_uint64, C.c_uint64]),
@@ -247,6 +248,20 @@ def position_max(q, t, matrix, al, go, ge):
     s = lib.hyo_position_max(_p(qb, _u8p), len(q), _p(tb, _u8p), len(t), _p(mat, _i32p), al, go, ge,
                              _p(out, _i32p), C.byref(te))
     return [int(v) for v in out[: len(t)]], int(s), (None if te.value < 0 else int(te.value))
+
+
+def position_max_many(q_res, q_off, t_res, t_off, matrix, al, go, ge, threads=8):
+    """(column maxima aligned with t_res, scores) of many pairs over `threads` threads."""
+    q_res, t_res = _u8(q_res), _u8(t_res)
+    q_off = np.ascontiguousarray(q_off, dtype=np.uint64)
+    t_off = np.ascontiguousarray(t_off, dtype=np.uint64)
+    n = len(q_off) - 1
+    out = np.zeros(max(1, int(t_off[-1] - t_off[0])), np.int32)
+    scores = np.zeros(max(n, 1), np.int32)
+    mat = _mat(matrix)
+    lib.hyo_position_max_mt(_p(q_res, _u8p), _p(q_off, _u64p), _p(t_res, _u8p), _p(t_off, _u64p), n,
+                            _p(mat, _i32p), al, go, ge, _p(out, _i32p), _p(scores, _i32p), threads)
+    return out, scores[:n]
 
 
 def score2(colmax, best_score, best_target_end, matrix_max, min_score):
