@@ -508,9 +508,9 @@ struct TbStripes {
 template <int R, int MODE, int KIND>
 __global__ void __launch_bounds__(TB_BLOCK) tb_stripe_kernel(TbParams P, TbStripes S) {
     using F = ModeFlags<MODE>;
-    const uint32_t warps = gridDim.x * (TB_BLOCK / 32);
+    const uint32_t warps = gridDim.x * (blockDim.x / 32);
     const int lane = threadIdx.x & 31;
-    for (uint32_t g = (blockIdx.x * TB_BLOCK + threadIdx.x) >> 5; g < S.n_stripes; g += warps) {
+    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < S.n_stripes; g += warps) {
         uint32_t lo = 0, hi = P.n_pairs;  // the pair x with first[x] <= g < first[x + 1]
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -873,20 +873,29 @@ static cudaError_t launch_walk(const TbParams &p, cudaStream_t st) {
 // Rows per lane of the stripe kernel: 128-row stripes, the most warps per pair.
 constexpr uint32_t TB_STRIPE_R = 4;
 
+// Blocks of the stripe kernel: two warps, so a pair's stripes spread over many SMs (each stripe is
+// a chain of dependent steps; a warp alone on its scheduler runs it at the lowest latency).
+constexpr int TB_STRIPE_BLOCK = 64;
+
 template <int MODE, int KIND>
 static cudaError_t launch_stripes(const TbParams &p, const TbStripes &S, cudaStream_t st, int device) {
     auto kern = tb_stripe_kernel<TB_STRIPE_R, MODE, KIND>;
+    // The stripes read their profile rows every step from global memory: keep L1 as large as
+    // the SM allows.
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxL1);
+    if (e != cudaSuccess) return e;
     int per_sm = 0, sms = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB_BLOCK, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB_STRIPE_BLOCK, 0);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    const uint64_t want = ((uint64_t)S.n_stripes * 32 + TB_BLOCK - 1) / TB_BLOCK;
+    const uint64_t want = ((uint64_t)S.n_stripes * 32 + TB_STRIPE_BLOCK - 1) / TB_STRIPE_BLOCK;
     const uint32_t blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per_sm * sms));
     TbParams pc = p;
     TbStripes sc = S;
     void *args[] = {(void *)&pc, (void *)&sc};
-    return cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(TB_BLOCK), args, 0, st);
+    return cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(TB_STRIPE_BLOCK), args, 0, st);
 }
 
 static cudaError_t dispatch_stripes(int mode, bool codes, const TbParams &p, const TbStripes &S,
