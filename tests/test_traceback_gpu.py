@@ -223,3 +223,25 @@ def test_database_scale_properties(mode, n_seqs):
         assert _rescore(a, q, seqs[k], BLOSUM62, 20, 11, 1) == a.score
     for k in rng.integers(0, len(seqs), 6):
         assert out[k].as_tuple() == o.traceback(q, seqs[k], BLOSUM62, 20, 11, 1, mode)
+
+
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_wide_score_range_and_tiny_queries(mode):
+    """Substitution scores of several hundred and gaps of tens (values far past 16 bits on the
+    longer targets), targets from 1 to 400 residues, queries of 300, 130 and 7 residues."""
+    rng = np.random.default_rng(41 + mode)
+    al = 8
+    mat = [int(v) for v in rng.integers(-120, 300, al * al)]
+    q = list(rng.integers(0, al, 300))
+    seqs = [_mutate(rng, q[a: a + L], al, 0.3) for a, L in
+            ((0, 300), (10, 20), (40, 60), (0, 100), (100, 150), (5, 9), (0, 1))]
+    seqs += [list(rng.integers(0, al, int(L))) for L in rng.integers(0, 400, 30)]
+    db = _db(seqs, mat, al, 40, 7, mode, 300)
+    sc = hy.Scratch(db)
+    ref = o.OracleDb(seqs, mat, al, 40, 7, mode, 1)
+    for ql in (300, 130, 7):
+        out = []
+        db.scan_all_aligned(sc, q[:ql], out)
+        want = ref.scan_all_aligned(q[:ql])
+        bad = [k for k in range(len(seqs)) if out[k].as_tuple() != want[k]]
+        assert not bad, (ql, bad[:5])
