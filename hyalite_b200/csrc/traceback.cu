@@ -133,6 +133,8 @@ struct TbRows {
 };
 
 constexpr uint32_t TB_PUBLISH = 32;        // columns between two progress updates of a stripe
+// Rows per lane of the stripe kernel: 128-row stripes, the most warps per pair.
+constexpr uint32_t TB_STRIPE_R = 4;
 constexpr uint32_t TB_SPIN_LIMIT = 1u << 22;  // polls (about 0.25 us each) before a wait gives up
 
 // Waits until *prog >= need (acquire); on running out of polls records the timeout in *err and
@@ -757,7 +759,7 @@ constexpr double TB_LONG_PAIR_CELLS = 1024.0 * 1024;
 constexpr uint32_t TB_STRIPE_PAIRS = 16;
 static void tb_plan(uint64_t m, uint64_t max_n, uint32_t n_pairs, uint32_t *R, bool *stripes) {
     *stripes = n_pairs <= TB_STRIPE_PAIRS && m > 128;
-    *R = *stripes ? 4u : tb_rows(m, max_n);  // 4: the stripe kernel's rows per lane
+    *R = *stripes ? TB_STRIPE_R : tb_rows(m, max_n);
 }
 
 static uint64_t tb_passes(uint64_t m, uint32_t R) { return std::max<uint64_t>(1, (m + 32 * R - 1) / (32 * R)); }
@@ -870,8 +872,6 @@ static cudaError_t launch_walk(const TbParams &p, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// Rows per lane of the stripe kernel: 128-row stripes, the most warps per pair.
-constexpr uint32_t TB_STRIPE_R = 4;
 
 // Blocks of the stripe kernel: two warps, so a pair's stripes spread over many SMs (each stripe is
 // a chain of dependent steps; a warp alone on its scheduler runs it at the lowest latency).
