@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -818,9 +819,9 @@ struct TbContext {
     uint64_t c_dir[2] = {0, 0};
     TbPair *h_pairs = nullptr;
     hy_alignment *h_out = nullptr;
-    uint8_t *h_ops = nullptr, *h_q = nullptr;
+    uint8_t *h_ops = nullptr, *h_q = nullptr, *h_stage = nullptr;
     uint64_t *h_total = nullptr;
-    uint64_t ch_pairs = 0, ch_out = 0, ch_ops = 0, ch_total = 0, ch_q = 0;
+    uint64_t ch_pairs = 0, ch_out = 0, ch_ops = 0, ch_total = 0, ch_q = 0, ch_stage = 0;
     uint64_t launches = 0;
     // Per chunk: fill start / end on `stream`, walk start / end on `stream_b`.
     std::vector<cudaEvent_t> ev;
@@ -837,7 +838,7 @@ struct TbContext {
                         (void *)d_ends, (void *)d_out, (void *)d_total, (void *)d_prog, (void *)d_first})
             cudaFree(p);
         for (void *p : {(void *)h_pairs, (void *)h_out, (void *)h_ops, (void *)h_total, (void *)h_q,
-                        (void *)h_first})
+                        (void *)h_first, (void *)h_stage})
             cudaFreeHost(p);
         if (stream_b) cudaStreamDestroy(stream_b);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -1180,11 +1181,12 @@ uint64_t hy_traceback_min_bytes_for_database(uint64_t max_m, uint64_t max_n) {
     return std::max({v, full_matrix_bytes(max_m, 0), full_matrix_bytes(0, max_n)});
 }
 
-static thread_local TbContext *g_align_ctx = nullptr;
+// Per calling thread, freed when the thread exits.
+static thread_local std::unique_ptr<TbContext> g_align_ctx;
 
 hy_status hy_traceback_timing(hy_scratch *scratch, double out[5]) {
     if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
-    tb_context_timing(scratch ? scratch_tb(scratch) : (void *)g_align_ctx, out);
+    tb_context_timing(scratch ? scratch_tb(scratch) : (void *)g_align_ctx.get(), out);
     return fail(HY_OK);
 }
 
@@ -1213,18 +1215,14 @@ hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, u
         cudaGetLastError();
         return fail(HY_ERR_CUDA, cudaErrorNoDevice);
     }
-    if (g_align_ctx && g_align_ctx->device != dev) {
-        delete g_align_ctx;
-        g_align_ctx = nullptr;
-    }
+    if (g_align_ctx && g_align_ctx->device != dev) g_align_ctx.reset();
     if (!g_align_ctx) {
-        g_align_ctx = new TbContext;
+        g_align_ctx.reset(new TbContext);
         g_align_ctx->device = dev;
         g_align_ctx->own_stream = true;
         if (cudaStreamCreateWithFlags(&g_align_ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
-            delete g_align_ctx;
-            g_align_ctx = nullptr;
+            g_align_ctx.reset();
             return fail(HY_ERR_CUDA, cudaErrorUnknown);
         }
     }
@@ -1301,7 +1299,7 @@ bool tb_long_pair(uint64_t qlen, uint64_t tlen) {
 
 uint64_t tb_long_pair_stripes(uint64_t qlen) { return tb_passes(qlen, TB_STRIPE_R); }
 
-static thread_local TbContext *g_pairs_ctx = nullptr;
+static thread_local std::unique_ptr<TbContext> g_pairs_ctx;
 
 hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
                               const uint64_t *t_off, const std::vector<uint32_t> &idx, const uint8_t *d_q,
@@ -1313,16 +1311,19 @@ hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const
     if (n == 0) return fail(HY_OK);
     int dev = 0;
     TB_CK(cudaGetDevice(&dev));
-    if (g_pairs_ctx && g_pairs_ctx->device != dev) {
-        delete g_pairs_ctx;
-        g_pairs_ctx = nullptr;
-    }
+    if (g_pairs_ctx && g_pairs_ctx->device != dev) g_pairs_ctx.reset();
     if (!g_pairs_ctx) {
-        g_pairs_ctx = new TbContext;
+        g_pairs_ctx.reset(new TbContext);
         g_pairs_ctx->device = dev;
     }
     TbContext &ctx = *g_pairs_ctx;
-    ctx.stream = stream;  // the caller's stream: ordered after its query upload, before its copy back
+    // The caller's stream, borrowed for this call only: ordered after its query upload, before its
+    // copy back.
+    ctx.stream = stream;
+    struct Unborrow {
+        TbContext &c;
+        ~Unborrow() { c.stream = nullptr; }
+    } unborrow{ctx};
     if (ctx.ev.size() < 2) {
         for (int x = 0; x < 2; ++x) {
             cudaEvent_t e;
@@ -1462,7 +1463,7 @@ static cudaError_t launch_colmax(const TbParams &p, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-static thread_local TbContext *g_pos_ctx = nullptr;
+static thread_local std::unique_ptr<TbContext> g_pos_ctx;
 
 }  // namespace hy
 
@@ -1585,12 +1586,9 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
     if (n_ok > 0) {
         int dev = 0;
         TB_CK(cudaGetDevice(&dev));
-        if (g_pos_ctx && g_pos_ctx->device != dev) {
-            delete g_pos_ctx;
-            g_pos_ctx = nullptr;
-        }
+        if (g_pos_ctx && g_pos_ctx->device != dev) g_pos_ctx.reset();
         if (!g_pos_ctx) {
-            g_pos_ctx = new TbContext;
+            g_pos_ctx.reset(new TbContext);
             g_pos_ctx->device = dev;
             g_pos_ctx->own_stream = true;
             TB_CK(cudaStreamCreateWithFlags(&g_pos_ctx->stream, cudaStreamNonBlocking));
@@ -1616,8 +1614,20 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
         int32_t *d_colmax = (int32_t *)ctx.d_ops_out;
         int32_t *d_res = (int32_t *)ctx.d_out;
         int32_t *d_scores = d_res, *d_tend = d_res + n_ok, *d_s2 = d_res + 2 * n_ok;
-        if (q_bytes) TB_CK(cudaMemcpyAsync(ctx.d_q, q_res + q0, q_bytes, cudaMemcpyHostToDevice, stream));
-        if (t_bytes) TB_CK(cudaMemcpyAsync(ctx.d_t, t_res + t0, t_bytes, cudaMemcpyHostToDevice, stream));
+        // Residues in through grow-only pinned staging, filled on all host threads (a pageable
+        // copy of gigabytes runs at a fraction of the link's speed).
+        TB_CK(cudaStreamSynchronize(stream));  // the staging buffers of the previous call are free
+        TB_CK(grow_pinned(ctx.h_q, ctx.ch_q, q_bytes));
+        TB_CK(grow_pinned(ctx.h_ops, ctx.ch_ops, t_bytes));
+        parallel_for(q_bytes + t_bytes, 1 << 24, [&](uint64_t a, uint64_t e, unsigned) {
+            if (a < q_bytes) memcpy(ctx.h_q + a, q_res + q0 + a, std::min(e, q_bytes) - a);
+            if (e > q_bytes) {
+                const uint64_t b = std::max(a, q_bytes);
+                memcpy(ctx.h_ops + (b - q_bytes), t_res + t0 + (b - q_bytes), e - b);
+            }
+        });
+        if (q_bytes) TB_CK(cudaMemcpyAsync(ctx.d_q, ctx.h_q, q_bytes, cudaMemcpyHostToDevice, stream));
+        if (t_bytes) TB_CK(cudaMemcpyAsync(ctx.d_t, ctx.h_ops, t_bytes, cudaMemcpyHostToDevice, stream));
         TB_CK(cudaMemcpyAsync(ctx.d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, stream));
         if (t_bytes) TB_CK(cudaMemsetAsync(d_colmax, 0, sizeof(int32_t) * t_bytes, stream));
@@ -1743,9 +1753,17 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
         std::vector<int32_t> h(4 * n_ok);
         TB_CK(cudaMemcpyAsync(h.data(), d_res, sizeof(int32_t) * (score2 ? 4 : 2) * n_ok, cudaMemcpyDeviceToHost,
                               stream));
-        if (colmax && t_bytes)
-            TB_CK(cudaMemcpyAsync(colmax, d_colmax, sizeof(int32_t) * t_bytes, cudaMemcpyDeviceToHost, stream));
+        int32_t *h_cm = nullptr;
+        if (colmax && t_bytes) {
+            TB_CK(grow_pinned(ctx.h_stage, ctx.ch_stage, sizeof(int32_t) * t_bytes));
+            h_cm = (int32_t *)ctx.h_stage;
+            TB_CK(cudaMemcpyAsync(h_cm, d_colmax, sizeof(int32_t) * t_bytes, cudaMemcpyDeviceToHost, stream));
+        }
         TB_CK(cudaStreamSynchronize(stream));
+        if (h_cm)
+            parallel_for(t_bytes, 1 << 22, [&](uint64_t a, uint64_t e, unsigned) {
+                memcpy(colmax + a, h_cm + a, sizeof(int32_t) * (e - a));
+            });
         for (uint64_t k = 0; k < n_ok; ++k) {
             out[k].score = h[k];
             out[k].reserved = 0;
