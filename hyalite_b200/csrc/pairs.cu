@@ -45,7 +45,9 @@ struct PairsContext {
         size_t n = 0;
     };
     Buf b[14];
-    Buf pinned[2];  // grow-only pinned host staging of the packed target residues (per partition)
+    // Grow-only pinned host staging: the packed target residues (one per partition), then the
+    // queries going in and the results coming back (in that stream order).
+    Buf pinned[3];
     double kernel_ms = 0.0, call_ms = 0.0;  // the last call: pair kernels' device time, whole call
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
@@ -185,38 +187,59 @@ static int pair_rows(uint64_t q, int32_t al) {
 }
 
 // Sorts pair indices (given in ascending order) by (query length desc, target length desc), index
-// asc for equal lengths: a stable LSD radix sort on 16-bit digits of the complemented lengths
-// (target length first, then query length), skipping digits every pair shares. O(n) per pass.
-static void sort_by_shape(std::vector<uint32_t> &o, const uint64_t *q_off, const uint64_t *t_off) {
+// asc for equal lengths: a stable LSD radix sort of 64-bit keys (complemented query length above
+// complemented target length) on 16-bit digits, skipping digits every pair shares. The keys are
+// built once from the offsets in input order and travel with the indices, so no pass reads the
+// offsets at random; histograms and scatters run on all host threads (per-thread ranges in order,
+// which keeps the sort stable). `keys` receives the sorted keys.
+static inline uint32_t key_qlen(uint64_t k) { return ~(uint32_t)(k >> 32); }
+static inline uint32_t key_tlen(uint64_t k) { return ~(uint32_t)k; }
+
+static void sort_by_shape(std::vector<uint32_t> &o, const uint64_t *q_off, const uint64_t *t_off,
+                          std::vector<uint64_t> &keys) {
     const size_t n = o.size();
+    keys.resize(n);
+    parallel_for(n, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
+        for (uint64_t i = a; i < e; ++i) {
+            const uint32_t k = o[i];
+            keys[i] = ((uint64_t)~(uint32_t)(q_off[k + 1] - q_off[k]) << 32) | ~(uint32_t)(t_off[k + 1] - t_off[k]);
+        }
+    });
     if (n < 2) return;
     std::vector<uint32_t> tmp(n);
-    std::vector<uint32_t> key(n), key_tmp(n);
-    std::vector<size_t> count(1 << 16);
-    for (int field = 0; field < 2; ++field) {  // 0: target length, 1: query length
-        for (size_t i = 0; i < n; ++i) {
-            const uint32_t k = o[i];
-            const uint64_t len = field == 0 ? t_off[k + 1] - t_off[k] : q_off[k + 1] - q_off[k];
-            key[i] = ~(uint32_t)len;
-        }
-        for (int shift = 0; shift < 32; shift += 16) {
-            std::fill(count.begin(), count.end(), 0);
-            for (size_t i = 0; i < n; ++i) ++count[(key[i] >> shift) & 0xffff];
-            if (count[(key[0] >> shift) & 0xffff] == n) continue;  // one digit value: nothing to do
-            size_t sum = 0;
-            for (size_t d = 0; d < count.size(); ++d) {
-                const size_t c = count[d];
-                count[d] = sum;
+    std::vector<uint64_t> key_tmp(n);
+    const unsigned nt = host_threads(n, 1 << 16);
+    const uint64_t per = (n + nt - 1) / nt;
+    std::vector<std::vector<size_t>> count(nt, std::vector<size_t>(1 << 16));
+    for (int shift = 0; shift < 64; shift += 16) {
+        parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+            for (uint64_t t = ta; t < te; ++t) {
+                std::fill(count[t].begin(), count[t].end(), 0);
+                for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i)
+                    ++count[t][(keys[i] >> shift) & 0xffff];
+            }
+        });
+        const size_t d0 = (keys[0] >> shift) & 0xffff;
+        size_t total0 = 0;
+        for (unsigned t = 0; t < nt; ++t) total0 += count[t][d0];
+        if (total0 == n) continue;  // one digit value: nothing to do
+        size_t sum = 0;
+        for (size_t d = 0; d < (1u << 16); ++d)
+            for (unsigned t = 0; t < nt; ++t) {
+                const size_t c = count[t][d];
+                count[t][d] = sum;
                 sum += c;
             }
-            for (size_t i = 0; i < n; ++i) {
-                const size_t dst = count[(key[i] >> shift) & 0xffff]++;
-                tmp[dst] = o[i];
-                key_tmp[dst] = key[i];
-            }
-            o.swap(tmp);
-            key.swap(key_tmp);
-        }
+        parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+            for (uint64_t t = ta; t < te; ++t)
+                for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i) {
+                    const size_t dst = count[t][(keys[i] >> shift) & 0xffff]++;
+                    tmp[dst] = o[i];
+                    key_tmp[dst] = keys[i];
+                }
+        });
+        o.swap(tmp);
+        keys.swap(key_tmp);
     }
 }
 
@@ -228,40 +251,54 @@ struct PairPart {
 };
 
 // Packs the pairs listed in `order` (already sorted by query length, then target length, both
-// descending). Pair16 items take two consecutive pairs when their query lengths are equal.
-static void pack_pairs(const std::vector<uint32_t> &order, const uint64_t *q_off,
-                       const uint64_t *t_off, bool two, PairPart &pp) {
+// descending; `keys` their sort keys). Pair16 items take two consecutive pairs when their query
+// lengths are equal. Item boundaries come from one sequential pass over the keys; the items are
+// then filled, and their column offsets prefix-summed, on all host threads.
+static void pack_pairs(const std::vector<uint32_t> &order, const std::vector<uint64_t> &keys,
+                       const uint64_t *q_off, bool two, PairPart &pp) {
     const uint64_t align = two ? 8 : 16;
-    size_t i = 0;
-    pp.meta.reserve(two ? order.size() / 2 + 1 : order.size());
-    while (i < order.size()) {
-        ItemMeta m;
-        m.pad_ = 0;
-        m.col_off = pp.cols;
-        const uint32_t a = order[i];
-        const uint64_t qa = q_off[a + 1] - q_off[a];
-        m.idx[0] = a;
-        m.n[0] = (uint32_t)(t_off[a + 1] - t_off[a]);
-        m.idx[1] = NO_INDEX;
-        m.n[1] = 0;
-        uint64_t qb_off = q_off[a];
-        ++i;
-        if (two && i < order.size()) {
-            const uint32_t b = order[i];
-            if (q_off[b + 1] - q_off[b] == qa) {
-                m.idx[1] = b;
-                m.n[1] = (uint32_t)(t_off[b + 1] - t_off[b]);
-                qb_off = q_off[b];
-                ++i;
-            }
-        }
-        m.w = std::max(m.n[0], m.n[1]);
-        pp.cols += (m.w + align - 1) / align * align;
-        pp.meta.push_back(m);
-        pp.qlen.push_back((uint32_t)qa);
-        pp.qoff.push_back(q_off[a]);
-        pp.qoff.push_back(qb_off);
+    std::vector<uint32_t> start;
+    start.reserve(two ? order.size() / 2 + 1 : order.size());
+    for (size_t i = 0; i < order.size();) {
+        start.push_back((uint32_t)i);
+        i += (two && i + 1 < order.size() && key_qlen(keys[i + 1]) == key_qlen(keys[i])) ? 2 : 1;
     }
+    const size_t n_items = start.size();
+    pp.meta.resize(n_items);
+    pp.qlen.resize(n_items);
+    pp.qoff.resize(2 * n_items);
+    const unsigned nt = host_threads(n_items, 1 << 15);
+    const uint64_t per = (n_items + nt - 1) / nt;
+    std::vector<uint64_t> part(nt + 1, 0);
+    parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+        for (uint64_t t = ta; t < te; ++t) {
+            uint64_t cols = 0;
+            for (uint64_t it = t * per; it < std::min<uint64_t>(n_items, (t + 1) * per); ++it) {
+                const size_t i = start[it];
+                const bool pair = it + 1 < n_items ? start[it + 1] - i == 2 : order.size() - i == 2;
+                ItemMeta &m = pp.meta[it];
+                m.pad_ = 0;
+                m.idx[0] = order[i];
+                m.n[0] = key_tlen(keys[i]);
+                m.idx[1] = pair ? order[i + 1] : NO_INDEX;
+                m.n[1] = pair ? key_tlen(keys[i + 1]) : 0;
+                m.w = std::max(m.n[0], m.n[1]);
+                m.col_off = cols;  // within this thread's range; shifted below
+                cols += (m.w + align - 1) / align * align;
+                pp.qlen[it] = key_qlen(keys[i]);
+                pp.qoff[2 * it] = q_off[m.idx[0]];
+                pp.qoff[2 * it + 1] = pair ? q_off[m.idx[1]] : q_off[m.idx[0]];
+            }
+            part[t + 1] = cols;
+        }
+    });
+    for (unsigned t = 0; t < nt; ++t) part[t + 1] += part[t];
+    parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+        for (uint64_t t = ta; t < te; ++t)
+            for (uint64_t it = t * per; it < std::min<uint64_t>(n_items, (t + 1) * per); ++it)
+                pp.meta[it].col_off += part[t];
+    });
+    pp.cols = part[nt];
 }
 
 template <class A, int G>
@@ -492,20 +529,26 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             HY_CK(cudaEventCreate(&ctx.ev1));
         }
         // Sort by (query length desc, target length desc, index asc) through 64-bit keys.
-        sort_by_shape(o16, q_off, t_off);
-        sort_by_shape(o32, q_off, t_off);
+        std::vector<uint64_t> k16, k32;
+        sort_by_shape(o16, q_off, t_off, k16);
+        sort_by_shape(o32, q_off, t_off, k32);
         PairPart p16, p32;
-        pack_pairs(o16, q_off, t_off, true, p16);
-        pack_pairs(o32, q_off, t_off, false, p32);
+        pack_pairs(o16, k16, q_off, true, p16);
+        pack_pairs(o32, k32, q_off, false, p32);
 
         void *d_q, *d_matrix, *d_out;
         const uint64_t qbytes = q_off[n_ok] - q_off[0];
         HY_CK(ctx.get(10, q_off[n_ok], &d_q));
         HY_CK(ctx.get(11, sizeof(int32_t) * alphabet_len * alphabet_len, &d_matrix));
         HY_CK(ctx.get(12, 3 * sizeof(int32_t) * n_ok, &d_out));
-        if (qbytes)
-            HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[0], q_res + q_off[0], qbytes,
-                                  cudaMemcpyHostToDevice, ctx.stream));
+        void *h_stage = nullptr;
+        HY_CK(ctx.get_pinned(2, std::max<uint64_t>(qbytes, 3 * sizeof(int32_t) * n_ok), &h_stage));
+        if (qbytes) {
+            parallel_for(qbytes, 1 << 24, [&](uint64_t a, uint64_t e, unsigned) {
+                memcpy((uint8_t *)h_stage + a, q_res + q_off[0] + a, e - a);
+            });
+            HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[0], h_stage, qbytes, cudaMemcpyHostToDevice, ctx.stream));
+        }
         HY_CK(cudaMemcpyAsync(d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, ctx.stream));
         int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + n_ok, *d_tend = d_qend + n_ok;
@@ -524,8 +567,9 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                                         (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
                                         gap_ext, mode, ends, d_scores, d_qend, d_tend);
         if (st != HY_OK) return st;
-        std::vector<int32_t> h(3 * n_ok);
-        HY_CK(cudaMemcpyAsync(h.data(), d_out, 3 * sizeof(int32_t) * n_ok, cudaMemcpyDeviceToHost, ctx.stream));
+        // Stream order: the query copy out of the staging buffer is done before this copy into it.
+        const int32_t *h = (const int32_t *)h_stage;
+        HY_CK(cudaMemcpyAsync(h_stage, d_out, 3 * sizeof(int32_t) * n_ok, cudaMemcpyDeviceToHost, ctx.stream));
         HY_CK(cudaStreamSynchronize(ctx.stream));
         parallel_for(n_ok, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
             for (uint64_t k = a; k < e; ++k) {
