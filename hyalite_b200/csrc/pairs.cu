@@ -29,6 +29,9 @@ constexpr int PAIR_R32 = 16;
 constexpr size_t PAIR_SMEM_LIMIT = 200 * 1024;
 // Largest global scratch for group profiles that do not fit in shared memory, per launch.
 constexpr size_t PAIR_GPROF_BYTES = 256ull << 20;
+// Chunks of items the residue packing is split into, so host packing overlaps the device's copies
+// and kernels (each chunk at least 65,536 items).
+constexpr size_t PAIR_PACK_CHUNKS = 8;
 // Most warps (128-row stripes) the long pairs of one call may take on the stripe kernel.
 constexpr uint64_t LONG_PAIR_MAX_STRIPES = 2048;
 // Rows per lane the int16x2 pair kernel is compiled for.
@@ -39,7 +42,7 @@ constexpr int PAIR_ROWS[] = {8, 12, 16, 20, 24, 32};
 struct PairsContext {
     int device = -1;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> ev;  // around each chunk's kernels
     struct Buf {
         void *p = nullptr;
         size_t n = 0;
@@ -52,8 +55,7 @@ struct PairsContext {
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
         for (auto &x : pinned) cudaFreeHost(x.p);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
     cudaError_t get_pinned(int slot, size_t bytes, void **out) {
@@ -323,32 +325,15 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
         multipass = multipass || pp.qlen[i] > (uint32_t)(G * rows[i]);
     }
     HY_CK(ctx.get(slot0 + 4, multipass ? 2 * sizeof(typename A::V) * pp.cols : 16, &d_bnd));
-    // Pack target residues (the shorter half of a pair item padded with symbol `al`).
-    // Packed straight into pinned staging (every column, padding included, is written below).
+    // Target residues (the shorter half of a pair item padded with symbol `al`) are packed
+    // straight into pinned staging (every column, padding included, is written), in chunks of
+    // items: while the device copies and aligns chunk c, the host threads pack chunk c + 1.
     void *h_res = nullptr;
     HY_CK(ctx.get_pinned(slot0 == 0 ? 0 : 1, res_bytes, &h_res));
     typename A::RES *res = static_cast<typename A::RES *>(h_res);
-    parallel_for(n_items, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
-        for (uint64_t it = a; it < e; ++it) {
-            const ItemMeta &m = pp.meta[it];
-            const uint64_t end = it + 1 < n_items ? pp.meta[it + 1].col_off : pp.cols;
-            const uint8_t *t0 = t_res + t_off[m.idx[0]];
-            const uint8_t *t1 = m.idx[1] == NO_INDEX ? nullptr : t_res + t_off[m.idx[1]];
-            for (uint64_t j = 0; j < end - m.col_off; ++j) {
-                if (two) {
-                    uint32_t lo = j < m.n[0] ? t0[j] : (uint32_t)al;
-                    uint32_t hi = (t1 && j < m.n[1]) ? t1[j] : (uint32_t)al;
-                    res[m.col_off + j] = (typename A::RES)(lo | (hi << 8));
-                } else {
-                    res[m.col_off + j] = (typename A::RES)(j < m.n[0] ? t0[j] : 0);
-                }
-            }
-        }
-    });
     HY_CK(cudaMemcpyAsync(d_meta, pp.meta.data(), sizeof(ItemMeta) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qlen, pp.qlen.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, ctx.stream));
     HY_CK(cudaMemcpyAsync(d_qoff, pp.qoff.data(), sizeof(uint64_t) * 2 * n_items, cudaMemcpyHostToDevice, ctx.stream));
-    HY_CK(cudaMemcpyAsync(d_res, res, res_bytes, cudaMemcpyHostToDevice, ctx.stream));
     PairParams p{};
     p.meta = (const ItemMeta *)d_meta;
     p.qlen = (const uint32_t *)d_qlen;
@@ -367,47 +352,84 @@ static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, cons
     p.qend = d_qend;
     p.tend = d_tend;
     p.gprof = nullptr;
-    HY_CK(cudaEventRecord(ctx.ev0, ctx.stream));
-    for (size_t i0 = 0; i0 < n_items;) {
-        size_t i1 = i0;
-        while (i1 < n_items && rows[i1] == rows[i0]) ++i1;
-        const int r = rows[i0];
-        const size_t group_bytes = (size_t)(al + 1) * G * r * profile_row_bytes<A>();
-        int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
-        gpb = gpb / (32 / G) * (32 / G);  // whole warps
-        p.group_bytes = (uint32_t)group_bytes;
-        if (gpb == 0) {
-            // Not one warp of group profiles fits in shared memory (a large alphabet): the groups
-            // keep their profiles in a global scratch region, in launches of bounded size.
-            gpb = 256 / G;
-            const size_t per_block = (size_t)gpb * group_bytes;
-            const size_t max_blocks = std::max<size_t>(1, PAIR_GPROF_BYTES / per_block);
-            const size_t need_blocks = (i1 - i0 + gpb - 1) / gpb;
-            void *d_gprof;
-            HY_CK(ctx.get(13, std::min(max_blocks, need_blocks) * per_block, &d_gprof));
-            p.gprof = (uint8_t *)d_gprof;
-            for (size_t j0 = i0; j0 < i1; j0 += max_blocks * gpb) {
-                const size_t j1 = std::min(i1, j0 + max_blocks * gpb);
-                p.item_base = (uint32_t)j0;
-                p.n_items = (uint32_t)j1;
-                const int blocks = (int)((j1 - j0 + gpb - 1) / gpb);
-                HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, 0, ctx.stream)));
+    // Kernels of items [a, b), split where the rows per lane change.
+    auto launch_range = [&](size_t a, size_t b) -> hy_status {
+        for (size_t i0 = a; i0 < b;) {
+            size_t i1 = i0;
+            while (i1 < b && rows[i1] == rows[i0]) ++i1;
+            const int r = rows[i0];
+            const size_t group_bytes = (size_t)(al + 1) * G * r * profile_row_bytes<A>();
+            int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
+            gpb = gpb / (32 / G) * (32 / G);  // whole warps
+            p.group_bytes = (uint32_t)group_bytes;
+            if (gpb == 0) {
+                // Not one warp of group profiles fits in shared memory (a large alphabet): the
+                // groups keep their profiles in a global scratch region, in launches of bounded size.
+                gpb = 256 / G;
+                const size_t per_block = (size_t)gpb * group_bytes;
+                const size_t max_blocks = std::max<size_t>(1, PAIR_GPROF_BYTES / per_block);
+                const size_t need_blocks = (i1 - i0 + gpb - 1) / gpb;
+                void *d_gprof;
+                HY_CK(ctx.get(13, std::min(max_blocks, need_blocks) * per_block, &d_gprof));
+                p.gprof = (uint8_t *)d_gprof;
+                for (size_t j0 = i0; j0 < i1; j0 += max_blocks * gpb) {
+                    const size_t j1 = std::min(i1, j0 + max_blocks * gpb);
+                    p.item_base = (uint32_t)j0;
+                    p.n_items = (uint32_t)j1;
+                    const int blocks = (int)((j1 - j0 + gpb - 1) / gpb);
+                    HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, 0, ctx.stream)));
+                }
+                p.gprof = nullptr;
+            } else {
+                p.item_base = (uint32_t)i0;
+                p.n_items = (uint32_t)i1;
+                const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
+                HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
             }
-            p.gprof = nullptr;
-        } else {
-            p.item_base = (uint32_t)i0;
-            p.n_items = (uint32_t)i1;
-            const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
-            HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
+            i0 = i1;
         }
-        i0 = i1;
+        return fail(HY_OK);
+    };
+    const size_t n_chunks = std::max<size_t>(1, std::min<size_t>(PAIR_PACK_CHUNKS, n_items / (1 << 16)));
+    while (ctx.ev.size() < 2 * n_chunks) {
+        cudaEvent_t e;
+        HY_CK(cudaEventCreate(&e));
+        ctx.ev.push_back(e);
     }
-    HY_CK(cudaEventRecord(ctx.ev1, ctx.stream));
+    for (size_t c = 0; c < n_chunks; ++c) {
+        const size_t a = n_items * c / n_chunks, b = n_items * (c + 1) / n_chunks;
+        parallel_for(b - a, 1 << 14, [&](uint64_t x0, uint64_t x1, unsigned) {
+            for (uint64_t it = a + x0; it < a + x1; ++it) {
+                const ItemMeta &m = pp.meta[it];
+                const uint64_t end = it + 1 < n_items ? pp.meta[it + 1].col_off : pp.cols;
+                const uint8_t *t0 = t_res + t_off[m.idx[0]];
+                const uint8_t *t1 = m.idx[1] == NO_INDEX ? nullptr : t_res + t_off[m.idx[1]];
+                for (uint64_t j = 0; j < end - m.col_off; ++j) {
+                    if (two) {
+                        uint32_t lo = j < m.n[0] ? t0[j] : (uint32_t)al;
+                        uint32_t hi = (t1 && j < m.n[1]) ? t1[j] : (uint32_t)al;
+                        res[m.col_off + j] = (typename A::RES)(lo | (hi << 8));
+                    } else {
+                        res[m.col_off + j] = (typename A::RES)(j < m.n[0] ? t0[j] : 0);
+                    }
+                }
+            }
+        });
+        const uint64_t c0 = pp.meta[a].col_off, c1 = b < n_items ? pp.meta[b].col_off : pp.cols;
+        HY_CK(cudaMemcpyAsync((typename A::RES *)d_res + c0, res + c0, (c1 - c0) * sizeof(typename A::RES),
+                              cudaMemcpyHostToDevice, ctx.stream));
+        HY_CK(cudaEventRecord(ctx.ev[2 * c], ctx.stream));
+        hy_status st = launch_range(a, b);
+        if (st != HY_OK) return st;
+        HY_CK(cudaEventRecord(ctx.ev[2 * c + 1], ctx.stream));
+    }
     // The host staging (the item vectors and the pinned residues) must outlive the async copies.
     HY_CK(cudaStreamSynchronize(ctx.stream));
-    float ms = 0.0f;
-    HY_CK(cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1));
-    ctx.kernel_ms += ms;
+    for (size_t c = 0; c < n_chunks; ++c) {
+        float ms = 0.0f;
+        HY_CK(cudaEventElapsedTime(&ms, ctx.ev[2 * c], ctx.ev[2 * c + 1]));
+        ctx.kernel_ms += ms;
+    }
     return fail(HY_OK);
 }
 
@@ -525,8 +547,6 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             new (&ctx) PairsContext();
             ctx.device = dev;
             HY_CK(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
-            HY_CK(cudaEventCreate(&ctx.ev0));
-            HY_CK(cudaEventCreate(&ctx.ev1));
         }
         // Sort by (query length desc, target length desc, index asc) through 64-bit keys.
         std::vector<uint64_t> k16, k32;
