@@ -33,4 +33,16 @@ inline unsigned host_threads(uint64_t n, uint64_t min_chunk) {
     return (unsigned)std::min<uint64_t>(t, std::max<uint64_t>(1, n / std::max<uint64_t>(min_chunk, 1)));
 }
 
+// The first symbol of seq[0 .. len) that is >= alphabet_len, or -1: a branch-free maximum over
+// the bytes (which the compiler vectorizes) and a scan for the offender only when there is one.
+inline int first_bad_symbol(const uint8_t *seq, uint64_t len, uint64_t alphabet_len) {
+    if (alphabet_len > 255) return -1;
+    uint8_t mx = 0;
+    for (uint64_t i = 0; i < len; ++i) mx = seq[i] > mx ? seq[i] : mx;
+    if (mx < alphabet_len) return -1;
+    for (uint64_t i = 0; i < len; ++i)
+        if (seq[i] >= alphabet_len) return seq[i];
+    return -1;
+}
+
 }  // namespace hy

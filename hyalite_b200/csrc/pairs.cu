@@ -477,13 +477,12 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                 for (int s = 0; s < 2 && ch.st == HY_OK; ++s) {
                     const uint8_t *seq = s == 0 ? q_res + q_off[k] : t_res + t_off[k];
                     const uint64_t len = s == 0 ? ql : tl;
-                    for (uint64_t i = 0; i < len; ++i)
-                        if (seq[i] >= alphabet_len) {
-                            ch.st = HY_ERR_SYMBOL_OUT_OF_RANGE;
-                            ch.d[0] = seq[i];
-                            ch.d[1] = (int64_t)alphabet_len;
-                            break;
-                        }
+                    const int bad = first_bad_symbol(seq, len, alphabet_len);
+                    if (bad >= 0) {
+                        ch.st = HY_ERR_SYMBOL_OUT_OF_RANGE;
+                        ch.d[0] = bad;
+                        ch.d[1] = (int64_t)alphabet_len;
+                    }
                 }
                 if (ch.st == HY_OK) {
                     const int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, ql, tl);
