@@ -541,27 +541,45 @@ def run_served(args):
     sigma 0.8, clipped 50..3000), half the requests a ScoreEnd scan and half scan_scores (every
     target's i32 score). Reports per rate the p50/p99 latency (submit -> result ready) and the
     GCUPS the server sustained, beside the plain per-request calls (Database.scan /
-    scan_scores one at a time)."""
+    scan_scores one at a time). --served-db dna_small serves the small DNA database of the
+    dna_small workload instead, every request a 64-bp ScoreEnd scan."""
     import torch
 
     import hyalite_b200 as hy
 
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    mat, residues, offsets, _ = make_workload(args.seed, n_seqs=args.served_seqs)
-    gen_s = time.perf_counter() - t0
-    db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
-          .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(3000).build())
-    total_res = float(offsets[-1])
-    base = np.random.default_rng(12345)
-    base.integers(-4, 4, size=(AL, AL))
-    base.integers(4, 12, size=AL)
-    background = base.dirichlet(np.full(AL, 4.0))
     rng = np.random.default_rng(args.seed + 7)
+    if args.served_db == "dna_small":
+        # The small DNA database of the dna_small workload; every request a 64-bp ScoreEnd scan.
+        drng = np.random.default_rng(args.seed)
+        lengths = drng.integers(50, 301, 10_000)
+        res, offsets = hy.concat([drng.integers(0, 4, int(n)).astype(np.uint8) for n in lengths])
+        dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
+        db = (hy.Database.builder().sequences_concat(res, offsets).scoring(hy.Scoring(4, dna, 2, 1))
+              .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(64).build())
 
-    def request():
-        L = int(np.clip(round(math.exp(math.log(350.0) + 0.8 * rng.standard_normal())), 50, 3000))
-        return rng.choice(AL, size=L, p=background).astype(np.uint8), bool(rng.random() < 0.5)
+        def request():
+            return rng.integers(0, 4, 64).astype(np.uint8), False
+        workload = ("served small DNA scan: 10,000 sequences of 50..300 bp, Poisson arrivals, every "
+                    "request a 64-bp SW ScoreEnd scan")
+    else:
+        mat, residues, offsets, _ = make_workload(args.seed, n_seqs=args.served_seqs)
+        db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
+              .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(3000).build())
+        base = np.random.default_rng(12345)
+        base.integers(-4, 4, size=(AL, AL))
+        base.integers(4, 12, size=AL)
+        background = base.dirichlet(np.full(AL, 4.0))
+
+        def request():
+            L = int(np.clip(round(math.exp(math.log(350.0) + 0.8 * rng.standard_normal())), 50, 3000))
+            return rng.choice(AL, size=L, p=background).astype(np.uint8), bool(rng.random() < 0.5)
+        workload = (f"served protein scan: {args.served_seqs} sequences, Poisson arrivals, log-normal "
+                    "query lengths (median 350, 50..3000), half ScoreEnd scan and half scan_scores "
+                    "(i32 per target)")
+    gen_s = time.perf_counter() - t0
+    total_res = float(offsets[-1])
 
     srv = hy.Server([db], max_batch=args.served_batch, in_flight=2)
     # Warm-up: one request of each kind.
@@ -621,10 +639,8 @@ def run_served(args):
     line = {
         "metric": "GCUPS", "value": best["gcups"], "unit": "GCUPS", "n_gpus": 1, "steps": len(rates),
         "warmup": 2, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "i16x2 (int32 for long sequences)", "data": "synthetic (seeded protein generator)",
-        "config": {"workload": f"served protein scan: {args.served_seqs} sequences, Poisson arrivals, "
-                               "log-normal query lengths (median 350, 50..3000), half ScoreEnd scan and "
-                               "half scan_scores (i32 per target)",
+        "dtype": "i16x2 (int32 for long sequences)", "data": "synthetic (seeded generators)",
+        "config": {"workload": workload,
                    "residues": int(total_res), "gen_s": round(gen_s, 1), "max_batch": args.served_batch,
                    "in_flight": 2},
         "served": points,
@@ -946,6 +962,7 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=8.0)
     ap.add_argument("--served-max-requests", type=int, default=300)
     ap.add_argument("--served-batch", type=int, default=64)
+    ap.add_argument("--served-db", default="protein", choices=["protein", "dna_small"])
     ap.add_argument("--served-plain-requests", type=int, default=40)
     args = ap.parse_args()
     N_SEQS = args.n_seqs
