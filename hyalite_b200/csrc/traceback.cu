@@ -136,6 +136,10 @@ struct TbRows {
 constexpr uint32_t TB_PUBLISH = 32;        // columns between two progress updates of a stripe
 // Rows per lane of the stripe kernel: 128-row stripes, the most warps per pair.
 constexpr uint32_t TB_STRIPE_R = 4;
+// Alphabets up to this size give each stripe a shared-memory copy of its profile rows (96 KB for
+// a two-warp block at the limit); larger ones read the profile from global memory.
+constexpr uint64_t TB_STRIPE_SMEM_AL = 96;
+inline uint32_t tb_stripe_smem_al(uint64_t al) { return al <= TB_STRIPE_SMEM_AL ? (uint32_t)al : 0u; }
 constexpr uint32_t TB_SPIN_LIMIT = 1u << 22;  // polls (about 0.25 us each) before a wait gives up
 
 // Waits until *prog >= need (acquire); on running out of polls records the timeout in *err and
@@ -158,9 +162,10 @@ __device__ inline uint32_t tb_wait(const uint32_t *prog, uint32_t need, uint32_t
 // One pass of 32 * R query rows (pass p) of pair `pr` over all its columns: the DP with the walk
 // codes stored, the row for the next pass, and the pass's end-cell candidates merged into
 // (bs, brow, bcol) of this lane.
-template <int R, int MODE, int KIND>
+template <int R, int MODE, int KIND, bool XC = false>
 __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int p, int passes, int lane,
-                                        const TbRows &rows, int32_t &bs, uint32_t &brow, uint32_t &bcol) {
+                                        const TbRows &rows, int32_t &bs, uint32_t &brow, uint32_t &bcol,
+                                        const int32_t *sprof = nullptr) {
     using F = ModeFlags<MODE>;
     constexpr bool CODES = KIND == TB_CODES;
     static_assert(KIND != TB_COLMAX || MODE == MODE_SW, "column maxima are a local-mode search");
@@ -185,7 +190,10 @@ __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int
     const bool has_m = km >= 0 && km < R;
     const int kv = min(R, m - i0 + 1);  // rows of this lane inside the query
     uint8_t *D = P.dir + pr.dir_off + (uint64_t)p * pass_stride;
-    const int32_t *pq = P.prof + pr.prof_off + (i0 - 1);
+    // The profile rows of this lane: from global memory, or (sprof) from the warp's shared-memory
+    // copy of this pass's 32 * R rows, letter-major.
+    const int32_t *pq = sprof ? sprof + lane * R : P.prof + pr.prof_off + (i0 - 1);
+    const uint64_t pstride = sprof ? (uint64_t)(32 * R) : (uint64_t)pr.m_pad;
     // The row above: in place (one warp per pair), lane 0 reads it one column ahead; between
     // stripes (published by another warp), all lanes load it 32 columns at a time from L2 once
     // those columns are published, and lane 0 takes column j from lane (j - 1) % 32.
@@ -211,7 +219,7 @@ __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int
     auto load_profile = [&](int s, int c) {
         const int col = s - lane + 1;
         if (col >= 1 && col <= n) {
-            const int32_t *pc = pq + (uint64_t)c * pr.m_pad;
+            const int32_t *pc = pq + (uint64_t)c * pstride;
 #pragma unroll
             for (int k = 0; k < R / 4; ++k) subn[k] = *(const int4 *)(pc + 4 * k);
         }
@@ -262,8 +270,40 @@ __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int
             int32_t hd = hdiag, hu = up_h, fu = up_f;
             uint32_t w0 = 0, w1 = 0;
             int32_t colmax = 0;
+            int32_t xp = 0;  // XC: the previous row's x
 #pragma unroll
             for (int k = 0; k < R; ++k) {
+                if constexpr (XC) {
+                    // The short-chain form for lone warps (the stripe kernel), whose steps are bound
+                    // by dependent latency: with x = max(d, E[, 0]) - go, H = max(x + go, F) and the
+                    // next row's F = max(F - ge, x) (go >= ge), so the row-to-row chain is the one
+                    // add-max on F. Every value equals the plain form's.
+                    const int32_t e = __viaddmax_s32(Hl[k], -go, E[k] - ge);
+                    const int32_t d = hd + sub[k];
+                    const int32_t x = (F::local ? __vimax3_s32_relu(d, e, d) : max(d, e)) - go;
+                    const int32_t hgp = k == 0 ? hu - go : __viaddmax_s32(fu, -go, xp);  // H(i-1,j) - go
+                    const int32_t f = k == 0 ? max(hgp, fu - ge) : __viaddmax_s32(fu, -ge, xp);
+                    const int32_t h = __viaddmax_s32(x, go, f);
+                    if constexpr (CODES) {
+                        const uint32_t e_ext = min((uint32_t)(e - Hl[k] + go), 1u);
+                        const uint32_t f_ext = min((uint32_t)(f - hgp), 1u);
+                        const uint32_t d_ne = min((uint32_t)(h - d), 1u);
+                        const uint32_t e_ne = min((uint32_t)(h - e), 1u);
+                        uint32_t code = d_ne * e_ne + d_ne;
+                        if (F::local) code |= 3u - 3u * min((uint32_t)h, 1u);
+                        code += e_ext * 4u + f_ext * 8u;
+                        if (k < 8) w0 += code << (4 * k);
+                        else w1 += code << (4 * (k - 8));
+                    }
+                    if (F::local) colmax = max(colmax, h);
+                    xp = x;
+                    hd = Hl[k];
+                    Hl[k] = h;
+                    E[k] = e;
+                    hu = h;
+                    fu = f;
+                    continue;
+                }
                 if constexpr (!CODES) {
                     // Score only (the DP of src/kernel.rs:168-232).
                     const int32_t e = __viaddmax_s32(Hl[k], -go, E[k] - ge);
@@ -503,6 +543,7 @@ __global__ void tb_position_hits_kernel(TbParams P, int32_t *scores, int32_t *te
 struct TbStripes {
     const uint32_t *first;  // per pair: first stripe (n_pairs + 1 entries)
     uint32_t n_stripes;
+    uint32_t al;            // letters; > 0: each warp copies its stripe's profile rows to shared memory
     int2 *bnd;              // per pair: (stripes - 1) rows of n + 1 entries at TbPair::bnd_off
     uint32_t *prog;         // per stripe: published columns of its last row (zeroed before launch)
     int *err;
@@ -531,7 +572,21 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_stripe_kernel(TbParams P, TbStrip
                           s == 0 ? nullptr : S.prog + g - 1, S.prog + g, S.err};
         int32_t bs = F::local ? 0 : INT32_MIN;
         uint32_t brow = 0, bcol = 0;
-        tb_pass<R, MODE, KIND>(P, pr, (int)s, passes, lane, rows, bs, brow, bcol);
+        // The stripe's profile rows (al letters x 32 R rows) into this warp's shared memory: every
+        // step then reads its profile words at shared-memory latency.
+        int32_t *sprof = nullptr;
+        if (S.al) {
+            extern __shared__ int32_t tb_smem[];
+            sprof = tb_smem + (size_t)(threadIdx.x >> 5) * S.al * 32 * R;
+            __syncwarp();
+            const int32_t *src = P.prof + pr.prof_off + (uint64_t)s * 32 * R;
+            for (uint32_t x = lane; x < S.al * 32 * R; x += 32) {
+                const uint32_t c = x / (32 * R), r = x - c * 32 * R;
+                sprof[x] = src[(uint64_t)c * pr.m_pad + r];
+            }
+            __syncwarp();
+        }
+        tb_pass<R, MODE, KIND, true>(P, pr, (int)s, passes, lane, rows, bs, brow, bcol, sprof);
         tb_write_end<MODE>(P.ends + pr.ends_off + s, lane, bs, brow, bcol);
     }
 }
@@ -886,8 +941,13 @@ static cudaError_t launch_stripes(const TbParams &p, const TbStripes &S, cudaStr
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxL1);
     if (e != cudaSuccess) return e;
+    const size_t smem = (size_t)S.al * 32 * TB_STRIPE_R * sizeof(int32_t) * (TB_STRIPE_BLOCK / 32);
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
     int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB_STRIPE_BLOCK, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB_STRIPE_BLOCK, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
@@ -896,7 +956,7 @@ static cudaError_t launch_stripes(const TbParams &p, const TbStripes &S, cudaStr
     TbParams pc = p;
     TbStripes sc = S;
     void *args[] = {(void *)&pc, (void *)&sc};
-    return cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(TB_STRIPE_BLOCK), args, 0, st);
+    return cudaLaunchCooperativeKernel((const void *)kern, dim3(blocks), dim3(TB_STRIPE_BLOCK), args, smem, st);
 }
 
 static cudaError_t dispatch_stripes(int mode, bool codes, const TbParams &p, const TbStripes &S,
@@ -947,6 +1007,7 @@ struct TbRun {
     const uint64_t *h_t_off;       // host offsets of the targets (n_targets + 1), or null
     const uint64_t *h_t_single;    // a single target: {offset, length} when h_t_off is null
     bool stripes;                  // fill with the stripe kernel (few long pairs)
+    uint64_t al;                   // alphabet size (profile letters)
 };
 
 static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, uint32_t n_idx,
@@ -1055,7 +1116,7 @@ static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, u
         TB_CK(cudaEventRecord(e[0], ctx.stream));
         if (run.m > 0 && run.stripes) {
             const uint32_t n_str = p.n_pairs * per_pair;
-            TbStripes S{ctx.d_first, n_str, ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+            TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(run.al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
             TB_CK(cudaMemsetAsync(S.prog, 0, sizeof(uint32_t) * n_str, ctx.stream));
             TB_CK(dispatch_stripes(run.mode, true, p, S, ctx.stream, ctx.device));
             ctx.launches += 2;
@@ -1246,6 +1307,7 @@ hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, u
     run.m_pad = m_pad;
     run.R = R;
     run.stripes = stripes;
+    run.al = alphabet_len;
     run.d_t_res = ctx.d_t;
     run.h_t_off = nullptr;
     const uint64_t single[2] = {0, tlen};
@@ -1286,6 +1348,7 @@ hy_status tb_scan_targets(const hy_db *db, void **ctx_slot, cudaStream_t stream,
     run.m_pad = m_pad;
     run.R = R;
     run.stripes = stripes;
+    run.al = db->al;
     run.d_t_res = db->d_tb_res;
     run.h_t_off = db->tb_off.data();
     run.h_t_single = nullptr;
@@ -1398,7 +1461,7 @@ hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const
     p.ends = ctx.d_ends;
     p.go = go;
     p.ge = ge;
-    TbStripes S{ctx.d_first, n_str, ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+    TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
     TB_CK(cudaEventRecord(ctx.ev[0], stream));
     TB_CK(dispatch_stripes(mode, false, p, S, stream, dev));
     TB_CK(cudaEventRecord(ctx.ev[1], stream));
@@ -1719,7 +1782,7 @@ hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_of
                     TB_CK(cudaMemcpyAsync(ctx.d_first, ctx.h_first, sizeof(uint32_t) * (b - a + 1),
                                           cudaMemcpyHostToDevice, stream));
                     TB_CK(cudaMemsetAsync(ctx.d_prog, 0, sizeof(uint32_t) * n_str + 16, stream));
-                    TbStripes S{ctx.d_first, n_str, ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+                    TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(alphabet_len), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
                     TB_CK((launch_stripes<MODE_SW, TB_COLMAX>(p, S, stream, dev)));
                     TB_CK(grow_pinned(ctx.h_total, ctx.ch_total, 16));
                     TB_CK(cudaMemcpyAsync(ctx.h_total, ctx.d_prog, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
