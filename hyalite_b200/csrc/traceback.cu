@@ -8,11 +8,15 @@
 // one 4-bit code while the DP runs, and walks the codes:
 //
 //   bits 0-1  which state H(i,j) came from: 0 diagonal (H == H(i-1,j-1) + sub), 1 E (H == E),
-//             2 F, 3 stop (local mode and H == 0); the walk's H-state rule, tie-break included
+//             2 F; the walk's H-state rule, tie-break included
 //   bit 2     E(i,j) != H(i,j-1) - gap_open  (the E state extends; clear: back to H)
 //   bit 3     F(i,j) != H(i-1,j) - gap_open  (the F state extends; clear: back to H)
 //
-// Half a byte a cell instead of twelve, written once and read only along the path. Cell values
+// The local-mode stop (H == 0) needs no bits: the walk carries the value of the cell it stands on,
+// from the end cell's score back through each operation (a diagonal step subtracts the
+// substitution score, a gap step adds gap_ext while the run extends and gap_open where it opens),
+// and stops where that value is 0. Half a byte a cell instead of twelve, written once and read only
+// along the path. Cell values
 // are int32 with the reference's arithmetic (its width proof keeps every real cell exact), so each
 // code equals the outcome of the reference's comparison and the walk emits the same operations.
 //
@@ -81,6 +85,8 @@ struct TbParams {
     uint8_t *ops_out;
     uint64_t *total;
     int32_t *colmax;  // TB_COLMAX: per pair at TbPair::ops_off, n entries, zeroed before the launch
+    const int32_t *matrix;  // the walk (local mode): substitution scores, al x al
+    uint32_t al;
     int32_t go, ge;
 };
 
@@ -290,7 +296,6 @@ __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int
                         const uint32_t d_ne = min((uint32_t)(h - d), 1u);
                         const uint32_t e_ne = min((uint32_t)(h - e), 1u);
                         uint32_t code = d_ne * e_ne + d_ne;
-                        if (F::local) code |= 3u - 3u * min((uint32_t)h, 1u);
                         code += e_ext * 4u + f_ext * 8u;
                         if (k < 8) w0 += code << (4 * k);
                         else w1 += code << (4 * (k - 8));
@@ -329,9 +334,8 @@ __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int
                 int32_t h = F::local ? __vimax3_s32_relu(d, e, f) : __vimax3_s32(d, e, f);
                 const uint32_t d_ne = min((uint32_t)(h - d), 1u);
                 const uint32_t e_ne = min((uint32_t)(h - e), 1u);
-                // Source: d_ne * (1 + e_ne) is 0 diagonal, 1 E, 2 F; local H == 0 forces 3.
+                // Source: d_ne * (1 + e_ne) is 0 diagonal, 1 E, 2 F.
                 uint32_t code = d_ne * e_ne + d_ne;
-                if (F::local) code |= 3u - 3u * min((uint32_t)h, 1u);
                 code += e_ext * 4u + f_ext * 8u;
                 if (k < 8) w0 += code << (4 * k);
                 else w1 += code << (4 * (k - 8));
@@ -667,6 +671,8 @@ __global__ void __launch_bounds__(64) tb_walk_kernel(TbParams P) {
     uint64_t cnt = 0;
     uint32_t i = brow, j = bcol;
     int state = 0;
+    int32_t v = bs;  // local mode: the value of the cell the walk stands on (H, E or F by state)
+    const int32_t go = P.go, ge = P.ge;
     // Each iteration emits an operation or changes state once between two operations, so the
     // walk ends within 2 (m + n) + 2 iterations.
     for (uint64_t it = 0; it < 2 * cap + 4; ++it) {
@@ -689,26 +695,38 @@ __global__ void __launch_bounds__(64) tb_walk_kernel(TbParams P) {
             }
             break;
         }
+        if (F::local && state == 0 && v == 0) break;  // local && H == 0 (src/align.rs:362-365)
         const uint32_t code = tb_code(D, r_log2, pass_stride, n, i, j);
         if (state == 0) {
             const uint32_t src = code & 3u;
-            if (src == 3u) break;
             if (src == 0u) {
-                if (cnt < cap) slot[cap - 1 - cnt++] = qs[i - 1] == ts[j - 1] ? 0 : 1;
+                const uint32_t a = qs[i - 1], b = ts[j - 1];
+                if (cnt < cap) slot[cap - 1 - cnt++] = a == b ? 0 : 1;
+                if (F::local) v -= P.matrix[a * P.al + b];  // H(i-1, j-1) = H(i, j) - sub
                 --i;
                 --j;
                 continue;
             }
-            state = (int)src;  // the gap step below reads the same cell's code
+            state = (int)src;  // the gap step below reads the same cell's code (E or F = H here)
         }
         if (state == 1) {
             if (cnt < cap) slot[cap - 1 - cnt++] = 3;
             --j;
-            if (!(code & 4u)) state = 0;
+            if (!(code & 4u)) {
+                state = 0;
+                if (F::local) v += go;  // H(i, j - 1) = E(i, j) + go
+            } else if (F::local) {
+                v += ge;  // E(i, j - 1) = E(i, j) + ge
+            }
         } else {
             if (cnt < cap) slot[cap - 1 - cnt++] = 2;
             --i;
-            if (!(code & 8u)) state = 0;
+            if (!(code & 8u)) {
+                state = 0;
+                if (F::local) v += go;  // H(i - 1, j) = F(i, j) + go
+            } else if (F::local) {
+                v += ge;  // F(i - 1, j) = F(i, j) + ge
+            }
         }
     }
     hy_alignment a;
@@ -1008,6 +1026,7 @@ struct TbRun {
     const uint64_t *h_t_single;    // a single target: {offset, length} when h_t_off is null
     bool stripes;                  // fill with the stripe kernel (few long pairs)
     uint64_t al;                   // alphabet size (profile letters)
+    const int32_t *d_matrix;       // substitution matrix on the device (the walk's values)
 };
 
 static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, uint32_t n_idx,
@@ -1094,9 +1113,12 @@ static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, u
     }
     TB_CK(cudaMemcpyAsync(ctx.d_pairs, ctx.h_pairs, sizeof(TbPair) * n_idx, cudaMemcpyHostToDevice, ctx.stream));
     TbParams p;
+    memset(&p, 0, sizeof(p));
     p.q_res = ctx.d_q;
     p.t_res = run.d_t_res;
     p.prof = ctx.d_prof;
+    p.matrix = run.d_matrix;
+    p.al = (uint32_t)run.al;
     p.bnd = ctx.d_bnd;
     p.ends = ctx.d_ends;
     p.out = ctx.d_out;
@@ -1308,6 +1330,7 @@ hy_status hy_align(const uint8_t *query, uint64_t qlen, const uint8_t *target, u
     run.R = R;
     run.stripes = stripes;
     run.al = alphabet_len;
+    run.d_matrix = ctx.d_matrix;
     run.d_t_res = ctx.d_t;
     run.h_t_off = nullptr;
     const uint64_t single[2] = {0, tlen};
@@ -1349,6 +1372,7 @@ hy_status tb_scan_targets(const hy_db *db, void **ctx_slot, cudaStream_t stream,
     run.R = R;
     run.stripes = stripes;
     run.al = db->al;
+    run.d_matrix = db->d_matrix;
     run.d_t_res = db->d_tb_res;
     run.h_t_off = db->tb_off.data();
     run.h_t_single = nullptr;
