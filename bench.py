@@ -931,6 +931,81 @@ def run_position_max(args):
     print(json.dumps(line), flush=True)
 
 
+def run_single_pair(args):
+    """Single long pairs (align_pair's single-pair path, src/kernel.rs:331-397, and align's
+    traceback): for each size in --single-sizes an m x m pair of seeded random residues of the
+    protein generator's background (the second a 15%-mutated copy of the first), SW, the protein
+    scoring. Per size: align_pair ScoreEnd (the score-only stripe kernel: device ms by CUDA events
+    and the whole call) and align (fill, walk and the whole call); `value` is align_pair's device
+    GCUPS on the first size. CPU baseline: the scalar align_core restatement on the first size."""
+    import torch
+
+    import hyalite_b200 as hy
+
+    torch.cuda.set_device(0)
+    mat, _, _, _ = make_workload(args.seed, n_seqs=2)
+    scoring = hy.Scoring(AL, [int(v) for v in mat], GO, GE)
+    rng = np.random.default_rng(args.seed)
+    base = np.random.default_rng(12345)
+    base.integers(-4, 4, size=(AL, AL))
+    base.integers(4, 12, size=AL)
+    background = base.dirichlet(np.full(AL, 4.0))
+    sizes = [int(x) for x in args.single_sizes.split(",")]
+    points = []
+    pairs = []
+    for m in sizes:
+        q = rng.choice(AL, size=m, p=background).astype(np.uint8)
+        t = q.copy()
+        mut = rng.random(m) < 0.15
+        t[mut] = rng.choice(AL, size=int(mut.sum()), p=background)
+        pairs.append((q, t))
+        for _ in range(args.warmup):
+            hy.align_pair(q, t, scoring, hy.Mode.Sw, hy.SearchType.ScoreEnd)
+            hy.align(q, t, scoring, hy.Mode.Sw, hy.USIZE_MAX)
+        kms = cms = fms = wms = ams = 0.0
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            h = hy.align_pair(q, t, scoring, hy.Mode.Sw, hy.SearchType.ScoreEnd)
+            cms += time.perf_counter() - t0
+            kms += hy.align_pairs_timing()[0]
+            t0 = time.perf_counter()
+            a = hy.align(q, t, scoring, hy.Mode.Sw, hy.USIZE_MAX)
+            ams += time.perf_counter() - t0
+            tt = hy.traceback_timing()
+            fms += tt["fill_ms"]
+            wms += tt["walk_ms"]
+        k = args.steps
+        points.append({"m": m, "n": m, "align_pair_kernel_ms": kms / k, "align_pair_call_ms": cms * 1e3 / k,
+                       "align_pair_gcups": m * m / (kms / k * 1e-3) / 1e9, "align_fill_ms": fms / k,
+                       "align_walk_ms": wms / k, "align_call_ms": ams * 1e3 / k, "score": h.score,
+                       "alignment_score": a.score, "ops": len(a.ops_bytes)})
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    q, t = pairs[0]
+    t0 = time.perf_counter()
+    want = pyoracle.align_pair(q, t, mat, AL, GO, GE, 0)
+    cpu_s = time.perf_counter() - t0
+    identical = (points[0]["score"], ) == (want[0], )
+    st, wa, _ = pyoracle.align(q, t, mat, AL, GO, GE, 0) if sizes[0] <= 5000 else (0, None, None)
+    if wa is not None:
+        identical &= hy.align(q, t, scoring, hy.Mode.Sw, hy.USIZE_MAX).as_tuple() == wa
+    line = {
+        "metric": "GCUPS", "value": points[0]["align_pair_gcups"], "unit": "GCUPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": points[0]["align_pair_kernel_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded protein background; the target a 15%-mutated copy of the query)",
+        "config": {"workload": "single long pairs: align_pair ScoreEnd and align (traceback), SW, protein scoring",
+                   "sizes": sizes},
+        "pairs": points,
+        "e2e": {"value": sizes[0] ** 2 / (points[0]["align_pair_call_ms"] * 1e-3) / 1e9, "unit": "GCUPS",
+                "h2d_bytes_per_step": 2 * sizes[0], "d2h_bytes_per_step": 32},
+        "identical_to_oracle": bool(identical),
+        "cpu_baseline": {"value": sizes[0] ** 2 / cpu_s / 1e9, "unit": "GCUPS", "cores": 1, "kind": "port",
+                         "sample": f"one {sizes[0]} x {sizes[0]} pair, scalar align_core restatement, one thread"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SEQS, QUERY_LENGTHS, N_QUERIES
     ap = argparse.ArgumentParser()
@@ -948,7 +1023,9 @@ def main():
     ap.add_argument("--n-queries", type=int, default=N_QUERIES)
     # Other workloads of the same backend (not the default benchmark line).
     ap.add_argument("--workload", default="scan",
-                    choices=["scan", "batched", "served", "pairs", "dna_small", "aligned", "position_max"])
+                    choices=["scan", "batched", "served", "pairs", "dna_small", "aligned", "position_max",
+                             "single_pair"])
+    ap.add_argument("--single-sizes", default="2000,5000,20000")
     ap.add_argument("--n-pos-pairs", type=int, default=1_000_000)
     ap.add_argument("--dna-queries", type=int, default=1000)
     ap.add_argument("--aligned-seqs", type=int, default=100_000)
@@ -982,6 +1059,8 @@ def main():
         run_aligned(args)
     elif args.workload == "position_max":
         run_position_max(args)
+    elif args.workload == "single_pair":
+        run_single_pair(args)
     else:
         run_cuda(args)
 
