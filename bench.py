@@ -714,12 +714,15 @@ def run_pairs(args):
     clocks = Clocks(0)
     clocks.start()
     kms, cms = 0.0, 0.0
+    phases = {}
     for _ in range(args.steps):
         hits, (err, _) = hy.align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
         assert err is None
         k, c = hy.align_pairs_timing()
         kms += k
         cms += c
+        for key, v in hy.align_pairs_phases().items():
+            phases[key] = phases.get(key, 0.0) + v / args.steps
     clk = clocks.stop()
     # Parity on a sample against the oracle, and the CPU baseline (the reference's align_pairs is
     # the scalar align_core loop) on a bounded sample over all host threads.
@@ -752,7 +755,8 @@ def run_pairs(args):
                    "l2": "inputs larger than L2 (reads and windows: gigabytes)"},
         "e2e": {"value": cells * args.steps / (cms * 1e-3) / 1e9, "unit": "GCUPS",
                 "h2d_bytes_per_step": int(len(q_res) + len(t_res) + 16 * args.n_pairs),
-                "d2h_bytes_per_step": 12 * args.n_pairs, "call_ms": cms / args.steps},
+                "d2h_bytes_per_step": 12 * args.n_pairs, "call_ms": cms / args.steps,
+                "phases_ms": {k: round(v, 1) for k, v in phases.items()}},
         "identical_to_oracle_on_sample": identical,
         "cpu_baseline": {"value": ccells / cpu_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
                          "sample": f"the first {n_cpu} pairs, scalar align_core restatement over {threads} threads"},

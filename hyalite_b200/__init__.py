@@ -828,6 +828,17 @@ def align_pairs_timing():
     return float(k.value), float(c.value)
 
 
+def align_pairs_phases():
+    """Phases (ms) of this thread's last align_pairs call: the host lengths pass and routing; host
+    sort and item packing and host staging copies, each summed over the chunks; the chunk pipeline
+    (wall time to the device's end, overlapping the two before); results; host waits for a staging
+    slot."""
+    out = (C.c_double * 6)()
+    _check(lib.hy_align_pairs_phases(out, 6))
+    return {"lengths": out[0], "sort_pack": out[1], "staging": out[2], "pipeline": out[3], "results": out[4],
+            "slot_wait": out[5]}
+
+
 def align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, min_score: Optional[int] = None):
     """align_pair_position_max over many pairs (src/kernel.rs:474-553) on the device: returns
     (hits ctypes array, column maxima int32 array aligned with t_res, score2 int32 array of

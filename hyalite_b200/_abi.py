@@ -117,6 +117,7 @@ SIGNATURES = {
     "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
     "hy_align_pairs_timing": (_st, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "hy_align_pairs_phases": (_st, [C.POINTER(C.c_double), C.c_uint32]),
     "hy_batch_create": (_st, [C.POINTER(_vp), C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_vp)]),
     "hy_batch_destroy": (None, [_vp]),
     "hy_scan_batch": (_st, [_vp, C.c_uint32, _u32p, _u8p, _u64p, C.POINTER(HyHit), _u32p]),

@@ -3,13 +3,125 @@
 
 #include <stdint.h>
 
+#include <pthread.h>
+
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 #include <vector>
 
 namespace hy {
 
-// Runs f(begin, end) over [0, n) split across the host's threads.
+// A pool of host worker threads (one fewer than the host's hardware threads; the caller is the
+// last), created on first use and kept for the process, so a parallel loop costs a wake-up rather
+// than thread creation. One loop runs on the pool at a time; a loop issued while the pool is busy
+// (another caller thread, or a loop inside a pool task) runs on threads of its own. A child made
+// by fork() starts a new pool.
+class HostPool {
+  public:
+    static HostPool *get() {
+        static std::once_flag once;
+        std::call_once(once, [] { pthread_atfork(nullptr, nullptr, [] { instance() = nullptr; }); });
+        HostPool *&p = instance();
+        static std::mutex make;
+        std::lock_guard<std::mutex> lk(make);
+        if (!p) p = new HostPool();  // kept for the process: workers wait on a condition at exit
+        return p;
+    }
+    unsigned size() const { return (unsigned)workers_.size() + 1; }
+    // Runs task(i) for i in [0, n_tasks) on the pool and the calling thread; false (nothing run)
+    // when the pool is busy.
+    template <class T>
+    bool run(unsigned n_tasks, T &task) {
+        if (in_task() || !busy_.try_lock()) return false;
+        Job job;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            job.call = [](void *ctx, unsigned i) { (*static_cast<T *>(ctx))(i); };
+            job.ctx = &task;
+            job.n = n_tasks;
+            job.gen = ++gen_;
+            job_ = job;
+            left_.store(n_tasks);
+            // Task indices are claimed from `next_`, whose high half names the job, so a worker
+            // still holding an earlier job claims nothing from this one.
+            next_.store(job.gen << 32);
+        }
+        cv_.notify_all();
+        work(job);
+        {
+            std::unique_lock<std::mutex> lk(m_);
+            done_.wait(lk, [&] { return left_.load() == 0; });
+        }
+        busy_.unlock();
+        return true;
+    }
+
+  private:
+    struct Job {
+        void (*call)(void *, unsigned) = nullptr;
+        void *ctx = nullptr;
+        unsigned n = 0;
+        uint64_t gen = 0;
+    };
+    HostPool() {
+        const unsigned t = std::max(1u, std::thread::hardware_concurrency());
+        for (unsigned i = 1; i < t; ++i)
+            workers_.emplace_back([this] {
+                in_task() = true;
+                uint64_t seen = 0;
+                for (;;) {
+                    Job job;
+                    {
+                        std::unique_lock<std::mutex> lk(m_);
+                        cv_.wait(lk, [&] { return gen_ != seen; });
+                        seen = gen_;
+                        job = job_;
+                    }
+                    work(job);
+                }
+            });
+        for (auto &w : workers_) w.detach();
+    }
+    static HostPool *&instance() {
+        static HostPool *p = nullptr;
+        return p;
+    }
+    static bool &in_task() {
+        static thread_local bool t = false;
+        return t;
+    }
+    void work(const Job &job) {
+        const bool was = in_task();
+        in_task() = true;
+        uint64_t cur = next_.load();
+        for (;;) {
+            if ((cur >> 32) != (job.gen & 0xffffffffu)) break;
+            const unsigned i = (unsigned)cur;
+            if (i >= job.n) break;
+            if (!next_.compare_exchange_weak(cur, cur + 1)) continue;
+            job.call(job.ctx, i);
+            if (left_.fetch_sub(1) == 1) {
+                std::lock_guard<std::mutex> lk(m_);
+                done_.notify_all();
+            }
+            cur = next_.load();
+        }
+        in_task() = was;
+    }
+    std::vector<std::thread> workers_;
+    std::mutex busy_, m_;
+    std::condition_variable cv_, done_;
+    Job job_;
+    uint64_t gen_ = 0;
+    std::atomic<uint64_t> next_{0};
+    std::atomic<unsigned> left_{0};
+};
+
+// Runs f(begin, end, part) over [0, n) split across the host's threads (at most one part per
+// min_chunk elements).
 template <class F>
 inline void parallel_for(uint64_t n, uint64_t min_chunk, F f) {
     unsigned t = std::max(1u, std::thread::hardware_concurrency());
@@ -18,8 +130,13 @@ inline void parallel_for(uint64_t n, uint64_t min_chunk, F f) {
         f(0, n, 0);
         return;
     }
-    std::vector<std::thread> th;
     const uint64_t per = (n + t - 1) / t;
+    auto task = [&](unsigned i) {
+        const uint64_t a = i * per, e = std::min(n, a + per);
+        if (a < e) f(a, e, i);
+    };
+    if (HostPool::get()->run(t, task)) return;
+    std::vector<std::thread> th;
     for (unsigned i = 0; i < t; ++i) {
         const uint64_t a = i * per, e = std::min(n, a + per);
         if (a >= e) break;

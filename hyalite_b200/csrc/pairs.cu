@@ -1,17 +1,24 @@
 // pairs.cu -- align_pairs (src/kernel.rs:429-452) on the device.
 //
-// Every pair has its own query and target. Pairs are validated in input order exactly like
-// align_pair_with (src/kernel.rs:354-415): symbols of the query then the target, then the width
-// proof on the pair's own lengths; the first failure ends the batch. The accepted prefix is
-// partitioned by the device width rule, sorted by (query length, target length), and packed two
-// pairs of EQUAL query length per int16x2 item so both halves share one row structure. Rows per
-// lane are chosen per query length so that a pass (8 lanes x rows) wastes the fewest padded
-// rows; items of one choice run in one launch. Validation and packing run on all host threads.
+// Every pair has its own query and target. The reference validates pairs in input order exactly
+// like align_pair_with (src/kernel.rs:354-415): symbols of the query then the target, then the
+// width proof on the pair's own lengths; the first failure ends the batch. Here the host checks
+// what depends on lengths only (the width proof and the routing) over all pairs, and the device
+// checks the symbols while it packs; the first failure in input order is then re-derived for the
+// one pair where it lies, so the error, its details and the prefix of results are the reference's.
+//
+// The accepted pairs run in chunks of input order. For each chunk the host sorts the pairs by
+// (query length, target length), groups two pairs of EQUAL query length per int16x2 item (both
+// halves share one row structure) and copies the chunk's raw residues and offsets into a pinned
+// staging slot; a copy stream moves them to the device while the compute stream packs and aligns
+// the previous chunk. Results do not depend on the order, only the speed does. Rows per lane are
+// chosen per query length so that a pass (8 lanes x rows) wastes the fewest padded rows; items of
+// one choice run in one launch.
 #include <string.h>
 
 #include <algorithm>
 #include <chrono>
-#include <mutex>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -29,34 +36,83 @@ constexpr int PAIR_R32 = 16;
 constexpr size_t PAIR_SMEM_LIMIT = 200 * 1024;
 // Largest global scratch for group profiles that do not fit in shared memory, per launch.
 constexpr size_t PAIR_GPROF_BYTES = 256ull << 20;
-// Chunks of items the residue packing is split into, so host packing overlaps the device's copies
-// and kernels (each chunk at least 65,536 items).
-constexpr size_t PAIR_PACK_CHUNKS = 8;
+// Chunks of input pairs the pipeline runs in: at most this many, each at least PAIR_CHUNK_MIN pairs.
+constexpr uint64_t PAIR_MAX_CHUNKS = 16;
+constexpr uint64_t PAIR_CHUNK_MIN = 1 << 16;
+// Pinned staging slots the chunks rotate through.
+constexpr int PAIR_SLOTS = 3;
 // Most warps (128-row stripes) the long pairs of one call may take on the stripe kernel.
 constexpr uint64_t LONG_PAIR_MAX_STRIPES = 2048;
 // Rows per lane the int16x2 pair kernel is compiled for.
 constexpr int PAIR_ROWS[] = {8, 12, 16, 20, 24, 32};
 
-// Grow-only device and pinned buffers of the calling thread (align_pairs keeps one PairScratch
-// per call in the reference; here the device buffers survive across calls of the same thread).
+// Per-pair routing from the lengths pass.
+constexpr uint8_t PAIR_I32 = 1;   // the width proof needs int32 lanes
+constexpr uint8_t PAIR_LONG = 2;  // a long single pair (the stripe kernel, if the call takes it)
+
+// Grow-only host array (no zeroing: every element read is written first in the same call).
+template <class T>
+struct HostArr {
+    std::unique_ptr<T[]> p;
+    size_t n = 0;
+    T *get(size_t want) {
+        want = std::max<size_t>(want, 1);
+        if (n < want) {
+            p.reset(new T[want]);
+            n = want;
+        }
+        return p.get();
+    }
+};
+
+// Device buffer slots of a PairsContext.
+enum PairSlot {
+    PS_Q = 0,    // raw query residues at their q_off positions
+    PS_T,        // raw target residues at their t_off positions
+    PS_QOFF,     // q_off[0 .. n] of the accepted pairs
+    PS_TOFF,     // t_off[0 .. n]
+    PS_META16,   // int16x2 items of the whole call (ItemMeta), then their query lengths and offsets
+    PS_QLEN16,
+    PS_IQOFF16,
+    PS_RES16,    // one chunk's packed target columns
+    PS_BND16,    // one chunk's boundary rows (queries longer than one pass)
+    PS_META32,   // the same for int32 items
+    PS_QLEN32,
+    PS_IQOFF32,
+    PS_RES32,
+    PS_BND32,
+    PS_MATRIX,
+    PS_OUT,      // scores, query ends, target ends per pair, then the first bad-symbol pair
+    PS_GPROF,    // group profiles in global memory (large alphabets)
+    PS_COUNT
+};
+
+// Grow-only device, pinned and host buffers of the calling thread, reused across its calls.
 struct PairsContext {
     int device = -1;
-    cudaStream_t stream = nullptr;
-    std::vector<cudaEvent_t> ev;  // around each chunk's kernels
+    cudaStream_t stream = nullptr;       // packing kernels, pair kernels, results
+    cudaStream_t copy_stream = nullptr;  // host-to-device copies of the chunks
+    std::vector<cudaEvent_t> ev;         // around each chunk's device work
+    cudaEvent_t slot_ev[PAIR_SLOTS] = {};
     struct Buf {
         void *p = nullptr;
         size_t n = 0;
     };
-    Buf b[14];
-    // Grow-only pinned host staging: the packed target residues (one per partition), then the
-    // queries going in and the results coming back (in that stream order).
-    Buf pinned[3];
-    double kernel_ms = 0.0, call_ms = 0.0;  // the last call: pair kernels' device time, whole call
+    Buf b[PS_COUNT];
+    Buf pinned[PAIR_SLOTS + 1];  // the staging ring, then the results
+    double kernel_ms = 0.0, call_ms = 0.0;  // the last call: device time of its kernels, whole call
+    // The last call's phases (ms): the lengths pass and routing, host sort and item packing, host
+    // staging copies, the chunk pipeline (wall time to the device's end), results, host waits for
+    // a staging slot.
+    double phase_ms[6] = {0, 0, 0, 0, 0, 0};
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
         for (auto &x : pinned) cudaFreeHost(x.p);
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        for (cudaEvent_t e : slot_ev)
+            if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
     }
     cudaError_t get_pinned(int slot, size_t bytes, void **out) {
         bytes = std::max<size_t>(bytes, 16);
@@ -71,9 +127,15 @@ struct PairsContext {
         *out = pinned[slot].p;
         return cudaSuccess;
     }
+    // Device buffer of at least `bytes`. Growing a buffer the compute stream may still be reading
+    // first waits for that stream.
     cudaError_t get(int slot, size_t bytes, void **out) {
         bytes = std::max<size_t>(bytes, 16);
         if (b[slot].n < bytes) {
+            if (stream) {
+                cudaError_t e = cudaStreamSynchronize(stream);
+                if (e != cudaSuccess) return e;
+            }
             cudaFree(b[slot].p);
             b[slot].p = nullptr;
             b[slot].n = 0;
@@ -87,6 +149,16 @@ struct PairsContext {
 };
 
 static thread_local PairsContext g_ctx;
+
+// Grow-only host arrays of the calling thread: per-pair routes, a chunk's sort and item arrays.
+struct PairsHost {
+    HostArr<uint8_t> route;
+    HostArr<uint32_t> ord[2], ord_tmp, start, qlen[2];
+    HostArr<uint64_t> keys[2], keys_tmp;
+    std::vector<std::vector<uint64_t>> count;  // radix histograms, one per host thread
+};
+
+static thread_local PairsHost g_host;
 
 #define HY_CK(call)                                                                                \
     do {                                                                                           \
@@ -188,247 +260,249 @@ static int pair_rows(uint64_t q, int32_t al) {
     return best;
 }
 
-// Sorts pair indices (given in ascending order) by (query length desc, target length desc), index
-// asc for equal lengths: a stable LSD radix sort of 64-bit keys (complemented query length above
-// complemented target length) on 16-bit digits, skipping digits every pair shares. The keys are
-// built once from the offsets in input order and travel with the indices, so no pass reads the
-// offsets at random; histograms and scatters run on all host threads (per-thread ranges in order,
-// which keeps the sort stable). `keys` receives the sorted keys.
-static inline uint32_t key_qlen(uint64_t k) { return ~(uint32_t)(k >> 32); }
-static inline uint32_t key_tlen(uint64_t k) { return ~(uint32_t)k; }
-
-static void sort_by_shape(std::vector<uint32_t> &o, const uint64_t *q_off, const uint64_t *t_off,
-                          std::vector<uint64_t> &keys) {
-    const size_t n = o.size();
-    keys.resize(n);
-    parallel_for(n, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
-        for (uint64_t i = a; i < e; ++i) {
-            const uint32_t k = o[i];
-            keys[i] = ((uint64_t)~(uint32_t)(q_off[k + 1] - q_off[k]) << 32) | ~(uint32_t)(t_off[k + 1] - t_off[k]);
-        }
-    });
-    if (n < 2) return;
-    std::vector<uint32_t> tmp(n);
-    std::vector<uint64_t> key_tmp(n);
-    const unsigned nt = host_threads(n, 1 << 16);
-    const uint64_t per = (n + nt - 1) / nt;
-    std::vector<std::vector<size_t>> count(nt, std::vector<size_t>(1 << 16));
-    for (int shift = 0; shift < 64; shift += 16) {
-        parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
-            for (uint64_t t = ta; t < te; ++t) {
-                std::fill(count[t].begin(), count[t].end(), 0);
-                for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i)
-                    ++count[t][(keys[i] >> shift) & 0xffff];
-            }
-        });
-        const size_t d0 = (keys[0] >> shift) & 0xffff;
-        size_t total0 = 0;
-        for (unsigned t = 0; t < nt; ++t) total0 += count[t][d0];
-        if (total0 == n) continue;  // one digit value: nothing to do
-        size_t sum = 0;
-        for (size_t d = 0; d < (1u << 16); ++d)
-            for (unsigned t = 0; t < nt; ++t) {
-                const size_t c = count[t][d];
-                count[t][d] = sum;
-                sum += c;
-            }
-        parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
-            for (uint64_t t = ta; t < te; ++t)
-                for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i) {
-                    const size_t dst = count[t][(keys[i] >> shift) & 0xffff]++;
-                    tmp[dst] = o[i];
-                    key_tmp[dst] = keys[i];
+// Packs the target columns of the int16x2 or int32 items [i0, i1) of one chunk (item columns run
+// from meta.col_off to the next item's col_off, the last item's to col_end): an int16x2 item keeps
+// pair 0 in the low byte and pair 1 in the high byte, the shorter padded with symbol `al`; an
+// int32 item one byte a column, padded with 0. Writes each item's query length and query offsets,
+// and checks every residue of the items' queries and targets against the alphabet: a symbol
+// >= al records its pair in *bad (the smallest such pair wins) and is replaced by a valid code, so
+// no kernel indexes a profile or the matrix with it. Such pairs are at or past the batch's first
+// failure, and their results are never returned. One warp an item.
+template <class A>
+__global__ void __launch_bounds__(256) pack_items_kernel(const ItemMeta *meta, uint32_t i0, uint32_t i1,
+                                                         uint64_t col_end, const uint64_t *q_off,
+                                                         const uint64_t *t_off, uint8_t *q_res,
+                                                         const uint8_t *t_res, typename A::RES *res,
+                                                         uint32_t *qlen, uint64_t *iqoff, uint32_t al,
+                                                         uint32_t *bad) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t it = i0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < i1; it += n_warps) {
+        const ItemMeta m = meta[it];
+        const uint64_t end = it + 1 < i1 ? meta[it + 1].col_off : col_end;
+        const bool two = A::NH == 2 && m.idx[1] != NO_INDEX;
+        const uint8_t *t0 = t_res + t_off[m.idx[0]];
+        const uint8_t *t1 = two ? t_res + t_off[m.idx[1]] : t0;
+        typename A::RES *out = res + m.col_off;
+        bool bad0 = false, bad1 = false;
+        for (uint64_t j = lane; j < end - m.col_off; j += 32) {
+            if constexpr (A::NH == 2) {
+                uint32_t lo = al, hi = al;
+                if (j < m.n[0]) {
+                    lo = t0[j];
+                    if (lo >= al) bad0 = true, lo = al;
                 }
-        });
-        o.swap(tmp);
-        keys.swap(key_tmp);
+                if (two && j < m.n[1]) {
+                    hi = t1[j];
+                    if (hi >= al) bad1 = true, hi = al;
+                }
+                out[j] = (typename A::RES)(lo | (hi << 8));
+            } else {
+                uint32_t v = 0;
+                if (j < m.n[0]) {
+                    v = t0[j];
+                    if (v >= al) bad0 = true, v = 0;
+                }
+                out[j] = (typename A::RES)v;
+            }
+        }
+        for (int h = 0; h < (two ? 2 : 1); ++h) {
+            const uint64_t qa = q_off[m.idx[h]], ql = q_off[m.idx[h] + 1] - qa;
+            bool bq = false;
+            for (uint64_t i = lane; i < ql; i += 32)
+                if (q_res[qa + i] >= al) bq = true, q_res[qa + i] = 0;
+            (h == 0 ? bad0 : bad1) |= bq;
+        }
+        bad0 = __any_sync(0xffffffffu, bad0);
+        bad1 = __any_sync(0xffffffffu, bad1);
+        if (lane == 0) {
+            const uint64_t qa = q_off[m.idx[0]];
+            qlen[it] = (uint32_t)(q_off[m.idx[0] + 1] - qa);
+            iqoff[2 * it] = qa;
+            iqoff[2 * it + 1] = two ? q_off[m.idx[1]] : qa;
+            if (bad0) atomicMin(bad, m.idx[0]);
+            if (bad1) atomicMin(bad, m.idx[1]);
+        }
     }
 }
 
-struct PairPart {
-    std::vector<ItemMeta> meta;
-    std::vector<uint32_t> qlen;
-    std::vector<uint64_t> qoff;
-    uint64_t cols = 0;
-};
+// Sort keys: complemented query length above complemented target length, so ascending keys are
+// query length desc, then target length desc.
+static inline uint64_t shape_key(uint64_t ql, uint64_t tl) {
+    return ((uint64_t)~(uint32_t)ql << 32) | ~(uint32_t)tl;
+}
+static inline uint32_t key_qlen(uint64_t k) { return ~(uint32_t)(k >> 32); }
+static inline uint32_t key_tlen(uint64_t k) { return ~(uint32_t)k; }
 
-// Packs the pairs listed in `order` (already sorted by query length, then target length, both
-// descending; `keys` their sort keys). Pair16 items take two consecutive pairs when their query
-// lengths are equal. Item boundaries come from one sequential pass over the keys; the items are
-// then filled, and their column offsets prefix-summed, on all host threads.
-static void pack_pairs(const std::vector<uint32_t> &order, const std::vector<uint64_t> &keys,
-                       const uint64_t *q_off, bool two, PairPart &pp) {
-    const uint64_t align = two ? 8 : 16;
-    std::vector<uint32_t> start;
-    start.reserve(two ? order.size() / 2 + 1 : order.size());
-    for (size_t i = 0; i < order.size();) {
-        start.push_back((uint32_t)i);
-        i += (two && i + 1 < order.size() && key_qlen(keys[i + 1]) == key_qlen(keys[i])) ? 2 : 1;
+// Sorts n pair indices (ascending on entry) with their keys: a stable LSD radix sort on 16-bit
+// digits, skipping digits every key shares; histograms and scatters on all host threads
+// (per-thread ranges in order keep it stable). o / keys end up pointing at the sorted arrays
+// (either the given ones or the scratch ones, which are swapped with them).
+static void sort_by_shape(PairsHost &hs, uint32_t *&o, uint64_t *&keys, uint32_t *&o_tmp,
+                          uint64_t *&k_tmp, size_t n) {
+    if (n < 2) return;
+    const unsigned nt = host_threads(n, 1 << 16);
+    const uint64_t per = (n + nt - 1) / nt;
+    if (hs.count.size() < nt) hs.count.resize(nt);
+    for (unsigned t = 0; t < nt; ++t) hs.count[t].resize(1 << 16);
+    // Bits in which some key differs from the first: digits without any are skipped.
+    std::vector<uint64_t> diff(nt, 0);
+    parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+        for (uint64_t t = ta; t < te; ++t) {
+            uint64_t acc = 0;
+            for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i) acc |= keys[i] ^ keys[0];
+            diff[t] = acc;
+        }
+    });
+    uint64_t varies = 0;
+    for (uint64_t x : diff) varies |= x;
+    for (int shift = 0; shift < 64; shift += 16) {
+        if (((varies >> shift) & 0xffff) == 0) continue;
+        parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+            for (uint64_t t = ta; t < te; ++t) {
+                std::vector<uint64_t> &c = hs.count[t];
+                std::fill(c.begin(), c.end(), 0);
+                for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i)
+                    ++c[(keys[i] >> shift) & 0xffff];
+            }
+        });
+        uint64_t sum = 0;
+        for (size_t d = 0; d < (1u << 16); ++d)
+            for (unsigned t = 0; t < nt; ++t) {
+                const uint64_t c = hs.count[t][d];
+                hs.count[t][d] = sum;
+                sum += c;
+            }
+        parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+            for (uint64_t t = ta; t < te; ++t) {
+                std::vector<uint64_t> &c = hs.count[t];
+                for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i) {
+                    const uint64_t dst = c[(keys[i] >> shift) & 0xffff]++;
+                    o_tmp[dst] = o[i];
+                    k_tmp[dst] = keys[i];
+                }
+            }
+        });
+        std::swap(o, o_tmp);
+        std::swap(keys, k_tmp);
     }
-    const size_t n_items = start.size();
-    pp.meta.resize(n_items);
-    pp.qlen.resize(n_items);
-    pp.qoff.resize(2 * n_items);
+}
+
+// Groups n sorted pairs into items (an int16x2 item takes two consecutive pairs of equal query
+// length) and writes their ItemMeta (columns from 0 within the chunk, each item's padded to
+// `align`) and query lengths; returns the item count and sets *cols. Boundaries come from one
+// sequential pass over the keys; the items are filled, and their column offsets prefix-summed, on
+// all host threads.
+static size_t pack_items(PairsHost &hs, const uint32_t *order, const uint64_t *keys, size_t n,
+                         bool two, ItemMeta *meta, uint32_t *qlen, uint64_t *cols) {
+    const uint64_t align = two ? 8 : 16;
+    uint32_t *start = hs.start.get(n + 1);
+    size_t n_items = 0;
+    for (size_t i = 0; i < n;) {
+        start[n_items++] = (uint32_t)i;
+        i += (two && i + 1 < n && key_qlen(keys[i + 1]) == key_qlen(keys[i])) ? 2 : 1;
+    }
+    start[n_items] = (uint32_t)n;
     const unsigned nt = host_threads(n_items, 1 << 15);
     const uint64_t per = (n_items + nt - 1) / nt;
     std::vector<uint64_t> part(nt + 1, 0);
     parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
         for (uint64_t t = ta; t < te; ++t) {
-            uint64_t cols = 0;
+            uint64_t c = 0;
             for (uint64_t it = t * per; it < std::min<uint64_t>(n_items, (t + 1) * per); ++it) {
                 const size_t i = start[it];
-                const bool pair = it + 1 < n_items ? start[it + 1] - i == 2 : order.size() - i == 2;
-                ItemMeta &m = pp.meta[it];
+                const bool pair = start[it + 1] - i == 2;
+                ItemMeta &m = meta[it];
                 m.pad_ = 0;
                 m.idx[0] = order[i];
                 m.n[0] = key_tlen(keys[i]);
                 m.idx[1] = pair ? order[i + 1] : NO_INDEX;
                 m.n[1] = pair ? key_tlen(keys[i + 1]) : 0;
                 m.w = std::max(m.n[0], m.n[1]);
-                m.col_off = cols;  // within this thread's range; shifted below
-                cols += (m.w + align - 1) / align * align;
-                pp.qlen[it] = key_qlen(keys[i]);
-                pp.qoff[2 * it] = q_off[m.idx[0]];
-                pp.qoff[2 * it + 1] = pair ? q_off[m.idx[1]] : q_off[m.idx[0]];
+                m.col_off = c;  // within this thread's range; shifted below
+                c += (m.w + align - 1) / align * align;
+                qlen[it] = key_qlen(keys[i]);
             }
-            part[t + 1] = cols;
+            part[t + 1] = c;
         }
     });
     for (unsigned t = 0; t < nt; ++t) part[t + 1] += part[t];
     parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
         for (uint64_t t = ta; t < te; ++t)
             for (uint64_t it = t * per; it < std::min<uint64_t>(n_items, (t + 1) * per); ++it)
-                pp.meta[it].col_off += part[t];
+                meta[it].col_off += part[t];
     });
-    pp.cols = part[nt];
+    *cols = part[nt];
+    return n_items;
 }
 
+// Packs and aligns one chunk's items of one lane arithmetic: the packing kernel, then one launch
+// per run of items with the same rows per lane (items are sorted by query length). Items
+// [ib, ib + n_items) of the call; qlen (host) their query lengths; cols the chunk's columns.
 template <class A, int G>
-static hy_status run_part(PairsContext &ctx, int slot0, const PairPart &pp, const uint8_t *t_res,
-                          const uint64_t *t_off, const uint8_t *d_q, const int32_t *d_matrix,
-                          int32_t al, int32_t go, int32_t ge, int mode, bool ends, int32_t *d_scores,
-                          int32_t *d_qend, int32_t *d_tend) {
-    if (pp.meta.empty()) return fail(HY_OK);
-    const bool two = A::NH == 2;
-    const size_t n_items = pp.meta.size();
-    void *d_meta, *d_qlen, *d_qoff, *d_res, *d_bnd;
-    HY_CK(ctx.get(slot0 + 0, sizeof(ItemMeta) * n_items, &d_meta));
-    HY_CK(ctx.get(slot0 + 1, sizeof(uint32_t) * n_items, &d_qlen));
-    HY_CK(ctx.get(slot0 + 2, sizeof(uint64_t) * 2 * n_items, &d_qoff));
-    const size_t res_bytes = pp.cols * sizeof(typename A::RES);
-    HY_CK(ctx.get(slot0 + 3, res_bytes, &d_res));
-    // Rows per lane of each item (a function of its query length; items are sorted by it).
-    std::vector<int> rows(n_items);
+static hy_status run_items(PairsContext &ctx, PairParams p, int res_slot, int bnd_slot,
+                           const uint32_t *qlen, size_t ib, size_t n_items, uint64_t cols,
+                           const uint64_t *d_qoff, const uint64_t *d_toff, uint8_t *d_q,
+                           const uint8_t *d_t, uint32_t *d_bad, int mode, bool ends) {
+    if (n_items == 0) return fail(HY_OK);
+    constexpr bool two = A::NH == 2;
+    void *d_res;
+    HY_CK(ctx.get(res_slot, cols * sizeof(typename A::RES), &d_res));
+    {
+        const int blocks = (int)std::min<uint64_t>((n_items + 7) / 8, 148 * 16);
+        pack_items_kernel<A><<<blocks, 256, 0, ctx.stream>>>(
+            p.meta, (uint32_t)ib, (uint32_t)(ib + n_items), cols, d_qoff, d_toff, d_q, d_t,
+            (typename A::RES *)d_res, const_cast<uint32_t *>(p.qlen), const_cast<uint64_t *>(p.qoff),
+            (uint32_t)p.al, d_bad);
+        HY_CK(cudaGetLastError());
+    }
+    // Rows per lane of each run of equal query lengths.
+    auto rows_of = [&](uint32_t q) { return two ? pair_rows(q, p.al) : PAIR_R32; };
     bool multipass = false;
-    for (size_t i = 0; i < n_items; ++i) {
-        rows[i] = two ? pair_rows(pp.qlen[i], al) : PAIR_R32;
-        multipass = multipass || pp.qlen[i] > (uint32_t)(G * rows[i]);
+    for (size_t i = 0; i < n_items;) {
+        size_t j = i;
+        while (j < n_items && qlen[j] == qlen[i]) ++j;
+        multipass = multipass || qlen[i] > (uint32_t)(G * rows_of(qlen[i]));
+        i = j;
     }
-    HY_CK(ctx.get(slot0 + 4, multipass ? 2 * sizeof(typename A::V) * pp.cols : 16, &d_bnd));
-    // Target residues (the shorter half of a pair item padded with symbol `al`) are packed
-    // straight into pinned staging (every column, padding included, is written), in chunks of
-    // items: while the device copies and aligns chunk c, the host threads pack chunk c + 1.
-    void *h_res = nullptr;
-    HY_CK(ctx.get_pinned(slot0 == 0 ? 0 : 1, res_bytes, &h_res));
-    typename A::RES *res = static_cast<typename A::RES *>(h_res);
-    HY_CK(cudaMemcpyAsync(d_meta, pp.meta.data(), sizeof(ItemMeta) * n_items, cudaMemcpyHostToDevice, ctx.stream));
-    HY_CK(cudaMemcpyAsync(d_qlen, pp.qlen.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice, ctx.stream));
-    HY_CK(cudaMemcpyAsync(d_qoff, pp.qoff.data(), sizeof(uint64_t) * 2 * n_items, cudaMemcpyHostToDevice, ctx.stream));
-    PairParams p{};
-    p.meta = (const ItemMeta *)d_meta;
-    p.qlen = (const uint32_t *)d_qlen;
-    p.qoff = (const uint64_t *)d_qoff;
-    p.q_res = d_q;
+    void *d_bnd = nullptr;
+    if (multipass) HY_CK(ctx.get(bnd_slot, 2 * sizeof(typename A::V) * cols, &d_bnd));
     p.res = d_res;
-    p.matrix = d_matrix;
-    p.al = al;
-    p.lim = two ? 32767 - go : 536870911;
-    p.go = go;
-    p.ge = ge;
-    p.sentinel = two ? -32768 + ge : INT32_MIN / 4;
-    p.top_free = (mode == MODE_SW || mode == MODE_HW || mode == MODE_OV) ? 1 : 0;
     p.boundary = d_bnd;
-    p.scores = d_scores;
-    p.qend = d_qend;
-    p.tend = d_tend;
     p.gprof = nullptr;
-    // Kernels of items [a, b), split where the rows per lane change.
-    auto launch_range = [&](size_t a, size_t b) -> hy_status {
-        for (size_t i0 = a; i0 < b;) {
-            size_t i1 = i0;
-            while (i1 < b && rows[i1] == rows[i0]) ++i1;
-            const int r = rows[i0];
-            const size_t group_bytes = (size_t)(al + 1) * G * r * profile_row_bytes<A>();
-            int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
-            gpb = gpb / (32 / G) * (32 / G);  // whole warps
-            p.group_bytes = (uint32_t)group_bytes;
-            if (gpb == 0) {
-                // Not one warp of group profiles fits in shared memory (a large alphabet): the
-                // groups keep their profiles in a global scratch region, in launches of bounded size.
-                gpb = 256 / G;
-                const size_t per_block = (size_t)gpb * group_bytes;
-                const size_t max_blocks = std::max<size_t>(1, PAIR_GPROF_BYTES / per_block);
-                const size_t need_blocks = (i1 - i0 + gpb - 1) / gpb;
-                void *d_gprof;
-                HY_CK(ctx.get(13, std::min(max_blocks, need_blocks) * per_block, &d_gprof));
-                p.gprof = (uint8_t *)d_gprof;
-                for (size_t j0 = i0; j0 < i1; j0 += max_blocks * gpb) {
-                    const size_t j1 = std::min(i1, j0 + max_blocks * gpb);
-                    p.item_base = (uint32_t)j0;
-                    p.n_items = (uint32_t)j1;
-                    const int blocks = (int)((j1 - j0 + gpb - 1) / gpb);
-                    HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, 0, ctx.stream)));
-                }
-                p.gprof = nullptr;
-            } else {
-                p.item_base = (uint32_t)i0;
-                p.n_items = (uint32_t)i1;
-                const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
-                HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
+    for (size_t i0 = 0; i0 < n_items;) {
+        const int r = rows_of(qlen[i0]);
+        size_t i1 = i0;
+        while (i1 < n_items && (qlen[i1] == qlen[i0] || rows_of(qlen[i1]) == r)) ++i1;
+        const size_t group_bytes = (size_t)(p.al + 1) * G * r * profile_row_bytes<A>();
+        int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
+        gpb = gpb / (32 / G) * (32 / G);  // whole warps
+        p.group_bytes = (uint32_t)group_bytes;
+        if (gpb == 0) {
+            // Not one warp of group profiles fits in shared memory (a large alphabet): the groups
+            // keep their profiles in a global scratch region, in launches of bounded size.
+            gpb = 256 / G;
+            const size_t per_block = (size_t)gpb * group_bytes;
+            const size_t max_blocks = std::max<size_t>(1, PAIR_GPROF_BYTES / per_block);
+            const size_t need_blocks = (i1 - i0 + gpb - 1) / gpb;
+            void *d_gprof;
+            HY_CK(ctx.get(PS_GPROF, std::min(max_blocks, need_blocks) * per_block, &d_gprof));
+            p.gprof = (uint8_t *)d_gprof;
+            for (size_t j0 = i0; j0 < i1; j0 += max_blocks * gpb) {
+                const size_t j1 = std::min(i1, j0 + max_blocks * gpb);
+                p.item_base = (uint32_t)(ib + j0);
+                p.n_items = (uint32_t)(ib + j1);
+                const int blocks = (int)((j1 - j0 + gpb - 1) / gpb);
+                HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, 0, ctx.stream)));
             }
-            i0 = i1;
+            p.gprof = nullptr;
+        } else {
+            p.item_base = (uint32_t)(ib + i0);
+            p.n_items = (uint32_t)(ib + i1);
+            const int blocks = (int)((i1 - i0 + gpb - 1) / gpb);
+            HY_CK((launch_pairs_rows<A, G>(r, mode, ends, p, blocks, gpb * G, gpb * group_bytes, ctx.stream)));
         }
-        return fail(HY_OK);
-    };
-    const size_t n_chunks = std::max<size_t>(1, std::min<size_t>(PAIR_PACK_CHUNKS, n_items / (1 << 16)));
-    while (ctx.ev.size() < 2 * n_chunks) {
-        cudaEvent_t e;
-        HY_CK(cudaEventCreate(&e));
-        ctx.ev.push_back(e);
-    }
-    for (size_t c = 0; c < n_chunks; ++c) {
-        const size_t a = n_items * c / n_chunks, b = n_items * (c + 1) / n_chunks;
-        parallel_for(b - a, 1 << 14, [&](uint64_t x0, uint64_t x1, unsigned) {
-            for (uint64_t it = a + x0; it < a + x1; ++it) {
-                const ItemMeta &m = pp.meta[it];
-                const uint64_t end = it + 1 < n_items ? pp.meta[it + 1].col_off : pp.cols;
-                const uint8_t *t0 = t_res + t_off[m.idx[0]];
-                const uint8_t *t1 = m.idx[1] == NO_INDEX ? nullptr : t_res + t_off[m.idx[1]];
-                for (uint64_t j = 0; j < end - m.col_off; ++j) {
-                    if (two) {
-                        uint32_t lo = j < m.n[0] ? t0[j] : (uint32_t)al;
-                        uint32_t hi = (t1 && j < m.n[1]) ? t1[j] : (uint32_t)al;
-                        res[m.col_off + j] = (typename A::RES)(lo | (hi << 8));
-                    } else {
-                        res[m.col_off + j] = (typename A::RES)(j < m.n[0] ? t0[j] : 0);
-                    }
-                }
-            }
-        });
-        const uint64_t c0 = pp.meta[a].col_off, c1 = b < n_items ? pp.meta[b].col_off : pp.cols;
-        HY_CK(cudaMemcpyAsync((typename A::RES *)d_res + c0, res + c0, (c1 - c0) * sizeof(typename A::RES),
-                              cudaMemcpyHostToDevice, ctx.stream));
-        HY_CK(cudaEventRecord(ctx.ev[2 * c], ctx.stream));
-        hy_status st = launch_range(a, b);
-        if (st != HY_OK) return st;
-        HY_CK(cudaEventRecord(ctx.ev[2 * c + 1], ctx.stream));
-    }
-    // The host staging (the item vectors and the pinned residues) must outlive the async copies.
-    HY_CK(cudaStreamSynchronize(ctx.stream));
-    for (size_t c = 0; c < n_chunks; ++c) {
-        float ms = 0.0f;
-        HY_CK(cudaEventElapsedTime(&ms, ctx.ev[2 * c], ctx.ev[2 * c + 1]));
-        ctx.kernel_ms += ms;
+        i0 = i1;
     }
     return fail(HY_OK);
 }
@@ -440,10 +514,16 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                                     const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
                                     int32_t gap_ext, hy_mode mode, hy_search_type search_type,
                                     hy_hit *out, uint64_t *failed_pair) {
-    const auto t_call = std::chrono::steady_clock::now();
+    using clock = std::chrono::steady_clock;
+    auto since = [](clock::time_point t) {
+        return std::chrono::duration<double, std::milli>(clock::now() - t).count();
+    };
+    const auto t_call = clock::now();
     PairsContext &ctx = g_ctx;
+    PairsHost &hs = g_host;
     ctx.kernel_ms = 0.0;
     ctx.call_ms = 0.0;
+    for (double &x : ctx.phase_ms) x = 0.0;
     if (failed_pair) *failed_pair = n_pairs;
     if ((int)mode < 0 || (int)mode > 4) return fail(HY_ERR_INVALID_ARGUMENT);
     if ((int)search_type < HY_SEARCH_SCORE || (int)search_type > HY_SEARCH_ALIGNMENT)
@@ -456,89 +536,90 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
     const int32_t min_e = *std::min_element(matrix, matrix + alphabet_len * alphabet_len);
     const int32_t max_e = *std::max_element(matrix, matrix + alphabet_len * alphabet_len);
 
-    // Validate in input order, chunked over the host threads: each chunk stops at its own first
-    // failure, and the batch's first failure is that of the first chunk that has one. The pairs
-    // before it are partitioned by the device width rule in input order.
+    // The lengths pass, chunked over the host threads: each pair's width proof and route; each
+    // chunk stops at its own first failure, and the batch's first length failure is that of the
+    // first chunk that has one.
     const unsigned nt = host_threads(n_pairs, 1 << 15);
-    struct Chunk {
+    struct LenPart {
         uint64_t first_bad = ~0ull;
         hy_status st = HY_OK;
-        int64_t d[3] = {0, 0, 0};
-        std::vector<uint32_t> o16, o32;
+        int64_t d0 = 0;
+        uint64_t n[2] = {0, 0};
+        std::vector<uint32_t> longs;
     };
-    std::vector<Chunk> chunks(nt);
-    const uint64_t per = (n_pairs + nt - 1) / nt;
-    parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
-        for (uint64_t c = ca; c < ce; ++c) {
-            Chunk &ch = chunks[c];
-            const uint64_t a = c * per, e = std::min(n_pairs, a + per);
-            for (uint64_t k = a; k < e && ch.st == HY_OK; ++k) {
-                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-                for (int s = 0; s < 2 && ch.st == HY_OK; ++s) {
-                    const uint8_t *seq = s == 0 ? q_res + q_off[k] : t_res + t_off[k];
-                    const uint64_t len = s == 0 ? ql : tl;
-                    const int bad = first_bad_symbol(seq, len, alphabet_len);
-                    if (bad >= 0) {
-                        ch.st = HY_ERR_SYMBOL_OUT_OF_RANGE;
-                        ch.d[0] = bad;
-                        ch.d[1] = (int64_t)alphabet_len;
-                    }
-                }
-                if (ch.st == HY_OK) {
+    std::vector<LenPart> parts(nt);
+    uint8_t *route = hs.route.get(n_pairs);
+    {
+        const uint64_t per = (n_pairs + nt - 1) / nt;
+        parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
+            for (uint64_t c = ca; c < ce; ++c) {
+                LenPart &pt = parts[c];
+                const uint64_t a = c * per, e = std::min(n_pairs, a + per);
+                for (uint64_t k = a; k < e; ++k) {
+                    const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
                     const int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, ql, tl);
-                    if (narrowest_width(b) < 0) {
-                        ch.st = HY_ERR_SCORE_RANGE_TOO_WIDE;
-                        ch.d[0] = b;
-                    } else if (ql >= (1u << 30) || tl >= (1u << 31)) {
-                        ch.st = HY_ERR_UNSUPPORTED;
-                    } else {
-                        (device_fits_i16(b, gap_open) ? ch.o16 : ch.o32).push_back((uint32_t)k);
+                    if (narrowest_width(b) < 0 || ql >= (1u << 30) || tl >= (1u << 31)) {
+                        pt.st = narrowest_width(b) < 0 ? HY_ERR_SCORE_RANGE_TOO_WIDE : HY_ERR_UNSUPPORTED;
+                        pt.d0 = narrowest_width(b) < 0 ? b : 0;
+                        pt.first_bad = k;
+                        break;
                     }
+                    uint8_t r = device_fits_i16(b, gap_open) ? 0 : PAIR_I32;
+                    if (tb_long_pair(ql, tl)) {
+                        r |= PAIR_LONG;
+                        pt.longs.push_back((uint32_t)k);
+                    }
+                    route[k] = r;
+                    ++pt.n[r & PAIR_I32];
                 }
-                if (ch.st != HY_OK) ch.first_bad = k;
             }
-        }
-    });
-    uint64_t n_ok = n_pairs;
-    hy_status first = HY_OK;
-    int64_t d[3] = {0, 0, 0};
-    std::vector<uint32_t> o16, o32;
-    for (Chunk &ch : chunks) {
-        o16.insert(o16.end(), ch.o16.begin(), ch.o16.end());
-        o32.insert(o32.end(), ch.o32.begin(), ch.o32.end());
-        if (ch.st != HY_OK) {
-            first = ch.st;
-            n_ok = ch.first_bad;
-            memcpy(d, ch.d, sizeof(d));
+        });
+    }
+    uint64_t n_len = n_pairs;  // pairs before the first length failure
+    hy_status len_st = HY_OK;
+    int64_t len_d0 = 0;
+    uint64_t n_part[2] = {0, 0};
+    std::vector<uint32_t> olong;
+    for (LenPart &pt : parts) {
+        olong.insert(olong.end(), pt.longs.begin(), pt.longs.end());
+        n_part[0] += pt.n[0];
+        n_part[1] += pt.n[1];
+        if (pt.st != HY_OK) {
+            n_len = pt.first_bad;
+            len_st = pt.st;
+            len_d0 = pt.d0;
             break;
         }
     }
-    if (failed_pair && first != HY_OK) *failed_pair = n_ok;
     // A few long pairs (the single-pair path) take the score-only stripe kernel: every 128 query
     // rows on their own warp. Many long pairs keep the packed pair kernels, whose throughput is
-    // higher once the whole GPU is busy.
-    std::vector<uint32_t> olong;
+    // higher once the whole GPU is busy. The host checks the long pairs' symbols (the device checks
+    // the others while packing them).
+    uint64_t n_long_bad = n_pairs;  // the first long pair with a symbol out of range
+    std::vector<uint32_t> run_long;
     {
         uint64_t stripes = 0;
-        for (const std::vector<uint32_t> *v : {&o16, &o32})
-            for (uint32_t k : *v) {
-                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-                if (tb_long_pair(ql, tl)) {
-                    olong.push_back(k);
-                    stripes += tb_long_pair_stripes(ql);
-                }
+        for (uint32_t k : olong) stripes += tb_long_pair_stripes(q_off[k + 1] - q_off[k]);
+        if (stripes > LONG_PAIR_MAX_STRIPES) olong.clear();
+        for (uint32_t k : olong) {
+            if (first_bad_symbol(q_res + q_off[k], q_off[k + 1] - q_off[k], alphabet_len) >= 0 ||
+                first_bad_symbol(t_res + t_off[k], t_off[k + 1] - t_off[k], alphabet_len) >= 0) {
+                n_long_bad = k;
+                break;
             }
-        if (stripes > LONG_PAIR_MAX_STRIPES) {
-            olong.clear();
-        } else if (!olong.empty()) {
-            std::vector<char> is_long(n_ok, 0);
-            for (uint32_t k : olong) is_long[k] = 1;
-            for (std::vector<uint32_t> *v : {&o16, &o32})
-                v->erase(std::remove_if(v->begin(), v->end(), [&](uint32_t k) { return is_long[k] != 0; }),
-                         v->end());
+            run_long.push_back(k);
         }
     }
-    if (n_ok > 0) {
+    const bool use_long = !olong.empty();
+    if (use_long)
+        for (uint32_t k : olong) --n_part[route[k] & PAIR_I32];
+    ctx.phase_ms[0] = since(t_call);
+
+    uint32_t dev_bad = NO_INDEX;  // the first pair whose symbols the device found out of range
+    const bool ends = search_type != HY_SEARCH_SCORE;
+    const int32_t *h_out = nullptr;
+    const auto t_pipe = clock::now();
+    if (n_len > 0) {
         int dev = 0;
         HY_CK(cudaGetDevice(&dev));
         if (ctx.device != dev) {
@@ -546,66 +627,235 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             new (&ctx) PairsContext();
             ctx.device = dev;
             HY_CK(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
+            HY_CK(cudaStreamCreateWithFlags(&ctx.copy_stream, cudaStreamNonBlocking));
+            for (cudaEvent_t &e : ctx.slot_ev) HY_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
-        // Sort by (query length desc, target length desc, index asc) through 64-bit keys.
-        std::vector<uint64_t> k16, k32;
-        sort_by_shape(o16, q_off, t_off, k16);
-        sort_by_shape(o32, q_off, t_off, k32);
-        PairPart p16, p32;
-        pack_pairs(o16, k16, q_off, true, p16);
-        pack_pairs(o32, k32, q_off, false, p32);
-
-        void *d_q, *d_matrix, *d_out;
-        const uint64_t qbytes = q_off[n_ok] - q_off[0];
-        HY_CK(ctx.get(10, q_off[n_ok], &d_q));
-        HY_CK(ctx.get(11, sizeof(int32_t) * alphabet_len * alphabet_len, &d_matrix));
-        HY_CK(ctx.get(12, 3 * sizeof(int32_t) * n_ok, &d_out));
-        void *h_stage = nullptr;
-        HY_CK(ctx.get_pinned(2, std::max<uint64_t>(qbytes, 3 * sizeof(int32_t) * n_ok), &h_stage));
-        if (qbytes) {
-            parallel_for(qbytes, 1 << 24, [&](uint64_t a, uint64_t e, unsigned) {
-                memcpy((uint8_t *)h_stage + a, q_res + q_off[0] + a, e - a);
-            });
-            HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[0], h_stage, qbytes, cudaMemcpyHostToDevice, ctx.stream));
+        const uint64_t L = n_len;
+        const uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(PAIR_MAX_CHUNKS, L / PAIR_CHUNK_MIN));
+        auto chunk_at = [&](uint64_t c) { return L * c / n_chunks; };
+        while (ctx.ev.size() < 2 * n_chunks) {
+            cudaEvent_t e;
+            HY_CK(cudaEventCreate(&e));
+            ctx.ev.push_back(e);
         }
+        // Buffers of the whole call, and the largest chunk's staging and packed columns.
+        uint64_t slot_bytes = 0, res_cols = 0;
+        for (uint64_t c = 0; c < n_chunks; ++c) {
+            const uint64_t a = chunk_at(c), b = chunk_at(c + 1);
+            const uint64_t qb = q_off[b] - q_off[a], tb = t_off[b] - t_off[a];
+            slot_bytes = std::max(slot_bytes, (qb + tb + 7) / 8 * 8 + 16 * (b - a + 1) + sizeof(ItemMeta) * (b - a));
+            res_cols = std::max(res_cols, tb + 16 * (b - a));
+        }
+        void *d_q, *d_t, *d_qoff, *d_toff, *d_matrix, *d_out, *scratch;
+        HY_CK(ctx.get(PS_Q, q_off[L], &d_q));
+        HY_CK(ctx.get(PS_T, t_off[L], &d_t));
+        HY_CK(ctx.get(PS_QOFF, sizeof(uint64_t) * (L + 1), &d_qoff));
+        HY_CK(ctx.get(PS_TOFF, sizeof(uint64_t) * (L + 1), &d_toff));
+        HY_CK(ctx.get(PS_MATRIX, sizeof(int32_t) * alphabet_len * alphabet_len, &d_matrix));
+        HY_CK(ctx.get(PS_OUT, 3 * sizeof(int32_t) * L + sizeof(uint32_t), &d_out));
+        int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + L, *d_tend = d_qend + L;
+        uint32_t *d_bad = (uint32_t *)(d_tend + L);
+        PairParams pp[2];
+        const int meta_slot[2] = {PS_META16, PS_META32}, qlen_slot[2] = {PS_QLEN16, PS_QLEN32};
+        const int iqoff_slot[2] = {PS_IQOFF16, PS_IQOFF32}, res_slot[2] = {PS_RES16, PS_RES32};
+        for (int h = 0; h < 2; ++h) {
+            PairParams &p = pp[h];
+            p = PairParams{};
+            if (n_part[h] == 0) continue;
+            void *m, *ql, *qo;
+            HY_CK(ctx.get(meta_slot[h], sizeof(ItemMeta) * n_part[h], &m));
+            HY_CK(ctx.get(qlen_slot[h], sizeof(uint32_t) * n_part[h], &ql));
+            HY_CK(ctx.get(iqoff_slot[h], 2 * sizeof(uint64_t) * n_part[h], &qo));
+            HY_CK(ctx.get(res_slot[h], res_cols * (h == 0 ? sizeof(Pair16::RES) : sizeof(Single32::RES)), &scratch));
+            p.meta = (const ItemMeta *)m;
+            p.qlen = (const uint32_t *)ql;
+            p.qoff = (const uint64_t *)qo;
+            p.q_res = (const uint8_t *)d_q;
+            p.matrix = (const int32_t *)d_matrix;
+            p.al = (int32_t)alphabet_len;
+            p.lim = h == 0 ? 32767 - gap_open : 536870911;
+            p.go = gap_open;
+            p.ge = gap_ext;
+            p.sentinel = h == 0 ? -32768 + gap_ext : INT32_MIN / 4;
+            p.top_free = ((int)mode == MODE_SW || (int)mode == MODE_HW || (int)mode == MODE_OV) ? 1 : 0;
+            p.scores = d_scores;
+            p.qend = d_qend;
+            p.tend = d_tend;
+        }
+        void *slots[PAIR_SLOTS];
+        for (int s = 0; s < PAIR_SLOTS && s < (int)n_chunks; ++s) HY_CK(ctx.get_pinned(s, slot_bytes, &slots[s]));
+        HY_CK(cudaMemsetAsync(d_bad, 0xff, sizeof(uint32_t), ctx.stream));
         HY_CK(cudaMemcpyAsync(d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, ctx.stream));
-        int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + n_ok, *d_tend = d_qend + n_ok;
-        const bool ends = search_type != HY_SEARCH_SCORE;
-        if (!olong.empty()) {
-            st = tb_long_pair_scores(q_res, q_off, t_res, t_off, olong, (const uint8_t *)d_q,
+        uint64_t ib[2] = {0, 0};
+        for (uint64_t c = 0; c < n_chunks; ++c) {
+            const uint64_t a = chunk_at(c), b = chunk_at(c + 1), n = b - a;
+            auto t0 = clock::now();
+            // This chunk's packed pairs of each lane arithmetic, in input order, with their keys.
+            uint32_t *o[2], *o_tmp[2];
+            uint64_t *k[2], *k_tmp[2];
+            for (int h = 0; h < 2; ++h) {
+                o[h] = hs.ord[h].get(n);
+                k[h] = hs.keys[h].get(n);
+            }
+            o_tmp[0] = hs.ord_tmp.get(n);
+            k_tmp[0] = hs.keys_tmp.get(n);
+            size_t cnt[2] = {0, 0};
+            {
+                const unsigned pt = host_threads(n, 1 << 15);
+                const uint64_t per = (n + pt - 1) / pt;
+                std::vector<uint64_t> at(2 * (pt + 1), 0);
+                parallel_for(pt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+                    for (uint64_t t = ta; t < te; ++t)
+                        for (uint64_t x = a + t * per; x < std::min<uint64_t>(b, a + (t + 1) * per); ++x)
+                            if (!(use_long && (route[x] & PAIR_LONG))) ++at[2 * (t + 1) + (route[x] & PAIR_I32)];
+                });
+                for (unsigned t = 0; t < pt; ++t) {
+                    at[2 * (t + 1)] += at[2 * t];
+                    at[2 * (t + 1) + 1] += at[2 * t + 1];
+                }
+                cnt[0] = at[2 * pt];
+                cnt[1] = at[2 * pt + 1];
+                parallel_for(pt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
+                    for (uint64_t t = ta; t < te; ++t) {
+                        uint64_t pos[2] = {at[2 * t], at[2 * t + 1]};
+                        for (uint64_t x = a + t * per; x < std::min<uint64_t>(b, a + (t + 1) * per); ++x) {
+                            if (use_long && (route[x] & PAIR_LONG)) continue;
+                            const int h = route[x] & PAIR_I32;
+                            o[h][pos[h]] = (uint32_t)x;
+                            k[h][pos[h]++] = shape_key(q_off[x + 1] - q_off[x], t_off[x + 1] - t_off[x]);
+                        }
+                    }
+                });
+            }
+            for (int h = 0; h < 2; ++h) {
+                o_tmp[h] = o_tmp[0];
+                k_tmp[h] = k_tmp[0];
+            }
+            // The staging slot: [query residues][target residues][q_off, t_off slices][items].
+            const int s = (int)(c % PAIR_SLOTS);
+            auto tw = clock::now();
+            if (c >= (uint64_t)PAIR_SLOTS) HY_CK(cudaEventSynchronize(ctx.slot_ev[s]));
+            ctx.phase_ms[5] += since(tw);
+            uint8_t *slot = (uint8_t *)slots[s];
+            const uint64_t qb = q_off[b] - q_off[a], tb = t_off[b] - t_off[a];
+            uint64_t *s_qoff = (uint64_t *)(slot + (qb + tb + 7) / 8 * 8), *s_toff = s_qoff + (n + 1);
+            ItemMeta *s_meta[2];
+            s_meta[0] = (ItemMeta *)(s_toff + (n + 1));
+            size_t n_items[2] = {0, 0};
+            uint64_t cols[2] = {0, 0};
+            uint32_t *qlen[2];
+            for (int h = 0; h < 2; ++h) {
+                if (h == 1) s_meta[1] = s_meta[0] + n_items[0];
+                qlen[h] = hs.qlen[h].get(cnt[h]);
+                if (cnt[h] == 0) continue;
+                // One scratch pair serves both arithmetics: sort and pack the first before the second.
+                sort_by_shape(hs, o[h], k[h], o_tmp[h], k_tmp[h], cnt[h]);
+                n_items[h] = pack_items(hs, o[h], k[h], cnt[h], h == 0, s_meta[h], qlen[h], &cols[h]);
+            }
+            ctx.phase_ms[1] += since(t0);
+            t0 = clock::now();
+            parallel_for(qb + tb, 1 << 24, [&](uint64_t x0, uint64_t x1, unsigned) {
+                if (x0 < qb) memcpy(slot + x0, q_res + q_off[a] + x0, std::min(x1, qb) - x0);
+                if (x1 > qb) {
+                    const uint64_t y0 = std::max(x0, qb);
+                    memcpy(slot + y0, t_res + t_off[a] + (y0 - qb), x1 - y0);
+                }
+            });
+            memcpy(s_qoff, q_off + a, sizeof(uint64_t) * (n + 1));
+            memcpy(s_toff, t_off + a, sizeof(uint64_t) * (n + 1));
+            ctx.phase_ms[2] += since(t0);
+            cudaStream_t cs = ctx.copy_stream;
+            if (qb) HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[a], slot, qb, cudaMemcpyHostToDevice, cs));
+            if (tb) HY_CK(cudaMemcpyAsync((uint8_t *)d_t + t_off[a], slot + qb, tb, cudaMemcpyHostToDevice, cs));
+            HY_CK(cudaMemcpyAsync((uint64_t *)d_qoff + a, s_qoff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cs));
+            HY_CK(cudaMemcpyAsync((uint64_t *)d_toff + a, s_toff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cs));
+            for (int h = 0; h < 2; ++h)
+                if (n_items[h])
+                    HY_CK(cudaMemcpyAsync(const_cast<ItemMeta *>(pp[h].meta) + ib[h], s_meta[h],
+                                          sizeof(ItemMeta) * n_items[h], cudaMemcpyHostToDevice, cs));
+            HY_CK(cudaEventRecord(ctx.slot_ev[s], cs));
+            HY_CK(cudaStreamWaitEvent(ctx.stream, ctx.slot_ev[s], 0));
+            HY_CK(cudaEventRecord(ctx.ev[2 * c], ctx.stream));
+            st = run_items<Pair16, PAIR_G>(ctx, pp[0], PS_RES16, PS_BND16, qlen[0], ib[0], n_items[0], cols[0],
+                                           (const uint64_t *)d_qoff, (const uint64_t *)d_toff, (uint8_t *)d_q,
+                                           (const uint8_t *)d_t, d_bad, mode, ends);
+            if (st != HY_OK) return st;
+            st = run_items<Single32, PAIR_G>(ctx, pp[1], PS_RES32, PS_BND32, qlen[1], ib[1], n_items[1], cols[1],
+                                             (const uint64_t *)d_qoff, (const uint64_t *)d_toff, (uint8_t *)d_q,
+                                             (const uint8_t *)d_t, d_bad, mode, ends);
+            if (st != HY_OK) return st;
+            HY_CK(cudaEventRecord(ctx.ev[2 * c + 1], ctx.stream));
+            ib[0] += n_items[0];
+            ib[1] += n_items[1];
+        }
+        // The long pairs, once every chunk's queries are on the device (the compute stream has
+        // waited for each chunk's copies).
+        if (!run_long.empty()) {
+            st = tb_long_pair_scores(q_res, q_off, t_res, t_off, run_long, (const uint8_t *)d_q,
                                      (const int32_t *)d_matrix, alphabet_len, gap_open, gap_ext, mode,
                                      ctx.stream, d_scores, d_qend, d_tend, &ctx.kernel_ms);
             if (st != HY_OK) return st;
         }
-        st = run_part<Pair16, PAIR_G>(ctx, 0, p16, t_res, t_off, (const uint8_t *)d_q,
-                                      (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
-                                      gap_ext, mode, ends, d_scores, d_qend, d_tend);
-        if (st != HY_OK) return st;
-        st = run_part<Single32, PAIR_G>(ctx, 5, p32, t_res, t_off, (const uint8_t *)d_q,
-                                        (const int32_t *)d_matrix, (int32_t)alphabet_len, gap_open,
-                                        gap_ext, mode, ends, d_scores, d_qend, d_tend);
-        if (st != HY_OK) return st;
-        // Stream order: the query copy out of the staging buffer is done before this copy into it.
-        const int32_t *h = (const int32_t *)h_stage;
-        HY_CK(cudaMemcpyAsync(h_stage, d_out, 3 * sizeof(int32_t) * n_ok, cudaMemcpyDeviceToHost, ctx.stream));
+        void *h_stage = nullptr;
+        HY_CK(ctx.get_pinned(PAIR_SLOTS, 3 * sizeof(int32_t) * L + sizeof(uint32_t), &h_stage));
+        HY_CK(cudaMemcpyAsync(h_stage, d_out, 3 * sizeof(int32_t) * L + sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.stream));
         HY_CK(cudaStreamSynchronize(ctx.stream));
+        for (uint64_t c = 0; c < n_chunks; ++c) {
+            float ms = 0.0f;
+            HY_CK(cudaEventElapsedTime(&ms, ctx.ev[2 * c], ctx.ev[2 * c + 1]));
+            ctx.kernel_ms += ms;
+        }
+        h_out = (const int32_t *)h_stage;
+        memcpy(&dev_bad, h_out + 3 * L, sizeof(uint32_t));
+    }
+    ctx.phase_ms[3] = since(t_pipe);
+    const auto t_res_fill = clock::now();
+    // The batch's first failure in input order, and its details from that pair alone: symbols of
+    // the query, then of the target, then the width proof.
+    const uint64_t n_ok = std::min<uint64_t>({n_len, n_long_bad, (uint64_t)dev_bad});
+    hy_status first = HY_OK;
+    int64_t d[3] = {0, 0, 0};
+    if (n_ok < n_pairs) {
+        const uint64_t kk = n_ok;
+        const int bq = first_bad_symbol(q_res + q_off[kk], q_off[kk + 1] - q_off[kk], alphabet_len);
+        const int bt = bq >= 0 ? -1 : first_bad_symbol(t_res + t_off[kk], t_off[kk + 1] - t_off[kk], alphabet_len);
+        if (bq >= 0 || bt >= 0) {
+            first = HY_ERR_SYMBOL_OUT_OF_RANGE;
+            d[0] = bq >= 0 ? bq : bt;
+            d[1] = (int64_t)alphabet_len;
+        } else {
+            first = len_st;
+            d[0] = len_d0;
+        }
+        if (failed_pair) *failed_pair = n_ok;
+    }
+    if (n_ok > 0) {
+        const uint64_t L = n_len;
+        const int32_t *h = h_out;
         parallel_for(n_ok, 1 << 16, [&](uint64_t a, uint64_t e, unsigned) {
             for (uint64_t k = a; k < e; ++k) {
                 out[k].score = h[k];
                 out[k].reserved = 0;
                 out[k].db_index = k;
-                out[k].query_end = ends ? (int64_t)h[n_ok + k] : -1;
-                out[k].target_end = ends ? (int64_t)h[2 * n_ok + k] : -1;
+                out[k].query_end = ends ? (int64_t)h[L + k] : -1;
+                out[k].target_end = ends ? (int64_t)h[2 * L + k] : -1;
             }
         });
     }
-    ctx.call_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
+    ctx.phase_ms[4] = since(t_res_fill);
+    ctx.call_ms = since(t_call);
     return fail(first, d[0], d[1], d[2]);
 }
 
 extern "C" hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms) {
     if (kernel_ms) *kernel_ms = g_ctx.kernel_ms;
     if (call_ms) *call_ms = g_ctx.call_ms;
+    return fail(HY_OK);
+}
+
+extern "C" hy_status hy_align_pairs_phases(double *ms, uint32_t n) {
+    if (!ms && n) return fail(HY_ERR_INVALID_ARGUMENT);
+    for (uint32_t i = 0; i < n && i < 6; ++i) ms[i] = g_ctx.phase_ms[i];
     return fail(HY_OK);
 }

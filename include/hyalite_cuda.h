@@ -321,8 +321,10 @@ hy_status hy_server_stats_read(hy_server *server, int reset, hy_server_stats *ou
  * validated in order (symbols query-then-target, then the width proof on its exact lengths); on
  * the first failing pair the call returns its error, *failed_pair receives its index and out[0 ..
  * index) holds the hits of the pairs before it. db_index of each hit is its pair index. The calling
- * thread keeps grow-only device buffers and a pinned host staging buffer for the packed targets
- * between calls (freed at thread exit). */
+ * thread keeps grow-only device buffers, a ring of pinned host staging slots and host work arrays
+ * between calls (freed at thread exit). Internally the width proof runs on the host over every
+ * pair and the symbol check on the device while it packs each chunk; the reported error, index and
+ * prefix are those of the in-order validation. */
 hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
                          const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
                          uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
@@ -330,6 +332,11 @@ hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint
 /* Timing of this thread's last hy_align_pairs call (no reference counterpart): the device time of
  * its pair kernels (CUDA events around the launches) and the wall time of the whole call. */
 hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
+/* Phases of this thread's last hy_align_pairs call, in ms (no reference counterpart): up to n of
+ * {the host lengths pass and routing, host sort and item packing (summed over chunks), host staging
+ * copies (summed), the chunk pipeline (wall time to the device's end, overlapping the two before),
+ * results back, host waits for a staging slot}. */
+hy_status hy_align_pairs_phases(double *ms, uint32_t n);
 
 /* ---- traceback: the Alignment search type (src/align.rs, src/database.rs:517-565) -------------- */
 

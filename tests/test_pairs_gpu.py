@@ -158,3 +158,100 @@ def test_single_long_pair_align_pair():
         h = hy.align_pair(q, t, hy.Scoring(20, BLOSUM62, 11, 1), hy.Mode(mode), hy.SearchType.ScoreEnd)
         assert (h.score, h.db_index, h.query_end, h.target_end) == \
             (lambda s: (s[0], 0, s[1], s[2]))(o.align_pair(q, t, BLOSUM62, 20, 11, 1, mode))
+
+
+def _concat(seqs):
+    off = np.zeros(len(seqs) + 1, np.uint64)
+    off[1:] = np.cumsum([len(s) for s in seqs])
+    return np.concatenate([np.asarray(s, np.uint8) for s in seqs]) if len(seqs) else np.zeros(0, np.uint8), off
+
+
+def _arrays_call(qs, ts, mat, al, go, ge, mode, st):
+    q_res, q_off = _concat(qs)
+    t_res, t_off = _concat(ts)
+    hits, (err, failed) = hy.align_pairs_arrays(q_res, q_off, t_res, t_off, hy.Scoring(al, mat, go, ge),
+                                                hy.Mode(mode), hy.SearchType(st))
+    return hits, err, failed
+
+
+def _check_sample(hits, qs, ts, idx, mat, al, go, ge, mode, st):
+    status, want, _ = o.align_pairs([qs[i] for i in idx], [ts[i] for i in idx], mat, al, go, ge, mode, st)
+    assert status == 0
+    got = [(hits[i].score, None if hits[i].query_end < 0 else hits[i].query_end,
+            None if hits[i].target_end < 0 else hits[i].target_end, hits[i].db_index) for i in idx]
+    assert got == [(w[0], w[2], w[3], i) for w, i in zip(want, idx)]
+
+
+@pytest.mark.parametrize("case", ["query_symbol", "width_first", "same_pair", "long_pair_symbol"])
+def test_first_failure_across_chunks(case):
+    """The batch's first failure in input order (src/kernel.rs:429-452) when the length checks run
+    on the host over all pairs and the symbol checks on the device per chunk: a bad query symbol
+    in a later chunk with a width failure after it; a width failure before a symbol failure; a
+    pair with both (symbols are checked first); a bad symbol inside a long pair of a many-chunk
+    batch. The prefix before the failure is complete and exact."""
+    rng = np.random.default_rng({"query_symbol": 1, "width_first": 2, "same_pair": 3, "long_pair_symbol": 4}[case])
+    n = 300_000
+    qs = [rng.integers(0, 4, int(rng.integers(5, 40))) for _ in range(n)]
+    ts = [rng.integers(0, 4, int(rng.integers(5, 60))) for _ in range(n)]
+    go, ge = 2, 1
+    # A wide matrix entry makes long pairs need int32 and very long ones exceed the width proof.
+    mat = [2 if a == b else -1 for a in range(4) for b in range(4)]
+    mat[5] = 3000
+    width_bad = 250_000
+    qs[width_bad] = rng.integers(0, 4, 200_000)
+    ts[width_bad] = rng.integers(0, 4, 200_000)
+    if case == "query_symbol":
+        bad = 180_000
+        qs[bad] = qs[bad].copy()
+        qs[bad][3] = 9
+        want_err, want_at = hy.Error("SymbolOutOfRange", symbol=9, alphabet_len=4), bad
+    elif case == "width_first":
+        bad = 260_000
+        ts[bad] = ts[bad].copy()
+        ts[bad][0] = 200
+        want_at = width_bad
+        want_err = None
+    elif case == "same_pair":
+        ts[width_bad] = ts[width_bad].copy()
+        ts[width_bad][17] = 4
+        want_err, want_at = hy.Error("SymbolOutOfRange", symbol=4, alphabet_len=4), width_bad
+    else:
+        # Long pairs (the stripe path) early in the batch; one carries a bad target symbol.
+        base = rng.integers(0, 4, 3000)
+        for j, k in enumerate((1_000, 70_000, 140_000)):
+            qs[k] = base[:1200]
+            ts[k] = rng.integers(0, 4, 1500)
+        bad = 140_000
+        ts[bad] = ts[bad].copy()
+        ts[bad][1400] = 6
+        want_err, want_at = hy.Error("SymbolOutOfRange", symbol=6, alphabet_len=4), bad
+    hits, err, failed = _arrays_call(qs, ts, mat, 4, go, ge, hy.Mode.Sw, 1)
+    assert failed == want_at
+    if want_err is None:
+        assert err.kind == "ScoreRangeTooWide"
+    else:
+        assert err == want_err
+    sample = sorted(set(list(range(0, want_at, 7919)) + [want_at - 1, 1_000, 70_000]) & set(range(want_at)))
+    _check_sample(hits, qs, ts, sample, mat, 4, go, ge, 0, 1)
+
+
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_many_chunks_mixed_widths_and_long_pairs(mode):
+    """A batch of several chunks mixing int16x2 pairs, int32 pairs (a wide matrix entry on long
+    pairs), empty sequences and a few long pairs on the stripe kernel: every result exact."""
+    rng = np.random.default_rng(90 + mode)
+    n = 200_000
+    mat = [int(v) for v in rng.integers(-3, 4, 16)]
+    mat[0] = 400
+    qs = [rng.integers(0, 4, int(rng.integers(0, 30))) for _ in range(n)]
+    ts = [rng.integers(0, 4, int(rng.integers(0, 50))) for _ in range(n)]
+    for k in rng.choice(n, 300, replace=False):
+        qs[k] = rng.integers(0, 4, int(rng.integers(90, 200)))
+        ts[k] = rng.integers(0, 4, int(rng.integers(100, 300)))
+    for k in (5, 99_999, 150_001):
+        qs[k] = rng.integers(0, 4, 1100)
+        ts[k] = rng.integers(0, 4, 1300)
+    hits, err, failed = _arrays_call(qs, ts, mat, 4, 9, 2, mode, 1)
+    assert err is None and failed == n
+    sample = sorted(set(list(range(0, n, 997)) + [5, 99_999, 150_001, n - 1]))
+    _check_sample(hits, qs, ts, sample, mat, 4, 9, 2, mode, 1)
