@@ -832,19 +832,23 @@ def align_pairs_phases():
     """Phases (ms) of this thread's last align_pairs call: the host lengths pass and routing; host
     sort and item packing and host staging copies, each summed over the chunks; the chunk pipeline
     (wall time to the device's end, overlapping the two before); results; host waits for a staging
-    slot."""
-    out = (C.c_double * 6)()
-    _check(lib.hy_align_pairs_phases(out, 6))
+    slot; host copies of the column maxima (align_pairs_position_max, whose last call it also
+    reports)."""
+    out = (C.c_double * 7)()
+    _check(lib.hy_align_pairs_phases(out, 7))
     return {"lengths": out[0], "sort_pack": out[1], "staging": out[2], "pipeline": out[3], "results": out[4],
-            "slot_wait": out[5]}
+            "slot_wait": out[5], "colmax_copy": out[6]}
 
 
-def align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, min_score: Optional[int] = None):
+def align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring: Scoring, min_score: Optional[int] = None,
+                                    colmax_out: Optional[np.ndarray] = None):
     """align_pair_position_max over many pairs (src/kernel.rs:474-553) on the device: returns
     (hits ctypes array, column maxima int32 array aligned with t_res, score2 int32 array of
     (score, position) per pair or None, (error or None, failed index)). ``min_score`` set: each pair's
     score2 (src/kernel.rs:741-792) with its best score, its target end (0 when None) and the
-    matrix's largest entry; position -1 means None."""
+    matrix's largest entry; position -1 means None. ``colmax_out``: a contiguous int32 array of at
+    least t_off[-1] - t_off[0] entries refilled in place and returned (the reference's ``out``
+    vector is likewise the caller's, cleared and refilled), instead of a new array a call."""
     q_res = np.ascontiguousarray(q_res, dtype=np.uint8)
     t_res = np.ascontiguousarray(t_res, dtype=np.uint8)
     q_res = q_res if q_res.size else np.zeros(1, np.uint8)
@@ -853,7 +857,13 @@ def align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring: Scoring
     t_off = np.ascontiguousarray(t_off, dtype=np.uint64)
     n = len(q_off) - 1
     out = (_abi.HyHit * max(n, 1))()
-    cm = np.zeros(max(1, int(t_off[-1] - t_off[0])) if n else 1, np.int32)
+    need = max(1, int(t_off[-1] - t_off[0])) if n else 1
+    if colmax_out is not None:
+        if colmax_out.dtype != np.int32 or not colmax_out.flags.c_contiguous or colmax_out.size < need:
+            raise ValueError("colmax_out must be a contiguous int32 array of t_off[-1] - t_off[0] entries")
+        cm = colmax_out
+    else:
+        cm = np.zeros(need, np.int32)
     s2 = np.zeros(2 * max(n, 1), np.int32) if min_score is not None else None
     failed = C.c_uint64()
     st = lib.hy_align_pairs_position_max(

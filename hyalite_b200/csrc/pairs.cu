@@ -82,8 +82,11 @@ enum PairSlot {
     PS_RES32,
     PS_BND32,
     PS_MATRIX,
-    PS_OUT,      // scores, query ends, target ends per pair, then the first bad-symbol pair
+    PS_OUT,      // scores, query ends, target ends per pair, the first bad-symbol pair, score2 pairs
     PS_GPROF,    // group profiles in global memory (large alphabets)
+    PS_ITOFF16,  // position maxima: items' target offsets per half
+    PS_ITOFF32,
+    PS_COLMAX,   // position maxima: column maxima at the targets' offsets
     PS_COUNT
 };
 
@@ -92,19 +95,20 @@ struct PairsContext {
     int device = -1;
     cudaStream_t stream = nullptr;       // packing kernels, pair kernels, results
     cudaStream_t copy_stream = nullptr;  // host-to-device copies of the chunks
-    std::vector<cudaEvent_t> ev;         // around each chunk's device work
+    cudaStream_t d2h_stream = nullptr;   // position maxima: each chunk's column maxima back
+    std::vector<cudaEvent_t> ev;         // around each chunk's device work, then its copy back
     cudaEvent_t slot_ev[PAIR_SLOTS] = {};
     struct Buf {
         void *p = nullptr;
         size_t n = 0;
     };
     Buf b[PS_COUNT];
-    Buf pinned[PAIR_SLOTS + 1];  // the staging ring, then the results
+    Buf pinned[PAIR_SLOTS + 2];  // the staging ring, the results, the column maxima
     double kernel_ms = 0.0, call_ms = 0.0;  // the last call: device time of its kernels, whole call
     // The last call's phases (ms): the lengths pass and routing, host sort and item packing, host
     // staging copies, the chunk pipeline (wall time to the device's end), results, host waits for
-    // a staging slot.
-    double phase_ms[6] = {0, 0, 0, 0, 0, 0};
+    // a staging slot, host copies of the column maxima into the caller's array (position maxima).
+    double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
     ~PairsContext() {
         for (auto &x : b) cudaFree(x.p);
         for (auto &x : pinned) cudaFreeHost(x.p);
@@ -113,6 +117,7 @@ struct PairsContext {
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (d2h_stream) cudaStreamDestroy(d2h_stream);
     }
     cudaError_t get_pinned(int slot, size_t bytes, void **out) {
         bytes = std::max<size_t>(bytes, 16);
@@ -169,10 +174,10 @@ static thread_local PairsHost g_host;
         }                                                                                          \
     } while (0)
 
-template <class A, int G, int R, int MODE, bool ENDS, bool GPROF>
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF, bool COLMAX = false>
 static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int threads, size_t smem,
                                      cudaStream_t st) {
-    auto kern = pairs_kernel<A, G, R, MODE, ENDS, GPROF>;
+    auto kern = pairs_kernel<A, G, R, MODE, ENDS, GPROF, COLMAX>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -182,11 +187,13 @@ static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int thread
 }
 
 // The form with group profiles in global memory (p.gprof set): only the smallest row shape of
-// each lane arithmetic, which is what a large alphabet runs.
+// each lane arithmetic, which is what a large alphabet runs. p.colmax set: the column-maxima form
+// (local mode, score only).
 template <class A, int G, int R>
 static cudaError_t launch_pairs_gprof(int mode, bool ends, const PairParams &p, int blocks,
                                       int threads, cudaStream_t st) {
     if constexpr ((A::NH == 2 && R == 8) || (A::NH == 1 && R == PAIR_R32)) {
+        if (p.colmax) return launch_pairs_mode<A, G, R, MODE_SW, false, true, true>(p, blocks, threads, 0, st);
 #define HY_MODE_CASE(M)                                                                     \
     case M:                                                                                 \
         return ends ? launch_pairs_mode<A, G, R, M, true, true>(p, blocks, threads, 0, st)  \
@@ -207,6 +214,7 @@ template <class A, int G, int R>
 static cudaError_t launch_pairs(int mode, bool ends, const PairParams &p, int blocks, int threads,
                                 size_t smem, cudaStream_t st) {
     if (p.gprof) return launch_pairs_gprof<A, G, R>(mode, ends, p, blocks, threads, st);
+    if (p.colmax) return launch_pairs_mode<A, G, R, MODE_SW, false, false, true>(p, blocks, threads, smem, st);
 #define HY_MODE_CASE(M)                                                                        \
     case M:                                                                                    \
         return ends ? launch_pairs_mode<A, G, R, M, true, false>(p, blocks, threads, smem, st) \
@@ -263,8 +271,8 @@ static int pair_rows(uint64_t q, int32_t al) {
 // Packs the target columns of the int16x2 or int32 items [i0, i1) of one chunk (item columns run
 // from meta.col_off to the next item's col_off, the last item's to col_end): an int16x2 item keeps
 // pair 0 in the low byte and pair 1 in the high byte, the shorter padded with symbol `al`; an
-// int32 item one byte a column, padded with 0. Writes each item's query length and query offsets,
-// and checks every residue of the items' queries and targets against the alphabet: a symbol
+// int32 item one byte a column, padded with 0. Writes each item's query length and query offsets
+// (and, for column maxima, target offsets), and checks every residue of the items' queries and targets against the alphabet: a symbol
 // >= al records its pair in *bad (the smallest such pair wins) and is replaced by a valid code, so
 // no kernel indexes a profile or the matrix with it. Such pairs are at or past the batch's first
 // failure, and their results are never returned. One warp an item.
@@ -273,8 +281,8 @@ __global__ void __launch_bounds__(256) pack_items_kernel(const ItemMeta *meta, u
                                                          uint64_t col_end, const uint64_t *q_off,
                                                          const uint64_t *t_off, uint8_t *q_res,
                                                          const uint8_t *t_res, typename A::RES *res,
-                                                         uint32_t *qlen, uint64_t *iqoff, uint32_t al,
-                                                         uint32_t *bad) {
+                                                         uint32_t *qlen, uint64_t *iqoff, uint64_t *itoff,
+                                                         uint32_t al, uint32_t *bad) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t it = i0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < i1; it += n_warps) {
@@ -320,6 +328,10 @@ __global__ void __launch_bounds__(256) pack_items_kernel(const ItemMeta *meta, u
             qlen[it] = (uint32_t)(q_off[m.idx[0] + 1] - qa);
             iqoff[2 * it] = qa;
             iqoff[2 * it + 1] = two ? q_off[m.idx[1]] : qa;
+            if (itoff) {
+                itoff[2 * it] = t_off[m.idx[0]];
+                itoff[2 * it + 1] = two ? t_off[m.idx[1]] : t_off[m.idx[0]];
+            }
             if (bad0) atomicMin(bad, m.idx[0]);
             if (bad1) atomicMin(bad, m.idx[1]);
         }
@@ -334,17 +346,17 @@ static inline uint64_t shape_key(uint64_t ql, uint64_t tl) {
 static inline uint32_t key_qlen(uint64_t k) { return ~(uint32_t)(k >> 32); }
 static inline uint32_t key_tlen(uint64_t k) { return ~(uint32_t)k; }
 
-// Sorts n pair indices (ascending on entry) with their keys: a stable LSD radix sort on 16-bit
-// digits, skipping digits every key shares; histograms and scatters on all host threads
+// Sorts n pair indices (ascending on entry) with their keys: a stable LSD radix sort on 8-bit
+// digits, skipping digits every key shares (lengths of one workload differ in a few low bits); histograms and scatters on all host threads
 // (per-thread ranges in order keep it stable). o / keys end up pointing at the sorted arrays
 // (either the given ones or the scratch ones, which are swapped with them).
 static void sort_by_shape(PairsHost &hs, uint32_t *&o, uint64_t *&keys, uint32_t *&o_tmp,
                           uint64_t *&k_tmp, size_t n) {
     if (n < 2) return;
-    const unsigned nt = host_threads(n, 1 << 16);
+    const unsigned nt = host_threads(n, 1 << 14);
     const uint64_t per = (n + nt - 1) / nt;
     if (hs.count.size() < nt) hs.count.resize(nt);
-    for (unsigned t = 0; t < nt; ++t) hs.count[t].resize(1 << 16);
+    for (unsigned t = 0; t < nt; ++t) hs.count[t].resize(256);
     // Bits in which some key differs from the first: digits without any are skipped.
     std::vector<uint64_t> diff(nt, 0);
     parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
@@ -356,18 +368,18 @@ static void sort_by_shape(PairsHost &hs, uint32_t *&o, uint64_t *&keys, uint32_t
     });
     uint64_t varies = 0;
     for (uint64_t x : diff) varies |= x;
-    for (int shift = 0; shift < 64; shift += 16) {
-        if (((varies >> shift) & 0xffff) == 0) continue;
+    for (int shift = 0; shift < 64; shift += 8) {
+        if (((varies >> shift) & 0xff) == 0) continue;
         parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
             for (uint64_t t = ta; t < te; ++t) {
                 std::vector<uint64_t> &c = hs.count[t];
                 std::fill(c.begin(), c.end(), 0);
                 for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i)
-                    ++c[(keys[i] >> shift) & 0xffff];
+                    ++c[(keys[i] >> shift) & 0xff];
             }
         });
         uint64_t sum = 0;
-        for (size_t d = 0; d < (1u << 16); ++d)
+        for (size_t d = 0; d < 256; ++d)
             for (unsigned t = 0; t < nt; ++t) {
                 const uint64_t c = hs.count[t][d];
                 hs.count[t][d] = sum;
@@ -377,7 +389,7 @@ static void sort_by_shape(PairsHost &hs, uint32_t *&o, uint64_t *&keys, uint32_t
             for (uint64_t t = ta; t < te; ++t) {
                 std::vector<uint64_t> &c = hs.count[t];
                 for (uint64_t i = t * per; i < std::min<uint64_t>(n, (t + 1) * per); ++i) {
-                    const uint64_t dst = c[(keys[i] >> shift) & 0xffff]++;
+                    const uint64_t dst = c[(keys[i] >> shift) & 0xff]++;
                     o_tmp[dst] = o[i];
                     k_tmp[dst] = keys[i];
                 }
@@ -403,7 +415,7 @@ static size_t pack_items(PairsHost &hs, const uint32_t *order, const uint64_t *k
         i += (two && i + 1 < n && key_qlen(keys[i + 1]) == key_qlen(keys[i])) ? 2 : 1;
     }
     start[n_items] = (uint32_t)n;
-    const unsigned nt = host_threads(n_items, 1 << 15);
+    const unsigned nt = host_threads(n_items, 1 << 14);
     const uint64_t per = (n_items + nt - 1) / nt;
     std::vector<uint64_t> part(nt + 1, 0);
     parallel_for(nt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
@@ -453,7 +465,7 @@ static hy_status run_items(PairsContext &ctx, PairParams p, int res_slot, int bn
         pack_items_kernel<A><<<blocks, 256, 0, ctx.stream>>>(
             p.meta, (uint32_t)ib, (uint32_t)(ib + n_items), cols, d_qoff, d_toff, d_q, d_t,
             (typename A::RES *)d_res, const_cast<uint32_t *>(p.qlen), const_cast<uint64_t *>(p.qoff),
-            (uint32_t)p.al, d_bad);
+            const_cast<uint64_t *>(p.toff), (uint32_t)p.al, d_bad);
         HY_CK(cudaGetLastError());
     }
     // Rows per lane of each run of equal query lengths.
@@ -507,13 +519,35 @@ static hy_status run_items(PairsContext &ctx, PairParams p, int res_slot, int bn
     return fail(HY_OK);
 }
 
-}  // namespace hy
+// align_pair_position_max's BestHit and score2 for pairs [0, n) from their column maxima at
+// colmax + t_off[k] (position_hits). One thread per pair.
+__global__ void pos_hits_kernel(uint64_t n, const uint64_t *t_off, const int32_t *colmax, int32_t *scores,
+                                int32_t *tend, int32_t matrix_max, int32_t min_score, int32_t *s2) {
+    const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    position_hits(colmax + t_off[k], (uint32_t)(t_off[k + 1] - t_off[k]), matrix_max, min_score, scores + k,
+                  tend + k, s2 ? s2 + 2 * k : nullptr);
+}
 
-extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
-                                    const uint8_t *t_res, const uint64_t *t_off, uint64_t n_pairs,
-                                    const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
-                                    int32_t gap_ext, hy_mode mode, hy_search_type search_type,
-                                    hy_hit *out, uint64_t *failed_pair) {
+// What a call computes besides align_pairs' hits: align_pair_position_max (posmax: SW, score only,
+// the column maxima, each pair's BestHit from them and, with score2, its score2).
+struct PairsCall {
+    bool posmax = false;
+    int32_t *colmax = nullptr;  // host, at t_off[k] - t_off[0] (null: not copied)
+    int32_t min_score = 0;
+    int32_t *score2 = nullptr;  // host, {score, position} per pair (null: not computed)
+};
+
+struct PosTiming {
+    double kernel_ms = 0.0, call_ms = 0.0, cells = 0.0;
+};
+static thread_local PosTiming g_pos_timing;
+
+static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                           const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
+                           uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
+                           hy_search_type search_type, hy_hit *out, uint64_t *failed_pair,
+                           const PairsCall &pc) {
     using clock = std::chrono::steady_clock;
     auto since = [](clock::time_point t) {
         return std::chrono::duration<double, std::milli>(clock::now() - t).count();
@@ -616,8 +650,10 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
     ctx.phase_ms[0] = since(t_call);
 
     uint32_t dev_bad = NO_INDEX;  // the first pair whose symbols the device found out of range
-    const bool ends = search_type != HY_SEARCH_SCORE;
+    const bool ends = !pc.posmax && search_type != HY_SEARCH_SCORE;
+    const bool posmax = pc.posmax;
     const int32_t *h_out = nullptr;
+    int32_t *h_cm = nullptr;  // posmax: pinned column maxima, from t_off[0]
     const auto t_pipe = clock::now();
     if (n_len > 0) {
         int dev = 0;
@@ -628,12 +664,13 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             ctx.device = dev;
             HY_CK(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
             HY_CK(cudaStreamCreateWithFlags(&ctx.copy_stream, cudaStreamNonBlocking));
+            HY_CK(cudaStreamCreateWithFlags(&ctx.d2h_stream, cudaStreamNonBlocking));
             for (cudaEvent_t &e : ctx.slot_ev) HY_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
         const uint64_t L = n_len;
         const uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(PAIR_MAX_CHUNKS, L / PAIR_CHUNK_MIN));
         auto chunk_at = [&](uint64_t c) { return L * c / n_chunks; };
-        while (ctx.ev.size() < 2 * n_chunks) {
+        while (ctx.ev.size() < 3 * n_chunks + 2) {
             cudaEvent_t e;
             HY_CK(cudaEventCreate(&e));
             ctx.ev.push_back(e);
@@ -652,12 +689,27 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
         HY_CK(ctx.get(PS_QOFF, sizeof(uint64_t) * (L + 1), &d_qoff));
         HY_CK(ctx.get(PS_TOFF, sizeof(uint64_t) * (L + 1), &d_toff));
         HY_CK(ctx.get(PS_MATRIX, sizeof(int32_t) * alphabet_len * alphabet_len, &d_matrix));
-        HY_CK(ctx.get(PS_OUT, 3 * sizeof(int32_t) * L + sizeof(uint32_t), &d_out));
+        // Scores, query ends, target ends, the first bad pair, then (posmax) score2 pairs.
+        const uint64_t out_words = posmax ? 5 * L + 2 : 3 * L + 1;
+        HY_CK(ctx.get(PS_OUT, sizeof(int32_t) * out_words, &d_out));
         int32_t *d_scores = (int32_t *)d_out, *d_qend = d_scores + L, *d_tend = d_qend + L;
         uint32_t *d_bad = (uint32_t *)(d_tend + L);
+        int32_t *d_s2 = d_tend + L + 2;
+        int32_t *d_colmax = nullptr;
+        if (posmax) {
+            void *cmv;
+            HY_CK(ctx.get(PS_COLMAX, sizeof(int32_t) * t_off[L], &cmv));
+            d_colmax = (int32_t *)cmv;
+            if (pc.colmax && t_off[L] > t_off[0]) {
+                void *hv;
+                HY_CK(ctx.get_pinned(PAIR_SLOTS + 1, sizeof(int32_t) * (t_off[L] - t_off[0]), &hv));
+                h_cm = (int32_t *)hv;
+            }
+        }
         PairParams pp[2];
         const int meta_slot[2] = {PS_META16, PS_META32}, qlen_slot[2] = {PS_QLEN16, PS_QLEN32};
         const int iqoff_slot[2] = {PS_IQOFF16, PS_IQOFF32}, res_slot[2] = {PS_RES16, PS_RES32};
+        const int itoff_slot[2] = {PS_ITOFF16, PS_ITOFF32};
         for (int h = 0; h < 2; ++h) {
             PairParams &p = pp[h];
             p = PairParams{};
@@ -681,6 +733,12 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             p.scores = d_scores;
             p.qend = d_qend;
             p.tend = d_tend;
+            if (posmax) {
+                void *to;
+                HY_CK(ctx.get(itoff_slot[h], 2 * sizeof(uint64_t) * n_part[h], &to));
+                p.toff = (const uint64_t *)to;
+                p.colmax = d_colmax;
+            }
         }
         void *slots[PAIR_SLOTS];
         for (int s = 0; s < PAIR_SLOTS && s < (int)n_chunks; ++s) HY_CK(ctx.get_pinned(s, slot_bytes, &slots[s]));
@@ -702,7 +760,7 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             k_tmp[0] = hs.keys_tmp.get(n);
             size_t cnt[2] = {0, 0};
             {
-                const unsigned pt = host_threads(n, 1 << 15);
+                const unsigned pt = host_threads(n, 1 << 14);
                 const uint64_t per = (n + pt - 1) / pt;
                 std::vector<uint64_t> at(2 * (pt + 1), 0);
                 parallel_for(pt, 1, [&](uint64_t ta, uint64_t te, unsigned) {
@@ -755,7 +813,7 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
             }
             ctx.phase_ms[1] += since(t0);
             t0 = clock::now();
-            parallel_for(qb + tb, 1 << 24, [&](uint64_t x0, uint64_t x1, unsigned) {
+            parallel_for(qb + tb, 1 << 20, [&](uint64_t x0, uint64_t x1, unsigned) {
                 if (x0 < qb) memcpy(slot + x0, q_res + q_off[a] + x0, std::min(x1, qb) - x0);
                 if (x1 > qb) {
                     const uint64_t y0 = std::max(x0, qb);
@@ -776,6 +834,7 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                                           sizeof(ItemMeta) * n_items[h], cudaMemcpyHostToDevice, cs));
             HY_CK(cudaEventRecord(ctx.slot_ev[s], cs));
             HY_CK(cudaStreamWaitEvent(ctx.stream, ctx.slot_ev[s], 0));
+            if (posmax && tb) HY_CK(cudaMemsetAsync(d_colmax + t_off[a], 0, sizeof(int32_t) * tb, ctx.stream));
             HY_CK(cudaEventRecord(ctx.ev[2 * c], ctx.stream));
             st = run_items<Pair16, PAIR_G>(ctx, pp[0], PS_RES16, PS_BND16, qlen[0], ib[0], n_items[0], cols[0],
                                            (const uint64_t *)d_qoff, (const uint64_t *)d_toff, (uint8_t *)d_q,
@@ -786,24 +845,73 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                                              (const uint8_t *)d_t, d_bad, mode, ends);
             if (st != HY_OK) return st;
             HY_CK(cudaEventRecord(ctx.ev[2 * c + 1], ctx.stream));
+            if (h_cm && tb) {
+                // This chunk's column maxima back while the next chunks run (a long pair's are
+                // copied again once the stripe kernel has written them).
+                HY_CK(cudaStreamWaitEvent(ctx.d2h_stream, ctx.ev[2 * c + 1], 0));
+                HY_CK(cudaMemcpyAsync(h_cm + (t_off[a] - t_off[0]), d_colmax + t_off[a], sizeof(int32_t) * tb,
+                                      cudaMemcpyDeviceToHost, ctx.d2h_stream));
+            }
+            HY_CK(cudaEventRecord(ctx.ev[2 * n_chunks + c], ctx.d2h_stream));
             ib[0] += n_items[0];
             ib[1] += n_items[1];
         }
         // The long pairs, once every chunk's queries are on the device (the compute stream has
         // waited for each chunk's copies).
         if (!run_long.empty()) {
+            const TbColmaxOut cmx{d_colmax, pc.score2 ? d_s2 : nullptr, max_e, pc.min_score};
             st = tb_long_pair_scores(q_res, q_off, t_res, t_off, run_long, (const uint8_t *)d_q,
                                      (const int32_t *)d_matrix, alphabet_len, gap_open, gap_ext, mode,
-                                     ctx.stream, d_scores, d_qend, d_tend, &ctx.kernel_ms);
+                                     ctx.stream, d_scores, d_qend, d_tend, &ctx.kernel_ms,
+                                     posmax ? &cmx : nullptr);
             if (st != HY_OK) return st;
         }
+        if (posmax) {
+            // Every pair's BestHit (and score2) from its column maxima.
+            HY_CK(cudaEventRecord(ctx.ev[3 * n_chunks], ctx.stream));
+            pos_hits_kernel<<<(unsigned)((L + 127) / 128), 128, 0, ctx.stream>>>(
+                L, (const uint64_t *)d_toff, d_colmax, d_scores, d_tend, max_e, pc.min_score,
+                pc.score2 ? d_s2 : nullptr);
+            HY_CK(cudaGetLastError());
+            HY_CK(cudaEventRecord(ctx.ev[3 * n_chunks + 1], ctx.stream));
+            if (h_cm && !run_long.empty()) {
+                // The long pairs' maxima over the zeros their chunks copied back.
+                HY_CK(cudaStreamWaitEvent(ctx.stream, ctx.ev[2 * n_chunks + n_chunks - 1], 0));
+                for (uint32_t k : run_long)
+                    if (t_off[k + 1] > t_off[k])
+                        HY_CK(cudaMemcpyAsync(h_cm + (t_off[k] - t_off[0]), d_colmax + t_off[k],
+                                              sizeof(int32_t) * (t_off[k + 1] - t_off[k]),
+                                              cudaMemcpyDeviceToHost, ctx.stream));
+            }
+        }
         void *h_stage = nullptr;
-        HY_CK(ctx.get_pinned(PAIR_SLOTS, 3 * sizeof(int32_t) * L + sizeof(uint32_t), &h_stage));
-        HY_CK(cudaMemcpyAsync(h_stage, d_out, 3 * sizeof(int32_t) * L + sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.stream));
+        HY_CK(ctx.get_pinned(PAIR_SLOTS, sizeof(int32_t) * out_words, &h_stage));
+        HY_CK(cudaMemcpyAsync(h_stage, d_out, sizeof(int32_t) * out_words, cudaMemcpyDeviceToHost, ctx.stream));
+        if (h_cm) {
+            // Chunks' column maxima into the caller's array as they arrive.
+            for (uint64_t c = 0; c < n_chunks; ++c) {
+                HY_CK(cudaEventSynchronize(ctx.ev[2 * n_chunks + c]));
+                const auto tc = clock::now();
+                const uint64_t x0 = t_off[chunk_at(c)] - t_off[0], x1 = t_off[chunk_at(c + 1)] - t_off[0];
+                parallel_for(x1 - x0, 1 << 18, [&](uint64_t e0, uint64_t e1, unsigned) {
+                    memcpy(pc.colmax + x0 + e0, h_cm + x0 + e0, sizeof(int32_t) * (e1 - e0));
+                });
+                ctx.phase_ms[6] += since(tc);
+            }
+        }
         HY_CK(cudaStreamSynchronize(ctx.stream));
+        if (h_cm)
+            for (uint32_t k : run_long)
+                memcpy(pc.colmax + (t_off[k] - t_off[0]), h_cm + (t_off[k] - t_off[0]),
+                       sizeof(int32_t) * (t_off[k + 1] - t_off[k]));
         for (uint64_t c = 0; c < n_chunks; ++c) {
             float ms = 0.0f;
             HY_CK(cudaEventElapsedTime(&ms, ctx.ev[2 * c], ctx.ev[2 * c + 1]));
+            ctx.kernel_ms += ms;
+        }
+        if (posmax) {
+            float ms = 0.0f;
+            HY_CK(cudaEventElapsedTime(&ms, ctx.ev[3 * n_chunks], ctx.ev[3 * n_chunks + 1]));
             ctx.kernel_ms += ms;
         }
         h_out = (const int32_t *)h_stage;
@@ -839,13 +947,63 @@ extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
                 out[k].reserved = 0;
                 out[k].db_index = k;
                 out[k].query_end = ends ? (int64_t)h[L + k] : -1;
-                out[k].target_end = ends ? (int64_t)h[2 * L + k] : -1;
+                out[k].target_end = (ends || posmax) ? (int64_t)h[2 * L + k] : -1;
+                if (posmax && pc.score2) {
+                    pc.score2[2 * k] = h[3 * L + 2 + 2 * k];
+                    pc.score2[2 * k + 1] = h[3 * L + 2 + 2 * k + 1];
+                }
             }
         });
     }
+    // Positions of the pairs from the failing one on are left at 0.
+    if (h_cm && n_ok < n_len)
+        memset(pc.colmax + (t_off[n_ok] - t_off[0]), 0, sizeof(int32_t) * (t_off[n_len] - t_off[n_ok]));
     ctx.phase_ms[4] = since(t_res_fill);
     ctx.call_ms = since(t_call);
+    if (posmax) {
+        g_pos_timing.kernel_ms = ctx.kernel_ms;
+        g_pos_timing.call_ms = ctx.call_ms;
+        double cells = 0.0;
+        for (uint64_t k = 0; k < n_ok; ++k)
+            cells += (double)(q_off[k + 1] - q_off[k]) * (double)(t_off[k + 1] - t_off[k]);
+        g_pos_timing.cells = cells;
+    }
     return fail(first, d[0], d[1], d[2]);
+}
+
+}  // namespace hy
+
+extern "C" hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off,
+                                    const uint8_t *t_res, const uint64_t *t_off, uint64_t n_pairs,
+                                    const int32_t *matrix, uint64_t alphabet_len, int32_t gap_open,
+                                    int32_t gap_ext, hy_mode mode, hy_search_type search_type,
+                                    hy_hit *out, uint64_t *failed_pair) {
+    return pairs_run(q_res, q_off, t_res, t_off, n_pairs, matrix, alphabet_len, gap_open, gap_ext, mode,
+                     search_type, out, failed_pair, PairsCall{});
+}
+
+extern "C" hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_off,
+                                                 const uint8_t *t_res, const uint64_t *t_off,
+                                                 uint64_t n_pairs, const int32_t *matrix,
+                                                 uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
+                                                 int32_t *colmax, hy_hit *out, int32_t min_score,
+                                                 int32_t *score2, uint64_t *failed_pair) {
+    g_pos_timing = PosTiming{};
+    PairsCall pc;
+    pc.posmax = true;
+    pc.colmax = colmax;
+    pc.min_score = min_score;
+    pc.score2 = score2;
+    return pairs_run(q_res, q_off, t_res, t_off, n_pairs, matrix, alphabet_len, gap_open, gap_ext, HY_MODE_SW,
+                     HY_SEARCH_SCORE, out, failed_pair, pc);
+}
+
+extern "C" hy_status hy_position_max_timing(double out[3]) {
+    if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
+    out[0] = g_pos_timing.kernel_ms;
+    out[1] = g_pos_timing.call_ms;
+    out[2] = g_pos_timing.cells;
+    return fail(HY_OK);
 }
 
 extern "C" hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms) {
@@ -856,6 +1014,6 @@ extern "C" hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms) {
 
 extern "C" hy_status hy_align_pairs_phases(double *ms, uint32_t n) {
     if (!ms && n) return fail(HY_ERR_INVALID_ARGUMENT);
-    for (uint32_t i = 0; i < n && i < 6; ++i) ms[i] = g_ctx.phase_ms[i];
+    for (uint32_t i = 0; i < n && i < 7; ++i) ms[i] = g_ctx.phase_ms[i];
     return fail(HY_OK);
 }

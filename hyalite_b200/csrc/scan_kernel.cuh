@@ -344,6 +344,15 @@ struct Sweep {
     // the first strict improvement is the smallest (column, row).
     typename A::V pbest;
     int32_t pid0, pid1;
+    typename A::V botM;  // column maxima (COLMAX): G maximum of this column down to this lane's rows
+};
+
+// Where a COLMAX sweep writes its column maxima: per half, the pair's array indexed by target
+// position (H of the column's best cell, so >= 0 in local mode); `atomic` when several passes
+// combine into one array.
+struct ColMaxOut {
+    int32_t *p[2];
+    bool atomic;
 };
 
 template <class A, int R, int MODE>
@@ -378,7 +387,7 @@ struct SweepConst {
 // caller runs unchecked steps only where every lane of the warp is live.
 // With PRE the step's residue code and (lane 0) boundary-row values come from the caller, which
 // loaded them one step ahead.
-template <class A, int G, int R, int MODE, bool ENDS, bool CHECKED, bool PRE = false>
+template <class A, int G, int R, int MODE, bool ENDS, bool CHECKED, bool PRE = false, bool COLMAX = false>
 __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const int lane,
                                            const int32_t w, const uint32_t (&n)[2],
                                            const typename A::RES *__restrict__ res,
@@ -388,14 +397,22 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                                            const int32_t qlen, const int32_t go, const int32_t ge,
                                            const SweepConst<A> &k, typename A::V &best,
                                            Cand (&cand)[2], const typename A::RES pre_r = 0,
-                                           const typename A::V pre_g = 0, const typename A::V pre_f = 0) {
+                                           const typename A::V pre_g = 0, const typename A::V pre_f = 0,
+                                           const ColMaxOut *cmo = nullptr) {
     typedef typename A::V V;
     typedef ModeFlags<MODE> Fl;
+    static_assert(!COLMAX || (Fl::local && !ENDS), "column maxima are a local score-only sweep");
     const V negge = k.negge, neggo = k.neggo;
     {
         const int32_t j = s - lane + 1;
         V upG = __shfl_up_sync(0xffffffffu, sw.botG, 1, G);
         V upF = __shfl_up_sync(0xffffffffu, sw.botF, 1, G);
+        // COLMAX: the column's maximum over the rows of the lanes above (lane 0: none this pass).
+        V upM;
+        if constexpr (COLMAX) {
+            upM = __shfl_up_sync(0xffffffffu, sw.botM, 1, G);
+            if (lane == 0) upM = neggo;
+        }
         const bool live = !CHECKED || (j >= 1 && j <= w);
         if (lane == 0) {
             if (first_pass) {
@@ -412,6 +429,8 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
             V pa[A::EPV], pb[A::EPV];
             V g_up = upG, f = upF, gd = sw.diag, hprev = A::splat(0), hlast = A::splat(0);
             V xprev = A::splat(0);
+            V cm;  // COLMAX: this column's G maximum, down to this lane's rows
+            if constexpr (COLMAX) cm = upM;
             const int32_t jR = j * R;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -447,6 +466,11 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                         sw.pbest = A::bmax(sw.pbest, h, u0, u1);
                         if (u0) sw.pid0 = jR + r;
                         if (u1) sw.pid1 = jR + r;
+                    } else if (COLMAX) {
+                        if (r & 1)
+                            cm = A::vmax3(cm, hprev, h);
+                        else
+                            hprev = h;
                     } else {
                         if (r & 1)
                             best = A::vmax3(best, hprev, h);
@@ -456,7 +480,28 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                 }
                 if (r == R - 1) hlast = h;
             }
-            if (Fl::local && !ENDS && (R & 1)) best = A::vmax(best, hprev);
+            if (Fl::local && !ENDS && (R & 1)) {
+                if (COLMAX)
+                    cm = A::vmax(cm, hprev);
+                else
+                    best = A::vmax(best, hprev);
+            }
+            if constexpr (COLMAX) {
+                // The last lane holds the column's maximum over the pass: H = G + go.
+                sw.botM = cm;
+                if (lane == G - 1) {
+#pragma unroll
+                    for (int h = 0; h < A::NH; ++h) {
+                        if (j <= (int32_t)n[h]) {
+                            const int32_t v = A::get(cm, h) + go;
+                            if (cmo->atomic)
+                                atomicMax(cmo->p[h] + (j - 1), v);
+                            else
+                                cmo->p[h][j - 1] = v;
+                        }
+                    }
+                }
+            }
             sw.botG = g_up;
             sw.botF = f;
             sw.diag = upG;
@@ -493,7 +538,7 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
 // With PREFETCH the unchecked steps load the next step's residue code and boundary-row values one
 // step ahead; only for callers whose boundary row was written by an earlier, completed pass (the
 // band kernel's warps read rows another warp is writing and keep their exact read timing).
-template <class A, int G, int R, int MODE, bool ENDS, bool PREFETCH = false>
+template <class A, int G, int R, int MODE, bool ENDS, bool PREFETCH = false, bool COLMAX = false>
 __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, const int s_end,
                                           const int w_min, const int lane, const int32_t w,
                                           const uint32_t (&n)[2],
@@ -503,7 +548,7 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
                                           const bool last_pass, typename A::V *bnd,
                                           const int32_t qlen, const int32_t go, const int32_t ge,
                                           const typename A::V Sv, typename A::V &best,
-                                          Cand (&cand)[2]) {
+                                          Cand (&cand)[2], const ColMaxOut *cmo = nullptr) {
     SweepConst<A> k;
     k.negge = A::splat(-(int64_t)ge);
     k.neggo = A::splat(-(int64_t)go);
@@ -513,8 +558,9 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
     const int fast_hi = max(fast_lo, min(s_end, w_min));
     const int head_end = min(s_end, fast_lo);
     for (int s = s_begin; s < head_end; ++s)
-        sweep_step<A, G, R, MODE, ENDS, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
-                                              first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+        sweep_step<A, G, R, MODE, ENDS, true, false, COLMAX>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                                             first_pass, last_pass, bnd, qlen, go, ge, k,
+                                                             best, cand, 0, 0, 0, cmo);
     if (PREFETCH && fast_lo < fast_hi) {
         typedef typename A::V V;
         // Every lane of the warp is inside its item in [fast_lo, fast_hi): the indices below
@@ -533,21 +579,24 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
                 g_next = bnd[2 * (sn - lane)];
                 f_next = bnd[2 * (sn - lane) + 1];
             }
-            sweep_step<A, G, R, MODE, ENDS, false, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
-                                                         first_pass, last_pass, bnd, qlen, go, ge, k,
-                                                         best, cand, r_cur, g_cur, f_cur);
+            sweep_step<A, G, R, MODE, ENDS, false, true, COLMAX>(sw, s, lane, w, n, res, prof_a, prof_b,
+                                                                 row0, first_pass, last_pass, bnd, qlen,
+                                                                 go, ge, k, best, cand, r_cur, g_cur,
+                                                                 f_cur, cmo);
             r_cur = r_next;
             g_cur = g_next;
             f_cur = f_next;
         }
     } else {
         for (int s = fast_lo; s < fast_hi; ++s)
-            sweep_step<A, G, R, MODE, ENDS, false>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
-                                                   first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+            sweep_step<A, G, R, MODE, ENDS, false, false, COLMAX>(sw, s, lane, w, n, res, prof_a, prof_b,
+                                                                  row0, first_pass, last_pass, bnd, qlen,
+                                                                  go, ge, k, best, cand, 0, 0, 0, cmo);
     }
     for (int s = max(fast_hi, head_end); s < s_end; ++s)
-        sweep_step<A, G, R, MODE, ENDS, true>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
-                                              first_pass, last_pass, bnd, qlen, go, ge, k, best, cand);
+        sweep_step<A, G, R, MODE, ENDS, true, false, COLMAX>(sw, s, lane, w, n, res, prof_a, prof_b, row0,
+                                                             first_pass, last_pass, bnd, qlen, go, ge, k,
+                                                             best, cand, 0, 0, 0, cmo);
 }
 
 template <class A, int R, int MODE, bool ENDS>
@@ -559,7 +608,7 @@ __device__ __forceinline__ void sweep_end(const Sweep<A, R> &sw, const int32_t r
 }
 
 // One whole pass: begin, every step, end.
-template <class A, int G, int R, int MODE, bool ENDS>
+template <class A, int G, int R, int MODE, bool ENDS, bool COLMAX = false>
 __device__ __forceinline__ void sweep_pass(const int lane, const int steps, const int w_min,
                                            const int32_t w, const uint32_t (&n)[2],
                                            const typename A::RES *__restrict__ res,
@@ -568,11 +617,13 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
                                            const bool last_pass, typename A::V *bnd,
                                            const int32_t qlen, const int32_t go, const int32_t ge,
                                            const typename A::V Sv, typename A::V &best,
-                                           Cand (&cand)[2]) {
+                                           Cand (&cand)[2], const ColMaxOut *cmo = nullptr) {
     Sweep<A, R> sw;
     sweep_begin<A, R, MODE>(sw, row0, go, ge, Sv);
-    sweep_run<A, G, R, MODE, ENDS, true>(sw, 0, steps, w_min, lane, w, n, res, prof_a, prof_b, row0,
-                                   first_pass, last_pass, bnd, qlen, go, ge, Sv, best, cand);
+    if constexpr (COLMAX) sw.botM = A::splat(-(int64_t)go);
+    sweep_run<A, G, R, MODE, ENDS, true, COLMAX>(sw, 0, steps, w_min, lane, w, n, res, prof_a, prof_b,
+                                                 row0, first_pass, last_pass, bnd, qlen, go, ge, Sv,
+                                                 best, cand, cmo);
     sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
 }
 
@@ -899,6 +950,10 @@ struct PairParams {
     // group g of block b builds and reads its profile at gprof + (b * groups_per_block + g) *
     // group_bytes.
     uint8_t *gprof;
+    // Column-maxima form (align_pair_position_max): pair half h of item i writes the maximum of H
+    // over each target column to colmax + toff[2 * i + h] + column.
+    int32_t *colmax;
+    const uint64_t *toff;
 };
 
 template <class A, int G, int R>
@@ -933,7 +988,7 @@ __device__ __forceinline__ void build_group_profile(uint8_t *dst, const uint8_t 
     }
 }
 
-template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false>
+template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false, bool COLMAX = false>
 __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     typedef typename A::V V;
     constexpr int RPP = G * R;
@@ -967,6 +1022,15 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
     const int32_t pmax = (int32_t)__reduce_max_sync(0xffffffffu, (uint32_t)n_passes);
+    ColMaxOut cmo;
+    if constexpr (COLMAX) {
+        cmo.p[0] = cmo.p[1] = p.colmax;
+        if (active) {
+            cmo.p[0] = p.colmax + p.toff[2 * (size_t)item];
+            cmo.p[1] = p.colmax + p.toff[2 * (size_t)item + 1];
+        }
+        cmo.atomic = n_passes > 1;
+    }
 
     V best = A::splat(ModeFlags<MODE>::local && !ENDS ? -(int64_t)p.go : 0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
@@ -984,13 +1048,15 @@ __global__ void __launch_bounds__(256) pairs_kernel(const PairParams p) {
         // `steps` stays warp-uniform; a group past its last pass sweeps zero columns.
         const int w_here = mine ? (int)meta.w : 0;
         const int w_min = (int)__reduce_min_sync(0xffffffffu, (uint32_t)w_here);
-        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, w_here, meta.n,
-                                        res, gprof_a, gprof_b, row_base + lane * R, pass == 0,
-                                        pass == n_passes - 1, bnd, qlen, p.go, p.ge, Sv, best, cand);
+        sweep_pass<A, G, R, MODE, ENDS, COLMAX>(lane, steps, w_min, w_here, meta.n, res, gprof_a,
+                                                gprof_b, row_base + lane * R, pass == 0,
+                                                pass == n_passes - 1, bnd, qlen, p.go, p.ge, Sv, best,
+                                                cand, COLMAX ? &cmo : nullptr);
         __syncwarp();
     }
-    finish_item<A, G, MODE, ENDS>(lane, active, meta, qlen, p.go, p.ge, best, cand, p.scores,
-                                  p.qend, p.tend, nullptr);
+    if constexpr (!COLMAX)
+        finish_item<A, G, MODE, ENDS>(lane, active, meta, qlen, p.go, p.ge, best, cand, p.scores,
+                                      p.qend, p.tend, nullptr);
 }
 
 // ---- query profile ----------------------------------------------------------------------------

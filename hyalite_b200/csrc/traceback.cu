@@ -459,82 +459,15 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_fill_kernel(TbParams P) {
     tb_write_end<MODE>(P.ends + pr.ends_off, lane, bs, brow, bcol);
 }
 
-// align_pair_position_max over many pairs (src/kernel.rs:474-553): one warp per pair, SW, score
-// only, every column's maximum of H max-reduced into P.colmax.
-template <int R>
-__global__ void __launch_bounds__(TB_BLOCK) tb_colmax_kernel(TbParams P) {
-    const uint32_t warp = (blockIdx.x * TB_BLOCK + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= P.n_pairs) return;
-    const TbPair pr = P.pairs[warp];
-    const int m = (int)pr.m, n = (int)pr.n;
-    if (m == 0 || n == 0) return;
-    int2 *B = P.bnd + pr.bnd_off;
-    for (int j = lane; j <= n; j += 32) B[j] = make_int2(0, TB_NEG);  // SW row 0
-    __syncwarp();
-    const int passes = (m + 32 * R - 1) / (32 * R);
-    int32_t bs = 0;
-    uint32_t brow = 0, bcol = 0;
-    for (int p = 0; p < passes; ++p) {
-        const TbRows rows{B, p + 1 < passes ? B : nullptr, nullptr, nullptr, nullptr};
-        tb_pass<R, MODE_SW, TB_COLMAX>(P, pr, p, passes, lane, rows, bs, brow, bcol);
-    }
-}
-
-// From each pair's column maxima: the BestHit of align_pair_position_max (score = the maximum,
-// target_end = its first position, None when the score is 0; src/kernel.rs:541-553) and, when
-// asked, bwa's score2 with that best and target end (None: position 0) (src/kernel.rs:741-792):
-// peaks of contiguous columns >= min_score collapsed to their maximum (contiguity checked against
-// the last kept maximum's position), the highest peak outside [te - w, te + w] with
-// w = ceil(score / matrix_max), ties to the smallest position. One thread per pair.
+// From each pair's column maxima (at its ops_off): its BestHit and, with s2, its score2
+// (position_hits). One thread per pair.
 __global__ void tb_position_hits_kernel(TbParams P, int32_t *scores, int32_t *tend, int32_t matrix_max,
                                         int32_t min_score, int32_t *s2) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= P.n_pairs) return;
     const TbPair pr = P.pairs[t];
-    const int32_t *cm = P.colmax + pr.ops_off;
-    int32_t best = 0;
-    int64_t te = -1;
-    for (uint32_t x = 0; x < pr.n; ++x)
-        if (cm[x] > best) {
-            best = cm[x];
-            te = x;
-        }
-    scores[pr.slot] = best;
-    tend[pr.slot] = (int32_t)te;
-    if (!s2) return;
-    int32_t s2_score = -1;
-    int64_t s2_pos = -1;
-    if (matrix_max > 0) {
-        const int64_t w = ((int64_t)best + matrix_max - 1) / matrix_max;
-        const int64_t c = te < 0 ? 0 : te;
-        const int64_t low = c - w, high = c + w;
-        auto consider = [&](int32_t score, int64_t pos) {
-            if ((pos < low || pos > high) && (s2_pos < 0 || score > s2_score)) {
-                s2_score = score;
-                s2_pos = pos;
-            }
-        };
-        int32_t cs = 0;
-        int64_t cp = -1;  // the open peak (score, position), none while cp < 0
-        for (uint32_t x = 0; x < pr.n; ++x) {
-            const int32_t v = cm[x];
-            if (v < min_score) continue;
-            if (cp >= 0 && cp + 1 == (int64_t)x) {
-                if (cs < v) {
-                    cs = v;
-                    cp = x;
-                }
-            } else {
-                if (cp >= 0) consider(cs, cp);
-                cs = v;
-                cp = x;
-            }
-        }
-        if (cp >= 0) consider(cs, cp);
-    }
-    s2[2 * pr.slot] = s2_pos < 0 ? 0 : s2_score;
-    s2[2 * pr.slot + 1] = (int32_t)s2_pos;
+    position_hits(P.colmax + pr.ops_off, pr.n, matrix_max, min_score, scores + pr.slot, tend + pr.slot,
+                  s2 ? s2 + 2 * (uint64_t)pr.slot : nullptr);
 }
 
 // Latency form for few long pairs: every pass (stripe) of every pair on its own warp, all warps
@@ -1392,7 +1325,7 @@ hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const
                               const uint64_t *t_off, const std::vector<uint32_t> &idx, const uint8_t *d_q,
                               const int32_t *d_matrix, uint64_t al, int32_t go, int32_t ge, int mode,
                               cudaStream_t stream, int32_t *d_scores, int32_t *d_qend, int32_t *d_tend,
-                              double *kernel_ms) {
+                              double *kernel_ms, const TbColmaxOut *cmx) {
     (void)q_res;
     const uint32_t n = (uint32_t)idx.size();
     if (n == 0) return fail(HY_OK);
@@ -1436,7 +1369,7 @@ hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const
         pp.t_off = t_total;
         pp.dir_off = 0;
         pp.bnd_off = bnd_total;
-        pp.ops_off = 0;
+        pp.ops_off = cmx ? t_off[k] : 0;  // column maxima at the pair's target offset
         pp.ends_off = n_str;
         pp.n_ends = S;
         pp.slot = k;
@@ -1486,15 +1419,24 @@ hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const
     p.go = go;
     p.ge = ge;
     TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
-    TB_CK(cudaEventRecord(ctx.ev[0], stream));
-    TB_CK(dispatch_stripes(mode, false, p, S, stream, dev));
-    TB_CK(cudaEventRecord(ctx.ev[1], stream));
-    switch (mode) {
-    case MODE_SW: tb_pair_hits_kernel<MODE_SW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
-    case MODE_NW: tb_pair_hits_kernel<MODE_NW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
-    case MODE_HW: tb_pair_hits_kernel<MODE_HW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
-    case MODE_OV: tb_pair_hits_kernel<MODE_OV><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
-    default: tb_pair_hits_kernel<MODE_SHW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+    if (cmx) {
+        p.colmax = cmx->colmax;
+        TB_CK(cudaEventRecord(ctx.ev[0], stream));
+        TB_CK((launch_stripes<MODE_SW, TB_COLMAX>(p, S, stream, dev)));
+        TB_CK(cudaEventRecord(ctx.ev[1], stream));
+        tb_position_hits_kernel<<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_tend, cmx->matrix_max,
+                                                                  cmx->min_score, cmx->s2);
+    } else {
+        TB_CK(cudaEventRecord(ctx.ev[0], stream));
+        TB_CK(dispatch_stripes(mode, false, p, S, stream, dev));
+        TB_CK(cudaEventRecord(ctx.ev[1], stream));
+        switch (mode) {
+        case MODE_SW: tb_pair_hits_kernel<MODE_SW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+        case MODE_NW: tb_pair_hits_kernel<MODE_NW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+        case MODE_HW: tb_pair_hits_kernel<MODE_HW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+        case MODE_OV: tb_pair_hits_kernel<MODE_OV><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+        default: tb_pair_hits_kernel<MODE_SHW><<<(n + 63) / 64, 64, 0, stream>>>(p, d_scores, d_qend, d_tend); break;
+        }
     }
     TB_CK(cudaGetLastError());
     TB_CK(grow_pinned(ctx.h_total, ctx.ch_total, 16));
@@ -1526,33 +1468,10 @@ uint64_t tb_context_launches(void *ctx) {
 
 }  // namespace hy
 
-// ---- align_pair_position_max / score2 (src/kernel.rs:454-553, 741-792) -------------------------
-
-namespace hy {
-
-// Pairs per launch of the position-max kernels (bounds the profile and boundary scratch).
-constexpr uint32_t POS_CHUNK_PAIRS = 1u << 16;
-
-// Profiles of many pairs' queries: block x builds pair x's (al x m_pad) table.
-__global__ void tb_profile_pairs_kernel(const TbPair *pairs, const uint8_t *q_res, const int32_t *matrix,
-                                        uint32_t al, int32_t *prof) {
-    const TbPair pr = pairs[blockIdx.x];
-    const uint64_t total = (uint64_t)al * pr.m_pad;
-    for (uint64_t x = threadIdx.x; x < total; x += blockDim.x) {
-        const uint32_t c = (uint32_t)(x / pr.m_pad), r = (uint32_t)(x - (uint64_t)c * pr.m_pad);
-        prof[pr.prof_off + x] = r < pr.m ? matrix[(uint64_t)q_res[pr.q_off + r] * al + c] : 0;
-    }
-}
-
-template <int R>
-static cudaError_t launch_colmax(const TbParams &p, cudaStream_t st) {
-    tb_colmax_kernel<R><<<(uint32_t)(((uint64_t)p.n_pairs * 32 + TB_BLOCK - 1) / TB_BLOCK), TB_BLOCK, 0, st>>>(p);
-    return cudaGetLastError();
-}
-
-static thread_local std::unique_ptr<TbContext> g_pos_ctx;
-
-}  // namespace hy
+// ---- score2 (src/kernel.rs:741-792) --------------------------------------------------------------
+//
+// align_pair_position_max over many pairs runs in pairs.cu (the pair kernel's column-maxima form);
+// its long pairs take this file's stripe kernel through tb_long_pair_scores.
 
 extern "C" {
 
@@ -1593,277 +1512,6 @@ int hy_score2(const int32_t *colmax, uint64_t n, int32_t best_score, uint64_t be
         if (pos) *pos = bp;
     }
     return have ? 1 : 0;
-}
-
-hy_status hy_position_max_timing(double out[3]) {
-    if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
-    out[0] = g_pos_ctx ? g_pos_ctx->fill_ms : 0.0;
-    out[1] = g_pos_ctx ? g_pos_ctx->call_ms : 0.0;
-    out[2] = g_pos_ctx ? g_pos_ctx->cells : 0.0;
-    return fail(HY_OK);
-}
-
-hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
-                                      const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
-                                      uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,
-                                      int32_t *colmax, hy_hit *out, int32_t min_score, int32_t *score2,
-                                      uint64_t *failed_pair) {
-    const auto t_call = std::chrono::steady_clock::now();
-    if (failed_pair) *failed_pair = n_pairs;
-    hy_status st = validate_scoring(alphabet_len, matrix, alphabet_len * alphabet_len, gap_open, gap_ext);
-    if (st != HY_OK) return st;
-    if (n_pairs == 0) return fail(HY_OK);
-    if (!q_off || !t_off || !out) return fail(HY_ERR_INVALID_ARGUMENT);
-    if (alphabet_len > 255 || n_pairs >= (1ull << 32)) return fail(HY_ERR_UNSUPPORTED);
-    const int32_t min_e = *std::min_element(matrix, matrix + alphabet_len * alphabet_len);
-    const int32_t max_e = *std::max_element(matrix, matrix + alphabet_len * alphabet_len);
-    // Validation in input order (src/kernel.rs:496-511: symbols, then the SW width proof), chunked
-    // over the host threads: each chunk stops at its own first failure, and the call's first
-    // failure is that of the first chunk that has one.
-    const unsigned nt = host_threads(n_pairs, 1 << 15);
-    struct Chunk {
-        uint64_t first_bad = ~0ull;
-        hy_status st = HY_OK;
-        int64_t d[2] = {0, 0};
-    };
-    std::vector<Chunk> chunks(nt);
-    const uint64_t per = (n_pairs + nt - 1) / nt;
-    parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
-        for (uint64_t c = ca; c < ce; ++c) {
-            Chunk &ch = chunks[c];
-            const uint64_t a = c * per, e = std::min(n_pairs, a + per);
-            for (uint64_t k = a; k < e && ch.st == HY_OK; ++k) {
-                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-                for (int side = 0; side < 2 && ch.st == HY_OK; ++side) {
-                    const uint8_t *seq = side == 0 ? q_res + q_off[k] : t_res + t_off[k];
-                    const uint64_t len = side == 0 ? ql : tl;
-                    const int bad = first_bad_symbol(seq, len, alphabet_len);
-                    if (bad >= 0) {
-                        ch.st = HY_ERR_SYMBOL_OUT_OF_RANGE;
-                        ch.d[0] = bad;
-                        ch.d[1] = (int64_t)alphabet_len;
-                    }
-                }
-                if (ch.st == HY_OK) {
-                    const int64_t b = magnitude_bound(MODE_SW, min_e, max_e, gap_open, gap_ext, ql, tl);
-                    if (narrowest_width(b) < 0) {
-                        ch.st = HY_ERR_SCORE_RANGE_TOO_WIDE;
-                        ch.d[0] = b;
-                    } else if (ql >= (1u << 30) || tl >= (1u << 31)) {
-                        ch.st = HY_ERR_UNSUPPORTED;
-                    }
-                }
-                if (ch.st != HY_OK) ch.first_bad = k;
-            }
-        }
-    });
-    uint64_t n_ok = n_pairs;
-    hy_status first = HY_OK;
-    int64_t d[2] = {0, 0};
-    for (const Chunk &ch : chunks)
-        if (ch.st != HY_OK) {
-            first = ch.st;
-            n_ok = ch.first_bad;
-            d[0] = ch.d[0];
-            d[1] = ch.d[1];
-            break;
-        }
-    if (failed_pair && first != HY_OK) *failed_pair = n_ok;
-    if (n_ok > 0) {
-        int dev = 0;
-        TB_CK(cudaGetDevice(&dev));
-        if (g_pos_ctx && g_pos_ctx->device != dev) g_pos_ctx.reset();
-        if (!g_pos_ctx) {
-            g_pos_ctx.reset(new TbContext);
-            g_pos_ctx->device = dev;
-            g_pos_ctx->own_stream = true;
-            TB_CK(cudaStreamCreateWithFlags(&g_pos_ctx->stream, cudaStreamNonBlocking));
-        }
-        TbContext &ctx = *g_pos_ctx;
-        cudaStream_t stream = ctx.stream;
-        while (ctx.ev.size() < 2) {
-            cudaEvent_t e;
-            TB_CK(cudaEventCreate(&e));
-            ctx.ev.push_back(e);
-        }
-        ctx.fill_ms = 0.0;
-        ctx.cells = 0.0;
-        for (uint64_t k = 0; k < n_ok; ++k)
-            ctx.cells += (double)(q_off[k + 1] - q_off[k]) * (double)(t_off[k + 1] - t_off[k]);
-        const uint64_t q0 = q_off[0], t0 = t_off[0];
-        const uint64_t q_bytes = q_off[n_ok] - q0, t_bytes = t_off[n_ok] - t0;
-        TB_CK(grow(ctx.d_q, ctx.c_q, q_bytes));
-        TB_CK(grow(ctx.d_t, ctx.c_t, t_bytes));
-        TB_CK(grow(ctx.d_matrix, ctx.c_matrix, sizeof(int32_t) * alphabet_len * alphabet_len));
-        TB_CK(grow(ctx.d_ops_out, ctx.c_ops_out, sizeof(int32_t) * std::max<uint64_t>(t_bytes, 1)));  // colmax
-        TB_CK(grow(ctx.d_out, ctx.c_out, sizeof(int32_t) * 4 * n_ok));  // score, tend, score2 pairs
-        int32_t *d_colmax = (int32_t *)ctx.d_ops_out;
-        int32_t *d_res = (int32_t *)ctx.d_out;
-        int32_t *d_scores = d_res, *d_tend = d_res + n_ok, *d_s2 = d_res + 2 * n_ok;
-        // Residues in through grow-only pinned staging, filled on all host threads (a pageable
-        // copy of gigabytes runs at a fraction of the link's speed).
-        TB_CK(cudaStreamSynchronize(stream));  // the staging buffers of the previous call are free
-        TB_CK(grow_pinned(ctx.h_q, ctx.ch_q, q_bytes));
-        TB_CK(grow_pinned(ctx.h_ops, ctx.ch_ops, t_bytes));
-        parallel_for(q_bytes + t_bytes, 1 << 24, [&](uint64_t a, uint64_t e, unsigned) {
-            if (a < q_bytes) memcpy(ctx.h_q + a, q_res + q0 + a, std::min(e, q_bytes) - a);
-            if (e > q_bytes) {
-                const uint64_t b = std::max(a, q_bytes);
-                memcpy(ctx.h_ops + (b - q_bytes), t_res + t0 + (b - q_bytes), e - b);
-            }
-        });
-        if (q_bytes) TB_CK(cudaMemcpyAsync(ctx.d_q, ctx.h_q, q_bytes, cudaMemcpyHostToDevice, stream));
-        if (t_bytes) TB_CK(cudaMemcpyAsync(ctx.d_t, ctx.h_ops, t_bytes, cudaMemcpyHostToDevice, stream));
-        TB_CK(cudaMemcpyAsync(ctx.d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
-                              cudaMemcpyHostToDevice, stream));
-        if (t_bytes) TB_CK(cudaMemsetAsync(d_colmax, 0, sizeof(int32_t) * t_bytes, stream));
-        // A few long pairs take the stripe kernel; the rest one warp each, R by the longest query.
-        std::vector<uint32_t> longs, bulk;
-        uint64_t stripes = 0;
-        for (uint64_t k = 0; k < n_ok; ++k) {
-            const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-            if (tb_long_pair(ql, tl)) {
-                longs.push_back((uint32_t)k);
-                stripes += tb_long_pair_stripes(ql);
-            } else {
-                bulk.push_back((uint32_t)k);
-            }
-        }
-        if (stripes > 2048) {
-            bulk.insert(bulk.end(), longs.begin(), longs.end());
-            longs.clear();
-        }
-        uint64_t bulk_max_m = 0, bulk_max_n = 0;
-        for (uint32_t k : bulk) {
-            bulk_max_m = std::max<uint64_t>(bulk_max_m, q_off[k + 1] - q_off[k]);
-            bulk_max_n = std::max<uint64_t>(bulk_max_n, t_off[k + 1] - t_off[k]);
-        }
-        const uint32_t Rb = tb_rows(bulk_max_m, bulk_max_n);
-        auto setup = [&](const std::vector<uint32_t> &ks, uint32_t a, uint32_t b, uint32_t R, bool stripe_form,
-                         uint64_t *prof_total, uint64_t *bnd_total, uint32_t *n_str) -> hy_status {
-            *prof_total = *bnd_total = 0;
-            *n_str = 0;
-            TB_CK(grow_pinned(ctx.h_pairs, ctx.ch_pairs, sizeof(TbPair) * (b - a)));
-            TB_CK(grow_pinned(ctx.h_first, ctx.ch_first, sizeof(uint32_t) * (b - a + 1)));
-            for (uint32_t x = a; x < b; ++x) {
-                const uint32_t k = ks[x];
-                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-                const uint32_t S = (uint32_t)tb_passes(ql, R);
-                TbPair &pp = ctx.h_pairs[x - a];
-                memset(&pp, 0, sizeof(pp));
-                pp.q_off = q_off[k] - q0;
-                pp.t_off = t_off[k] - t0;
-                pp.ops_off = t_off[k] - t0;  // this pair's column maxima
-                pp.m = (uint32_t)ql;
-                pp.n = (uint32_t)tl;
-                pp.m_pad = S * 32 * R;
-                pp.prof_off = *prof_total;
-                pp.bnd_off = *bnd_total;
-                pp.slot = k;
-                pp.rows = R;
-                pp.ends_off = *n_str;
-                pp.n_ends = stripe_form ? S : 1;
-                ctx.h_first[x - a] = *n_str;
-                *prof_total += alphabet_len * pp.m_pad;
-                *bnd_total += stripe_form ? (uint64_t)(S - 1) * (tl + 1) : tl + 1;
-                *n_str += stripe_form ? S : 1;
-            }
-            ctx.h_first[b - a] = *n_str;
-            return fail(HY_OK);
-        };
-        auto run = [&](const std::vector<uint32_t> &ks, uint32_t R, bool stripe_form) -> hy_status {
-            for (uint32_t a = 0; a < (uint32_t)ks.size(); a += POS_CHUNK_PAIRS) {
-                const uint32_t b = (uint32_t)std::min<uint64_t>(ks.size(), (uint64_t)a + POS_CHUNK_PAIRS);
-                uint64_t prof_total, bnd_total;
-                uint32_t n_str;
-                TB_CK(cudaStreamSynchronize(stream));  // the previous chunk is done with the buffers
-                hy_status s2 = setup(ks, a, b, R, stripe_form, &prof_total, &bnd_total, &n_str);
-                if (s2 != HY_OK) return s2;
-                TB_CK(grow(ctx.d_pairs, ctx.c_pairs, sizeof(TbPair) * (b - a)));
-                TB_CK(grow(ctx.d_prof, ctx.c_prof, sizeof(int32_t) * std::max<uint64_t>(prof_total, 1)));
-                TB_CK(grow(ctx.d_bnd, ctx.c_bnd, sizeof(int2) * std::max<uint64_t>(bnd_total, 1)));
-                TB_CK(grow(ctx.d_ends, ctx.c_ends, sizeof(TbEnd) * std::max<uint32_t>(n_str, 1)));
-                TB_CK(cudaMemcpyAsync(ctx.d_pairs, ctx.h_pairs, sizeof(TbPair) * (b - a), cudaMemcpyHostToDevice, stream));
-                TB_CK(cudaEventRecord(ctx.ev[0], stream));
-                tb_profile_pairs_kernel<<<b - a, 256, 0, stream>>>(ctx.d_pairs, ctx.d_q, ctx.d_matrix,
-                                                                  (uint32_t)alphabet_len, ctx.d_prof);
-                TB_CK(cudaGetLastError());
-                TbParams p;
-                memset(&p, 0, sizeof(p));
-                p.pairs = ctx.d_pairs;
-                p.n_pairs = b - a;
-                p.q_res = ctx.d_q;
-                p.t_res = ctx.d_t;
-                p.prof = ctx.d_prof;
-                p.bnd = ctx.d_bnd;
-                p.ends = ctx.d_ends;
-                p.colmax = d_colmax;
-                p.go = gap_open;
-                p.ge = gap_ext;
-                if (stripe_form) {
-                    TB_CK(grow(ctx.d_first, ctx.c_first, sizeof(uint32_t) * (b - a + 1)));
-                    TB_CK(grow(ctx.d_prog, ctx.c_prog, sizeof(uint32_t) * n_str + 16));
-                    TB_CK(cudaMemcpyAsync(ctx.d_first, ctx.h_first, sizeof(uint32_t) * (b - a + 1),
-                                          cudaMemcpyHostToDevice, stream));
-                    TB_CK(cudaMemsetAsync(ctx.d_prog, 0, sizeof(uint32_t) * n_str + 16, stream));
-                    TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(alphabet_len), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
-                    TB_CK((launch_stripes<MODE_SW, TB_COLMAX>(p, S, stream, dev)));
-                    TB_CK(grow_pinned(ctx.h_total, ctx.ch_total, 16));
-                    TB_CK(cudaMemcpyAsync(ctx.h_total, ctx.d_prog, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-                    TB_CK(cudaStreamSynchronize(stream));
-                    if (*(const uint32_t *)ctx.h_total) return fail(HY_ERR_TIMEOUT);
-                } else {
-                    TB_CK(R == 4 ? launch_colmax<4>(p, stream) : R == 8 ? launch_colmax<8>(p, stream)
-                                                                        : launch_colmax<16>(p, stream));
-                }
-                tb_position_hits_kernel<<<(b - a + 63) / 64, 64, 0, stream>>>(
-                    p, d_scores, d_tend, max_e, min_score, score2 ? d_s2 : nullptr);
-                TB_CK(cudaGetLastError());
-                TB_CK(cudaEventRecord(ctx.ev[1], stream));
-                TB_CK(cudaEventSynchronize(ctx.ev[1]));
-                float ms = 0.f;
-                TB_CK(cudaEventElapsedTime(&ms, ctx.ev[0], ctx.ev[1]));
-                ctx.fill_ms += ms;
-                ctx.launches += 3;
-            }
-            return fail(HY_OK);
-        };
-        if (!longs.empty()) {
-            st = run(longs, TB_STRIPE_R, true);
-            if (st != HY_OK) return st;
-        }
-        if (!bulk.empty()) {
-            st = run(bulk, Rb, false);
-            if (st != HY_OK) return st;
-        }
-        std::vector<int32_t> h(4 * n_ok);
-        TB_CK(cudaMemcpyAsync(h.data(), d_res, sizeof(int32_t) * (score2 ? 4 : 2) * n_ok, cudaMemcpyDeviceToHost,
-                              stream));
-        int32_t *h_cm = nullptr;
-        if (colmax && t_bytes) {
-            TB_CK(grow_pinned(ctx.h_stage, ctx.ch_stage, sizeof(int32_t) * t_bytes));
-            h_cm = (int32_t *)ctx.h_stage;
-            TB_CK(cudaMemcpyAsync(h_cm, d_colmax, sizeof(int32_t) * t_bytes, cudaMemcpyDeviceToHost, stream));
-        }
-        TB_CK(cudaStreamSynchronize(stream));
-        if (h_cm)
-            parallel_for(t_bytes, 1 << 22, [&](uint64_t a, uint64_t e, unsigned) {
-                memcpy(colmax + a, h_cm + a, sizeof(int32_t) * (e - a));
-            });
-        for (uint64_t k = 0; k < n_ok; ++k) {
-            out[k].score = h[k];
-            out[k].reserved = 0;
-            out[k].db_index = k;
-            out[k].query_end = -1;
-            out[k].target_end = h[n_ok + k];
-            if (score2) {
-                score2[2 * k] = h[2 * n_ok + 2 * k];
-                score2[2 * k + 1] = h[2 * n_ok + 2 * k + 1];
-            }
-        }
-        ctx.call_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
-    }
-    return fail(first, d[0], d[1]);
 }
 
 }  // extern "C"

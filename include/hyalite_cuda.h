@@ -335,7 +335,8 @@ hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
 /* Phases of this thread's last hy_align_pairs call, in ms (no reference counterpart): up to n of
  * {the host lengths pass and routing, host sort and item packing (summed over chunks), host staging
  * copies (summed), the chunk pipeline (wall time to the device's end, overlapping the two before),
- * results back, host waits for a staging slot}. */
+ * results back, host waits for a staging slot, host copies of the column maxima into the caller's
+ * array (hy_align_pairs_position_max)}. The last call of either entry point. */
 hy_status hy_align_pairs_phases(double *ms, uint32_t n);
 
 /* ---- traceback: the Alignment search type (src/align.rs, src/database.rs:517-565) -------------- */
@@ -380,10 +381,12 @@ hy_status hy_traceback_timing(hy_scratch *scratch, double out[5]);
  * index in *failed_pair and the pairs before it are computed). out[k]: score = max of the pair's
  * column maxima, query_end -1 (not tracked), target_end = first position of that maximum or -1 when
  * the score is 0, db_index k. colmax (NULL: not copied) receives every pair's per-target-position
- * maxima at t_off[k] - t_off[0] (|t_k| entries, each >= 0). score2 (NULL: not computed) receives
- * {score, position} per pair: bwa's score2 (hy_score2) of the pair's maxima with its best score,
- * its target end (position 0 when -1), the matrix's largest entry and min_score; {0, -1} when no
- * peak qualifies. A few long pairs run on the stripe kernel, the rest one warp each. */
+ * maxima at t_off[k] - t_off[0] (|t_k| entries, each >= 0; on an error, the positions of the
+ * pairs from the failing one on are 0). score2 (NULL: not computed) receives {score, position} per
+ * pair: bwa's score2 (hy_score2) of the pair's maxima with its best score, its target end
+ * (position 0 when -1), the matrix's largest entry and min_score; {0, -1} when no peak qualifies.
+ * The pairs run through align_pairs' chunked pipeline and pair kernels (their column-maxima
+ * form); a few long pairs on the stripe kernel. */
 hy_status hy_align_pairs_position_max(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
                                       const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
                                       uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext,

@@ -91,3 +91,72 @@ def test_single_pair_entry_matches_batch_and_score2():
     assert out == want and h.score == score and h.target_end == te
     assert hy.score2(out, h.score, h.target_end, max(BLOSUM62), 30) == o.score2(want, score, te, max(BLOSUM62), 30)
     assert hy.score2(out, h.score, h.target_end, max(BLOSUM62), 30) is not None  # the second copy
+
+
+def _sample_check(qs, ts, idx, hits, cm, s2, t_off, mat, al, go, ge, min_score):
+    mmax = max(mat)
+    for k in idx:
+        want, score, te = o.position_max(qs[k], ts[k], mat, al, go, ge)
+        got = [int(v) for v in cm[int(t_off[k] - t_off[0]): int(t_off[k + 1] - t_off[0])]]
+        assert got == want, k
+        h = hits[k]
+        assert (h.score, h.db_index, h.query_end, h.target_end) == (score, k, -1, -1 if te is None else te), k
+        w2 = o.score2(want, score, 0 if te is None else te, mmax, min_score)
+        assert (int(s2[2 * k]), int(s2[2 * k + 1])) == ((0, -1) if w2 is None else w2), k
+
+
+def test_many_chunks_multi_pass_int32_and_long_pairs():
+    """A batch of several chunks: mate-rescue pairs, queries longer than one pass (maxima of the
+    passes combined), pairs whose width proof needs int32 (a large matrix entry on longer pairs),
+    empty sequences and a few long pairs on the stripe kernel; the caller's column-maxima array
+    refilled in place (every entry written)."""
+    rng = np.random.default_rng(12)
+    n = 150_000
+    mat = [int(v) for v in rng.integers(-3, 5, 16)]
+    mat[5] = 300
+    qs = [rng.integers(0, 4, int(rng.integers(0, 40))) for _ in range(n)]
+    ts = [rng.integers(0, 4, int(rng.integers(0, 80))) for _ in range(n)]
+    special = [int(k) for k in rng.choice(n, 400, replace=False)]
+    for k in special[:200]:  # two or three passes of 256 rows
+        qs[k] = rng.integers(0, 4, int(rng.integers(257, 700)))
+        ts[k] = rng.integers(0, 4, int(rng.integers(50, 400)))
+    for k in special[200:]:  # int32 by the width proof
+        qs[k] = rng.integers(0, 4, int(rng.integers(120, 200)))
+        ts[k] = rng.integers(0, 4, int(rng.integers(120, 300)))
+    longs = [7, 80_001, 149_990]
+    for k in longs:
+        qs[k] = rng.integers(0, 4, 1100)
+        ts[k] = np.concatenate([rng.integers(0, 4, 400), qs[k][100:900], rng.integers(0, 4, 300)])
+    q_res, q_off = hy.concat(qs)
+    t_res, t_off = hy.concat(ts)
+    buf = np.full(int(t_off[-1]), -7, np.int32)
+    hits, cm, s2, (err, failed) = hy.align_pairs_position_max_arrays(
+        q_res, q_off, t_res, t_off, hy.Scoring(4, mat, 6, 1), 15, colmax_out=buf)
+    assert err is None and failed == n and cm is buf
+    assert int(buf.min()) >= 0  # every position written
+    idx = sorted(set(list(range(0, n, 1009)) + special[::9] + longs + [n - 1]))
+    _sample_check(qs, ts, idx, hits, cm, s2, t_off, mat, 4, 6, 1, 15)
+
+
+def test_failure_in_a_later_chunk_leaves_a_correct_prefix():
+    """The first bad symbol (a query's, in a later chunk) ends the batch there: its index and
+    error, every earlier pair's maxima, hits and score2 exact, the positions from it on 0."""
+    rng = np.random.default_rng(13)
+    n = 140_000
+    qs = [rng.integers(0, 4, int(rng.integers(1, 40))) for _ in range(n)]
+    ts = [rng.integers(0, 4, int(rng.integers(1, 80))) for _ in range(n)]
+    bad = 100_003
+    qs[bad] = qs[bad].copy()
+    qs[bad][0] = 5
+    ts[bad + 7] = ts[bad + 7].copy()
+    ts[bad + 7][0] = 9
+    q_res, q_off = hy.concat(qs)
+    t_res, t_off = hy.concat(ts)
+    buf = np.full(int(t_off[-1]), -7, np.int32)
+    hits, cm, s2, (err, failed) = hy.align_pairs_position_max_arrays(
+        q_res, q_off, t_res, t_off, hy.Scoring(4, DNA, 2, 1), 10, colmax_out=buf)
+    assert err == hy.Error("SymbolOutOfRange", symbol=5, alphabet_len=4) and failed == bad
+    assert int(buf[: int(t_off[bad])].min()) >= 0
+    assert not buf[int(t_off[bad]):].any()
+    idx = sorted(set(list(range(0, bad, 997)) + [bad - 1]))
+    _sample_check(qs, ts, idx, hits, cm, s2, t_off, DNA, 4, 2, 1, 10)
