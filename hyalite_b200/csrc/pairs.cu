@@ -181,6 +181,9 @@ static cudaError_t launch_pairs_mode(const PairParams &p, int blocks, int thread
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+        // All shared memory: the blocks' group profiles decide how many fit on an SM.
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
     }
     kern<<<blocks, threads, smem, st>>>(p);
     return cudaGetLastError();
@@ -249,19 +252,42 @@ static cudaError_t launch_pairs_rows(int rows, int mode, bool ends, const PairPa
     }
 }
 
-// Rows per lane for an int16x2 item of query length q: the fewest padded rows over the pass
-// shapes whose per-group profile keeps at least two warps of groups per block; ties go to more
-// rows (fewer passes).
+// Shared memory of an SM (B200), and what each resident block reserves of it.
+constexpr size_t SM_SMEM = 228 * 1024, BLOCK_SMEM_RESERVE = 1024;
+
+// Groups per block of the pair kernel for group profiles of gb bytes: up to 256 threads, whole
+// warps, within PAIR_SMEM_LIMIT; 0 when not one warp of groups fits (the global-profile form).
+static int pair_groups_per_block(size_t gb, int G) {
+    int g = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / gb);
+    return g / (32 / G) * (32 / G);
+}
+
+// Warps of pair-kernel groups one SM holds with group profiles of gb bytes: as many blocks as its
+// shared memory and registers (at most 128 a thread) allow.
+static double pair_resident_warps(size_t gb, int G) {
+    const int gpb = pair_groups_per_block(gb, G);
+    if (gpb == 0) return 0.0;
+    const size_t by_smem = SM_SMEM / ((size_t)gpb * gb + BLOCK_SMEM_RESERVE);
+    const size_t by_regs = 65536 / ((size_t)gpb * G * 128);
+    return (double)std::min(by_smem, by_regs) * gpb * G / 32.0;
+}
+
+// Rows per lane for an int16x2 item of query length q: the least estimated time over the pass
+// shapes, counting the padded rows of the last pass, the per-step work shared by a lane's rows,
+// and the warps an SM holds (each group keeps its own query profile in shared memory, so more rows
+// per lane means fewer resident warps; about 12 warps keep the pipes busy). Ties go to more rows.
 static int pair_rows(uint64_t q, int32_t al) {
     int best = 8;
-    uint64_t best_pad = ~0ull;
+    double best_cost = 1e300;
     for (int r : PAIR_ROWS) {
-        const size_t group_bytes = (size_t)(al + 1) * PAIR_G * r * profile_row_bytes<Pair16>();
-        if (r > 8 && group_bytes * 8 > PAIR_SMEM_LIMIT) continue;
+        const size_t gb = (size_t)(al + 1) * PAIR_G * r * profile_row_bytes<Pair16H>();
+        const double w = pair_resident_warps(gb, PAIR_G);
+        if (w <= 0.0) continue;
         const uint64_t rpp = (uint64_t)PAIR_G * r;
-        const uint64_t pad = (q + rpp - 1) / rpp * rpp;
-        if (pad <= best_pad) {
-            best_pad = pad;
+        const double pad = (double)((q + rpp - 1) / rpp * rpp);
+        const double cost = pad * (r + 6.0) / r / std::min(1.0, w / 12.0);
+        if (cost <= best_cost) {
+            best_cost = cost;
             best = r;
         }
     }
@@ -487,8 +513,7 @@ static hy_status run_items(PairsContext &ctx, PairParams p, int res_slot, int bn
         size_t i1 = i0;
         while (i1 < n_items && (qlen[i1] == qlen[i0] || rows_of(qlen[i1]) == r)) ++i1;
         const size_t group_bytes = (size_t)(p.al + 1) * G * r * profile_row_bytes<A>();
-        int gpb = (int)std::min<size_t>(256 / G, PAIR_SMEM_LIMIT / group_bytes);
-        gpb = gpb / (32 / G) * (32 / G);  // whole warps
+        int gpb = pair_groups_per_block(group_bytes, G);
         p.group_bytes = (uint32_t)group_bytes;
         if (gpb == 0) {
             // Not one warp of group profiles fits in shared memory (a large alphabet): the groups
@@ -718,7 +743,7 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             HY_CK(ctx.get(meta_slot[h], sizeof(ItemMeta) * n_part[h], &m));
             HY_CK(ctx.get(qlen_slot[h], sizeof(uint32_t) * n_part[h], &ql));
             HY_CK(ctx.get(iqoff_slot[h], 2 * sizeof(uint64_t) * n_part[h], &qo));
-            HY_CK(ctx.get(res_slot[h], res_cols * (h == 0 ? sizeof(Pair16::RES) : sizeof(Single32::RES)), &scratch));
+            HY_CK(ctx.get(res_slot[h], res_cols * (h == 0 ? sizeof(Pair16H::RES) : sizeof(Single32::RES)), &scratch));
             p.meta = (const ItemMeta *)m;
             p.qlen = (const uint32_t *)ql;
             p.qoff = (const uint64_t *)qo;
@@ -836,7 +861,7 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             HY_CK(cudaStreamWaitEvent(ctx.stream, ctx.slot_ev[s], 0));
             if (posmax && tb) HY_CK(cudaMemsetAsync(d_colmax + t_off[a], 0, sizeof(int32_t) * tb, ctx.stream));
             HY_CK(cudaEventRecord(ctx.ev[2 * c], ctx.stream));
-            st = run_items<Pair16, PAIR_G>(ctx, pp[0], PS_RES16, PS_BND16, qlen[0], ib[0], n_items[0], cols[0],
+            st = run_items<Pair16H, PAIR_G>(ctx, pp[0], PS_RES16, PS_BND16, qlen[0], ib[0], n_items[0], cols[0],
                                            (const uint64_t *)d_qoff, (const uint64_t *)d_toff, (uint8_t *)d_q,
                                            (const uint8_t *)d_t, d_bad, mode, ends);
             if (st != HY_OK) return st;

@@ -150,6 +150,30 @@ struct Pair16 {
     __host__ __device__ static constexpr uint32_t code(uint32_t lo, uint32_t hi, uint32_t) { return lo | (hi << 8); }
 };
 
+// The int16x2 arithmetic with a half-size query profile, for kernels whose groups each keep their
+// own profile in shared memory (the pair kernel): each table holds 16-bit entries, and a row's
+// word is assembled from the two tables' entries by one byte permute instead of merging two 32-bit
+// words by an add. The same values; half the shared memory, so twice the groups fit on an SM.
+struct Pair16H : Pair16 {
+    typedef uint16_t PE;
+    __device__ __forceinline__ static V diag(V g, V p, V) { return __vadd2(g, p); }
+    template <int R, int G>
+    __device__ __forceinline__ static void load_chunk(const uint8_t *prof_lo, const uint8_t *prof_hi,
+                                                      int a, int b, int lane, int k, V (&pa)[EPV],
+                                                      V (&pb)[EPV]) {
+        constexpr int KCH = R / EPV;
+        const uint2 A = reinterpret_cast<const uint2 *>(prof_lo)[((size_t)a * KCH + k) * G + lane];
+        const uint2 B = reinterpret_cast<const uint2 *>(prof_hi)[((size_t)b * KCH + k) * G + lane];
+        // Row 2i: the low entries of both tables' word i; row 2i + 1: the high entries.
+        pa[0] = __byte_perm(A.x, B.x, 0x5410);
+        pa[1] = __byte_perm(A.x, B.x, 0x7632);
+        pa[2] = __byte_perm(A.y, B.y, 0x5410);
+        pa[3] = __byte_perm(A.y, B.y, 0x7632);
+        pb[0] = pb[1] = pb[2] = pb[3] = 0;
+    }
+    __host__ __device__ __forceinline__ static PE word(int64_t v, int) { return (uint16_t)(int16_t)v; }
+};
+
 // The Precomputed layout (src/inter.rs:317-330: "a precomputed score table, so each cell's
 // substitution vector is a direct load with no gather"), restated for the device: the database
 // stores each pair column as one code c = lo * (al + 1) + hi, and the pass's profile is a single
