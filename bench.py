@@ -724,6 +724,19 @@ def run_pairs(args):
         for key, v in hy.align_pairs_phases().items():
             phases[key] = phases.get(key, 0.0) + v / args.steps
     clk = clocks.stop()
+    # The same calls with the reads and windows already in page-locked memory (a caller that keeps
+    # them pinned): the device copies the residues from where they are, with no staging copy.
+    pq = torch.empty(len(q_res), dtype=torch.uint8, pin_memory=True).numpy()
+    pt = torch.empty(len(t_res), dtype=torch.uint8, pin_memory=True).numpy()
+    pq[:] = q_res
+    pt[:] = t_res
+    hy.align_pairs_arrays(pq, q_off, pt, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
+    cms_pinned = 0.0
+    for _ in range(args.steps):
+        hits_p, (err, _) = hy.align_pairs_arrays(pq, q_off, pt, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
+        assert err is None
+        cms_pinned += hy.align_pairs_timing()[1]
+    same_pinned = bytes(hits_p) == bytes(hits)
     # Parity on a sample against the oracle, and the CPU baseline (the reference's align_pairs is
     # the scalar align_core loop) on a bounded sample over all host threads.
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -757,6 +770,8 @@ def run_pairs(args):
                 "h2d_bytes_per_step": int(len(q_res) + len(t_res) + 16 * args.n_pairs),
                 "d2h_bytes_per_step": 12 * args.n_pairs, "call_ms": cms / args.steps,
                 "phases_ms": {k: round(v, 1) for k, v in phases.items()}},
+        "e2e_pinned_inputs": {"value": cells * args.steps / (cms_pinned * 1e-3) / 1e9, "unit": "GCUPS",
+                              "call_ms": cms_pinned / args.steps, "hits_identical": same_pinned},
         "identical_to_oracle_on_sample": identical,
         "cpu_baseline": {"value": ccells / cpu_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
                          "sample": f"the first {n_cpu} pairs, scalar align_core restatement over {threads} threads"},
@@ -903,6 +918,21 @@ def run_position_max(args):
         for key, v in hy.align_pairs_phases().items():
             phases[key] = phases.get(key, 0.0) + v / args.steps
     clk = clocks.stop()
+    # The same calls with page-locked inputs and column-maxima array (a caller that keeps them
+    # pinned): no staging copy in, the maxima copied from the device straight into the array.
+    pq = torch.empty(len(q_res), dtype=torch.uint8, pin_memory=True).numpy()
+    pt = torch.empty(len(t_res), dtype=torch.uint8, pin_memory=True).numpy()
+    pcm = torch.empty(len(cm_buf), dtype=torch.int32, pin_memory=True).numpy()
+    pq[:] = q_res
+    pt[:] = t_res
+    hy.align_pairs_position_max_arrays(pq, q_off, pt, t_off, scoring, 20, pcm)
+    cms_pinned = 0.0
+    for _ in range(args.steps):
+        pcm.fill(-1)
+        hits_p, _, s2_p, (err, _) = hy.align_pairs_position_max_arrays(pq, q_off, pt, t_off, scoring, 20, pcm)
+        assert err is None
+        cms_pinned += hy.position_max_timing()["call_ms"]
+    same_pinned = bool(np.array_equal(pcm, cm) and bytes(hits_p) == bytes(hits) and np.array_equal(s2_p, s2))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     rng = np.random.default_rng(2)
@@ -935,6 +965,8 @@ def run_position_max(args):
                 "h2d_bytes_per_step": int(len(q_res) + len(t_res)),
                 "d2h_bytes_per_step": int(4 * len(t_res) + 16 * args.n_pos_pairs), "call_ms": cms / args.steps,
                 "phases_ms": {k: round(v, 1) for k, v in phases.items()}},
+        "e2e_pinned_buffers": {"value": cells * args.steps / (cms_pinned * 1e-3) / 1e9, "unit": "GCUPS",
+                               "call_ms": cms_pinned / args.steps, "results_identical": same_pinned},
         "identical_to_oracle_on_sample": bool(identical),
         "cpu_baseline": {"value": ccells / cpu_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
                          "sample": f"the first {n_cpu} pairs, scalar position-max restatement over {threads} threads"},

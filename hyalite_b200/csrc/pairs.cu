@@ -554,6 +554,18 @@ __global__ void pos_hits_kernel(uint64_t n, const uint64_t *t_off, const int32_t
                   tend + k, s2 ? s2 + 2 * k : nullptr);
 }
 
+// Whether p lies in page-locked host memory the device can copy from or to directly (memory from
+// cudaMallocHost / cudaHostAlloc / cudaHostRegister, such as a pinned tensor's).
+static bool host_pinned(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost;
+}
+
 // What a call computes besides align_pairs' hits: align_pair_position_max (posmax: SW, score only,
 // the column maxima, each pair's BestHit from them and, with score2, its score2).
 struct PairsCall {
@@ -679,6 +691,7 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
     const bool posmax = pc.posmax;
     const int32_t *h_out = nullptr;
     int32_t *h_cm = nullptr;  // posmax: pinned column maxima, from t_off[0]
+    bool cm_direct = false;   // h_cm is the caller's own (pinned) array
     const auto t_pipe = clock::now();
     if (n_len > 0) {
         int dev = 0;
@@ -726,8 +739,10 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             HY_CK(ctx.get(PS_COLMAX, sizeof(int32_t) * t_off[L], &cmv));
             d_colmax = (int32_t *)cmv;
             if (pc.colmax && t_off[L] > t_off[0]) {
-                void *hv;
-                HY_CK(ctx.get_pinned(PAIR_SLOTS + 1, sizeof(int32_t) * (t_off[L] - t_off[0]), &hv));
+                // A pinned caller array takes the column maxima straight from the device.
+                cm_direct = host_pinned(pc.colmax);
+                void *hv = pc.colmax;
+                if (!cm_direct) HY_CK(ctx.get_pinned(PAIR_SLOTS + 1, sizeof(int32_t) * (t_off[L] - t_off[0]), &hv));
                 h_cm = (int32_t *)hv;
             }
         }
@@ -765,6 +780,9 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
                 p.colmax = d_colmax;
             }
         }
+        // Residues already in pinned memory are copied to the device from where they are; others go
+        // through the staging slots.
+        const bool q_pinned = host_pinned(q_res), t_pinned = host_pinned(t_res);
         void *slots[PAIR_SLOTS];
         for (int s = 0; s < PAIR_SLOTS && s < (int)n_chunks; ++s) HY_CK(ctx.get_pinned(s, slot_bytes, &slots[s]));
         HY_CK(cudaMemsetAsync(d_bad, 0xff, sizeof(uint32_t), ctx.stream));
@@ -838,19 +856,24 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             }
             ctx.phase_ms[1] += since(t0);
             t0 = clock::now();
-            parallel_for(qb + tb, 1 << 20, [&](uint64_t x0, uint64_t x1, unsigned) {
-                if (x0 < qb) memcpy(slot + x0, q_res + q_off[a] + x0, std::min(x1, qb) - x0);
-                if (x1 > qb) {
-                    const uint64_t y0 = std::max(x0, qb);
-                    memcpy(slot + y0, t_res + t_off[a] + (y0 - qb), x1 - y0);
+            const uint64_t sq = q_pinned ? 0 : qb, st_b = t_pinned ? 0 : tb;  // bytes to stage
+            parallel_for(sq + st_b, 1 << 20, [&](uint64_t x0, uint64_t x1, unsigned) {
+                if (x0 < sq) memcpy(slot + x0, q_res + q_off[a] + x0, std::min(x1, sq) - x0);
+                if (x1 > sq) {
+                    const uint64_t y0 = std::max(x0, sq);
+                    memcpy(slot + qb + (y0 - sq), t_res + t_off[a] + (y0 - sq), x1 - y0);
                 }
             });
             memcpy(s_qoff, q_off + a, sizeof(uint64_t) * (n + 1));
             memcpy(s_toff, t_off + a, sizeof(uint64_t) * (n + 1));
             ctx.phase_ms[2] += since(t0);
             cudaStream_t cs = ctx.copy_stream;
-            if (qb) HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[a], slot, qb, cudaMemcpyHostToDevice, cs));
-            if (tb) HY_CK(cudaMemcpyAsync((uint8_t *)d_t + t_off[a], slot + qb, tb, cudaMemcpyHostToDevice, cs));
+            if (qb)
+                HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[a], q_pinned ? q_res + q_off[a] : slot, qb,
+                                      cudaMemcpyHostToDevice, cs));
+            if (tb)
+                HY_CK(cudaMemcpyAsync((uint8_t *)d_t + t_off[a], t_pinned ? t_res + t_off[a] : slot + qb, tb,
+                                      cudaMemcpyHostToDevice, cs));
             HY_CK(cudaMemcpyAsync((uint64_t *)d_qoff + a, s_qoff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cs));
             HY_CK(cudaMemcpyAsync((uint64_t *)d_toff + a, s_toff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cs));
             for (int h = 0; h < 2; ++h)
@@ -912,7 +935,8 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
         void *h_stage = nullptr;
         HY_CK(ctx.get_pinned(PAIR_SLOTS, sizeof(int32_t) * out_words, &h_stage));
         HY_CK(cudaMemcpyAsync(h_stage, d_out, sizeof(int32_t) * out_words, cudaMemcpyDeviceToHost, ctx.stream));
-        if (h_cm) {
+        if (h_cm && cm_direct) HY_CK(cudaStreamSynchronize(ctx.d2h_stream));
+        if (h_cm && !cm_direct) {
             // Chunks' column maxima into the caller's array as they arrive.
             for (uint64_t c = 0; c < n_chunks; ++c) {
                 HY_CK(cudaEventSynchronize(ctx.ev[2 * n_chunks + c]));
@@ -925,7 +949,7 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             }
         }
         HY_CK(cudaStreamSynchronize(ctx.stream));
-        if (h_cm)
+        if (h_cm && !cm_direct)
             for (uint32_t k : run_long)
                 memcpy(pc.colmax + (t_off[k] - t_off[0]), h_cm + (t_off[k] - t_off[0]),
                        sizeof(int32_t) * (t_off[k + 1] - t_off[k]));

@@ -255,3 +255,41 @@ def test_many_chunks_mixed_widths_and_long_pairs(mode):
     assert err is None and failed == n
     sample = sorted(set(list(range(0, n, 997)) + [5, 99_999, 150_001, n - 1]))
     _check_sample(hits, qs, ts, sample, mat, 4, 9, 2, mode, 1)
+
+
+def test_pinned_buffers_give_the_same_results():
+    """Residues (and, for position maxima, the column-maxima array) in page-locked memory are
+    copied from and to where they are, with no staging: results identical to pageable buffers,
+    across several chunks, with a failure in a later chunk."""
+    import torch
+
+    rng = np.random.default_rng(31)
+    n = 150_000
+    qs = [rng.integers(0, 4, int(rng.integers(0, 40))) for _ in range(n)]
+    ts = [rng.integers(0, 4, int(rng.integers(0, 90))) for _ in range(n)]
+    qs[120_001] = qs[120_001].copy()
+    if len(qs[120_001]) == 0:
+        qs[120_001] = np.array([0], np.uint8)
+    qs[120_001][0] = 6
+    q_res, q_off = _concat(qs)
+    t_res, t_off = _concat(ts)
+
+    def pinned(a):
+        p = torch.empty(len(a), dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True).numpy()
+        p[:] = a
+        return p
+
+    scoring = hy.Scoring(4, DNA, 2, 1)
+    h1, (e1, f1) = hy.align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, hy.Mode.Sw, hy.SearchType.ScoreEnd)
+    pq, pt = pinned(q_res), pinned(t_res)
+    h2, (e2, f2) = hy.align_pairs_arrays(pq, q_off, pt, t_off, scoring, hy.Mode.Sw, hy.SearchType.ScoreEnd)
+    assert (e1, f1) == (e2, f2) and f1 == 120_001 and e1.kind == "SymbolOutOfRange"
+    assert bytes(h1)[: 32 * f1] == bytes(h2)[: 32 * f2]
+    cm1 = np.full(int(t_off[-1]), -3, np.int32)
+    cm2 = pinned(cm1)
+    r1 = hy.align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring, 8, colmax_out=cm1)
+    r2 = hy.align_pairs_position_max_arrays(pq, q_off, pt, t_off, scoring, 8, colmax_out=cm2)
+    assert r1[3] == r2[3] and r1[3][1] == 120_001
+    assert np.array_equal(cm1, cm2)
+    assert bytes(r1[0])[: 32 * 120_001] == bytes(r2[0])[: 32 * 120_001]
+    assert np.array_equal(r1[2][: 2 * 120_001], r2[2][: 2 * 120_001])
