@@ -52,6 +52,18 @@ struct hy_scratch {
     // operations of the last traceback call.
     void *tb = nullptr;
     std::vector<uint8_t> tb_ops;
+    // CUDA graphs of small scans (hy_scan / hy_scan_scores / hy_scan_all): one per call kind and
+    // query length, captured on first use and replayed instead of launching each kernel; exec is
+    // null for a call whose capture failed (it then launches directly).
+    struct Graph {
+        int kind;
+        uint64_t qlen;
+        cudaGraphExec_t exec;
+        uint64_t launches;  // kernels the graph launches
+        uint64_t last_use;
+    };
+    std::vector<Graph> graphs;
+    uint64_t graph_clock = 0;
 };
 
 namespace hy {
@@ -394,11 +406,89 @@ static hy_status check_query(const hy_db *db, const uint8_t *query, uint64_t qle
     return fail(HY_OK);
 }
 
-static hy_status upload_query(hy_scratch *sc, const uint8_t *query, uint64_t qlen) {
-    if (qlen) {
-        memcpy(sc->h_query, query, qlen);
-        HY_CK(cudaMemcpyAsync(sc->d_query, sc->h_query, qlen, cudaMemcpyHostToDevice, sc->stream));
+// ---- small scans through CUDA graphs ------------------------------------------------------------
+//
+// A scan of a small database is launch-bound: its kernels run for tens of microseconds, and each
+// of the call's ten or so stream operations costs a few microseconds of host and device time. Such
+// calls capture their device work (query upload, kernels, copies back) once per query length into
+// a CUDA graph and replay it.
+
+// Calls whose query meets at most this many database residues x query rows use graphs.
+constexpr double GRAPH_MAX_CELLS = 2e9;
+constexpr size_t GRAPH_CACHE = 32;  // graphs a scratch keeps (least recently used evicted)
+enum { GRAPH_SCAN = 0, GRAPH_SCORES = 1, GRAPH_ALL = 2 };
+
+static uint64_t db_residues(const hy_db *db) {
+    return db->p16.res_prefix.empty() ? 0 : db->p16.res_prefix.back();
+}
+
+// Enqueues a call's device work on sc->stream through `issue`: directly, or by replaying the
+// scratch's graph for (kind, qlen), capturing it on first use.
+template <class F>
+static hy_status run_captured(const hy_db *db, hy_scratch *sc, int kind, uint64_t qlen, F issue) {
+    if (sc->profile || (double)qlen * (double)db_residues(db) > GRAPH_MAX_CELLS) return issue();
+    for (auto &gr : sc->graphs) {
+        if (gr.kind != kind || gr.qlen != qlen) continue;
+        gr.last_use = ++sc->graph_clock;
+        if (!gr.exec) return issue();
+        HY_CK(cudaGraphLaunch(gr.exec, sc->stream));
+        sc->launches += gr.launches;
+        return fail(HY_OK);
     }
+    if (sc->graphs.size() >= GRAPH_CACHE) {
+        auto old = std::min_element(sc->graphs.begin(), sc->graphs.end(),
+                                    [](const hy_scratch::Graph &a, const hy_scratch::Graph &b) {
+                                        return a.last_use < b.last_use;
+                                    });
+        if (old->exec) cudaGraphExecDestroy(old->exec);
+        sc->graphs.erase(old);
+    }
+    const uint64_t launches0 = sc->launches;
+    HY_CK(cudaStreamBeginCapture(sc->stream, cudaStreamCaptureModeThreadLocal));
+    hy_status st = issue();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(sc->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (st == HY_OK && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (st != HY_OK) return st;
+    sc->graphs.push_back({kind, qlen, e == cudaSuccess ? exec : nullptr, sc->launches - launches0,
+                          ++sc->graph_clock});
+    if (!sc->graphs.back().exec) {
+        // Not capturable here: this call and later ones of its kind and length launch directly.
+        sc->launches = launches0;
+        return issue();
+    }
+    HY_CK(cudaGraphLaunch(exec, sc->stream));
+    return fail(HY_OK);
+}
+
+// The device error flag back with the call's results (part of a call's captured work).
+static hy_status issue_err_back(hy_scratch *sc) {
+    HY_CK(cudaMemcpyAsync(sc->h_err, sc->d_err, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+    return fail(HY_OK);
+}
+
+// Waits for the call's work; a set device error flag (a bounded wait that gave up) is cleared and
+// reported.
+static hy_status wait_and_check(hy_scratch *sc) {
+    HY_CK(cudaStreamSynchronize(sc->stream));
+    if (*sc->h_err) {
+        *sc->h_err = 0;
+        HY_CK(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
+        HY_CK(cudaStreamSynchronize(sc->stream));
+        return fail(HY_ERR_TIMEOUT);
+    }
+    return fail(HY_OK);
+}
+
+// The query into the scratch's pinned buffer (host) and its copy to the device (enqueued).
+static void stage_query(hy_scratch *sc, const uint8_t *query, uint64_t qlen) {
+    if (qlen) memcpy(sc->h_query, query, qlen);
+}
+static hy_status issue_query(hy_scratch *sc, uint64_t qlen) {
+    if (qlen) HY_CK(cudaMemcpyAsync(sc->d_query, sc->h_query, qlen, cudaMemcpyHostToDevice, sc->stream));
     return fail(HY_OK);
 }
 
@@ -789,6 +879,8 @@ void hy_scratch_destroy(hy_scratch *sc) {
     cudaFreeHost(sc->h_hit);
     cudaFreeHost(sc->h_err);
     cudaFreeHost(sc->h_out);
+    for (auto &gr : sc->graphs)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
     for (auto &e : sc->events) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
@@ -856,10 +948,16 @@ hy_status hy_scan(const hy_db *db, hy_scratch *sc, const uint8_t *query, uint64_
     hy_status st = check_query(db, query, qlen);
     if (st != HY_OK) return st;
     DeviceGuard g(db->device);
-    if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
-    if ((st = enqueue_scan(db, sc, sc->d_query, qlen, sc->d_hit)) != HY_OK) return st;
-    HY_CK(cudaMemcpyAsync(sc->h_hit, sc->d_hit, sizeof(hy_hit), cudaMemcpyDeviceToHost, sc->stream));
-    if ((st = sync_and_check(sc)) != HY_OK) return st;
+    stage_query(sc, query, qlen);
+    st = run_captured(db, sc, GRAPH_SCAN, qlen, [&]() -> hy_status {
+        hy_status s2;
+        if ((s2 = issue_query(sc, qlen)) != HY_OK) return s2;
+        if ((s2 = enqueue_scan(db, sc, sc->d_query, qlen, sc->d_hit)) != HY_OK) return s2;
+        HY_CK(cudaMemcpyAsync(sc->h_hit, sc->d_hit, sizeof(hy_hit), cudaMemcpyDeviceToHost, sc->stream));
+        return issue_err_back(sc);
+    });
+    if (st != HY_OK) return st;
+    if ((st = wait_and_check(sc)) != HY_OK) return st;
     *out = *sc->h_hit;
     return fail(HY_OK);
 }
@@ -887,10 +985,16 @@ hy_status hy_scan_scores(const hy_db *db, hy_scratch *sc, const uint8_t *query, 
     if (st != HY_OK) return st;
     DeviceGuard g(db->device);
     if ((st = ensure_host_out(sc)) != HY_OK) return st;
-    if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
-    if ((st = enqueue_scores(db, sc, sc->d_query, qlen, false, nullptr, sc->d_scores)) != HY_OK) return st;
-    HY_CK(cudaMemcpyAsync(sc->h_out, sc->d_scores, 4 * db->n_seqs, cudaMemcpyDeviceToHost, sc->stream));
-    if ((st = sync_and_check(sc)) != HY_OK) return st;
+    stage_query(sc, query, qlen);
+    st = run_captured(db, sc, GRAPH_SCORES, qlen, [&]() -> hy_status {
+        hy_status s2;
+        if ((s2 = issue_query(sc, qlen)) != HY_OK) return s2;
+        if ((s2 = enqueue_scores(db, sc, sc->d_query, qlen, false, nullptr, sc->d_scores)) != HY_OK) return s2;
+        HY_CK(cudaMemcpyAsync(sc->h_out, sc->d_scores, 4 * db->n_seqs, cudaMemcpyDeviceToHost, sc->stream));
+        return issue_err_back(sc);
+    });
+    if (st != HY_OK) return st;
+    if ((st = wait_and_check(sc)) != HY_OK) return st;
     memcpy(out, sc->h_out, 4 * db->n_seqs);
     return fail(HY_OK);
 }
@@ -904,14 +1008,20 @@ hy_status hy_scan_all(const hy_db *db, hy_scratch *sc, const uint8_t *query, uin
     const bool ends = db->search_type != HY_SEARCH_SCORE;
     const uint64_t n = db->n_seqs;
     if ((st = ensure_host_out(sc)) != HY_OK) return st;
-    if ((st = upload_query(sc, query, qlen)) != HY_OK) return st;
-    if ((st = enqueue_scores(db, sc, sc->d_query, qlen, ends, nullptr, sc->d_scores)) != HY_OK) return st;
-    HY_CK(cudaMemcpyAsync(sc->h_out, sc->d_scores, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
-    if (ends) {
-        HY_CK(cudaMemcpyAsync(sc->h_out + n, sc->d_qend, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
-        HY_CK(cudaMemcpyAsync(sc->h_out + 2 * n, sc->d_tend, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
-    }
-    if ((st = sync_and_check(sc)) != HY_OK) return st;
+    stage_query(sc, query, qlen);
+    st = run_captured(db, sc, GRAPH_ALL, qlen, [&]() -> hy_status {
+        hy_status s2;
+        if ((s2 = issue_query(sc, qlen)) != HY_OK) return s2;
+        if ((s2 = enqueue_scores(db, sc, sc->d_query, qlen, ends, nullptr, sc->d_scores)) != HY_OK) return s2;
+        HY_CK(cudaMemcpyAsync(sc->h_out, sc->d_scores, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
+        if (ends) {
+            HY_CK(cudaMemcpyAsync(sc->h_out + n, sc->d_qend, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
+            HY_CK(cudaMemcpyAsync(sc->h_out + 2 * n, sc->d_tend, 4 * n, cudaMemcpyDeviceToHost, sc->stream));
+        }
+        return issue_err_back(sc);
+    });
+    if (st != HY_OK) return st;
+    if ((st = wait_and_check(sc)) != HY_OK) return st;
     for (uint64_t k = 0; k < n; ++k) {
         out[k].score = sc->h_out[k];
         out[k].reserved = 0;

@@ -270,3 +270,17 @@ def test_query_validation():
     with pytest.raises(hy.Error) as e:
         db.scan(sc, [0, 7])
     assert e.value == hy.Error("SymbolOutOfRange", symbol=7, alphabet_len=4)
+
+
+@pytest.mark.parametrize("mode", [0, 2, 4])
+def test_graph_replay_many_query_lengths(mode):
+    """Small scans replay a CUDA graph per call kind and query length from the scratch (captured on
+    first use, the least recently used of 32 evicted): 45 query lengths, each scanned, then scanned
+    again in the reverse order with other residues (replays of evicted and kept graphs), every
+    scan, scan_all and scan_scores equal to the oracle."""
+    rng = np.random.default_rng(400 + mode)
+    seqs = rand_seqs(rng, 3000, 4, 0, 120)
+    first = [list(rng.integers(0, 4, n)) for n in range(1, 46)]
+    second = [list(rng.integers(0, 4, n)) for n in range(45, 0, -1)]
+    for st in (0, 1):
+        check(seqs, DNA, 4, 2, 1, mode, st, first + second + first[:5], mql=45)
