@@ -696,8 +696,10 @@ def make_pairs_workload(seed: int, n_pairs: int, genome_len: int = 10_000_000, r
 
 def run_pairs(args):
     """align_pairs over (read, window) pairs: Mode::Hw, ScoreEnd, +2/-1, gap_open 6, gap_ext 1.
-    `value` is real cells / the pair kernels' device time; `e2e` is the whole hy_align_pairs call
-    (host validation, sort and packing, copies, kernels, results) with host buffers."""
+    `value` is real cells / the device time of the call's kernels (each chunk's packing and pair
+    kernels, CUDA events); `e2e` is the whole hy_align_pairs call (host lengths pass, sort and item
+    packing, staging copies, kernels, results) with pageable host buffers; `e2e_pinned_inputs` the
+    same with the residues already page-locked."""
     import torch
 
     import hyalite_b200 as hy

@@ -822,7 +822,8 @@ def traceback_min_bytes_for_database(max_m: int, max_n: int) -> int:
 
 
 def align_pairs_timing():
-    """(pair kernels' device ms, whole call ms) of this thread's last align_pairs call."""
+    """(device ms of the call's kernels: packing, pair and stripe kernels; whole call ms) of this
+    thread's last align_pairs call."""
     k, c = C.c_double(), C.c_double()
     _check(lib.hy_align_pairs_timing(C.byref(k), C.byref(c)))
     return float(k.value), float(c.value)

@@ -330,7 +330,8 @@ hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint
                          uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
                          hy_search_type search_type, hy_hit *out, uint64_t *failed_pair);
 /* Timing of this thread's last hy_align_pairs call (no reference counterpart): the device time of
- * its pair kernels (CUDA events around the launches) and the wall time of the whole call. */
+ * its kernels (CUDA events around each chunk's packing and pair kernels, plus the long pairs'
+ * stripe kernel) and the wall time of the whole call. */
 hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
 /* Phases of this thread's last hy_align_pairs call, in ms (no reference counterpart): up to n of
  * {the host lengths pass and routing, host sort and item packing (summed over chunks), host staging
