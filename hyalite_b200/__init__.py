@@ -831,7 +831,8 @@ def align_pairs_timing():
 
 def align_pairs_phases():
     """Phases (ms) of this thread's last align_pairs call: the host lengths pass and routing; host
-    sort and item packing and host staging copies, each summed over the chunks; the chunk pipeline
+    sort and item packing, and waits for the staging copies (which run on their own threads beside
+    the next chunk's sort), each summed over the chunks; the chunk pipeline
     (wall time to the device's end, overlapping the two before); results; host waits for a staging
     slot; host copies of the column maxima (align_pairs_position_max, whose last call it also
     reports)."""

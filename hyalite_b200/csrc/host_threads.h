@@ -4,6 +4,8 @@
 #include <stdint.h>
 
 #include <pthread.h>
+#include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -118,6 +120,102 @@ class HostPool {
     uint64_t gen_ = 0;
     std::atomic<uint64_t> next_{0};
     std::atomic<unsigned> left_{0};
+};
+
+// Copies up to two byte ranges on threads of its own while the caller goes on, one job at a time:
+// start() hands the ranges over and returns, wait() returns once they are copied. In a process made
+// by fork() after the threads started, start() copies synchronously (the threads are not there).
+class AsyncCopy {
+  public:
+    explicit AsyncCopy(unsigned threads) : pid_(getpid()) {
+        for (unsigned i = 0; i < std::max(1u, threads); ++i) workers_.emplace_back([this] { loop(); });
+    }
+    ~AsyncCopy() {
+        if (getpid() != pid_) {
+            for (auto &w : workers_) w.detach();
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &w : workers_) w.join();
+    }
+    void start(uint8_t *d0, const uint8_t *s0, uint64_t n0, uint8_t *d1, const uint8_t *s1, uint64_t n1) {
+        if (getpid() != pid_) {
+            if (n0) memcpy(d0, s0, n0);
+            if (n1) memcpy(d1, s1, n1);
+            return;
+        }
+        Job j{d0, s0, n0, d1, s1, n1, 0, 0};
+        j.pieces = (n0 + n1 + PIECE - 1) / PIECE;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            j.gen = ++gen_;
+            job_ = j;
+            left_.store(j.pieces);
+            next_.store(j.gen << 32);
+        }
+        if (j.pieces) cv_.notify_all();
+    }
+    void wait() {
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return left_.load() == 0; });
+    }
+
+  private:
+    static constexpr uint64_t PIECE = 1 << 20;
+    struct Job {
+        uint8_t *d0;
+        const uint8_t *s0;
+        uint64_t n0;
+        uint8_t *d1;
+        const uint8_t *s1;
+        uint64_t n1;
+        uint64_t pieces;
+        uint64_t gen;
+    };
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                j = job_;
+            }
+            uint64_t cur = next_.load();
+            for (;;) {
+                if ((cur >> 32) != (j.gen & 0xffffffffu)) break;
+                const uint64_t i = cur & 0xffffffffu;
+                if (i >= j.pieces) break;
+                if (!next_.compare_exchange_weak(cur, cur + 1)) continue;
+                // Piece i of the two ranges laid end to end.
+                const uint64_t a = i * PIECE, e = std::min(j.n0 + j.n1, a + PIECE);
+                if (a < j.n0) memcpy(j.d0 + a, j.s0 + a, std::min(e, j.n0) - a);
+                if (e > j.n0) {
+                    const uint64_t b = std::max(a, j.n0) - j.n0;
+                    memcpy(j.d1 + b, j.s1 + b, e - j.n0 - b);
+                }
+                if (left_.fetch_sub(1) == 1) {
+                    std::lock_guard<std::mutex> lk(m_);
+                    done_.notify_all();
+                }
+                cur = next_.load();
+            }
+        }
+    }
+    const pid_t pid_;
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    Job job_{};
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+    std::atomic<uint64_t> next_{0}, left_{0};
 };
 
 // Runs f(begin, end, part) over [0, n) split across the host's threads (at most one part per

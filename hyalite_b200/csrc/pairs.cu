@@ -158,9 +158,23 @@ static thread_local PairsContext g_ctx;
 // Grow-only host arrays of the calling thread: per-pair routes, a chunk's sort and item arrays.
 struct PairsHost {
     HostArr<uint8_t> route;
-    HostArr<uint32_t> ord[2], ord_tmp, start, qlen[2];
+    HostArr<uint32_t> ord[2], ord_tmp, start, qlen[4];  // qlen: two chunks x two arithmetics
     HostArr<uint64_t> keys[2], keys_tmp;
     std::vector<std::vector<uint64_t>> count;  // radix histograms, one per host thread
+    // Copies a chunk's residues into its staging slot while the next chunk is sorted and packed.
+    std::unique_ptr<AsyncCopy> copier;
+};
+
+// One chunk of pairs between its host preparation and its issue to the device.
+struct ChunkState {
+    uint64_t c, a, b, n, qb, tb;
+    int s;  // staging slot
+    uint8_t *slot;
+    uint64_t *s_qoff, *s_toff;
+    ItemMeta *s_meta[2];
+    size_t n_items[2];
+    uint64_t cols[2];
+    uint32_t *qlen[2];
 };
 
 static thread_local PairsHost g_host;
@@ -789,7 +803,9 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
         HY_CK(cudaMemcpyAsync(d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, ctx.stream));
         uint64_t ib[2] = {0, 0};
-        for (uint64_t c = 0; c < n_chunks; ++c) {
+        // Host side of chunk c: its pairs partitioned, sorted and packed into items, written with
+        // its offsets to its staging slot (the residues follow on the copier).
+        auto prep = [&](uint64_t c, ChunkState &cs) -> hy_status {
             const uint64_t a = chunk_at(c), b = chunk_at(c + 1), n = b - a;
             auto t0 = clock::now();
             // This chunk's packed pairs of each lane arithmetic, in input order, with their keys.
@@ -833,65 +849,69 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
                 o_tmp[h] = o_tmp[0];
                 k_tmp[h] = k_tmp[0];
             }
-            // The staging slot: [query residues][target residues][q_off, t_off slices][items].
+            // The staging slot: [query residues][target residues][q_off, t_off slices][items]. It was
+            // last used by chunk c - 3, already issued.
             const int s = (int)(c % PAIR_SLOTS);
             auto tw = clock::now();
             if (c >= (uint64_t)PAIR_SLOTS) HY_CK(cudaEventSynchronize(ctx.slot_ev[s]));
             ctx.phase_ms[5] += since(tw);
-            uint8_t *slot = (uint8_t *)slots[s];
-            const uint64_t qb = q_off[b] - q_off[a], tb = t_off[b] - t_off[a];
-            uint64_t *s_qoff = (uint64_t *)(slot + (qb + tb + 7) / 8 * 8), *s_toff = s_qoff + (n + 1);
-            ItemMeta *s_meta[2];
-            s_meta[0] = (ItemMeta *)(s_toff + (n + 1));
-            size_t n_items[2] = {0, 0};
-            uint64_t cols[2] = {0, 0};
-            uint32_t *qlen[2];
+            cs.c = c;
+            cs.a = a;
+            cs.b = b;
+            cs.n = n;
+            cs.s = s;
+            cs.slot = (uint8_t *)slots[s];
+            cs.qb = q_off[b] - q_off[a];
+            cs.tb = t_off[b] - t_off[a];
+            cs.s_qoff = (uint64_t *)(cs.slot + (cs.qb + cs.tb + 7) / 8 * 8);
+            cs.s_toff = cs.s_qoff + (n + 1);
+            cs.s_meta[0] = (ItemMeta *)(cs.s_toff + (n + 1));
             for (int h = 0; h < 2; ++h) {
-                if (h == 1) s_meta[1] = s_meta[0] + n_items[0];
-                qlen[h] = hs.qlen[h].get(cnt[h]);
+                cs.n_items[h] = 0;
+                cs.cols[h] = 0;
+                if (h == 1) cs.s_meta[1] = cs.s_meta[0] + cs.n_items[0];
+                cs.qlen[h] = hs.qlen[2 * (c & 1) + h].get(cnt[h]);
                 if (cnt[h] == 0) continue;
                 // One scratch pair serves both arithmetics: sort and pack the first before the second.
                 sort_by_shape(hs, o[h], k[h], o_tmp[h], k_tmp[h], cnt[h]);
-                n_items[h] = pack_items(hs, o[h], k[h], cnt[h], h == 0, s_meta[h], qlen[h], &cols[h]);
+                cs.n_items[h] = pack_items(hs, o[h], k[h], cnt[h], h == 0, cs.s_meta[h], cs.qlen[h], &cs.cols[h]);
             }
-            ctx.phase_ms[1] += since(t0);
-            t0 = clock::now();
-            const uint64_t sq = q_pinned ? 0 : qb, st_b = t_pinned ? 0 : tb;  // bytes to stage
-            parallel_for(sq + st_b, 1 << 20, [&](uint64_t x0, uint64_t x1, unsigned) {
-                if (x0 < sq) memcpy(slot + x0, q_res + q_off[a] + x0, std::min(x1, sq) - x0);
-                if (x1 > sq) {
-                    const uint64_t y0 = std::max(x0, sq);
-                    memcpy(slot + qb + (y0 - sq), t_res + t_off[a] + (y0 - sq), x1 - y0);
-                }
+            parallel_for(2 * (n + 1), 1 << 18, [&](uint64_t x0, uint64_t x1, unsigned) {
+                for (uint64_t x = x0; x < x1; ++x)
+                    (x <= n ? cs.s_qoff[x] : cs.s_toff[x - n - 1]) = x <= n ? q_off[a + x] : t_off[a + x - n - 1];
             });
-            memcpy(s_qoff, q_off + a, sizeof(uint64_t) * (n + 1));
-            memcpy(s_toff, t_off + a, sizeof(uint64_t) * (n + 1));
-            ctx.phase_ms[2] += since(t0);
-            cudaStream_t cs = ctx.copy_stream;
+            ctx.phase_ms[1] += since(t0);
+            return fail(HY_OK);
+        };
+        // Device side of a prepared chunk whose residues are staged: its copies on the copy stream,
+        // then its packing and pair kernels on the compute stream.
+        auto issue = [&](const ChunkState &cs) -> hy_status {
+            const uint64_t c = cs.c, a = cs.a, n = cs.n, qb = cs.qb, tb = cs.tb;
+            cudaStream_t cp = ctx.copy_stream;
             if (qb)
-                HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[a], q_pinned ? q_res + q_off[a] : slot, qb,
-                                      cudaMemcpyHostToDevice, cs));
+                HY_CK(cudaMemcpyAsync((uint8_t *)d_q + q_off[a], q_pinned ? q_res + q_off[a] : cs.slot, qb,
+                                      cudaMemcpyHostToDevice, cp));
             if (tb)
-                HY_CK(cudaMemcpyAsync((uint8_t *)d_t + t_off[a], t_pinned ? t_res + t_off[a] : slot + qb, tb,
-                                      cudaMemcpyHostToDevice, cs));
-            HY_CK(cudaMemcpyAsync((uint64_t *)d_qoff + a, s_qoff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cs));
-            HY_CK(cudaMemcpyAsync((uint64_t *)d_toff + a, s_toff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cs));
+                HY_CK(cudaMemcpyAsync((uint8_t *)d_t + t_off[a], t_pinned ? t_res + t_off[a] : cs.slot + qb, tb,
+                                      cudaMemcpyHostToDevice, cp));
+            HY_CK(cudaMemcpyAsync((uint64_t *)d_qoff + a, cs.s_qoff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cp));
+            HY_CK(cudaMemcpyAsync((uint64_t *)d_toff + a, cs.s_toff, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, cp));
             for (int h = 0; h < 2; ++h)
-                if (n_items[h])
-                    HY_CK(cudaMemcpyAsync(const_cast<ItemMeta *>(pp[h].meta) + ib[h], s_meta[h],
-                                          sizeof(ItemMeta) * n_items[h], cudaMemcpyHostToDevice, cs));
-            HY_CK(cudaEventRecord(ctx.slot_ev[s], cs));
-            HY_CK(cudaStreamWaitEvent(ctx.stream, ctx.slot_ev[s], 0));
+                if (cs.n_items[h])
+                    HY_CK(cudaMemcpyAsync(const_cast<ItemMeta *>(pp[h].meta) + ib[h], cs.s_meta[h],
+                                          sizeof(ItemMeta) * cs.n_items[h], cudaMemcpyHostToDevice, cp));
+            HY_CK(cudaEventRecord(ctx.slot_ev[cs.s], cp));
+            HY_CK(cudaStreamWaitEvent(ctx.stream, ctx.slot_ev[cs.s], 0));
             if (posmax && tb) HY_CK(cudaMemsetAsync(d_colmax + t_off[a], 0, sizeof(int32_t) * tb, ctx.stream));
             HY_CK(cudaEventRecord(ctx.ev[2 * c], ctx.stream));
-            st = run_items<Pair16H, PAIR_G>(ctx, pp[0], PS_RES16, PS_BND16, qlen[0], ib[0], n_items[0], cols[0],
-                                           (const uint64_t *)d_qoff, (const uint64_t *)d_toff, (uint8_t *)d_q,
-                                           (const uint8_t *)d_t, d_bad, mode, ends);
-            if (st != HY_OK) return st;
-            st = run_items<Single32, PAIR_G>(ctx, pp[1], PS_RES32, PS_BND32, qlen[1], ib[1], n_items[1], cols[1],
-                                             (const uint64_t *)d_qoff, (const uint64_t *)d_toff, (uint8_t *)d_q,
-                                             (const uint8_t *)d_t, d_bad, mode, ends);
-            if (st != HY_OK) return st;
+            hy_status s2 = run_items<Pair16H, PAIR_G>(ctx, pp[0], PS_RES16, PS_BND16, cs.qlen[0], ib[0], cs.n_items[0],
+                                                      cs.cols[0], (const uint64_t *)d_qoff, (const uint64_t *)d_toff,
+                                                      (uint8_t *)d_q, (const uint8_t *)d_t, d_bad, mode, ends);
+            if (s2 != HY_OK) return s2;
+            s2 = run_items<Single32, PAIR_G>(ctx, pp[1], PS_RES32, PS_BND32, cs.qlen[1], ib[1], cs.n_items[1],
+                                             cs.cols[1], (const uint64_t *)d_qoff, (const uint64_t *)d_toff,
+                                             (uint8_t *)d_q, (const uint8_t *)d_t, d_bad, mode, ends);
+            if (s2 != HY_OK) return s2;
             HY_CK(cudaEventRecord(ctx.ev[2 * c + 1], ctx.stream));
             if (h_cm && tb) {
                 // This chunk's column maxima back while the next chunks run (a long pair's are
@@ -901,9 +921,35 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
                                       cudaMemcpyDeviceToHost, ctx.d2h_stream));
             }
             HY_CK(cudaEventRecord(ctx.ev[2 * n_chunks + c], ctx.d2h_stream));
-            ib[0] += n_items[0];
-            ib[1] += n_items[1];
+            ib[0] += cs.n_items[0];
+            ib[1] += cs.n_items[1];
+            return fail(HY_OK);
+        };
+        // Chunk c is sorted and packed on the host threads while the copier stages chunk c - 1's
+        // residues; chunk c - 1 then goes to the device and chunk c's staging starts.
+        if (!hs.copier) hs.copier.reset(new AsyncCopy(std::max(2u, std::thread::hardware_concurrency() / 2)));
+        AsyncCopy &copier = *hs.copier;
+        struct CopierWait {  // no return leaves a copy running into a staging slot
+            AsyncCopy &cp;
+            ~CopierWait() { cp.wait(); }
+        } copier_wait{copier};
+        ChunkState cur{}, pend{};
+        bool have_pend = false;
+        auto flush = [&]() -> hy_status {
+            const auto tw = clock::now();
+            copier.wait();
+            ctx.phase_ms[2] += since(tw);
+            return issue(pend);
+        };
+        for (uint64_t c = 0; c < n_chunks; ++c) {
+            if ((st = prep(c, cur)) != HY_OK) return st;
+            if (have_pend && (st = flush()) != HY_OK) return st;
+            copier.start(cur.slot, q_res + q_off[cur.a], q_pinned ? 0 : cur.qb, cur.slot + cur.qb,
+                         t_res + t_off[cur.a], t_pinned ? 0 : cur.tb);
+            pend = cur;
+            have_pend = true;
         }
+        if (have_pend && (st = flush()) != HY_OK) return st;
         // The long pairs, once every chunk's queries are on the device (the compute stream has
         // waited for each chunk's copies).
         if (!run_long.empty()) {

@@ -334,8 +334,9 @@ hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint
  * stripe kernel) and the wall time of the whole call. */
 hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
 /* Phases of this thread's last hy_align_pairs call, in ms (no reference counterpart): up to n of
- * {the host lengths pass and routing, host sort and item packing (summed over chunks), host staging
- * copies (summed), the chunk pipeline (wall time to the device's end, overlapping the two before),
+ * {the host lengths pass and routing, host sort and item packing (summed over chunks), waits for the
+ * staging copies (which run on their own threads beside the next chunk's sort and packing), the
+ * chunk pipeline (wall time to the device's end, overlapping the two before),
  * results back, host waits for a staging slot, host copies of the column maxima into the caller's
  * array (hy_align_pairs_position_max)}. The last call of either entry point. */
 hy_status hy_align_pairs_phases(double *ms, uint32_t n);
