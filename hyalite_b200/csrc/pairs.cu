@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <memory>
 #include <thread>
 #include <vector>
@@ -161,8 +162,75 @@ struct PairsHost {
     HostArr<uint32_t> ord[2], ord_tmp, start, qlen[4];  // qlen: two chunks x two arithmetics
     HostArr<uint64_t> keys[2], keys_tmp;
     std::vector<std::vector<uint64_t>> count;  // radix histograms, one per host thread
-    // Copies a chunk's residues into its staging slot while the next chunk is sorted and packed.
-    std::unique_ptr<AsyncCopy> copier;
+    // Copies a chunk's residues into its staging slot while the next chunk is sorted and packed;
+    // the second copies column maxima back into the caller's array.
+    std::unique_ptr<AsyncCopy> copier, cm_copier;
+};
+
+// Position maxima into a pageable caller array over several chunks: a thread of its own waits for
+// each issued chunk's column maxima to reach the pinned copy and moves them into the caller's
+// array while the calling thread prepares and issues later chunks.
+class ColmaxDrainer {
+  public:
+    ColmaxDrainer(int device, uint64_t n_chunks, AsyncCopy &cp, const std::vector<cudaEvent_t> &ev,
+                  uint64_t ev_base, std::function<void(uint64_t, uint64_t *, uint64_t *)> range,
+                  int32_t *dst, const int32_t *src)
+        : n_(n_chunks), cp_(cp) {
+        th_ = std::thread([=, &ev] {
+            cudaSetDevice(device);
+            for (uint64_t c = 0; c < n_; ++c) {
+                {
+                    std::unique_lock<std::mutex> lk(m_);
+                    cv_.wait(lk, [&] { return stop_ || issued_ > (int64_t)c; });
+                    if (stop_ && issued_ <= (int64_t)c) return;
+                }
+                if (cudaEventSynchronize(ev[ev_base + c]) != cudaSuccess) {
+                    cudaGetLastError();
+                    failed_ = true;
+                    return;
+                }
+                const auto t0 = std::chrono::steady_clock::now();
+                uint64_t x0, x1;
+                range(c, &x0, &x1);
+                cp_.start((uint8_t *)(dst + x0), (const uint8_t *)(src + x0), 4 * (x1 - x0), nullptr, nullptr, 0);
+                cp_.wait();
+                ms_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            }
+        });
+    }
+    // Chunk c's copy back is enqueued (its event recorded).
+    void issued(uint64_t c) {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            issued_ = (int64_t)c + 1;
+        }
+        cv_.notify_one();
+    }
+    // Waits for the thread (after every chunk, or, on an early return, after the issued ones).
+    double join(bool *ok) {
+        if (th_.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                stop_ = true;
+            }
+            cv_.notify_one();
+            th_.join();
+        }
+        if (ok) *ok = !failed_;
+        return ms_;
+    }
+    ~ColmaxDrainer() { join(nullptr); }
+
+  private:
+    const uint64_t n_;
+    AsyncCopy &cp_;
+    std::thread th_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    int64_t issued_ = 0;
+    bool stop_ = false;
+    std::atomic<bool> failed_{false};
+    double ms_ = 0.0;
 };
 
 // One chunk of pairs between its host preparation and its issue to the device.
@@ -803,6 +871,17 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
         HY_CK(cudaMemcpyAsync(d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, ctx.stream));
         uint64_t ib[2] = {0, 0};
+        std::unique_ptr<ColmaxDrainer> drainer;
+        if (h_cm && !cm_direct && n_chunks > 1) {
+            if (!hs.cm_copier) hs.cm_copier.reset(new AsyncCopy(std::max(2u, std::thread::hardware_concurrency() / 2)));
+            drainer.reset(new ColmaxDrainer(
+                dev, n_chunks, *hs.cm_copier, ctx.ev, 2 * n_chunks,
+                [&](uint64_t c, uint64_t *x0, uint64_t *x1) {
+                    *x0 = t_off[chunk_at(c)] - t_off[0];
+                    *x1 = t_off[chunk_at(c + 1)] - t_off[0];
+                },
+                pc.colmax, h_cm));
+        }
         // Host side of chunk c: its pairs partitioned, sorted and packed into items, written with
         // its offsets to its staging slot (the residues follow on the copier).
         auto prep = [&](uint64_t c, ChunkState &cs) -> hy_status {
@@ -921,6 +1000,7 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
                                       cudaMemcpyDeviceToHost, ctx.d2h_stream));
             }
             HY_CK(cudaEventRecord(ctx.ev[2 * n_chunks + c], ctx.d2h_stream));
+            if (drainer) drainer->issued(c);
             ib[0] += cs.n_items[0];
             ib[1] += cs.n_items[1];
             return fail(HY_OK);
@@ -982,8 +1062,13 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
         HY_CK(ctx.get_pinned(PAIR_SLOTS, sizeof(int32_t) * out_words, &h_stage));
         HY_CK(cudaMemcpyAsync(h_stage, d_out, sizeof(int32_t) * out_words, cudaMemcpyDeviceToHost, ctx.stream));
         if (h_cm && cm_direct) HY_CK(cudaStreamSynchronize(ctx.d2h_stream));
-        if (h_cm && !cm_direct) {
-            // Chunks' column maxima into the caller's array as they arrive.
+        if (drainer) {
+            bool ok = true;
+            ctx.phase_ms[6] += drainer->join(&ok);
+            drainer.reset();
+            if (!ok) return fail(HY_ERR_CUDA);
+        } else if (h_cm && !cm_direct) {
+            // The chunk's column maxima into the caller's array.
             for (uint64_t c = 0; c < n_chunks; ++c) {
                 HY_CK(cudaEventSynchronize(ctx.ev[2 * n_chunks + c]));
                 const auto tc = clock::now();
