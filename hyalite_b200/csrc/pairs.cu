@@ -662,6 +662,92 @@ struct PosTiming {
 };
 static thread_local PosTiming g_pos_timing;
 
+// The pairs' routing from their lengths alone, chunked over the host threads: each pair's width
+// proof (int16x2 or int32 lanes) and whether it is a long single pair for the stripe kernel, into
+// route[k]. Each chunk stops at its own first failure, and the batch's first length failure is
+// that of the first chunk that has one. A few long pairs (the single-pair path) take the
+// score-only stripe kernel, every 128 query rows on their own warp; many keep the packed pair
+// kernels, whose throughput is higher once the whole GPU is busy. The host checks the long pairs'
+// symbols (the device checks the others while packing them).
+struct LengthsPlan {
+    uint64_t n_len = 0;          // pairs before the first length failure
+    hy_status len_st = HY_OK;    // that failure's error and detail
+    int64_t len_d0 = 0;
+    uint64_t n_part[2] = {0, 0};  // packed pairs of each lane arithmetic (long pairs apart)
+    bool use_long = false;       // the long pairs take the stripe kernel
+    std::vector<uint32_t> run_long;  // the long pairs it runs: those before the first bad one
+    uint64_t n_long_bad = 0;     // the first long pair with a symbol out of range (n_pairs: none)
+};
+
+static LengthsPlan plan_lengths(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
+                                const uint64_t *t_off, uint64_t n_pairs, int mode, int32_t min_e,
+                                int32_t max_e, int32_t gap_open, int32_t gap_ext, uint64_t alphabet_len,
+                                uint8_t *route) {
+    LengthsPlan lp;
+    const unsigned nt = host_threads(n_pairs, 1 << 15);
+    struct LenPart {
+        uint64_t first_bad = ~0ull;
+        hy_status st = HY_OK;
+        int64_t d0 = 0;
+        uint64_t n[2] = {0, 0};
+        std::vector<uint32_t> longs;
+    };
+    std::vector<LenPart> parts(nt);
+    const uint64_t per = (n_pairs + nt - 1) / nt;
+    parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
+        for (uint64_t c = ca; c < ce; ++c) {
+            LenPart &pt = parts[c];
+            const uint64_t a = c * per, e = std::min(n_pairs, a + per);
+            for (uint64_t k = a; k < e; ++k) {
+                const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
+                const int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, ql, tl);
+                if (narrowest_width(b) < 0 || ql >= (1u << 30) || tl >= (1u << 31)) {
+                    pt.st = narrowest_width(b) < 0 ? HY_ERR_SCORE_RANGE_TOO_WIDE : HY_ERR_UNSUPPORTED;
+                    pt.d0 = narrowest_width(b) < 0 ? b : 0;
+                    pt.first_bad = k;
+                    break;
+                }
+                uint8_t r = device_fits_i16(b, gap_open) ? 0 : PAIR_I32;
+                if (tb_long_pair(ql, tl)) {
+                    r |= PAIR_LONG;
+                    pt.longs.push_back((uint32_t)k);
+                }
+                route[k] = r;
+                ++pt.n[r & PAIR_I32];
+            }
+        }
+    });
+    lp.n_len = n_pairs;
+    std::vector<uint32_t> olong;
+    for (LenPart &pt : parts) {
+        olong.insert(olong.end(), pt.longs.begin(), pt.longs.end());
+        lp.n_part[0] += pt.n[0];
+        lp.n_part[1] += pt.n[1];
+        if (pt.st != HY_OK) {
+            lp.n_len = pt.first_bad;
+            lp.len_st = pt.st;
+            lp.len_d0 = pt.d0;
+            break;
+        }
+    }
+    lp.n_long_bad = n_pairs;
+    uint64_t stripes = 0;
+    for (uint32_t k : olong) stripes += tb_long_pair_stripes(q_off[k + 1] - q_off[k]);
+    if (stripes > LONG_PAIR_MAX_STRIPES) olong.clear();
+    for (uint32_t k : olong) {
+        if (first_bad_symbol(q_res + q_off[k], q_off[k + 1] - q_off[k], alphabet_len) >= 0 ||
+            first_bad_symbol(t_res + t_off[k], t_off[k + 1] - t_off[k], alphabet_len) >= 0) {
+            lp.n_long_bad = k;
+            break;
+        }
+        lp.run_long.push_back(k);
+    }
+    lp.use_long = !olong.empty();
+    if (lp.use_long)
+        for (uint32_t k : olong) --lp.n_part[route[k] & PAIR_I32];
+    return lp;
+}
+
 static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const uint8_t *t_res,
                            const uint64_t *t_off, uint64_t n_pairs, const int32_t *matrix,
                            uint64_t alphabet_len, int32_t gap_open, int32_t gap_ext, hy_mode mode,
@@ -689,83 +775,13 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
     const int32_t min_e = *std::min_element(matrix, matrix + alphabet_len * alphabet_len);
     const int32_t max_e = *std::max_element(matrix, matrix + alphabet_len * alphabet_len);
 
-    // The lengths pass, chunked over the host threads: each pair's width proof and route; each
-    // chunk stops at its own first failure, and the batch's first length failure is that of the
-    // first chunk that has one.
-    const unsigned nt = host_threads(n_pairs, 1 << 15);
-    struct LenPart {
-        uint64_t first_bad = ~0ull;
-        hy_status st = HY_OK;
-        int64_t d0 = 0;
-        uint64_t n[2] = {0, 0};
-        std::vector<uint32_t> longs;
-    };
-    std::vector<LenPart> parts(nt);
-    uint8_t *route = hs.route.get(n_pairs);
-    {
-        const uint64_t per = (n_pairs + nt - 1) / nt;
-        parallel_for(nt, 1, [&](uint64_t ca, uint64_t ce, unsigned) {
-            for (uint64_t c = ca; c < ce; ++c) {
-                LenPart &pt = parts[c];
-                const uint64_t a = c * per, e = std::min(n_pairs, a + per);
-                for (uint64_t k = a; k < e; ++k) {
-                    const uint64_t ql = q_off[k + 1] - q_off[k], tl = t_off[k + 1] - t_off[k];
-                    const int64_t b = magnitude_bound(mode, min_e, max_e, gap_open, gap_ext, ql, tl);
-                    if (narrowest_width(b) < 0 || ql >= (1u << 30) || tl >= (1u << 31)) {
-                        pt.st = narrowest_width(b) < 0 ? HY_ERR_SCORE_RANGE_TOO_WIDE : HY_ERR_UNSUPPORTED;
-                        pt.d0 = narrowest_width(b) < 0 ? b : 0;
-                        pt.first_bad = k;
-                        break;
-                    }
-                    uint8_t r = device_fits_i16(b, gap_open) ? 0 : PAIR_I32;
-                    if (tb_long_pair(ql, tl)) {
-                        r |= PAIR_LONG;
-                        pt.longs.push_back((uint32_t)k);
-                    }
-                    route[k] = r;
-                    ++pt.n[r & PAIR_I32];
-                }
-            }
-        });
-    }
-    uint64_t n_len = n_pairs;  // pairs before the first length failure
-    hy_status len_st = HY_OK;
-    int64_t len_d0 = 0;
-    uint64_t n_part[2] = {0, 0};
-    std::vector<uint32_t> olong;
-    for (LenPart &pt : parts) {
-        olong.insert(olong.end(), pt.longs.begin(), pt.longs.end());
-        n_part[0] += pt.n[0];
-        n_part[1] += pt.n[1];
-        if (pt.st != HY_OK) {
-            n_len = pt.first_bad;
-            len_st = pt.st;
-            len_d0 = pt.d0;
-            break;
-        }
-    }
-    // A few long pairs (the single-pair path) take the score-only stripe kernel: every 128 query
-    // rows on their own warp. Many long pairs keep the packed pair kernels, whose throughput is
-    // higher once the whole GPU is busy. The host checks the long pairs' symbols (the device checks
-    // the others while packing them).
-    uint64_t n_long_bad = n_pairs;  // the first long pair with a symbol out of range
-    std::vector<uint32_t> run_long;
-    {
-        uint64_t stripes = 0;
-        for (uint32_t k : olong) stripes += tb_long_pair_stripes(q_off[k + 1] - q_off[k]);
-        if (stripes > LONG_PAIR_MAX_STRIPES) olong.clear();
-        for (uint32_t k : olong) {
-            if (first_bad_symbol(q_res + q_off[k], q_off[k + 1] - q_off[k], alphabet_len) >= 0 ||
-                first_bad_symbol(t_res + t_off[k], t_off[k + 1] - t_off[k], alphabet_len) >= 0) {
-                n_long_bad = k;
-                break;
-            }
-            run_long.push_back(k);
-        }
-    }
-    const bool use_long = !olong.empty();
-    if (use_long)
-        for (uint32_t k : olong) --n_part[route[k] & PAIR_I32];
+    LengthsPlan lp = plan_lengths(q_res, q_off, t_res, t_off, n_pairs, mode, min_e, max_e, gap_open, gap_ext,
+                                  alphabet_len, hs.route.get(n_pairs));
+    const uint8_t *route = hs.route.get(n_pairs);
+    const uint64_t n_len = lp.n_len, n_long_bad = lp.n_long_bad;
+    const bool use_long = lp.use_long;
+    const uint64_t *n_part = lp.n_part;
+    const std::vector<uint32_t> &run_long = lp.run_long;
     ctx.phase_ms[0] = since(t_call);
 
     uint32_t dev_bad = NO_INDEX;  // the first pair whose symbols the device found out of range
@@ -1113,8 +1129,8 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             d[0] = bq >= 0 ? bq : bt;
             d[1] = (int64_t)alphabet_len;
         } else {
-            first = len_st;
-            d[0] = len_d0;
+            first = lp.len_st;
+            d[0] = lp.len_d0;
         }
         if (failed_pair) *failed_pair = n_ok;
     }
