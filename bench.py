@@ -728,8 +728,8 @@ def run_pairs(args):
     clk = clocks.stop()
     # The same calls with the reads and windows already in page-locked memory (a caller that keeps
     # them pinned): the device copies the residues from where they are, with no staging copy.
-    pq = torch.empty(len(q_res), dtype=torch.uint8, pin_memory=True).numpy()
-    pt = torch.empty(len(t_res), dtype=torch.uint8, pin_memory=True).numpy()
+    pq = hy.pinned_empty(len(q_res), np.uint8)
+    pt = hy.pinned_empty(len(t_res), np.uint8)
     pq[:] = q_res
     pt[:] = t_res
     hy.align_pairs_arrays(pq, q_off, pt, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
@@ -922,9 +922,9 @@ def run_position_max(args):
     clk = clocks.stop()
     # The same calls with page-locked inputs and column-maxima array (a caller that keeps them
     # pinned): no staging copy in, the maxima copied from the device straight into the array.
-    pq = torch.empty(len(q_res), dtype=torch.uint8, pin_memory=True).numpy()
-    pt = torch.empty(len(t_res), dtype=torch.uint8, pin_memory=True).numpy()
-    pcm = torch.empty(len(cm_buf), dtype=torch.int32, pin_memory=True).numpy()
+    pq = hy.pinned_empty(len(q_res), np.uint8)
+    pt = hy.pinned_empty(len(t_res), np.uint8)
+    pcm = hy.pinned_empty(len(cm_buf), np.int32)
     pq[:] = q_res
     pt[:] = t_res
     hy.align_pairs_position_max_arrays(pq, q_off, pt, t_off, scoring, 20, pcm)

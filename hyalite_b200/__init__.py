@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 import os
+import weakref
 from dataclasses import dataclass
 from typing import Iterable, List, Optional, Sequence
 
@@ -827,6 +828,19 @@ def align_pairs_timing():
     k, c = C.c_double(), C.c_double()
     _check(lib.hy_align_pairs_timing(C.byref(k), C.byref(c)))
     return float(k.value), float(c.value)
+
+
+def pinned_empty(n: int, dtype=np.uint8) -> np.ndarray:
+    """An uninitialised numpy array of n elements in page-locked host memory (hy_host_alloc), freed
+    when the last view of it goes. align_pairs / align_pairs_position_max copy such residues and
+    column-maxima arrays from and to where they are, without staging copies."""
+    dt = np.dtype(dtype)
+    nbytes = max(1, int(n) * dt.itemsize)
+    ptr = C.c_void_p()
+    _check(lib.hy_host_alloc(nbytes, C.byref(ptr)))
+    buf = (C.c_uint8 * nbytes).from_address(ptr.value)
+    weakref.finalize(buf, lib.hy_host_free, ptr.value)
+    return np.frombuffer(buf, dtype=dt, count=int(n))
 
 
 def align_pairs_phases():

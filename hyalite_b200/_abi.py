@@ -118,6 +118,8 @@ SIGNATURES = {
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
     "hy_align_pairs_timing": (_st, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "hy_align_pairs_phases": (_st, [C.POINTER(C.c_double), C.c_uint32]),
+    "hy_host_alloc": (_st, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    "hy_host_free": (_st, [C.c_void_p]),
     "hy_batch_create": (_st, [C.POINTER(_vp), C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_vp)]),
     "hy_batch_destroy": (None, [_vp]),
     "hy_scan_batch": (_st, [_vp, C.c_uint32, _u32p, _u8p, _u64p, C.POINTER(HyHit), _u32p]),

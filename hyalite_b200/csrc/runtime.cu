@@ -932,6 +932,18 @@ hy_status hy_scratch_profile_read(hy_scratch *sc, double kernel_ms[3], uint64_t 
     return fail(HY_OK);
 }
 
+hy_status hy_host_alloc(uint64_t bytes, void **out) {
+    if (!out) return fail(HY_ERR_INVALID_ARGUMENT);
+    *out = nullptr;
+    HY_CK(cudaMallocHost(out, std::max<uint64_t>(bytes, 1)));
+    return fail(HY_OK);
+}
+
+hy_status hy_host_free(void *p) {
+    if (p) HY_CK(cudaFreeHost(p));
+    return fail(HY_OK);
+}
+
 hy_status hy_query_validate(const hy_db *db, const uint8_t *query, uint64_t qlen) {
     if (!db) return fail(HY_ERR_INVALID_ARGUMENT);
     return check_query(db, query, qlen);

@@ -315,6 +315,12 @@ hy_status hy_server_wait(hy_server *server, uint64_t request_id, double timeout_
 /* Counters and latency percentiles since the last reset (reset != 0 clears them). */
 hy_status hy_server_stats_read(hy_server *server, int reset, hy_server_stats *out);
 
+/* Page-locked host memory (no reference counterpart): buffers from hy_host_alloc given to
+ * hy_align_pairs / hy_align_pairs_position_max as residues or column maxima are copied from and to
+ * where they are, without the calls' staging copies. Freed with hy_host_free. */
+hy_status hy_host_alloc(uint64_t bytes, void **out);
+hy_status hy_host_free(void *p);
+
 /* ---- pairwise batch (src/kernel.rs:429-452) -------------------------------------------------- */
 
 /* align_pairs: pair p is (q_res[q_off[p]..q_off[p+1]], t_res[t_off[p]..t_off[p+1]]). Each pair is

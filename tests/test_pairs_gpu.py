@@ -261,8 +261,6 @@ def test_pinned_buffers_give_the_same_results():
     """Residues (and, for position maxima, the column-maxima array) in page-locked memory are
     copied from and to where they are, with no staging: results identical to pageable buffers,
     across several chunks, with a failure in a later chunk."""
-    import torch
-
     rng = np.random.default_rng(31)
     n = 150_000
     qs = [rng.integers(0, 4, int(rng.integers(0, 40))) for _ in range(n)]
@@ -275,7 +273,7 @@ def test_pinned_buffers_give_the_same_results():
     t_res, t_off = _concat(ts)
 
     def pinned(a):
-        p = torch.empty(len(a), dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True).numpy()
+        p = hy.pinned_empty(len(a), a.dtype)
         p[:] = a
         return p
 
