@@ -37,9 +37,12 @@ constexpr int PAIR_R32 = 16;
 constexpr size_t PAIR_SMEM_LIMIT = 200 * 1024;
 // Largest global scratch for group profiles that do not fit in shared memory, per launch.
 constexpr size_t PAIR_GPROF_BYTES = 256ull << 20;
-// Chunks of input pairs the pipeline runs in: at most this many, each at least PAIR_CHUNK_MIN pairs.
+// Chunks of input pairs the pipeline runs in: up to PAIR_MAX_CHUNKS of at least PAIR_CHUNK_MIN
+// pairs each, and more when that would put over PAIR_CHUNK_BYTES of residues in one chunk (the
+// pinned staging holds three chunks).
 constexpr uint64_t PAIR_MAX_CHUNKS = 16;
 constexpr uint64_t PAIR_CHUNK_MIN = 1 << 16;
+constexpr uint64_t PAIR_CHUNK_BYTES = 512ull << 20;
 // Pinned staging slots the chunks rotate through.
 constexpr int PAIR_SLOTS = 3;
 // Most warps (128-row stripes) the long pairs of one call may take on the stripe kernel.
@@ -804,7 +807,10 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             for (cudaEvent_t &e : ctx.slot_ev) HY_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
         const uint64_t L = n_len;
-        const uint64_t n_chunks = std::max<uint64_t>(1, std::min<uint64_t>(PAIR_MAX_CHUNKS, L / PAIR_CHUNK_MIN));
+        const uint64_t res_bytes = (q_off[L] - q_off[0]) + (t_off[L] - t_off[0]);
+        const uint64_t n_chunks = std::min<uint64_t>(
+            L, std::max<uint64_t>({1, std::min<uint64_t>(PAIR_MAX_CHUNKS, L / PAIR_CHUNK_MIN),
+                                   (res_bytes + PAIR_CHUNK_BYTES - 1) / PAIR_CHUNK_BYTES}));
         auto chunk_at = [&](uint64_t c) { return L * c / n_chunks; };
         while (ctx.ev.size() < 3 * n_chunks + 2) {
             cudaEvent_t e;
