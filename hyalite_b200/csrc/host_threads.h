@@ -123,8 +123,9 @@ class HostPool {
 };
 
 // Copies up to two byte ranges on threads of its own while the caller goes on, one job at a time:
-// start() hands the ranges over and returns, wait() returns once they are copied. In a process made
-// by fork() after the threads started, start() copies synchronously (the threads are not there).
+// start() hands the ranges over and returns, wait() returns once they are copied (start_widen():
+// one range of int16 values widened to int32). In a process made by fork() after the threads
+// started, both work synchronously (the threads are not there).
 class AsyncCopy {
   public:
     explicit AsyncCopy(unsigned threads) : pid_(getpid()) {
@@ -148,16 +149,14 @@ class AsyncCopy {
             if (n1) memcpy(d1, s1, n1);
             return;
         }
-        Job j{d0, s0, n0, d1, s1, n1, 0, 0};
-        j.pieces = (n0 + n1 + PIECE - 1) / PIECE;
-        {
-            std::lock_guard<std::mutex> lk(m_);
-            j.gen = ++gen_;
-            job_ = j;
-            left_.store(j.pieces);
-            next_.store(j.gen << 32);
+        submit(Job{d0, s0, n0, d1, s1, n1, 0, 0, false});
+    }
+    void start_widen(int32_t *d, const int16_t *src, uint64_t n) {
+        if (getpid() != pid_) {
+            widen(d, src, n);
+            return;
         }
-        if (j.pieces) cv_.notify_all();
+        submit(Job{(uint8_t *)d, (const uint8_t *)src, 2 * n, nullptr, nullptr, 0, 0, 0, true});
     }
     void wait() {
         std::unique_lock<std::mutex> lk(m_);
@@ -169,13 +168,28 @@ class AsyncCopy {
     struct Job {
         uint8_t *d0;
         const uint8_t *s0;
-        uint64_t n0;
+        uint64_t n0;  // bytes (of the int16 source when widening)
         uint8_t *d1;
         const uint8_t *s1;
         uint64_t n1;
         uint64_t pieces;
         uint64_t gen;
+        bool widen;
     };
+    static void widen(int32_t *d, const int16_t *src, uint64_t n) {
+        for (uint64_t i = 0; i < n; ++i) d[i] = src[i];
+    }
+    void submit(Job j) {
+        j.pieces = (j.n0 + j.n1 + PIECE - 1) / PIECE;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            j.gen = ++gen_;
+            job_ = j;
+            left_.store(j.pieces);
+            next_.store(j.gen << 32);
+        }
+        if (j.pieces) cv_.notify_all();
+    }
     void loop() {
         uint64_t seen = 0;
         for (;;) {
@@ -193,10 +207,13 @@ class AsyncCopy {
                 const uint64_t i = cur & 0xffffffffu;
                 if (i >= j.pieces) break;
                 if (!next_.compare_exchange_weak(cur, cur + 1)) continue;
-                // Piece i of the two ranges laid end to end.
+                // Piece i of the two ranges laid end to end (whole int16 values when widening).
                 const uint64_t a = i * PIECE, e = std::min(j.n0 + j.n1, a + PIECE);
-                if (a < j.n0) memcpy(j.d0 + a, j.s0 + a, std::min(e, j.n0) - a);
-                if (e > j.n0) {
+                if (j.widen)
+                    widen((int32_t *)j.d0 + a / 2, (const int16_t *)j.s0 + a / 2, (e - a) / 2);
+                else if (a < j.n0)
+                    memcpy(j.d0 + a, j.s0 + a, std::min(e, j.n0) - a);
+                if (!j.widen && e > j.n0) {
                     const uint64_t b = std::max(a, j.n0) - j.n0;
                     memcpy(j.d1 + b, j.s1 + b, e - j.n0 - b);
                 }

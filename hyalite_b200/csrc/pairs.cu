@@ -91,6 +91,7 @@ enum PairSlot {
     PS_ITOFF16,  // position maxima: items' target offsets per half
     PS_ITOFF32,
     PS_COLMAX,   // position maxima: column maxima at the targets' offsets
+    PS_CM16,     // position maxima: one chunk's column maxima narrowed for the copy back
     PS_COUNT
 };
 
@@ -177,9 +178,9 @@ class ColmaxDrainer {
   public:
     ColmaxDrainer(int device, uint64_t n_chunks, AsyncCopy &cp, const std::vector<cudaEvent_t> &ev,
                   uint64_t ev_base, std::function<void(uint64_t, uint64_t *, uint64_t *)> range,
-                  int32_t *dst, const int32_t *src)
+                  int32_t *dst, const int32_t *src, const std::vector<char> &narrow)
         : n_(n_chunks), cp_(cp) {
-        th_ = std::thread([=, &ev] {
+        th_ = std::thread([=, &ev, &narrow] {
             cudaSetDevice(device);
             for (uint64_t c = 0; c < n_; ++c) {
                 {
@@ -195,7 +196,11 @@ class ColmaxDrainer {
                 const auto t0 = std::chrono::steady_clock::now();
                 uint64_t x0, x1;
                 range(c, &x0, &x1);
-                cp_.start((uint8_t *)(dst + x0), (const uint8_t *)(src + x0), 4 * (x1 - x0), nullptr, nullptr, 0);
+                // A narrowed chunk's int16 maxima sit at the start of its region of the pinned copy.
+                if (narrow[c])
+                    cp_.start_widen(dst + x0, (const int16_t *)(src + x0), x1 - x0);
+                else
+                    cp_.start((uint8_t *)(dst + x0), (const uint8_t *)(src + x0), 4 * (x1 - x0), nullptr, nullptr, 0);
                 cp_.wait();
                 ms_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             }
@@ -246,6 +251,7 @@ struct ChunkState {
     size_t n_items[2];
     uint64_t cols[2];
     uint32_t *qlen[2];
+    bool narrow;  // position maxima: the chunk's column maxima go back as int16
 };
 
 static thread_local PairsHost g_host;
@@ -629,6 +635,13 @@ static hy_status run_items(PairsContext &ctx, PairParams p, int res_slot, int bn
     return fail(HY_OK);
 }
 
+// One chunk's column maxima narrowed to int16 for the copy back: every pair of the chunk proved
+// int16 lanes, so every maximum (at most 32767 - gap_open) fits.
+__global__ void narrow_colmax_kernel(const int32_t *src, int16_t *dst, uint64_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (int16_t)src[i];
+}
+
 // align_pair_position_max's BestHit and score2 for pairs [0, n) from their column maxima at
 // colmax + t_off[k] (position_hits). One thread per pair.
 __global__ void pos_hits_kernel(uint64_t n, const uint64_t *t_off, const int32_t *colmax, int32_t *scores,
@@ -894,7 +907,15 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
                               cudaMemcpyHostToDevice, ctx.stream));
         uint64_t ib[2] = {0, 0};
         std::unique_ptr<ColmaxDrainer> drainer;
+        std::vector<char> chunk_narrow(n_chunks, 0);
+        int16_t *d_cm16 = nullptr;
         if (h_cm && !cm_direct && n_chunks > 1) {
+            uint64_t max_tb = 0;
+            for (uint64_t c = 0; c < n_chunks; ++c)
+                max_tb = std::max(max_tb, t_off[chunk_at(c + 1)] - t_off[chunk_at(c)]);
+            void *p16;
+            HY_CK(ctx.get(PS_CM16, sizeof(int16_t) * max_tb, &p16));
+            d_cm16 = (int16_t *)p16;
             if (!hs.cm_copier) hs.cm_copier.reset(new AsyncCopy(std::max(2u, std::thread::hardware_concurrency() / 2)));
             drainer.reset(new ColmaxDrainer(
                 dev, n_chunks, *hs.cm_copier, ctx.ev, 2 * n_chunks,
@@ -902,7 +923,7 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
                     *x0 = t_off[chunk_at(c)] - t_off[0];
                     *x1 = t_off[chunk_at(c + 1)] - t_off[0];
                 },
-                pc.colmax, h_cm));
+                pc.colmax, h_cm, chunk_narrow));
         }
         // Host side of chunk c: its pairs partitioned, sorted and packed into items, written with
         // its offsets to its staging slot (the residues follow on the copier).
@@ -967,6 +988,8 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             cs.s_qoff = (uint64_t *)(cs.slot + (cs.qb + cs.tb + 7) / 8 * 8);
             cs.s_toff = cs.s_qoff + (n + 1);
             cs.s_meta[0] = (ItemMeta *)(cs.s_toff + (n + 1));
+            // Every pair int16 and none on the stripe kernel: the maxima fit int16.
+            cs.narrow = d_cm16 != nullptr && cnt[1] == 0 && cnt[0] == n;
             for (int h = 0; h < 2; ++h) {
                 cs.n_items[h] = 0;
                 cs.cols[h] = 0;
@@ -1016,12 +1039,21 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             HY_CK(cudaEventRecord(ctx.ev[2 * c + 1], ctx.stream));
             if (h_cm && tb) {
                 // This chunk's column maxima back while the next chunks run (a long pair's are
-                // copied again once the stripe kernel has written them).
+                // copied again once the stripe kernel has written them), narrowed when they fit.
                 HY_CK(cudaStreamWaitEvent(ctx.d2h_stream, ctx.ev[2 * c + 1], 0));
-                HY_CK(cudaMemcpyAsync(h_cm + (t_off[a] - t_off[0]), d_colmax + t_off[a], sizeof(int32_t) * tb,
-                                      cudaMemcpyDeviceToHost, ctx.d2h_stream));
+                if (cs.narrow) {
+                    const int blocks = (int)std::min<uint64_t>((tb + 255) / 256, 148 * 8);
+                    narrow_colmax_kernel<<<blocks, 256, 0, ctx.d2h_stream>>>(d_colmax + t_off[a], d_cm16, tb);
+                    HY_CK(cudaGetLastError());
+                    HY_CK(cudaMemcpyAsync(h_cm + (t_off[a] - t_off[0]), d_cm16, sizeof(int16_t) * tb,
+                                          cudaMemcpyDeviceToHost, ctx.d2h_stream));
+                } else {
+                    HY_CK(cudaMemcpyAsync(h_cm + (t_off[a] - t_off[0]), d_colmax + t_off[a], sizeof(int32_t) * tb,
+                                          cudaMemcpyDeviceToHost, ctx.d2h_stream));
+                }
             }
             HY_CK(cudaEventRecord(ctx.ev[2 * n_chunks + c], ctx.d2h_stream));
+            chunk_narrow[c] = cs.narrow ? 1 : 0;
             if (drainer) drainer->issued(c);
             ib[0] += cs.n_items[0];
             ib[1] += cs.n_items[1];

@@ -1,7 +1,7 @@
 // Host-side checks of hyalite_b200/csrc/host_threads.h, built and run by tests/test_host_threads.py:
 // parallel_for covers every index exactly once (the worker pool repeatedly, from several threads
-// at once, and nested); AsyncCopy copies two ranges laid end to end, across many jobs, and in a
-// child process made by fork() after its threads started.
+// at once, and nested); AsyncCopy copies two ranges laid end to end and widens int16 to int32,
+// across many jobs, and in a child process made by fork() after its threads started.
 #include <sys/wait.h>
 
 #include <atomic>
@@ -59,6 +59,16 @@ int main() {
         CHECK(std::equal(s0.begin(), s0.begin() + n0, d0.begin()));
         CHECK(std::equal(s1.begin(), s1.begin() + n1, d1.begin()));
         CHECK(d0[n0] == 0 && d1[n1] == 0);  // nothing past the ranges
+    }
+    for (int r = 0; r < 20; ++r) {
+        const uint64_t n = rng() % (2u << 20);
+        std::vector<int16_t> src(n);
+        std::vector<int32_t> dst(n + 1, 77);
+        for (auto &x : src) x = (int16_t)rng();
+        copier.start_widen(dst.data(), src.data(), n);
+        copier.wait();
+        for (uint64_t i = 0; i < n; ++i) CHECK(dst[i] == (int32_t)src[i]);
+        CHECK(dst[n] == 77);
     }
     const pid_t child = fork();
     if (child == 0) {
