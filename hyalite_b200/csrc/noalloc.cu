@@ -14,6 +14,11 @@
 // the timeout flag is cleared at the start of each call and every other byte a call reads it has
 // first written. Calls whose kernels overlap on the GPU (two host threads, two streams) race on the
 // array and corrupt each other's results: callers must serialise them.
+//
+// The first call on each device does a one-time set-up: it looks up the array's device address and
+// loads every kernel the entry point launches (a lazily loaded kernel would otherwise allocate at
+// its first launch). That first call may therefore allocate, and it should be made before the
+// caller reserves all device memory and before any stream capture; later calls allocate nothing.
 #include <mutex>
 
 #include "db_internal.h"
@@ -32,12 +37,31 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 void *g_scratch_addr[MAX_DEVICES] = {};
 
+// Under CUDA's lazy module loading a kernel's code is loaded onto the device at its first launch,
+// and loading can allocate device memory. The set-up of each device therefore loads every kernel
+// this entry point can launch, so that no later call loads (or allocates) anything.
+template <class A, int G, int R>
+cudaError_t preload_arith() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, build_profile_kernel<A, G, R>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, scan_kernel<A, G, R, MODE_SW, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, scan_kernel<A, G, R, MODE_NW, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, scan_kernel<A, G, R, MODE_HW, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, scan_kernel<A, G, R, MODE_OV, false>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, scan_kernel<A, G, R, MODE_SHW, false>);
+    return e;
+}
+
+// Once per device, with that device current: the array's device address, and every kernel loaded.
 hy_status scratch_address(int device, uint8_t **out) {
     if (device < 0 || device >= MAX_DEVICES) return fail(HY_ERR_UNSUPPORTED);
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_scratch_addr[device]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e == cudaSuccess) e = preload_arith<Pair16, MAIN_G, MAIN_R16>();
+        if (e == cudaSuccess) e = preload_arith<PairTab16, MAIN_G, MAIN_R16>();
+        if (e == cudaSuccess) e = preload_arith<Single32, MAIN_G32, MAIN_R32>();
         if (e != cudaSuccess) {
             cudaGetLastError();
             return fail(HY_ERR_CUDA, e);

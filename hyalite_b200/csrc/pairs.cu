@@ -906,8 +906,10 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
         HY_CK(cudaMemcpyAsync(d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                               cudaMemcpyHostToDevice, ctx.stream));
         uint64_t ib[2] = {0, 0};
-        std::unique_ptr<ColmaxDrainer> drainer;
+        // Declared before the drainer, whose thread reads it: locals are destroyed in reverse
+        // order, so the thread is joined (on any early return) before this vector goes away.
         std::vector<char> chunk_narrow(n_chunks, 0);
+        std::unique_ptr<ColmaxDrainer> drainer;
         int16_t *d_cm16 = nullptr;
         if (h_cm && !cm_direct && n_chunks > 1) {
             uint64_t max_tb = 0;

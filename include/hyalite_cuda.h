@@ -3,8 +3,8 @@
  *
  * Plain pointers and sizes only; no CUDA or torch types cross this boundary (the one stream
  * accessor hands out an opaque pointer). Each declaration names the reference interface it
- * replaces (paths inside Psy-Fer/hyalite). The matching Rust-side `extern "C"` block a maintainer
- * would add is in INTEGRATION.md.
+ * replaces (paths inside Psy-Fer/hyalite), for the Rust-side `extern "C"` binding a maintainer
+ * adds over it.
  *
  * Threading (src/database.rs:1-7, tests/database.rs:136-176): an hy_db is immutable after
  * creation and may be shared by any number of host threads; an hy_scratch belongs to one thread
@@ -196,7 +196,11 @@ hy_status hy_scan_scores_device(const hy_db *db, hy_scratch *scratch, const uint
  * `stream` (a cudaStream_t, or NULL for the legacy default stream) and returns once the scores
  * are written. Calls share the array: calls whose kernels
  * overlap on the GPU race and must be serialised by the caller. The query's symbols must already
- * be validated (hy_query_validate); the current device must be the database's. */
+ * be validated (hy_query_validate); the current device must be the database's. The first call on
+ * each device does a one-time set-up (the array's device address, and loading every kernel this
+ * entry point launches, which CUDA's lazy module loading would otherwise do, allocating, at each
+ * kernel's first launch): make it before device memory is fully reserved and before any stream
+ * capture. Later calls allocate nothing. */
 hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_query, uint64_t qlen,
                                  int32_t *d_scores, void *stream);
 /* The checks hy_scan performs on a host query (length, then symbols). */
