@@ -10,8 +10,9 @@ sum over queries and targets of |q| * |t| per second.
 `value` is timed on the device (CUDA events on the scan's stream, inputs resident in HBM);
 `e2e` goes through the public host API (hy_scan: query host->device, hit device->host per call).
 Under torchrun each rank holds its own 500,000-sequence shard of an N-times larger database
-(weak scaling) and the per-shard best hits are all-gathered over NCCL and reduced with the
-reference's tie-break (highest score, then smallest global index).
+(weak scaling) through hyalite_b200.sharded.ShardedDatabase: the per-shard best hits are
+all-gathered over NCCL and reduced with the reference's tie-break (highest score, then smallest
+global index).
 
 --impl reference times the CPU baseline instead: a C++ restatement of hyalite's AVX2 backend
 (oracle/avx2_port.cpp) over all host threads, on a bounded sample of the same database.
@@ -115,25 +116,49 @@ def dist_setup():
     return world, rank, local
 
 
+def cpu_sample(residues, offsets, first, count):
+    """Sequences [first, first + count) of the database as (residues, offsets)."""
+    off = offsets[first: first + count + 1]
+    return residues[int(off[0]): int(off[-1])], off - off[0]
+
+
 def cpu_baseline_run(mat, residues, offsets, queries, sample_seqs, threads, steps=1, warmup=0):
-    """The AVX2 restatement over `threads` host threads on the first `sample_seqs` sequences;
-    returns (GCUPS, seconds per step, sample description)."""
+    """The AVX2 restatement over `threads` host threads: the queries against consecutive samples
+    of `sample_seqs` sequences (step k takes the k-th sample, wrapping over the database), each
+    sample held in slices so that every (query, slice) unit runs on the next free thread, longest
+    query first (no thread idles on a long query). Returns (GCUPS, seconds per step, sample
+    description, one-query-per-thread GCUPS on the first sample)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
-    off = offsets[: sample_seqs + 1]
-    res = residues[: int(off[-1])]
-    db = pyoracle.Avx2Db(res, off, mat, AL, GO, GE, 0, 1, max(len(q) for q in queries))
+    n = len(offsets) - 1
+    n_samples = max(1, n // sample_seqs)
+    mql = max(len(q) for q in queries)
     qlist = [list(map(int, q)) for q in queries]
-    cells = float(sum(len(q) for q in queries)) * float(off[-1])
-    for _ in range(warmup):
-        db.scan_many(qlist, threads)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        db.scan_many(qlist, threads)
-    dt = (time.perf_counter() - t0) / steps
-    return cells / dt / 1e9, dt, (f"{N_QUERIES} queries ({'/'.join(map(str, QUERY_LENGTHS))} aa, cycled) against the "
-                                  f"first {sample_seqs} of the {N_SEQS} sequences ({int(off[-1])} residues)")
+    qres = float(sum(len(q) for q in queries))
+    cells = secs = 0.0
+    per_thread = None
+    for k in range(warmup + steps):
+        first = (k % n_samples) * sample_seqs
+        res, off = cpu_sample(residues, offsets, first, sample_seqs)
+        db = pyoracle.Avx2SlicedDb(res, off, mat, AL, GO, GE, 0, 1, mql, n_slices=4 * threads)
+        t0 = time.perf_counter()
+        db.scan_stream(qlist, threads)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            cells += qres * float(off[-1])
+            secs += dt
+        if k == 0 and steps <= 2:
+            # The same sample with one query per thread (the reference's one Scratch per thread and
+            # a stream of whole queries): long queries leave the other threads idle.
+            whole = pyoracle.Avx2Db(res, off, mat, AL, GO, GE, 0, 1, mql)
+            t0 = time.perf_counter()
+            whole.scan_many(qlist, threads)
+            per_thread = qres * float(off[-1]) / (time.perf_counter() - t0) / 1e9
+    desc = (f"{len(queries)} queries ({'/'.join(map(str, QUERY_LENGTHS))} aa, cycled) against "
+            f"{min(steps, n_samples)} consecutive sample(s) of {sample_seqs} of the {n} sequences, "
+            f"{4 * threads} slices each, (query, slice) units over {threads} threads")
+    return cells / secs / 1e9, secs / steps, desc, per_thread
 
 
 def run_reference(args):
@@ -142,13 +167,15 @@ def run_reference(args):
         return
     mat, residues, offsets, queries = make_workload(args.seed, n_seqs=args.ref_seqs)
     threads = os.cpu_count() or 1
-    gcups, dt, sample = cpu_baseline_run(mat, residues, offsets, queries, args.ref_seqs, threads,
-                                         steps=args.steps, warmup=args.warmup)
+    gcups, dt, sample, _ = cpu_baseline_run(mat, residues, offsets, queries, args.ref_sample_seqs, threads,
+                                            steps=args.steps, warmup=args.warmup)
     line = {
         "impl": "reference", "metric": "GCUPS", "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "i8/i16/i32 lanes (AVX2)", "data": "synthetic",
-        "config": {"workload": "protein SW ScoreEnd scan, 500k log-normal sequences x 16 queries (100..5000), AVX2 port on a bounded sample", "parallelism": f"{threads} host threads"},
+        "config": {"workload": "protein SW ScoreEnd scan, 500k log-normal sequences x 16 queries (100..5000), "
+                               "AVX2 port on bounded samples of a 100,000-sequence subsample",
+                   "parallelism": f"{threads} host threads"},
         "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -170,11 +197,25 @@ def run_cuda(args):
     from hyalite_b200 import _abi
 
     lib = _abi.lib
+    # This rank's shard: block `rank` of an N-times larger database (global sequences
+    # [rank * n_seqs, (rank + 1) * n_seqs)), generated here from its own seed.
     mat, residues, offsets, queries = make_workload(args.seed + rank, n_seqs=N_SEQS)
     n_seqs = len(offsets) - 1
+
+    def configure(b):
+        return (b.scoring(hy.Scoring(AL, mat, GO, GE)).mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd)
+                .max_query_len(max(QUERY_LENGTHS)))
+
     t_build = time.perf_counter()
-    db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
-          .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(max(QUERY_LENGTHS)).build())
+    sdb = None
+    if world > 1:
+        from hyalite_b200 import sharded
+
+        sdb = sharded.ShardedDatabase.from_shard(residues, offsets, np.arange(n_seqs) + rank * n_seqs,
+                                                 world * n_seqs, configure)
+        db = sdb.db
+    else:
+        db = configure(hy.Database.builder().sequences_concat(residues, offsets)).build()
     build_s = time.perf_counter() - t_build
     sc = hy.Scratch(db)
     n16, n32 = db.partition()
@@ -195,17 +236,12 @@ def run_cuda(args):
             if st != 0:
                 raise hy.Error.from_status(st)
 
-    # This rank's shard is global sequences [rank * n_seqs, (rank + 1) * n_seqs).
-    local_to_global = torch.arange(n_seqs, dtype=torch.int64, device=f"cuda:{local}") + rank * n_seqs
-
     def gather_best(hits_dev):
         """The per-query best hits of all shards, merged on the device (one all_gather)."""
         if world == 1:
             return hits_dev
-        from hyalite_b200 import sharded
-
         with torch.cuda.stream(stream):
-            return sharded.all_gather_best(sharded.device_hit_rows(hits_dev, local_to_global))
+            return sdb.merge_device_hits(hits_dev)
 
     def barrier():
         if world > 1:
@@ -252,12 +288,7 @@ def run_cuda(args):
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        hits = [db.scan(sc, q) for q in host_queries]
-        if world > 1:
-            from hyalite_b200 import sharded
-
-            rows = sharded.hit_rows(hits, np.arange(n_seqs) + rank * n_seqs).to(f"cuda:{local}")
-            hits = sharded.all_gather_best(rows).cpu()
+        hits = [(sdb or db).scan(sc, q) for q in host_queries]
     e2e_s = time.perf_counter() - t0
     if world > 1:
         import torch.distributed as dist
@@ -292,8 +323,11 @@ def run_cuda(args):
         threads = os.cpu_count() or 1
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            g, dt, sample = cpu_baseline_run(mat, residues, offsets, queries, args.cpu_sample_seqs, threads)
-            cpu = {"value": g, "unit": "GCUPS", "cores": threads, "kind": "port", "sample": sample}
+            g, dt, sample, per_thread = cpu_baseline_run(mat, residues, offsets, queries, args.cpu_sample_seqs,
+                                                         threads)
+            cpu = {"value": g, "unit": "GCUPS", "cores": threads, "kind": "port", "sample": sample,
+                   "one_query_per_thread": {"value": per_thread, "unit": "GCUPS",
+                                            "form": "the same sample, each thread one whole query at a time"}}
         line = {
             "metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -326,6 +360,12 @@ def run_cuda(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_extras:
+            # The metric's other forms at their full sizes, one compact measurement each.
+            for key, fn in (("batched", extra_batched), ("served", extra_served), ("pairs", extra_pairs)):
+                t0 = time.perf_counter()
+                line[key] = fn(args.seed)
+                line[key]["run_s"] = round(time.perf_counter() - t0, 1)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -354,7 +394,7 @@ def make_reads_workload(seed: int, n_reads: int, n_queries: int, read_len: int =
         idx = np.where(deletion, j + (j >= p), np.where(insertion, j - (j > p), j))
         r = np.take_along_axis(win, idx, axis=1)
         r = np.where(insertion & (j == p), rng.integers(0, 4, (n, 1), dtype=np.uint8), r)
-        sub = rng.random((n, read_len)) < 0.01
+        sub = rng.integers(0, 100, (n, read_len), dtype=np.uint8) == 0  # 1% of the bases
         r = np.where(sub, (r + rng.integers(1, 4, (n, read_len), dtype=np.uint8)) % 4, r).astype(np.uint8)
         reads[lo:lo + n] = r
     offsets = np.arange(n_reads + 1, dtype=np.uint64) * read_len
@@ -449,6 +489,216 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+# ---- the metric's other forms, compact, for the default line -----------------------------------
+
+def _hit4(h):
+    return (int(h.score), int(h.db_index), None if h.query_end is None or h.query_end < 0 else int(h.query_end),
+            None if h.target_end is None or h.target_end < 0 else int(h.target_end))
+
+
+def _oracle_best(ref, query, threads):
+    """The reference scan's best hit from the oracle's per-target results: the highest score, the
+    smallest db index on ties, the winner's own ends (src/database.rs:117-130, 186-197)."""
+    best = None
+    for h in ref.scan_all(query, threads=threads):
+        if best is None or h[0] > best[0]:
+            best = h
+    return best
+
+
+def extra_batched(seed, warm_tune=True):
+    """The batched multi-mode workload at its full size (256 DNA queries of 32..2000 bp, modes
+    SW/NW/HW/SHW/OV round-robin, ScoreEnd, against 1,000,000 reads of 150 bp): one autotuned
+    hy_scan_batch call timed by CUDA events on the batch's stream and by the host clock, against the
+    same queries as 256 sequential Database.scan calls; the three shortest queries of different
+    modes checked against the oracle."""
+    import torch
+
+    import hyalite_b200 as hy
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    residues, offsets, queries = make_reads_workload(seed, 1_000_000, 256)
+    modes = [hy.Mode.Sw, hy.Mode.Nw, hy.Mode.Hw, hy.Mode.Shw, hy.Mode.Ov]
+    dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
+    dbs = [(hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(4, dna, 2, 1))
+            .mode(m).search_type(hy.SearchType.ScoreEnd).max_query_len(2000).build()) for m in modes]
+    dbq = [i % len(modes) for i in range(len(queries))]
+    cells = float(sum(len(q) for q in queries)) * float(offsets[-1])
+    batch = hy.Batch(dbs, max_queries=len(queries), autotune=True)
+    stream = torch.cuda.ExternalStream(batch.stream_ptr())
+    t0 = time.perf_counter()
+    batch.scan(queries, dbq)  # the first call of the shape runs the autotuner
+    first_s = time.perf_counter() - t0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    t0 = time.perf_counter()
+    hits_b = batch.scan(queries, dbq)
+    wall_b = time.perf_counter() - t0
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dev_b = ev0.elapsed_time(ev1) / 1e3
+    scratches = [hy.Scratch(d) for d in dbs]
+    for k, d in enumerate(dbs):
+        d.scan(scratches[k], queries[k])
+    t0 = time.perf_counter()
+    hits_p = [dbs[k].scan(scratches[k], q) for q, k in zip(queries, dbq)]
+    wall_p = time.perf_counter() - t0
+    picked, seen = [], set()
+    for i in sorted(range(len(queries)), key=lambda i: len(queries[i])):
+        if dbq[i] not in seen:
+            picked.append(i)
+            seen.add(dbq[i])
+        if len(picked) == 3:
+            break
+    threads = os.cpu_count() or 1
+    oracle_ok = all(_hit4(hits_b[i]) == _oracle_best(pyoracle.OracleDb((residues, offsets), dna, 4, 2, 1,
+                                                                      int(modes[dbq[i]]), 1), queries[i], threads)
+                    for i in picked)
+    return {"workload": "256 DNA queries (32..2000 bp; SW/NW/HW/SHW/OV round-robin; ScoreEnd) x 1,000,000 "
+                        "reads of 150 bp, one hy_scan_batch call (persistent kernels under a CUDA graph)",
+            "value": cells / dev_b / 1e9, "unit": "GCUPS", "cells": cells,
+            "e2e": {"value": cells / wall_b / 1e9, "unit": "GCUPS", "call_s": wall_b,
+                    "h2d_bytes": int(sum(len(q) for q in queries)) + 4 * len(queries), "d2h_bytes": 32 * len(queries)},
+            "plain": {"value": cells / wall_p / 1e9, "unit": "GCUPS", "seconds": wall_p,
+                      "form": "256 sequential Database.scan calls, host query in, hit out"},
+            "batched_over_plain": wall_p / wall_b, "first_call_s_incl_autotune": first_s,
+            "tuned_config": list(batch.config()),
+            "identical_to_plain": [_hit4(h) for h in hits_b] == [_hit4(h) for h in hits_p],
+            "identical_to_oracle_on_sample": bool(oracle_ok),
+            "oracle_sample": f"queries {picked} (the shortest of three modes) against all 1,000,000 reads"}
+
+
+def extra_served(seed, rate=10.0, seconds=6.0):
+    """The served protein workload at its full size (1,000,000 sequences of the protein generator;
+    log-normal query lengths, median 350, 50..3000; half ScoreEnd scans, half scan_scores) at one
+    offered rate below saturation: p50/p99 latency and GCUPS, every result against the plain call,
+    and the shortest request of each kind against the oracle."""
+    import hyalite_b200 as hy
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    mat, residues, offsets, _ = make_workload(seed, n_seqs=1_000_000)
+    db = (hy.Database.builder().sequences_concat(residues, offsets).scoring(hy.Scoring(AL, mat, GO, GE))
+          .mode(hy.Mode.Sw).search_type(hy.SearchType.ScoreEnd).max_query_len(3000).build())
+    rng = np.random.default_rng(seed + 7)
+    base = np.random.default_rng(12345)
+    base.integers(-4, 4, size=(AL, AL))
+    base.integers(4, 12, size=AL)
+    background = base.dirichlet(np.full(AL, 4.0))
+
+    def request():
+        L = int(np.clip(round(math.exp(math.log(350.0) + 0.8 * rng.standard_normal())), 50, 3000))
+        return rng.choice(AL, size=L, p=background).astype(np.uint8), bool(rng.random() < 0.5)
+
+    total_res = float(offsets[-1])
+    srv = hy.Server([db], max_batch=64, in_flight=2)
+    for kind in (False, True):
+        q, _ = request()
+        srv.wait(srv.submit(q, want_scores=kind))
+    srv.stats(reset=True)
+    n = int(rate * seconds)
+    reqs = [request() for _ in range(n)]
+    gaps = rng.exponential(1.0 / rate, n)
+    handles = []
+    t_start = time.perf_counter()
+    t_next = t_start
+    for (q, kind), g in zip(reqs, gaps):
+        t_next += g
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        handles.append(srv.submit(q, want_scores=kind))
+    served = [(srv.wait(h), h.scores) for h in handles]
+    wall = time.perf_counter() - t_start
+    st = srv.stats(reset=True)
+    srv.close()
+    sc = hy.Scratch(db)
+    same = True
+    t0 = time.perf_counter()
+    cells = 0.0
+    for (q, kind), (hit, scores) in zip(reqs, served):
+        if kind:
+            same &= bool(np.array_equal(scores, db.scan_scores_array(sc, q)))
+        else:
+            same &= _hit4(hit) == _hit4(db.scan(sc, q))
+        cells += len(q) * total_res
+    plain_s = time.perf_counter() - t0
+    ref = pyoracle.OracleDb((residues, offsets), mat, AL, GO, GE, 0, 1)
+    threads = os.cpu_count() or 1
+    oracle_ok = True
+    for kind in (False, True):
+        i = min((i for i in range(n) if reqs[i][1] == kind), key=lambda i: len(reqs[i][0]))
+        q = reqs[i][0]
+        if kind:
+            oracle_ok &= bool(np.array_equal(served[i][1], ref.scan_scores(q, threads=threads)))
+        else:
+            oracle_ok &= _hit4(served[i][0]) == _oracle_best(ref, q, threads)
+    return {"workload": "1,000,000 protein sequences (log-normal lengths), Poisson arrivals, log-normal query "
+                        "lengths (median 350, 50..3000), half ScoreEnd scan and half scan_scores (i32 per target)",
+            "offered_qps": rate, "requests": n, "completed": int(st["completed"]), "achieved_qps": st["completed"] / wall,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"],
+            "value": st["gcups"], "unit": "GCUPS",
+            "plain": {"value": cells / plain_s / 1e9, "unit": "GCUPS", "seconds": plain_s,
+                      "form": "the same requests one at a time (Database.scan / scan_scores)"},
+            "identical_to_plain": bool(same), "identical_to_oracle_on_sample": bool(oracle_ok),
+            "oracle_sample": "the shortest scan and the shortest scan_scores request, against all 1,000,000 sequences"}
+
+
+def extra_pairs(seed, n_pairs=10_000_000, steps=2):
+    """align_pairs at its full size (10,000,000 (150-bp read, 200..500-bp window) pairs, HW,
+    ScoreEnd, +2/-1, gap_open 6, gap_ext 1): device GCUPS (the call's kernels, CUDA events), the
+    whole call with host buffers, and 2,000 sampled pairs against the oracle."""
+    import hyalite_b200 as hy
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    q_res, q_off, t_res, t_off = make_pairs_workload(seed, n_pairs)
+    dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
+    scoring = hy.Scoring(4, dna, 6, 1)
+    cells = float(np.dot(np.diff(q_off).astype(np.float64), np.diff(t_off).astype(np.float64)))
+    hy.align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
+    kms = cms = 0.0
+    for _ in range(steps):
+        hits, (err, _) = hy.align_pairs_arrays(q_res, q_off, t_res, t_off, scoring, hy.Mode.Hw, hy.SearchType.ScoreEnd)
+        assert err is None
+        k, c = hy.align_pairs_timing()
+        kms += k
+        cms += c
+    rng = np.random.default_rng(1)
+    sample = np.sort(rng.choice(n_pairs, min(n_pairs, 2000), replace=False))
+    qs = [q_res[int(q_off[i]):int(q_off[i + 1])] for i in sample]
+    ts = [t_res[int(t_off[i]):int(t_off[i + 1])] for i in sample]
+    st, want, _ = pyoracle.align_pairs(qs, ts, dna, 4, 6, 1, 2, 1, threads=os.cpu_count() or 1)
+    got = [(hits[i].score, None if hits[i].query_end < 0 else hits[i].query_end,
+            None if hits[i].target_end < 0 else hits[i].target_end) for i in sample]
+    return {"workload": f"align_pairs: {n_pairs} (150-bp read, 200..500-bp window) pairs, HW, ScoreEnd, +2/-1, "
+                        "gap_open 6, gap_ext 1",
+            "value": cells * steps / (kms * 1e-3) / 1e9, "unit": "GCUPS", "cells": cells,
+            "e2e": {"value": cells * steps / (cms * 1e-3) / 1e9, "unit": "GCUPS", "call_ms": cms / steps,
+                    "h2d_bytes": int(len(q_res) + len(t_res) + 16 * n_pairs), "d2h_bytes": 12 * n_pairs},
+            "identical_to_oracle_on_sample": bool(st == 0 and got == [(w[0], w[2], w[3]) for w in want]),
+            "oracle_sample": "2,000 random pairs"}
+
+
+def make_dna_small_workload(seed: int, n_queries: int, n_seqs: int = 10_000, n_planted: int = 50):
+    """The small DNA scan: `n_seqs` sequences of uniform length 50..300 and uniform bases, and
+    `n_queries` queries of 64 uniform bases; `n_planted` sequences are replaced by copies of the
+    first query with 5% of its bases (3 of 64) substituted. Returns (seqs, queries, planted)."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(50, 301, n_seqs)
+    seqs = [rng.integers(0, 4, int(n)).astype(np.uint8) for n in lengths]
+    queries = [rng.integers(0, 4, 64).astype(np.uint8) for _ in range(n_queries)]
+    planted = rng.choice(n_seqs, n_planted, replace=False)
+    for k in planted:
+        s = queries[0].copy()
+        sub = rng.choice(64, 3, replace=False)  # 5% of 64
+        s[sub] = (s[sub] + rng.integers(1, 4, 3)) % 4
+        seqs[k] = s
+    return seqs, queries, planted
+
+
 def run_dna_small(args):
     """The small plain DNA scan: alphabet 4, +2/-1, gap_open 2, gap_ext 1, SW ScoreEnd, a stream of
     --dna-queries queries of 64 uniform bases against 10,000 sequences of uniform length 50..300
@@ -461,16 +711,7 @@ def run_dna_small(args):
     import hyalite_b200 as hy
 
     torch.cuda.set_device(0)
-    rng = np.random.default_rng(args.seed)
-    lengths = rng.integers(50, 301, 10_000)
-    seqs = [rng.integers(0, 4, int(n)).astype(np.uint8) for n in lengths]
-    queries = [rng.integers(0, 4, 64).astype(np.uint8) for _ in range(args.dna_queries)]
-    planted = rng.choice(10_000, 50, replace=False)
-    for k in planted:
-        s = queries[0].copy()
-        sub = rng.choice(64, 3, replace=False)  # 5% of 64
-        s[sub] = (s[sub] + rng.integers(1, 4, 3)) % 4
-        seqs[k] = s
+    seqs, queries, planted = make_dna_small_workload(args.seed, args.dna_queries)
     res, off = hy.concat(seqs)
     dna = [2 if a == b else -1 for a in range(4) for b in range(4)]
     db = (hy.Database.builder().sequences_concat(res, off).scoring(hy.Scoring(4, dna, 2, 1)).mode(hy.Mode.Sw)
@@ -655,41 +896,51 @@ def run_served(args):
 def make_pairs_workload(seed: int, n_pairs: int, genome_len: int = 10_000_000, read_len: int = 150):
     """(read, window) pairs: reads of `read_len` from a seeded uniform genome with 2% substitutions
     and, with probability 0.75 per read (0.5% per base), one 1..3-bp insertion or deletion; each
-    window 200..500 bp long and placed so that it contains the read's origin."""
+    window 200..500 bp long and placed so that it contains the read's origin. Blocks of 250,000
+    pairs are generated on all host threads, each from its own seeded stream."""
+    from concurrent.futures import ThreadPoolExecutor
+
     rng = np.random.default_rng(seed)
     genome = rng.integers(0, 4, genome_len, dtype=np.uint8)
     reads = np.empty((n_pairs, read_len), np.uint8)
     wlen = rng.integers(200, 501, n_pairs).astype(np.int64)
     wstart = np.empty(n_pairs, np.int64)
-    j = np.arange(read_len)[None, :]
-    span = read_len + 3
-    for lo in range(0, n_pairs, 250_000):
-        n = min(250_000, n_pairs - lo)
-        W = wlen[lo:lo + n]
-        origin = rng.integers(600, genome_len - 600, n)
-        win = genome[origin[:, None] + np.arange(span)[None, :]]
-        p = rng.integers(0, read_len, n)[:, None]
-        dl = rng.integers(1, 4, n)[:, None]
-        kind = rng.random(n)
-        deletion = (kind < 0.375)[:, None]
-        insertion = ((kind >= 0.375) & (kind < 0.75))[:, None]
-        idx = np.where(deletion, j + dl * (j >= p), np.where(insertion, np.maximum(j - dl * (j >= p + dl), 0), j))
-        r = np.take_along_axis(win, idx, axis=1)
-        r = np.where(insertion & (j >= p) & (j < p + dl), rng.integers(0, 4, (n, read_len), dtype=np.uint8), r)
-        sub = rng.random((n, read_len)) < 0.02
-        r = np.where(sub, (r + rng.integers(1, 4, (n, read_len), dtype=np.uint8)) % 4, r).astype(np.uint8)
-        reads[lo:lo + n] = r
-        wstart[lo:lo + n] = origin - rng.integers(0, W - read_len + 1)
     t_off = np.zeros(n_pairs + 1, np.uint64)
     t_off[1:] = np.cumsum(wlen)
     t_res = np.empty(int(t_off[-1]), np.uint8)
-    for lo in range(0, n_pairs, 250_000):
-        hi = min(n_pairs, lo + 250_000)
-        W = wlen[lo:hi]
-        base = int(t_off[lo])
-        seg = (np.repeat(wstart[lo:hi] - (t_off[lo:hi].astype(np.int64) - base), W)
-               + np.arange(int(t_off[hi]) - base, dtype=np.int64))
-        t_res[base:int(t_off[hi])] = genome[seg]
+    j = np.arange(read_len, dtype=np.int16)[None, :]
+    span = read_len + 3
+    read_view = np.lib.stride_tricks.sliding_window_view(genome, span)
+    # Each window is the first wlen bases of a 500-base view of the genome at its start.
+    win_view = np.lib.stride_tricks.sliding_window_view(genome, 500)
+    cols = np.arange(500)[None, :]
+    block = 250_000
+
+    def make_block(lo):
+        brng = np.random.default_rng([seed, lo])
+        n = min(block, n_pairs - lo)
+        W = wlen[lo:lo + n]
+        origin = brng.integers(600, genome_len - 600, n)
+        win = read_view[origin]
+        p = brng.integers(0, read_len, n)[:, None].astype(np.int16)
+        dl = brng.integers(1, 4, n)[:, None].astype(np.int16)
+        kind = brng.random(n)
+        deletion = (kind < 0.375)[:, None]
+        insertion = ((kind >= 0.375) & (kind < 0.75))[:, None]
+        # Source base of each read position: a deletion skips dl bases at p; after an insertion of
+        # dl bases at p the read continues with the base at p.
+        idx = j + (deletion & (j >= p)) * dl - (insertion & (j >= p + dl)) * dl
+        r = np.take_along_axis(win, idx.astype(np.intp), axis=1)
+        r = np.where(insertion & (j >= p) & (j < p + dl), brng.integers(0, 4, (n, read_len), dtype=np.uint8), r)
+        sub = brng.integers(0, 50, (n, read_len), dtype=np.uint8) == 0  # 2% of the bases
+        r = np.where(sub, (r + brng.integers(1, 4, (n, read_len), dtype=np.uint8)) % 4, r).astype(np.uint8)
+        reads[lo:lo + n] = r
+        ws = origin - brng.integers(0, W - read_len + 1)
+        wstart[lo:lo + n] = ws
+        t_res[int(t_off[lo]):int(t_off[lo + n])] = win_view[ws][cols < W[:, None]]
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        list(ex.map(make_block, range(0, n_pairs, block)))
     q_off = np.arange(n_pairs + 1, dtype=np.uint64) * read_len
     return reads.reshape(-1), q_off, t_res, t_off
 
@@ -1060,9 +1311,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--cpu-sample-seqs", type=int, default=12_000)
-    ap.add_argument("--ref-seqs", type=int, default=12_000)
+    ap.add_argument("--cpu-sample-seqs", type=int, default=20_000)
+    ap.add_argument("--ref-seqs", type=int, default=100_000)
+    ap.add_argument("--ref-sample-seqs", type=int, default=5_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the batched, served and align_pairs forms from the default line")
     # Smaller shapes of the same generator (profiling cases; the default is the benchmark).
     ap.add_argument("--n-seqs", type=int, default=N_SEQS)
     ap.add_argument("--query-lengths", default=",".join(map(str, QUERY_LENGTHS)))

@@ -114,6 +114,9 @@ SIGNATURES = {
     "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, C.POINTER(C.c_double), _u64p]),
     "hy_measure_dpx_peak": (_st, [C.POINTER(C.c_double)]),
     "hy_measure_dpx_peak_i32": (_st, [C.POINTER(C.c_double)]),
+    "hy_debug_fail_device_alloc": (None, [C.c_int64]),
+    "hy_debug_live_device_allocations": (C.c_int64, []),
+    "hy_debug_set_wait_polls": (None, [C.c_int64]),
     "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
     "hy_align_pairs_timing": (_st, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),

@@ -336,7 +336,7 @@ void batch_free(hy_batch *b) {
     void *dev[] = {b->d_queries, b->d_ctl, b->d_order, b->d_qres, b->d_prof, b->d_bnd_bulk,
                    b->d_bnd_side, b->d_bnd_band, b->d_keys, b->d_ends, b->d_hits, b->d_err};
     for (void *p : dev)
-        if (p) cudaFree(p);
+        if (p) hy::dev_free(p);
     void *host[] = {b->h_queries, b->h_ctl, b->h_order, b->h_qres, b->h_hits, b->h_err};
     for (void *p : host)
         if (p) cudaFreeHost(p);
@@ -438,6 +438,7 @@ hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const Bat
             p.scores = it.d_scores;
             p.best_key = b->d_keys + i;
             p.err = b->d_err;
+            p.wait_polls = wait_polls();
             if (!k.need[kk]) continue;
             p.pass_bytes = k.qp[kk].pass_bytes;
             p.n_passes = k.qp[kk].n_passes;
@@ -698,7 +699,7 @@ hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_que
         ck(cudaEventCreate(&b->ev_t0));
         ck(cudaEventCreate(&b->ev_t1));
         auto dalloc = [&](void **p, size_t bytes) {
-            ck(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+            ck(hy::dev_malloc(p, std::max<size_t>(bytes, 16)));
             if (st == HY_OK) b->device_bytes += bytes;
         };
         dalloc((void **)&b->d_queries, sizeof(BatchQuery) * max_queries);

@@ -9,9 +9,43 @@
 #include <cuda_runtime.h>
 #include <string>
 
+#include <algorithm>
+#include <atomic>
+
 namespace hy {
 
 static thread_local int64_t g_detail[3] = {0, 0, 0};
+
+// Live device allocations, and the test hook's countdown to a failing one (-1: off).
+static std::atomic<int64_t> g_live_allocs{0};
+static std::atomic<int64_t> g_fail_countdown{-1};
+static std::atomic<uint32_t> g_wait_polls{WAIT_POLLS_DEFAULT};
+static std::atomic<uint64_t> g_wait_epoch{0};
+
+cudaError_t dev_malloc_bytes(void **p, size_t bytes) {
+    int64_t c = g_fail_countdown.load();
+    while (c >= 0) {
+        if (g_fail_countdown.compare_exchange_weak(c, c - 1)) {
+            if (c == 0) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) g_live_allocs.fetch_add(1);
+    return e;
+}
+
+cudaError_t dev_free(void *p) {
+    if (!p) return cudaSuccess;
+    g_live_allocs.fetch_sub(1);
+    return cudaFree(p);
+}
+
+uint32_t wait_polls() { return g_wait_polls.load(); }
+uint64_t wait_polls_epoch() { return g_wait_epoch.load(); }
 
 hy_status fail(hy_status st, int64_t d0, int64_t d1, int64_t d2) {
     g_detail[0] = d0;
@@ -184,6 +218,19 @@ hy_status hy_required_width(hy_mode mode, int32_t min_entry, int32_t max_entry, 
     if (w < 0) return fail(HY_ERR_SCORE_RANGE_TOO_WIDE, b);
     if (width) *width = (hy_score_width)w;
     return fail(HY_OK);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+void hy_debug_fail_device_alloc(int64_t after) { hy::g_fail_countdown.store(after < 0 ? -1 : after); }
+
+int64_t hy_debug_live_device_allocations(void) { return hy::g_live_allocs.load(); }
+
+void hy_debug_set_wait_polls(int64_t polls) {
+    hy::g_wait_polls.store(polls < 0 ? hy::WAIT_POLLS_DEFAULT : (uint32_t)std::min<int64_t>(polls, UINT32_MAX));
+    hy::g_wait_epoch.fetch_add(1);
 }
 
 }  // extern "C"

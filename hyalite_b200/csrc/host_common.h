@@ -2,11 +2,32 @@
 // the width proof and scoring validation (pure host code, callable without a GPU).
 #pragma once
 
+#include <stddef.h>
 #include <stdint.h>
+
+#include <cuda_runtime.h>
 
 #include "../../include/hyalite_cuda.h"
 
 namespace hy {
+
+// Every device allocation of the library goes through dev_malloc / dev_free: they count the live
+// allocations and, when a test asks for it (hy_debug_fail_device_alloc), make a chosen request
+// fail with cudaErrorMemoryAllocation as a full device would.
+cudaError_t dev_malloc_bytes(void **p, size_t bytes);
+template <class T>
+inline cudaError_t dev_malloc(T **p, size_t bytes) {
+    return dev_malloc_bytes(reinterpret_cast<void **>(p), bytes);
+}
+cudaError_t dev_free(void *p);
+
+// Polls a bounded device wait makes before it gives up (the kernels take it as a launch
+// parameter). The default bounds a wait to seconds; a test may lower it to make waits run out.
+constexpr uint32_t WAIT_POLLS_DEFAULT = 1u << 24;
+uint32_t wait_polls();
+// Counts the changes of wait_polls(): work captured into a CUDA graph under an older value (the
+// limit is a kernel parameter, frozen at capture) is captured again.
+uint64_t wait_polls_epoch();
 
 // Records the detail fields of the status being returned on this thread (hy_last_error_detail).
 hy_status fail(hy_status st, int64_t d0 = 0, int64_t d1 = 0, int64_t d2 = 0);

@@ -153,6 +153,7 @@ hy_status run_partition(const hy_db *db, const Partition &part, uint32_t item_ba
     p.tend = nullptr;
     p.best_key = nullptr;
     p.err = d_err;
+    p.wait_polls = wait_polls();
     const int gpb = BLOCK / G;
     const int blocks = (int)((item_end - item_base + gpb - 1) / gpb);
     cudaError_t e = launch_scores_mode<A, G, R>(db->mode, p, blocks, 2 * (size_t)rg.qp.pass_bytes + 16, st);

@@ -115,7 +115,7 @@ struct PairsContext {
     // a staging slot, host copies of the column maxima into the caller's array (position maxima).
     double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
     ~PairsContext() {
-        for (auto &x : b) cudaFree(x.p);
+        for (auto &x : b) hy::dev_free(x.p);
         for (auto &x : pinned) cudaFreeHost(x.p);
         for (cudaEvent_t e : ev) cudaEventDestroy(e);
         for (cudaEvent_t e : slot_ev)
@@ -146,10 +146,10 @@ struct PairsContext {
                 cudaError_t e = cudaStreamSynchronize(stream);
                 if (e != cudaSuccess) return e;
             }
-            cudaFree(b[slot].p);
+            hy::dev_free(b[slot].p);
             b[slot].p = nullptr;
             b[slot].n = 0;
-            cudaError_t e = cudaMalloc(&b[slot].p, bytes);
+            cudaError_t e = hy::dev_malloc(&b[slot].p, bytes);
             if (e != cudaSuccess) return e;
             b[slot].n = bytes;
         }

@@ -61,6 +61,7 @@ struct hy_scratch {
         cudaGraphExec_t exec;
         uint64_t launches;  // kernels the graph launches
         uint64_t last_use;
+        uint64_t epoch;     // wait_polls_epoch() at capture
     };
     std::vector<Graph> graphs;
     uint64_t graph_clock = 0;
@@ -183,6 +184,7 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
     p.tend = sc->d_tend;
     p.best_key = key;
     p.err = sc->d_err;
+    p.wait_polls = wait_polls();
     size_t smem = 2 * (size_t)qp.pass_bytes + 16;
     const bool gprof = smem > db->smem_limit;
     if (gprof) smem = 16;
@@ -275,9 +277,14 @@ static hy_status enqueue_scores(const hy_db *db, hy_scratch *sc, const uint8_t *
 }
 
 // The winner's item: its int16x2 pair when that pair ran packed for this query (pair >= k0),
-// else its int32 single (the 2*k0 longest sequences). The other slot gets NO_INDEX.
+// else its int32 single (the 2*k0 longest sequences). The other slot gets NO_INDEX. A key of 0
+// means no item recorded a hit (a scan kernel gave up on a bounded wait): no winner then.
 __global__ void winner_loc_kernel(const unsigned long long *key, const uint32_t *rank, uint32_t k0,
                                   uint32_t *win) {
+    if (*key == 0) {
+        win[0] = win[1] = NO_INDEX;
+        return;
+    }
     const uint32_t idx = ~(uint32_t)(*key & 0xffffffffu);
     const uint32_t r = rank[idx];
     const bool packed = r / 2 >= k0;
@@ -325,6 +332,7 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     p.tend = sc->d_tend;
     p.best_key = nullptr;
     p.err = sc->d_err;
+    p.wait_polls = wait_polls();
     // One pass slice per warp in shared memory; a slice too large for that runs from the profile
     // in global memory.
     const size_t budget = std::min<size_t>(BAND_SMEM_BUDGET, db->smem_limit - 16);
@@ -360,8 +368,10 @@ __global__ void finalize_kernel(const unsigned long long *key, const int32_t *qe
     h.score = (int32_t)((uint32_t)(k >> 32) ^ 0x80000000u);
     h.reserved = 0;
     h.db_index = idx;
-    h.query_end = with_ends ? (int64_t)qend[idx] : -1;
-    h.target_end = with_ends ? (int64_t)tend[idx] : -1;
+    // A key of 0 (no hit recorded: the call reports a timeout) names no sequence to read.
+    const bool ends = with_ends && k != 0;
+    h.query_end = ends ? (int64_t)qend[idx] : -1;
+    h.target_end = ends ? (int64_t)tend[idx] : -1;
     *out = h;
 }
 
@@ -427,6 +437,16 @@ static uint64_t db_residues(const hy_db *db) {
 template <class F>
 static hy_status run_captured(const hy_db *db, hy_scratch *sc, int kind, uint64_t qlen, F issue) {
     if (sc->profile || (double)qlen * (double)db_residues(db) > GRAPH_MAX_CELLS) return issue();
+    // Graphs captured under another wait limit are captured again.
+    const uint64_t epoch = wait_polls_epoch();
+    for (size_t i = 0; i < sc->graphs.size();) {
+        if (sc->graphs[i].epoch == epoch) {
+            ++i;
+            continue;
+        }
+        if (sc->graphs[i].exec) cudaGraphExecDestroy(sc->graphs[i].exec);
+        sc->graphs.erase(sc->graphs.begin() + i);
+    }
     for (auto &gr : sc->graphs) {
         if (gr.kind != kind || gr.qlen != qlen) continue;
         gr.last_use = ++sc->graph_clock;
@@ -454,7 +474,7 @@ static hy_status run_captured(const hy_db *db, hy_scratch *sc, int kind, uint64_
     cudaGetLastError();
     if (st != HY_OK) return st;
     sc->graphs.push_back({kind, qlen, e == cudaSuccess ? exec : nullptr, sc->launches - launches0,
-                          ++sc->graph_clock});
+                          ++sc->graph_clock, epoch});
     if (!sc->graphs.back().exec) {
         // Not capturable here: this call and later ones of its kind and length launch directly.
         sc->launches = launches0;
@@ -570,7 +590,7 @@ static hy_status build_partition(hy_db *db, Partition &part, const std::vector<u
     part.res_prefix.assign(part.n_items + 1, 0);
     for (uint32_t it = 0; it < part.n_items; ++it)
         part.res_prefix[it + 1] = part.res_prefix[it] + meta[it].n[0] + meta[it].n[1];
-    HY_CK(cudaMalloc(&part.d_meta, sizeof(ItemMeta) * part.n_items));
+    HY_CK(hy::dev_malloc(&part.d_meta, sizeof(ItemMeta) * part.n_items));
     HY_CK(cudaMemcpy(part.d_meta, meta.data(), sizeof(ItemMeta) * part.n_items, cudaMemcpyHostToDevice));
     db->device_bytes += sizeof(ItemMeta) * part.n_items;
     if (pairs) {
@@ -591,7 +611,7 @@ static hy_status build_partition(hy_db *db, Partition &part, const std::vector<u
                 res[m.col_off + j] = code(lo, hi);
             }
         }
-        HY_CK(cudaMalloc(&part.d_res, res.size() * sizeof(uint16_t)));
+        HY_CK(hy::dev_malloc(&part.d_res, res.size() * sizeof(uint16_t)));
         HY_CK(cudaMemcpy(part.d_res, res.data(), res.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         db->device_bytes += res.size() * sizeof(uint16_t);
     } else {
@@ -600,7 +620,7 @@ static hy_status build_partition(hy_db *db, Partition &part, const std::vector<u
             const ItemMeta &m = meta[it];
             memcpy(&res[m.col_off], residues + offsets[m.idx[0]], m.n[0]);
         }
-        HY_CK(cudaMalloc(&part.d_res, res.size()));
+        HY_CK(hy::dev_malloc(&part.d_res, res.size()));
         HY_CK(cudaMemcpy(part.d_res, res.data(), res.size(), cudaMemcpyHostToDevice));
         db->device_bytes += res.size();
     }
@@ -609,13 +629,13 @@ static hy_status build_partition(hy_db *db, Partition &part, const std::vector<u
 
 static void free_db(hy_db *db) {
     if (!db) return;
-    cudaFree(db->d_matrix);
-    cudaFree(db->p16.d_meta);
-    cudaFree(db->p16.d_res);
-    cudaFree(db->p32.d_meta);
-    cudaFree(db->p32.d_res);
-    cudaFree(db->d_rank);
-    cudaFree(db->d_tb_res);
+    hy::dev_free(db->d_matrix);
+    hy::dev_free(db->p16.d_meta);
+    hy::dev_free(db->p16.d_res);
+    hy::dev_free(db->p32.d_meta);
+    hy::dev_free(db->p32.d_res);
+    hy::dev_free(db->d_rank);
+    hy::dev_free(db->d_tb_res);
     delete db;
 }
 
@@ -720,7 +740,7 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
             bst = fail(e == cudaErrorMemoryAllocation ? HY_ERR_OUT_OF_MEMORY : HY_ERR_CUDA, e);
         }
     };
-    ck(cudaMalloc(&db->d_matrix, sizeof(int32_t) * alphabet_len * alphabet_len));
+    ck(hy::dev_malloc(&db->d_matrix, sizeof(int32_t) * alphabet_len * alphabet_len));
     if (bst == HY_OK)
         ck(cudaMemcpy(db->d_matrix, matrix, sizeof(int32_t) * alphabet_len * alphabet_len,
                       cudaMemcpyHostToDevice));
@@ -729,7 +749,7 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
     if (bst == HY_OK) {
         std::vector<uint32_t> rank(n_seqs);
         for (uint64_t r = 0; r < n_seqs; ++r) rank[order[r]] = (uint32_t)r;
-        ck(cudaMalloc(&db->d_rank, sizeof(uint32_t) * n_seqs));
+        ck(hy::dev_malloc(&db->d_rank, sizeof(uint32_t) * n_seqs));
         if (bst == HY_OK)
             ck(cudaMemcpy(db->d_rank, rank.data(), sizeof(uint32_t) * n_seqs, cudaMemcpyHostToDevice));
         db->device_bytes += sizeof(uint32_t) * n_seqs + sizeof(int32_t) * alphabet_len * alphabet_len;
@@ -739,7 +759,7 @@ hy_status hy_db_create(const uint8_t *residues, const uint64_t *offsets, uint64_
         const uint64_t total = offsets[n_seqs] - offsets[0];
         db->tb_off.resize(n_seqs + 1);
         for (uint64_t k = 0; k <= n_seqs; ++k) db->tb_off[k] = offsets[k] - offsets[0];
-        ck(cudaMalloc(&db->d_tb_res, std::max<uint64_t>(total, 16)));
+        ck(hy::dev_malloc(&db->d_tb_res, std::max<uint64_t>(total, 16)));
         if (bst == HY_OK && total)
             ck(cudaMemcpy(db->d_tb_res, residues + offsets[0], total, cudaMemcpyHostToDevice));
         db->device_bytes += total;
@@ -817,26 +837,26 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
     ck(cudaEventCreateWithFlags(&sc->ev_join3, cudaEventDisableTiming));
     ck(cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming));
     ck(cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming));
-    ck(cudaMalloc(&sc->d_query, mq));
+    ck(hy::dev_malloc(&sc->d_query, mq));
     auto prof_bytes = [&](int rpp, size_t slice_row_bytes) {
         return std::max<uint64_t>(1, npass(mq, rpp) * rpp * slice_row_bytes);
     };
     const uint64_t pr = pair_slice_row_bytes(db), sr = profile_slice_row_bytes<Single32>(db->al);
-    ck(cudaMalloc(&sc->d_prof16, prof_bytes(BULK_MAX_RPP, pr)));
-    ck(cudaMalloc(&sc->d_prof16l, prof_bytes(LONG_G * LONG_R, pr)));
-    ck(cudaMalloc(&sc->d_prof32, prof_bytes(MAIN_G32 * MAIN_R32, sr)));
-    ck(cudaMalloc(&sc->d_profw16, prof_bytes(WIN_G * WIN_R, pr)));
-    ck(cudaMalloc(&sc->d_profw32, prof_bytes(WIN_G * WIN_R, sr)));
+    ck(hy::dev_malloc(&sc->d_prof16, prof_bytes(BULK_MAX_RPP, pr)));
+    ck(hy::dev_malloc(&sc->d_prof16l, prof_bytes(LONG_G * LONG_R, pr)));
+    ck(hy::dev_malloc(&sc->d_prof32, prof_bytes(MAIN_G32 * MAIN_R32, sr)));
+    ck(hy::dev_malloc(&sc->d_profw16, prof_bytes(WIN_G * WIN_R, pr)));
+    ck(hy::dev_malloc(&sc->d_profw32, prof_bytes(WIN_G * WIN_R, sr)));
     const bool multipass = mq > (uint64_t)std::min({MAIN_G * 8, MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R});
-    ck(cudaMalloc(&sc->d_bnd16, multipass ? std::max<uint64_t>(8, 8 * db->p16.total_cols) : 8));
-    ck(cudaMalloc(&sc->d_bnd32, multipass ? std::max<uint64_t>(8, 8 * db->p32.total_cols) : 8));
-    ck(cudaMalloc(&sc->d_scores, 4 * n));
-    ck(cudaMalloc(&sc->d_qend, 4 * n));
-    ck(cudaMalloc(&sc->d_tend, 4 * n));
-    ck(cudaMalloc(&sc->d_key, 64));
-    ck(cudaMalloc(&sc->d_win, 64));
-    ck(cudaMalloc(&sc->d_hit, sizeof(hy_hit)));
-    ck(cudaMalloc(&sc->d_err, 64));
+    ck(hy::dev_malloc(&sc->d_bnd16, multipass ? std::max<uint64_t>(8, 8 * db->p16.total_cols) : 8));
+    ck(hy::dev_malloc(&sc->d_bnd32, multipass ? std::max<uint64_t>(8, 8 * db->p32.total_cols) : 8));
+    ck(hy::dev_malloc(&sc->d_scores, 4 * n));
+    ck(hy::dev_malloc(&sc->d_qend, 4 * n));
+    ck(hy::dev_malloc(&sc->d_tend, 4 * n));
+    ck(hy::dev_malloc(&sc->d_key, 64));
+    ck(hy::dev_malloc(&sc->d_win, 64));
+    ck(hy::dev_malloc(&sc->d_hit, sizeof(hy_hit)));
+    ck(hy::dev_malloc(&sc->d_err, 64));
     ck(cudaMallocHost(&sc->h_query, mq));
     ck(cudaMallocHost(&sc->h_hit, sizeof(hy_hit)));
     ck(cudaMallocHost(&sc->h_err, sizeof(int)));
@@ -860,21 +880,21 @@ void hy_scratch_destroy(hy_scratch *sc) {
     DeviceGuard g(sc->device);
     if (sc->stream) cudaStreamSynchronize(sc->stream);
     tb_context_destroy(sc->tb);
-    cudaFree(sc->d_query);
-    cudaFree(sc->d_prof16);
-    cudaFree(sc->d_prof16l);
-    cudaFree(sc->d_prof32);
-    cudaFree(sc->d_profw16);
-    cudaFree(sc->d_profw32);
-    cudaFree(sc->d_bnd16);
-    cudaFree(sc->d_bnd32);
-    cudaFree(sc->d_scores);
-    cudaFree(sc->d_qend);
-    cudaFree(sc->d_tend);
-    cudaFree(sc->d_key);
-    cudaFree(sc->d_win);
-    cudaFree(sc->d_hit);
-    cudaFree(sc->d_err);
+    hy::dev_free(sc->d_query);
+    hy::dev_free(sc->d_prof16);
+    hy::dev_free(sc->d_prof16l);
+    hy::dev_free(sc->d_prof32);
+    hy::dev_free(sc->d_profw16);
+    hy::dev_free(sc->d_profw32);
+    hy::dev_free(sc->d_bnd16);
+    hy::dev_free(sc->d_bnd32);
+    hy::dev_free(sc->d_scores);
+    hy::dev_free(sc->d_qend);
+    hy::dev_free(sc->d_tend);
+    hy::dev_free(sc->d_key);
+    hy::dev_free(sc->d_win);
+    hy::dev_free(sc->d_hit);
+    hy::dev_free(sc->d_err);
     cudaFreeHost(sc->h_query);
     cudaFreeHost(sc->h_hit);
     cudaFreeHost(sc->h_err);

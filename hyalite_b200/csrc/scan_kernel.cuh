@@ -82,6 +82,7 @@ struct ScanParams {
     // Band recovery only: when set, the winner named by *best_key is written here as {score,
     // query end, target end} instead of to scores / qend / tend.
     int32_t *ends_out;
+    uint32_t wait_polls;  // polls a wait for a profile copy makes before it gives up
 };
 
 // ---- lane arithmetic -----------------------------------------------------------------------
@@ -339,11 +340,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: gives up after a fixed number of polls (each poll may itself suspend briefly).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    for (uint32_t it = 0; it < (1u << 24); ++it)
+// Bounded wait: gives up after `polls` polls (each poll may itself suspend briefly).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t polls) {
+    for (uint32_t it = 0; it < polls; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// After a wait gave up: lets the copies still in flight into this block's shared memory land
+// before the block exits (bounded again, by the default number of polls). `pending` holds the
+// barriers with a copy outstanding (bit b: bars[b]) and `phase` the parity each waits for.
+__device__ __forceinline__ void mbar_drain(uint64_t *bars, uint32_t pending, uint32_t phase) {
+    for (int b = 0; b < 2; ++b)
+        if ((pending >> b) & 1u) mbar_wait_bounded(&bars[b], (phase >> b) & 1u, 1u << 24);
 }
 
 __device__ __forceinline__ unsigned long long hit_key(int32_t score, uint32_t idx) {
@@ -774,12 +783,18 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
         if (GPROF) {
             prof = p.profile + (size_t)pass * p.pass_bytes;
         } else {
-            const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u);
-            phase ^= 1u << buf;
+            const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u, p.wait_polls);
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) atomicExch(p.err, 1);
+                if (threadIdx.x == 0) {
+                    atomicExch(p.err, 1);
+                    // This pass's copy and, if issued, the next pass's are still outstanding.
+                    const uint32_t pending = (1u << buf) | (pass + 1 < p.n_passes ? 1u << (buf ^ 1) : 0u);
+                    mbar_drain(bars, pending, phase);
+                }
+                __syncthreads();
                 return false;
             }
+            phase ^= 1u << buf;
             prof = prof_buf[buf];
         }
         sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof,
@@ -864,12 +879,16 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
         if (!GPROF) {
             if (threadIdx.x == 0)
                 bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
-            const bool ok = mbar_wait_bounded(bar, phase & 1u);
-            phase ^= 1u;
+            const bool ok = mbar_wait_bounded(bar, phase & 1u, p.wait_polls);
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) atomicExch(p.err, 1);
+                if (threadIdx.x == 0) {
+                    atomicExch(p.err, 1);
+                    mbar_drain(bar, 1u, phase);  // the round's copy is still outstanding
+                }
+                __syncthreads();
                 return;
             }
+            phase ^= 1u;
         }
         const int pass = first + warp;
         const bool mine = warp < cnt && w > 0;

@@ -82,7 +82,7 @@ void free_slots(hy_server *s) {
     for (ServerSlot &sl : s->slots) {
         if (sl.b) batch_free(sl.b);
         if (sl.done) cudaEventDestroy(sl.done);
-        if (sl.d_scores) cudaFree(sl.d_scores);
+        if (sl.d_scores) hy::dev_free(sl.d_scores);
         if (sl.h_scores) cudaFreeHost(sl.h_scores);
     }
     s->slots.clear();
@@ -273,7 +273,7 @@ hy_status hy_server_create(const hy_db *const *dbs, uint32_t n_dbs, const hy_ser
             sl.b->cfg.long_w = (uint32_t)std::min<int32_t>(std::max<int32_t>(c.launch_config[2], 1), 4096);
         }
         if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
-            cudaMalloc(&sl.d_scores, std::max<uint64_t>(c.scores_budget, 16)) != cudaSuccess ||
+            hy::dev_malloc(&sl.d_scores, std::max<uint64_t>(c.scores_budget, 16)) != cudaSuccess ||
             cudaMallocHost(&sl.h_scores, std::max<uint64_t>(c.scores_budget, 16)) != cudaSuccess) {
             cudaGetLastError();
             st = fail(HY_ERR_OUT_OF_MEMORY);

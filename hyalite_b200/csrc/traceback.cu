@@ -137,6 +137,7 @@ struct TbRows {
     const uint32_t *in_prog;
     uint32_t *out_prog;
     int *err;
+    uint32_t spin;  // polls a wait on in_prog makes before it gives up
 };
 
 constexpr uint32_t TB_PUBLISH = 32;        // columns between two progress updates of a stripe
@@ -146,16 +147,19 @@ constexpr uint32_t TB_STRIPE_R = 4;
 // a two-warp block at the limit); larger ones read the profile from global memory.
 constexpr uint64_t TB_STRIPE_SMEM_AL = 96;
 inline uint32_t tb_stripe_smem_al(uint64_t al) { return al <= TB_STRIPE_SMEM_AL ? (uint32_t)al : 0u; }
-constexpr uint32_t TB_SPIN_LIMIT = 1u << 22;  // polls (about 0.25 us each) before a wait gives up
+// Polls (about 0.25 us each) before a wait gives up: the default bound of the library's waits
+// divided down to this wait's longer poll interval.
+inline uint32_t tb_spin_limit() { return wait_polls() >> 2; }
 
-// Waits until *prog >= need (acquire); on running out of polls records the timeout in *err and
-// stops waiting for good (the results are then discarded by the host).
-__device__ inline uint32_t tb_wait(const uint32_t *prog, uint32_t need, uint32_t avail, int *err) {
+// Waits until *prog >= need (acquire); after `spin` polls without it records the timeout in *err
+// and stops waiting for good (the results are then discarded by the host).
+__device__ inline uint32_t tb_wait(const uint32_t *prog, uint32_t need, uint32_t avail, int *err,
+                                   uint32_t spin) {
     uint32_t it = 0;
     while (avail < need) {
         avail = *(const volatile uint32_t *)prog;
         if (avail >= need) break;
-        if (++it > TB_SPIN_LIMIT) {
+        if (++it > spin) {
             atomicExch(err, 1);
             return 0xffffffffu;
         }
@@ -237,7 +241,7 @@ __device__ __forceinline__ void tb_pass(const TbParams &P, const TbPair &pr, int
         const int j = s - lane + 1;  // this lane's DP column
         if (batched && (s & 31) == 0 && s < n) {
             const uint32_t need = min((uint32_t)n, (uint32_t)s + 32);
-            if (lane == 0 && need > avail) avail = tb_wait(rows.in_prog, need, avail, rows.err);
+            if (lane == 0 && need > avail) avail = tb_wait(rows.in_prog, need, avail, rows.err, rows.spin);
             __syncwarp();
             const int col = s + 1 + lane;
             cur = col <= n ? __ldcg(rows.in + col) : make_int2(0, TB_NEG);
@@ -453,7 +457,7 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_fill_kernel(TbParams P) {
     int32_t bs = F::local ? 0 : INT32_MIN;
     uint32_t brow = 0, bcol = 0;
     for (int p = 0; p < passes; ++p) {
-        const TbRows rows{B, p + 1 < passes ? B : nullptr, nullptr, nullptr, nullptr};
+        const TbRows rows{B, p + 1 < passes ? B : nullptr, nullptr, nullptr, nullptr, 0};
         tb_pass<R, MODE, TB_CODES>(P, pr, p, passes, lane, rows, bs, brow, bcol);
     }
     tb_write_end<MODE>(P.ends + pr.ends_off, lane, bs, brow, bcol);
@@ -484,6 +488,7 @@ struct TbStripes {
     int2 *bnd;              // per pair: (stripes - 1) rows of n + 1 entries at TbPair::bnd_off
     uint32_t *prog;         // per stripe: published columns of its last row (zeroed before launch)
     int *err;
+    uint32_t spin;          // polls a wait makes before it gives up
 };
 
 template <int R, int MODE, int KIND>
@@ -506,7 +511,7 @@ __global__ void __launch_bounds__(TB_BLOCK) tb_stripe_kernel(TbParams P, TbStrip
         int2 *B = S.bnd + pr.bnd_off;
         const TbRows rows{s == 0 ? nullptr : B + (uint64_t)(s - 1) * (n + 1),
                           (int)s + 1 < passes ? B + (uint64_t)s * (n + 1) : nullptr,
-                          s == 0 ? nullptr : S.prog + g - 1, S.prog + g, S.err};
+                          s == 0 ? nullptr : S.prog + g - 1, S.prog + g, S.err, S.spin};
         int32_t bs = F::local ? 0 : INT32_MIN;
         uint32_t brow = 0, bcol = 0;
         // The stripe's profile rows (al letters x 32 R rows) into this warp's shared memory: every
@@ -782,10 +787,10 @@ template <class T>
 static cudaError_t grow(T *&p, uint64_t &cap, uint64_t need) {
     need = std::max<uint64_t>(need, 16);
     if (cap >= need) return cudaSuccess;
-    cudaFree(p);
+    hy::dev_free(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc((void **)&p, need);
+    cudaError_t e = hy::dev_malloc((void **)&p, need);
     if (e == cudaSuccess) cap = need;
     return e;
 }
@@ -842,7 +847,7 @@ struct TbContext {
         for (void *p : {(void *)d_q, (void *)d_t, (void *)d_dir[0], (void *)d_dir[1], (void *)d_ops,
                         (void *)d_ops_out, (void *)d_prof, (void *)d_matrix, (void *)d_bnd, (void *)d_pairs,
                         (void *)d_ends, (void *)d_out, (void *)d_total, (void *)d_prog, (void *)d_first})
-            cudaFree(p);
+            hy::dev_free(p);
         for (void *p : {(void *)h_pairs, (void *)h_out, (void *)h_ops, (void *)h_total, (void *)h_q,
                         (void *)h_first, (void *)h_stage})
             cudaFreeHost(p);
@@ -1071,7 +1076,8 @@ static hy_status tb_run(TbContext &ctx, const TbRun &run, const uint32_t *idx, u
         TB_CK(cudaEventRecord(e[0], ctx.stream));
         if (run.m > 0 && run.stripes) {
             const uint32_t n_str = p.n_pairs * per_pair;
-            TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(run.al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+            TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(run.al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog,
+                        tb_spin_limit()};
             TB_CK(cudaMemsetAsync(S.prog, 0, sizeof(uint32_t) * n_str, ctx.stream));
             TB_CK(dispatch_stripes(run.mode, true, p, S, ctx.stream, ctx.device));
             ctx.launches += 2;
@@ -1418,7 +1424,8 @@ hy_status tb_long_pair_scores(const uint8_t *q_res, const uint64_t *q_off, const
     p.ends = ctx.d_ends;
     p.go = go;
     p.ge = ge;
-    TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog};
+    TbStripes S{ctx.d_first, n_str, tb_stripe_smem_al(al), ctx.d_bnd, ctx.d_prog + 4, (int *)ctx.d_prog,
+                tb_spin_limit()};
     if (cmx) {
         p.colmax = cmx->colmax;
         TB_CK(cudaEventRecord(ctx.ev[0], stream));

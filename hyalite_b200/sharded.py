@@ -32,6 +32,19 @@ def shard_indices(lengths: Sequence[int], world: int) -> List[np.ndarray]:
     return [np.sort(order[rank == r]) for r in range(world)]
 
 
+def take_sequences(residues, offsets, indices):
+    """Sequences `indices` of a concatenated database, concatenated in that order: (residues,
+    offsets)."""
+    offsets = np.asarray(offsets, dtype=np.uint64)
+    indices = np.asarray(indices, dtype=np.int64)
+    starts = offsets[indices].astype(np.int64)
+    lens = (offsets[indices + 1] - offsets[indices]).astype(np.int64)
+    out_off = np.zeros(len(lens) + 1, np.uint64)
+    out_off[1:] = np.cumsum(lens)
+    idx = np.repeat(starts - out_off[:-1].astype(np.int64), lens) + np.arange(int(out_off[-1]), dtype=np.int64)
+    return np.asarray(residues, dtype=np.uint8)[idx], out_off
+
+
 def hit_rows(hits, local_to_global):
     """Rows (score, global index, query end, target end) for a list of BestHit of one shard."""
     import torch
@@ -78,32 +91,57 @@ def all_gather_best(rows, group=None):
     return merge_hit_rows(torch.stack(out))
 
 
-def all_gather_scores(local_scores, local_to_global, n_total: int, group=None):
-    """Per-target scores of every shard scattered into global order ([n_total] int32 on every
-    rank). Shards may differ in size: each is padded to the largest before the all_gather."""
+def all_gather_scatter(local, local_to_global, n_total: int, group=None):
+    """Per-target rows of every shard ([n_local, ...] on this rank) scattered into global order
+    ([n_total, ...] on every rank). Shards may differ in size: each is padded to the largest
+    before the all_gather."""
     import torch
     import torch.distributed as dist
 
     world = dist.get_world_size(group)
-    dev = local_scores.device
+    dev = local.device
     g = torch.as_tensor(np.asarray(local_to_global, dtype=np.int64), device=dev)
-    n_local = torch.tensor([local_scores.numel()], dtype=torch.int64, device=dev)
+    n_local = torch.tensor([local.shape[0]], dtype=torch.int64, device=dev)
     sizes = [torch.empty_like(n_local) for _ in range(world)]
     dist.all_gather(sizes, n_local, group=group)
     m = int(max(int(s.item()) for s in sizes))
-    pad_s = torch.zeros(m, dtype=torch.int32, device=dev)
-    pad_s[: local_scores.numel()] = local_scores
+    pad_s = torch.zeros((m,) + tuple(local.shape[1:]), dtype=local.dtype, device=dev)
+    pad_s[: local.shape[0]] = local
     pad_g = torch.full((m,), -1, dtype=torch.int64, device=dev)
     pad_g[: g.numel()] = g
     all_s = [torch.empty_like(pad_s) for _ in range(world)]
     all_g = [torch.empty_like(pad_g) for _ in range(world)]
     dist.all_gather(all_s, pad_s, group=group)
     dist.all_gather(all_g, pad_g, group=group)
-    out = torch.empty(n_total, dtype=torch.int32, device=dev)
+    out = torch.empty((n_total,) + tuple(local.shape[1:]), dtype=local.dtype, device=dev)
     for s, gi, n in zip(all_s, all_g, sizes):
         k = int(n.item())
         out[gi[:k]] = s[:k]
     return out
+
+
+def all_gather_scores(local_scores, local_to_global, n_total: int, group=None):
+    """Per-target scores of every shard scattered into global order ([n_total] int32 on every
+    rank)."""
+    return all_gather_scatter(local_scores, local_to_global, n_total, group)
+
+
+def all_gather_hits(local_rows, local_to_global, n_total: int, group=None):
+    """scan_all across shards (src/database.rs:347-464): every shard's per-target rows (score,
+    global index, query end, target end) scattered into global order ([n_total, 4] int64 on every
+    rank). A target's row is its own, so no tie-break is involved."""
+    return all_gather_scatter(local_rows, local_to_global, n_total, group)
+
+
+def merge_aligned(candidates):
+    """scan_aligned across shards (src/database.rs:527-536): from each rank's (score, global
+    index, alignment) the winner under the scan's tie-break (highest score, then smallest global
+    index)."""
+    best = None
+    for c in candidates:
+        if best is None or c[0] > best[0] or (c[0] == best[0] and c[1] < best[1]):
+            best = c
+    return best
 
 
 class ShardedDatabase:
@@ -114,17 +152,66 @@ class ShardedDatabase:
     ``scan`` returns the same BestHit as a single Database over all sequences."""
 
     def __init__(self, sequences: Sequence, configure, group=None):
-        import torch.distributed as dist
-
         from . import Database
 
-        self.group = group
-        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
-        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self._init_group(group)
         self.n_total = len(sequences)
         self.local_to_global = shard_indices([len(s) for s in sequences], self.world)[self.rank]
         local = [sequences[i] for i in self.local_to_global]
         self.db = configure(Database.builder().sequences(local)).build()
+        self._d_l2g = None
+
+    def _init_group(self, group):
+        import torch.distributed as dist
+
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+
+    @classmethod
+    def from_concat(cls, residues, offsets, configure, group=None) -> "ShardedDatabase":
+        """The same sharding over a database given as concatenated residues and offsets (every rank
+        passes the whole database; each keeps only its shard on its device)."""
+        from . import Database
+
+        self = cls.__new__(cls)
+        self._init_group(group)
+        offsets = np.asarray(offsets, dtype=np.uint64)
+        self.n_total = len(offsets) - 1
+        self.local_to_global = shard_indices(np.diff(offsets.astype(np.int64)), self.world)[self.rank]
+        loc_res, loc_off = take_sequences(residues, offsets, self.local_to_global)
+        self.db = configure(Database.builder().sequences_concat(loc_res, loc_off)).build()
+        self._d_l2g = None
+        return self
+
+    @classmethod
+    def from_shard(cls, residues, offsets, local_to_global, n_total: int, configure,
+                   group=None) -> "ShardedDatabase":
+        """A rank that already holds its own shard (for example read from its own file): its
+        sequences as concatenated residues and offsets, their global indices in ascending order,
+        and the size of the whole database. Shards must partition 0..n_total."""
+        from . import Database
+
+        self = cls.__new__(cls)
+        self._init_group(group)
+        self.n_total = int(n_total)
+        self.local_to_global = np.asarray(local_to_global, dtype=np.int64)
+        if len(self.local_to_global) != len(offsets) - 1 or np.any(np.diff(self.local_to_global) <= 0):
+            raise ValueError("local_to_global must give one ascending global index per sequence")
+        self.db = configure(Database.builder().sequences_concat(residues, offsets)).build()
+        self._d_l2g = None
+        return self
+
+    def merge_device_hits(self, hits_u8):
+        """Per-query best hits of the whole database from this shard's device hit records ([Q, 32]
+        uint8 hy_hit, as hy_scan_device writes them): rows (score, global index, query end,
+        target end) on the device, after one all_gather over the group (NCCL)."""
+        import torch
+
+        if self._d_l2g is None or self._d_l2g.device != hits_u8.device:
+            self._d_l2g = torch.as_tensor(self.local_to_global, dtype=torch.int64, device=hits_u8.device)
+        rows = device_hit_rows(hits_u8, self._d_l2g)
+        return rows if self.world == 1 else all_gather_best(rows, self.group)
 
     def scan(self, scratch, query):
         from . import BestHit
@@ -138,6 +225,57 @@ class ShardedDatabase:
 
         local = torch.from_numpy(self.db.scan_scores_array(scratch, query)).to(self._device())
         return all_gather_scores(local, self.local_to_global, self.n_total, self.group).cpu().numpy()
+
+    def scan_all(self, scratch, query) -> list:
+        """One BestHit per sequence of the whole database, in global order (db_index global)."""
+        import torch
+
+        from . import BestHit
+
+        arr = self.db.scan_all_array(scratch, query)
+        g = np.asarray(self.local_to_global, dtype=np.int64)
+        rows = np.empty((len(g), HIT_COLUMNS), np.int64)
+        for k in range(len(g)):
+            rows[k] = (arr[k].score, g[k], arr[k].query_end, arr[k].target_end)
+        local = torch.from_numpy(rows).to(self._device())
+        if self.world == 1:
+            full = local.cpu().numpy()
+        else:
+            full = all_gather_hits(local, self.local_to_global, self.n_total, self.group).cpu().numpy()
+        return [BestHit(int(r[0]), int(r[1]), None if r[2] < 0 else int(r[2]), None if r[3] < 0 else int(r[3]))
+                for r in full]
+
+    def scan_aligned(self, scratch, query):
+        """The winner's (global index, Alignment) over the whole database (SearchType.Alignment
+        databases): every shard's own winner, the best of them by the scan's tie-break."""
+        import torch.distributed as dist
+
+        hit = self.db.scan_aligned(scratch, query)
+        mine = (int(hit.alignment.score), int(self.local_to_global[hit.db_index]), hit.alignment)
+        if self.world == 1:
+            return mine[1], mine[2]
+        cands = [None] * self.world
+        dist.all_gather_object(cands, mine, group=self.group)
+        best = merge_aligned(cands)
+        return best[1], best[2]
+
+    def scan_all_aligned(self, scratch, query) -> list:
+        """Every sequence's Alignment over the whole database, in global order."""
+        import torch.distributed as dist
+
+        out = []
+        self.db.scan_all_aligned(scratch, query, out)
+        mine = list(zip((int(i) for i in self.local_to_global), out))
+        if self.world == 1:
+            parts = [mine]
+        else:
+            parts = [None] * self.world
+            dist.all_gather_object(parts, mine, group=self.group)
+        full = [None] * self.n_total
+        for part in parts:
+            for gi, a in part:
+                full[gi] = a
+        return full
 
     def _device(self):
         import torch

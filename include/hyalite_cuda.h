@@ -225,6 +225,20 @@ hy_status hy_measure_dpx_peak(double *cells_per_second);
  * (the traceback fill and the int32 scan items), in DP cells per second. */
 hy_status hy_measure_dpx_peak_i32(double *cells_per_second);
 
+/* ---- failure injection for tests (no reference counterpart: the reference's scan cannot fail) -- */
+
+/* Makes the `after`-th next device allocation of this library fail as a full device would (0: the
+ * very next one), so that tests can drive every allocation's error path; -1 turns it off. The
+ * failing call returns HY_ERR_OUT_OF_MEMORY and frees what it had allocated. */
+void hy_debug_fail_device_alloc(int64_t after);
+/* Device allocations this library holds right now (a test's leak check). */
+int64_t hy_debug_live_device_allocations(void);
+/* Polls every bounded device wait makes before it gives up (a wait for a query-profile copy into
+ * shared memory, a stripe waiting on the stripe above); -1 restores the default, which bounds a
+ * wait to seconds. 0 makes every such wait give up at once, which a test uses to see
+ * HY_ERR_TIMEOUT reported and the scratch still usable afterwards. */
+void hy_debug_set_wait_polls(int64_t polls);
+
 /* ---- batched scan (no reference counterpart: the reference scans one query per call) ---------- */
 
 /* A batch runner over a fixed set of databases on one device. hy_scan_batch computes, for many

@@ -354,6 +354,79 @@ void hyb_scan(const void *dbp, void *scp, const uint8_t *q, uint64_t qlen, hyo_h
     }
 }
 
+// The best score of a query over one database and its smallest db index among ties (the grouped
+// scan's reduction, src/database.rs:160-208), without the winner's ends.
+static void best_score(const Database &db, Scratch &sc, const uint8_t *q, uint64_t qlen, int64_t *best_out,
+                       uint64_t *idx_out) {
+    int64_t best = INT32_MIN;
+    uint64_t best_idx = 0;
+    auto reduce = [&](const std::vector<uint64_t> &ix, auto &scores) {
+        for (size_t i = 0; i < ix.size(); ++i) {
+            int64_t s = scores[i];
+            if (s > best || (s == best && ix[i] < best_idx)) {
+                best = s;
+                best_idx = ix[i];
+            }
+        }
+    };
+    fill_scores(db, db.g8, q, qlen, sc.h8, sc.f8, sc.s8);
+    reduce(db.g8.indices, sc.s8);
+    fill_scores(db, db.g16, q, qlen, sc.h16, sc.f16, sc.s16);
+    reduce(db.g16.indices, sc.s16);
+    fill_scores(db, db.g32, q, qlen, sc.h32, sc.f32, sc.s32);
+    reduce(db.g32.indices, sc.s32);
+    *best_out = best;
+    *idx_out = best_idx;
+}
+
+// A query stream against one database held as `n_slices` consecutive slices (slice s holds global
+// indices slice_base[s] ..), balanced over `threads` threads so that no thread idles while a long
+// query runs: the (query, slice) units go longest query first to threads that take them one at a
+// time, each thread with its own Scratch. Per query the slices' best hits reduce to the grouped
+// scan's answer (highest score, then smallest global index), and ScoreEnd takes the winner's ends
+// from align_core, as hyb_scan does for a whole database.
+void hyb_scan_stream(const void *const *dbs, const uint64_t *slice_base, uint64_t n_slices,
+                     const uint8_t *queries, const uint64_t *qoff, uint64_t nq, hyo_hit *out,
+                     int threads) {
+    if (threads < 1) threads = 1;
+    std::vector<uint64_t> order(nq);
+    for (uint64_t k = 0; k < nq; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) {
+        return qoff[a + 1] - qoff[a] > qoff[b + 1] - qoff[b];
+    });
+    std::vector<int64_t> bs(nq * n_slices);
+    std::vector<uint64_t> bi(nq * n_slices);
+    const int64_t units = (int64_t)(nq * n_slices);
+#pragma omp parallel num_threads(threads)
+    {
+        Scratch sc;
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t u = 0; u < units; ++u) {
+            const uint64_t k = order[(uint64_t)u / n_slices], s = (uint64_t)u % n_slices;
+            best_score(*(const Database *)dbs[s], sc, queries + qoff[k], qoff[k + 1] - qoff[k],
+                       &bs[k * n_slices + s], &bi[k * n_slices + s]);
+        }
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t i = 0; i < (int64_t)nq; ++i) {
+            const uint64_t k = order[(uint64_t)i];
+            uint64_t ws = 0;
+            for (uint64_t s = 1; s < n_slices; ++s)
+                if (bs[k * n_slices + s] > bs[k * n_slices + ws]) ws = s;
+            const Database &db = *(const Database *)dbs[ws];
+            const uint64_t local = bi[k * n_slices + ws];
+            out[k].score = (int32_t)bs[k * n_slices + ws];
+            out[k].db_index = slice_base[ws] + local;
+            out[k].query_end = out[k].target_end = -1;
+            if (db.search_type == 1) {
+                int32_t sc2;
+                hyo_align_core(queries + qoff[k], qoff[k + 1] - qoff[k], db.residues.data() + db.offsets[local],
+                               db.offsets[local + 1] - db.offsets[local], db.matrix.data(), db.al, db.go,
+                               db.ge, db.mode, &sc2, &out[k].query_end, &out[k].target_end);
+            }
+        }
+    }
+}
+
 // A query stream over `threads` threads, one Scratch per thread (tests/database.rs:136-176):
 // query k is queries[qoff[k] .. qoff[k+1]].
 void hyb_scan_many(const void *dbp, const uint8_t *queries, const uint64_t *qoff, uint64_t nq,

@@ -66,6 +66,8 @@ def _load():
         "hyb_scan": (None, [C.c_void_p, C.c_void_p, _u8p, C.c_uint64, C.POINTER(Hit)]),
         "hyb_scan_scores": (None, [C.c_void_p, C.c_void_p, _u8p, C.c_uint64, _i32p]),
         "hyb_scan_many": (None, [C.c_void_p, _u8p, _u64p, C.c_uint64, C.POINTER(Hit), C.c_int]),
+        "hyb_scan_stream": (None, [C.POINTER(C.c_void_p), _u64p, C.c_uint64, _u8p, _u64p, C.c_uint64,
+                                   C.POINTER(Hit), C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -336,3 +338,35 @@ class Avx2Db:
         lib.hyb_scan_scores(self.h, sc, _p(q, _u8p), len(query), _p(out, _i32p))
         lib.hyb_scratch_destroy(sc)
         return out[: self.n]
+
+
+class Avx2SlicedDb:
+    """The AVX2 baseline over one database held as consecutive slices of about equal residues, so
+    that a query stream can be spread over every host thread in (query, slice) units
+    (hyb_scan_stream): the same hits as Avx2Db.scan_many, with no thread idle on a long query."""
+
+    def __init__(self, res, off, matrix, al, go, ge, mode, search_type, max_query_len, n_slices):
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        n = len(off) - 1
+        total = int(off[-1] - off[0])
+        cuts = [0]
+        for s in range(1, n_slices):
+            k = int(np.searchsorted(off, off[0] + total * s // n_slices))
+            if cuts[-1] < k < n:
+                cuts.append(k)
+        cuts.append(n)
+        self.slices = []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            sub_off = off[a:b + 1] - off[a]
+            self.slices.append(Avx2Db(np.asarray(res)[int(off[a]):int(off[b])], sub_off, matrix, al, go, ge, mode,
+                                      search_type, max_query_len))
+        self.base = np.ascontiguousarray(cuts[:-1], dtype=np.uint64)
+        self.n = n
+
+    def scan_stream(self, queries, threads):
+        qr, qo = concat(queries)
+        out = (Hit * max(len(queries), 1))()
+        hs = (C.c_void_p * len(self.slices))(*[d.h for d in self.slices])
+        lib.hyb_scan_stream(hs, _p(self.base, _u64p), len(self.slices), _p(qr, _u8p), _p(qo, _u64p),
+                            len(queries), out, threads)
+        return [as_hit(out[k]) for k in range(len(queries))]

@@ -272,3 +272,22 @@ def test_avx2_port_matches_oracle(mode):
         for q, g in zip(queries, got):
             assert g == ref.scan(q)
             assert list(port.scan_scores(q)) == list(ref.scan_scores(q))
+
+
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_avx2_sliced_stream_matches_oracle(mode):
+    """The balanced CPU baseline (one database in slices, (query, slice) units over threads) gives
+    the whole database's hits, ties across slice borders included."""
+    rng = np.random.default_rng(300 + mode)
+    mat = [int(v) for v in rng.integers(-4, 12, 400)]
+    seqs = [list(rng.integers(0, 20, int(rng.integers(0, 90)))) for _ in range(200)]
+    for k in (3, 77, 78, 150):  # equal best candidates in several slices: the smallest index wins
+        seqs[k] = list(range(20)) * 3
+    res, off = o.concat(seqs)
+    queries = [list(rng.integers(0, 20, int(n))) for n in (0, 1, 17, 60, 120)] + [list(range(20)) * 3]
+    mql = max(len(q) for q in queries)
+    port = o.Avx2SlicedDb(res, off, mat, 20, 11, 1, mode, 1, mql, n_slices=5)
+    assert len(port.slices) == 5
+    ref = o.OracleDb((res, off), mat, 20, 11, 1, mode, 1)
+    for q, g in zip(queries, port.scan_stream(queries, 4)):
+        assert g == ref.scan(q)

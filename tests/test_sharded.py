@@ -44,6 +44,21 @@ def test_shard_indices_partition_and_balance():
         assert max(res) - min(res) <= 2 * int(lengths.max())
 
 
+def test_take_sequences_gathers_a_shard():
+    rng = np.random.default_rng(2)
+    seqs = [list(rng.integers(0, 20, int(n))) for n in rng.integers(0, 50, 200)]
+    res, off = o.concat(seqs)
+    for world in (1, 3):
+        for mine in sharded.shard_indices([len(x) for x in seqs], world):
+            r, f = sharded.take_sequences(res, off, mine)
+            assert [list(r[int(f[i]):int(f[i + 1])]) for i in range(len(mine))] == [seqs[k] for k in mine]
+
+
+def test_merge_aligned_tie_break():
+    cands = [(30, 9, "a"), (31, 12, "b"), (31, 4, "c"), (29, 1, "d")]
+    assert sharded.merge_aligned(cands) == (31, 4, "c")
+
+
 def test_merge_hit_rows_tie_break():
     rows = torch.tensor([[[10, 7, 1, 2], [5, 3, -1, -1]],
                          [[10, 4, 3, 4], [6, 9, 0, 0]],
@@ -71,6 +86,27 @@ def _rank(rank, world, port, out_dir):
                 assert got == want, (rank, mode, st, len(q), got, want)
                 scores = sharded.all_gather_scores(torch.from_numpy(ref_local.scan_scores(q)), mine, len(seqs))
                 assert np.array_equal(scores.numpy(), ref_full.scan_scores(q)), (rank, mode, len(q))
+                # scan_all: every shard's per-target hits, scattered to global order.
+                local_all = sharded.hit_rows([Hit(*h) for h in ref_local.scan_all(q)], mine)
+                got_all = sharded.all_gather_hits(local_all, mine, len(seqs)).tolist()
+                want_all = [[s, k, -1 if qe is None else qe, -1 if te is None else te]
+                            for (s, _, qe, te), k in zip(ref_full.scan_all(q), range(len(seqs)))]
+                assert got_all == want_all, (rank, mode, st, len(q))
+            if mode in (0, 2):
+                # scan_aligned / scan_all_aligned: the winner's alignment, and every alignment.
+                for q in queries:
+                    k, aln = ref_local.scan_aligned(q)
+                    cands = [None] * world
+                    dist.all_gather_object(cands, (aln[0], int(mine[k]), aln))
+                    best = sharded.merge_aligned(cands)
+                    assert (best[1], best[2]) == ref_full.scan_aligned(q), (rank, mode, len(q))
+                    parts = [None] * world
+                    dist.all_gather_object(parts, list(zip(mine.tolist(), ref_local.scan_all_aligned(q))))
+                    full = [None] * len(seqs)
+                    for part in parts:
+                        for gi, a in part:
+                            full[gi] = a
+                    assert full == ref_full.scan_all_aligned(q), (rank, mode, len(q))
         open(os.path.join(out_dir, f"ok{rank}"), "w").close()
     finally:
         dist.destroy_process_group()
