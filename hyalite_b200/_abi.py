@@ -2,7 +2,10 @@
 
 The shared library is built in-tree (hyalite_b200/libhyalite_cuda.so). There is no fallback:
 importing the package without the library raises, so a missing build is never silently replaced by
-CPU code.
+CPU code. HYALITE_CUDA_BUILD=bounds loads the bounds-checked build instead
+(hyalite_b200/libhyalite_cuda_bounds.so, `make -C hyalite_b200/csrc bounds`): every kernel checks the
+indices each item's data can produce before using them and reports DeviceCheck instead of
+reading outside an array.
 """
 from __future__ import annotations
 
@@ -10,7 +13,11 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libhyalite_cuda.so")
+_BUILDS = {"release": "libhyalite_cuda.so", "bounds": "libhyalite_cuda_bounds.so"}
+_BUILD = os.environ.get("HYALITE_CUDA_BUILD", "release")
+if _BUILD not in _BUILDS:
+    raise ImportError(f"HYALITE_CUDA_BUILD={_BUILD!r}: expected one of {sorted(_BUILDS)}")
+LIB_PATH = os.path.join(_HERE, _BUILDS[_BUILD])
 
 # Status codes (hy_status).
 OK = 0
@@ -21,7 +28,7 @@ STATUS_NAMES = {
     7: "IncompleteBuilder", 8: "EmptyDatabase", 9: "BackendUnavailable",
     10: "InvalidBackendName", 11: "TracebackBudgetExceeded", 20: "InvalidArgument",
     21: "QueryTooLong", 22: "Cuda", 23: "OutOfMemory", 24: "Timeout", 25: "Unsupported",
-    26: "Rejected",
+    26: "Rejected", 27: "DeviceCheck",
 }
 CHOICE_UNSET = -2
 CHOICE_AUTO = -1

@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) batch_scan_ke
         ScanParams p = bq.sp[PK];
         p.boundary = L.bnd + (size_t)blockIdx.x * L.bnd_stride;
         p.bnd_col0 = p.meta[first].col_off;
+        p.bnd_cols = L.bnd_stride / (2 * sizeof(typename A::V));
         bool ok = true;
         switch (bq.mode) {
         case MODE_SW: ok = scan_unit<A, G, R, MODE_SW, false>(p, first, end, bufs, bars, phase); break;
@@ -186,6 +187,7 @@ __global__ void __launch_bounds__(1024) batch_band_kernel(const BandLaunch L) {
     ScanParams p = sp0;
     p.boundary = L.bnd + (size_t)slot * L.bnd_stride;
     p.bnd_col0 = p.meta[item].col_off;
+    p.bnd_cols = L.bnd_stride / (2 * sizeof(typename A::V));
     p.ends_out = L.ends + 3 * (size_t)slot;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     if (threadIdx.x == 0) {
@@ -439,6 +441,11 @@ hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const Bat
             p.best_key = b->d_keys + i;
             p.err = b->d_err;
             p.wait_polls = wait_polls();
+            if (i16)
+                set_extents<Pair16>(p, db, part, 0);
+            else
+                set_extents<Single32>(p, db, part, 0);
+            if (i16 && bq.tab) p.letters = (uint32_t)PairTab16::letters((int64_t)db->al);
             if (!k.need[kk]) continue;
             p.pass_bytes = k.qp[kk].pass_bytes;
             p.n_passes = k.qp[kk].n_passes;
@@ -490,11 +497,11 @@ hy_status batch_launch(hy_batch *b, uint32_t n) {
 }
 
 hy_status batch_collect(hy_batch *b, uint32_t n, hy_hit *out) {
-    if (*b->h_err) {
+    if (const int w = *b->h_err) {
         *b->h_err = 0;
         HB_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
         HB_CK(cudaStreamSynchronize(b->stream));
-        return fail(HY_ERR_TIMEOUT);
+        return fail(device_error(w));
     }
     if (n && out) memcpy(out, b->h_hits, sizeof(hy_hit) * n);
     return fail(HY_OK);

@@ -24,10 +24,16 @@ constexpr int WIN_R = 8;
 // on a high-priority stream so the longest items start first and do not form the kernel's tail.
 constexpr int LONG_G = 32;
 constexpr int LONG_R = 8;
-constexpr uint32_t LONG_W = 4096;  // measured: 1.3% faster than 2048 on the protein benchmark
+#ifndef HY_EXP_LONG_W
+#define HY_EXP_LONG_W 4096
+#endif
+constexpr uint32_t LONG_W = HY_EXP_LONG_W;  // measured: 1.3% faster than 2048 on the protein benchmark
 constexpr int BLOCK = 256;
 // Rows per lane of the bulk int16x2 kernel for a query of length qlen (passes of MAIN_G * rows).
-inline int bulk_rows(uint64_t qlen) { return qlen <= 64 ? 8 : qlen <= 192 ? 16 : 32; }
+#ifndef HY_EXP_R32_MIN
+#define HY_EXP_R32_MIN 192
+#endif
+inline int bulk_rows(uint64_t qlen) { return qlen <= 64 ? 8 : qlen <= HY_EXP_R32_MIN ? 16 : 32; }
 constexpr int BULK_MAX_RPP = 8 * 32;
 constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;
 
@@ -94,6 +100,17 @@ struct hy_db {
 };
 
 namespace hy {
+
+// The extents a bounds-checked build (HY_BOUNDS) verifies each item of `part` against: the
+// partition's residue columns, `bnd_cols` columns of boundary region, the database's indices and
+// the profile letters of lane arithmetic A.
+template <class A>
+inline void set_extents(ScanParams &p, const hy_db *db, const Partition &part, uint64_t bnd_cols) {
+    p.res_cols = part.total_cols;
+    p.bnd_cols = bnd_cols;
+    p.n_seqs = (uint32_t)db->n_seqs;
+    p.letters = (uint32_t)A::letters((int64_t)db->al);
+}
 
 // Which items one query runs in which lanes. The width proof is redone with the actual query
 // length: pairs [k0, n) fit int16 for this query and run packed; the 2*k0 longest sequences run

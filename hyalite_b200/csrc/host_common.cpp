@@ -131,6 +131,7 @@ const char *hy_status_name(hy_status s) {
     case HY_ERR_TIMEOUT: return "Timeout";
     case HY_ERR_UNSUPPORTED: return "Unsupported";
     case HY_ERR_REJECTED: return "Rejected";
+    case HY_ERR_DEVICE_CHECK: return "DeviceCheck";
     }
     return "Unknown";
 }

@@ -29,6 +29,10 @@ uint32_t wait_polls();
 // limit is a kernel parameter, frozen at capture) is captured again.
 uint64_t wait_polls_epoch();
 
+// The status of a device error word (ScanParams::err): 1 a bounded wait gave up, 2 the
+// bounds-checked build found an item it could not index safely.
+inline hy_status device_error(int word) { return word == 2 ? HY_ERR_DEVICE_CHECK : HY_ERR_TIMEOUT; }
+
 // Records the detail fields of the status being returned on this thread (hy_last_error_detail).
 hy_status fail(hy_status st, int64_t d0 = 0, int64_t d1 = 0, int64_t d2 = 0);
 

@@ -154,6 +154,7 @@ hy_status run_partition(const hy_db *db, const Partition &part, uint32_t item_ba
     p.best_key = nullptr;
     p.err = d_err;
     p.wait_polls = wait_polls();
+    set_extents<A>(p, db, part, part.total_cols);
     const int gpb = BLOCK / G;
     const int blocks = (int)((item_end - item_base + gpb - 1) / gpb);
     cudaError_t e = launch_scores_mode<A, G, R>(db->mode, p, blocks, 2 * (size_t)rg.qp.pass_bytes + 16, st);
@@ -204,5 +205,5 @@ extern "C" hy_status hy_scan_scores_noalloc(const hy_db *db, const uint8_t *d_qu
     e = cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(HY_ERR_CUDA, e);
-    return err ? fail(HY_ERR_TIMEOUT) : fail(HY_OK);
+    return err ? fail(device_error(err)) : fail(HY_OK);
 }

@@ -185,6 +185,7 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
     p.best_key = key;
     p.err = sc->d_err;
     p.wait_polls = wait_polls();
+    set_extents<A>(p, db, part, part.total_cols);
     size_t smem = 2 * (size_t)qp.pass_bytes + 16;
     const bool gprof = smem > db->smem_limit;
     if (gprof) smem = 16;
@@ -333,6 +334,7 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     p.best_key = nullptr;
     p.err = sc->d_err;
     p.wait_polls = wait_polls();
+    set_extents<A>(p, db, part, part.total_cols);
     // One pass slice per warp in shared memory; a slice too large for that runs from the profile
     // in global memory.
     const size_t budget = std::min<size_t>(BAND_SMEM_BUDGET, db->smem_limit - 16);
@@ -494,11 +496,11 @@ static hy_status issue_err_back(hy_scratch *sc) {
 // reported.
 static hy_status wait_and_check(hy_scratch *sc) {
     HY_CK(cudaStreamSynchronize(sc->stream));
-    if (*sc->h_err) {
+    if (const int w = *sc->h_err) {
         *sc->h_err = 0;
         HY_CK(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
         HY_CK(cudaStreamSynchronize(sc->stream));
-        return fail(HY_ERR_TIMEOUT);
+        return fail(device_error(w));
     }
     return fail(HY_OK);
 }
@@ -515,11 +517,11 @@ static hy_status issue_query(hy_scratch *sc, uint64_t qlen) {
 static hy_status sync_and_check(hy_scratch *sc) {
     HY_CK(cudaMemcpyAsync(sc->h_err, sc->d_err, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
     HY_CK(cudaStreamSynchronize(sc->stream));
-    if (*sc->h_err) {
+    if (const int w = *sc->h_err) {
         *sc->h_err = 0;
         HY_CK(cudaMemsetAsync(sc->d_err, 0, sizeof(int), sc->stream));
         HY_CK(cudaStreamSynchronize(sc->stream));
-        return fail(HY_ERR_TIMEOUT);
+        return fail(device_error(w));
     }
     return fail(HY_OK);
 }

@@ -83,7 +83,16 @@ struct ScanParams {
     // query end, target end} instead of to scores / qend / tend.
     int32_t *ends_out;
     uint32_t wait_polls;  // polls a wait for a profile copy makes before it gives up
+    // Extents the bounds-checked build (HY_BOUNDS) verifies every item against before use.
+    uint64_t res_cols;  // columns of the residue array
+    uint64_t bnd_cols;  // columns the boundary region holds, from bnd_col0
+    uint32_t n_seqs;    // db indices are below this
+    uint32_t letters;   // profile letters per table
 };
+
+// Error words a kernel leaves in ScanParams::err: a bounded wait gave up, or (bounds-checked
+// build) an item failed its check and was skipped.
+enum { ERR_WAIT = 1, ERR_BOUNDS = 2 };
 
 // ---- lane arithmetic -----------------------------------------------------------------------
 //
@@ -471,7 +480,11 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                     A::template load_chunk<R, G>(prof_a, prof_b, a, b, lane, r / A::EPV, pa, pb);
                 sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
                 V h;
+#ifndef HY_EXP_SW_LONG
                 if (Fl::local && !ENDS) {
+#else
+                if (false) {
+#endif
                     // SW scores, with a one-op dependency chain from row to row: with x = max(d,
                     // E, 0) - go, G = max(F - go, x) and, since go >= ge, F of the next row =
                     // max(F - ge, G) = max(F - ge, x). x >= -go, so nothing leaves int16. h here is
@@ -492,6 +505,9 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                     const V g = A::vadd(h, neggo);
                     sw.Gp[r] = g;
                     g_up = g;
+#ifdef HY_EXP_SW_LONG
+                    if (Fl::local && !ENDS) h = g;  // the score path keeps its maximum on G
+#endif
                 }
                 if (Fl::local) {
                     if (ENDS) {
@@ -719,6 +735,34 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
     }
 }
 
+#ifdef HY_BOUNDS
+// The bounds-checked build: before an item is used, every index its metadata and residue codes
+// can produce is checked against the extents in `p` (residue columns, boundary region, db
+// indices, profile letters). All G lanes of a group call it for their group's item (`active`:
+// the group has one); returns whether the item may be swept.
+template <class A, int G>
+__device__ bool item_in_bounds(const ScanParams &p, const ItemMeta &m, const int lane, const bool active) {
+    bool ok = true;
+    if (active) {
+        ok = m.col_off + m.w <= p.res_cols && m.n[0] <= m.w && m.n[1] <= m.w &&
+             (m.idx[0] == NO_INDEX || m.idx[0] < p.n_seqs) && (m.idx[1] == NO_INDEX || m.idx[1] < p.n_seqs) &&
+             (A::NH == 2 || m.idx[1] == NO_INDEX) &&
+             (p.n_passes <= 1 || (m.col_off >= p.bnd_col0 && m.col_off - p.bnd_col0 + m.w <= p.bnd_cols));
+        if (ok) {
+            const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + m.col_off;
+            for (uint32_t j = lane; j < m.w; j += G) {
+                int a, b;
+                A::residues(res[j], a, b);
+                if ((uint32_t)a >= p.letters || (uint32_t)b >= p.letters) ok = false;
+            }
+        }
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) ok &= __shfl_xor_sync(0xffffffffu, (int)ok, off, G) != 0;
+    return ok;
+}
+#endif
+
 // ---- the database scan kernel ---------------------------------------------------------------
 //
 // All groups of a block step through the passes together: the pass's query profile is one
@@ -753,11 +797,16 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
 
     const int lane = threadIdx.x % G;
     const uint32_t item = item_first == NO_INDEX ? NO_INDEX : item_first + threadIdx.x / G;
-    const bool active = item != NO_INDEX && item < item_end;
+    bool active = item != NO_INDEX && item < item_end;
     ItemMeta meta;
-    if (active) {
-        meta = p.meta[item];
-    } else {
+    if (active) meta = p.meta[item];
+#ifdef HY_BOUNDS
+    if (!item_in_bounds<A, G>(p, meta, lane, active)) {
+        if (lane == 0) atomicExch(p.err, ERR_BOUNDS);
+        active = false;
+    }
+#endif
+    if (!active) {
         meta.col_off = p.bnd_col0;
         meta.w = 0;
         meta.n[0] = meta.n[1] = 0;
@@ -786,7 +835,7 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
             const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u, p.wait_polls);
             if (__syncthreads_or(!ok)) {
                 if (threadIdx.x == 0) {
-                    atomicExch(p.err, 1);
+                    atomicExch(p.err, ERR_WAIT);
                     // This pass's copy and, if issued, the next pass's are still outstanding.
                     const uint32_t pending = (1u << buf) | (pass + 1 < p.n_passes ? 1u << (buf ^ 1) : 0u);
                     mbar_drain(bars, pending, phase);
@@ -865,6 +914,13 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
     const int W = blockDim.x / G;
     const int warp = threadIdx.x / G, lane = threadIdx.x % G;
     const ItemMeta meta = p.meta[item];
+#ifdef HY_BOUNDS
+    // Every warp checks the item (the same answer in all of them), so all skip it together.
+    if (!item_in_bounds<A, G>(p, meta, lane, true)) {
+        if (threadIdx.x == 0) atomicExch(p.err, ERR_BOUNDS);
+        return;
+    }
+#endif
     const int32_t w = (int32_t)meta.w;
     const V Sv = A::splat(p.sentinel);
     const typename A::RES *res = reinterpret_cast<const typename A::RES *>(p.res) + meta.col_off;
@@ -882,7 +938,7 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
             const bool ok = mbar_wait_bounded(bar, phase & 1u, p.wait_polls);
             if (__syncthreads_or(!ok)) {
                 if (threadIdx.x == 0) {
-                    atomicExch(p.err, 1);
+                    atomicExch(p.err, ERR_WAIT);
                     mbar_drain(bar, 1u, phase);  // the round's copy is still outstanding
                 }
                 __syncthreads();

@@ -42,7 +42,9 @@ typedef enum {
     HY_ERR_OUT_OF_MEMORY = 23,           /* device or pinned allocation failed */
     HY_ERR_TIMEOUT = 24,                 /* a bounded device wait ran out; the context stays usable */
     HY_ERR_UNSUPPORTED = 25,             /* a search type or option this backend does not build */
-    HY_ERR_REJECTED = 26                 /* serving: admission refused (queue or memory full) */
+    HY_ERR_REJECTED = 26,                /* serving: admission refused (queue or memory full) */
+    HY_ERR_DEVICE_CHECK = 27             /* bounds-checked build: a kernel skipped an item whose
+                                          * indices fell outside their arrays */
 } hy_status;
 
 typedef enum { HY_MODE_SW = 0, HY_MODE_NW = 1, HY_MODE_HW = 2, HY_MODE_OV = 3, HY_MODE_SHW = 4 } hy_mode;
