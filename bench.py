@@ -297,6 +297,29 @@ def run_cuda(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # ---- per query length: each query alone (synchronised), kernel times by class ----
+    by_len = {}
+    for i, q in enumerate(d_queries):
+        lib.hy_scratch_profile(sc._h, 1)
+        st = lib.hy_scan_device(db._h, sc._h, C.c_void_p(q.data_ptr()), len(queries[i]),
+                                C.c_void_p(d_hits[i].data_ptr()))
+        if st != 0:
+            raise hy.Error.from_status(st)
+        qms, ql, qc = (C.c_double * 3)(), (C.c_uint64 * 3)(), (C.c_double * 3)()
+        lib.hy_scratch_profile_read(sc._h, qms, ql, qc, None)
+        e = by_len.setdefault(len(queries[i]), {"queries": 0, "bulk_ms": 0.0, "bulk_cells": 0.0,
+                                                "int32_ms": 0.0, "int32_cells": 0.0, "long_ms": 0.0})
+        e["queries"] += 1
+        e["bulk_ms"] += qms[0]
+        e["bulk_cells"] += qc[0]
+        e["int32_ms"] += qms[1]
+        e["int32_cells"] += qc[1]
+        e["long_ms"] += qms[2]
+    lib.hy_scratch_profile(sc._h, 0)
+    for e in by_len.values():
+        e["bulk_gcups"] = e["bulk_cells"] / (e["bulk_ms"] * 1e-3) / 1e9 if e["bulk_ms"] > 0 else None
+        e["int32_gcups"] = e["int32_cells"] / (e["int32_ms"] * 1e-3) / 1e9 if e["int32_ms"] > 0 else None
+
     # ---- roofline of the dominant kernel (int16x2 pair kernel) ----
     peak = C.c_double()
     lib.hy_measure_dpx_peak(C.byref(peak))
@@ -310,7 +333,8 @@ def run_cuda(args):
     def _kinfo(i):
         return {"launches": int(kl[i]), "ms_per_step": kms[i] / args.steps, "cells_per_step": kcells[i] / args.steps,
                 "gcups": kcells[i] / (kms[i] * 1e-3) / 1e9 if kms[i] > 0 else None}
-    kernels = {"bulk_int16x2_pairs": _kinfo(0), "long_int16x2_pairs": _kinfo(2), "int32_items": _kinfo(1)}
+    kernels = {"bulk_int16x2_pairs": _kinfo(0), "long_int16x2_pairs": _kinfo(2), "int32_items": _kinfo(1),
+               "by_query_length_alone": {str(k): v for k, v in sorted(by_len.items())}}
     meas = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm_peak = meas.get("hbm_gbs", 6650.0)

@@ -121,6 +121,7 @@ SIGNATURES = {
     "hy_scratch_profile_read": (_st, [_vp, C.POINTER(C.c_double), _u64p, C.POINTER(C.c_double), _u64p]),
     "hy_measure_dpx_peak": (_st, [C.POINTER(C.c_double)]),
     "hy_measure_dpx_peak_i32": (_st, [C.POINTER(C.c_double)]),
+    "hy_measure_dpx_peak_i8x4": (_st, [C.POINTER(C.c_double)]),
     "hy_debug_fail_device_alloc": (None, [C.c_int64]),
     "hy_debug_live_device_allocations": (C.c_int64, []),
     "hy_debug_set_wait_polls": (None, [C.c_int64]),

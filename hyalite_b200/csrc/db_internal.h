@@ -20,20 +20,22 @@ constexpr int MAIN_G32 = 32;
 constexpr int MAIN_R32 = 16;
 constexpr int WIN_G = 32;
 constexpr int WIN_R = 8;
-// Pairs longer than LONG_W columns: one full warp each (LONG_G lanes of LONG_R rows), launched
-// on a high-priority stream so the longest items start first and do not form the kernel's tail.
+// The batched form's pairs longer than LONG_W columns run one full warp each (LONG_G lanes of
+// LONG_R rows) in a class of their own, whose boundary regions the bulk classes then need not
+// size for. Plain scans keep every pair in the bulk kernel (measured: the same time as a separate
+// long-pair kernel on the protein benchmark, with one kernel and stream fewer).
 constexpr int LONG_G = 32;
 constexpr int LONG_R = 8;
-#ifndef HY_EXP_LONG_W
-#define HY_EXP_LONG_W 4096
-#endif
-constexpr uint32_t LONG_W = HY_EXP_LONG_W;  // measured: 1.3% faster than 2048 on the protein benchmark
+constexpr uint32_t LONG_W = 4096;
+constexpr uint32_t NO_LONG_SPLIT = 0xffffffffu;
 constexpr int BLOCK = 256;
 // Rows per lane of the bulk int16x2 kernel for a query of length qlen (passes of MAIN_G * rows).
-#ifndef HY_EXP_R32_MIN
-#define HY_EXP_R32_MIN 192
-#endif
-inline int bulk_rows(uint64_t qlen) { return qlen <= 64 ? 8 : qlen <= HY_EXP_R32_MIN ? 16 : 32; }
+// SW scores run the two-column sweep at up to 16 rows per lane; the other kinds one column of up
+// to 32 rows.
+inline int bulk_rows(uint64_t qlen, bool two_col) {
+    if (qlen <= 64) return 8;
+    return two_col || qlen <= 192 ? 16 : 32;
+}
 constexpr int BULK_MAX_RPP = 8 * 32;
 constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;
 
@@ -121,7 +123,7 @@ struct QuerySplit {
     uint32_t n_i32 = 0;   // int32 items [0, n_i32)
 };
 
-inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen, uint32_t long_w = LONG_W) {
+inline QuerySplit split_for_query(const hy_db *db, uint64_t qlen, uint32_t long_w = NO_LONG_SPLIT) {
     QuerySplit q;
     // Longest target length t whose bound for this query keeps the int16 kernel exact.
     auto fits = [&](uint64_t n) {

@@ -89,6 +89,43 @@ __global__ void __launch_bounds__(256) dpx_probe_i32_kernel(int cols, uint32_t s
     if (threadIdx.x == 0 && blockIdx.x == 0) sink[0] = best & 1;
 }
 
+// The packed-int8 form (four cells per 32-bit lane op, the reference's i8 lanes restated with the
+// SIMD-video intrinsics): saturating __vsubss4 / __vaddss4 for the gaps and the diagonal,
+// __vmaxs4 for E, F, H (with a max against 0 for the local floor) and the running maximum. It
+// measures whether int8x4 lanes could beat int16x2 lanes for i8-proven sequences.
+template <int R>
+__global__ void __launch_bounds__(256) dpx_probe_i8x4_kernel(int cols, uint32_t seed, uint32_t *sink) {
+    const uint32_t ge4 = 0x01010101u, go4 = 0x0b0b0b0bu;
+    uint32_t Gp[R], E[R], P[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        Gp[r] = 0xf5f5f5f5u;
+        E[r] = 0x81818181u;
+        P[r] = (seed + threadIdx.x * 7u + r * 13u) & 0x07070707u;
+    }
+    uint32_t best = 0, diag = 0xf5f5f5f5u, up = 0xf5f5f5f5u, fup = 0x81818181u;
+    for (int j = 0; j < cols; ++j) {
+        uint32_t g_up = up, f = fup, gd = diag;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            E[r] = __vmaxs4(__vsubss4(E[r], ge4), Gp[r]);
+            f = __vmaxs4(__vsubss4(f, ge4), g_up);
+            const uint32_t d = __vaddss4(gd, P[r]);
+            const uint32_t h = __vmaxs4(__vmaxs4(d, E[r]), __vmaxs4(f, 0u));
+            gd = Gp[r];
+            const uint32_t g = __vsubss4(h, go4);
+            Gp[r] = g;
+            g_up = g;
+            best = __vmaxs4(best, h);
+        }
+        diag = up;
+        up = g_up ^ (uint32_t)j;
+        fup = f;
+    }
+    if (best == 0xdeadbeefu) sink[threadIdx.x] = best;
+    if (threadIdx.x == 0 && blockIdx.x == 0) sink[0] = best & 1u;
+}
+
 template <class K>
 static hy_status time_probe(K launch, double cells_per_launch, double *cells_per_second) {
     cudaEvent_t a, b;
@@ -162,4 +199,21 @@ extern "C" hy_status hy_measure_dpx_peak(double *cells_per_second) {
     const double cells = (double)blocks * threads * cols * R * 2.0;
     *cells_per_second = cells / (best_ms * 1e-3);
     return fail(HY_OK);
+}
+
+extern "C" hy_status hy_measure_dpx_peak_i8x4(double *cells_per_second) {
+    using namespace hy;
+    if (!cells_per_second) return fail(HY_ERR_INVALID_ARGUMENT);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint32_t *sink = nullptr;
+    if (cudaMalloc(&sink, 1024 * sizeof(uint32_t)) != cudaSuccess) return fail(HY_ERR_OUT_OF_MEMORY);
+    constexpr int R = 16;
+    const int blocks = sms * 8, threads = 256, cols = 1024;
+    hy_status st = time_probe(
+        [&](int it) { dpx_probe_i8x4_kernel<R><<<blocks, threads>>>(cols, (uint32_t)it, sink); },
+        (double)blocks * threads * cols * R * 4.0, cells_per_second);
+    cudaFree(sink);
+    return st;
 }

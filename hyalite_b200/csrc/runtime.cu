@@ -23,10 +23,7 @@ struct hy_scratch {
     // The int32 part of a scan runs on a second stream, forked from and joined back into `stream`.
     cudaStream_t stream2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    // The long int16x2 pairs run on a third stream; both side streams have the highest priority.
-    cudaStream_t stream3 = nullptr;
-    cudaEvent_t ev_join3 = nullptr;
-    uint8_t *d_prof16l = nullptr;
+
     uint8_t *d_query = nullptr;
     uint8_t *d_prof16 = nullptr, *d_prof32 = nullptr, *d_profw16 = nullptr, *d_profw32 = nullptr;
     void *d_bnd16 = nullptr, *d_bnd32 = nullptr;
@@ -93,11 +90,10 @@ static cudaError_t launch_mode(const ScanParams &p, int blocks, int threads, siz
 }
 
 // The launch shapes that also exist in the global-memory-profile form (large alphabets): the bulk
-// pairs with 8 rows per lane, the long pairs and the int32 items.
+// pairs with 8 rows per lane and the int32 items.
 template <class A, int G, int R>
 constexpr bool has_gprof_form() {
-    return (A::NH == 2 && G == MAIN_G && R == 8) || (A::NH == 2 && G == LONG_G && R == LONG_R) ||
-           (A::NH == 1 && G == MAIN_G32 && R == MAIN_R32);
+    return (A::NH == 2 && G == MAIN_G && R == 8) || (A::NH == 1 && G == MAIN_G32 && R == MAIN_R32);
 }
 
 template <class A, int G, int R>
@@ -198,7 +194,7 @@ static hy_status enqueue_partition(const hy_db *db, hy_scratch *sc, const Partit
             sc->events.push_back({a, b});
             sc->event_part.push_back(0);
         }
-        const int cls = i16 ? (G == LONG_G ? 2 : 0) : 1;
+        const int cls = i16 ? 0 : 1;
         sc->event_part[sc->n_events] = cls;
         sc->event_cells[cls] +=
             (double)qlen * (double)(part.res_prefix[item_end] - part.res_prefix[item_base]);
@@ -236,29 +232,16 @@ static hy_status enqueue_scores_p(const hy_db *db, hy_scratch *sc, const uint8_t
         if (st != HY_OK) return st;
         HY_CK(cudaEventRecord(sc->ev_join, sc->stream2));
     }
-    const bool long_pairs = split.kl > split.k0;
-    if (long_pairs) {
-        HY_CK(cudaEventRecord(sc->ev_fork, sc->stream));
-        HY_CK(cudaStreamWaitEvent(sc->stream3, sc->ev_fork, 0));
-        const int gpbl = BLOCK / LONG_G;
-        const int blocks = (int)((split.kl - split.k0 + gpbl - 1) / gpbl);
-        st = enqueue_partition<P, LONG_G, LONG_R>(db, sc, db->p16, split.k0, split.kl, d_query,
-                                                      qlen, ends, key, scores, sc->d_prof16l,
-                                                      sc->d_bnd16, nullptr, blocks, BLOCK,
-                                                      sc->stream3);
-        if (st != HY_OK) return st;
-        HY_CK(cudaEventRecord(sc->ev_join3, sc->stream3));
-    }
-    if (split.kl < db->p16.n_items) {
-        const int blocks = (int)((db->p16.n_items - split.kl + gpb - 1) / gpb);
+    if (split.k0 < db->p16.n_items) {
+        const int blocks = (int)((db->p16.n_items - split.k0 + gpb - 1) / gpb);
         // Rows per lane by query length: more rows amortise the per-step work, fewer keep the
         // padding of a short query's single pass small. An alphabet whose two pass slices do not
         // fit in shared memory runs with 8 rows, from the profile in global memory if need be.
-        int rows = bulk_rows(qlen);
+        int rows = bulk_rows(qlen, db->mode == MODE_SW && !ends);
         const size_t slice = profile_slice_row_bytes<P>(db->al) * MAIN_G;
         if (2 * slice * rows + 16 > db->smem_limit) rows = 8;
 #define HY_BULK(RR)                                                                              \
-    enqueue_partition<P, MAIN_G, RR>(db, sc, db->p16, split.kl, db->p16.n_items, d_query,        \
+    enqueue_partition<P, MAIN_G, RR>(db, sc, db->p16, split.k0, db->p16.n_items, d_query,        \
                                           qlen, ends, key, scores, sc->d_prof16, sc->d_bnd16,    \
                                           nullptr, blocks, BLOCK, sc->stream)
         st = rows == 8 ? HY_BULK(8) : rows == 16 ? HY_BULK(16) : HY_BULK(32);
@@ -266,7 +249,6 @@ static hy_status enqueue_scores_p(const hy_db *db, hy_scratch *sc, const uint8_t
         if (st != HY_OK) return st;
     }
     if (forked) HY_CK(cudaStreamWaitEvent(sc->stream, sc->ev_join, 0));
-    if (long_pairs) HY_CK(cudaStreamWaitEvent(sc->stream, sc->ev_join3, 0));
     return fail(HY_OK);
 }
 
@@ -808,7 +790,6 @@ uint64_t hy_db_scratch_bytes(const hy_db *db) {
     uint64_t b = mq + 3 * 4 * db->n_seqs + 64 + sizeof(hy_hit);
     const uint64_t pr = pair_slice_row_bytes(db), sr = profile_slice_row_bytes<Single32>(db->al);
     b += npass(mq, BULK_MAX_RPP) * BULK_MAX_RPP * pr;
-    b += npass(mq, LONG_G * LONG_R) * LONG_G * LONG_R * pr;
     b += npass(mq, MAIN_G32 * MAIN_R32) * MAIN_G32 * MAIN_R32 * sr;
     b += npass(mq, WIN_G * WIN_R) * WIN_G * WIN_R * (pr + sr);
     if (mq > (uint64_t)std::min({MAIN_G * 8, MAIN_G * MAIN_R16, MAIN_G32 * MAIN_R32, WIN_G * WIN_R}))
@@ -835,8 +816,6 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
     int prio_low = 0, prio_high = 0;
     ck(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
     ck(cudaStreamCreateWithPriority(&sc->stream2, cudaStreamNonBlocking, prio_high));
-    ck(cudaStreamCreateWithPriority(&sc->stream3, cudaStreamNonBlocking, prio_high));
-    ck(cudaEventCreateWithFlags(&sc->ev_join3, cudaEventDisableTiming));
     ck(cudaEventCreateWithFlags(&sc->ev_fork, cudaEventDisableTiming));
     ck(cudaEventCreateWithFlags(&sc->ev_join, cudaEventDisableTiming));
     ck(hy::dev_malloc(&sc->d_query, mq));
@@ -845,7 +824,6 @@ hy_status hy_scratch_create(const hy_db *db, hy_scratch **out) {
     };
     const uint64_t pr = pair_slice_row_bytes(db), sr = profile_slice_row_bytes<Single32>(db->al);
     ck(hy::dev_malloc(&sc->d_prof16, prof_bytes(BULK_MAX_RPP, pr)));
-    ck(hy::dev_malloc(&sc->d_prof16l, prof_bytes(LONG_G * LONG_R, pr)));
     ck(hy::dev_malloc(&sc->d_prof32, prof_bytes(MAIN_G32 * MAIN_R32, sr)));
     ck(hy::dev_malloc(&sc->d_profw16, prof_bytes(WIN_G * WIN_R, pr)));
     ck(hy::dev_malloc(&sc->d_profw32, prof_bytes(WIN_G * WIN_R, sr)));
@@ -884,7 +862,6 @@ void hy_scratch_destroy(hy_scratch *sc) {
     tb_context_destroy(sc->tb);
     hy::dev_free(sc->d_query);
     hy::dev_free(sc->d_prof16);
-    hy::dev_free(sc->d_prof16l);
     hy::dev_free(sc->d_prof32);
     hy::dev_free(sc->d_profw16);
     hy::dev_free(sc->d_profw32);
@@ -908,9 +885,6 @@ void hy_scratch_destroy(hy_scratch *sc) {
         cudaEventDestroy(e.second);
     }
     if (sc->stream2) cudaStreamSynchronize(sc->stream2);
-    if (sc->stream3) cudaStreamSynchronize(sc->stream3);
-    if (sc->ev_join3) cudaEventDestroy(sc->ev_join3);
-    if (sc->stream3) cudaStreamDestroy(sc->stream3);
     if (sc->ev_fork) cudaEventDestroy(sc->ev_fork);
     if (sc->ev_join) cudaEventDestroy(sc->ev_join);
     if (sc->stream2) cudaStreamDestroy(sc->stream2);

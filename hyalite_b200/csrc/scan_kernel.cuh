@@ -356,10 +356,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
-// After a wait gave up: lets the copies still in flight into this block's shared memory land
-// before the block exits (bounded again, by the default number of polls). `pending` holds the
-// barriers with a copy outstanding (bit b: bars[b]) and `phase` the parity each waits for.
-__device__ __forceinline__ void mbar_drain(uint64_t *bars, uint32_t pending, uint32_t phase) {
+// After a wait gave up (one thread of the block): records the timeout and lets the copies still
+// in flight into the block's shared memory land before the block exits (bounded again, by the
+// default number of polls; the block's shared memory stays allocated while this thread runs).
+// `pending` holds the barriers with a copy outstanding (bit b: bars[b]) and `phase` the parity
+// each waits for. Out of line: the scan kernels' hot loops keep their register allocation.
+static __device__ __noinline__ void wait_gave_up(int *err, uint64_t *bars, uint32_t pending, uint32_t phase) {
+    atomicExch(err, ERR_WAIT);
     for (int b = 0; b < 2; ++b)
         if ((pending >> b) & 1u) mbar_wait_bounded(&bars[b], (phase >> b) & 1u, 1u << 24);
 }
@@ -480,11 +483,7 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                     A::template load_chunk<R, G>(prof_a, prof_b, a, b, lane, r / A::EPV, pa, pb);
                 sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
                 V h;
-#ifndef HY_EXP_SW_LONG
                 if (Fl::local && !ENDS) {
-#else
-                if (false) {
-#endif
                     // SW scores, with a one-op dependency chain from row to row: with x = max(d,
                     // E, 0) - go, G = max(F - go, x) and, since go >= ge, F of the next row =
                     // max(F - ge, G) = max(F - ge, x). x >= -go, so nothing leaves int16. h here is
@@ -505,9 +504,6 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                     const V g = A::vadd(h, neggo);
                     sw.Gp[r] = g;
                     g_up = g;
-#ifdef HY_EXP_SW_LONG
-                    if (Fl::local && !ENDS) h = g;  // the score path keeps its maximum on G
-#endif
                 }
                 if (Fl::local) {
                     if (ENDS) {
@@ -676,6 +672,157 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
     sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
 }
 
+// ---- two columns per step: the SW score sweep of int16x2 pairs ----------------------------------
+//
+// Lane L works on columns j0 = 2(s - L) + 1 and j1 = j0 + 1 at step s, R rows each: the per-step
+// work (shuffles, residue and boundary loads, loop control) is spread over 2R rows of work while a
+// lane keeps only R rows of state, and the F chains of the two columns (column j1 one row behind
+// column j0) give the scheduler two independent dependency chains. Long form of the recurrence
+// (E, F, H = max(d, E, F, 0), G = H - go); the running maximum is kept on G.
+template <class A, int R>
+struct Sweep2 {
+    typename A::V Gp[R], E[R];        // G of the previous column and E, per row slot
+    typename A::V diag;               // G of the row above the lane at the column before j0
+    typename A::V botG[2], botF[2];   // this lane's last row at columns j0, j1, for lane L + 1
+};
+
+// One column of R rows: E, F, H, G in place; returns the last row's G and F.
+template <class A, int G, int R>
+__device__ __forceinline__ void sweep2_column(Sweep2<A, R> &sw, const int a, const int b, const int lane,
+                                              const uint8_t *prof_a, const uint8_t *prof_b,
+                                              typename A::V g_up, typename A::V f, typename A::V gd,
+                                              const typename A::V negge, const typename A::V neggo,
+                                              typename A::V &best, typename A::V &outG,
+                                              typename A::V &outF) {
+    typedef typename A::V V;
+    V pa[A::EPV], pb[A::EPV];
+    V hprev = A::splat(0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (r % A::EPV == 0) A::template load_chunk<R, G>(prof_a, prof_b, a, b, lane, r / A::EPV, pa, pb);
+        sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
+        f = A::addmax(f, negge, g_up);
+        const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
+        const V h = A::vmax3_relu(d, sw.E[r], f);
+        gd = sw.Gp[r];
+        const V g = A::vadd(h, neggo);
+        sw.Gp[r] = g;
+        g_up = g;
+        if (r & 1)
+            best = A::vmax3(best, hprev, g);
+        else
+            hprev = g;
+    }
+    if (R & 1) best = A::vmax(best, hprev);
+    outG = g_up;
+    outF = f;
+}
+
+// Step s of one lane (see above). The residue codes of columns j0, j1 come as one 32-bit word
+// (`codes`) and, for lane 0 after the first pass, the boundary values of both columns as one
+// 16-byte word (`up`: G, F of j0, then of j1). CHECKED steps test each column against [1, w].
+template <class A, int G, int R, bool CHECKED>
+__device__ __forceinline__ void sweep2_step(Sweep2<A, R> &sw, const int s, const int lane, const int32_t w,
+                                            const uint8_t *prof_a, const uint8_t *prof_b,
+                                            const bool first_pass, const bool last_pass,
+                                            typename A::V *bnd, const SweepConst<A> &k,
+                                            typename A::V &best, const uint32_t codes, const uint4 up) {
+    typedef typename A::V V;
+    const int32_t j0 = 2 * (s - lane) + 1;
+    V upG0 = __shfl_up_sync(0xffffffffu, sw.botG[0], 1, G);
+    V upF0 = __shfl_up_sync(0xffffffffu, sw.botF[0], 1, G);
+    V upG1 = __shfl_up_sync(0xffffffffu, sw.botG[1], 1, G);
+    V upF1 = __shfl_up_sync(0xffffffffu, sw.botF[1], 1, G);
+    const bool live0 = !CHECKED || (j0 >= 1 && j0 <= w);
+    const bool live1 = !CHECKED || (j0 + 1 >= 1 && j0 + 1 <= w);
+    if (lane == 0) {
+        if (first_pass) {
+            upG0 = upG1 = k.top_free_g;
+            upF0 = upF1 = k.Sv;
+        } else {
+            upG0 = up.x;
+            upF0 = up.y;
+            upG1 = up.z;
+            upF1 = up.w;
+        }
+    }
+    int a, b;
+    if (live0) {
+        A::residues((typename A::RES)(codes & 0xffffu), a, b);
+        sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG0, upF0, sw.diag, k.negge, k.neggo, best,
+                               sw.botG[0], sw.botF[0]);
+    }
+    if (live1) {
+        A::residues((typename A::RES)(codes >> 16), a, b);
+        sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG1, upF1, upG0, k.negge, k.neggo, best,
+                               sw.botG[1], sw.botF[1]);
+    }
+    if (live0) sw.diag = live1 ? upG1 : upG0;
+    if (lane == G - 1 && !last_pass && live0)
+        *reinterpret_cast<uint4 *>(bnd + 2 * (j0 - 1)) = make_uint4(sw.botG[0], sw.botF[0], sw.botG[1], sw.botF[1]);
+}
+
+// One whole pass of the two-column sweep: `steps` = ceil(wmax / 2) + G - 1; steps in
+// [G - 1, w_min / 2) have both columns of every lane of the warp inside its item and run
+// unchecked, with the next step's codes and boundary values loaded one step ahead.
+template <class A, int G, int R>
+__device__ __forceinline__ void sweep2_pass(const int lane, const int steps, const int w_min, const int32_t w,
+                                            const typename A::RES *__restrict__ res, const uint8_t *prof_a,
+                                            const uint8_t *prof_b, const int32_t row0, const bool first_pass,
+                                            const bool last_pass, typename A::V *bnd, const int32_t go,
+                                            const int32_t ge, const typename A::V Sv, typename A::V &best) {
+    typedef typename A::V V;
+    static_assert(A::NH == 2 && sizeof(typename A::RES) == 2, "two-column steps pair int16 codes");
+    Sweep2<A, R> sw;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        sw.Gp[r] = A::splat(-(int64_t)go);  // local mode: the left border is free (H = 0)
+        sw.E[r] = Sv;
+    }
+    sw.diag = A::splat(-(int64_t)go);
+    sw.botG[0] = sw.botG[1] = sw.botF[0] = sw.botF[1] = A::splat(0);
+    (void)row0;
+    SweepConst<A> k;
+    k.negge = A::splat(-(int64_t)ge);
+    k.neggo = A::splat(-(int64_t)go);
+    k.Sv = Sv;
+    k.top_free_g = A::splat(-(int64_t)go);
+    const uint32_t *res2 = reinterpret_cast<const uint32_t *>(res);  // codes of columns (2i+1, 2i+2)
+    const uint4 *bnd4 = reinterpret_cast<const uint4 *>(bnd);          // boundary of the same pair
+    const uint4 none = make_uint4(0, 0, 0, 0);
+    // Loads of step s for this lane: column pair index s - lane (clamped to the item for
+    // checked steps, where a dead pair's values are never used).
+    auto codes_at = [&](int s, int32_t wl) -> uint32_t {
+        const int i = s - lane;
+        return (i >= 0 && 2 * i < wl) ? res2[i] : 0u;
+    };
+    auto up_at = [&](int s, int32_t wl) -> uint4 {
+        const int i = s - lane;
+        return (lane == 0 && !first_pass && i >= 0 && 2 * i < wl) ? bnd4[i] : none;
+    };
+    const int fast_lo = min(steps, G - 1);
+    const int fast_hi = max(fast_lo, min(steps, w_min / 2));
+    for (int s = 0; s < fast_lo; ++s)
+        sweep2_step<A, G, R, true>(sw, s, lane, w, prof_a, prof_b, first_pass, last_pass, bnd, k, best,
+                                   codes_at(s, w), up_at(s, w));
+    if (fast_lo < fast_hi) {
+        uint32_t c_cur = res2[fast_lo - lane];
+        uint4 u_cur = (lane == 0 && !first_pass) ? bnd4[fast_lo - lane] : none;
+        for (int s = fast_lo; s < fast_hi; ++s) {
+            const int sn = min(s + 1, fast_hi - 1);
+            const uint32_t c_next = res2[sn - lane];
+            const uint4 u_next = (lane == 0 && !first_pass) ? bnd4[sn - lane] : u_cur;
+            sweep2_step<A, G, R, false>(sw, s, lane, w, prof_a, prof_b, first_pass, last_pass, bnd, k, best,
+                                        c_cur, u_cur);
+            c_cur = c_next;
+            u_cur = u_next;
+        }
+    }
+    for (int s = fast_hi; s < steps; ++s)
+        sweep2_step<A, G, R, true>(sw, s, lane, w, prof_a, prof_b, first_pass, last_pass, bnd, k, best,
+                                   codes_at(s, w), up_at(s, w));
+}
+
 // Group reduction of the per-lane candidates, border seeds, output and best-key fold. Every lane
 // of the warp must call it (it shuffles).
 template <class A, int G, int MODE, bool ENDS>
@@ -733,6 +880,14 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
         }
         if ((threadIdx.x & 31) == 0 && key != 0) atomicMax(best_key, key);
     }
+}
+
+// Whether a scan launch shape runs the two-column sweep: SW scores of int16x2 pairs with at most
+// 16 rows per lane (measured: on the protein benchmark as fast as one column of 32 rows, 10%
+// faster on 64-residue DNA queries).
+template <class A, int R, int MODE, bool ENDS, bool GPROF>
+__host__ __device__ constexpr bool two_col_form() {
+    return A::NH == 2 && ModeFlags<MODE>::local && !ENDS && !GPROF && R <= 16;
 }
 
 #ifdef HY_BOUNDS
@@ -818,6 +973,7 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
     const int w_min = (int)__reduce_min_sync(0xffffffffu, meta.w);
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
+    const int steps2 = wmax == 0 ? 0 : (int)(wmax + 1) / 2 + G - 1;  // two-column form
 
     V best = A::splat(ModeFlags<MODE>::local && !ENDS ? -(int64_t)p.go : 0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
@@ -833,24 +989,27 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
             prof = p.profile + (size_t)pass * p.pass_bytes;
         } else {
             const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u, p.wait_polls);
+            phase ^= 1u << buf;
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) {
-                    atomicExch(p.err, ERR_WAIT);
-                    // This pass's copy and, if issued, the next pass's are still outstanding.
-                    const uint32_t pending = (1u << buf) | (pass + 1 < p.n_passes ? 1u << (buf ^ 1) : 0u);
-                    mbar_drain(bars, pending, phase);
-                }
-                __syncthreads();
+                // This pass's copy and, if issued, the next pass's are still outstanding.
+                if (threadIdx.x == 0)
+                    wait_gave_up(p.err, bars, (1u << buf) | (pass + 1 < p.n_passes ? 1u << (buf ^ 1) : 0u),
+                                 phase ^ (1u << buf));
                 return false;
             }
-            phase ^= 1u << buf;
             prof = prof_buf[buf];
         }
-        sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof,
-                                        prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
-                                        p.vrow0 + pass * RPP + lane * R, pass == 0,
-                                        pass == p.n_passes - 1, bnd, p.qlen, p.go, p.ge, Sv, best,
-                                        cand);
+        if constexpr (two_col_form<A, R, MODE, ENDS, GPROF>())
+            sweep2_pass<A, G, R>(lane, steps2, w_min, (int32_t)meta.w, res, prof,
+                                 prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
+                                 p.vrow0 + pass * RPP + lane * R, pass == 0, pass == p.n_passes - 1, bnd,
+                                 p.go, p.ge, Sv, best);
+        else
+            sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof,
+                                            prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
+                                            p.vrow0 + pass * RPP + lane * R, pass == 0,
+                                            pass == p.n_passes - 1, bnd, p.qlen, p.go, p.ge, Sv, best,
+                                            cand);
         __syncthreads();  // the profile buffer and boundary row are free again
         if (!GPROF && threadIdx.x == 0 && pass + 2 < p.n_passes)
             bulk_load(smem + (size_t)buf * p.pass_bytes, p.profile + (size_t)(pass + 2) * p.pass_bytes,
@@ -862,13 +1021,16 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
 }
 
 // Resident 256-thread blocks per SM each launch shape is compiled for (its register budget).
-template <class A, int G, int R>
+// The two-column sweep of 16 rows per lane is compiled for two blocks (measured faster than three
+// with the spills three would need).
+template <class A, int G, int R, bool TWO_COL = false>
 constexpr int scan_min_blocks() {
-    return A::NH == 1 ? 2 : (G == 8 && R == 8) ? 4 : (G == 8 && R == 32) ? 2 : 3;
+    return A::NH == 1 ? 2 : (G == 8 && R == 8) ? 4 : (G == 8 && R == 32) ? 2 : (TWO_COL && R == 16) ? 2 : 3;
 }
 
 template <class A, int G, int R, int MODE, bool ENDS, bool GPROF = false>
-__global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) scan_kernel(const ScanParams p) {
+__global__ void __launch_bounds__(256, (scan_min_blocks<A, G, R, two_col_form<A, R, MODE, ENDS, GPROF>()>()))
+    scan_kernel(const ScanParams p) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (GPROF ? 0 : 2 * (size_t)p.pass_bytes));
     const int gpb = blockDim.x / G;
@@ -936,15 +1098,11 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
             if (threadIdx.x == 0)
                 bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
             const bool ok = mbar_wait_bounded(bar, phase & 1u, p.wait_polls);
+            phase ^= 1u;
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) {
-                    atomicExch(p.err, ERR_WAIT);
-                    mbar_drain(bar, 1u, phase);  // the round's copy is still outstanding
-                }
-                __syncthreads();
+                if (threadIdx.x == 0) wait_gave_up(p.err, bar, 1u, phase ^ 1u);  // the round's copy
                 return;
             }
-            phase ^= 1u;
         }
         const int pass = first + warp;
         const bool mine = warp < cnt && w > 0;

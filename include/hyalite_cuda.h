@@ -214,9 +214,9 @@ hy_status hy_scratch_sync(hy_scratch *scratch);
 
 /* While enabled, every main scan-kernel launch on this scratch is bracketed by CUDA events on the
  * stream it runs on. _read synchronises and returns, since the last read (or enable), the summed
- * kernel time, launch count and real DP cells of the bulk int16x2 pair kernel ([0]), the int32
- * kernel ([1]) and the long-pair int16x2 kernel ([2]), plus the number of kernels of every kind
- * this scratch launched; then resets them. */
+ * kernel time, launch count and real DP cells of the bulk int16x2 pair kernel ([0]) and the int32
+ * kernel ([1]) ([2] is kept for a separate long-pair kernel, which plain scans no longer launch:
+ * zero), plus the number of kernels of every kind this scratch launched; then resets them. */
 hy_status hy_scratch_profile(hy_scratch *scratch, int enable);
 hy_status hy_scratch_profile_read(hy_scratch *scratch, double kernel_ms[3], uint64_t launches[3],
                                   double cells[3], uint64_t *all_launches);
@@ -226,6 +226,10 @@ hy_status hy_measure_dpx_peak(double *cells_per_second);
 /* The same recurrence in int32 DPX lanes (one cell per op): the roofline of the int32 kernels
  * (the traceback fill and the int32 scan items), in DP cells per second. */
 hy_status hy_measure_dpx_peak_i32(double *cells_per_second);
+/* The same recurrence in packed int8x4 lanes (four cells per op, saturating SIMD-video
+ * intrinsics, as the reference's i8 lanes saturate), in DP cells per second: the measurement
+ * behind keeping i8-proven sequences in int16x2 lanes. */
+hy_status hy_measure_dpx_peak_i8x4(double *cells_per_second);
 
 /* ---- failure injection for tests (no reference counterpart: the reference's scan cannot fail) -- */
 

@@ -72,6 +72,27 @@ def test_scan_wait_that_gives_up_is_a_timeout_and_the_scratch_recovers():
     assert got == ref.scan_all(q)
 
 
+def test_int32_pipeline_wait_that_gives_up_is_a_timeout_and_the_scratch_recovers():
+    # A 3000-residue query against targets longer than 2978 residues: those run in int32 lanes
+    # (BLOSUM62's largest entry 11: 11 * 2979 + 11 > 32767), as pipelined passes.
+    hy = _hy()
+    rng = np.random.default_rng(506)
+    seqs = [rng.integers(0, 20, int(k)).astype(np.uint8) for k in rng.integers(1, 400, 300)]
+    seqs += [rng.integers(0, 20, int(k)).astype(np.uint8) for k in (3100, 3500, 4200)]
+    db = (hy.Database.builder().sequences(seqs).scoring(hy.Scoring(20, BLOSUM62, 11, 1)).mode(hy.Mode.Sw)
+          .search_type(hy.SearchType.ScoreEnd).max_query_len(3000).build())
+    assert db.partition()[1] > 0
+    ref = o.OracleDb(seqs, BLOSUM62, 20, 11, 1, 0, 1)
+    sc = hy.Scratch(db)
+    q = seqs[-2][:3000].copy()
+    with _WaitPolls(hy, 0):
+        with pytest.raises(hy.Error) as e:
+            db.scan_scores_array(sc, q)
+        assert e.value.kind == "Timeout"
+    assert np.array_equal(db.scan_scores_array(sc, q), ref.scan_scores(q))
+    assert hit_tuple(db.scan(sc, q)) == ref.scan(q)
+
+
 def test_batch_wait_that_gives_up_is_a_timeout_and_the_batch_recovers():
     hy = _hy()
     rng = np.random.default_rng(502)
