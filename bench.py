@@ -39,10 +39,11 @@ N_SEQS = 500_000
 GO, GE = 11, 1
 AL = 20
 # DRAM bytes (read + write) per DP cell of the int16x2 pair kernel, from one ncu capture of
-# scan_kernel<Pair16, 8, 32> on 400,000 sequences x one 1000-residue query: 1.358e9 bytes for
-# 1.563e11 cells. The traffic is the boundary rows between query passes plus the residues, so it
-# grows with cells at a fixed rows-per-pass; profiles/ holds the capture's summary and command.
-DRAM_BYTES_PER_CELL = 1.358e9 / 1.563e11
+# scan_kernel<Pair16, 8, 16> (two-column sweep) on 400,000 sequences x one 1000-residue query:
+# 1.039e9 + 1.625e9 bytes for 1.655e11 cells. The traffic is the boundary rows between query
+# passes plus the residues, so it grows with cells at a fixed rows-per-pass; profiles/ holds the
+# capture's summary and command.
+DRAM_BYTES_PER_CELL = (1.039e9 + 1.625e9) / 1.655e11
 
 
 def make_workload(seed: int, n_seqs: int = N_SEQS):
@@ -374,7 +375,7 @@ def run_cuda(args):
                          "traffic": cells16_per_launch * DRAM_BYTES_PER_CELL,
                          "traffic_note": "bytes per launch: dram read+write per cell from one ncu capture "
                                          "(400k sequences x 1000-residue query) times this launch's cells",
-                         "kernel": "scan_kernel<Pair16,8,R,SW>, R = 8/16/32 rows per lane by query length",
+                         "kernel": "scan_kernel<Pair16,8,R,SW>, two-column sweep, R = 8 (queries <= 64) or 16 rows per lane",
                          "avg_launch_ms": avg16_ms,
                          "launches": int(kl[0]), "cells_per_launch": cells16_per_launch,
                          "peak_source": "measured: hy_measure_dpx_peak (register-resident per-cell DPX mix)"},

@@ -43,6 +43,29 @@ constexpr size_t PAIR_GPROF_BYTES = 256ull << 20;
 constexpr uint64_t PAIR_MAX_CHUNKS = 16;
 constexpr uint64_t PAIR_CHUNK_MIN = 1 << 16;
 constexpr uint64_t PAIR_CHUNK_BYTES = 512ull << 20;
+// The chunk boundaries of pairs [0, L): cut at equal shares of the residues (query plus target
+// bytes), so that no chunk holds much more than PAIR_CHUNK_BYTES whatever the order of long and
+// short pairs (one pair is never split); every chunk gets at least one pair.
+static std::vector<uint64_t> plan_pair_chunks(const uint64_t *q_off, const uint64_t *t_off, uint64_t L) {
+    auto residues = [&](uint64_t a) { return (q_off[a] - q_off[0]) + (t_off[a] - t_off[0]); };
+    const uint64_t total = residues(L);
+    const uint64_t n_chunks = std::min<uint64_t>(
+        L, std::max<uint64_t>({1, std::min<uint64_t>(PAIR_MAX_CHUNKS, L / PAIR_CHUNK_MIN),
+                               (total + PAIR_CHUNK_BYTES - 1) / PAIR_CHUNK_BYTES}));
+    std::vector<uint64_t> b(n_chunks + 1, 0);
+    b[n_chunks] = L;
+    for (uint64_t c = 1; c < n_chunks; ++c) {
+        const uint64_t target = (uint64_t)((unsigned __int128)total * c / n_chunks);
+        uint64_t lo = 0, hi = L;  // first a with residues(a) >= target
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (residues(mid) >= target) hi = mid; else lo = mid + 1;
+        }
+        b[c] = std::min(std::max(lo, b[c - 1] + 1), L - (n_chunks - c));
+    }
+    return b;
+}
+
 // Pinned staging slots the chunks rotate through.
 constexpr int PAIR_SLOTS = 3;
 // Most warps (128-row stripes) the long pairs of one call may take on the stripe kernel.
@@ -820,11 +843,9 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
             for (cudaEvent_t &e : ctx.slot_ev) HY_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
         const uint64_t L = n_len;
-        const uint64_t res_bytes = (q_off[L] - q_off[0]) + (t_off[L] - t_off[0]);
-        const uint64_t n_chunks = std::min<uint64_t>(
-            L, std::max<uint64_t>({1, std::min<uint64_t>(PAIR_MAX_CHUNKS, L / PAIR_CHUNK_MIN),
-                                   (res_bytes + PAIR_CHUNK_BYTES - 1) / PAIR_CHUNK_BYTES}));
-        auto chunk_at = [&](uint64_t c) { return L * c / n_chunks; };
+        const std::vector<uint64_t> bounds = plan_pair_chunks(q_off, t_off, L);
+        const uint64_t n_chunks = bounds.size() - 1;
+        auto chunk_at = [&](uint64_t c) { return bounds[c]; };
         while (ctx.ev.size() < 3 * n_chunks + 2) {
             cudaEvent_t e;
             HY_CK(cudaEventCreate(&e));
@@ -1252,4 +1273,14 @@ extern "C" hy_status hy_align_pairs_phases(double *ms, uint32_t n) {
     if (!ms && n) return fail(HY_ERR_INVALID_ARGUMENT);
     for (uint32_t i = 0; i < n && i < 7; ++i) ms[i] = g_ctx.phase_ms[i];
     return fail(HY_OK);
+}
+
+// The chunk boundaries hy_align_pairs would use for these offsets (introspection for tests):
+// writes up to `cap` boundaries and returns the number of chunks.
+extern "C" uint64_t hy_debug_pair_chunks(const uint64_t *q_off, const uint64_t *t_off, uint64_t n_pairs,
+                                         uint64_t *bounds, uint64_t cap) {
+    if (!q_off || !t_off || n_pairs == 0) return 0;
+    const std::vector<uint64_t> b = plan_pair_chunks(q_off, t_off, n_pairs);
+    for (uint64_t i = 0; i < b.size() && i < cap; ++i) bounds[i] = b[i];
+    return b.size() - 1;
 }

@@ -704,8 +704,8 @@ __device__ __forceinline__ void sweep2_column(Sweep2<A, R> &sw, const int a, con
         f = A::addmax(f, negge, g_up);
         const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
         const V h = A::vmax3_relu(d, sw.E[r], f);
-        gd = sw.Gp[r];
         const V g = A::vadd(h, neggo);
+        gd = sw.Gp[r];
         sw.Gp[r] = g;
         g_up = g;
         if (r & 1)

@@ -244,6 +244,12 @@ int64_t hy_debug_live_device_allocations(void);
  * wait to seconds. 0 makes every such wait give up at once, which a test uses to see
  * HY_ERR_TIMEOUT reported and the scratch still usable afterwards. */
 void hy_debug_set_wait_polls(int64_t polls);
+/* The chunks hy_align_pairs would run pairs [0, n_pairs) in, for these offsets: writes up to `cap`
+ * chunk boundaries (the first pair of each chunk, then n_pairs) and returns the number of chunks.
+ * Chunks are cut at equal shares of the residues, so that no chunk's staging much exceeds its
+ * bound (512 MiB) however long and short pairs are ordered. */
+uint64_t hy_debug_pair_chunks(const uint64_t *q_off, const uint64_t *t_off, uint64_t n_pairs,
+                              uint64_t *bounds, uint64_t cap);
 
 /* ---- batched scan (no reference counterpart: the reference scans one query per call) ---------- */
 

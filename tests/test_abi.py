@@ -146,3 +146,30 @@ def test_env_var_precedence_in_a_fresh_process():
     lines = out.stdout.split()
     assert lines[0] == "InvalidBackendName", out.stderr
     assert lines[1] == "BackendUnavailable"
+
+
+def test_align_pairs_chunks_bound_their_residues_however_pairs_are_ordered():
+    """hy_align_pairs cuts its pipeline chunks at equal residue shares: a batch whose long pairs
+    cluster in one range still gives chunks of at most 512 MiB of residues plus one pair."""
+    import numpy as np
+
+    bound = 512 << 20
+    rng = np.random.default_rng(9)
+    for long_first in (True, False):
+        n = 300_000
+        t_len = np.full(n, 300, np.uint64)
+        long_idx = np.arange(0, 1500) if long_first else np.arange(n - 1500, n)
+        t_len[long_idx] = 1 << 20  # 1,500 windows of 1 MiB: 1.5 GiB in one range of the input
+        q_len = rng.integers(50, 200, n).astype(np.uint64)
+        q_off = np.zeros(n + 1, np.uint64)
+        q_off[1:] = np.cumsum(q_len)
+        t_off = np.zeros(n + 1, np.uint64)
+        t_off[1:] = np.cumsum(t_len)
+        out = np.zeros(64, np.uint64)
+        k = _abi.lib.hy_debug_pair_chunks(q_off.ctypes.data_as(_abi._u64p), t_off.ctypes.data_as(_abi._u64p), n,
+                                          out.ctypes.data_as(_abi._u64p), len(out))
+        b = out[: k + 1].astype(np.int64)
+        assert b[0] == 0 and b[-1] == n and np.all(np.diff(b) >= 1)
+        res = (q_off[b[1:]] - q_off[b[:-1]]) + (t_off[b[1:]] - t_off[b[:-1]])
+        assert int(res.max()) <= bound + (1 << 20) + 200, (long_first, k, res.max())
+        assert int(res.sum()) == int(q_off[-1] + t_off[-1])

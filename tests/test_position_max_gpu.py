@@ -160,3 +160,45 @@ def test_failure_in_a_later_chunk_leaves_a_correct_prefix():
     assert not buf[int(t_off[bad]):].any()
     idx = sorted(set(list(range(0, bad, 997)) + [bad - 1]))
     _sample_check(qs, ts, idx, hits, cm, s2, t_off, DNA, 4, 2, 1, 10)
+
+
+def test_narrowed_chunks_every_column_maximum():
+    """Chunks whose pairs all proved int16 send their column maxima back as int16 and the host
+    widens them. A pageable column-maxima array over many such chunks (and, in the second call,
+    one chunk made wide by int32 pairs among narrowed ones) must equal, entry for entry, the
+    page-locked path, which copies the int32 maxima straight into the caller's array; a sample is
+    checked against the oracle."""
+    rng = np.random.default_rng(14)
+    n = 400_000
+    # Queries of at most 100 residues: int16 even under the large entry of the second call
+    # (100 * 300 + 6 <= 32767).
+    qs = [rng.integers(0, 4, int(rng.integers(1, 101))) for _ in range(n)]
+    ts = [rng.integers(0, 4, int(rng.integers(1, 300))) for _ in range(n)]
+    for mixed in (False, True):
+        mat = list(DNA)
+        if mixed:  # int32 by the width proof, only inside one range of the input (one chunk)
+            mat = [int(v) for v in DNA]
+            mat[5] = 300
+            for k in range(200_000, 200_400):
+                qs[k] = rng.integers(0, 4, 180)
+                ts[k] = rng.integers(0, 4, 250)
+        q_res, q_off = hy.concat(qs)
+        t_res, t_off = hy.concat(ts)
+        scoring = hy.Scoring(4, mat, 6, 1)
+        page = np.full(int(t_off[-1]), -7, np.int32)
+        hits, cm, s2, (err, _) = hy.align_pairs_position_max_arrays(q_res, q_off, t_res, t_off, scoring, 20,
+                                                                    colmax_out=page)
+        assert err is None
+        pq = hy.pinned_empty(len(q_res), np.uint8)
+        pt = hy.pinned_empty(len(t_res), np.uint8)
+        pcm = hy.pinned_empty(len(page), np.int32)
+        pq[:] = q_res
+        pt[:] = t_res
+        pcm[:] = -7
+        hits_p, cm_p, s2_p, (err_p, _) = hy.align_pairs_position_max_arrays(pq, q_off, pt, t_off, scoring, 20,
+                                                                            colmax_out=pcm)
+        assert err_p is None
+        assert np.array_equal(page, pcm), int(np.flatnonzero(page != pcm)[0])
+        assert bytes(hits) == bytes(hits_p) and np.array_equal(s2, s2_p)
+        idx = sorted(set(list(range(0, n, 4999)) + list(range(200_000, 200_400, 37)) + [n - 1]))
+        _sample_check(qs, ts, idx, hits, cm, s2, t_off, mat, 4, 6, 1, 20)
