@@ -643,13 +643,26 @@ def extra_served(seed, rate=10.0, seconds=6.0):
     same = True
     t0 = time.perf_counter()
     cells = 0.0
+    plain_ms = []
     for (q, kind), (hit, scores) in zip(reqs, served):
+        t1 = time.perf_counter()
         if kind:
             same &= bool(np.array_equal(scores, db.scan_scores_array(sc, q)))
         else:
             same &= _hit4(hit) == _hit4(db.scan(sc, q))
+        plain_ms.append((time.perf_counter() - t1) * 1e3)
         cells += len(q) * total_res
     plain_s = time.perf_counter() - t0
+    # Latency by query length: what a request waited for beyond its own scan time.
+    by_len = {}
+    for (q, _), h, pm in zip(reqs, handles, plain_ms):
+        c = "short (<= 350 aa)" if len(q) <= 350 else "long (> 350 aa)"
+        by_len.setdefault(c, ([], []))
+        by_len[c][0].append(h.latency_ms)
+        by_len[c][1].append(pm)
+    latency_by_length = {c: {"requests": len(l), "p50_ms": float(np.percentile(l, 50)),
+                             "p99_ms": float(np.percentile(l, 99)), "plain_call_p50_ms": float(np.percentile(p, 50))}
+                         for c, (l, p) in by_len.items()}
     ref = pyoracle.OracleDb((residues, offsets), mat, AL, GO, GE, 0, 1)
     threads = os.cpu_count() or 1
     oracle_ok = True
@@ -664,6 +677,7 @@ def extra_served(seed, rate=10.0, seconds=6.0):
                         "lengths (median 350, 50..3000), half ScoreEnd scan and half scan_scores (i32 per target)",
             "offered_qps": rate, "requests": n, "completed": int(st["completed"]), "achieved_qps": st["completed"] / wall,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"],
+            "latency_by_query_length": latency_by_length,
             "value": st["gcups"], "unit": "GCUPS",
             "plain": {"value": cells / plain_s / 1e9, "unit": "GCUPS", "seconds": plain_s,
                       "form": "the same requests one at a time (Database.scan / scan_scores)"},

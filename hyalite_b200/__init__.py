@@ -702,6 +702,7 @@ class ServerRequest:
         self.id = rid
         self.db = db
         self.scores = scores
+        self.latency_ms: Optional[float] = None  # submit to result ready, once waited for
 
 
 class Server:
@@ -761,11 +762,15 @@ class Server:
         return bool(done.value)
 
     def wait(self, req: ServerRequest, timeout: float = 600.0) -> BestHit:
+        """The request's BestHit (for a scores request, its scores are then in ``req.scores``);
+        ``req.latency_ms`` receives its latency, submit to result ready."""
         out = _abi.HyHit()
-        st = lib.hy_server_wait(self._h, req.id, float(timeout), C.byref(out))
+        lat = C.c_double()
+        st = lib.hy_server_wait_timed(self._h, req.id, float(timeout), C.byref(out), C.byref(lat))
         if st != _abi.TIMEOUT:
             self._live.pop(req.id, None)
         _check(st)
+        req.latency_ms = float(lat.value)
         return BestHit._from(out)
 
     def stats(self, reset: bool = False) -> dict:

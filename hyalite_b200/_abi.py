@@ -146,6 +146,7 @@ SIGNATURES = {
     "hy_server_request_bytes": (C.c_uint64, [_vp, C.c_uint32, C.c_uint64, C.c_int, _u64p]),
     "hy_server_poll": (_st, [_vp, C.c_uint64, C.POINTER(C.c_int)]),
     "hy_server_wait": (_st, [_vp, C.c_uint64, C.c_double, C.POINTER(HyHit)]),
+    "hy_server_wait_timed": (_st, [_vp, C.c_uint64, C.c_double, C.POINTER(HyHit), C.POINTER(C.c_double)]),
     "hy_server_stats_read": (_st, [_vp, C.c_int, C.POINTER(HyServerStats)]),
 }
 

@@ -718,6 +718,62 @@ __device__ __forceinline__ void sweep2_column(Sweep2<A, R> &sw, const int a, con
     outF = f;
 }
 
+// Both columns of a step, interleaved one row apart (row r of column j0 with row r - 1 of column
+// j1, which needs rows r - 1 of column j0 only): the same values as sweep2_column twice, with the
+// two columns' dependency chains side by side in the instruction stream.
+template <class A, int G, int R>
+__device__ __forceinline__ void sweep2_both(Sweep2<A, R> &sw, const int a0, const int b0, const int a1,
+                                            const int b1, const int lane, const uint8_t *prof_a,
+                                            const uint8_t *prof_b, const typename A::V upG0,
+                                            const typename A::V upF0, const typename A::V upG1,
+                                            const typename A::V upF1, const typename A::V negge,
+                                            const typename A::V neggo, typename A::V &best) {
+    typedef typename A::V V;
+    V p0a[A::EPV], p0b[A::EPV], p1a[A::EPV], p1b[A::EPV];
+    V g_up0 = upG0, f0 = upF0, gd0 = sw.diag, hprev0 = A::splat(0);
+    V g_up1 = upG1, f1 = upF1, gd1 = upG0, hprev1 = A::splat(0);
+#pragma unroll
+    for (int t = 0; t <= R; ++t) {
+        if (t < R) {  // column j0, row t
+            const int r = t;
+            if (r % A::EPV == 0) A::template load_chunk<R, G>(prof_a, prof_b, a0, b0, lane, r / A::EPV, p0a, p0b);
+            sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
+            f0 = A::addmax(f0, negge, g_up0);
+            const V d = A::diag(gd0, p0a[r % A::EPV], p0b[r % A::EPV]);
+            const V h = A::vmax3_relu(d, sw.E[r], f0);
+            const V g = A::vadd(h, neggo);
+            gd0 = sw.Gp[r];
+            sw.Gp[r] = g;
+            g_up0 = g;
+            if (r & 1)
+                best = A::vmax3(best, hprev0, g);
+            else
+                hprev0 = g;
+        }
+        if (t >= 1) {  // column j1, row t - 1
+            const int r = t - 1;
+            if (r % A::EPV == 0) A::template load_chunk<R, G>(prof_a, prof_b, a1, b1, lane, r / A::EPV, p1a, p1b);
+            sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
+            f1 = A::addmax(f1, negge, g_up1);
+            const V d = A::diag(gd1, p1a[r % A::EPV], p1b[r % A::EPV]);
+            const V h = A::vmax3_relu(d, sw.E[r], f1);
+            const V g = A::vadd(h, neggo);
+            gd1 = sw.Gp[r];
+            sw.Gp[r] = g;
+            g_up1 = g;
+            if (r & 1)
+                best = A::vmax3(best, hprev1, g);
+            else
+                hprev1 = g;
+        }
+    }
+    if (R & 1) best = A::vmax3(best, hprev0, hprev1);
+    sw.botG[0] = g_up0;
+    sw.botF[0] = f0;
+    sw.botG[1] = g_up1;
+    sw.botF[1] = f1;
+}
+
 // Step s of one lane (see above). The residue codes of columns j0, j1 come as one 32-bit word
 // (`codes`) and, for lane 0 after the first pass, the boundary values of both columns as one
 // 16-byte word (`up`: G, F of j0, then of j1). CHECKED steps test each column against [1, w].
@@ -747,15 +803,26 @@ __device__ __forceinline__ void sweep2_step(Sweep2<A, R> &sw, const int s, const
         }
     }
     int a, b;
-    if (live0) {
+#ifdef HY_EXP_2COL_IL
+    if (!CHECKED) {
+        int a1, b1;
         A::residues((typename A::RES)(codes & 0xffffu), a, b);
-        sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG0, upF0, sw.diag, k.negge, k.neggo, best,
-                               sw.botG[0], sw.botF[0]);
-    }
-    if (live1) {
-        A::residues((typename A::RES)(codes >> 16), a, b);
-        sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG1, upF1, upG0, k.negge, k.neggo, best,
-                               sw.botG[1], sw.botF[1]);
+        A::residues((typename A::RES)(codes >> 16), a1, b1);
+        sweep2_both<A, G, R>(sw, a, b, a1, b1, lane, prof_a, prof_b, upG0, upF0, upG1, upF1, k.negge, k.neggo,
+                             best);
+    } else
+#endif
+    {
+        if (live0) {
+            A::residues((typename A::RES)(codes & 0xffffu), a, b);
+            sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG0, upF0, sw.diag, k.negge, k.neggo, best,
+                                   sw.botG[0], sw.botF[0]);
+        }
+        if (live1) {
+            A::residues((typename A::RES)(codes >> 16), a, b);
+            sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG1, upF1, upG0, k.negge, k.neggo, best,
+                                   sw.botG[1], sw.botF[1]);
+        }
     }
     if (live0) sw.diag = live1 ? upG1 : upG0;
     if (lane == G - 1 && !last_pass && live0)
@@ -808,6 +875,9 @@ __device__ __forceinline__ void sweep2_pass(const int lane, const int steps, con
     if (fast_lo < fast_hi) {
         uint32_t c_cur = res2[fast_lo - lane];
         uint4 u_cur = (lane == 0 && !first_pass) ? bnd4[fast_lo - lane] : none;
+#ifdef HY_EXP_2COL_UNROLL
+#pragma unroll 2
+#endif
         for (int s = fast_lo; s < fast_hi; ++s) {
             const int sn = min(s + 1, fast_hi - 1);
             const uint32_t c_next = res2[sn - lane];

@@ -369,6 +369,10 @@ hy_status hy_server_poll(hy_server *s, uint64_t id, int *done) {
 }
 
 hy_status hy_server_wait(hy_server *s, uint64_t id, double timeout_s, hy_hit *out) {
+    return hy_server_wait_timed(s, id, timeout_s, out, nullptr);
+}
+
+hy_status hy_server_wait_timed(hy_server *s, uint64_t id, double timeout_s, hy_hit *out, double *latency_ms) {
     if (!s) return fail(HY_ERR_INVALID_ARGUMENT);
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->reqs.find(id);
@@ -379,6 +383,7 @@ hy_status hy_server_wait(hy_server *s, uint64_t id, double timeout_s, hy_hit *ou
     if (!s->cv_done.wait_until(lk, deadline, [&] { return r->done; })) return fail(HY_ERR_TIMEOUT);
     const hy_status st = r->status;
     if (out) *out = r->hit;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
     s->reqs.erase(it);
     delete r;
     return fail(st);

@@ -342,6 +342,9 @@ hy_status hy_server_poll(hy_server *server, uint64_t request_id, int *done);
 /* Waits up to timeout_s for the request; on completion writes its hit, releases the request and
  * returns its status. HY_ERR_TIMEOUT leaves the request queued. */
 hy_status hy_server_wait(hy_server *server, uint64_t request_id, double timeout_s, hy_hit *out);
+/* hy_server_wait that also returns the request's latency, submit to result ready, in ms. */
+hy_status hy_server_wait_timed(hy_server *server, uint64_t request_id, double timeout_s, hy_hit *out,
+                               double *latency_ms);
 /* Counters and latency percentiles since the last reset (reset != 0 clears them). */
 hy_status hy_server_stats_read(hy_server *server, int reset, hy_server_stats *out);
 
