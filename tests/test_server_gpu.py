@@ -77,6 +77,7 @@ def test_results_match_the_oracle():
     for h, (q, k, _) in zip(hs, reqs[:12]):
         mode = (0, 2, 4)[k]
         assert hit_tuple(srv.wait(h)) == o.OracleDb(seqs, mat, 20, 11, 1, mode, 1).scan(q)
+        assert h.latency_ms is not None and h.latency_ms > 0.0  # submit to ready (hy_server_wait_timed)
     srv.close()
 
 
