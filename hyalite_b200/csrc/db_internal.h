@@ -34,6 +34,9 @@ constexpr int BLOCK = 256;
 // to 32 rows.
 inline int bulk_rows(uint64_t qlen, bool two_col) {
     if (qlen <= 64) return 8;
+#ifdef HY_EXP_R8ALL
+    if (two_col) return 8;
+#endif
     return two_col || qlen <= 192 ? 16 : 32;
 }
 constexpr int BULK_MAX_RPP = 8 * 32;
