@@ -65,11 +65,7 @@ __device__ __forceinline__ void class_range(const BatchQuery &bq, int cls, uint3
 // One persistent kernel per launch class: blocks take units off the class queue until it is empty.
 // Shared memory: the two profile mbarriers, then two pass slices of the largest pass of the batch.
 template <class A, int G, int R, int PK>
-#ifdef HY_EXP_BATCH_SW16
-__global__ void __launch_bounds__(256, scan_min_blocks<A, G, R, A::NH == 2 && R == 16>()) batch_scan_kernel(const ClassLaunch L) {
-#else
 __global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) batch_scan_kernel(const ClassLaunch L) {
-#endif
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ uint32_t s_unit;
     constexpr uint32_t IPU = 256 / G;  // items per unit: one per group of the block
@@ -253,11 +249,7 @@ struct QueryKinds {
 static void plan_kinds(const hy_db *db, uint64_t qlen, bool ends, const BatchConfig &cfg, QueryKinds &k) {
     const bool tab = db->layout == HY_LAYOUT_PRECOMPUTED;
     k.split = split_for_query(db, qlen, cfg.long_w);
-#ifdef HY_EXP_BATCH_SW16
-    k.rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (db->mode == MODE_SW || (int64_t)qlen <= cfg.rows16_max) ? 16 : 32;
-#else
     k.rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
-#endif
     const QuerySplit &sp = k.split;
     k.need[PK_BULK] = sp.kl < db->p16.n_items;
     k.need[PK_W16] = sp.kl > sp.k0 || ends;

@@ -30,14 +30,17 @@ constexpr uint32_t LONG_W = 4096;
 constexpr uint32_t NO_LONG_SPLIT = 0xffffffffu;
 constexpr int BLOCK = 256;
 // Rows per lane of the bulk int16x2 kernel for a query of length qlen (passes of MAIN_G * rows).
-// SW scores run the two-column sweep at up to 16 rows per lane; the other kinds one column of up
-// to 32 rows.
+// SW scores run the two-column sweep at 8 or 16 rows per lane: 16 unless 8 pads the query to so
+// many fewer rows that it wins at 8 rows' rate per padded row (measured 10/11 of 16 rows' rate:
+// 300 residues take 320 rows at 8 against 384 at 16, 9% faster; 150 residues 21% faster). The
+// other kinds run one column of up to 32 rows.
 inline int bulk_rows(uint64_t qlen, bool two_col) {
     if (qlen <= 64) return 8;
-#ifdef HY_EXP_R8ALL
-    if (two_col) return 8;
-#endif
-    return two_col || qlen <= 192 ? 16 : 32;
+    if (two_col) {
+        const uint64_t rows8 = (qlen + 63) / 64 * 64, rows16 = (qlen + 127) / 128 * 128;
+        return 11 * rows8 < 10 * rows16 ? 8 : 16;
+    }
+    return qlen <= 192 ? 16 : 32;
 }
 constexpr int BULK_MAX_RPP = 8 * 32;
 constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;

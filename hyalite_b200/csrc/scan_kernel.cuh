@@ -803,16 +803,14 @@ __device__ __forceinline__ void sweep2_step(Sweep2<A, R> &sw, const int s, const
         }
     }
     int a, b;
-#ifdef HY_EXP_2COL_IL
     if (!CHECKED) {
+        // Both columns live: interleaved (measured 0.6% faster than one after the other).
         int a1, b1;
         A::residues((typename A::RES)(codes & 0xffffu), a, b);
         A::residues((typename A::RES)(codes >> 16), a1, b1);
         sweep2_both<A, G, R>(sw, a, b, a1, b1, lane, prof_a, prof_b, upG0, upF0, upG1, upF1, k.negge, k.neggo,
                              best);
-    } else
-#endif
-    {
+    } else {
         if (live0) {
             A::residues((typename A::RES)(codes & 0xffffu), a, b);
             sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG0, upF0, sw.diag, k.negge, k.neggo, best,
@@ -875,9 +873,6 @@ __device__ __forceinline__ void sweep2_pass(const int lane, const int steps, con
     if (fast_lo < fast_hi) {
         uint32_t c_cur = res2[fast_lo - lane];
         uint4 u_cur = (lane == 0 && !first_pass) ? bnd4[fast_lo - lane] : none;
-#ifdef HY_EXP_2COL_UNROLL
-#pragma unroll 2
-#endif
         for (int s = fast_lo; s < fast_hi; ++s) {
             const int sn = min(s + 1, fast_hi - 1);
             const uint32_t c_next = res2[sn - lane];
