@@ -827,65 +827,111 @@ __device__ __forceinline__ void sweep2_step(Sweep2<A, R> &sw, const int s, const
         *reinterpret_cast<uint4 *>(bnd + 2 * (j0 - 1)) = make_uint4(sw.botG[0], sw.botF[0], sw.botG[1], sw.botF[1]);
 }
 
-// One whole pass of the two-column sweep: `steps` = ceil(wmax / 2) + G - 1; steps in
-// [G - 1, w_min / 2) have both columns of every lane of the warp inside its item and run
-// unchecked, with the next step's codes and boundary values loaded one step ahead.
+// Every pass of one item's two-column sweep, the passes back to back. With W column pairs a pass
+// (warp-uniform), lane L works virtual column pair v = s - L at step s, that is pass v / W at
+// column pair v % W: when lane 0 has finished a pass it starts the next one while lanes 1..G-1
+// finish theirs, so the G - 1 fill and drain steps of the wavefront are paid once per item, not
+// once per pass. A pass p >= 1 begins with G - 1 transition steps (lanes L <= t at column pair
+// t - L of pass p, the others at W + t - L of pass p - 1), then its interior steps (every lane in
+// pass p; the ones with both columns of every lane inside its item run unchecked, with the next
+// step's codes and boundary values loaded one step ahead).
+//
+// Shared memory: pass p's profile slice is in buffer p % 2. After the transition into pass p no
+// lane of the block reads pass p - 1's slice any more: the block barrier there (one per pass, in
+// every warp) frees that buffer for pass p + 1's copy, issued by thread 0. The boundary row: lane
+// G-1 writes column pair c of pass p at step pW + c + G - 1, lane 0 reads it for pass p + 1 at
+// step (p + 1)W + c (one step earlier with the prefetch). W >= 2G keeps every such read at least G
+// steps after its write; the warp barrier at the start of each transition orders the writes the
+// transition's reads need, and the block barrier after it orders the rest.
+//
+// Every thread of the block calls it with the block's `phase` (see scan_unit). Returns false if a
+// profile copy did not arrive in time (the error flag is then set and the block must stop).
 template <class A, int G, int R>
-__device__ __forceinline__ void sweep2_pass(const int lane, const int steps, const int w_min, const int32_t w,
-                                            const typename A::RES *__restrict__ res, const uint8_t *prof_a,
-                                            const uint8_t *prof_b, const int32_t row0, const bool first_pass,
-                                            const bool last_pass, typename A::V *bnd, const int32_t go,
-                                            const int32_t ge, const typename A::V Sv, typename A::V &best) {
+__device__ __forceinline__ bool sweep2_item(const ScanParams &p, const int lane, const int W, const int wfast,
+                                            const int32_t w, const typename A::RES *__restrict__ res,
+                                            typename A::V *bnd, uint8_t *smem, uint64_t *bars,
+                                            uint32_t &phase, const typename A::V Sv, typename A::V &best) {
     typedef typename A::V V;
     static_assert(A::NH == 2 && sizeof(typename A::RES) == 2, "two-column steps pair int16 codes");
-    Sweep2<A, R> sw;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        sw.Gp[r] = A::splat(-(int64_t)go);  // local mode: the left border is free (H = 0)
-        sw.E[r] = Sv;
-    }
-    sw.diag = A::splat(-(int64_t)go);
-    sw.botG[0] = sw.botG[1] = sw.botF[0] = sw.botF[1] = A::splat(0);
-    (void)row0;
+    const int n_passes = p.n_passes;
+    const uint32_t hi_off = (A::TABLES - 1) * (p.pass_bytes / A::TABLES);
     SweepConst<A> k;
-    k.negge = A::splat(-(int64_t)ge);
-    k.neggo = A::splat(-(int64_t)go);
+    k.negge = A::splat(-(int64_t)p.ge);
+    k.neggo = A::splat(-(int64_t)p.go);
     k.Sv = Sv;
-    k.top_free_g = A::splat(-(int64_t)go);
+    k.top_free_g = A::splat(-(int64_t)p.go);
+    Sweep2<A, R> sw;
+    // A lane's state at the start of a pass: local mode, the left border is free (H = 0).
+    auto reset = [&]() {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            sw.Gp[r] = k.top_free_g;
+            sw.E[r] = Sv;
+        }
+        sw.diag = k.top_free_g;
+    };
+    reset();
+    sw.botG[0] = sw.botG[1] = sw.botF[0] = sw.botF[1] = A::splat(0);
     const uint32_t *res2 = reinterpret_cast<const uint32_t *>(res);  // codes of columns (2i+1, 2i+2)
     const uint4 *bnd4 = reinterpret_cast<const uint4 *>(bnd);          // boundary of the same pair
     const uint4 none = make_uint4(0, 0, 0, 0);
-    // Loads of step s for this lane: column pair index s - lane (clamped to the item for
-    // checked steps, where a dead pair's values are never used).
-    auto codes_at = [&](int s, int32_t wl) -> uint32_t {
-        const int i = s - lane;
-        return (i >= 0 && 2 * i < wl) ? res2[i] : 0u;
+    // Loads for column pair c of this lane (-1: no column; a dead pair's values are never used).
+    auto codes_at = [&](int c) -> uint32_t { return (c >= 0 && 2 * c < w) ? res2[c] : 0u; };
+    auto up_at = [&](int c, bool first) -> uint4 {
+        return (lane == 0 && !first && c >= 0 && 2 * c < w) ? bnd4[c] : none;
     };
-    auto up_at = [&](int s, int32_t wl) -> uint4 {
-        const int i = s - lane;
-        return (lane == 0 && !first_pass && i >= 0 && 2 * i < wl) ? bnd4[i] : none;
+    // One checked step of this lane at column pair c of pass lp (lp < 0 or c < 0: no column).
+    auto checked = [&](int lp, int c) {
+        const uint8_t *pa = smem + (size_t)(lp & 1) * p.pass_bytes;
+        if (lp < 0) c = -1;
+        sweep2_step<A, G, R, true>(sw, c + lane, lane, w, pa, pa + hi_off, lp == 0, lp == n_passes - 1, bnd, k,
+                                   best, codes_at(c), up_at(c, lp == 0));
     };
-    const int fast_lo = min(steps, G - 1);
-    const int fast_hi = max(fast_lo, min(steps, w_min / 2));
-    for (int s = 0; s < fast_lo; ++s)
-        sweep2_step<A, G, R, true>(sw, s, lane, w, prof_a, prof_b, first_pass, last_pass, bnd, k, best,
-                                   codes_at(s, w), up_at(s, w));
-    if (fast_lo < fast_hi) {
-        uint32_t c_cur = res2[fast_lo - lane];
-        uint4 u_cur = (lane == 0 && !first_pass) ? bnd4[fast_lo - lane] : none;
-        for (int s = fast_lo; s < fast_hi; ++s) {
-            const int sn = min(s + 1, fast_hi - 1);
-            const uint32_t c_next = res2[sn - lane];
-            const uint4 u_next = (lane == 0 && !first_pass) ? bnd4[sn - lane] : u_cur;
-            sweep2_step<A, G, R, false>(sw, s, lane, w, prof_a, prof_b, first_pass, last_pass, bnd, k, best,
-                                        c_cur, u_cur);
-            c_cur = c_next;
-            u_cur = u_next;
+    for (int pass = 0; pass < n_passes; ++pass) {
+        const int buf = pass & 1;
+        const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u, p.wait_polls);
+        phase ^= 1u << buf;
+        if (W > 0) {
+            __syncwarp();
+            for (int t = 0; t < G - 1; ++t) {
+                const bool fresh = lane <= t;  // this lane has entered pass `pass`
+                if (fresh && lane == t && pass > 0) reset();
+                checked(fresh ? pass : pass - 1, fresh ? t - lane : W + t - lane);
+            }
+            if (lane == G - 1 && pass > 0) reset();  // lane G-1 enters at the first interior step
         }
+        if (__syncthreads_or(!ok)) {
+            // This pass's copy and, in the first pass, the second one are still outstanding.
+            if (threadIdx.x == 0)
+                wait_gave_up(p.err, bars, (1u << buf) | (pass == 0 && n_passes > 1 ? 2u : 0u), phase ^ (1u << buf));
+            return false;
+        }
+        if (threadIdx.x == 0 && pass >= 1 && pass + 1 < n_passes)
+            bulk_load(smem + (size_t)(buf ^ 1) * p.pass_bytes, p.profile + (size_t)(pass + 1) * p.pass_bytes,
+                      p.pass_bytes, &bars[buf ^ 1]);
+        if (W == 0) continue;
+        const uint8_t *pa = smem + (size_t)buf * p.pass_bytes, *pb = pa + hi_off;
+        const bool first = pass == 0, last = pass == n_passes - 1;
+        const int fast_hi = max(G - 1, wfast);
+        if (G - 1 < fast_hi) {
+            uint32_t c_cur = res2[G - 1 - lane];
+            uint4 u_cur = (lane == 0 && !first) ? bnd4[G - 1] : none;
+            for (int s = G - 1; s < fast_hi; ++s) {
+                const int sn = min(s + 1, fast_hi - 1);
+                const uint32_t c_next = res2[sn - lane];
+                const uint4 u_next = (lane == 0 && !first) ? bnd4[sn] : u_cur;
+                sweep2_step<A, G, R, false>(sw, s, lane, w, pa, pb, first, last, bnd, k, best, c_cur, u_cur);
+                c_cur = c_next;
+                u_cur = u_next;
+            }
+        }
+        for (int s = fast_hi; s < W; ++s) checked(pass, s - lane);
     }
-    for (int s = fast_hi; s < steps; ++s)
-        sweep2_step<A, G, R, true>(sw, s, lane, w, prof_a, prof_b, first_pass, last_pass, bnd, k, best,
-                                   codes_at(s, w), up_at(s, w));
+    // The last pass's drain: lanes L > t finish their columns W + t - L.
+    if (W > 0)
+        for (int t = 0; t < G - 1; ++t) checked(lane > t ? n_passes - 1 : -1, W + t - lane);
+    __syncthreads();  // both profile buffers are free for the block's next unit
+    return true;
 }
 
 // Group reduction of the per-lane candidates, border seeds, output and best-key fold. Every lane
@@ -1038,7 +1084,6 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, meta.w);
     const int w_min = (int)__reduce_min_sync(0xffffffffu, meta.w);
     const int steps = wmax == 0 ? 0 : (int)wmax + G - 1;
-    const int steps2 = wmax == 0 ? 0 : (int)(wmax + 1) / 2 + G - 1;  // two-column form
 
     V best = A::splat(ModeFlags<MODE>::local && !ENDS ? -(int64_t)p.go : 0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
@@ -1047,38 +1092,39 @@ __device__ __forceinline__ bool scan_unit(const ScanParams &p, const uint32_t it
         bulk_load(smem, p.profile, p.pass_bytes, &bars[0]);
         if (p.n_passes > 1) bulk_load(smem + p.pass_bytes, p.profile + p.pass_bytes, p.pass_bytes, &bars[1]);
     }
-    for (int pass = 0; pass < p.n_passes; ++pass) {
-        const int buf = pass & 1;
-        const uint8_t *prof;
-        if (GPROF) {
-            prof = p.profile + (size_t)pass * p.pass_bytes;
-        } else {
-            const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u, p.wait_polls);
-            phase ^= 1u << buf;
-            if (__syncthreads_or(!ok)) {
-                // This pass's copy and, if issued, the next pass's are still outstanding.
-                if (threadIdx.x == 0)
-                    wait_gave_up(p.err, bars, (1u << buf) | (pass + 1 < p.n_passes ? 1u << (buf ^ 1) : 0u),
-                                 phase ^ (1u << buf));
-                return false;
+    if constexpr (two_col_form<A, R, MODE, ENDS, GPROF>()) {
+        // Column pairs a pass: at least 2G (the boundary row's read-after-write distance).
+        const int W = wmax == 0 ? 0 : max((int)(wmax + 1) / 2, 2 * G);
+        if (!sweep2_item<A, G, R>(p, lane, W, min(W, w_min / 2), (int32_t)meta.w, res, bnd, smem, bars, phase, Sv,
+                                  best))
+            return false;
+    } else {
+        for (int pass = 0; pass < p.n_passes; ++pass) {
+            const int buf = pass & 1;
+            const uint8_t *prof;
+            if (GPROF) {
+                prof = p.profile + (size_t)pass * p.pass_bytes;
+            } else {
+                const bool ok = mbar_wait_bounded(&bars[buf], (phase >> buf) & 1u, p.wait_polls);
+                phase ^= 1u << buf;
+                if (__syncthreads_or(!ok)) {
+                    // This pass's copy and, if issued, the next pass's are still outstanding.
+                    if (threadIdx.x == 0)
+                        wait_gave_up(p.err, bars, (1u << buf) | (pass + 1 < p.n_passes ? 1u << (buf ^ 1) : 0u),
+                                     phase ^ (1u << buf));
+                    return false;
+                }
+                prof = prof_buf[buf];
             }
-            prof = prof_buf[buf];
-        }
-        if constexpr (two_col_form<A, R, MODE, ENDS, GPROF>())
-            sweep2_pass<A, G, R>(lane, steps2, w_min, (int32_t)meta.w, res, prof,
-                                 prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
-                                 p.vrow0 + pass * RPP + lane * R, pass == 0, pass == p.n_passes - 1, bnd,
-                                 p.go, p.ge, Sv, best);
-        else
             sweep_pass<A, G, R, MODE, ENDS>(lane, steps, w_min, (int32_t)meta.w, meta.n, res, prof,
                                             prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES),
-                                            p.vrow0 + pass * RPP + lane * R, pass == 0,
-                                            pass == p.n_passes - 1, bnd, p.qlen, p.go, p.ge, Sv, best,
-                                            cand);
-        __syncthreads();  // the profile buffer and boundary row are free again
-        if (!GPROF && threadIdx.x == 0 && pass + 2 < p.n_passes)
-            bulk_load(smem + (size_t)buf * p.pass_bytes, p.profile + (size_t)(pass + 2) * p.pass_bytes,
-                      p.pass_bytes, &bars[buf]);
+                                            p.vrow0 + pass * RPP + lane * R, pass == 0, pass == p.n_passes - 1,
+                                            bnd, p.qlen, p.go, p.ge, Sv, best, cand);
+            __syncthreads();  // the profile buffer and boundary row are free again
+            if (!GPROF && threadIdx.x == 0 && pass + 2 < p.n_passes)
+                bulk_load(smem + (size_t)buf * p.pass_bytes, p.profile + (size_t)(pass + 2) * p.pass_bytes,
+                          p.pass_bytes, &bars[buf]);
+        }
     }
     finish_item<A, G, MODE, ENDS>(lane, active, meta, p.qlen, p.go, p.ge, best, cand, p.scores,
                                   p.qend, p.tend, p.best_key);
