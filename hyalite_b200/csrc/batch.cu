@@ -64,8 +64,10 @@ __device__ __forceinline__ void class_range(const BatchQuery &bq, int cls, uint3
 
 // One persistent kernel per launch class: blocks take units off the class queue until it is empty.
 // Shared memory: the two profile mbarriers, then two pass slices of the largest pass of the batch.
-template <class A, int G, int R, int PK>
-__global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) batch_scan_kernel(const ClassLaunch L) {
+// SW_ONLY: the SW classes, compiled for the SW sweep alone (the two-column form's register budget).
+template <class A, int G, int R, int PK, bool SW_ONLY = false>
+__global__ void __launch_bounds__(256, (scan_min_blocks<A, G, R, SW_ONLY && two_col_form<A, R, MODE_SW, false, false>()>()))
+    batch_scan_kernel(const ClassLaunch L) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ uint32_t s_unit;
     constexpr uint32_t IPU = 256 / G;  // items per unit: one per group of the block
@@ -97,12 +99,16 @@ __global__ void __launch_bounds__(256, scan_min_blocks<A, G, R>()) batch_scan_ke
         p.bnd_col0 = p.meta[first].col_off;
         p.bnd_cols = L.bnd_stride / (2 * sizeof(typename A::V));
         bool ok = true;
-        switch (bq.mode) {
-        case MODE_SW: ok = scan_unit<A, G, R, MODE_SW, false>(p, first, end, bufs, bars, phase); break;
-        case MODE_NW: ok = scan_unit<A, G, R, MODE_NW, false>(p, first, end, bufs, bars, phase); break;
-        case MODE_HW: ok = scan_unit<A, G, R, MODE_HW, false>(p, first, end, bufs, bars, phase); break;
-        case MODE_OV: ok = scan_unit<A, G, R, MODE_OV, false>(p, first, end, bufs, bars, phase); break;
-        default: ok = scan_unit<A, G, R, MODE_SHW, false>(p, first, end, bufs, bars, phase); break;
+        if constexpr (SW_ONLY) {
+            ok = scan_unit<A, G, R, MODE_SW, false>(p, first, end, bufs, bars, phase);
+        } else {
+            switch (bq.mode) {
+            case MODE_SW: ok = scan_unit<A, G, R, MODE_SW, false>(p, first, end, bufs, bars, phase); break;
+            case MODE_NW: ok = scan_unit<A, G, R, MODE_NW, false>(p, first, end, bufs, bars, phase); break;
+            case MODE_HW: ok = scan_unit<A, G, R, MODE_HW, false>(p, first, end, bufs, bars, phase); break;
+            case MODE_OV: ok = scan_unit<A, G, R, MODE_OV, false>(p, first, end, bufs, bars, phase); break;
+            default: ok = scan_unit<A, G, R, MODE_SHW, false>(p, first, end, bufs, bars, phase); break;
+            }
         }
         if (!ok) return;
     }
@@ -249,7 +255,12 @@ struct QueryKinds {
 static void plan_kinds(const hy_db *db, uint64_t qlen, bool ends, const BatchConfig &cfg, QueryKinds &k) {
     const bool tab = db->layout == HY_LAYOUT_PRECOMPUTED;
     k.split = split_for_query(db, qlen, cfg.long_w);
-    k.rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
+    // SW scores (the bulk classes never record ends) take the plain scan's two-column shapes; the
+    // other modes the tuned thresholds.
+    if (db->mode == MODE_SW)
+        k.rows = bulk_rows(qlen, true);
+    else
+        k.rows = (int64_t)qlen <= cfg.rows8_max ? 8 : (int64_t)qlen <= cfg.rows16_max ? 16 : 32;
     const QuerySplit &sp = k.split;
     k.need[PK_BULK] = sp.kl < db->p16.n_items;
     k.need[PK_W16] = sp.kl > sp.k0 || ends;
@@ -266,9 +277,9 @@ static void plan_kinds(const hy_db *db, uint64_t qlen, bool ends, const BatchCon
     }
 }
 
-template <class A, int G, int R, int PK>
+template <class A, int G, int R, int PK, bool SW_ONLY = false>
 static cudaError_t prepare_class(hy_batch *b, int cls, size_t smem, int n_sm) {
-    auto kern = batch_scan_kernel<A, G, R, PK>;
+    auto kern = batch_scan_kernel<A, G, R, PK, SW_ONLY>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -279,7 +290,7 @@ static cudaError_t prepare_class(hy_batch *b, int cls, size_t smem, int n_sm) {
     return cudaSuccess;
 }
 
-template <class A, int G, int R, int PK>
+template <class A, int G, int R, int PK, bool SW_ONLY = false>
 static void launch_class(hy_batch *b, int cls, uint8_t *bnd, size_t stride, cudaStream_t st) {
     ClassLaunch L;
     L.queries = b->d_queries;
@@ -288,7 +299,7 @@ static void launch_class(hy_batch *b, int cls, uint8_t *bnd, size_t stride, cuda
     L.cls = cls;
     L.bnd = bnd;
     L.bnd_stride = stride;
-    batch_scan_kernel<A, G, R, PK><<<b->grid[cls], 256, b->smem[cls], st>>>(L);
+    batch_scan_kernel<A, G, R, PK, SW_ONLY><<<b->grid[cls], 256, b->smem[cls], st>>>(L);
 }
 
 // Records the batch's device work on b->stream (under stream capture).
@@ -310,6 +321,10 @@ static hy_status record_graph_body(hy_batch *b) {
     launch_class<PairTab16, MAIN_G, 32, PK_BULK>(b, BC_TBULK32, b->d_bnd_bulk, b->stride_bulk, b->stream);
     launch_class<PairTab16, MAIN_G, 16, PK_BULK>(b, BC_TBULK16, b->d_bnd_bulk, b->stride_bulk, b->stream);
     launch_class<PairTab16, MAIN_G, 8, PK_BULK>(b, BC_TBULK8, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<Pair16, MAIN_G, 16, PK_BULK, true>(b, BC_SW16, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<Pair16, MAIN_G, 8, PK_BULK, true>(b, BC_SW8, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<PairTab16, MAIN_G, 16, PK_BULK, true>(b, BC_TSW16, b->d_bnd_bulk, b->stride_bulk, b->stream);
+    launch_class<PairTab16, MAIN_G, 8, PK_BULK, true>(b, BC_TSW8, b->d_bnd_bulk, b->stride_bulk, b->stream);
     HB_CK(cudaGetLastError());
     HB_CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
     BandLaunch bl;
@@ -324,7 +339,7 @@ static hy_status record_graph_body(hy_batch *b) {
     batch_finalize_kernel<<<(b->max_queries + 127) / 128, 128, 0, b->stream>>>(b->d_queries, b->d_ctl,
                                                                                b->d_ends, b->d_hits);
     HB_CK(cudaGetLastError());
-    b->kernels_per_run = 15;
+    b->kernels_per_run = 19;
     return fail(HY_OK);
 }
 
@@ -454,8 +469,10 @@ hy_status batch_stage(hy_batch *b, const BatchItem *items, uint32_t n, const Bat
             prof_off += align128((size_t)p.pass_bytes * p.n_passes);
         }
         q_off += qlen;
-        const int bulk_cls = (k.rows == 8 ? BC_BULK8 : k.rows == 16 ? BC_BULK16 : BC_BULK32) +
-                             (bq.tab ? BC_TBULK8 - BC_BULK8 : 0);
+        const int bulk_cls = db->mode == MODE_SW
+                                 ? (k.rows == 8 ? BC_SW8 : BC_SW16) + (bq.tab ? BC_TSW8 - BC_SW8 : 0)
+                                 : (k.rows == 8 ? BC_BULK8 : k.rows == 16 ? BC_BULK16 : BC_BULK32) +
+                                       (bq.tab ? BC_TBULK8 - BC_BULK8 : 0);
         const int long_cls = bq.tab ? BC_TLONG : BC_LONG;
         if (sp.kl < db->p16.n_items) {
             lists[bulk_cls].push_back(i);
@@ -674,6 +691,10 @@ hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_que
         ck(prepare_class<PairTab16, MAIN_G, 16, PK_BULK>(b, BC_TBULK16, sm_tbulk16, n_sm));
         ck(prepare_class<PairTab16, MAIN_G, 32, PK_BULK>(b, BC_TBULK32, sm_tbulk32, n_sm));
         ck(prepare_class<PairTab16, LCG, LCR, PK_W16>(b, BC_TLONG, sm_tlong, n_sm));
+        ck(prepare_class<Pair16, MAIN_G, 8, PK_BULK, true>(b, BC_SW8, sm_bulk8, n_sm));
+        ck(prepare_class<Pair16, MAIN_G, 16, PK_BULK, true>(b, BC_SW16, sm_bulk16, n_sm));
+        ck(prepare_class<PairTab16, MAIN_G, 8, PK_BULK, true>(b, BC_TSW8, sm_tbulk8, n_sm));
+        ck(prepare_class<PairTab16, MAIN_G, 16, PK_BULK, true>(b, BC_TSW16, sm_tbulk16, n_sm));
         int warps = (int)std::min<size_t>(32, BAND_SMEM_BUDGET / std::max<size_t>(band_pass, 1));
         warps = std::max(1, warps);
         b->band_threads = 32 * warps;
@@ -690,7 +711,8 @@ hy_status batch_create(const hy_db *const *dbs, uint32_t n_dbs, uint32_t max_que
     b->stride_band = align128((b->max_t + 16) * 2 * sizeof(uint32_t));
     const int side_grid = std::max({b->grid[BC_LONG], b->grid[BC_I32], b->grid[BC_TLONG]});
     const int bulk_grid = std::max({b->grid[BC_BULK8], b->grid[BC_BULK16], b->grid[BC_BULK32],
-                                    b->grid[BC_TBULK8], b->grid[BC_TBULK16], b->grid[BC_TBULK32]});
+                                    b->grid[BC_TBULK8], b->grid[BC_TBULK16], b->grid[BC_TBULK32],
+                                    b->grid[BC_SW8], b->grid[BC_SW16], b->grid[BC_TSW8], b->grid[BC_TSW16]});
     const uint64_t mq = b->mql_max;
     const uint64_t pair_row = std::max<uint64_t>(pass_bytes_of(al, 1, pb16), tab_row);
     const uint64_t per_query = align128(pair_row * (mq + 255)) +                   // bulk, any rows

@@ -11,10 +11,12 @@
 namespace hy {
 
 // Launch classes (one persistent kernel each; the T classes run databases of the Precomputed
-// layout) and profile kinds (one query profile each).
+// layout; the SW classes the bulk pairs of SW databases, in a kernel of that mode alone with the
+// plain scan's register budget) and profile kinds (one query profile each).
 enum {
     BC_BULK8 = 0, BC_BULK16 = 1, BC_BULK32 = 2, BC_LONG = 3, BC_I32 = 4,
-    BC_TBULK8 = 5, BC_TBULK16 = 6, BC_TBULK32 = 7, BC_TLONG = 8, BC_N = 9
+    BC_TBULK8 = 5, BC_TBULK16 = 6, BC_TBULK32 = 7, BC_TLONG = 8,
+    BC_SW8 = 9, BC_SW16 = 10, BC_TSW8 = 11, BC_TSW16 = 12, BC_N = 13
 };
 enum { PK_BULK = 0, PK_W16 = 1, PK_I32 = 2, PK_W32 = 3, PK_N = 4 };
 

@@ -914,16 +914,24 @@ __device__ __forceinline__ bool sweep2_item(const ScanParams &p, const int lane,
         const bool first = pass == 0, last = pass == n_passes - 1;
         const int fast_hi = max(G - 1, wfast);
         if (G - 1 < fast_hi) {
-            uint32_t c_cur = res2[G - 1 - lane];
-            uint4 u_cur = (lane == 0 && !first) ? bnd4[G - 1] : none;
-            for (int s = G - 1; s < fast_hi; ++s) {
-                const int sn = min(s + 1, fast_hi - 1);
-                const uint32_t c_next = res2[sn - lane];
-                const uint4 u_next = (lane == 0 && !first) ? bnd4[sn] : u_cur;
-                sweep2_step<A, G, R, false>(sw, s, lane, w, pa, pb, first, last, bnd, k, best, c_cur, u_cur);
-                c_cur = c_next;
-                u_cur = u_next;
+            // Two steps an iteration with two sets of registers for the one-step-ahead loads (only
+            // lane 0 reads the boundary row: the other lanes' copies are never used).
+            const bool up_lane = lane == 0 && !first;
+            uint32_t c_a = res2[G - 1 - lane], c_b = 0;
+            uint4 u_a = none, u_b = none;
+            if (up_lane) u_a = bnd4[G - 1];
+            int s = G - 1;
+            for (; s + 1 < fast_hi; s += 2) {
+                c_b = res2[s + 1 - lane];
+                if (up_lane) u_b = bnd4[s + 1];
+                sweep2_step<A, G, R, false>(sw, s, lane, w, pa, pb, first, last, bnd, k, best, c_a, u_a);
+                const int s2 = min(s + 2, fast_hi - 1);
+                c_a = res2[s2 - lane];
+                if (up_lane) u_a = bnd4[s2];
+                sweep2_step<A, G, R, false>(sw, s + 1, lane, w, pa, pb, first, last, bnd, k, best, c_b, u_b);
             }
+            if (s < fast_hi)
+                sweep2_step<A, G, R, false>(sw, s, lane, w, pa, pb, first, last, bnd, k, best, c_a, u_a);
         }
         for (int s = fast_hi; s < W; ++s) checked(pass, s - lane);
     }
