@@ -35,6 +35,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace hy {
 
 enum { MODE_SW = 0, MODE_NW = 1, MODE_HW = 2, MODE_OV = 3, MODE_SHW = 4 };
@@ -672,13 +674,23 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
     sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
 }
 
-// ---- two columns per step: the SW score sweep of int16x2 pairs ----------------------------------
+// ---- two columns per step: the SW score sweep of int16x2 pairs and int32 items ------------------
 //
 // Lane L works on columns j0 = 2(s - L) + 1 and j1 = j0 + 1 at step s, R rows each: the per-step
 // work (shuffles, residue and boundary loads, loop control) is spread over 2R rows of work while a
 // lane keeps only R rows of state, and the F chains of the two columns (column j1 one row behind
 // column j0) give the scheduler two independent dependency chains. Long form of the recurrence
 // (E, F, H = max(d, E, F, 0), G = H - go); the running maximum is kept on G.
+
+// The residue codes of two adjacent columns as one load: two 16-bit pair codes (int16x2 pairs) or
+// two 8-bit residues (int32 items). OK: the lane arithmetic has a two-column form.
+template <class A>
+struct TwoCodes {
+    static constexpr bool OK = (A::NH == 2 && sizeof(typename A::RES) == 2) || (A::NH == 1 && sizeof(typename A::RES) == 1);
+    static constexpr int BITS = 8 * (int)sizeof(typename A::RES);
+    typedef typename std::conditional<sizeof(typename A::RES) == 2, uint32_t, uint16_t>::type W;
+};
+
 template <class A, int R>
 struct Sweep2 {
     typename A::V Gp[R], E[R];        // G of the previous column and E, per row slot
@@ -784,6 +796,8 @@ __device__ __forceinline__ void sweep2_step(Sweep2<A, R> &sw, const int s, const
                                             typename A::V *bnd, const SweepConst<A> &k,
                                             typename A::V &best, const uint32_t codes, const uint4 up) {
     typedef typename A::V V;
+    constexpr int CODE_BITS = TwoCodes<A>::BITS;
+    constexpr uint32_t CODE_MASK = (1u << CODE_BITS) - 1u;
     const int32_t j0 = 2 * (s - lane) + 1;
     V upG0 = __shfl_up_sync(0xffffffffu, sw.botG[0], 1, G);
     V upF0 = __shfl_up_sync(0xffffffffu, sw.botF[0], 1, G);
@@ -806,18 +820,18 @@ __device__ __forceinline__ void sweep2_step(Sweep2<A, R> &sw, const int s, const
     if (!CHECKED) {
         // Both columns live: interleaved (measured 0.6% faster than one after the other).
         int a1, b1;
-        A::residues((typename A::RES)(codes & 0xffffu), a, b);
-        A::residues((typename A::RES)(codes >> 16), a1, b1);
+        A::residues((typename A::RES)(codes & CODE_MASK), a, b);
+        A::residues((typename A::RES)(codes >> CODE_BITS), a1, b1);
         sweep2_both<A, G, R>(sw, a, b, a1, b1, lane, prof_a, prof_b, upG0, upF0, upG1, upF1, k.negge, k.neggo,
                              best);
     } else {
         if (live0) {
-            A::residues((typename A::RES)(codes & 0xffffu), a, b);
+            A::residues((typename A::RES)(codes & CODE_MASK), a, b);
             sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG0, upF0, sw.diag, k.negge, k.neggo, best,
                                    sw.botG[0], sw.botF[0]);
         }
         if (live1) {
-            A::residues((typename A::RES)(codes >> 16), a, b);
+            A::residues((typename A::RES)(codes >> CODE_BITS), a, b);
             sweep2_column<A, G, R>(sw, a, b, lane, prof_a, prof_b, upG1, upF1, upG0, k.negge, k.neggo, best,
                                    sw.botG[1], sw.botF[1]);
         }
@@ -852,7 +866,7 @@ __device__ __forceinline__ bool sweep2_item(const ScanParams &p, const int lane,
                                             typename A::V *bnd, uint8_t *smem, uint64_t *bars,
                                             uint32_t &phase, const typename A::V Sv, typename A::V &best) {
     typedef typename A::V V;
-    static_assert(A::NH == 2 && sizeof(typename A::RES) == 2, "two-column steps pair int16 codes");
+    typedef typename TwoCodes<A>::W W2;
     const int n_passes = p.n_passes;
     const uint32_t hi_off = (A::TABLES - 1) * (p.pass_bytes / A::TABLES);
     SweepConst<A> k;
@@ -872,7 +886,7 @@ __device__ __forceinline__ bool sweep2_item(const ScanParams &p, const int lane,
     };
     reset();
     sw.botG[0] = sw.botG[1] = sw.botF[0] = sw.botF[1] = A::splat(0);
-    const uint32_t *res2 = reinterpret_cast<const uint32_t *>(res);  // codes of columns (2i+1, 2i+2)
+    const W2 *res2 = reinterpret_cast<const W2 *>(res);  // codes of columns (2i+1, 2i+2)
     const uint4 *bnd4 = reinterpret_cast<const uint4 *>(bnd);          // boundary of the same pair
     const uint4 none = make_uint4(0, 0, 0, 0);
     // Loads for column pair c of this lane (-1: no column; a dead pair's values are never used).
@@ -1001,12 +1015,13 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
     }
 }
 
-// Whether a scan launch shape runs the two-column sweep: SW scores of int16x2 pairs with at most
-// 16 rows per lane (measured: on the protein benchmark as fast as one column of 32 rows, 10%
-// faster on 64-residue DNA queries).
+// Whether a scan launch shape runs the two-column sweep: SW scores of int16x2 pairs or int32 items
+// with at most 16 rows per lane (measured on the protein benchmark: the pairs 5.5 against 4.9
+// TCUPS for one column of 32 rows; the int32 items of a 5000-residue query 1014 against 594 GCUPS,
+// two independent column chains per lane for their latency-bound warps).
 template <class A, int R, int MODE, bool ENDS, bool GPROF>
 __host__ __device__ constexpr bool two_col_form() {
-    return A::NH == 2 && ModeFlags<MODE>::local && !ENDS && !GPROF && R <= 16;
+    return TwoCodes<A>::OK && ModeFlags<MODE>::local && !ENDS && !GPROF && R <= 16;
 }
 
 #ifdef HY_BOUNDS
