@@ -1016,9 +1016,10 @@ __device__ __forceinline__ void finish_item(const int lane, const bool active, c
 }
 
 // Whether a scan launch shape runs the two-column sweep: SW scores of int16x2 pairs or int32 items
-// with at most 16 rows per lane (measured on the protein benchmark: the pairs 5.5 against 4.9
-// TCUPS for one column of 32 rows; the int32 items of a 5000-residue query 1014 against 594 GCUPS,
-// two independent column chains per lane for their latency-bound warps).
+// with at most 16 rows per lane. Measured on the protein benchmark: for the pairs as fast as one
+// column of 32 rows, with half the per-lane state and 10% faster on 64-residue DNA queries; for the
+// int32 items of a 5000-residue query 1014 against 594 GCUPS (two independent column chains per
+// lane for their latency-bound warps).
 template <class A, int R, int MODE, bool ENDS, bool GPROF>
 __host__ __device__ constexpr bool two_col_form() {
     return TwoCodes<A>::OK && ModeFlags<MODE>::local && !ENDS && !GPROF && R <= 16;
