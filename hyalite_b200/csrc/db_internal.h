@@ -44,6 +44,8 @@ inline int bulk_rows(uint64_t qlen, bool two_col) {
 }
 constexpr int BULK_MAX_RPP = 8 * 32;
 constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;
+// Blocks of one band-kernel cluster at most (the portable cluster size).
+constexpr int BAND_CLUSTER_MAX = 8;
 
 struct Partition {
     uint32_t n_items = 0;

@@ -275,15 +275,32 @@ __global__ void winner_loc_kernel(const unsigned long long *key, const uint32_t 
     win[1] = packed ? NO_INDEX : r;
 }
 
+// The band kernel on one block, or on a cluster of `blocks` blocks (at most 8, the portable
+// cluster size every launch shape of one block per SM can be given).
 template <class A, int MODE, bool GPROF>
-static cudaError_t launch_band_mode(const ScanParams &p, int warps, size_t smem, cudaStream_t st) {
+static cudaError_t launch_band_mode(const ScanParams &p, int warps, int blocks, size_t smem, cudaStream_t st) {
     auto kern = band_kernel<A, WIN_R, MODE, GPROF>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<1, 32 * warps, smem, st>>>(p);
-    return cudaGetLastError();
+    if (GPROF || blocks <= 1) {
+        kern<<<1, 32 * warps, smem, st>>>(p);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(32u * (unsigned)warps);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, p);
 }
 
 // End positions of the single item *item_ptr with the block-cooperative band kernel.
@@ -323,12 +340,20 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     const bool gprof = qp.pass_bytes > budget;
     int warps = gprof ? 32 : (int)std::min<size_t>(32, budget / std::max<uint32_t>(qp.pass_bytes, 1));
     warps = std::max(1, std::min(warps, std::max(qp.n_passes, 1)));
+    // More passes than one block's slices hold: a cluster of blocks, so that the passes run in
+    // as few rounds as possible (one pass slice per warp in each block's shared memory).
+    int blocks = 1;
+    if (!gprof && qp.n_passes > warps) {
+        blocks = std::min(BAND_CLUSTER_MAX, (qp.n_passes + warps - 1) / warps);
+        const int rounds = (qp.n_passes + blocks * warps - 1) / (blocks * warps);
+        warps = (qp.n_passes + rounds * blocks - 1) / (rounds * blocks);  // as few as those rounds need
+    }
     const size_t smem = gprof ? 16 : (size_t)warps * qp.pass_bytes + 16;
     cudaError_t e = cudaErrorInvalidValue;
 #define HY_BAND_CASE(M)                                                                        \
     case M:                                                                                    \
-        e = gprof ? launch_band_mode<A, M, true>(p, warps, smem, sc->stream)                   \
-                  : launch_band_mode<A, M, false>(p, warps, smem, sc->stream);                 \
+        e = gprof ? launch_band_mode<A, M, true>(p, warps, 1, smem, sc->stream)                \
+                  : launch_band_mode<A, M, false>(p, warps, blocks, smem, sc->stream);         \
         break;
     switch (db->mode) {
         HY_BAND_CASE(MODE_SW)

@@ -369,6 +369,48 @@ static __device__ __noinline__ void wait_gave_up(int *err, uint64_t *bars, uint3
         if ((pending >> b) & 1u) mbar_wait_bounded(&bars[b], (phase >> b) & 1u, 1u << 24);
 }
 
+// ---- thread-block clusters (the band kernel's blocks) -----------------------------------------
+// A block not launched as part of a cluster is a cluster of one: rank 0 of 1.
+__device__ __forceinline__ int cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return (int)r;
+}
+__device__ __forceinline__ int cluster_size() {
+    uint32_t n;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+    return (int)n;
+}
+// Every thread of every block of the cluster; orders memory at cluster scope (release, acquire).
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// The 32-bit word at the address of `p` in the shared memory of block `rank` of the cluster.
+__device__ __forceinline__ uint32_t ld_cluster_u32(const void *p, int rank) {
+    uint32_t a, v;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+// The block barrier of a cluster of one, else the cluster barrier.
+__device__ __forceinline__ void band_sync(const int csize) {
+    if (csize > 1)
+        cluster_barrier();
+    else
+        __syncthreads();
+}
+// Whether `v` holds in any block of the cluster (`v` block-uniform; every thread calls it).
+// `flag` is a shared word of this block; no block returns before every block has read the others'.
+__device__ __forceinline__ bool cluster_any(const bool v, uint32_t *flag, const int csize) {
+    if (csize == 1) return v;
+    if (threadIdx.x == 0) *flag = v ? 1u : 0u;
+    cluster_barrier();
+    const uint32_t o = (int)threadIdx.x < csize ? ld_cluster_u32(flag, (int)threadIdx.x) : 0u;
+    const bool any = __syncthreads_or(o != 0);
+    cluster_barrier();
+    return any;
+}
+
 __device__ __forceinline__ unsigned long long hit_key(int32_t score, uint32_t idx) {
     return ((unsigned long long)((uint32_t)score ^ 0x80000000u) << 32) | (uint32_t)(~idx);
 }
@@ -1195,11 +1237,14 @@ __global__ void __launch_bounds__(256, (scan_min_blocks<A, G, R, two_col_form<A,
 // BAND_K steps before the read). The round's profile slices are staged by one TMA bulk copy.
 constexpr int BAND_K = 32;
 
-// The band recovery of item `item` (a valid item of p.meta) by the whole block. `bar` is an
-// initialised mbarrier whose next wait parity is `phase`; the block's dynamic shared memory
-// (`smem`) holds W = blockDim/32 pass slices. Every thread of the block must call it.
-// With GPROF the warps read their pass slices from the profile in global memory; `smem` and `bar`
-// are then unused.
+// The band recovery of item `item` (a valid item of p.meta) by the whole block, or by every block
+// of a thread-block cluster: the cluster's warps take the passes in rounds of W * (blocks), block
+// b's warps the passes b * W .. b * W + W - 1 of a round, and a cluster barrier takes the place of
+// the block barrier between windows (it orders the boundary-row writes of one block's warps before
+// the next block's reads). `bar` is an initialised mbarrier whose next wait parity is `phase`; the
+// block's dynamic shared memory (`smem`) holds W = blockDim/32 pass slices. Every thread of every
+// block must call it. With GPROF (single blocks only) the warps read their pass slices from the
+// profile in global memory; `smem` and `bar` are then unused.
 template <class A, int R, int MODE, bool GPROF = false>
 __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t item, uint8_t *smem,
                                           uint64_t *bar, uint32_t &phase) {
@@ -1210,6 +1255,10 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
     static_assert(R % A::EPV == 0, "rows per lane must fill whole profile vectors");
     const int W = blockDim.x / G;
     const int warp = threadIdx.x / G, lane = threadIdx.x % G;
+    const int crank = cluster_rank(), csize = cluster_size();
+    const int WT = W * csize;          // warps of the cluster
+    const int gw = crank * W + warp;   // this warp's index in the cluster
+    __shared__ uint32_t s_flag;
     const ItemMeta meta = p.meta[item];
 #ifdef HY_BOUNDS
     // Every warp checks the item (the same answer in all of them), so all skip it together.
@@ -1225,29 +1274,35 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
     V best = A::splat(0);
     Cand cand[2] = {{INT32_MIN, INT32_MAX, INT32_MAX}, {INT32_MIN, INT32_MAX, INT32_MAX}};
     const int pass_steps = w + G - 1;
-    const int rounds = (p.n_passes + W - 1) / W;
+    const int rounds = (p.n_passes + WT - 1) / WT;
     for (int round = 0; round < rounds; ++round) {
-        const int first = round * W;
-        const int cnt = min(W, p.n_passes - first);
+        const int first = round * WT;
+        const int cnt = min(WT, p.n_passes - first);          // warps of the cluster with a pass
+        const int bcnt = max(0, min(W, cnt - crank * W));      // ... of this block
         if (!GPROF) {
-            if (threadIdx.x == 0)
-                bulk_load(smem, p.profile + (size_t)first * p.pass_bytes, (uint32_t)cnt * p.pass_bytes, bar);
-            const bool ok = mbar_wait_bounded(bar, phase & 1u, p.wait_polls);
-            phase ^= 1u;
-            if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) wait_gave_up(p.err, bar, 1u, phase ^ 1u);  // the round's copy
+            bool fail = false;
+            if (bcnt > 0) {
+                if (threadIdx.x == 0)
+                    bulk_load(smem, p.profile + (size_t)(first + crank * W) * p.pass_bytes,
+                              (uint32_t)bcnt * p.pass_bytes, bar);
+                const bool ok = mbar_wait_bounded(bar, phase & 1u, p.wait_polls);
+                phase ^= 1u;
+                fail = __syncthreads_or(!ok);
+            }
+            if (cluster_any(fail, &s_flag, csize)) {
+                if (threadIdx.x == 0 && fail) wait_gave_up(p.err, bar, 1u, phase ^ 1u);  // the round's copy
                 return;
             }
         }
-        const int pass = first + warp;
-        const bool mine = warp < cnt && w > 0;
+        const int pass = first + gw;
+        const bool mine = gw < cnt && w > 0;
         const int32_t row0 = p.vrow0 + pass * RPP + lane * R;
         const uint8_t *prof = GPROF ? p.profile + (size_t)min(pass, p.n_passes - 1) * p.pass_bytes
                                     : smem + (size_t)warp * p.pass_bytes;
         const uint8_t *prof_hi = prof + (A::TABLES - 1) * (p.pass_bytes / A::TABLES);
         Sweep<A, R> sw;
         sweep_begin<A, R, MODE>(sw, row0, p.go, p.ge, Sv);
-        const int lag = 2 * BAND_K * warp;
+        const int lag = 2 * BAND_K * gw;
         const int total = pass_steps + 2 * BAND_K * (cnt - 1);
         for (int t0 = 0; t0 < total; t0 += BAND_K) {
             const int s0 = max(t0 - lag, 0), s1 = min(t0 + BAND_K - lag, pass_steps);
@@ -1255,7 +1310,7 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
                 sweep_run<A, G, R, MODE, true>(sw, s0, s1, w, lane, w, meta.n, res, prof, prof_hi, row0,
                                                pass == 0, pass == p.n_passes - 1, bnd, p.qlen, p.go,
                                                p.ge, Sv, best, cand);
-            __syncthreads();
+            band_sync(csize);
         }
         if (mine) sweep_end<A, R, MODE, true>(sw, row0, cand);
         __syncthreads();  // the slices may be restaged for the next round
@@ -1275,14 +1330,22 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
         }
         if (lane == 0) s_cand[warp][h] = cand[h];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    band_sync(csize);  // every block's candidates are in its shared memory
+    if (threadIdx.x == 0 && crank == 0) {
         for (int h = 0; h < A::NH; ++h) {
             const uint32_t idx = meta.idx[h];
             if (idx == NO_INDEX) continue;
             Cand c = border_seed<MODE>(p.qlen, (int32_t)meta.n[h], p.go, p.ge);
-            for (int k = 0; k < W; ++k)
-                if (better(s_cand[k][h], c)) c = s_cand[k][h];
+            for (int b = 0; b < csize; ++b)
+                for (int k = 0; k < W; ++k) {
+                    Cand o = s_cand[k][h];
+                    if (b > 0) {
+                        o.s = (int32_t)ld_cluster_u32(&s_cand[k][h].s, b);
+                        o.col = (int32_t)ld_cluster_u32(&s_cand[k][h].col, b);
+                        o.row = (int32_t)ld_cluster_u32(&s_cand[k][h].row, b);
+                    }
+                    if (better(o, c)) c = o;
+                }
             if (p.ends_out) {
                 if (idx == ~(uint32_t)(*p.best_key & 0xffffffffu)) {
                     p.ends_out[0] = c.s;
@@ -1296,6 +1359,7 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
             }
         }
     }
+    if (csize > 1) cluster_barrier();  // block 0 has read every block's candidates
 }
 
 template <class A, int R, int MODE, bool GPROF = false>

@@ -72,6 +72,25 @@ def test_scan_wait_that_gives_up_is_a_timeout_and_the_scratch_recovers():
     assert got == ref.scan_all(q)
 
 
+def test_band_cluster_wait_that_gives_up_is_a_timeout_and_the_scratch_recovers():
+    # A 2000-residue query: 8 band passes of 256 rows, more than one block's shared memory holds
+    # (4 pass slices of int16x2 pairs for this alphabet), so the winner's ends run on a cluster of
+    # two blocks; every block gives up at its first profile wait and the whole cluster returns.
+    hy = _hy()
+    rng = np.random.default_rng(507)
+    seqs, db = _protein_db(hy, rng, n=800, mql=2000)
+    ref = o.OracleDb(seqs, BLOSUM62, 20, 11, 1, 0, 1)
+    sc = hy.Scratch(db)
+    q = rng.integers(0, 20, 2000).astype(np.uint8)
+    want = ref.scan(q)
+    assert hit_tuple(db.scan(sc, q)) == want
+    with _WaitPolls(hy, 0):
+        with pytest.raises(hy.Error) as e:
+            db.scan(sc, q)
+        assert e.value.kind == "Timeout"
+    assert hit_tuple(db.scan(sc, q)) == want
+
+
 def test_int32_pipeline_wait_that_gives_up_is_a_timeout_and_the_scratch_recovers():
     # A 3000-residue query against targets longer than 2978 residues: those run in int32 lanes
     # (BLOSUM62's largest entry 11: 11 * 2979 + 11 > 32767), as pipelined passes.
