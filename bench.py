@@ -40,10 +40,10 @@ GO, GE = 11, 1
 AL = 20
 # DRAM bytes (read + write) per DP cell of the int16x2 pair kernel, from one ncu capture of
 # scan_kernel<Pair16, 8, 16> (two-column sweep) on 400,000 sequences x one 1000-residue query:
-# 1.039e9 + 1.625e9 bytes for 1.655e11 cells. The traffic is the boundary rows between query
+# 0.537e9 + 1.285e9 bytes for 1.655e11 cells. The traffic is the boundary rows between query
 # passes plus the residues, so it grows with cells at a fixed rows-per-pass; profiles/ holds the
 # capture's summary and command.
-DRAM_BYTES_PER_CELL = (1.039e9 + 1.625e9) / 1.655e11
+DRAM_BYTES_PER_CELL = (0.537e9 + 1.285e9) / 1.655e11
 
 
 def make_workload(seed: int, n_seqs: int = N_SEQS):
