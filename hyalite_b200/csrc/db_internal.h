@@ -31,14 +31,14 @@ constexpr uint32_t NO_LONG_SPLIT = 0xffffffffu;
 constexpr int BLOCK = 256;
 // Rows per lane of the bulk int16x2 kernel for a query of length qlen (passes of MAIN_G * rows).
 // SW scores run the two-column sweep at 8 or 16 rows per lane: 16 unless 8 pads the query to so
-// many fewer rows that it wins at 8 rows' rate per padded row (measured 10/11 of 16 rows' rate:
-// 300 residues take 320 rows at 8 against 384 at 16, 9% faster; 150 residues 21% faster). The
-// other kinds run one column of up to 32 rows.
+// many fewer rows that it wins at 8 rows' rate per padded row (measured 0.853 of 16 rows' rate,
+// 4813 against 5641 GCUPS for 1000-residue queries on the protein benchmark: 150 residues take 192
+// rows at 8 against 256 at 16). The other kinds run one column of up to 32 rows.
 inline int bulk_rows(uint64_t qlen, bool two_col) {
     if (qlen <= 64) return 8;
     if (two_col) {
         const uint64_t rows8 = (qlen + 63) / 64 * 64, rows16 = (qlen + 127) / 128 * 128;
-        return 11 * rows8 < 10 * rows16 ? 8 : 16;
+        return 7 * rows8 < 6 * rows16 ? 8 : 16;
     }
     return qlen <= 192 ? 16 : 32;
 }
