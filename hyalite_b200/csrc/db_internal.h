@@ -47,6 +47,17 @@ constexpr size_t BAND_SMEM_BUDGET = 200 * 1024;
 // Blocks of one band-kernel cluster at most (the portable cluster size).
 constexpr int BAND_CLUSTER_MAX = 8;
 
+// One long pair's BestHit cell on the band kernel (int32 lanes): the query already on the device
+// (d_q, m residues), the target on the host (t, tl residues, copied here). Writes the score and the
+// 0-based query and target ends (-1 for row or column 0) at index `slot` of d_scores / d_qend /
+// d_tend on stream `st` and waits for them; adds the band kernel's time to *kernel_ms.
+// Whether a long pair with an m-residue query runs its band passes in one round of one block or
+// cluster (band_long_pair's shape); longer queries take the stripe kernel.
+bool band_long_pair_fits(uint64_t m, uint64_t al);
+hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *d_matrix,
+                         uint64_t al, int32_t go, int32_t ge, int mode, cudaStream_t st, uint32_t slot,
+                         int32_t *d_scores, int32_t *d_qend, int32_t *d_tend, double *kernel_ms);
+
 struct Partition {
     uint32_t n_items = 0;
     uint64_t n_seqs = 0;

@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <numeric>
 #include <vector>
 
@@ -303,6 +304,33 @@ static cudaError_t launch_band_mode(const ScanParams &p, int warps, int blocks, 
     return cudaLaunchKernelEx(&cfg, kern, p);
 }
 
+// Launch shape of the band kernel for a query plan: one pass slice per warp in shared memory (a
+// slice too large for that runs from the profile in global memory, 32 warps on one block); more
+// passes than one block's slices hold take a cluster of blocks, so that the passes run in as few
+// rounds as possible.
+struct BandShape {
+    bool gprof;
+    int warps, blocks;
+    size_t smem;
+};
+static BandShape band_shape(const QueryPlan &qp, size_t smem_limit) {
+    BandShape sh;
+    const size_t budget = std::min<size_t>(BAND_SMEM_BUDGET, smem_limit - 16);
+    sh.gprof = qp.pass_bytes > budget;
+    int warps = sh.gprof ? 32 : (int)std::min<size_t>(32, budget / std::max<uint32_t>(qp.pass_bytes, 1));
+    warps = std::max(1, std::min(warps, std::max(qp.n_passes, 1)));
+    int blocks = 1;
+    if (!sh.gprof && qp.n_passes > warps) {
+        blocks = std::min(BAND_CLUSTER_MAX, (qp.n_passes + warps - 1) / warps);
+        const int rounds = (qp.n_passes + blocks * warps - 1) / (blocks * warps);
+        warps = (qp.n_passes + rounds * blocks - 1) / (rounds * blocks);  // as few as those rounds need
+    }
+    sh.warps = warps;
+    sh.blocks = blocks;
+    sh.smem = sh.gprof ? 16 : (size_t)warps * qp.pass_bytes + 16;
+    return sh;
+}
+
 // End positions of the single item *item_ptr with the block-cooperative band kernel.
 template <class A>
 static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &part,
@@ -334,21 +362,10 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     p.err = sc->d_err;
     p.wait_polls = wait_polls();
     set_extents<A>(p, db, part, part.total_cols);
-    // One pass slice per warp in shared memory; a slice too large for that runs from the profile
-    // in global memory.
-    const size_t budget = std::min<size_t>(BAND_SMEM_BUDGET, db->smem_limit - 16);
-    const bool gprof = qp.pass_bytes > budget;
-    int warps = gprof ? 32 : (int)std::min<size_t>(32, budget / std::max<uint32_t>(qp.pass_bytes, 1));
-    warps = std::max(1, std::min(warps, std::max(qp.n_passes, 1)));
-    // More passes than one block's slices hold: a cluster of blocks, so that the passes run in
-    // as few rounds as possible (one pass slice per warp in each block's shared memory).
-    int blocks = 1;
-    if (!gprof && qp.n_passes > warps) {
-        blocks = std::min(BAND_CLUSTER_MAX, (qp.n_passes + warps - 1) / warps);
-        const int rounds = (qp.n_passes + blocks * warps - 1) / (blocks * warps);
-        warps = (qp.n_passes + rounds * blocks - 1) / (rounds * blocks);  // as few as those rounds need
-    }
-    const size_t smem = gprof ? 16 : (size_t)warps * qp.pass_bytes + 16;
+    BandShape sh = band_shape(qp, db->smem_limit);
+    const bool gprof = sh.gprof;
+    const int warps = sh.warps, blocks = sh.blocks;
+    const size_t smem = sh.smem;
     cudaError_t e = cudaErrorInvalidValue;
 #define HY_BAND_CASE(M)                                                                        \
     case M:                                                                                    \
@@ -365,6 +382,156 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
 #undef HY_BAND_CASE
     HY_CK(e);
     sc->launches += qp.n_passes > 0 ? 2 : 1;
+    return fail(HY_OK);
+}
+
+// Device buffers of band_long_pair, grow-only, per calling thread and device.
+struct BandPairContext {
+    int device = -1;
+    size_t smem_limit = 0;
+    uint8_t *prof = nullptr, *t = nullptr;
+    size_t c_prof = 0, c_t = 0;
+    int32_t *bnd = nullptr;
+    size_t c_bnd = 0;
+    ItemMeta *meta = nullptr;  // one item, then its index (a uint32) and the error word
+    uint8_t *h_stage = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~BandPairContext() {
+        hy::dev_free(prof);
+        hy::dev_free(t);
+        hy::dev_free(bnd);
+        hy::dev_free(meta);
+        if (h_stage) cudaFreeHost(h_stage);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+static thread_local std::unique_ptr<BandPairContext> g_band_pair;
+
+template <class T>
+static cudaError_t grow_dev(T *&p, size_t &cap, size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    cudaError_t e = hy::dev_free(p);
+    p = nullptr;
+    cap = 0;
+    if (e != cudaSuccess) return e;
+    e = hy::dev_malloc(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+}
+
+bool band_long_pair_fits(uint64_t m, uint64_t al) {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const QueryPlan qp = plan_for<Single32>(m, WIN_G * WIN_R, al);
+    const BandShape sh = band_shape(qp, (size_t)optin);
+    return !sh.gprof && qp.n_passes <= sh.warps * sh.blocks;
+}
+
+hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *d_matrix,
+                         uint64_t al, int32_t go, int32_t ge, int mode, cudaStream_t st, uint32_t slot,
+                         int32_t *d_scores, int32_t *d_qend, int32_t *d_tend, double *kernel_ms) {
+    int dev = 0;
+    HY_CK(cudaGetDevice(&dev));
+    if (g_band_pair && g_band_pair->device != dev) g_band_pair.reset();
+    if (!g_band_pair) {
+        std::unique_ptr<BandPairContext> c(new BandPairContext);
+        c->device = dev;
+        int optin = 0;
+        HY_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        c->smem_limit = (size_t)optin;
+        HY_CK(hy::dev_malloc(&c->meta, 64));
+        HY_CK(cudaMallocHost((void **)&c->h_stage, 64));
+        HY_CK(cudaEventCreate(&c->ev[0]));
+        HY_CK(cudaEventCreate(&c->ev[1]));
+        g_band_pair = std::move(c);
+    }
+    BandPairContext &c = *g_band_pair;
+    const QueryPlan qp = plan_for<Single32>(m, WIN_G * WIN_R, al);
+    HY_CK(grow_dev(c.prof, c.c_prof, std::max<size_t>(16, (size_t)qp.pass_bytes * qp.n_passes)));
+    HY_CK(grow_dev(c.t, c.c_t, std::max<uint64_t>(16, tl)));
+    HY_CK(grow_dev(c.bnd, c.c_bnd, sizeof(int32_t) * std::max<uint64_t>(16, 2 * tl)));
+    // The item (the target as one int32 column run, the pair's slot as its index), its index and
+    // a cleared error word, staged together; then the target's residues.
+    ItemMeta im{};
+    im.col_off = 0;
+    im.w = (uint32_t)tl;
+    im.n[0] = (uint32_t)tl;
+    im.n[1] = 0;
+    im.idx[0] = slot;
+    im.idx[1] = NO_INDEX;
+    const uint32_t zero_item = 0;
+    const int zero_err = 0;
+    memcpy(c.h_stage, &im, sizeof(im));
+    memcpy(c.h_stage + 32, &zero_item, 4);
+    memcpy(c.h_stage + 36, &zero_err, 4);
+    HY_CK(cudaMemcpyAsync(c.meta, c.h_stage, 40, cudaMemcpyHostToDevice, st));
+    if (tl) HY_CK(cudaMemcpyAsync(c.t, t, tl, cudaMemcpyHostToDevice, st));
+    const uint8_t *base = reinterpret_cast<const uint8_t *>(c.meta);
+    const bool top_free = mode == MODE_SW || mode == MODE_HW || mode == MODE_OV;
+    const int64_t words = Single32::letters((int64_t)al) * WIN_G * WIN_R * (int64_t)qp.n_passes;
+    if (words > 0) {
+        build_profile_kernel<Single32, WIN_G, WIN_R><<<(int)std::min<int64_t>((words + 255) / 256, 148 * 16), 256, 0, st>>>(
+            d_q, (int32_t)m, d_matrix, (int32_t)al, go, LIM32, top_free ? 1 : 0, qp.vrow0, qp.n_passes,
+            reinterpret_cast<Single32::PE *>(c.prof));
+        HY_CK(cudaGetLastError());
+    }
+    ScanParams p{};
+    p.meta = c.meta;
+    p.item_base = 0;
+    p.n_items = 1;
+    p.item_ptr = reinterpret_cast<const uint32_t *>(base + 32);
+    p.res = c.t;
+    p.profile = c.prof;
+    p.pass_bytes = qp.pass_bytes;
+    p.n_passes = qp.n_passes;
+    p.vrow0 = qp.vrow0;
+    p.qlen = (int32_t)m;
+    p.go = go;
+    p.ge = ge;
+    p.sentinel = INT32_MIN / 4;
+    p.boundary = c.bnd;
+    p.bnd_col0 = 0;
+    p.scores = d_scores;
+    p.qend = d_qend;
+    p.tend = d_tend;
+    p.best_key = nullptr;
+    p.err = reinterpret_cast<int *>(const_cast<uint8_t *>(base) + 36);
+    p.wait_polls = wait_polls();
+    p.res_cols = tl;
+    p.bnd_cols = tl;
+    p.n_seqs = slot + 1;
+    p.letters = (uint32_t)Single32::letters((int64_t)al);
+    const BandShape sh = band_shape(qp, c.smem_limit);
+    cudaError_t e = cudaErrorInvalidValue;
+    HY_CK(cudaEventRecord(c.ev[0], st));
+#define HY_PAIR_BAND_CASE(M)                                                                      \
+    case M:                                                                                       \
+        e = sh.gprof ? launch_band_mode<Single32, M, true>(p, sh.warps, 1, sh.smem, st)           \
+                     : launch_band_mode<Single32, M, false>(p, sh.warps, sh.blocks, sh.smem, st); \
+        break;
+    switch (mode) {
+        HY_PAIR_BAND_CASE(MODE_SW)
+        HY_PAIR_BAND_CASE(MODE_NW)
+        HY_PAIR_BAND_CASE(MODE_HW)
+        HY_PAIR_BAND_CASE(MODE_OV)
+        HY_PAIR_BAND_CASE(MODE_SHW)
+    }
+#undef HY_PAIR_BAND_CASE
+    HY_CK(e);
+    HY_CK(cudaEventRecord(c.ev[1], st));
+    HY_CK(cudaMemcpyAsync(c.h_stage + 36, base + 36, 4, cudaMemcpyDeviceToHost, st));
+    HY_CK(cudaStreamSynchronize(st));
+    int err = 0;
+    memcpy(&err, c.h_stage + 36, 4);
+    if (err) return fail(device_error(err));
+    float ms = 0.f;
+    HY_CK(cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]));
+    if (kernel_ms) *kernel_ms += ms;
     return fail(HY_OK);
 }
 

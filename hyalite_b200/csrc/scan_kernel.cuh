@@ -428,7 +428,7 @@ struct Sweep {
     typename A::V Gp[R], E[R];  // G (= H - go) of the previous column and E, per row slot
     typename A::V diag;         // G of the row above at the previous column (row slot 0)
     typename A::V botG, botF;   // this lane's last row at its current column, for lane L+1
-    // SW end tracking within a pass: the running per-half maximum and the cell id
+    // SW end tracking within a pass: the running per-half maximum of G (= H - go) and the cell id
     // (column * R + slot) where it was first reached; column-major order inside the lane means
     // the first strict improvement is the smallest (column, row).
     typename A::V pbest;
@@ -527,11 +527,12 @@ __device__ __forceinline__ void sweep_step(Sweep<A, R> &sw, const int s, const i
                     A::template load_chunk<R, G>(prof_a, prof_b, a, b, lane, r / A::EPV, pa, pb);
                 sw.E[r] = A::addmax(sw.E[r], negge, sw.Gp[r]);
                 V h;
-                if (Fl::local && !ENDS) {
-                    // SW scores, with a one-op dependency chain from row to row: with x = max(d,
-                    // E, 0) - go, G = max(F - go, x) and, since go >= ge, F of the next row =
-                    // max(F - ge, G) = max(F - ge, x). x >= -go, so nothing leaves int16. h here is
-                    // G; the running maximum is kept in G (started at -go, go added at the end).
+                if (Fl::local) {
+                    // SW, with a one-op dependency chain from row to row: with x = max(d, E, 0) -
+                    // go, G = max(F - go, x) and, since go >= ge, F of the next row = max(F - ge,
+                    // G) = max(F - ge, x). x >= -go, so nothing leaves int16. h here is G; the
+                    // running maximum (and with ENDS the tracked best cell) is kept in G, go added
+                    // at the end.
                     f = A::addmax(f, negge, r == 0 ? g_up : xprev);
                     const V d = A::diag(gd, pa[r % A::EPV], pb[r % A::EPV]);
                     const V x = A::vadd(A::vmax3_relu(d, sw.E[r], d), neggo);
@@ -688,11 +689,14 @@ __device__ __forceinline__ void sweep_run(Sweep<A, R> &sw, const int s_begin, co
                                                              best, cand, 0, 0, 0, cmo);
 }
 
+// The lane's tracked best cell of the pass as a candidate (local mode: pbest holds G = H - go).
 template <class A, int R, int MODE, bool ENDS>
-__device__ __forceinline__ void sweep_end(const Sweep<A, R> &sw, const int32_t row0, Cand (&cand)[2]) {
+__device__ __forceinline__ void sweep_end(const Sweep<A, R> &sw, const int32_t row0, const int32_t go,
+                                          Cand (&cand)[2]) {
     if (ModeFlags<MODE>::local && ENDS) {
-        if (sw.pid0 >= 0) consider(cand[0], A::get(sw.pbest, 0), sw.pid0 / R, row0 + sw.pid0 % R);
-        if (A::NH > 1 && sw.pid1 >= 0) consider(cand[1], A::get(sw.pbest, 1), sw.pid1 / R, row0 + sw.pid1 % R);
+        if (sw.pid0 >= 0) consider(cand[0], A::get(sw.pbest, 0) + go, sw.pid0 / R, row0 + sw.pid0 % R);
+        if (A::NH > 1 && sw.pid1 >= 0)
+            consider(cand[1], A::get(sw.pbest, 1) + go, sw.pid1 / R, row0 + sw.pid1 % R);
     }
 }
 
@@ -713,7 +717,7 @@ __device__ __forceinline__ void sweep_pass(const int lane, const int steps, cons
     sweep_run<A, G, R, MODE, ENDS, true, COLMAX>(sw, 0, steps, w_min, lane, w, n, res, prof_a, prof_b,
                                                  row0, first_pass, last_pass, bnd, qlen, go, ge, Sv,
                                                  best, cand, cmo);
-    sweep_end<A, R, MODE, ENDS>(sw, row0, cand);
+    sweep_end<A, R, MODE, ENDS>(sw, row0, go, cand);
 }
 
 // ---- two columns per step: the SW score sweep of int16x2 pairs and int32 items ------------------
@@ -1312,7 +1316,7 @@ __device__ __forceinline__ void band_item(const ScanParams &p, const uint32_t it
                                                p.ge, Sv, best, cand);
             band_sync(csize);
         }
-        if (mine) sweep_end<A, R, MODE, true>(sw, row0, cand);
+        if (mine) sweep_end<A, R, MODE, true>(sw, row0, p.go, cand);
         __syncthreads();  // the slices may be restaged for the next round
     }
     // Reduce every lane's candidates: inside each warp, then across warps in shared memory.

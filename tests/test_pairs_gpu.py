@@ -160,6 +160,30 @@ def test_single_long_pair_align_pair():
             (lambda s: (s[0], 0, s[1], s[2]))(o.align_pair(q, t, BLOSUM62, 20, 11, 1, mode))
 
 
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_single_long_pair_band_shapes(mode):
+    """One long pair runs on the band kernel in int32 lanes, its 256-row passes on the warps of one
+    block or of a cluster: 2000 rows (8 passes, one block), 5000 rows (20 passes, a cluster of 3
+    blocks of 7 warps, one round), 20000 rows against 60 columns (79 passes, a cluster of 8 blocks
+    of 9 warps, two rounds); an int32-range scoring; Score and ScoreEnd (src/kernel.rs:331-397)."""
+    rng = np.random.default_rng(90 + mode)
+    base = list(rng.integers(0, 20, 5000))
+    cases = [(base[:2000], _related(rng, base[:2000], 20, 0.3)),
+             (base, _related(rng, base, 20, 0.15)),
+             (list(rng.integers(0, 20, 20000)), list(rng.integers(0, 20, 60)))]
+    sc = hy.Scoring(20, BLOSUM62, 11, 1)
+    for q, t in cases:
+        for st in (hy.SearchType.Score, hy.SearchType.ScoreEnd):
+            h = hy.align_pair(q, t, sc, hy.Mode(mode), st)
+            s, qe, te = o.align_pair(q, t, BLOSUM62, 20, 11, 1, mode)
+            want = (s, 0, qe, te) if st == hy.SearchType.ScoreEnd else (s, 0, None, None)
+            assert (h.score, h.db_index, h.query_end, h.target_end) == want, (len(q), len(t), st)
+    big = [int(v) for v in rng.integers(-900, 900, 400)]
+    q, t = cases[0]
+    h = hy.align_pair(q, t, hy.Scoring(20, big, 50, 3), hy.Mode(mode), hy.SearchType.ScoreEnd)
+    assert (h.score, h.query_end, h.target_end) == o.align_pair(q, t, big, 20, 50, 3, mode)
+
+
 def _concat(seqs):
     off = np.zeros(len(seqs) + 1, np.uint64)
     off[1:] = np.cumsum([len(s) for s in seqs])
