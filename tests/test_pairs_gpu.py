@@ -162,10 +162,11 @@ def test_single_long_pair_align_pair():
 
 @pytest.mark.parametrize("mode", ALL_MODES)
 def test_single_long_pair_band_shapes(mode):
-    """One long pair runs on the band kernel in int32 lanes, its 256-row passes on the warps of one
-    block or of a cluster: 2000 rows (8 passes, one block), 5000 rows (20 passes, a cluster of 3
-    blocks of 7 warps, one round), 20000 rows against 60 columns (79 passes, a cluster of 8 blocks
-    of 9 warps, two rounds); an int32-range scoring; Score and ScoreEnd (src/kernel.rs:331-397)."""
+    """One long pair runs on the band kernel in int32 lanes when its 256-row passes fit one round,
+    on the warps of one block or of a cluster: 2000 rows (8 passes, one block), 5000 rows (20
+    passes, a cluster of 3 blocks of 7 warps); 20000 rows against 60 columns (79 passes, more than
+    one round) takes the stripe kernel; an int32-range scoring; Score and ScoreEnd
+    (src/kernel.rs:331-397)."""
     rng = np.random.default_rng(90 + mode)
     base = list(rng.integers(0, 20, 5000))
     cases = [(base[:2000], _related(rng, base[:2000], 20, 0.3)),

@@ -30,6 +30,22 @@ def test_rows_per_lane_and_pass_boundaries(mode):
         check(seqs, mat, 20, 11, 1, mode, st, queries, mql=max(SHAPE_QLENS))
 
 
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_winner_band_on_a_cluster_over_two_rounds(mode):
+    # A 9000-residue ScoreEnd query: the winner's end recovery has 36 passes of 256 rows, more than
+    # a cluster of 8 blocks holds slices for (4 int16x2 slices a block for this alphabet), so it
+    # runs in two rounds on 8 blocks of 3 warps (src/database.rs:186-197).
+    from gpu_helpers import BLOSUM62
+
+    rng = np.random.default_rng(320 + mode)
+    seqs = rand_seqs(rng, 120, 20, 20, 300)
+    q = list(rng.integers(0, 20, 9000))
+    seqs[37] = q[4000:4250]  # a clear winner inside the query
+    db = build(seqs, BLOSUM62, 20, 11, 1, mode, 1, mql=9000)
+    ref = o.OracleDb(seqs, BLOSUM62, 20, 11, 1, mode, 1)
+    assert hit_tuple(db.scan(hy.Scratch(db), q)) == ref.scan(q)
+
+
 def _protein(n_seqs, seed):
     rng = np.random.default_rng(seed)
     base = np.random.default_rng(12345)
