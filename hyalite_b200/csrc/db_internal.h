@@ -57,6 +57,11 @@ bool band_long_pair_fits(uint64_t m, uint64_t al);
 hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *d_matrix,
                          uint64_t al, int32_t go, int32_t ge, int mode, cudaStream_t st, uint32_t slot,
                          int32_t *d_scores, int32_t *d_qend, int32_t *d_tend, double *kernel_ms);
+// The same for a lone pair whose query, target and matrix are on the host (align_pair's direct
+// path): one copy in, the profile and band kernels, one copy out. out = {score, query end, target
+// end}.
+hy_status band_single_pair(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *matrix,
+                           uint64_t al, int32_t go, int32_t ge, int mode, int32_t out[3], double *kernel_ms);
 
 struct Partition {
     uint32_t n_items = 0;

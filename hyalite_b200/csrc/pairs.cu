@@ -823,6 +823,23 @@ static hy_status pairs_run(const uint8_t *q_res, const uint64_t *q_off, const ui
     const uint64_t *n_part = lp.n_part;
     const std::vector<uint32_t> &run_long = lp.run_long;
     ctx.phase_ms[0] = since(t_call);
+    // One long pair whose band passes fit one round (align_pair's single-pair path): straight to the
+    // band kernel with one copy in and one copy out, without the chunk pipeline.
+    if (n_pairs == 1 && !pc.posmax && n_len == 1 && n_long_bad == 1 && run_long.size() == 1 &&
+        band_long_pair_fits(q_off[1] - q_off[0], alphabet_len)) {
+        int32_t r[3];
+        st = band_single_pair(q_res + q_off[0], q_off[1] - q_off[0], t_res + t_off[0], t_off[1] - t_off[0], matrix,
+                              alphabet_len, gap_open, gap_ext, (int)mode, r, &ctx.kernel_ms);
+        if (st != HY_OK) return st;
+        const bool with_ends = search_type != HY_SEARCH_SCORE;
+        out[0].score = r[0];
+        out[0].reserved = 0;
+        out[0].db_index = 0;
+        out[0].query_end = with_ends ? (int64_t)r[1] : -1;
+        out[0].target_end = with_ends ? (int64_t)r[2] : -1;
+        ctx.call_ms = since(t_call);
+        return fail(HY_OK);
+    }
 
     uint32_t dev_bad = NO_INDEX;  // the first pair whose symbols the device found out of range
     const bool ends = !pc.posmax && search_type != HY_SEARCH_SCORE;

@@ -385,25 +385,31 @@ static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &
     return fail(HY_OK);
 }
 
-// Device buffers of band_long_pair, grow-only, per calling thread and device.
+// Device buffers of the long-pair band paths, grow-only, per calling thread and device.
 struct BandPairContext {
     int device = -1;
     size_t smem_limit = 0;
-    uint8_t *prof = nullptr, *t = nullptr;
-    size_t c_prof = 0, c_t = 0;
+    cudaStream_t stream = nullptr;  // band_single_pair's own
+    uint8_t *prof = nullptr, *in = nullptr;
+    size_t c_prof = 0, c_in = 0;
     int32_t *bnd = nullptr;
     size_t c_bnd = 0;
-    ItemMeta *meta = nullptr;  // one item, then its index (a uint32) and the error word
-    uint8_t *h_stage = nullptr;
+    // One item (32 bytes), its index (a uint32 at +32), the error word (+36) and band_single_pair's
+    // score, query end and target end (+40).
+    ItemMeta *meta = nullptr;
+    uint8_t *h_stage = nullptr, *h_in = nullptr;
+    size_t ch_in = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     ~BandPairContext() {
         hy::dev_free(prof);
-        hy::dev_free(t);
+        hy::dev_free(in);
         hy::dev_free(bnd);
         hy::dev_free(meta);
         if (h_stage) cudaFreeHost(h_stage);
+        if (h_in) cudaFreeHost(h_in);
         for (cudaEvent_t e : ev)
             if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
     }
 };
 static thread_local std::unique_ptr<BandPairContext> g_band_pair;
@@ -432,9 +438,8 @@ bool band_long_pair_fits(uint64_t m, uint64_t al) {
     return !sh.gprof && qp.n_passes <= sh.warps * sh.blocks;
 }
 
-hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *d_matrix,
-                         uint64_t al, int32_t go, int32_t ge, int mode, cudaStream_t st, uint32_t slot,
-                         int32_t *d_scores, int32_t *d_qend, int32_t *d_tend, double *kernel_ms) {
+// The calling thread's context on the current device.
+static hy_status band_pair_context(BandPairContext *&out) {
     int dev = 0;
     HY_CK(cudaGetDevice(&dev));
     if (g_band_pair && g_band_pair->device != dev) g_band_pair.reset();
@@ -448,15 +453,25 @@ hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint6
         HY_CK(cudaMallocHost((void **)&c->h_stage, 64));
         HY_CK(cudaEventCreate(&c->ev[0]));
         HY_CK(cudaEventCreate(&c->ev[1]));
+        HY_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         g_band_pair = std::move(c);
     }
-    BandPairContext &c = *g_band_pair;
+    out = g_band_pair.get();
+    return fail(HY_OK);
+}
+
+// Enqueues one long pair's profile and band kernel on `st`: the query, target and matrix already on
+// the device, the item staged in c.h_stage (its first 40 bytes go with it). Records the band's time
+// between c.ev[0] and c.ev[1].
+static hy_status band_pair_enqueue(BandPairContext &c, const uint8_t *d_q, uint64_t m, const uint8_t *d_t, uint64_t tl,
+                                   const int32_t *d_matrix, uint64_t al, int32_t go, int32_t ge, int mode,
+                                   cudaStream_t st, uint32_t slot, int32_t *d_scores, int32_t *d_qend,
+                                   int32_t *d_tend) {
     const QueryPlan qp = plan_for<Single32>(m, WIN_G * WIN_R, al);
     HY_CK(grow_dev(c.prof, c.c_prof, std::max<size_t>(16, (size_t)qp.pass_bytes * qp.n_passes)));
-    HY_CK(grow_dev(c.t, c.c_t, std::max<uint64_t>(16, tl)));
     HY_CK(grow_dev(c.bnd, c.c_bnd, sizeof(int32_t) * std::max<uint64_t>(16, 2 * tl)));
     // The item (the target as one int32 column run, the pair's slot as its index), its index and
-    // a cleared error word, staged together; then the target's residues.
+    // a cleared error word.
     ItemMeta im{};
     im.col_off = 0;
     im.w = (uint32_t)tl;
@@ -470,7 +485,6 @@ hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint6
     memcpy(c.h_stage + 32, &zero_item, 4);
     memcpy(c.h_stage + 36, &zero_err, 4);
     HY_CK(cudaMemcpyAsync(c.meta, c.h_stage, 40, cudaMemcpyHostToDevice, st));
-    if (tl) HY_CK(cudaMemcpyAsync(c.t, t, tl, cudaMemcpyHostToDevice, st));
     const uint8_t *base = reinterpret_cast<const uint8_t *>(c.meta);
     const bool top_free = mode == MODE_SW || mode == MODE_HW || mode == MODE_OV;
     const int64_t words = Single32::letters((int64_t)al) * WIN_G * WIN_R * (int64_t)qp.n_passes;
@@ -485,7 +499,7 @@ hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint6
     p.item_base = 0;
     p.n_items = 1;
     p.item_ptr = reinterpret_cast<const uint32_t *>(base + 32);
-    p.res = c.t;
+    p.res = d_t;
     p.profile = c.prof;
     p.pass_bytes = qp.pass_bytes;
     p.n_passes = qp.n_passes;
@@ -524,11 +538,63 @@ hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint6
 #undef HY_PAIR_BAND_CASE
     HY_CK(e);
     HY_CK(cudaEventRecord(c.ev[1], st));
+    return fail(HY_OK);
+}
+
+hy_status band_long_pair(const uint8_t *d_q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *d_matrix,
+                         uint64_t al, int32_t go, int32_t ge, int mode, cudaStream_t st, uint32_t slot,
+                         int32_t *d_scores, int32_t *d_qend, int32_t *d_tend, double *kernel_ms) {
+    BandPairContext *cp = nullptr;
+    hy_status s0 = band_pair_context(cp);
+    if (s0 != HY_OK) return s0;
+    BandPairContext &c = *cp;
+    HY_CK(grow_dev(c.in, c.c_in, std::max<uint64_t>(16, tl)));
+    if (tl) HY_CK(cudaMemcpyAsync(c.in, t, tl, cudaMemcpyHostToDevice, st));
+    s0 = band_pair_enqueue(c, d_q, m, c.in, tl, d_matrix, al, go, ge, mode, st, slot, d_scores, d_qend, d_tend);
+    if (s0 != HY_OK) return s0;
+    const uint8_t *base = reinterpret_cast<const uint8_t *>(c.meta);
     HY_CK(cudaMemcpyAsync(c.h_stage + 36, base + 36, 4, cudaMemcpyDeviceToHost, st));
     HY_CK(cudaStreamSynchronize(st));
     int err = 0;
     memcpy(&err, c.h_stage + 36, 4);
     if (err) return fail(device_error(err));
+    float ms = 0.f;
+    HY_CK(cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]));
+    if (kernel_ms) *kernel_ms += ms;
+    return fail(HY_OK);
+}
+
+hy_status band_single_pair(const uint8_t *q, uint64_t m, const uint8_t *t, uint64_t tl, const int32_t *matrix,
+                           uint64_t al, int32_t go, int32_t ge, int mode, int32_t out[3], double *kernel_ms) {
+    BandPairContext *cp = nullptr;
+    hy_status s0 = band_pair_context(cp);
+    if (s0 != HY_OK) return s0;
+    BandPairContext &c = *cp;
+    // Query, target and matrix staged together for one copy (the matrix 4-byte aligned).
+    const uint64_t mat_off = (m + tl + 3) / 4 * 4, bytes = mat_off + sizeof(int32_t) * al * al;
+    if (bytes > c.ch_in) {
+        if (c.h_in) cudaFreeHost(c.h_in);
+        c.h_in = nullptr;
+        c.ch_in = 0;
+        HY_CK(cudaMallocHost((void **)&c.h_in, bytes));
+        c.ch_in = bytes;
+    }
+    memcpy(c.h_in, q, m);
+    memcpy(c.h_in + m, t, tl);
+    memcpy(c.h_in + mat_off, matrix, sizeof(int32_t) * al * al);
+    HY_CK(grow_dev(c.in, c.c_in, bytes));
+    HY_CK(cudaMemcpyAsync(c.in, c.h_in, bytes, cudaMemcpyHostToDevice, c.stream));
+    int32_t *d_res = reinterpret_cast<int32_t *>(reinterpret_cast<uint8_t *>(c.meta) + 40);
+    s0 = band_pair_enqueue(c, c.in, m, c.in + m, tl, reinterpret_cast<const int32_t *>(c.in + mat_off), al, go, ge,
+                           mode, c.stream, 0, d_res, d_res + 1, d_res + 2);
+    if (s0 != HY_OK) return s0;
+    HY_CK(cudaMemcpyAsync(c.h_stage + 36, reinterpret_cast<const uint8_t *>(c.meta) + 36, 16, cudaMemcpyDeviceToHost,
+                          c.stream));
+    HY_CK(cudaStreamSynchronize(c.stream));
+    int err = 0;
+    memcpy(&err, c.h_stage + 36, 4);
+    if (err) return fail(device_error(err));
+    memcpy(out, c.h_stage + 40, 12);
     float ms = 0.f;
     HY_CK(cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]));
     if (kernel_ms) *kernel_ms += ms;
