@@ -370,7 +370,7 @@ hy_status hy_align_pairs(const uint8_t *q_res, const uint64_t *q_off, const uint
                          hy_search_type search_type, hy_hit *out, uint64_t *failed_pair);
 /* Timing of this thread's last hy_align_pairs call (no reference counterpart): the device time of
  * its kernels (CUDA events around each chunk's packing and pair kernels, plus the long pairs'
- * stripe kernel) and the wall time of the whole call. */
+ * stripe kernel, or a lone long pair's band kernel) and the wall time of the whole call. */
 hy_status hy_align_pairs_timing(double *kernel_ms, double *call_ms);
 /* Phases of this thread's last hy_align_pairs call, in ms (no reference counterpart): up to n of
  * {the host lengths pass and routing, host sort and item packing (summed over chunks), waits for the
