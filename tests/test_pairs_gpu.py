@@ -149,6 +149,21 @@ def test_long_pairs_take_the_stripe_kernel(mode):
     assert got == want
 
 
+@pytest.mark.parametrize("mode", ALL_MODES)
+def test_one_long_pair_among_short_pairs(mode):
+    """Exactly one long pair in a call of many (src/kernel.rs:429-452): it runs on the band kernel
+    inside the chunk pipeline while the short pairs keep the packed kernels; Score and ScoreEnd."""
+    rng = np.random.default_rng(110 + mode)
+    base = list(rng.integers(0, 20, 2500))
+    qs = [list(rng.integers(0, 20, int(rng.integers(1, 200)))) for _ in range(40)]
+    ts = [list(rng.integers(0, 20, int(rng.integers(1, 300)))) for _ in range(40)]
+    qs.insert(17, base[:1500])
+    ts.insert(17, _related(rng, base, 20, 0.3))
+    for st in (0, 1):
+        got, want = run_both(qs, ts, BLOSUM62, 20, 11, 1, mode, st)
+        assert got == want, [(k, got[k], want[k]) for k in range(len(got)) if got[k] != want[k]][:4]
+
+
 def test_single_long_pair_align_pair():
     """The 2000 x 2000 single pair of the single-pair path, every mode."""
     rng = np.random.default_rng(77)
