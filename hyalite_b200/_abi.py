@@ -126,6 +126,7 @@ SIGNATURES = {
     "hy_debug_live_device_allocations": (C.c_int64, []),
     "hy_debug_set_wait_polls": (None, [C.c_int64]),
     "hy_debug_pair_chunks": (C.c_uint64, [_u64p, _u64p, C.c_uint64, _u64p, C.c_uint64]),
+    "hy_debug_band_shape": (None, [C.c_uint32, C.c_int32, C.c_uint64, _i32p]),
     "hy_align_pairs": (_st, [_u8p, _u64p, _u8p, _u64p, C.c_uint64, _i32p, C.c_uint64, C.c_int32,
                              C.c_int32, C.c_int, C.c_int, C.POINTER(HyHit), _u64p]),
     "hy_align_pairs_timing": (_st, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),

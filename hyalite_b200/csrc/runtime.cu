@@ -331,6 +331,21 @@ static BandShape band_shape(const QueryPlan &qp, size_t smem_limit) {
     return sh;
 }
 
+}  // namespace hy
+
+extern "C" void hy_debug_band_shape(uint32_t pass_bytes, int32_t n_passes, uint64_t smem_limit, int32_t out[4]) {
+    hy::QueryPlan qp;
+    qp.pass_bytes = pass_bytes;
+    qp.n_passes = n_passes;
+    const hy::BandShape sh = hy::band_shape(qp, (size_t)smem_limit);
+    out[0] = sh.gprof ? 1 : 0;
+    out[1] = sh.warps;
+    out[2] = sh.blocks;
+    out[3] = (n_passes + sh.warps * sh.blocks - 1) / (sh.warps * sh.blocks);
+}
+
+namespace hy {
+
 // End positions of the single item *item_ptr with the block-cooperative band kernel.
 template <class A>
 static hy_status enqueue_band(const hy_db *db, hy_scratch *sc, const Partition &part,

@@ -250,6 +250,11 @@ void hy_debug_set_wait_polls(int64_t polls);
  * bound (512 MiB) however long and short pairs are ordered. */
 uint64_t hy_debug_pair_chunks(const uint64_t *q_off, const uint64_t *t_off, uint64_t n_pairs,
                               uint64_t *bounds, uint64_t cap);
+/* The launch shape of the end-recovery band kernel (a scan's winner, a long pair) for a query of
+ * n_passes pass slices of pass_bytes each, with smem_limit bytes of shared memory a block: out =
+ * {slices read from global memory (1) or shared memory (0), warps a block, blocks of the cluster,
+ * rounds}. One slice per warp; more passes than one block holds take a cluster of up to 8 blocks. */
+void hy_debug_band_shape(uint32_t pass_bytes, int32_t n_passes, uint64_t smem_limit, int32_t out[4]);
 
 /* ---- batched scan (no reference counterpart: the reference scans one query per call) ---------- */
 

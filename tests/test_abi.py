@@ -173,3 +173,34 @@ def test_align_pairs_chunks_bound_their_residues_however_pairs_are_ordered():
         res = (q_off[b[1:]] - q_off[b[:-1]]) + (t_off[b[1:]] - t_off[b[:-1]])
         assert int(res.max()) <= bound + (1 << 20) + 200, (long_first, k, res.max())
         assert int(res.sum()) == int(q_off[-1] + t_off[-1])
+
+
+def test_band_kernel_launch_shape():
+    """The end-recovery band kernel's launch shape: one pass slice per warp in shared memory (at
+    most 200 KB of slices a block, 32 warps), a cluster of up to 8 blocks when the passes exceed one
+    block, as few rounds as that allows and as few warps as those rounds need; slices larger than
+    the budget read from global memory on one block."""
+    import ctypes as C
+
+    limit = 227 * 1024
+
+    def shape(pass_bytes, n_passes):
+        out = (C.c_int32 * 4)()
+        _abi.lib.hy_debug_band_shape(pass_bytes, n_passes, limit, out)
+        return tuple(out)
+
+    i32_slice, i16_slice = 21 * 256 * 4, 21 * 256 * 8  # 20-letter alphabet, 256-row passes
+    assert shape(i32_slice, 1) == (0, 1, 1, 1)
+    assert shape(i32_slice, 8) == (0, 8, 1, 1)
+    assert shape(i32_slice, 20) == (0, 7, 3, 1)  # a 5000-residue query: a cluster of 3 blocks
+    assert shape(i32_slice, 79) == (0, 5, 8, 2)  # 20,000 rows: two rounds on 8 blocks
+    assert shape(i16_slice, 36) == (0, 3, 8, 2)
+    assert shape(300 * 1024, 5) == (1, 5, 1, 1)  # slices beyond the budget: global memory
+    for pb in (1024, 10 * 1024, i32_slice, i16_slice, 100 * 1024, 200 * 1024):
+        per_block = min(32, (200 * 1024) // pb)
+        for n in range(1, 400, 7):
+            g, w, b, r = shape(pb, n)
+            assert g == 0 and 1 <= b <= 8 and 1 <= w <= per_block
+            assert w * pb + 16 <= limit
+            assert w * b * r >= n and (w - 1) * b * r < n  # every pass placed, no spare warp
+            assert r == -(-n // (min(8, -(-n // per_block)) * per_block)) or n <= per_block
